@@ -1,0 +1,90 @@
+"""ctypes binding of libfdtd_b200.so (include/fdtd_c.h).
+
+There is no fallback: if the library cannot be loaded the import of the solver
+fails with the reason.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+from .scene import GhostFace, Options, SceneDesc, SolverInfo, GaussianSourceDesc
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_lib", "libfdtd_b200.so")
+
+# every symbol include/fdtd_c.h declares
+EXPORTS = [
+    "fdtd_abi_version", "fdtd_last_error", "fdtd_device_count", "fdtd_gaussian_source_defaults",
+    "fdtd_solver_create", "fdtd_solver_destroy", "fdtd_solver_reset", "fdtd_solver_step",
+    "fdtd_solver_step_device", "fdtd_solver_fetch_listeners", "fdtd_solver_info_get",
+    "fdtd_solver_get_classification", "fdtd_solver_get_field", "fdtd_solver_synchronize",
+    "fdtd_solver_stream", "fdtd_solver_last_error", "fdtd_solver_last_launch_count",
+    "fdtd_solver_snapshot", "fdtd_solver_restore", "fdtd_scene_from_xml", "fdtd_scene_desc_get",
+    "fdtd_scene_number_of_steps", "fdtd_scene_output_pattern", "fdtd_scene_free", "fdtd_audio_append",
+]
+
+_lib = None
+
+
+class FDTDError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        from .scene import STATUS
+        super().__init__(f"{STATUS.get(status, status)}: {msg}")
+        self.status = status
+
+
+def load(build_if_missing: bool = False):
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        if build_if_missing:
+            from .build import build
+            build()
+        else:
+            raise ImportError(f"{LIB_PATH} is missing: run `python -m acoustics_b200.build` (nvcc, sm_100a)")
+    L = C.CDLL(LIB_PATH)
+    vp, i32, i64, dbl = C.c_void_p, C.c_int32, C.c_int64, C.c_double
+    sig = {
+        "fdtd_abi_version": ([], i32),
+        "fdtd_last_error": ([], C.c_char_p),
+        "fdtd_device_count": ([C.POINTER(i32)], i32),
+        "fdtd_gaussian_source_defaults": ([C.POINTER(GaussianSourceDesc), dbl], i32),
+        "fdtd_solver_create": ([C.POINTER(SceneDesc), C.POINTER(Options), C.POINTER(vp)], i32),
+        "fdtd_solver_destroy": ([vp], i32),
+        "fdtd_solver_reset": ([vp, dbl], i32),
+        "fdtd_solver_step": ([vp, i32, vp], i32),
+        "fdtd_solver_step_device": ([vp, i32, vp], i32),
+        "fdtd_solver_fetch_listeners": ([vp, vp], i32),
+        "fdtd_solver_info_get": ([vp, C.POINTER(SolverInfo)], i32),
+        "fdtd_solver_get_classification": ([vp, vp, vp, C.POINTER(i64)], i32),
+        "fdtd_solver_get_field": ([vp, i32, vp, i64], i32),
+        "fdtd_solver_synchronize": ([vp], i32),
+        "fdtd_solver_stream": ([vp], vp),
+        "fdtd_solver_last_error": ([vp], C.c_char_p),
+        "fdtd_solver_last_launch_count": ([vp], i64),
+        "fdtd_solver_snapshot": ([vp, vp, C.POINTER(i64)], i32),
+        "fdtd_solver_restore": ([vp, vp, i64], i32),
+        "fdtd_scene_from_xml": ([C.c_char_p, C.POINTER(vp)], i32),
+        "fdtd_scene_desc_get": ([vp], C.POINTER(SceneDesc)),
+        "fdtd_scene_number_of_steps": ([vp], i32),
+        "fdtd_scene_output_pattern": ([vp], C.c_char_p),
+        "fdtd_scene_free": ([vp], None),
+        "fdtd_audio_append": ([C.c_char_p, vp, i64], i32),
+    }
+    for name, (args, res) in sig.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def check(status: int, handle=None) -> int:
+    """Raise FDTDError for negative status codes; return the status otherwise."""
+    if status < 0:
+        L = load()
+        msg = L.fdtd_solver_last_error(handle) if handle else L.fdtd_last_error()
+        raise FDTDError(status, (msg or b"").decode(errors="replace"))
+    return status

@@ -1,0 +1,624 @@
+// fdtd_api.cpp — the C-ABI of include/fdtd_c.h: solver lifecycle, the
+// host-side FP64 geometry (computed with the reference's own expressions and
+// operation order, -ffp-contract=off), classification driver, step loop with
+// CUDA graphs, read-back, snapshot/restore.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <limits>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/fdtd_c.h"
+#include "fdtd_device.cuh"
+#include "fdtd_geometry.cuh"
+#include "fdtd_internal.hpp"
+#include "fdtd_launch.hpp"
+
+using namespace fdtd;
+
+namespace {
+thread_local std::string g_last_error;
+const double EPS = 1e-10;                  // src/config.h:45
+const double GAUSSIAN_CHECK_BOUND = 2.0;   // Wavesolver_ConstantsAndTypes.h:77
+}  // namespace
+
+namespace fdtd {
+void set_error(fdtd_solver* s, const std::string& msg) {
+    g_last_error = msg;
+    if (s) s->err = msg;
+}
+}  // namespace fdtd
+
+#define CUDA_TRY(s, expr)                                                                         \
+    do {                                                                                          \
+        cudaError_t _e = (expr);                                                                  \
+        if (_e != cudaSuccess) {                                                                  \
+            set_error((s), std::string("CUDA: ") + cudaGetErrorString(_e) + " at " #expr);       \
+            return _e == cudaErrorMemoryAllocation ? FDTD_ERR_OOM : FDTD_ERR_CUDA;                \
+        }                                                                                         \
+    } while (0)
+
+// ---------------------------------------------------------------------------
+// Host geometry (FP64, reference expressions)
+// ---------------------------------------------------------------------------
+namespace fdtd {
+
+// MAC_Grid::PML_absorptionCoefficient, quadratic profile, preset 0 (MAC_Grid.cpp:4064-4090);
+// pow(x,2) written as x*x (the compiler folds it identically without fast-math).
+static double absorption(double x, double mn, double mx, double w, double S) {
+    const double hMin = x - mn, hMax = mx - x;
+    const double a2 = w * w;
+    const double distMin = w - hMin, distMax = w - hMax;
+    if (hMin <= w) return S * (distMin * distMin) / a2;
+    if (hMax <= w) return S * (distMax * distMax) / a2;
+    return 0.0;
+}
+
+// one dimension of MAC_Grid::InsidePML (MAC_Grid.cpp:4027-4062)
+static bool inside_pml_1d(double x, double mn, double mx, double w) {
+    const double pmlWidth = w + 1E-12;
+    return (x - mn) <= pmlWidth || (mx - x) <= pmlWidth;
+}
+
+void host_object_pose(HostObject& o, double t) {
+    for (int a = 0; a < 3; ++a) {
+        if (o.d.motion == FDTD_MOTION_BALLISTIC)
+            o.c[a] = o.d.center[a] + o.d.velocity[a] * t + 0.5 * o.d.gravity[a] * t * t;
+        else
+            o.c[a] = o.d.center[a];
+    }
+}
+
+static void half_extent(const HostObject& o, double e[3]) {
+    for (int i = 0; i < 3; ++i) {
+        if (o.d.shape == FDTD_SHAPE_SPHERE) { e[i] = o.d.size[0]; continue; }
+        double s = 0.0;
+        for (int j = 0; j < 3; ++j) {
+            const double rij = o.d.rotation[i * 3 + j];
+            if (o.d.shape == FDTD_SHAPE_BOX) s = s + std::fabs(rij) * o.d.size[j];
+            else s = s + (rij * o.d.size[j]) * (rij * o.d.size[j]);
+        }
+        e[i] = (o.d.shape == FDTD_SHAPE_BOX) ? s : std::sqrt(s);
+    }
+}
+
+// FDTD_RigidObject::UpdateBoundingBox (FDTD_RigidObject.cpp:190-226) with the
+// BoundingBox::Update / Union arithmetic of FDTD_MovableObject.h:81-99
+void host_update_bbox(HostObject& o) {
+    for (int d = 0; d < 3; ++d) { o.umin[d] = o.bmin[d]; o.umax[d] = o.bmax[d]; }
+    double e[3];
+    half_extent(o, e);
+    for (int d = 0; d < 3; ++d) { o.bmin[d] = o.c[d] - e[d]; o.bmax[d] = o.c[d] + e[d]; }
+    for (int d = 0; d < 3; ++d) {
+        o.umin[d] = std::min(o.bmin[d], o.umin[d]);
+        o.umax[d] = std::max(o.bmax[d], o.umax[d]);
+    }
+}
+
+void host_reset_union(HostObject& o) {
+    for (int d = 0; d < 3; ++d) { o.umin[d] = o.bmin[d]; o.umax[d] = o.bmax[d]; }
+}
+
+static void to_dev_object(const HostObject& o, DevObject& d) {
+    std::memset(&d, 0, sizeof(d));
+    d.shape = o.d.shape;
+    d.accel_kind = o.d.accel_kind;
+    d.motion = o.d.motion;
+    for (int i = 0; i < 3; ++i) {
+        d.c[i] = o.c[i];
+        d.size[i] = o.d.size[i];
+        d.bmin[i] = o.bmin[i];
+        d.bmax[i] = o.bmax[i];
+        d.bdim[i] = o.bmax[i] - o.bmin[i];
+        d.bcen[i] = (o.bmax[i] + o.bmin[i]) / 2.0;
+        d.dir[i] = o.d.accel_dir[i];
+    }
+    for (int i = 0; i < 9; ++i) d.R[i] = o.d.rotation[i];
+    d.amp = o.d.accel_amplitude;
+    d.t0 = o.d.accel_t0;
+    d.tau = o.d.accel_tau;
+}
+
+void to_dev_objects(fdtd_solver* s) {
+    for (size_t i = 0; i < s->objs.size(); ++i) to_dev_object(s->objs[i], s->hP.obj[i]);
+}
+
+// ScalarField::GetIterationBox (ScalarField.cpp:288-314), clamped to the grid
+static void iteration_box(const fdtd_solver* s, double mn[3], double mx[3], int start[3], int range[3]) {
+    auto inside = [&](const double* x) {
+        return x[0] >= s->bmin[0] && x[1] >= s->bmin[1] && x[2] >= s->bmin[2] && x[0] <= s->bmax[0] &&
+               x[1] <= s->bmax[1] && x[2] <= s->bmax[2];
+    };
+    const double imn[3] = {mn[0], mn[1], mn[2]}, imx[3] = {mx[0], mx[1], mx[2]};
+    if (!inside(imn)) for (int d = 0; d < 3; ++d) mn[d] = std::max(s->bmin[d], mn[d]);
+    if (!inside(imx)) for (int d = 0; d < 3; ++d) mx[d] = std::min(s->bmax[d], mx[d]);
+    for (int d = 0; d < 3; ++d) {
+        start[d] = (int)std::floor((mn[d] - s->bmin[d]) / s->h);
+        const int end = (int)std::ceil((mx[d] - s->bmin[d]) / s->h);
+        range[d] = std::max(end - start[d], 1);
+        if (start[d] < 0) { range[d] += start[d]; start[d] = 0; }
+        if (start[d] + range[d] > s->N[d]) range[d] = s->N[d] - start[d];
+        if (range[d] < 0) range[d] = 0;
+    }
+}
+
+// The object and constraint boxes that classifyCells_FAST iterates (MAC_Grid.cpp:3510-3551)
+void classification_boxes(const fdtd_solver* s, std::vector<std::array<int, 6>>& boxes) {
+    boxes.clear();
+    for (const auto& o : s->objs) {
+        double mn[3] = {o.umin[0], o.umin[1], o.umin[2]}, mx[3] = {o.umax[0], o.umax[1], o.umax[2]};
+        for (const auto& pl : s->planes) {
+            if (pl.normal_sign > 0) mn[pl.normal_dir] = std::max(mn[pl.normal_dir], pl.height);
+            else mx[pl.normal_dir] = std::min(mx[pl.normal_dir], pl.height);
+        }
+        int st[3], rg[3];
+        iteration_box(s, mn, mx, st, rg);
+        boxes.push_back({st[0], st[1], st[2], rg[0], rg[1], rg[2]});
+    }
+    for (const auto& pl : s->planes) {
+        const double NEG_INF = std::numeric_limits<double>::lowest(), POS_INF = std::numeric_limits<double>::max();
+        double mn[3] = {NEG_INF, NEG_INF, NEG_INF}, mx[3] = {POS_INF, POS_INF, POS_INF};
+        if (pl.normal_sign > 0) mx[pl.normal_dir] = pl.height;
+        else mn[pl.normal_dir] = pl.height;
+        int st[3], rg[3];
+        iteration_box(s, mn, mx, st, rg);
+        boxes.push_back({st[0], st[1], st[2], rg[0], rg[1], rg[2]});
+    }
+}
+
+}  // namespace fdtd
+
+// ---------------------------------------------------------------------------
+// device memory
+// ---------------------------------------------------------------------------
+namespace {
+
+size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+struct Carver {
+    size_t off = 0;
+    std::vector<std::pair<void**, size_t>> req;
+    void add(void** p, size_t bytes) {
+        req.push_back({p, off});
+        off += align256(bytes);
+    }
+};
+
+fdtd_status upload_params(fdtd_solver* s) {
+    CUDA_TRY(s, cudaMemcpyAsync(s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice, s->stream));
+    return FDTD_OK;
+}
+
+fdtd_status run_classification(fdtd_solver* s) {
+    std::vector<std::array<int, 6>> boxes;
+    classification_boxes(s, boxes);
+    CUDA_TRY(s, launch_cls_reset(s->dP, s->ncell, s->stream));
+    s->launches++;
+    for (const auto& b : boxes) {
+        const int st[3] = {b[0], b[1], b[2]}, rg[3] = {b[3], b[4], b[5]};
+        CUDA_TRY(s, launch_cls_solid(s->dP, st, rg, s->stream));
+        s->launches++;
+    }
+    CUDA_TRY(s, launch_cls_ghost(s->dP, s->ncell, s->stream));
+    s->launches++;
+    return FDTD_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// create / reset
+// ---------------------------------------------------------------------------
+namespace fdtd {
+
+fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
+    s->h = sc->cell_size;
+    s->c = sc->sound_speed;
+    s->rho = sc->density;
+    s->k = sc->time_step;
+    s->end_time = sc->end_time;
+    // BoundingBox(cellSize, divisions, center) (BoundingBox.h:89-99) -> ScalarField (ScalarField.cpp:29-50)
+    for (int d = 0; d < 3; ++d) {
+        const double mn = sc->domain_center[d] - s->h * (double)sc->divisions[d] / 2.0;
+        const double mx = sc->domain_center[d] + s->h * (double)sc->divisions[d] / 2.0;
+        s->N[d] = (int)std::ceil(((mx - mn) - EPS) / s->h);
+        s->bmin[d] = mn;
+        s->bmax[d] = s->bmin[d];
+        s->bmax[d] += s->h * (double)s->N[d];
+    }
+    s->ncell = (long long)s->N[0] * s->N[1] * s->N[2];
+    const double w = sc->pml_width * s->h;  // setPMLBoundaryWidth (MAC_Grid.cpp:146-150)
+    const double S = sc->pml_strength;
+    const double one_over_k = 1.0 / s->k;
+    for (int d = 0; d < 3; ++d) {
+        const int n = s->N[d];
+        auto& T = s->tab[d];
+        T.pml_cell.assign(n, 0);
+        T.pml_face.assign(n + 1, 0);
+        T.cpos.assign(n, 0.0);
+        T.fpos.assign(n + 1, 0.0);
+        T.pupd.assign(n, 0.0);
+        T.pdiv.assign(n, 0.0);
+        T.vupd.assign(n + 1, 0.0);
+        T.vgrad.assign(n + 1, 0.0);
+        for (int i = 0; i < n; ++i) {
+            double p = s->bmin[d];
+            p += (0.5 + (double)i) * s->h;  // ScalarField::cellPosition (ScalarField.cpp:131-140)
+            T.cpos[i] = p;
+            T.pml_cell[i] = inside_pml_1d(p, s->bmin[d], s->bmax[d], w);
+            const double sigma = absorption(p, s->bmin[d], s->bmax[d], w, S);
+            const double directional = one_over_k + sigma / 2.0;           // MAC_Grid.h:550-553
+            T.pupd[i] = (1.0 / s->k - sigma / 2.0) / directional;          // MAC_Grid.h:558-561
+            T.pdiv[i] = (-1.0 * s->rho * s->c * s->c / directional);       // MAC_Grid.h:566-569
+        }
+        const double vmin = s->bmin[d] - s->h / 2.0;  // MAC_Grid.cpp:103-113
+        for (int i = 0; i <= n; ++i) {
+            double p = vmin;
+            p += (0.5 + (double)i) * s->h;
+            T.fpos[i] = p;
+            T.pml_face[i] = inside_pml_1d(p, s->bmin[d], s->bmax[d], w);
+            const double sigma = absorption(p, s->bmin[d], s->bmax[d], w, S);
+            double u = 1.0 / s->k - sigma / 2.0;  // MAC_Grid.h:530-536
+            u /= 1.0 / s->k + sigma / 2.0;
+            T.vupd[i] = u;
+            double g = 1.0 / s->k + sigma / 2.0;  // MAC_Grid.h:541-547
+            g *= s->rho * s->h;
+            T.vgrad[i] = -1.0 / g;
+        }
+    }
+    // PML / interior counts
+    long long inner = 1;
+    for (int d = 0; d < 3; ++d) {
+        long long m = 0;
+        for (int i = 0; i < s->N[d]; ++i) m += s->tab[d].pml_cell[i] ? 0 : 1;
+        inner *= m;
+    }
+    s->n_interior = inner;
+    s->n_pml = s->ncell - inner;
+    return FDTD_OK;
+}
+
+}  // namespace fdtd
+
+static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
+    if (!sc) return (set_error(nullptr, "scene is NULL"), FDTD_ERR_INVALID_ARG);
+    if (!(sc->cell_size > 0) || !(sc->time_step > 0) || !(sc->sound_speed > 0) || !(sc->density > 0))
+        return (set_error(nullptr, "cell_size, time_step, sound_speed and density must be positive"), FDTD_ERR_INVALID_ARG);
+    for (int d = 0; d < 3; ++d)
+        if (sc->divisions[d] < 4 || sc->divisions[d] > 4096)
+            return (set_error(nullptr, "divisions must lie in [4, 4096]"), FDTD_ERR_INVALID_ARG);
+    if ((long long)sc->divisions[0] * sc->divisions[1] * sc->divisions[2] >= (1LL << 31))
+        return (set_error(nullptr, "grid has 2^31 cells or more (flat index is int32, as ScalarField)"), FDTD_ERR_INVALID_ARG);
+    if (sc->boundary_condition_preset != 0)
+        return (set_error(nullptr, "boundary_condition_preset other than 0 (Engquist walls) is not on this path"), FDTD_ERR_UNSUPPORTED);
+    if (sc->pml_width < 1.5)
+        return (set_error(nullptr, "PML width below 1.5 cells reaches the Engquist-Majda branch (MAC_Grid.cpp:533-920)"), FDTD_ERR_UNSUPPORTED);
+    if (sc->air_viscosity_alpha != 0.0)
+        return (set_error(nullptr, "air viscosity (alpha > 0) is not on this path"), FDTD_ERR_UNSUPPORTED);
+    if (sc->n_objects < 0 || sc->n_objects > FDTD_MAX_OBJECTS)
+        return (set_error(nullptr, "too many objects (max " + std::to_string(FDTD_MAX_OBJECTS) + ")"), FDTD_ERR_INVALID_ARG);
+    if (sc->n_sources < 0 || sc->n_sources > FDTD_MAX_SOURCES)
+        return (set_error(nullptr, "too many pressure sources (max " + std::to_string(FDTD_MAX_SOURCES) + ")"), FDTD_ERR_INVALID_ARG);
+    if (sc->n_constraints < 0 || sc->n_constraints > 4)
+        return (set_error(nullptr, "too many plane constraints (max 4)"), FDTD_ERR_INVALID_ARG);
+    if (sc->n_listeners < 0 || (sc->n_listeners > 0 && !sc->listeners))
+        return (set_error(nullptr, "listener array missing"), FDTD_ERR_INVALID_ARG);
+    if ((sc->n_objects > 0 && !sc->objects) || (sc->n_sources > 0 && !sc->sources) ||
+        (sc->n_constraints > 0 && !sc->constraints))
+        return (set_error(nullptr, "scene array missing"), FDTD_ERR_INVALID_ARG);
+    for (int i = 0; i < sc->n_objects; ++i) {
+        const auto& o = sc->objects[i];
+        if (o.shape < 0 || o.shape > 2) return (set_error(nullptr, "unknown object shape"), FDTD_ERR_INVALID_ARG);
+        if (o.accel_kind == FDTD_ACCEL_GAUSSIAN_PULSATION && o.shape != FDTD_SHAPE_SPHERE)
+            return (set_error(nullptr, "pulsating acceleration is defined for spheres only"), FDTD_ERR_UNSUPPORTED);
+        if (o.motion == FDTD_MOTION_BALLISTIC && o.shape == FDTD_SHAPE_ELLIPSOID)
+            return (set_error(nullptr, "moving ellipsoids are not supported (no closest-point query)"), FDTD_ERR_UNSUPPORTED);
+        if (o.accel_kind != FDTD_ACCEL_NONE && !(o.accel_tau > 0))
+            return (set_error(nullptr, "accel_tau must be positive"), FDTD_ERR_INVALID_ARG);
+        for (int d = 0; d < 3; ++d)
+            if ((o.shape != FDTD_SHAPE_SPHERE || d == 0) && !(o.size[d] > 0))
+                return (set_error(nullptr, "object size must be positive"), FDTD_ERR_INVALID_ARG);
+    }
+    for (int i = 0; i < sc->n_sources; ++i)
+        if (!(sc->sources[i].width_time > 0)) return (set_error(nullptr, "source_width_time must be positive"), FDTD_ERR_INVALID_ARG);
+    return FDTD_OK;
+}
+
+extern "C" {
+
+int32_t fdtd_abi_version(void) { return FDTD_ABI_VERSION; }
+
+const char* fdtd_last_error(void) { return g_last_error.c_str(); }
+
+fdtd_status fdtd_device_count(int32_t* count) {
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess) {
+        *count = 0;
+        set_error(nullptr, cudaGetErrorString(e));
+        return FDTD_ERR_CUDA;
+    }
+    *count = n;
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_gaussian_source_defaults(fdtd_gaussian_source_desc* src, double sound_speed) {
+    if (!src) return FDTD_ERR_INVALID_ARG;
+    // ImpulseResponseParser.cpp:660-663
+    if (src->width_space <= 0) src->width_space = sound_speed * src->width_time;
+    if (src->normalize_constant == 0)
+        src->normalize_constant = 1.0 / std::pow(std::sqrt(2.0 * M_PI) * src->width_space, 3);
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* opt, fdtd_solver** out) {
+    if (!out) return (set_error(nullptr, "out is NULL"), FDTD_ERR_INVALID_ARG);
+    *out = nullptr;
+    fdtd_status st = validate_scene(sc);
+    if (st != FDTD_OK) return st;
+    fdtd_options o{};
+    if (opt) o = *opt;
+    if (o.precision != FDTD_PRECISION_FP64 && o.precision != FDTD_PRECISION_FP32_COMPENSATED)
+        return (set_error(nullptr, "unknown precision"), FDTD_ERR_INVALID_ARG);
+    if (o.kernel == FDTD_KERNEL_PHASED && o.precision != FDTD_PRECISION_FP64)
+        return (set_error(nullptr, "the phased kernel path is FP64 only"), FDTD_ERR_INVALID_ARG);
+    if (o.graph_steps < 0 || (o.graph_steps % 2) != 0)
+        return (set_error(nullptr, "graph_steps must be a non-negative even number"), FDTD_ERR_INVALID_ARG);
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return (set_error(nullptr, "no CUDA device visible"), FDTD_ERR_CUDA);
+    if (o.device < 0 || o.device >= ndev) return (set_error(nullptr, "device ordinal out of range"), FDTD_ERR_INVALID_ARG);
+
+    std::unique_ptr<fdtd_solver> s(new fdtd_solver());
+    s->opt = o;
+    s->precision = o.precision;
+    CUDA_TRY(nullptr, cudaSetDevice(o.device));
+    CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    solver_init_geometry(s.get(), sc);
+    for (int i = 0; i < sc->n_objects; ++i) {
+        HostObject h;
+        h.d = sc->objects[i];
+        s->objs.push_back(h);
+        if (h.d.motion != FDTD_MOTION_STATIC) s->moving = true;
+    }
+    for (int i = 0; i < sc->n_constraints; ++i) s->planes.push_back(sc->constraints[i]);
+    for (int i = 0; i < sc->n_sources; ++i) {
+        fdtd_gaussian_source_desc g = sc->sources[i];
+        fdtd_gaussian_source_defaults(&g, s->c);
+        s->sources.push_back(g);
+    }
+    s->listeners.assign(sc->listeners, sc->listeners + 3 * (size_t)sc->n_listeners);
+    s->L = sc->n_listeners;
+    s->start_time = sc->start_time;
+
+    // ---- device arena ----
+    const size_t w = s->precision == FDTD_PRECISION_FP64 ? 8 : 4;
+    const long long n = s->ncell;
+    const int* N = s->N;
+    SolveParams& P = s->hP;
+    std::memset(&P, 0, sizeof(P));
+    Carver cv;
+    void* dummy[64];
+    int di = 0;
+    cv.add((void**)&s->dP, sizeof(SolveParams));
+    cv.add((void**)&P.cls, n);
+    cv.add((void**)&P.gobj, n);
+    cv.add(&P.p[0], n * w);
+    cv.add(&P.p[1], n * w);
+    if (s->precision != FDTD_PRECISION_FP64) cv.add((void**)&P.dinc, n * 4);
+    for (int d = 0; d < 3; ++d) cv.add(&P.pd[d], n * w);
+    for (int d = 0; d < 3; ++d) {
+        const long long nf = (long long)(N[0] + (d == 0)) * (N[1] + (d == 1)) * (N[2] + (d == 2));
+        s->vcount[d] = nf;
+        cv.add(&P.v[0][d], nf * w);
+        if (o.kernel == FDTD_KERNEL_FUSED) cv.add(&P.v[1][d], nf * w);
+    }
+    if (o.kernel == FDTD_KERNEL_PHASED) cv.add((void**)&s->d_lap, n * 8);
+    cv.add((void**)&P.clock, 8);
+    cv.add((void**)&P.consts, sizeof(StepConsts));
+    cv.add((void**)&s->d_status, 16);
+    cv.add((void**)&P.listeners, std::max<size_t>(1, s->listeners.size()) * 8);
+    for (int d = 0; d < 3; ++d) {
+        cv.add((void**)&P.pml_cell[d], N[d]);
+        cv.add((void**)&P.pml_face[d], N[d] + 1);
+        cv.add((void**)&P.cpos[d], N[d] * 8);
+        cv.add((void**)&P.fpos[d], (N[d] + 1) * 8);
+        cv.add((void**)&P.pupd[d], N[d] * 8);
+        cv.add((void**)&P.pdiv[d], N[d] * 8);
+        cv.add((void**)&P.vupd[d], (N[d] + 1) * 8);
+        cv.add((void**)&P.vgrad[d], (N[d] + 1) * 8);
+        cv.add((void**)&P.pupd_f[d], N[d] * 4);
+        cv.add((void**)&P.pdiv_f[d], N[d] * 4);
+        cv.add((void**)&P.vupd_f[d], (N[d] + 1) * 4);
+        cv.add((void**)&P.vgrad_f[d], (N[d] + 1) * 4);
+    }
+    (void)dummy;
+    (void)di;
+    s->lis_cap_steps = std::max(256, o.graph_steps);
+    cv.add((void**)&s->d_lis, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8);
+    void* base = nullptr;
+    cudaError_t e = cudaMalloc(&base, cv.off);
+    if (e != cudaSuccess) {
+        set_error(nullptr, std::string("cudaMalloc of ") + std::to_string(cv.off) + " bytes failed: " + cudaGetErrorString(e));
+        cudaStreamDestroy(s->stream);
+        return FDTD_ERR_OOM;
+    }
+    s->arena = base;
+    s->arena_bytes = cv.off;
+    for (auto& r : cv.req) *r.first = (char*)base + r.second;
+
+    // ---- constants ----
+    for (int d = 0; d < 3; ++d) {
+        P.N[d] = N[d];
+        P.bmin[d] = s->bmin[d];
+        for (int e2 = 0; e2 < 3; ++e2) P.vN[d][e2] = N[e2] + (d == e2 ? 1 : 0);
+        P.vcount[d] = s->vcount[d];
+    }
+    P.ncell = n;
+    P.h = s->h;
+    P.inv_h = 1.0 / s->h;
+    P.rho = s->rho;
+    P.c = s->c;
+    P.k = s->k;
+    P.c2k2 = (s->c * s->k) * (s->c * s->k);
+    P.lap_scale = 1.0 / (s->h * s->h);
+    P.q = 0.75 * s->h;
+    P.quarter_h = 0.25 * s->h;
+    P.n_obj = (int)s->objs.size();
+    P.n_plane = (int)s->planes.size();
+    P.n_src = (int)s->sources.size();
+    P.n_lis = s->L;
+    P.precision = s->precision;
+    for (int i = 0; i < P.n_plane; ++i) {
+        P.plane[i].dir = s->planes[i].normal_dir;
+        P.plane[i].sign = s->planes[i].normal_sign;
+        P.plane[i].height = s->planes[i].height;
+    }
+    for (int i = 0; i < P.n_src; ++i) {
+        const auto& g = s->sources[i];
+        DevSource& D = P.src[i];
+        // GaussianPressureSource bbox (GaussianPressureSource.h:34-37) and centroid (FDTD_MovableObject.h:54-58)
+        for (int d = 0; d < 3; ++d) {
+            D.bmin[d] = g.position[d] - g.width_space * GAUSSIAN_CHECK_BOUND;
+            D.bmax[d] = g.position[d] + g.width_space * GAUSSIAN_CHECK_BOUND;
+            D.cen[d] = (D.bmax[d] + D.bmin[d]) / 2.0;
+        }
+        D.denom = 2.0 * g.width_space * g.width_space;
+        D.t0 = g.offset_time;
+        D.wt = g.width_time;
+        D.scale = 1. / 3.6836 * g.normalize_constant;
+    }
+    // tables
+    for (int d = 0; d < 3; ++d) {
+        auto& T = s->tab[d];
+        std::vector<float> f1(T.pupd.begin(), T.pupd.end()), f2(T.pdiv.begin(), T.pdiv.end());
+        std::vector<float> f3(T.vupd.begin(), T.vupd.end()), f4(T.vgrad.begin(), T.vgrad.end());
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pml_cell[d], T.pml_cell.data(), N[d], cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pml_face[d], T.pml_face.data(), N[d] + 1, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.cpos[d], T.cpos.data(), N[d] * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.fpos[d], T.fpos.data(), (N[d] + 1) * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pupd[d], T.pupd.data(), N[d] * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pdiv[d], T.pdiv.data(), N[d] * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.vupd[d], T.vupd.data(), (N[d] + 1) * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.vgrad[d], T.vgrad.data(), (N[d] + 1) * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pupd_f[d], f1.data(), N[d] * 4, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pdiv_f[d], f2.data(), N[d] * 4, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.vupd_f[d], f3.data(), (N[d] + 1) * 4, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.vgrad_f[d], f4.data(), (N[d] + 1) * 4, cudaMemcpyHostToDevice));
+    }
+    if (s->L > 0)
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.listeners, s->listeners.data(), s->listeners.size() * 8, cudaMemcpyHostToDevice));
+    CUDA_TRY(s.get(), cudaMallocHost((void**)&s->h_lis_stage, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8));
+    // tile choice: 8 rows; x chunk so that the grid has >= 4 waves on 148 SMs
+    s->tile_y = o.tile_y > 0 ? o.tile_y : 8;
+    if (o.x_chunk > 0) s->xchunk = o.x_chunk;
+    else {
+        const long long cols = (long long)((N[2] + 31) / 32) * ((N[1] + s->tile_y - 1) / s->tile_y);
+        long long chunks = (148LL * 8 + cols - 1) / cols;
+        if (chunks < 1) chunks = 1;
+        int xc = (int)((N[0] + chunks - 1) / chunks);
+        if (xc < 4) xc = 4;
+        s->xchunk = xc;
+    }
+    st = fdtd_solver_reset(s.get(), sc->start_time);
+    if (st != FDTD_OK) return st;
+    *out = s.release();
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_solver_destroy(fdtd_solver* s) {
+    if (!s) return FDTD_OK;
+    cudaSetDevice(s->opt.device);
+    cudaStreamSynchronize(s->stream);
+    for (int i = 0; i < 2; ++i)
+        if (s->graph_exec[i]) cudaGraphExecDestroy(s->graph_exec[i]);
+    if (s->arena) cudaFree(s->arena);
+    if (s->h_lis_stage) cudaFreeHost(s->h_lis_stage);
+    cudaStreamDestroy(s->stream);
+    delete s;
+    return FDTD_OK;
+}
+
+// PML_WaveSolver::Reinitialize_PML_WaveSolver(true, t0) (PML_WaveSolver.cpp:102-146)
+// + FDTD_AcousticSimulator::ResetStartTime (FDTD_AcousticSimulator.cpp:458-523)
+fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
+    if (!s) return FDTD_ERR_INVALID_ARG;
+    CUDA_TRY(s, cudaSetDevice(s->opt.device));
+    SolveParams& P = s->hP;
+    const size_t w = s->precision == FDTD_PRECISION_FP64 ? 8 : 4;
+    // zero all state (fields, velocities, split pressures, flags)
+    CUDA_TRY(s, cudaMemsetAsync(P.p[0], 0, s->ncell * w, s->stream));
+    CUDA_TRY(s, cudaMemsetAsync(P.p[1], 0, s->ncell * w, s->stream));
+    if (P.dinc) CUDA_TRY(s, cudaMemsetAsync(P.dinc, 0, s->ncell * 4, s->stream));
+    for (int d = 0; d < 3; ++d) {
+        CUDA_TRY(s, cudaMemsetAsync(P.pd[d], 0, s->ncell * w, s->stream));
+        CUDA_TRY(s, cudaMemsetAsync(P.v[0][d], 0, s->vcount[d] * w, s->stream));
+        if (P.v[1][d]) CUDA_TRY(s, cudaMemsetAsync(P.v[1][d], 0, s->vcount[d] * w, s->stream));
+    }
+    // initFieldRasterized: every cell bulk with valid history (MAC_Grid.cpp:2459-2470, :4170-4180)
+    CUDA_TRY(s, cudaMemsetAsync(P.cls, CLS_BULK | CLS_VALID, s->ncell, s->stream));
+    CUDA_TRY(s, cudaMemsetAsync(P.gobj, GOBJ_NONE, s->ncell, s->stream));
+    CUDA_TRY(s, cudaMemsetAsync(P.consts, 0, sizeof(StepConsts), s->stream));
+    CUDA_TRY(s, cudaMemsetAsync(s->d_status, 0, 16, s->stream));
+    s->time = t0;
+    s->state_time = t0;
+    s->step_index = 0;
+    s->cur = 0;
+    for (auto& o : s->objs) {
+        host_object_pose(o, t0);
+        host_update_bbox(o);
+        host_reset_union(o);
+    }
+    for (size_t i = 0; i < s->objs.size(); ++i) to_dev_object(s->objs[i], P.obj[i]);
+    s->n_solid_pml = 0;
+    P.solid_pml = nullptr;
+    P.n_solid_pml = 0;
+    fdtd_status st = upload_params(s);
+    if (st != FDTD_OK) return st;
+    CUDA_TRY(s, cudaMemcpyAsync(P.clock, &s->time, 8, cudaMemcpyHostToDevice, s->stream));
+    s->launches = 0;
+    st = run_classification(s);
+    if (st != FDTD_OK) return st;
+    // ResetCellHistory(true): every cell has a valid history after reset
+    // (the classification kernels keep it in bit 6; re-set it on all cells)
+    std::vector<uint8_t> cls(s->ncell);
+    CUDA_TRY(s, cudaMemcpyAsync(cls.data(), P.cls, s->ncell, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    std::vector<int> solid_pml;
+    for (long long c = 0; c < s->ncell; ++c) {
+        cls[c] |= CLS_VALID;
+        if (!(cls[c] & CLS_BULK)) {
+            const int i = (int)(c / ((long long)s->N[1] * s->N[2]));
+            const int j = (int)((c / s->N[2]) % s->N[1]);
+            const int k = (int)(c % s->N[2]);
+            if (s->tab[0].pml_cell[i] || s->tab[1].pml_cell[j] || s->tab[2].pml_cell[k]) solid_pml.push_back((int)c);
+        }
+    }
+    CUDA_TRY(s, cudaMemcpy(P.cls, cls.data(), s->ncell, cudaMemcpyHostToDevice));
+    if (s->d_solid_pml) {
+        cudaFree(s->d_solid_pml);
+        s->d_solid_pml = nullptr;
+    }
+    if (!solid_pml.empty() && !s->moving) {
+        CUDA_TRY(s, cudaMalloc((void**)&s->d_solid_pml, solid_pml.size() * sizeof(int)));
+        CUDA_TRY(s, cudaMemcpy(s->d_solid_pml, solid_pml.data(), solid_pml.size() * sizeof(int), cudaMemcpyHostToDevice));
+        P.solid_pml = s->d_solid_pml;
+        P.n_solid_pml = (int)solid_pml.size();
+        s->n_solid_pml = P.n_solid_pml;
+    }
+    st = upload_params(s);
+    if (st != FDTD_OK) return st;
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    for (int i = 0; i < 2; ++i) {
+        if (s->graph_exec[i]) cudaGraphExecDestroy(s->graph_exec[i]);
+        s->graph_exec[i] = nullptr;
+    }
+    return FDTD_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,116 @@
+// fdtd_device.cuh — device-side data layout and helpers shared by the FP64 and
+// FP32 kernel translation units.
+//
+// HBM layout of one solve (all arrays 256-byte aligned, flat index
+// i*Ny*Nz + j*Nz + k, z contiguous as in ScalarField.cpp:86-97):
+//   cls[N]      u8   bit7 bulk, bit6 valid history, bits0-5 solid-neighbour mask
+//                    (bit 2d: -d side, bit 2d+1: +d side)
+//   gobj[N]     u8   for solid cells: closest object (LowestObjectDistance) | 0x80 constraint
+//   p[2][N]     T    pressure ping-pong (FP64: p^n and p^{n-1}, p^{n+1} overwrites p^{n-1};
+//                    FP32: p^n and p^{n+1})
+//   dinc[N]     f32  FP32 only: increment p^n - p^{n-1} (compensated accumulation)
+//   pd[3][N]    T    PML split pressures (touched on PML cells only)
+//   v[2][3][Nf] T    face velocities, double-buffered (touched on PML faces only)
+// Per-axis tables replace the reference's per-cell PML coefficient lists
+// (MAC_Grid.cpp:2495-2523, :2653-2677): every coefficient depends on one
+// coordinate only.
+#pragma once
+#include <cstdint>
+
+#ifndef FDTD_MAX_OBJECTS
+#define FDTD_MAX_OBJECTS 8
+#endif
+#ifndef FDTD_MAX_SOURCES
+#define FDTD_MAX_SOURCES 4
+#endif
+
+namespace fdtd {
+
+constexpr uint8_t CLS_BULK = 0x80;
+constexpr uint8_t CLS_VALID = 0x40;
+constexpr uint8_t CLS_MASK = 0x3F;
+constexpr uint8_t GOBJ_CONSTRAINT = 0x80;
+constexpr uint8_t GOBJ_NONE = 0x7F;
+
+struct DevObject {
+    int shape, accel_kind, motion, _pad;
+    double c[3];        // current centre
+    double R[9];        // object->world rotation, row-major
+    double size[3];
+    double bmin[3], bmax[3], bdim[3], bcen[3];  // _bboxWorld
+    double amp, t0, tau, dir[3];
+};
+
+struct DevPlane {
+    int dir, sign;
+    double height;
+};
+
+struct DevSource {
+    double cen[3];       // _bboxWorld.centroid
+    double bmin[3], bmax[3];
+    double denom;        // 2*w*w
+    double t0, wt;       // offset, width in time
+    double scale;        // (1/3.6836) * normalize constant
+};
+
+// Written by the step prologue, read by the rest of the step.
+struct StepConsts {
+    double t;                       // simulation time at the start of the step
+    double src_tf[FDTD_MAX_SOURCES];  // exp(-((t+k/2 - t0)/wt)^2/2)
+    int64_t step;
+    int32_t error;                  // sticky device-side error flags
+    int32_t _pad;
+};
+
+struct SolveParams {
+    int N[3];
+    int vN[3][3];         // velocity grid divisions per face orientation
+    long long ncell;
+    long long vcount[3];
+    double h, inv_h, rho, c, k;
+    double c2k2;          // (c k)^2
+    double lap_scale;     // 1/(h*h)
+    double q;             // 0.75*h  (ghost extrapolation distance, MAC_Grid.cpp:1281)
+    double quarter_h;     // 0.25*h
+    double bmin[3];
+    int n_obj, n_plane, n_src, n_lis;
+    DevObject obj[FDTD_MAX_OBJECTS];
+    DevPlane plane[4];
+    DevSource src[FDTD_MAX_SOURCES];
+    // per-axis tables
+    const uint8_t* pml_cell[3];   // [N_d]
+    const uint8_t* pml_face[3];   // [N_d+1]
+    const double* cpos[3];        // [N_d] cell centre coordinate
+    const double* fpos[3];        // [N_d+1] face coordinate
+    const double* pupd[3];        // [N_d]
+    const double* pdiv[3];        // [N_d]
+    const double* vupd[3];        // [N_d+1]
+    const double* vgrad[3];       // [N_d+1]
+    const float* pupd_f[3];
+    const float* pdiv_f[3];
+    const float* vupd_f[3];
+    const float* vgrad_f[3];
+    // state
+    uint8_t* cls;
+    uint8_t* gobj;
+    void* p[2];
+    float* dinc;
+    void* pd[3];
+    void* v[2][3];
+    double* clock;                // simulation time of the next step
+    StepConsts* consts;
+    const double* listeners;      // 3*n_lis
+    int* solid_pml;               // solid cells inside the PML (re-zeroed every step)
+    int n_solid_pml;
+    int precision;                // 0 fp64, 1 fp32 compensated
+};
+
+// Szudzik pairing of two cell indices (MAC_Grid.h:108-116)
+__host__ __device__ inline unsigned long long szudzik(int a_, int b_) {
+    const unsigned long long a = a_ < b_ ? a_ : b_;
+    const unsigned long long b = a_ < b_ ? b_ : a_;
+    return (a >= b ? a * a + a + b : a + b * b);
+}
+
+}  // namespace fdtd

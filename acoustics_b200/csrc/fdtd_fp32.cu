@@ -1,0 +1,36 @@
+// fdtd_fp32.cu — FP32 fused step kernel with compensated (increment-form)
+// pressure accumulation.  Multiply-add contraction is allowed here.
+#include <cuda_runtime.h>
+
+#include "fdtd_device.cuh"
+#include "fdtd_launch.hpp"
+#include "fdtd_stencil.cuh"
+
+namespace fdtd {
+
+cudaError_t launch_prologue_fp32(const SolveParams* dP, int n_solid_pml, cudaStream_t s) {
+    int blocks = 1;
+    if (n_solid_pml > 0) blocks = (n_solid_pml + 255) / 256 > 2368 ? 2368 : (n_solid_pml + 255) / 256;
+    k_prologue<float><<<blocks, 256, 0, s>>>(dP);
+    return cudaGetLastError();
+}
+
+template <int BY>
+static cudaError_t launch_fused_by(const SolveParams* dP, const int N[3], int cur, int xchunk, cudaStream_t s) {
+    dim3 block(32, BY);
+    dim3 grid((N[2] + 31) / 32, (N[1] + BY - 1) / BY, (N[0] + xchunk - 1) / xchunk);
+    k_step_fused<float, BY><<<grid, block, 0, s>>>(dP, cur, xchunk);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_step_fused_fp32(const SolveParams* dP, const int N[3], int cur, int tile_y, int xchunk,
+                                   cudaStream_t s) {
+    switch (tile_y) {
+        case 2: return launch_fused_by<2>(dP, N, cur, xchunk, s);
+        case 4: return launch_fused_by<4>(dP, N, cur, xchunk, s);
+        case 16: return launch_fused_by<16>(dP, N, cur, xchunk, s);
+        default: return launch_fused_by<8>(dP, N, cur, xchunk, s);
+    }
+}
+
+}  // namespace fdtd

@@ -1,0 +1,469 @@
+// fdtd_fp64.cu — FP64 step kernels, cell classification, listener sampling and
+// fresh-cell interpolation.  Compiled with -fmad=false: every product and sum
+// is rounded on its own, in the order the reference writes it, which keeps the
+// FP64 path and the classification bit-reproducible against a CPU build of the
+// same expressions.
+#include <cuda_runtime.h>
+
+#include "fdtd_device.cuh"
+#include "fdtd_geometry.cuh"
+#include "fdtd_launch.hpp"
+#include "fdtd_stencil.cuh"
+
+namespace fdtd {
+
+// ---------------------------------------------------------------------------
+// Cell classification (MAC_Grid::classifyCells_FAST, MAC_Grid.cpp:3455-3891)
+// ---------------------------------------------------------------------------
+
+// validHistory <- isBulk; isBulk <- true (MAC_Grid.cpp:3464-3472)
+__global__ void k_cls_reset(const SolveParams* __restrict__ Pp, long long n) {
+    uint8_t* cls = Pp->cls;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const uint8_t code = cls[c];
+        cls[c] = CLS_BULK | ((code & CLS_BULK) ? CLS_VALID : 0);
+    }
+}
+
+// Solid test over one object / constraint iteration box (MAC_Grid.cpp:3608-3653)
+// and zeroing of the pressure buffers at solid cells (MAC_Grid.cpp:3796-3798).
+__global__ void k_cls_solid(const SolveParams* __restrict__ Pp, int s0, int s1, int s2, int r0, int r1, int r2) {
+    const SolveParams& P = *Pp;
+    const long long total = (long long)r0 * r1 * r2;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int i = s0 + (int)(t / ((long long)r1 * r2));
+        const int j = s1 + (int)((t / r2) % r1);
+        const int k = s2 + (int)(t % r2);
+        const long long c = ((long long)i * P.N[1] + j) * P.N[2] + k;
+        const double pos[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
+        int type = 0;
+        if (!is_fluid(P, pos, type)) {
+            P.cls[c] = P.cls[c] & (uint8_t)~CLS_BULK;
+            P.gobj[c] = type ? GOBJ_CONSTRAINT : 0;
+            if (P.precision == 0) {
+                ((double*)P.p[0])[c] = 0.0;
+                ((double*)P.p[1])[c] = 0.0;
+            } else {
+                ((float*)P.p[0])[c] = 0.0f;
+                ((float*)P.p[1])[c] = 0.0f;
+                P.dinc[c] = 0.0f;
+            }
+        }
+    }
+}
+
+// Neighbour masks: for a solid cell the directions of its bulk neighbours (one
+// ghost face each, MakeGhostCell MAC_Grid.cpp:4310-4340) and its closest
+// object (LowestObjectDistance, MAC_Grid.cpp:3810-3814); for a bulk cell the
+// directions of its solid (ghost) neighbours, read by the Laplacian.
+__global__ void k_cls_ghost(const SolveParams* __restrict__ Pp, long long n) {
+    const SolveParams& P = *Pp;
+    const long long sx = (long long)P.N[1] * P.N[2];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c / sx);
+        const int j = (int)((c / P.N[2]) % P.N[1]);
+        const int k = (int)(c % P.N[2]);
+        const int idx[3] = {i, j, k};
+        const long long strides[3] = {sx, P.N[2], 1};
+        const uint8_t code = P.cls[c];
+        const bool bulk = code & CLS_BULK;
+        unsigned mask = 0;
+        for (int d = 0; d < 3; ++d) {
+            if (idx[d] > 0) {
+                const bool nb = P.cls[c - strides[d]] & CLS_BULK;
+                if (bulk != nb) mask |= 1u << (2 * d);
+            }
+            if (idx[d] + 1 < P.N[d]) {
+                const bool nb = P.cls[c + strides[d]] & CLS_BULK;
+                if (bulk != nb) mask |= 1u << (2 * d + 1);
+            }
+        }
+        if (!bulk) {
+            const double pos[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
+            const int o = lowest_object(P, pos);
+            P.gobj[c] = (P.gobj[c] & GOBJ_CONSTRAINT) | (uint8_t)(o < 0 ? GOBJ_NONE : o);
+        }
+        P.cls[c] = (uint8_t)((code & (CLS_BULK | CLS_VALID)) | mask);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Listener sampling (PML_WaveSolver::FetchScalarData, PML_WaveSolver.cpp:210-317)
+// ---------------------------------------------------------------------------
+constexpr int MAX_MLS_POINTS = 8 * 6;
+
+// Gather the MLS stencil of point pt: enclosing cells (ascending flat index),
+// NaN cells dropped, ghost cells replaced by their ghost faces in key order
+// (neighbour flat index ascending: -x, -y, -z, +z, +y, +x).
+template <typename T>
+__device__ double sample_point(const SolveParams& P, const T* __restrict__ pnew, const T* __restrict__ pold,
+                               double t, const double pt[3], int* bad) {
+    int cells[8];
+    const int nc = enclosing_neighbours(P, pt, cells);
+    const long long sx = (long long)P.N[1] * P.N[2];
+    double A[MAX_MLS_POINTS * 4];
+    double b[MAX_MLS_POINTS];
+    int np = 0;
+    int kept[8];
+    int nk = 0;
+    for (int q = 0; q < nc; ++q) {
+        const int cell = cells[q];
+        const double v = (double)pnew[cell];
+        if (isnan(v)) continue;
+        kept[nk++] = cell;
+        const uint8_t code = P.cls[cell];
+        const int i = (int)(cell / sx), j = (int)((cell / P.N[2]) % P.N[1]), k = (int)(cell % P.N[2]);
+        const double cp[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
+        const unsigned mask = code & CLS_MASK;
+        if ((code & CLS_BULK) || mask == 0) {
+            mls_row(pt, cp, v, &A[np * 4], b[np]);
+            ++np;
+        } else {
+            const int order_dim[6] = {0, 1, 2, 2, 1, 0};
+            const int order_sgn[6] = {-1, -1, -1, +1, +1, +1};
+            const long long strides[3] = {sx, P.N[2], 1};
+            for (int f = 0; f < 6; ++f) {
+                const int d = order_dim[f], s = order_sgn[f];
+                if (!((mask >> (2 * d + (s > 0 ? 1 : 0))) & 1u)) continue;
+                const long long nbr = cell + s * strides[d];
+                const double pg = ghost_pressure(P, P.gobj[cell], cp, d, s, (double)pold[nbr], t);
+                double fp[3] = {cp[0], cp[1], cp[2]};
+                fp[d] += (s > 0 ? 1.0 : -1.0) * 0.25 * P.h;
+                mls_row(pt, fp, pg, &A[np * 4], b[np]);
+                ++np;
+            }
+        }
+    }
+    if (nk == 0) {
+        *bad = 1;
+        return 0.0;
+    }
+    if (nk < 4) {  // nearest cell (PML_WaveSolver.cpp:294-309)
+        int best = -1;
+        double bestD = DBL_MAX;
+        for (int q = 0; q < nk; ++q) {
+            const int cell = kept[q];
+            const int i = (int)(cell / sx), j = (int)((cell / P.N[2]) % P.N[1]), k = (int)(cell % P.N[2]);
+            const double dx = P.cpos[0][i] - pt[0], dy = P.cpos[1][j] - pt[1], dz = P.cpos[2][k] - pt[2];
+            const double d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 < bestD) { best = cell; bestD = d2; }
+        }
+        return (double)pnew[best];
+    }
+    double c0 = 0.0;
+    if (!householder_ls4(A, b, np, c0)) {
+        *bad = 1;
+        c0 = 0.0;
+    }
+    return c0;
+}
+
+template <typename T>
+__global__ void k_listeners(const SolveParams* __restrict__ Pp, int newp, double* __restrict__ out_row) {
+    const SolveParams& P = *Pp;
+    const int li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= P.n_lis) return;
+    const T* pnew = (const T*)P.p[newp];
+    const T* pold = (const T*)P.p[newp ^ 1];
+    const double pt[3] = {P.listeners[3 * li], P.listeners[3 * li + 1], P.listeners[3 * li + 2]};
+    int bad = 0;
+    const double v = sample_point<T>(P, pnew, pold, P.consts->t, pt, &bad);
+    out_row[li] = v;
+    if (bad) atomicOr(&P.consts->error, 1);
+}
+
+// ---------------------------------------------------------------------------
+// Fresh-cell interpolation (MAC_Grid::InterpolateFreshPressureCell, MLS branch,
+// MAC_Grid.cpp:1993-2254): a cell that is bulk now but was solid before gets
+// p = p_MLS(image point) + rho (a . n) |s| in p^{n-1} and p^n.
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ double fresh_value(const SolveParams& P, const T* __restrict__ pa, const T* __restrict__ pb, bool diff,
+                              long long c, double t, int* status) {
+    // value of buffer "a" (or a - b when diff) at cell n
+    auto val = [&](long long n) -> double { return diff ? (double)pa[n] - (double)pb[n] : (double)pa[n]; };
+    const long long sx = (long long)P.N[1] * P.N[2];
+    const int i = (int)(c / sx), j = (int)((c / P.N[2]) % P.N[1]), k = (int)(c % P.N[2]);
+    const double cp[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
+    double distance = DBL_MAX;
+    const int oid = lowest_object(P, cp, &distance);
+    if (oid < 0 || distance < DISTANCE_TOLERANCE) {
+        *status = 2;
+        return 0.0;
+    }
+    const DevObject& o = P.obj[oid];
+    double image[3], bp[3], nrm[3], travelled;
+    reflect_against_boundary(o, cp, image, bp, nrm, travelled);
+    int cells[8];
+    const int nc = enclosing_neighbours(P, image, cells);
+    double A[8 * 4], b[8];
+    int kept[8];
+    int nk = 0;
+    for (int q = 0; q < nc; ++q) {
+        const int n = cells[q];
+        if (!(P.cls[n] & CLS_VALID)) continue;
+        const int ni = n / (int)sx, nj = (n / P.N[2]) % P.N[1], nn = n % P.N[2];
+        const double np_[3] = {P.cpos[0][ni], P.cpos[1][nj], P.cpos[2][nn]};
+        mls_row(image, np_, val(n), &A[nk * 4], b[nk]);
+        kept[nk++] = n;
+    }
+    if (nk < 4) {
+        if (nk != 0) {
+            double md = DBL_MAX;
+            int mid = -1;
+            for (int q = 0; q < nk; ++q) {
+                const int n = kept[q];
+                const int ni = n / (int)sx, nj = (n / P.N[2]) % P.N[1], nn = n % P.N[2];
+                const double dx = image[0] - P.cpos[0][ni], dy = image[1] - P.cpos[1][nj], dz = image[2] - P.cpos[2][nn];
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (d2 < md) { md = d2; mid = n; }
+            }
+            return val(mid);
+        }
+        const int idx[3] = {i, j, k};
+        const long long strides[3] = {sx, P.N[2], 1};
+        for (int d = 0; d < 3; ++d)
+            for (int s = 1; s >= -1; s -= 2) {
+                if (idx[d] + s < 0 || idx[d] + s >= P.N[d]) continue;
+                const long long n = c + s * strides[d];
+                if (P.cls[n] & CLS_BULK) return val(n);
+            }
+        return 0.0;
+    }
+    double c0 = 0.0;
+    if (!householder_ls4(A, b, nk, c0)) c0 = 0.0;
+    double acc[3];
+    boundary_accel(o, bp, t, acc);
+    const double an = acc[0] * nrm[0] + acc[1] * nrm[1] + acc[2] * nrm[2];
+    return c0 + P.rho * an * fabs(travelled);
+}
+
+template <typename T>
+__global__ void k_fresh_cells(const SolveParams* __restrict__ Pp, int cur, long long n, int* status) {
+    const SolveParams& P = *Pp;
+    const double t = *P.clock;  // runs before the prologue: the clock holds t_n
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const uint8_t code = P.cls[c];
+        if (!(code & CLS_BULK) || (code & CLS_VALID)) continue;
+        int st = 0;
+        if (sizeof(T) == 8) {
+            double* pl = (double*)P.p[cur ^ 1];
+            double* pc = (double*)P.p[cur];
+            const double vl = fresh_value<double>(P, pl, pl, false, c, t, &st);
+            const double vc = fresh_value<double>(P, pc, pc, false, c, t, &st);
+            pl[c] = vl;
+            pc[c] = vc;
+        } else {
+            // FP32 keeps p^n and the increment; p^{n-1} = p^n - d
+            float* pc = (float*)P.p[cur];
+            const double vc = fresh_value<float>(P, pc, pc, false, c, t, &st);
+            const double vl = fresh_value<float>(P, pc, P.dinc, true, c, t, &st);
+            pc[c] = (float)vc;
+            P.dinc[c] = (float)(vc - vl);
+        }
+        if (st) atomicMax(status, st);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Plain FP64 path: one kernel per reference phase over full-grid arrays, as
+// PML_WaveSolver::stepCollocated sequences them (PML_WaveSolver.cpp:800-823).
+// ---------------------------------------------------------------------------
+__global__ void k_phase_velocity(const SolveParams* __restrict__ Pp, int cur, int dim) {
+    const SolveParams& P = *Pp;
+    const int* vN = P.vN[dim];
+    const long long total = (long long)vN[0] * vN[1] * vN[2];
+    const double* p = (const double*)P.p[cur];
+    double* v = (double*)P.v[0][dim];
+    for (long long f = blockIdx.x * (long long)blockDim.x + threadIdx.x; f < total; f += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(f / ((long long)vN[1] * vN[2]));
+        const int j = (int)((f / vN[2]) % vN[1]);
+        const int k = (int)(f % vN[2]);
+        int a[3] = {i, j, k};
+        if (a[dim] == 0 || a[dim] == vN[dim] - 1) continue;
+        bool inpml = P.pml_face[dim][a[dim]] != 0;
+        for (int d = 0; d < 3; ++d)
+            if (d != dim) inpml = inpml || P.pml_cell[d][a[d]] != 0;
+        if (!inpml) continue;
+        const long long pr = ((long long)a[0] * P.N[1] + a[1]) * P.N[2] + a[2];
+        a[dim] -= 1;
+        const long long pl = ((long long)a[0] * P.N[1] + a[1]) * P.N[2] + a[2];
+        v[f] = vel_update<double>(v[f], P.vupd[dim][a[dim] + 1], P.vgrad[dim][a[dim] + 1], p[pr], p[pl]);
+    }
+}
+
+__global__ void k_phase_laplacian(const SolveParams* __restrict__ Pp, int cur, double* __restrict__ lap) {
+    const SolveParams& P = *Pp;
+    const double* p = (const double*)P.p[cur];
+    const long long sx = (long long)P.N[1] * P.N[2];
+    const double t = P.consts->t;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.ncell; c += (long long)gridDim.x * blockDim.x) {
+        const uint8_t code = P.cls[c];
+        if (!(code & CLS_BULK)) { lap[c] = 0.0; continue; }
+        const int idx[3] = {(int)(c / sx), (int)((c / P.N[2]) % P.N[1]), (int)(c % P.N[2])};
+        const long long strides[3] = {sx, P.N[2], 1};
+        const unsigned mask = code & CLS_MASK;
+        double L = 0.0;
+        int surrounded = 0;
+        const double p0 = p[c];
+        for (int d = 0; d < 3; ++d) {
+            const double pp = idx[d] + 1 < P.N[d] ? p[c + strides[d]] : p0;
+            const double pm = idx[d] > 0 ? p[c - strides[d]] : p0;
+            const bool gn = (mask >> (2 * d)) & 1u, gp = (mask >> (2 * d + 1)) & 1u;
+            double own[3] = {P.cpos[0][idx[0]], P.cpos[1][idx[1]], P.cpos[2][idx[2]]};
+            double gpv = 0, gnv = 0;
+            if (gp) {
+                own[d] = P.cpos[d][idx[d] + 1];
+                gpv = ghost_pressure(P, P.gobj[c + strides[d]], own, d, -1, p0, t);
+            }
+            if (gn) {
+                own[d] = P.cpos[d][idx[d] - 1];
+                gnv = ghost_pressure(P, P.gobj[c - strides[d]], own, d, +1, p0, t);
+            }
+            if (gp && gn) {
+                L += (gpv + gnv - 2.0 * p0) / (9.0 / 16.0);
+                ++surrounded;
+            } else if (gp) {
+                L += (gpv + 0.75 * pm - (7.0 / 4.0) * p0) / (21.0 / 32.0);
+            } else if (gn) {
+                L += (0.75 * pp + gnv - (7.0 / 4.0) * p0) / (21.0 / 32.0);
+            } else {
+                L += (pp + pm - 2.0 * p0);
+            }
+        }
+        L *= P.lap_scale;
+        (void)surrounded;  // the pressure phase re-derives the cavity flag from the mask
+        lap[c] = L;
+    }
+}
+
+__global__ void k_phase_pressure(const SolveParams* __restrict__ Pp, int cur, const double* __restrict__ lap) {
+    const SolveParams& P = *Pp;
+    const double* pc = (const double*)P.p[cur];
+    double* pn = (double*)P.p[cur ^ 1];
+    const long long sx = (long long)P.N[1] * P.N[2];
+    const StepConsts sc = *P.consts;
+    bool any_src = false;
+    for (int s = 0; s < P.n_src; ++s) any_src |= (sc.src_tf[s] != 0.0);
+    const double* v0 = (const double*)P.v[0][0];
+    const double* v1 = (const double*)P.v[0][1];
+    const double* v2 = (const double*)P.v[0][2];
+    double* pd0 = (double*)P.pd[0];
+    double* pd1 = (double*)P.pd[1];
+    double* pd2 = (double*)P.pd[2];
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.ncell; c += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(c / sx), j = (int)((c / P.N[2]) % P.N[1]), k = (int)(c % P.N[2]);
+        const bool pml = P.pml_cell[0][i] || P.pml_cell[1][j] || P.pml_cell[2][k];
+        if (pml) {
+            const long long f0 = c, f1 = ((long long)i * (P.N[1] + 1) + j) * P.N[2] + k,
+                            f2 = ((long long)i * P.N[1] + j) * (P.N[2] + 1) + k;
+            const double a = pd_update<double>(pd0[c], P.pupd[0][i], P.pdiv[0][i], v0[f0 + sx], v0[f0], P.inv_h);
+            const double b = pd_update<double>(pd1[c], P.pupd[1][j], P.pdiv[1][j], v1[f1 + P.N[2]], v1[f1], P.inv_h);
+            const double d = pd_update<double>(pd2[c], P.pupd[2][k], P.pdiv[2][k], v2[f2 + 1], v2[f2], P.inv_h);
+            pd0[c] = a;
+            pd1[c] = b;
+            pd2[c] = d;
+            pn[c] = a + b + d;
+            continue;
+        }
+        const uint8_t code = P.cls[c];
+        if (!(code & CLS_BULK)) continue;
+        const unsigned mask = code & CLS_MASK;
+        int surrounded = 0;
+        for (int dd = 0; dd < 3; ++dd)
+            if (((mask >> (2 * dd)) & 3u) == 3u) ++surrounded;
+        double pnext;
+        if (surrounded > 1 && (code & CLS_VALID)) pnext = pc[c];
+        else pnext = 2.0 * pc[c] - pn[c] + lap[c] * P.c2k2;
+        if (P.n_src > 0) {
+            double src = 0.0;
+            if (any_src) src = source_sum(P, sc, P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]);
+            pnext += src * P.k;
+        }
+        pn[c] = pnext;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static int grid_for(long long n, int block) {
+    long long g = (n + block - 1) / block;
+    if (g > 148LL * 16) g = 148LL * 16;
+    if (g < 1) g = 1;
+    return (int)g;
+}
+
+cudaError_t launch_prologue_fp64(const SolveParams* dP, int n_solid_pml, cudaStream_t s) {
+    const int blocks = n_solid_pml > 0 ? grid_for(n_solid_pml, 256) : 1;
+    k_prologue<double><<<blocks, 256, 0, s>>>(dP);
+    return cudaGetLastError();
+}
+
+template <int BY>
+static cudaError_t launch_fused_by(const SolveParams* dP, const int N[3], int cur, int xchunk, cudaStream_t s) {
+    dim3 block(32, BY);
+    dim3 grid((N[2] + 31) / 32, (N[1] + BY - 1) / BY, (N[0] + xchunk - 1) / xchunk);
+    k_step_fused<double, BY><<<grid, block, 0, s>>>(dP, cur, xchunk);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_step_fused_fp64(const SolveParams* dP, const int N[3], int cur, int tile_y, int xchunk,
+                                   cudaStream_t s) {
+    switch (tile_y) {
+        case 2: return launch_fused_by<2>(dP, N, cur, xchunk, s);
+        case 4: return launch_fused_by<4>(dP, N, cur, xchunk, s);
+        case 16: return launch_fused_by<16>(dP, N, cur, xchunk, s);
+        default: return launch_fused_by<8>(dP, N, cur, xchunk, s);
+    }
+}
+
+cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int n_lis, double* out_row,
+                             cudaStream_t s) {
+    if (n_lis <= 0) return cudaSuccess;
+    const int block = 64;
+    const int grid = (n_lis + block - 1) / block;
+    if (precision == 0) k_listeners<double><<<grid, block, 0, s>>>(dP, newp, out_row);
+    else k_listeners<float><<<grid, block, 0, s>>>(dP, newp, out_row);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cls_reset(const SolveParams* dP, long long ncell, cudaStream_t s) {
+    k_cls_reset<<<grid_for(ncell, 256), 256, 0, s>>>(dP, ncell);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cls_solid(const SolveParams* dP, const int start[3], const int range[3], cudaStream_t s) {
+    const long long total = (long long)range[0] * range[1] * range[2];
+    if (total <= 0) return cudaSuccess;
+    k_cls_solid<<<grid_for(total, 128), 128, 0, s>>>(dP, start[0], start[1], start[2], range[0], range[1], range[2]);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_cls_ghost(const SolveParams* dP, long long ncell, cudaStream_t s) {
+    k_cls_ghost<<<grid_for(ncell, 256), 256, 0, s>>>(dP, ncell);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fresh_cells(const SolveParams* dP, int precision, int cur, long long ncell, int* d_status,
+                               cudaStream_t s) {
+    if (precision == 0) k_fresh_cells<double><<<grid_for(ncell, 256), 256, 0, s>>>(dP, cur, ncell, d_status);
+    else k_fresh_cells<float><<<grid_for(ncell, 256), 256, 0, s>>>(dP, cur, ncell, d_status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_phased_fp64(const SolveParams* dP, const int N[3], int cur, double* lap, cudaStream_t s,
+                               int* launches) {
+    const long long n = (long long)N[0] * N[1] * N[2];
+    for (int d = 0; d < 3; ++d) {
+        const long long nf = n + (long long)(d == 0 ? N[1] * N[2] : d == 1 ? N[0] * N[2] : N[0] * N[1]);
+        k_phase_velocity<<<grid_for(nf, 256), 256, 0, s>>>(dP, cur, d);
+    }
+    k_phase_laplacian<<<grid_for(n, 256), 256, 0, s>>>(dP, cur, lap);
+    k_phase_pressure<<<grid_for(n, 256), 256, 0, s>>>(dP, cur, lap);
+    if (launches) *launches += 5;
+    return cudaGetLastError();
+}
+
+}  // namespace fdtd

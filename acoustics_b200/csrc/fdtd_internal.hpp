@@ -1,0 +1,80 @@
+// fdtd_internal.hpp — host-side state of one solver handle.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <array>
+#include <string>
+#include <vector>
+
+#include "../../include/fdtd_c.h"
+#include "fdtd_device.cuh"
+
+namespace fdtd {
+
+struct HostObject {
+    fdtd_object_desc d;
+    double c[3] = {0, 0, 0};
+    double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};  // _bboxWorld
+    double umin[3] = {0, 0, 0}, umax[3] = {0, 0, 0};  // _bboxWorldUnion2Steps
+};
+
+struct AxisTables {
+    std::vector<uint8_t> pml_cell, pml_face;
+    std::vector<double> cpos, fpos, pupd, pdiv, vupd, vgrad;
+};
+
+void host_object_pose(HostObject& o, double t);
+void host_update_bbox(HostObject& o);
+void host_reset_union(HostObject& o);
+
+}  // namespace fdtd
+
+struct fdtd_solver {
+    fdtd_options opt{};
+    int precision = 0;
+    cudaStream_t stream = nullptr;
+    // geometry
+    double h = 0, c = 0, rho = 0, k = 0, end_time = 0, start_time = 0;
+    int N[3] = {0, 0, 0};
+    long long ncell = 0, n_pml = 0, n_interior = 0;
+    long long vcount[3] = {0, 0, 0};
+    double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};
+    fdtd::AxisTables tab[3];
+    std::vector<fdtd::HostObject> objs;
+    std::vector<fdtd_plane_desc> planes;
+    std::vector<fdtd_gaussian_source_desc> sources;
+    std::vector<double> listeners;
+    int L = 0;
+    bool moving = false;
+    // device
+    fdtd::SolveParams hP{};
+    fdtd::SolveParams* dP = nullptr;
+    void* arena = nullptr;
+    size_t arena_bytes = 0;
+    int* d_solid_pml = nullptr;
+    int n_solid_pml = 0;
+    double* d_lap = nullptr;
+    int* d_status = nullptr;
+    double* d_lis = nullptr;
+    double* h_lis_stage = nullptr;
+    int lis_cap_steps = 0;
+    int tile_y = 8, xchunk = 16;
+    // stepping state
+    int cur = 0;
+    long long step_index = 0;
+    double time = 0.0;        // simulation time of the next step (host mirror of the device clock)
+    double state_time = 0.0;  // SimWorld::_state.time for object animation
+    bool classified_after_first_step = false;
+    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    long long launches = 0;
+    long long last_launches = 0;
+    long long graph_launches_per_exec = 0;
+    std::string err;
+};
+
+namespace fdtd {
+void set_error(fdtd_solver* s, const std::string& msg);
+fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc);
+void classification_boxes(const fdtd_solver* s, std::vector<std::array<int, 6>>& boxes);
+void to_dev_objects(fdtd_solver* s);
+}  // namespace fdtd

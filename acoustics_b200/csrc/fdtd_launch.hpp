@@ -1,0 +1,30 @@
+// fdtd_launch.hpp — host-callable launchers of the device kernels.
+#pragma once
+#include <cuda_runtime.h>
+
+#include "fdtd_device.cuh"
+
+namespace fdtd {
+
+// fdtd_fp64.cu (compiled with -fmad=false)
+cudaError_t launch_prologue_fp64(const SolveParams* dP, int n_solid_pml, cudaStream_t s);
+cudaError_t launch_step_fused_fp64(const SolveParams* dP, const int N[3], int cur, int tile_y, int xchunk,
+                                   cudaStream_t s);
+cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int n_lis, double* out_row,
+                             cudaStream_t s);
+cudaError_t launch_cls_reset(const SolveParams* dP, long long ncell, cudaStream_t s);
+cudaError_t launch_cls_solid(const SolveParams* dP, const int start[3], const int range[3], cudaStream_t s);
+cudaError_t launch_cls_ghost(const SolveParams* dP, long long ncell, cudaStream_t s);
+cudaError_t launch_fresh_cells(const SolveParams* dP, int precision, int cur, long long ncell, int* d_status,
+                               cudaStream_t s);
+
+// plain FP64 path, one kernel per reference phase
+cudaError_t launch_phased_fp64(const SolveParams* dP, const int N[3], int cur, double* lap, cudaStream_t s,
+                               int* launches);
+
+// fdtd_fp32.cu
+cudaError_t launch_prologue_fp32(const SolveParams* dP, int n_solid_pml, cudaStream_t s);
+cudaError_t launch_step_fused_fp32(const SolveParams* dP, const int N[3], int cur, int tile_y, int xchunk,
+                                   cudaStream_t s);
+
+}  // namespace fdtd

@@ -1,0 +1,449 @@
+// fdtd_step.cpp — the step loop (SimWorld::StepWorld -> RunForSteps(1) ->
+// PML_WaveSolver::stepSystem -> FetchPressureData, SimWorld.cpp:507-600), CUDA
+// graph capture of static scenes, read-back and snapshot/restore.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/fdtd_c.h"
+#include "fdtd_device.cuh"
+#include "fdtd_internal.hpp"
+#include "fdtd_launch.hpp"
+
+using namespace fdtd;
+
+#define CUDA_TRY(s, expr)                                                                   \
+    do {                                                                                    \
+        cudaError_t _e = (expr);                                                            \
+        if (_e != cudaSuccess) {                                                            \
+            set_error((s), std::string("CUDA: ") + cudaGetErrorString(_e) + " at " #expr); \
+            return _e == cudaErrorMemoryAllocation ? FDTD_ERR_OOM : FDTD_ERR_CUDA;          \
+        }                                                                                   \
+    } while (0)
+
+namespace {
+
+void classification_launches(fdtd_solver* s, fdtd_status& st) {
+    std::vector<std::array<int, 6>> boxes;
+    classification_boxes(s, boxes);
+    cudaError_t e = launch_cls_reset(s->dP, s->ncell, s->stream);
+    s->launches++;
+    for (const auto& b : boxes) {
+        if (e != cudaSuccess) break;
+        const int a[3] = {b[0], b[1], b[2]}, r[3] = {b[3], b[4], b[5]};
+        e = launch_cls_solid(s->dP, a, r, s->stream);
+        s->launches++;
+    }
+    if (e == cudaSuccess) e = launch_cls_ghost(s->dP, s->ncell, s->stream);
+    s->launches++;
+    if (e != cudaSuccess) {
+        set_error(s, std::string("classification launch: ") + cudaGetErrorString(e));
+        st = FDTD_ERR_CUDA;
+    }
+}
+
+// Enqueue one time step with the pressure parity `cur`; listener row to dev_row.
+fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify) {
+    fdtd_status st = FDTD_OK;
+    if (classify) {
+        // MAC_Grid::classifyCells_FAST + InterpolateFreshPressureCell (PML_WaveSolver.cpp:807-812)
+        classification_launches(s, st);
+        if (st != FDTD_OK) return st;
+        if (s->moving) {
+            CUDA_TRY(s, launch_fresh_cells(s->dP, s->precision, cur, s->ncell, s->d_status, s->stream));
+            s->launches++;
+        }
+    }
+    if (s->precision == FDTD_PRECISION_FP64) {
+        CUDA_TRY(s, launch_prologue_fp64(s->dP, s->n_solid_pml, s->stream));
+        s->launches++;
+        if (s->opt.kernel == FDTD_KERNEL_PHASED) {
+            int l = 0;
+            CUDA_TRY(s, launch_phased_fp64(s->dP, s->N, cur, s->d_lap, s->stream, &l));
+            s->launches += l;
+        } else {
+            CUDA_TRY(s, launch_step_fused_fp64(s->dP, s->N, cur, s->tile_y, s->xchunk, s->stream));
+            s->launches++;
+        }
+    } else {
+        CUDA_TRY(s, launch_prologue_fp32(s->dP, s->n_solid_pml, s->stream));
+        s->launches++;
+        CUDA_TRY(s, launch_step_fused_fp32(s->dP, s->N, cur, s->tile_y, s->xchunk, s->stream));
+        s->launches++;
+    }
+    if (s->L > 0 && dev_row) {
+        // the phased path keeps p^{n+1} in the same slot as the fused one
+        CUDA_TRY(s, launch_listeners(s->dP, s->precision, cur ^ 1, s->L, dev_row, s->stream));
+        s->launches++;
+    }
+    return FDTD_OK;
+}
+
+// Host bookkeeping after a step: parity, clock mirror, object animation
+// (SimWorld::UpdateObjectState(t + dt), SimWorld.cpp:596-600).
+fdtd_status after_step(fdtd_solver* s) {
+    s->cur ^= 1;
+    s->step_index++;
+    s->time += s->k;
+    if (s->moving) {
+        s->state_time += s->k;
+        for (size_t i = 0; i < s->objs.size(); ++i) {
+            auto& o = s->objs[i];
+            if (o.d.motion == FDTD_MOTION_STATIC) continue;
+            host_object_pose(o, s->state_time);
+            host_update_bbox(o);
+        }
+        to_dev_objects(s);
+        CUDA_TRY(s, cudaMemcpyAsync(&s->dP->obj[0], &s->hP.obj[0], sizeof(DevObject) * s->objs.size(),
+                                    cudaMemcpyHostToDevice, s->stream));
+    }
+    return FDTD_OK;
+}
+
+fdtd_status check_device_errors(fdtd_solver* s) {
+    StepConsts sc;
+    int status[4] = {0, 0, 0, 0};
+    CUDA_TRY(s, cudaMemcpyAsync(&sc, s->hP.consts, sizeof(sc), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(status, s->d_status, sizeof(status), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (status[0] == 2) {
+        set_error(s, "fresh cell inside an object (MAC_Grid.cpp:2050-2053)");
+        return FDTD_ERR_GEOMETRY;
+    }
+    if (sc.error & 1) {
+        set_error(s, "degenerate listener stencil (no cell or rank-deficient MLS)");
+        return FDTD_ERR_NUMERIC;
+    }
+    return FDTD_OK;
+}
+
+// Capture `n` steps starting at parity `cur` into a graph (static scenes only).
+fdtd_status capture_graph(fdtd_solver* s, int cur, int n, cudaGraphExec_t* out) {
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+    fdtd_status st = FDTD_OK;
+    int c = cur;
+    for (int i = 0; i < n && st == FDTD_OK; ++i) {
+        st = enqueue_step(s, c, s->d_lis + (size_t)i * s->L, false);
+        c ^= 1;
+    }
+    cudaError_t e = cudaStreamEndCapture(s->stream, &g);
+    if (st != FDTD_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) {
+        set_error(s, std::string("graph capture: ") + cudaGetErrorString(e));
+        return FDTD_ERR_CUDA;
+    }
+    e = cudaGraphInstantiate(out, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        set_error(s, std::string("graph instantiate: ") + cudaGetErrorString(e));
+        return FDTD_ERR_CUDA;
+    }
+    return FDTD_OK;
+}
+
+// Run n steps; listener rows land in the device ring d_lis (chunks of at most
+// lis_cap_steps) and are passed to `sink(first_step, count)` after each chunk.
+// Static scenes replay captured graphs of graph_steps steps once the first
+// step (which classifies) has run.
+template <typename Sink>
+fdtd_status run_steps(fdtd_solver* s, int n, Sink sink) {
+    CUDA_TRY(s, cudaSetDevice(s->opt.device));
+    const long long launches0 = s->launches;
+    const int G = s->opt.graph_steps;
+    int done = 0;
+    while (done < n) {
+        const int remaining = n - done;
+        const bool classify_now = s->moving || s->step_index == 0;
+        if (!classify_now && G > 0 && remaining >= G) {
+            if (!s->graph_exec[s->cur]) {
+                const long long l0 = s->launches;
+                fdtd_status st = capture_graph(s, s->cur, G, &s->graph_exec[s->cur]);
+                if (st != FDTD_OK) return st;
+                s->graph_launches_per_exec = s->launches - l0;
+                s->launches = l0;
+            }
+            CUDA_TRY(s, cudaGraphLaunch(s->graph_exec[s->cur], s->stream));
+            s->launches += s->graph_launches_per_exec;
+            for (int q = 0; q < G; ++q) {
+                fdtd_status st = after_step(s);
+                if (st != FDTD_OK) return st;
+            }
+            fdtd_status st = sink(done, G);
+            if (st != FDTD_OK) return st;
+            done += G;
+            continue;
+        }
+        int m = std::min(remaining, s->lis_cap_steps);
+        if (G > 0 && !s->moving && classify_now) m = 1;
+        for (int i = 0; i < m; ++i) {
+            const bool classify = s->moving || s->step_index == 0;
+            fdtd_status st = enqueue_step(s, s->cur, s->d_lis + (size_t)i * s->L, classify);
+            if (st != FDTD_OK) return st;
+            st = after_step(s);
+            if (st != FDTD_OK) return st;
+        }
+        fdtd_status st = sink(done, m);
+        if (st != FDTD_OK) return st;
+        done += m;
+    }
+    s->last_launches = s->launches - launches0;
+    return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fdtd_status fdtd_solver_step(fdtd_solver* s, int32_t n_steps, double* listener_out) {
+    if (!s || n_steps < 0) return (set_error(s, "invalid arguments"), FDTD_ERR_INVALID_ARG);
+    const int L = s->L;
+    fdtd_status st = run_steps(s, n_steps, [&](int first, int count) -> fdtd_status {
+        if (listener_out && L > 0) {
+            CUDA_TRY(s, cudaMemcpyAsync(s->h_lis_stage, s->d_lis, (size_t)count * L * 8, cudaMemcpyDeviceToHost,
+                                        s->stream));
+            CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+            std::memcpy(listener_out + (size_t)first * L, s->h_lis_stage, (size_t)count * L * 8);
+        }
+        return FDTD_OK;
+    });
+    if (st != FDTD_OK) return st;
+    st = check_device_errors(s);
+    if (st != FDTD_OK) return st;
+    if (s->end_time > 0.0 && s->time >= s->end_time) return FDTD_END_OF_TIME;
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_solver_step_device(fdtd_solver* s, int32_t n_steps, void* device_listener_out) {
+    if (!s || n_steps < 0) return (set_error(s, "invalid arguments"), FDTD_ERR_INVALID_ARG);
+    const int L = s->L;
+    double* out = (double*)device_listener_out;
+    fdtd_status st = run_steps(s, n_steps, [&](int first, int count) -> fdtd_status {
+        if (out && L > 0)
+            CUDA_TRY(s, cudaMemcpyAsync(out + (size_t)first * L, s->d_lis, (size_t)count * L * 8,
+                                        cudaMemcpyDeviceToDevice, s->stream));
+        return FDTD_OK;
+    });
+    return st;
+}
+
+fdtd_status fdtd_solver_fetch_listeners(fdtd_solver* s, double* out) {
+    if (!s || (!out && s->L > 0)) return (set_error(s, "invalid arguments"), FDTD_ERR_INVALID_ARG);
+    if (s->L == 0) return FDTD_OK;
+    CUDA_TRY(s, cudaSetDevice(s->opt.device));
+    CUDA_TRY(s, launch_listeners(s->dP, s->precision, s->cur, s->L, s->d_lis, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(out, s->d_lis, (size_t)s->L * 8, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_solver_synchronize(fdtd_solver* s) {
+    if (!s) return FDTD_ERR_INVALID_ARG;
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    return FDTD_OK;
+}
+
+void* fdtd_solver_stream(fdtd_solver* s) { return s ? (void*)s->stream : nullptr; }
+
+const char* fdtd_solver_last_error(fdtd_solver* s) { return s ? s->err.c_str() : ""; }
+
+int64_t fdtd_solver_last_launch_count(fdtd_solver* s) { return s ? s->last_launches : 0; }
+
+fdtd_status fdtd_solver_info_get(fdtd_solver* s, fdtd_solver_info* info) {
+    if (!s || !info) return FDTD_ERR_INVALID_ARG;
+    std::memset(info, 0, sizeof(*info));
+    for (int d = 0; d < 3; ++d) info->divisions[d] = s->N[d];
+    info->n_listeners = s->L;
+    info->n_cells = s->ncell;
+    info->n_pml_cells = s->n_pml;
+    info->n_interior_cells = s->n_interior;
+    info->device_bytes = (int64_t)s->arena_bytes;
+    info->step_index = s->step_index;
+    info->time = s->time;
+    info->time_step = s->k;
+    const double w = s->precision == FDTD_PRECISION_FP64 ? 8.0 : 4.0;
+    info->algorithmic_bytes_per_step = w * (3.0 * (double)s->n_interior + 14.0 * (double)s->n_pml);
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_solver_get_classification(fdtd_solver* s, uint8_t* flags, fdtd_ghost_face* faces, int64_t* n_faces) {
+    if (!s) return FDTD_ERR_INVALID_ARG;
+    CUDA_TRY(s, cudaSetDevice(s->opt.device));
+    std::vector<uint8_t> cls(s->ncell), gobj(s->ncell);
+    CUDA_TRY(s, cudaMemcpyAsync(cls.data(), s->hP.cls, s->ncell, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(gobj.data(), s->hP.gobj, s->ncell, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    const long long sx = (long long)s->N[1] * s->N[2];
+    int64_t count = 0;
+    const int64_t cap = (faces && n_faces) ? *n_faces : 0;
+    for (long long c = 0; c < s->ncell; ++c) {
+        const uint8_t code = cls[c];
+        const bool bulk = code & CLS_BULK;
+        const unsigned mask = code & CLS_MASK;
+        const int i = (int)(c / sx), j = (int)((c / s->N[2]) % s->N[1]), k = (int)(c % s->N[2]);
+        if (flags) {
+            uint8_t f = 0;
+            if (bulk) f |= FDTD_CELL_BULK;
+            if (!bulk && mask) f |= FDTD_CELL_GHOST;
+            if (code & CLS_VALID) f |= FDTD_CELL_VALID_HISTORY;
+            if (s->tab[0].pml_cell[i] || s->tab[1].pml_cell[j] || s->tab[2].pml_cell[k]) f |= FDTD_CELL_PML;
+            if (!bulk && (gobj[c] & GOBJ_CONSTRAINT)) f |= FDTD_CELL_CONSTRAINT;
+            flags[c] = f;
+        }
+        if (bulk || !mask) continue;
+        // faces in key order: neighbour flat index ascending (-x, -y, -z, +z, +y, +x)
+        static const int od[6] = {0, 1, 2, 2, 1, 0};
+        static const int os[6] = {-1, -1, -1, +1, +1, +1};
+        const long long strides[3] = {sx, s->N[2], 1};
+        for (int f = 0; f < 6; ++f) {
+            if (!((mask >> (2 * od[f] + (os[f] > 0))) & 1u)) continue;
+            if (count < cap) {
+                fdtd_ghost_face& g = faces[count];
+                std::memset(&g, 0, sizeof(g));
+                g.owner_cell = (int32_t)c;
+                g.neighbour_cell = (int32_t)(c + os[f] * strides[od[f]]);
+                g.topology = os[f] * (od[f] + 1);
+                g.type = (gobj[c] & GOBJ_CONSTRAINT) ? 1 : 0;
+                const int o = gobj[c] & 0x7F;
+                g.boundary_object = (o == GOBJ_NONE) ? -1 : o;
+                g.key = szudzik(g.owner_cell, g.neighbour_cell);
+            }
+            ++count;
+        }
+    }
+    if (n_faces) *n_faces = count;
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, int64_t count) {
+    if (!s || !out) return FDTD_ERR_INVALID_ARG;
+    CUDA_TRY(s, cudaSetDevice(s->opt.device));
+    const SolveParams& P = s->hP;
+    const bool f64 = s->precision == FDTD_PRECISION_FP64;
+    const size_t w = f64 ? 8 : 4;
+    const void* src = nullptr;
+    long long n = s->ncell;
+    int vbuf = s->opt.kernel == FDTD_KERNEL_PHASED ? 0 : s->cur;
+    switch (which) {
+        case FDTD_FIELD_PRESSURE: src = P.p[s->cur]; break;
+        case FDTD_FIELD_PRESSURE_PREV: src = f64 ? P.p[s->cur ^ 1] : P.p[s->cur]; break;
+        case FDTD_FIELD_PML_PX: case FDTD_FIELD_PML_PY: case FDTD_FIELD_PML_PZ: src = P.pd[which - FDTD_FIELD_PML_PX]; break;
+        case FDTD_FIELD_VX: case FDTD_FIELD_VY: case FDTD_FIELD_VZ:
+            src = P.v[vbuf][which - FDTD_FIELD_VX];
+            n = s->vcount[which - FDTD_FIELD_VX];
+            break;
+        default: return (set_error(s, "unknown field"), FDTD_ERR_INVALID_ARG);
+    }
+    if (count != n) return (set_error(s, "count does not match the field size"), FDTD_ERR_INVALID_ARG);
+    if (f64) {
+        CUDA_TRY(s, cudaMemcpyAsync(out, src, n * 8, cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+        return FDTD_OK;
+    }
+    std::vector<float> tmp(n), inc;
+    CUDA_TRY(s, cudaMemcpyAsync(tmp.data(), src, n * w, cudaMemcpyDeviceToHost, s->stream));
+    if (which == FDTD_FIELD_PRESSURE_PREV) {
+        inc.resize(n);
+        CUDA_TRY(s, cudaMemcpyAsync(inc.data(), P.dinc, n * 4, cudaMemcpyDeviceToHost, s->stream));
+    }
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    for (long long i = 0; i < n; ++i) out[i] = inc.empty() ? (double)tmp[i] : (double)tmp[i] - (double)inc[i];
+    return FDTD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// snapshot / restore (FDTD_AcousticSimulator::_SaveSimulationSnapshot, :381-415)
+// ---------------------------------------------------------------------------
+namespace {
+struct SnapHeader {
+    uint64_t magic;
+    int64_t ncell;
+    int32_t precision, kernel, cur, n_obj;
+    int64_t step_index;
+    double time, state_time;
+};
+const uint64_t SNAP_MAGIC = 0x314e53445446ULL;  // "FTDSN1"
+
+std::vector<std::pair<void*, size_t>> snap_regions(fdtd_solver* s) {
+    const SolveParams& P = s->hP;
+    const size_t w = s->precision == FDTD_PRECISION_FP64 ? 8 : 4;
+    std::vector<std::pair<void*, size_t>> r;
+    r.push_back({P.p[0], s->ncell * w});
+    r.push_back({P.p[1], s->ncell * w});
+    if (P.dinc) r.push_back({P.dinc, s->ncell * 4});
+    for (int d = 0; d < 3; ++d) r.push_back({P.pd[d], s->ncell * w});
+    for (int b = 0; b < 2; ++b)
+        for (int d = 0; d < 3; ++d)
+            if (P.v[b][d]) r.push_back({P.v[b][d], s->vcount[d] * w});
+    r.push_back({P.cls, (size_t)s->ncell});
+    r.push_back({P.gobj, (size_t)s->ncell});
+    r.push_back({P.clock, 8});
+    r.push_back({P.consts, sizeof(StepConsts)});
+    return r;
+}
+}  // namespace
+
+fdtd_status fdtd_solver_snapshot(fdtd_solver* s, void* buffer, int64_t* bytes) {
+    if (!s || !bytes) return FDTD_ERR_INVALID_ARG;
+    auto regs = snap_regions(s);
+    size_t total = sizeof(SnapHeader) + s->objs.size() * sizeof(HostObject);
+    for (auto& r : regs) total += r.second;
+    if (!buffer) {
+        *bytes = (int64_t)total;
+        return FDTD_OK;
+    }
+    if (*bytes < (int64_t)total) return (set_error(s, "snapshot buffer too small"), FDTD_ERR_INVALID_ARG);
+    CUDA_TRY(s, cudaSetDevice(s->opt.device));
+    SnapHeader h{SNAP_MAGIC, s->ncell, s->precision, s->opt.kernel, s->cur, (int32_t)s->objs.size(),
+                 s->step_index, s->time, s->state_time};
+    char* p = (char*)buffer;
+    std::memcpy(p, &h, sizeof(h));
+    p += sizeof(h);
+    std::memcpy(p, s->objs.data(), s->objs.size() * sizeof(HostObject));
+    p += s->objs.size() * sizeof(HostObject);
+    for (auto& r : regs) {
+        CUDA_TRY(s, cudaMemcpyAsync(p, r.first, r.second, cudaMemcpyDeviceToHost, s->stream));
+        p += r.second;
+    }
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    *bytes = (int64_t)total;
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_solver_restore(fdtd_solver* s, const void* buffer, int64_t bytes) {
+    if (!s || !buffer) return FDTD_ERR_INVALID_ARG;
+    SnapHeader h;
+    if (bytes < (int64_t)sizeof(h)) return (set_error(s, "snapshot truncated"), FDTD_ERR_INVALID_ARG);
+    std::memcpy(&h, buffer, sizeof(h));
+    if (h.magic != SNAP_MAGIC || h.ncell != s->ncell || h.precision != s->precision || h.kernel != s->opt.kernel ||
+        h.n_obj != (int32_t)s->objs.size())
+        return (set_error(s, "snapshot does not match this solver"), FDTD_ERR_INVALID_ARG);
+    auto regs = snap_regions(s);
+    size_t total = sizeof(SnapHeader) + s->objs.size() * sizeof(HostObject);
+    for (auto& r : regs) total += r.second;
+    if (bytes < (int64_t)total) return (set_error(s, "snapshot truncated"), FDTD_ERR_INVALID_ARG);
+    CUDA_TRY(s, cudaSetDevice(s->opt.device));
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    const char* p = (const char*)buffer + sizeof(h);
+    std::memcpy(s->objs.data(), p, s->objs.size() * sizeof(HostObject));
+    p += s->objs.size() * sizeof(HostObject);
+    for (auto& r : regs) {
+        CUDA_TRY(s, cudaMemcpy(r.first, p, r.second, cudaMemcpyHostToDevice));
+        p += r.second;
+    }
+    s->cur = h.cur;
+    s->step_index = h.step_index;
+    s->time = h.time;
+    s->state_time = h.state_time;
+    to_dev_objects(s);
+    CUDA_TRY(s, cudaMemcpy(s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice));
+    return FDTD_OK;
+}
+
+}  // extern "C"

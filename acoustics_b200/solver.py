@@ -1,0 +1,222 @@
+"""Host-side mirror of the reference's solver interface.
+
+`PML_WaveSolver` keeps the member names of src/wavesolver/PML_WaveSolver.h
+(stepSystem, FetchPressureData, Reinitialize_PML_WaveSolver, GetGrid) and
+`FDTD_AcousticSimulator` those of src/wavesolver/FDTD_AcousticSimulator.h
+(InitializeSolver, RunForSteps, Run, GetSolver).  Both drive the CUDA library
+through the C-ABI of include/fdtd_c.h; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional
+
+import numpy as np
+
+from ._lib import FDTDError, check, load
+from .scene import (FIELD_PRESSURE, GHOST_FACE_DTYPE, KERNEL_FUSED, PRECISION_FP64, Options, Scene,
+                    SceneDesc, SolverInfo)
+
+
+class PML_WaveSolver:
+    """One resident solve on one GPU (PML_WaveSolver.h:122-255)."""
+
+    def __init__(self, scene: Scene, precision: int = PRECISION_FP64, kernel: int = KERNEL_FUSED,
+                 graph_steps: int = 0, device: int = 0, tile_y: int = 0, x_chunk: int = 0):
+        self._L = load()
+        self.scene = scene
+        desc, self._keep = scene.to_c()
+        opt = Options(precision=precision, device=device, kernel=kernel, graph_steps=graph_steps,
+                      tile_y=tile_y, x_chunk=x_chunk)
+        h = C.c_void_p()
+        check(self._L.fdtd_solver_create(C.byref(desc), C.byref(opt), C.byref(h)))
+        self._h = h
+        self.precision = precision
+        self.n_listeners = scene.n_listeners
+        info = self.info()
+        self.divisions = tuple(info.divisions)
+        self.n_cells = int(info.n_cells)
+
+    # ---- lifecycle ----
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.fdtd_solver_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def Reinitialize_PML_WaveSolver(self, start_time: float = 0.0):
+        check(self._L.fdtd_solver_reset(self._h, float(start_time)), self._h)
+
+    # ---- stepping ----
+    def step(self, n: int, record: bool = True) -> np.ndarray:
+        """n x (stepSystem + FetchPressureData): listener series, shape (n, L)."""
+        out = np.zeros((n, max(1, self.n_listeners)), dtype=np.float64) if record else None
+        st = self._L.fdtd_solver_step(self._h, int(n), out.ctypes.data if record else None)
+        check(st, self._h)
+        self.last_status = st
+        return out[:, : self.n_listeners] if record else None
+
+    def step_device(self, n: int, device_ptr: int) -> int:
+        return check(self._L.fdtd_solver_step_device(self._h, int(n), C.c_void_p(device_ptr)), self._h)
+
+    def stepSystem(self) -> bool:
+        """One step; False once the end time is reached (PML_WaveSolver.cpp:579-609)."""
+        st = self._L.fdtd_solver_step(self._h, 1, None)
+        check(st, self._h)
+        return st != 1
+
+    def FetchPressureData(self) -> np.ndarray:
+        """Listener values at the current state (PML_WaveSolver.cpp:319-373)."""
+        out = np.zeros(max(1, self.n_listeners))
+        check(self._L.fdtd_solver_fetch_listeners(self._h, out.ctypes.data), self._h)
+        return out[: self.n_listeners]
+
+    def synchronize(self):
+        check(self._L.fdtd_solver_synchronize(self._h), self._h)
+
+    @property
+    def stream(self) -> int:
+        return int(self._L.fdtd_solver_stream(self._h) or 0)
+
+    def last_launch_count(self) -> int:
+        return int(self._L.fdtd_solver_last_launch_count(self._h))
+
+    # ---- introspection ----
+    def info(self) -> SolverInfo:
+        info = SolverInfo()
+        check(self._L.fdtd_solver_info_get(self._h, C.byref(info)), self._h)
+        return info
+
+    @property
+    def time(self) -> float:
+        return float(self.info().time)
+
+    def GetGrid(self):
+        """(flags[N] uint8, ghost faces) after the last classification (MAC_Grid.h:372-484)."""
+        flags = np.zeros(self.n_cells, dtype=np.uint8)
+        n = C.c_int64(0)
+        check(self._L.fdtd_solver_get_classification(self._h, flags.ctypes.data, None, C.byref(n)), self._h)
+        faces = np.zeros(n.value, dtype=GHOST_FACE_DTYPE)
+        cap = C.c_int64(n.value)
+        check(self._L.fdtd_solver_get_classification(self._h, None, faces.ctypes.data, C.byref(cap)), self._h)
+        return flags, faces
+
+    def field(self, which: int = FIELD_PRESSURE) -> np.ndarray:
+        N = list(self.divisions)
+        if which >= 5:
+            N[which - 5] += 1
+        count = N[0] * N[1] * N[2]
+        out = np.zeros(count, dtype=np.float64)
+        check(self._L.fdtd_solver_get_field(self._h, int(which), out.ctypes.data, count), self._h)
+        return out
+
+    def snapshot(self) -> bytes:
+        n = C.c_int64(0)
+        check(self._L.fdtd_solver_snapshot(self._h, None, C.byref(n)), self._h)
+        buf = (C.c_char * n.value)()
+        check(self._L.fdtd_solver_snapshot(self._h, buf, C.byref(n)), self._h)
+        return bytes(buf)
+
+    def restore(self, blob: bytes):
+        buf = C.create_string_buffer(blob, len(blob))
+        check(self._L.fdtd_solver_restore(self._h, buf, len(blob)), self._h)
+
+
+def scene_from_xml(path: str) -> Scene:
+    """Read an <impulse_response> XML scene through the library's reader."""
+    L = load()
+    h = C.c_void_p()
+    check(L.fdtd_scene_from_xml(path.encode(), C.byref(h)))
+    try:
+        d = L.fdtd_scene_desc_get(h).contents
+        from .scene import GaussianSource, PlaneConstraint, RigidObject
+        sc = Scene(cell_size=d.cell_size, divisions=tuple(d.divisions), time_step=d.time_step,
+                   domain_center=tuple(d.domain_center), sound_speed=d.sound_speed, density=d.density,
+                   pml_width=d.pml_width, pml_strength=d.pml_strength,
+                   boundary_condition_preset=d.boundary_condition_preset,
+                   air_viscosity_alpha=d.air_viscosity_alpha, start_time=d.start_time, end_time=d.end_time)
+        for i in range(d.n_objects):
+            o = d.objects[i]
+            sc.objects.append(RigidObject(o.shape, tuple(o.center), tuple(o.size), tuple(o.rotation), o.accel_kind,
+                                          o.accel_amplitude, o.accel_t0, o.accel_tau, tuple(o.accel_dir), o.motion,
+                                          tuple(o.velocity), tuple(o.gravity)))
+        for i in range(d.n_constraints):
+            p = d.constraints[i]
+            sc.constraints.append(PlaneConstraint(p.normal_dir, p.normal_sign, p.height))
+        for i in range(d.n_sources):
+            s = d.sources[i]
+            sc.sources.append(GaussianSource(tuple(s.position), s.width_time, s.width_space, s.offset_time,
+                                             s.normalize_constant))
+        if d.n_listeners:
+            sc.listeners = np.ctypeslib.as_array(d.listeners, shape=(d.n_listeners * 3,)).reshape(-1, 3).copy()
+        sc.steps = int(L.fdtd_scene_number_of_steps(h))
+        sc.output_pattern = (L.fdtd_scene_output_pattern(h) or b"%s").decode()
+        return sc
+    finally:
+        L.fdtd_scene_free(h)
+
+
+class FDTD_AcousticSimulator:
+    """Façade of FDTD_AcousticSimulator (FDTD_AcousticSimulator.cpp:419-621) with the
+    headless TUI_Run loop and the all_audio.dat listener output of SimWorld/AudioOutput."""
+
+    def __init__(self, scene_or_xml, precision: int = PRECISION_FP64, graph_steps: int = 0, device: int = 0):
+        self.scene = scene_from_xml(scene_or_xml) if isinstance(scene_or_xml, str) else scene_or_xml
+        self.precision = precision
+        self.graph_steps = graph_steps
+        self.device = device
+        self._solver: Optional[PML_WaveSolver] = None
+
+    def InitializeSolver(self):
+        self._solver = PML_WaveSolver(self.scene, precision=self.precision, graph_steps=self.graph_steps,
+                                      device=self.device)
+        return self._solver
+
+    def GetSolver(self) -> PML_WaveSolver:
+        if self._solver is None:
+            self.InitializeSolver()
+        return self._solver
+
+    def ResetStartTime(self, start_time: float):
+        self.GetSolver().Reinitialize_PML_WaveSolver(start_time)
+
+    def RunForSteps(self, n: int) -> np.ndarray:
+        return self.GetSolver().step(n)
+
+    def Run(self, n_steps: Optional[int] = None, audio_path: Optional[str] = None, chunk: int = 1000) -> np.ndarray:
+        """Step `n_steps` (default scene.steps) and append the listener rows to
+        `audio_path` (all_audio.dat layout: raw doubles, step-major)."""
+        n = int(n_steps if n_steps is not None else self.scene.steps)
+        rows = []
+        done = 0
+        while done < n:
+            m = min(chunk, n - done)
+            y = self.GetSolver().step(m)
+            if audio_path:
+                write_audio(audio_path, y)
+            rows.append(y)
+            done += m
+        return np.concatenate(rows, axis=0) if rows else np.zeros((0, self.scene.n_listeners))
+
+
+def write_audio(path: str, rows: np.ndarray):
+    data = np.ascontiguousarray(rows, dtype=np.float64)
+    check(load().fdtd_audio_append(path.encode(), data.ctypes.data, data.size))
+
+
+def device_count() -> int:
+    n = C.c_int32(0)
+    st = load().fdtd_device_count(C.byref(n))
+    return int(n.value) if st == 0 else 0

@@ -1,0 +1,249 @@
+/*
+ * fdtd_c.h — C-ABI of the B200 FDTD time-stepping library (libfdtd_b200.so).
+ *
+ * The reference exposes this path as the C++ class interface of PML_WaveSolver
+ * (src/wavesolver/PML_WaveSolver.h:122-255) driven by FDTD_AcousticSimulator
+ * (src/wavesolver/FDTD_AcousticSimulator.cpp:419-621) and SimWorld::StepWorld
+ * (src/wavesolver/SimWorld.cpp:507-592).  Each entry point below names the
+ * reference member it replaces.  Signatures use plain pointers and sizes only;
+ * no exception crosses this boundary: every call returns an fdtd_status and the
+ * message of the last failure is kept per handle (fdtd_solver_last_error) and
+ * per thread (fdtd_last_error).
+ *
+ * Units are SI (m, s, kg/m^3).  Flat cell index is i*Ny*Nz + j*Nz + k with z
+ * contiguous (src/field/ScalarField.cpp:86-97).
+ */
+#ifndef FDTD_C_H
+#define FDTD_C_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FDTD_ABI_VERSION 1
+
+typedef int32_t fdtd_status;
+enum {
+    FDTD_OK = 0,
+    FDTD_END_OF_TIME = 1,          /* stepSystem() returning false at endTime (PML_WaveSolver.cpp:605-606) */
+    FDTD_ERR_INVALID_ARG = -1,     /* std::runtime_error on bad input */
+    FDTD_ERR_OOM = -2,
+    FDTD_ERR_CUDA = -3,
+    FDTD_ERR_NUMERIC = -4,         /* NaN/Inf seen in a listener series */
+    FDTD_ERR_TIMEOUT = -5,         /* a bounded device wait ran out */
+    FDTD_ERR_GEOMETRY = -6,        /* fresh cell inside an object (MAC_Grid.cpp:2050-2053) */
+    FDTD_ERR_UNSUPPORTED = -7,     /* a reference feature outside this library's scope */
+    FDTD_ERR_IO = -8,
+    FDTD_ERR_BUSY = -9             /* server queue full / slot table full */
+};
+
+/* ---------------------------------------------------------------------------
+ * Scene description (plain data, copied at create time)
+ * ------------------------------------------------------------------------- */
+enum { FDTD_SHAPE_SPHERE = 0, FDTD_SHAPE_BOX = 1, FDTD_SHAPE_ELLIPSOID = 2 };
+
+/* Boundary normal-acceleration model of an object (replaces the vibrational
+ * sources summed by FDTD_RigidObject::EvaluateBoundaryAcceleration,
+ * src/wavesolver/FDTD_RigidObject.cpp:330-368).  g(t) = A*exp(-((t-t0)/tau)^2/2). */
+enum {
+    FDTD_ACCEL_NONE = 0,
+    FDTD_ACCEL_GAUSSIAN_TRANSLATION = 1, /* a(x,t) = g(t) * dir (rigid translation)       */
+    FDTD_ACCEL_GAUSSIAN_PULSATION = 2    /* a(x,t) = g(t) * n(x) (sphere only, monopole) */
+};
+
+enum { FDTD_MOTION_STATIC = 0, FDTD_MOTION_BALLISTIC = 1 };
+
+typedef struct {
+    int32_t shape;
+    int32_t accel_kind;
+    int32_t motion;
+    int32_t _pad;
+    double center[3];     /* body centre at t = 0 (world)                            */
+    double rotation[9];   /* row-major object->world rotation (identity if unused)    */
+    double size[3];       /* sphere: size[0]=radius; box: half extents; ellipsoid: semi-axes */
+    double accel_amplitude;
+    double accel_t0;
+    double accel_tau;
+    double accel_dir[3];
+    double velocity[3];   /* ballistic: x(t) = c + v t + g t^2 / 2                    */
+    double gravity[3];
+} fdtd_object_desc;
+
+/* FDTD_PlaneConstraint (src/wavesolver/FDTD_PlaneConstraint.h:9-44) */
+typedef struct {
+    int32_t normal_dir;   /* 0,1,2 */
+    int32_t normal_sign;  /* +1 / -1 */
+    double height;
+} fdtd_plane_desc;
+
+/* GaussianPressureSource (src/wavesolver/GaussianPressureSource.h:11-51).  The
+ * parser defaults (ImpulseResponseParser.cpp:657-669) are applied by
+ * fdtd_gaussian_source_defaults(). */
+typedef struct {
+    double position[3];
+    double width_time;
+    double width_space;
+    double offset_time;
+    double normalize_constant;
+} fdtd_gaussian_source_desc;
+
+typedef struct {
+    double cell_size;              /* <solver cellsize>                                   */
+    int32_t divisions[3];          /* <solver_control_policy gridresolution> (per axis)   */
+    int32_t boundary_condition_preset; /* only 0 ("no wall") is on this path            */
+    double domain_center[3];
+    double sound_speed;
+    double density;
+    double time_step;              /* 1 / timestepfrequency                               */
+    double pml_width;              /* cells                                               */
+    double pml_strength;
+    double air_viscosity_alpha;    /* 0 on this path                                      */
+    double start_time;
+    double end_time;               /* <= 0: no end                                         */
+    int32_t n_objects;
+    int32_t n_constraints;
+    int32_t n_sources;
+    int32_t n_listeners;
+    const fdtd_object_desc* objects;
+    const fdtd_plane_desc* constraints;
+    const fdtd_gaussian_source_desc* sources;
+    const double* listeners;       /* 3 * n_listeners, world coordinates                  */
+} fdtd_scene_desc;
+
+enum {
+    FDTD_PRECISION_FP64 = 0,              /* bit-faithful FP64 path                       */
+    FDTD_PRECISION_FP32_COMPENSATED = 1   /* FP32 fields, increment-form accumulation     */
+};
+
+enum {
+    FDTD_KERNEL_FUSED = 0,    /* one fused stencil kernel per step                       */
+    FDTD_KERNEL_PHASED = 1    /* plain path: one kernel per reference phase (FP64 only)   */
+};
+
+typedef struct {
+    int32_t precision;        /* FDTD_PRECISION_*                                        */
+    int32_t device;           /* CUDA ordinal                                            */
+    int32_t kernel;           /* FDTD_KERNEL_*                                           */
+    int32_t graph_steps;      /* >0: capture this many steps per CUDA graph launch       */
+    int32_t tile_y;           /* 0: autotuned/default                                    */
+    int32_t x_chunk;          /* 0: autotuned/default                                    */
+} fdtd_options;
+
+typedef struct {
+    int32_t divisions[3];
+    int32_t n_listeners;
+    int64_t n_cells;
+    int64_t n_pml_cells;
+    int64_t n_interior_cells;      /* non-PML cells                                     */
+    int64_t device_bytes;          /* HBM held by this solver                           */
+    int64_t step_index;
+    double time;                   /* current simulation time                          */
+    double time_step;
+    double algorithmic_bytes_per_step; /* w*(3*N_interior + 14*N_pml)                  */
+} fdtd_solver_info;
+
+/* One ghost face, MAC_Grid::GhostCell (src/wavesolver/MAC_Grid.h:97-145). */
+typedef struct {
+    int32_t owner_cell;
+    int32_t neighbour_cell;
+    int32_t topology;        /* +-(dim+1), owner -> neighbour                       */
+    int32_t type;            /* 0 object, 1 constraint                              */
+    int32_t boundary_object; /* index into scene objects                            */
+    int32_t _pad;
+    uint64_t key;            /* Szudzik(min, max), MAC_Grid.h:108-116                */
+} fdtd_ghost_face;
+
+/* Per-cell classification byte returned by fdtd_solver_get_classification. */
+enum {
+    FDTD_CELL_BULK = 1,          /* _isBulkCell                                   */
+    FDTD_CELL_GHOST = 2,         /* _isGhostCell                                  */
+    FDTD_CELL_VALID_HISTORY = 4, /* _pressureCellHasValidHistory                  */
+    FDTD_CELL_PML = 8,           /* _isPMLCell                                    */
+    FDTD_CELL_CONSTRAINT = 16    /* solid because a plane constraint holds it      */
+};
+
+enum {
+    FDTD_FIELD_PRESSURE = 0,        /* p^{n}   : _pCollocated[_pCollocatedInd]      */
+    FDTD_FIELD_PRESSURE_PREV = 1,   /* p^{n-1}                                       */
+    FDTD_FIELD_PML_PX = 2,          /* split pressures _p[0..2] (N cells)            */
+    FDTD_FIELD_PML_PY = 3,
+    FDTD_FIELD_PML_PZ = 4,
+    FDTD_FIELD_VX = 5,              /* face velocities _v[0..2]                      */
+    FDTD_FIELD_VY = 6,
+    FDTD_FIELD_VZ = 7
+};
+
+typedef struct fdtd_solver fdtd_solver;
+
+/* ------------------------------------------------------------------------ */
+/* library                                                                  */
+int32_t fdtd_abi_version(void);
+const char* fdtd_last_error(void);           /* thread-local message of the last failed call */
+fdtd_status fdtd_device_count(int32_t* count);
+
+/* Parser defaults of <gaussian_pressure_source> (ImpulseResponseParser.cpp:657-669):
+ * width_space <= 0 -> sound_speed*width_time; normalize_constant == 0 ->
+ * 1/pow(sqrt(2*pi)*width_space, 3). */
+fdtd_status fdtd_gaussian_source_defaults(fdtd_gaussian_source_desc* src, double sound_speed);
+
+/* ------------------------------------------------------------------------ */
+/* solver: replaces PML_WaveSolver                                          */
+
+/* PML_WaveSolver(bbox, settings, objects) + Reinitialize_PML_WaveSolver(useBoundary=true, t0)
+ * (PML_WaveSolver.cpp:78-146) + FDTD_AcousticSimulator::ResetStartTime (:458-523). */
+fdtd_status fdtd_solver_create(const fdtd_scene_desc* scene, const fdtd_options* options,
+                               fdtd_solver** out);
+fdtd_status fdtd_solver_destroy(fdtd_solver* s);
+/* Reinitialize_PML_WaveSolver(true, t0) + ResetCellHistory(true) (PML_WaveSolver.cpp:102-146) */
+fdtd_status fdtd_solver_reset(fdtd_solver* s, double start_time);
+/* n x (stepSystem() + FetchPressureData(listeners)) : SimWorld::StepWorld (SimWorld.cpp:507-592).
+ * listener_out: host buffer of n_steps*n_listeners doubles (row = step), may be NULL.
+ * Returns FDTD_END_OF_TIME when end_time was reached. */
+fdtd_status fdtd_solver_step(fdtd_solver* s, int32_t n_steps, double* listener_out);
+/* Same, with the listener series written to device memory (n_steps*n_listeners doubles)
+ * and no host synchronisation. */
+fdtd_status fdtd_solver_step_device(fdtd_solver* s, int32_t n_steps, void* device_listener_out);
+/* FetchPressureData(listeningPoints, data, -1) at the current state (PML_WaveSolver.cpp:319-373) */
+fdtd_status fdtd_solver_fetch_listeners(fdtd_solver* s, double* out);
+fdtd_status fdtd_solver_info_get(fdtd_solver* s, fdtd_solver_info* info);
+/* classifyCells_FAST result (MAC_Grid.cpp:3455-3891): flags_n (n_cells bytes, may be NULL);
+ * faces (capacity *n_faces on entry, count on return; may be NULL to query the count). Faces are
+ * ordered by (owner_cell, key). */
+fdtd_status fdtd_solver_get_classification(fdtd_solver* s, uint8_t* flags_n, fdtd_ghost_face* faces,
+                                           int64_t* n_faces);
+/* Field read-back as doubles (FetchCell / GetGrid accessors). */
+fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, int64_t count);
+/* Synchronise the solver's stream. */
+fdtd_status fdtd_solver_synchronize(fdtd_solver* s);
+/* The cudaStream_t every kernel of this solver is launched on (for event timing). */
+void* fdtd_solver_stream(fdtd_solver* s);
+const char* fdtd_solver_last_error(fdtd_solver* s);
+/* Kernel launches issued by the most recent fdtd_solver_step* call. */
+int64_t fdtd_solver_last_launch_count(fdtd_solver* s);
+
+/* Snapshot / restore of the resident state (_SaveSimulationSnapshot,
+ * FDTD_AcousticSimulator.cpp:381-415).  bytes: query with buffer NULL. */
+fdtd_status fdtd_solver_snapshot(fdtd_solver* s, void* buffer, int64_t* bytes);
+fdtd_status fdtd_solver_restore(fdtd_solver* s, const void* buffer, int64_t bytes);
+
+/* ------------------------------------------------------------------------ */
+/* XML scene reader (ImpulseResponseParser subset, ImpulseResponseParser.cpp:55-751) */
+typedef struct fdtd_scene fdtd_scene;
+fdtd_status fdtd_scene_from_xml(const char* path, fdtd_scene** out);
+const fdtd_scene_desc* fdtd_scene_desc_get(const fdtd_scene* sc);
+/* int steps from <number_of_timesteps> (0 if absent) and the output pattern */
+int32_t fdtd_scene_number_of_steps(const fdtd_scene* sc);
+const char* fdtd_scene_output_pattern(const fdtd_scene* sc);
+void fdtd_scene_free(fdtd_scene* sc);
+
+/* all_audio.dat writer (AudioOutput, src/wavesolver/AudioOutput.cpp:27-64): appends
+ * n_steps*n_listeners raw doubles. */
+fdtd_status fdtd_audio_append(const char* path, const double* data, int64_t count);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FDTD_C_H */
