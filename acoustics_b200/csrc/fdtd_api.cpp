@@ -280,6 +280,38 @@ fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
     }
     s->n_interior = inner;
     s->n_pml = s->ncell - inner;
+    // non-PML box and the PML shell as six disjoint slabs (x slabs full, y slabs
+    // inside the x range, z slabs inside the x and y ranges)
+    int lo[3], hi[3];
+    for (int d = 0; d < 3; ++d) {
+        lo[d] = 0;
+        while (lo[d] < s->N[d] && s->tab[d].pml_cell[lo[d]]) ++lo[d];
+        hi[d] = s->N[d];
+        while (hi[d] > lo[d] && s->tab[d].pml_cell[hi[d] - 1]) --hi[d];
+        s->interior.lo[d] = lo[d];
+        s->interior.hi[d] = hi[d];
+    }
+    ShellBoxes& B = s->shell;
+    std::memset(&B, 0, sizeof(B));
+    auto add = [&](int x0, int x1, int y0, int y1, int z0, int z1) {
+        if (x1 <= x0 || y1 <= y0 || z1 <= z0) return;
+        B.start[B.n][0] = x0; B.start[B.n][1] = y0; B.start[B.n][2] = z0;
+        B.size[B.n][0] = x1 - x0; B.size[B.n][1] = y1 - y0; B.size[B.n][2] = z1 - z0;
+        B.first[B.n + 1] = B.first[B.n] + (long long)(x1 - x0) * (y1 - y0) * (z1 - z0);
+        ++B.n;
+    };
+    const int* N = s->N;
+    if (lo[0] >= hi[0] || lo[1] >= hi[1] || lo[2] >= hi[2]) {
+        add(0, N[0], 0, N[1], 0, N[2]);  // every cell is a PML cell
+        for (int d = 0; d < 3; ++d) s->interior.lo[d] = s->interior.hi[d] = 0;
+    } else {
+        add(0, lo[0], 0, N[1], 0, N[2]);
+        add(hi[0], N[0], 0, N[1], 0, N[2]);
+        add(lo[0], hi[0], 0, lo[1], 0, N[2]);
+        add(lo[0], hi[0], hi[1], N[1], 0, N[2]);
+        add(lo[0], hi[0], lo[1], hi[1], 0, lo[2]);
+        add(lo[0], hi[0], lo[1], hi[1], hi[2], N[2]);
+    }
     return FDTD_OK;
 }
 
@@ -441,6 +473,28 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     (void)di;
     s->lis_cap_steps = std::max(256, o.graph_steps);
     cv.add((void**)&s->d_lis, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8);
+    // ghost-neighbour list: at most 6 bulk neighbours per solid cell; solid cells lie
+    // in the object boxes (dilated by 2 cells, and by the travel of moving bodies)
+    {
+        double cells = 4096;
+        for (int i = 0; i < sc->n_objects; ++i) {
+            HostObject tmp;
+            tmp.d = sc->objects[i];
+            host_object_pose(tmp, sc->start_time);
+            host_update_bbox(tmp);
+            double vol = 1.0;
+            for (int d = 0; d < 3; ++d) {
+                double ext = (tmp.bmax[d] - tmp.bmin[d]) / s->h + 4.0;
+                if (tmp.d.motion != FDTD_MOTION_STATIC) ext *= 2.0;
+                vol *= std::min(ext, (double)N[d]);
+            }
+            cells += 6.0 * vol;
+        }
+        cells += 2.0 * sc->n_constraints * ((double)N[0] * N[1] + (double)N[1] * N[2] + (double)N[0] * N[2]);
+        s->region.ghost_cap = (int)std::min<double>(cells, (double)n);
+        cv.add((void**)&s->d_ghost_list, (size_t)s->region.ghost_cap * 4);
+        cv.add((void**)&s->d_ghost_count, 16);
+    }
     void* base = nullptr;
     cudaError_t e = cudaMalloc(&base, cv.off);
     if (e != cudaSuccess) {
@@ -474,6 +528,31 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     P.n_src = (int)s->sources.size();
     P.n_lis = s->L;
     P.precision = s->precision;
+    P.ghost_list = s->d_ghost_list;
+    P.ghost_count = s->d_ghost_count;
+    P.ghost_cap = s->region.ghost_cap;
+    s->region.interior = s->interior;
+    s->region.shell = s->shell;
+    s->region.sources = 0;
+    // bounding box of the source supports (cells whose centre may lie strictly inside)
+    {
+        Box3 r{};
+        bool any = false;
+        for (const auto& g : s->sources) {
+            for (int d = 0; d < 3; ++d) {
+                const double a = (g.position[d] - 2.0 * g.width_space - s->bmin[d]) / s->h - 0.5;
+                const double b = (g.position[d] + 2.0 * g.width_space - s->bmin[d]) / s->h - 0.5;
+                const int lo = std::max(s->interior.lo[d], (int)std::floor(a));
+                const int hi = std::min(s->interior.hi[d], (int)std::ceil(b) + 1);
+                if (!any) { r.lo[d] = lo; r.hi[d] = hi; }
+                else { r.lo[d] = std::min(r.lo[d], lo); r.hi[d] = std::max(r.hi[d], hi); }
+            }
+            any = true;
+        }
+        for (int d = 0; d < 3; ++d)
+            if (!any || r.hi[d] < r.lo[d]) r.hi[d] = r.lo[d];
+        s->region.src_region = r;
+    }
     for (int i = 0; i < P.n_plane; ++i) {
         P.plane[i].dir = s->planes[i].normal_dir;
         P.plane[i].sign = s->planes[i].normal_sign;
@@ -516,6 +595,8 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     CUDA_TRY(s.get(), cudaMallocHost((void**)&s->h_lis_stage, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8));
     // tile choice: 8 rows; x chunk so that the grid has >= 4 waves on 148 SMs
     s->tile_y = o.tile_y > 0 ? o.tile_y : 8;
+    s->xb = (o.x_chunk == 2 || o.x_chunk == 4 || o.x_chunk == 8) ? o.x_chunk : 4;
+    s->region.xb = s->xb;
     if (o.x_chunk > 0) s->xchunk = o.x_chunk;
     else {
         const long long cols = (long long)((N[2] + 31) / 32) * ((N[1] + s->tile_y - 1) / s->tile_y);
@@ -535,7 +616,7 @@ fdtd_status fdtd_solver_destroy(fdtd_solver* s) {
     if (!s) return FDTD_OK;
     cudaSetDevice(s->opt.device);
     cudaStreamSynchronize(s->stream);
-    for (int i = 0; i < 2; ++i)
+    for (int i = 0; i < 4; ++i)
         if (s->graph_exec[i]) cudaGraphExecDestroy(s->graph_exec[i]);
     if (s->arena) cudaFree(s->arena);
     if (s->h_lis_stage) cudaFreeHost(s->h_lis_stage);
@@ -614,7 +695,7 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     st = upload_params(s);
     if (st != FDTD_OK) return st;
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-    for (int i = 0; i < 2; ++i) {
+    for (int i = 0; i < 4; ++i) {
         if (s->graph_exec[i]) cudaGraphExecDestroy(s->graph_exec[i]);
         s->graph_exec[i] = nullptr;
     }

@@ -54,6 +54,30 @@ struct DevSource {
     double scale;        // (1/3.6836) * normalize constant
 };
 
+// Non-PML box [lo, hi) of the grid.
+struct Box3 {
+    int lo[3];
+    int hi[3];
+};
+
+// The PML shell as up to six disjoint boxes; first[] holds prefix sums of cell counts.
+struct ShellBoxes {
+    int n;
+    int start[6][3];
+    int size[6][3];
+    long long first[7];
+};
+
+// Launch description of one region-split step.
+struct RegionLaunch {
+    Box3 interior;
+    ShellBoxes shell;
+    Box3 src_region;   // bounding box of the source supports inside the non-PML box
+    int sources;       // launch the source kernel this step
+    int ghost_cap;     // capacity of the ghost-neighbour list (0: no list kernel)
+    int xb;            // x planes per interior thread
+};
+
 // Written by the step prologue, read by the rest of the step.
 struct StepConsts {
     double t;                       // simulation time at the start of the step
@@ -103,6 +127,9 @@ struct SolveParams {
     const double* listeners;      // 3*n_lis
     int* solid_pml;               // solid cells inside the PML (re-zeroed every step)
     int n_solid_pml;
+    int* ghost_list;              // non-PML bulk cells with a solid neighbour
+    int* ghost_count;
+    int ghost_cap;
     int precision;                // 0 fp64, 1 fp32 compensated
 };
 

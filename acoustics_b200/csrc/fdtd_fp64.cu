@@ -19,6 +19,7 @@ namespace fdtd {
 // validHistory <- isBulk; isBulk <- true (MAC_Grid.cpp:3464-3472)
 __global__ void k_cls_reset(const SolveParams* __restrict__ Pp, long long n) {
     uint8_t* cls = Pp->cls;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *Pp->ghost_count = 0;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
         const uint8_t code = cls[c];
         cls[c] = CLS_BULK | ((code & CLS_BULK) ? CLS_VALID : 0);
@@ -83,6 +84,10 @@ __global__ void k_cls_ghost(const SolveParams* __restrict__ Pp, long long n) {
             const double pos[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
             const int o = lowest_object(P, pos);
             P.gobj[c] = (P.gobj[c] & GOBJ_CONSTRAINT) | (uint8_t)(o < 0 ? GOBJ_NONE : o);
+        } else if (mask && !(P.pml_cell[0][i] || P.pml_cell[1][j] || P.pml_cell[2][k])) {
+            // non-PML bulk cell next to a solid: updated by k_ghost_cells
+            const int slot = atomicAdd(P.ghost_count, 1);
+            if (slot < P.ghost_cap) P.ghost_list[slot] = (int)c;
         }
         P.cls[c] = (uint8_t)((code & (CLS_BULK | CLS_VALID)) | mask);
     }
@@ -466,4 +471,15 @@ cudaError_t launch_phased_fp64(const SolveParams* dP, const int N[3], int cur, d
     return cudaGetLastError();
 }
 
+}  // namespace fdtd
+
+// ---------------------------------------------------------------------------
+// region-split step, FP64
+// ---------------------------------------------------------------------------
+#include "fdtd_region.cuh"
+namespace fdtd {
+cudaError_t launch_step_regions_fp64(const SolveParams* dP, const RegionLaunch& R, int cur, cudaStream_t s,
+                                     int* launches) {
+    return launch_regions<double>(dP, R, cur, s, launches);
+}
 }  // namespace fdtd

@@ -59,13 +59,19 @@ struct fdtd_solver {
     double* h_lis_stage = nullptr;
     int lis_cap_steps = 0;
     int tile_y = 8, xchunk = 16;
+    int xb = 4;                       // planes per thread of the interior kernel
+    fdtd::Box3 interior{};            // non-PML box
+    fdtd::ShellBoxes shell{};         // PML shell boxes
+    fdtd::RegionLaunch region{};      // launch description of the region-split step
+    int* d_ghost_list = nullptr;
+    int* d_ghost_count = nullptr;
     // stepping state
     int cur = 0;
     long long step_index = 0;
     double time = 0.0;        // simulation time of the next step (host mirror of the device clock)
     double state_time = 0.0;  // SimWorld::_state.time for object animation
     bool classified_after_first_step = false;
-    cudaGraphExec_t graph_exec[2] = {nullptr, nullptr};
+    cudaGraphExec_t graph_exec[4] = {nullptr, nullptr, nullptr, nullptr};  // [parity + 2*sources]
     long long launches = 0;
     long long last_launches = 0;
     long long graph_launches_per_exec = 0;

@@ -6,6 +6,12 @@
 
 namespace fdtd {
 
+// region-split step: PML shell, interior, ghost-neighbour list and (while active) sources
+cudaError_t launch_step_regions_fp64(const SolveParams* dP, const RegionLaunch& R, int cur, cudaStream_t s,
+                                     int* launches);
+cudaError_t launch_step_regions_fp32(const SolveParams* dP, const RegionLaunch& R, int cur, cudaStream_t s,
+                                     int* launches);
+
 // fdtd_fp64.cu (compiled with -fmad=false)
 cudaError_t launch_prologue_fp64(const SolveParams* dP, int n_solid_pml, cudaStream_t s);
 cudaError_t launch_step_fused_fp64(const SolveParams* dP, const int N[3], int cur, int tile_y, int xchunk,

@@ -1,0 +1,303 @@
+// fdtd_region.cuh — the step split by region, one lean kernel per region:
+//
+//   k_interior   non-PML cells, box [lo, hi): ghost-aware Laplacian, leapfrog /
+//                compensated increment, Gaussian sources
+//                (MAC_Grid.cpp:187-299 + :921-944).  Only pressure words move:
+//                p^n (neighbours from the CTA's rows), p^{n-1} or the increment,
+//                p^{n+1}, plus one classification byte.
+//   k_pml_shell  the six slab boxes of the PML shell: face velocities
+//                (MAC_Grid.cpp:461-479) and split-field pressures (:496-508).
+//
+// Face ownership: a PML face is written by the cell to its right; the one face
+// layer whose right cell is not a PML cell (x = W h on the low side) is written
+// by its left (PML) cell, so the interior kernel never touches velocities.
+//
+// Cells next to a solid (a compact list built by the classification) and the
+// Gaussian sources while they are active have kernels of their own, so the
+// interior kernel is a pure 7-point leapfrog.
+//
+// Interior mapping: a CTA of 32 (z) x 8 (y) threads, each thread owns XB
+// consecutive x planes of one (y, z) column.  All loads of the XB planes
+// (p^n at XB+2 planes, y neighbours, p^{n-1}/increment, classification) are
+// issued before any arithmetic so that every thread keeps ~5*XB independent
+// HBM requests in flight; z neighbours come from the warp with shuffles.
+#pragma once
+#include "fdtd_device.cuh"
+#include "fdtd_geometry.cuh"
+#include "fdtd_stencil.cuh"
+
+namespace fdtd {
+
+// Ghost-aware Laplacian of one bulk cell with at least one solid neighbour
+// (MAC_Grid.cpp:267-297); returns the unscaled sum and the number of axes with
+// ghost cells on both sides.
+template <typename T>
+__device__ __noinline__ T ghost_laplacian(const SolveParams& P, long long c, const int idx[3], unsigned mask, T p0,
+                                          const T nbp[3], const T nbm[3], double t, int* surrounded) {
+    const long long strides[3] = {(long long)P.N[1] * P.N[2], P.N[2], 1};
+    T lap = 0.0;
+    int s = 0;
+    for (int d = 0; d < 3; ++d) {
+        const bool gn = (mask >> (2 * d)) & 1u;
+        const bool gp = (mask >> (2 * d + 1)) & 1u;
+        T gpv = 0, gnv = 0;
+        if (gp || gn) {
+            double own[3] = {P.cpos[0][idx[0]], P.cpos[1][idx[1]], P.cpos[2][idx[2]]};
+            if (gp) {
+                own[d] = P.cpos[d][idx[d] + 1];
+                gpv = (T)ghost_pressure(P, P.gobj[c + strides[d]], own, d, -1, (double)p0, t);
+            }
+            if (gn) {
+                own[d] = P.cpos[d][idx[d] - 1];
+                gnv = (T)ghost_pressure(P, P.gobj[c - strides[d]], own, d, +1, (double)p0, t);
+            }
+        }
+        if (gp && gn) {
+            lap = lap + (gpv + gnv - (T)2.0 * p0) / (T)(9.0 / 16.0);
+            ++s;
+        } else if (gp) {
+            lap = lap + (gpv + (T)0.75 * nbm[d] - (T)(7.0 / 4.0) * p0) / (T)(21.0 / 32.0);
+        } else if (gn) {
+            lap = lap + ((T)0.75 * nbp[d] + gnv - (T)(7.0 / 4.0) * p0) / (T)(21.0 / 32.0);
+        } else {
+            lap = lap + (nbp[d] + nbm[d] - (T)2.0 * p0);
+        }
+    }
+    *surrounded = s;
+    return lap;
+}
+
+// Full update of one non-PML bulk cell next to a solid (ghost-aware Laplacian,
+// cavity freeze), everything re-read from memory.  Sources are added by
+// k_sources afterwards, as the reference adds them after the update
+// (MAC_Grid.cpp:938-944).
+template <typename T>
+__global__ void __launch_bounds__(128) k_ghost_cells(const SolveParams* __restrict__ Pp, int cur) {
+    const SolveParams& P = *Pp;
+    const int n = *P.ghost_count;
+    const int Ny = P.N[1], Nz = P.N[2];
+    const long long sx = (long long)Ny * Nz;
+    const T* __restrict__ pc = (const T*)P.p[cur];
+    T* __restrict__ pn = (T*)P.p[cur ^ 1];
+    const double t = P.consts->t;
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n && g < P.ghost_cap; g += gridDim.x * blockDim.x) {
+        const long long c = P.ghost_list[g];
+        const int x = (int)(c / sx), y = (int)((c / Nz) % Ny), z = (int)(c % Nz);
+        const uint8_t code = P.cls[c];
+        const T p0 = pc[c];
+        const T nbp[3] = {pc[c + sx], pc[c + Nz], pc[c + 1]};
+        const T nbm[3] = {pc[c - sx], pc[c - Nz], pc[c - 1]};
+        const int idx[3] = {x, y, z};
+        int surrounded = 0;
+        T lap = ghost_laplacian<T>(P, c, idx, code & CLS_MASK, p0, nbp, nbm, t, &surrounded);
+        lap = lap * (T)P.lap_scale;
+        const bool cavity = (surrounded > 1) && (code & CLS_VALID);
+        if constexpr (sizeof(T) == 8) {
+            pn[c] = cavity ? p0 : (T)2.0 * p0 - pn[c] + lap * (T)P.c2k2;
+        } else {
+            const float d = cavity ? 0.0f : P.dinc[c] + (float)(lap * (T)P.c2k2);
+            P.dinc[c] = d;
+            pn[c] = p0 + d;
+        }
+    }
+}
+
+// pNext += k * sum_s G_s(x, t + k/2) over the bounding box of the source
+// supports clipped to the non-PML box (GaussianPressureSource.cpp:6-30).
+template <typename T>
+__global__ void __launch_bounds__(256) k_sources(const SolveParams* __restrict__ Pp, int cur, Box3 region) {
+    const SolveParams& P = *Pp;
+    const StepConsts& sc = *P.consts;
+    bool any_src = false;
+    for (int s = 0; s < P.n_src; ++s) any_src |= (sc.src_tf[s] != 0.0);
+    if (!any_src) return;
+    const int nx = region.hi[0] - region.lo[0], ny = region.hi[1] - region.lo[1], nz = region.hi[2] - region.lo[2];
+    const long long total = (long long)nx * ny * nz;
+    const int Ny = P.N[1], Nz = P.N[2];
+    const T* __restrict__ pc = (const T*)P.p[cur];
+    T* __restrict__ pn = (T*)P.p[cur ^ 1];
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+        const int z = region.lo[2] + (int)(t % nz);
+        const int y = region.lo[1] + (int)((t / nz) % ny);
+        const int x = region.lo[0] + (int)(t / ((long long)nz * ny));
+        const long long c = ((long long)x * Ny + y) * Nz + z;
+        if (!(P.cls[c] & CLS_BULK)) continue;
+        const double src = source_sum(P, sc, P.cpos[0][x], P.cpos[1][y], P.cpos[2][z]);
+        if constexpr (sizeof(T) == 8) {
+            pn[c] += src * P.k;
+        } else {
+            const float d = P.dinc[c] + (float)(src * P.k);
+            P.dinc[c] = d;
+            pn[c] = pc[c] + d;
+        }
+    }
+}
+
+template <typename T, int XB>
+__global__ void __launch_bounds__(256) k_interior(const SolveParams* __restrict__ Pp, int cur, Box3 box) {
+    const SolveParams& P = *Pp;
+    constexpr bool COMP = sizeof(T) == 4;
+    const int lane = threadIdx.x;
+    const int z = box.lo[2] + blockIdx.x * 32 + lane;
+    const int y = box.lo[1] + blockIdx.y * 8 + threadIdx.y;
+    const int x0 = box.lo[0] + blockIdx.z * XB;
+    const bool active = (z < box.hi[2]) && (y < box.hi[1]);
+    const int zc = min(z, box.hi[2] - 1);
+    const int yc = min(y, box.hi[1] - 1);
+    const int nx = min(XB, box.hi[0] - x0);
+    const int Nz = P.N[2];
+    const int sx = P.N[1] * Nz;
+    const long long off = (long long)x0 * sx + (long long)yc * Nz + zc;
+    const T* __restrict__ pc = (const T*)P.p[cur] + off;
+    T* __restrict__ pn = (T*)P.p[cur ^ 1] + off;
+    float* __restrict__ dinc = P.dinc + off;
+    const uint8_t* __restrict__ cls = P.cls + off;
+
+    // ---- issue every load of the XB planes before any arithmetic ----
+    T pcol[XB + 2];
+    T ym[XB], yp[XB], prev[XB];
+    uint8_t code[XB];
+    pcol[0] = pc[-sx];
+#pragma unroll
+    for (int i = 0; i < XB + 1; ++i)
+        if (i <= nx) pcol[i + 1] = pc[i * sx];
+#pragma unroll
+    for (int i = 0; i < XB; ++i) {
+        if (i < nx) {
+            ym[i] = pc[i * sx - Nz];
+            yp[i] = pc[i * sx + Nz];
+            if constexpr (COMP) prev[i] = (T)dinc[i * sx];
+            else prev[i] = pn[i * sx];
+            code[i] = cls[i * sx];
+        }
+    }
+    const T c2k2 = (T)P.c2k2;
+    const T lap_scale = (T)P.lap_scale;
+
+#pragma unroll
+    for (int i = 0; i < XB; ++i) {
+        if (i >= nx) break;
+        const T p0 = pcol[i + 1];
+        T zm = __shfl_up_sync(0xffffffffu, p0, 1);
+        T zp = __shfl_down_sync(0xffffffffu, p0, 1);
+        if (lane == 0) zm = pc[i * sx - 1];
+        if (lane == 31 || z + 1 >= box.hi[2]) zp = pc[i * sx + 1];
+        // solid cells stay untouched; cells next to a solid go to k_ghost_cells
+        if (!active || (code[i] & (CLS_BULK | CLS_MASK)) != CLS_BULK) continue;
+        T lap = 0.0;
+        lap = lap + (pcol[i + 2] + pcol[i] - (T)2.0 * p0);
+        lap = lap + (yp[i] + ym[i] - (T)2.0 * p0);
+        lap = lap + (zp + zm - (T)2.0 * p0);
+        lap = lap * lap_scale;
+        if constexpr (!COMP) {
+            pn[i * sx] = (T)2.0 * p0 - prev[i] + lap * c2k2;
+        } else {
+            const float d = (float)prev[i] + (float)(lap * c2k2);
+            dinc[i * sx] = d;
+            pn[i * sx] = p0 + d;
+        }
+    }
+}
+
+// One PML cell per thread over the concatenated shell boxes (z fastest).
+template <typename T>
+__global__ void __launch_bounds__(256) k_pml_shell(const SolveParams* __restrict__ Pp, int cur, ShellBoxes B) {
+    const SolveParams& P = *Pp;
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= B.first[B.n]) return;
+    int b = 0;
+    while (t >= B.first[b + 1]) ++b;
+    long long r = t - B.first[b];
+    const int z = B.start[b][2] + (int)(r % B.size[b][2]);
+    r /= B.size[b][2];
+    const int y = B.start[b][1] + (int)(r % B.size[b][1]);
+    const int x = B.start[b][0] + (int)(r / B.size[b][1]);
+    const int N[3] = {P.N[0], P.N[1], P.N[2]};
+    const long long sx = (long long)N[1] * N[2];
+    const long long c = (long long)x * sx + (long long)y * N[2] + z;
+    const T* __restrict__ pc = (const T*)P.p[cur];
+    T* __restrict__ pn = (T*)P.p[cur ^ 1];
+    const T p0 = pc[c];
+    const int idx[3] = {x, y, z};
+    const long long pstride[3] = {sx, N[2], 1};
+    const long long fl[3] = {c, ((long long)x * (N[1] + 1) + y) * N[2] + z, ((long long)x * N[1] + y) * (N[2] + 1) + z};
+    const long long fstride[3] = {sx, N[2], 1};
+    const bool pmlc[3] = {P.pml_cell[0][x] != 0, P.pml_cell[1][y] != 0, P.pml_cell[2][z] != 0};
+    const T inv_h = (T)P.inv_h;
+    T acc = 0;
+    T pdn[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
+        const bool other = pmlc[d1] || pmlc[d2];
+        const int i = idx[d];
+        const T* __restrict__ vo = (const T*)P.v[cur][d];
+        T* __restrict__ vn = (T*)P.v[cur ^ 1][d];
+        const T* __restrict__ vupd = Coef<T>::vupd(P, d);
+        const T* __restrict__ vgrad = Coef<T>::vgrad(P, d);
+        // left face (owned)
+        T vl = vo[fl[d]];
+        if (i > 0 && (P.pml_face[d][i] != 0 || other)) {
+            vl = vel_update<T>(vl, vupd[i], vgrad[i], p0, pc[c - pstride[d]]);
+            vn[fl[d]] = vl;
+        }
+        // right face (owned only when the right cell is not in the PML)
+        const long long fr = fl[d] + fstride[d];
+        T vr = vo[fr];
+        if (i + 1 < N[d] && (P.pml_face[d][i + 1] != 0 || other)) {
+            vr = vel_update<T>(vr, vupd[i + 1], vgrad[i + 1], pc[c + pstride[d]], p0);
+            const bool right_pml = P.pml_cell[d][i + 1] != 0 || other;
+            if (!right_pml) vn[fr] = vr;
+        }
+        T* __restrict__ pd = (T*)P.pd[d];
+        const T a = pd_update<T>(pd[c], Coef<T>::pupd(P, d)[i], Coef<T>::pdiv(P, d)[i], vr, vl, inv_h);
+        pd[c] = a;
+        pdn[d] = a;
+    }
+    acc = pdn[0] + pdn[1] + pdn[2];
+    pn[c] = acc;
+}
+
+}  // namespace fdtd
+
+namespace fdtd {
+
+// Host side: one step of the region-split path on `s`.
+template <typename T>
+cudaError_t launch_regions(const SolveParams* dP, const RegionLaunch& R, int cur, cudaStream_t s, int* launches) {
+    int l = 0;
+    const long long n = R.shell.first[R.shell.n];
+    if (n > 0) {
+        k_pml_shell<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(dP, cur, R.shell);
+        ++l;
+    }
+    const Box3& b = R.interior;
+    const int nx = b.hi[0] - b.lo[0], ny = b.hi[1] - b.lo[1], nz = b.hi[2] - b.lo[2];
+    if (nx > 0 && ny > 0 && nz > 0) {
+        dim3 block(32, 8);
+        const int xb = (R.xb == 2 || R.xb == 8) ? R.xb : 4;
+        dim3 grid((nz + 31) / 32, (ny + 7) / 8, (nx + xb - 1) / xb);
+        if (xb == 2) k_interior<T, 2><<<grid, block, 0, s>>>(dP, cur, b);
+        else if (xb == 8) k_interior<T, 8><<<grid, block, 0, s>>>(dP, cur, b);
+        else k_interior<T, 4><<<grid, block, 0, s>>>(dP, cur, b);
+        ++l;
+    }
+    if (R.ghost_cap > 0) {
+        const int blocks = (R.ghost_cap + 127) / 128 < 1184 ? (R.ghost_cap + 127) / 128 : 1184;
+        k_ghost_cells<T><<<blocks, 128, 0, s>>>(dP, cur);
+        ++l;
+    }
+    if (R.sources) {
+        const Box3& r = R.src_region;
+        const long long total = (long long)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);
+        if (total > 0) {
+            const long long g = (total + 255) / 256;
+            k_sources<T><<<(unsigned)(g < 148 * 16 ? g : 148 * 16), 256, 0, s>>>(dP, cur, r);
+            ++l;
+        }
+    }
+    if (launches) *launches += l;
+    return cudaGetLastError();
+}
+
+}  // namespace fdtd

@@ -66,8 +66,8 @@ __device__ __forceinline__ T pd_update(T pd, T upd, T div, T vR, T vL, T inv_h) 
 
 // Sum of the Gaussian pressure sources at a cell centre (GaussianPressureSource.cpp:6-30,
 // FDTD_Objects.cpp:356-367); the time factor comes precomputed from the prologue.
-__device__ __forceinline__ double source_sum(const SolveParams& P, const StepConsts& sc, double x, double y,
-                                             double z) {
+static __device__ __noinline__ double source_sum(const SolveParams& P, const StepConsts& sc, double x, double y,
+                                          double z) {
     double sum = 0;
     for (int s = 0; s < P.n_src; ++s) {
         const DevSource& S = P.src[s];

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -45,8 +46,28 @@ void classification_launches(fdtd_solver* s, fdtd_status& st) {
     }
 }
 
+// True when a Gaussian source may contribute at a step starting at time t:
+// exp(-u^2/2) underflows to zero for |u| > 38.6 (GaussianPressureSource.cpp:21-24).
+bool sources_active(const fdtd_solver* s, double t) {
+    const double ts = t + 0.5 * s->k;
+    for (const auto& g : s->sources)
+        if (std::fabs((ts - g.offset_time) / g.width_time) < 40.0) return true;
+    return false;
+}
+
+// Sources active at any step of [t, t + n k)
+bool sources_active_window(const fdtd_solver* s, double t, int n) {
+    for (const auto& g : s->sources) {
+        const double a = (t + 0.5 * s->k - g.offset_time) / g.width_time;
+        const double b = (t + (n - 0.5) * s->k - g.offset_time) / g.width_time;
+        if (b > -40.0 && a < 40.0) return true;
+    }
+    return false;
+}
+
 // Enqueue one time step with the pressure parity `cur`; listener row to dev_row.
-fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify) {
+fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify, bool src) {
+    s->region.sources = src ? 1 : 0;
     fdtd_status st = FDTD_OK;
     if (classify) {
         // MAC_Grid::classifyCells_FAST + InterpolateFreshPressureCell (PML_WaveSolver.cpp:807-812)
@@ -60,19 +81,27 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
     if (s->precision == FDTD_PRECISION_FP64) {
         CUDA_TRY(s, launch_prologue_fp64(s->dP, s->n_solid_pml, s->stream));
         s->launches++;
+        int l = 0;
         if (s->opt.kernel == FDTD_KERNEL_PHASED) {
-            int l = 0;
             CUDA_TRY(s, launch_phased_fp64(s->dP, s->N, cur, s->d_lap, s->stream, &l));
-            s->launches += l;
-        } else {
+        } else if (s->opt.kernel == FDTD_KERNEL_STREAMING) {
             CUDA_TRY(s, launch_step_fused_fp64(s->dP, s->N, cur, s->tile_y, s->xchunk, s->stream));
-            s->launches++;
+            l = 1;
+        } else {
+            CUDA_TRY(s, launch_step_regions_fp64(s->dP, s->region, cur, s->stream, &l));
         }
+        s->launches += l;
     } else {
         CUDA_TRY(s, launch_prologue_fp32(s->dP, s->n_solid_pml, s->stream));
         s->launches++;
-        CUDA_TRY(s, launch_step_fused_fp32(s->dP, s->N, cur, s->tile_y, s->xchunk, s->stream));
-        s->launches++;
+        int l = 0;
+        if (s->opt.kernel == FDTD_KERNEL_STREAMING) {
+            CUDA_TRY(s, launch_step_fused_fp32(s->dP, s->N, cur, s->tile_y, s->xchunk, s->stream));
+            l = 1;
+        } else {
+            CUDA_TRY(s, launch_step_regions_fp32(s->dP, s->region, cur, s->stream, &l));
+        }
+        s->launches += l;
     }
     if (s->L > 0 && dev_row) {
         // the phased path keeps p^{n+1} in the same slot as the fused one
@@ -109,6 +138,13 @@ fdtd_status check_device_errors(fdtd_solver* s) {
     CUDA_TRY(s, cudaMemcpyAsync(&sc, s->hP.consts, sizeof(sc), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaMemcpyAsync(status, s->d_status, sizeof(status), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    int ghosts = 0;
+    CUDA_TRY(s, cudaMemcpy(&ghosts, s->d_ghost_count, sizeof(int), cudaMemcpyDeviceToHost));
+    if (ghosts > s->region.ghost_cap) {
+        set_error(s, "ghost-neighbour list overflow (" + std::to_string(ghosts) + " > " +
+                         std::to_string(s->region.ghost_cap) + ")");
+        return FDTD_ERR_OOM;
+    }
     if (status[0] == 2) {
         set_error(s, "fresh cell inside an object (MAC_Grid.cpp:2050-2053)");
         return FDTD_ERR_GEOMETRY;
@@ -121,13 +157,13 @@ fdtd_status check_device_errors(fdtd_solver* s) {
 }
 
 // Capture `n` steps starting at parity `cur` into a graph (static scenes only).
-fdtd_status capture_graph(fdtd_solver* s, int cur, int n, cudaGraphExec_t* out) {
+fdtd_status capture_graph(fdtd_solver* s, int cur, int n, bool src, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
     CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     fdtd_status st = FDTD_OK;
     int c = cur;
     for (int i = 0; i < n && st == FDTD_OK; ++i) {
-        st = enqueue_step(s, c, s->d_lis + (size_t)i * s->L, false);
+        st = enqueue_step(s, c, s->d_lis + (size_t)i * s->L, false, src);
         c ^= 1;
     }
     cudaError_t e = cudaStreamEndCapture(s->stream, &g);
@@ -162,14 +198,16 @@ fdtd_status run_steps(fdtd_solver* s, int n, Sink sink) {
         const int remaining = n - done;
         const bool classify_now = s->moving || s->step_index == 0;
         if (!classify_now && G > 0 && remaining >= G) {
-            if (!s->graph_exec[s->cur]) {
+            const bool src = sources_active_window(s, s->time, G);
+            const int key = s->cur + (src ? 2 : 0);
+            if (!s->graph_exec[key]) {
                 const long long l0 = s->launches;
-                fdtd_status st = capture_graph(s, s->cur, G, &s->graph_exec[s->cur]);
+                fdtd_status st = capture_graph(s, s->cur, G, src, &s->graph_exec[key]);
                 if (st != FDTD_OK) return st;
                 s->graph_launches_per_exec = s->launches - l0;
                 s->launches = l0;
             }
-            CUDA_TRY(s, cudaGraphLaunch(s->graph_exec[s->cur], s->stream));
+            CUDA_TRY(s, cudaGraphLaunch(s->graph_exec[key], s->stream));
             s->launches += s->graph_launches_per_exec;
             for (int q = 0; q < G; ++q) {
                 fdtd_status st = after_step(s);
@@ -184,7 +222,7 @@ fdtd_status run_steps(fdtd_solver* s, int n, Sink sink) {
         if (G > 0 && !s->moving && classify_now) m = 1;
         for (int i = 0; i < m; ++i) {
             const bool classify = s->moving || s->step_index == 0;
-            fdtd_status st = enqueue_step(s, s->cur, s->d_lis + (size_t)i * s->L, classify);
+            fdtd_status st = enqueue_step(s, s->cur, s->d_lis + (size_t)i * s->L, classify, sources_active(s, s->time));
             if (st != FDTD_OK) return st;
             st = after_step(s);
             if (st != FDTD_OK) return st;
@@ -240,6 +278,41 @@ fdtd_status fdtd_solver_fetch_listeners(fdtd_solver* s, double* out) {
     CUDA_TRY(s, launch_listeners(s->dP, s->precision, s->cur, s->L, s->d_lis, s->stream));
     CUDA_TRY(s, cudaMemcpyAsync(out, s->d_lis, (size_t)s->L * 8, cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_solver_time_stencil(fdtd_solver* s, int32_t n_launches, float* elapsed_ms) {
+    if (!s || n_launches <= 0 || !elapsed_ms) return (set_error(s, "invalid arguments"), FDTD_ERR_INVALID_ARG);
+    CUDA_TRY(s, cudaSetDevice(s->opt.device));
+    cudaEvent_t e0, e1;
+    CUDA_TRY(s, cudaEventCreate(&e0));
+    CUDA_TRY(s, cudaEventCreate(&e1));
+    CUDA_TRY(s, cudaEventRecord(e0, s->stream));
+    int c = s->cur;
+    for (int i = 0; i < n_launches; ++i) {
+        cudaError_t e;
+        if (s->precision == FDTD_PRECISION_FP64) {
+            if (s->opt.kernel == FDTD_KERNEL_PHASED) e = launch_phased_fp64(s->dP, s->N, c, s->d_lap, s->stream, nullptr);
+            else if (s->opt.kernel == FDTD_KERNEL_STREAMING)
+                e = launch_step_fused_fp64(s->dP, s->N, c, s->tile_y, s->xchunk, s->stream);
+            else e = launch_step_regions_fp64(s->dP, s->region, c, s->stream, nullptr);
+        } else {
+            if (s->opt.kernel == FDTD_KERNEL_STREAMING)
+                e = launch_step_fused_fp32(s->dP, s->N, c, s->tile_y, s->xchunk, s->stream);
+            else e = launch_step_regions_fp32(s->dP, s->region, c, s->stream, nullptr);
+        }
+        if (e != cudaSuccess) {
+            set_error(s, std::string("stencil launch: ") + cudaGetErrorString(e));
+            return FDTD_ERR_CUDA;
+        }
+        c ^= 1;
+    }
+    CUDA_TRY(s, cudaEventRecord(e1, s->stream));
+    CUDA_TRY(s, cudaEventSynchronize(e1));
+    CUDA_TRY(s, cudaEventElapsedTime(elapsed_ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    s->cur = c;
     return FDTD_OK;
 }
 

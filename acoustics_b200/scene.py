@@ -22,7 +22,7 @@ SHAPE_SPHERE, SHAPE_BOX, SHAPE_ELLIPSOID = 0, 1, 2
 ACCEL_NONE, ACCEL_GAUSSIAN_TRANSLATION, ACCEL_GAUSSIAN_PULSATION = 0, 1, 2
 MOTION_STATIC, MOTION_BALLISTIC = 0, 1
 PRECISION_FP64, PRECISION_FP32_COMPENSATED = 0, 1
-KERNEL_FUSED, KERNEL_PHASED = 0, 1
+KERNEL_FUSED, KERNEL_PHASED, KERNEL_STREAMING = 0, 1, 2
 
 CELL_BULK, CELL_GHOST, CELL_VALID_HISTORY, CELL_PML, CELL_CONSTRAINT = 1, 2, 4, 8, 16
 (FIELD_PRESSURE, FIELD_PRESSURE_PREV, FIELD_PML_PX, FIELD_PML_PY, FIELD_PML_PZ,
@@ -250,13 +250,15 @@ def _sample_listeners(rng, sc: Scene, n: int, keep_out) -> np.ndarray:
     return np.asarray(pts, dtype=np.float64)
 
 
-def config1(seed_src: int = 1, seed_lis: int = 2) -> Scene:
+def config1(seed_src: int = 1, seed_lis: int = 2, divisions=(64, 64, 64), pml_width: float = 10,
+            radius: float = 0.04, steps: int = 500) -> Scene:
     """64^3, h=5 mm, 10-cell PML, sphere r=4 cm at the centre, Gaussian pulse
-    sigma_t=2e-4 s at a seeded offset outside the sphere, 8 listeners, 500 steps."""
+    sigma_t=2e-4 s at a seeded offset outside the sphere, 8 listeners, 500 steps.
+    Other grid sizes re-draw the source and listeners inside the new fluid region."""
     h = 0.005
-    sc = Scene(cell_size=h, divisions=(64, 64, 64), time_step=reference_time_step(h), pml_width=10,
-               steps=500, name="cfg1_64cube_sphere_fp64")
-    r = 0.04
+    sc = Scene(cell_size=h, divisions=tuple(divisions), time_step=reference_time_step(h), pml_width=pml_width,
+               steps=steps, name="cfg1_64cube_sphere_fp64" if tuple(divisions) == (64, 64, 64) else "cfg1_variant")
+    r = radius
     sc.objects.append(RigidObject(SHAPE_SPHERE, (0.0, 0.0, 0.0), (r, 0, 0)))
     rng = np.random.default_rng(seed_src)
     lo, hi = _non_pml_box(sc, 2.0)

@@ -93,6 +93,13 @@ class PML_WaveSolver:
     def last_launch_count(self) -> int:
         return int(self._L.fdtd_solver_last_launch_count(self._h))
 
+    def time_stencil(self, n_launches: int) -> float:
+        """Milliseconds for n back-to-back launches of the step kernel (CUDA events
+        on the solver stream).  Advances the state without prologue/listeners."""
+        ms = C.c_float(0.0)
+        check(self._L.fdtd_solver_time_stencil(self._h, int(n_launches), C.byref(ms)), self._h)
+        return float(ms.value)
+
     # ---- introspection ----
     def info(self) -> SolverInfo:
         info = SolverInfo()

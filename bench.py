@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark of the FDTD step (Gcell-steps/s and fraction of the HBM roofline).
+
+Workload: the single large solve, 256^3 cells, h = 2.5 mm, 16-cell PML, three
+static rigid bodies (sphere, box, ellipsoid) with a Gaussian-in-time boundary
+acceleration of 1e3 m/s^2, 64 listeners; seeded synthetic scene.  One bench
+"step" is one FDTD time step of that solve (every cell updated once, listeners
+sampled).  Headline precision: FP32 with compensated accumulation; the FP64
+fused path, the plain FP64 path (one kernel per reference phase) and the FP32
+listener error against FP64 are reported beside it.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Under torchrun each rank runs its own independent solve on its own GPU (the
+path shards across solves, not within one): value = sum over ranks of cells x
+steps / max-over-ranks time, scaling "weak".
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Gcell-steps/s & %HBM roofline; served solves/s, p99, at ≤1e-4 rel-L2 vs FP64"
+UNIT = "Gcell-steps/s"
+L2_BYTES = 126 * 2**20
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.idx), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.3)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        with open(self.path) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        pg = dist
+    return world, rank, local, pg
+
+
+def max_over_ranks(x: float, pg) -> float:
+    if pg is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg):
+    if pg is not None:
+        pg.barrier()
+
+
+def bench_scene(steps_for_accuracy=None):
+    from acoustics_b200.scene import config2
+    return config2()
+
+
+def cpu_baseline(scene, budget_s: float, max_steps: int):
+    """The FP64 CPU oracle (restatement of the reference step) on the host cores."""
+    from oracle import loader
+    threads = loader.set_threads(os.cpu_count() or 1)
+    o = loader.OracleSolver(scene)
+    o.step(1)  # warm-up, untimed
+    t0 = time.perf_counter()
+    n = 0
+    while n < max_steps:
+        o.step(1)
+        n += 1
+        if time.perf_counter() - t0 > budget_s:
+            break
+    dt = time.perf_counter() - t0
+    o.close()
+    return scene.n_cells * n / dt / 1e9, n, threads, dt
+
+
+def run_reference(args, world, rank, pg):
+    if rank != 0:
+        return 0
+    sc = bench_scene()
+    budget = float(os.environ.get("FDTD_REF_BUDGET_S", "120"))
+    val, n, threads, dt = cpu_baseline(sc, budget, max(1, args.steps))
+    sample = (f"{n} full FDTD steps of the 256^3 solve ({sc.n_cells} cells) after 1 warm-up step, "
+              f"{dt:.1f} s, FP64 CPU oracle (restatement of the reference step; the reference itself "
+              f"cannot be built here)")
+    line = {
+        "metric": METRIC, "value": val, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+        "steps": n, "warmup": 1, "ms_per_step": dt / n * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": sc.name, "cells": sc.n_cells, "divisions": list(sc.divisions),
+                   "pml_width": sc.pml_width, "listeners": sc.n_listeners, "objects": len(sc.objects)},
+        "cpu_baseline": {"value": val, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": val, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def read_traffic(name: str):
+    """DRAM bytes per launch from the committed ncu summary, if one exists."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(p):
+        return None
+    with open(p) as f:
+        d = json.load(f)
+    v = d.get(name)
+    return v.get("dram_bytes_per_launch") if isinstance(v, dict) else None
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=20)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp64-plain"])
+    ap.add_argument("--graph-steps", type=int, default=50)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-variants", action="store_true")
+    ap.add_argument("--accuracy-steps", type=int, default=4000)
+    ap.add_argument("--cpu-budget", type=float, default=15.0)
+    args = ap.parse_args()
+    args.warmup = max(3, args.warmup)
+    world, rank, local, pg = dist_setup()
+    if args.impl == "reference":
+        return run_reference(args, world, rank, pg)
+
+    import torch
+
+    from acoustics_b200 import scene as S
+    from acoustics_b200.solver import PML_WaveSolver
+
+    torch.cuda.set_device(local)
+    sc = bench_scene()
+    prec = {"fp32": S.PRECISION_FP32_COMPENSATED, "fp64": S.PRECISION_FP64, "fp64-plain": S.PRECISION_FP64}[args.precision]
+    kern = S.KERNEL_PHASED if args.precision == "fp64-plain" else S.KERNEL_FUSED
+    G = args.graph_steps if args.graph_steps % 2 == 0 else args.graph_steps + 1
+    K, W = args.steps, args.warmup
+    L = sc.n_listeners
+    dev_out = torch.empty(max(1, (K + W) * L), dtype=torch.float64, device="cuda")
+    solver = PML_WaveSolver(sc, precision=prec, kernel=kern, graph_steps=G, device=local)
+    info = solver.info()
+    ext = torch.cuda.ExternalStream(solver.stream)
+    solver.step_device(W, dev_out.data_ptr())
+    solver.synchronize()
+    barrier(pg)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clk:
+        torch.cuda.synchronize()
+        e0.record(ext)
+        solver.step_device(K, dev_out.data_ptr() + W * L * 8)
+        e1.record(ext)
+        e1.synchronize()
+        torch.cuda.synchronize()
+        launches = solver.last_launch_count()
+        # kernel-only timing of the dominant step kernel (same stream)
+        kernel_ms = solver.time_stencil(K) / K
+    ms = e0.elapsed_time(e1)
+    barrier(pg)
+    ms_max = max_over_ranks(ms, pg)
+    ms_step = ms_max / K
+    value = world * sc.n_cells * K / (ms_max / 1e3) / 1e9
+    alg_bytes = float(info.algorithmic_bytes_per_step)
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
+    kname = {"fp32": "k_step_fused<float,8>", "fp64": "k_step_fused<double,8>", "fp64-plain": "phased fp64"}[args.precision]
+    traffic = read_traffic(kname)
+    clocks = clk.summary()
+    y_ours = dev_out[W * L:(W + K) * L].cpu().numpy().reshape(K, L)
+    solver.close()
+
+    # end to end through the public API: create (scene upload + classification),
+    # K steps with listener rows read back to host memory every chunk, destroy
+    torch.cuda.synchronize()
+    barrier(pg)
+    t0 = time.perf_counter()
+    s2 = PML_WaveSolver(sc, precision=prec, kernel=kern, graph_steps=G, device=local)
+    y_e2e = s2.step(K)
+    s2.close()
+    e2e_s = time.perf_counter() - t0
+    e2e_s = max_over_ranks(e2e_s, pg)
+    e2e_val = world * sc.n_cells * K / e2e_s / 1e9
+    scene_bytes = 4096 + 8 * 3 * L
+
+    variants = {}
+    if not args.no_variants:
+        for name, p2, k2 in (("fp64_fused", S.PRECISION_FP64, S.KERNEL_FUSED),
+                             ("fp64_plain", S.PRECISION_FP64, S.KERNEL_PHASED),
+                             ("fp32_compensated", S.PRECISION_FP32_COMPENSATED, S.KERNEL_FUSED)):
+            sv = PML_WaveSolver(sc, precision=p2, kernel=k2, graph_steps=G if k2 == S.KERNEL_FUSED else 0, device=local)
+            n = min(K, 200)
+            sv.step_device(5, dev_out.data_ptr())
+            sv.synchronize()
+            ext2 = torch.cuda.ExternalStream(sv.stream)
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(ext2)
+            sv.step_device(n, dev_out.data_ptr())
+            b.record(ext2)
+            b.synchronize()
+            t = a.elapsed_time(b) / n
+            kms = sv.time_stencil(n) / n
+            ab = float(sv.info().algorithmic_bytes_per_step)
+            variants[name] = {"gcell_steps_s": sc.n_cells / (t / 1e3) / 1e9, "ms_per_step": t,
+                              "kernel_ms": kms, "kernel_hbm_frac": ab / (kms / 1e3) / 1e9 / peak,
+                              "alg_bytes_per_step": ab}
+            sv.close()
+        if args.accuracy_steps > 0:
+            ref = PML_WaveSolver(sc, precision=S.PRECISION_FP64, device=local)
+            y64 = ref.step(args.accuracy_steps)
+            ref.close()
+            f32 = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED, graph_steps=G, device=local)
+            y32 = f32.step(args.accuracy_steps)
+            f32.close()
+            variants["fp32_listener_rel_l2_vs_fp64"] = float(np.linalg.norm(y32 - y64) / np.linalg.norm(y64))
+            variants["accuracy_steps"] = args.accuracy_steps
+        if "fp64_plain" in variants and "fp32_compensated" in variants:
+            variants["fp32_over_fp64_plain"] = variants["fp32_compensated"]["gcell_steps_s"] / variants["fp64_plain"]["gcell_steps_s"]
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        val, n, threads, dt = cpu_baseline(sc, args.cpu_budget, 1000)
+        cpu = {"value": val, "unit": UNIT, "cores": threads, "kind": "port",
+               "sample": f"{n} full FDTD steps of this 256^3 solve in {dt:.1f} s (FP64 CPU oracle, OpenMP)"}
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+            "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp32": "f32", "fp64": "f64", "fp64-plain": "f64"}[args.precision], "data": "synthetic",
+            "config": {"workload": sc.name, "cells": sc.n_cells, "divisions": list(sc.divisions),
+                       "pml_width": sc.pml_width, "objects": len(sc.objects), "listeners": L,
+                       "precision": args.precision, "graph_steps": G,
+                       "l2": f"inputs larger than L2: {alg_bytes / 2**20:.0f} MiB algorithmic traffic per step "
+                             f"vs {L2_BYTES / 2**20:.0f} MiB L2",
+                       "parallelism": f"replicas x{world} (independent solves)"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
+                         "kernel": kname, "kernel_ms": kernel_ms, "alg_bytes_per_launch": alg_bytes},
+            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": scene_bytes / K,
+                    "d2h_bytes_per_step": 8 * L,
+                    "note": "create (scene upload, classification) + K steps with listener rows to host + destroy"},
+            "gpu_launches": int(launches),
+            "clocks": clocks,
+            "variants": variants,
+        }
+        if cpu:
+            line["cpu_baseline"] = cpu
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

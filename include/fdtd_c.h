@@ -119,8 +119,9 @@ enum {
 };
 
 enum {
-    FDTD_KERNEL_FUSED = 0,    /* one fused stencil kernel per step                       */
-    FDTD_KERNEL_PHASED = 1    /* plain path: one kernel per reference phase (FP64 only)   */
+    FDTD_KERNEL_FUSED = 0,    /* region-split fused step: interior kernel + PML-shell kernel */
+    FDTD_KERNEL_PHASED = 1,   /* plain path: one kernel per reference phase (FP64 only)      */
+    FDTD_KERNEL_STREAMING = 2 /* single kernel, one thread per column marching along x       */
 };
 
 typedef struct {
@@ -223,6 +224,13 @@ void* fdtd_solver_stream(fdtd_solver* s);
 const char* fdtd_solver_last_error(fdtd_solver* s);
 /* Kernel launches issued by the most recent fdtd_solver_step* call. */
 int64_t fdtd_solver_last_launch_count(fdtd_solver* s);
+
+/* Profiling hook (no counterpart in the reference): launch the dominant step kernel
+ * n_launches times back to back on the solver's stream (alternating buffer parity,
+ * no prologue or listener work) between two CUDA events and return the elapsed
+ * milliseconds.  The solver state is left advanced by those launches; use a solver
+ * created for measurement. */
+fdtd_status fdtd_solver_time_stencil(fdtd_solver* s, int32_t n_launches, float* elapsed_ms);
 
 /* Snapshot / restore of the resident state (_SaveSimulationSnapshot,
  * FDTD_AcousticSimulator.cpp:381-415).  bytes: query with buffer NULL. */

@@ -1,0 +1,115 @@
+"""GPU paths against the FP64 oracle through the C-ABI: FP32 compensated,
+plain (phased) FP64, CUDA graphs, snapshot/restore, accelerating bodies,
+plane constraints and moving bodies."""
+import numpy as np
+import pytest
+
+from acoustics_b200 import scene as S
+from acoustics_b200.solver import PML_WaveSolver
+from tests._util import rel_l2, small_config2
+
+pytestmark = pytest.mark.gpu
+
+TOL_FP64 = 1e-12
+TOL_FP32 = 1e-4
+
+
+def test_fp32_compensated_config1(oracle_lib, fdtd_lib):
+    sc = S.config1()
+    yo = oracle_lib.OracleSolver(sc).step(500)
+    g = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED)
+    yg = g.step(500)
+    err = rel_l2(yg, yo)
+    print("cfg1 fp32 listener rel L2", err)
+    assert err <= TOL_FP32
+
+
+def test_phased_fp64_matches_oracle(oracle_lib, fdtd_lib):
+    sc = S.config1()
+    yo = oracle_lib.OracleSolver(sc).step(200)
+    g = PML_WaveSolver(sc, kernel=S.KERNEL_PHASED)
+    yg = g.step(200)
+    assert rel_l2(yg, yo) <= TOL_FP64
+
+
+@pytest.mark.parametrize("precision", [S.PRECISION_FP64, S.PRECISION_FP32_COMPENSATED])
+def test_graph_replay_identical_to_eager(fdtd_lib, precision):
+    sc = S.config1(divisions=(48, 40, 56), pml_width=8, radius=0.025)
+    a = PML_WaveSolver(sc, precision=precision).step(75)
+    b = PML_WaveSolver(sc, precision=precision, graph_steps=10).step(75)
+    assert np.array_equal(a, b)
+
+
+def test_snapshot_restore_roundtrip(fdtd_lib):
+    sc = S.config1()
+    g = PML_WaveSolver(sc)
+    g.step(40)
+    blob = g.snapshot()
+    y1 = g.step(30)
+    g.restore(blob)
+    y2 = g.step(30)
+    assert np.array_equal(y1, y2)
+
+
+def test_accelerating_bodies_fp64(oracle_lib, fdtd_lib):
+    sc = small_config2()
+    o = oracle_lib.OracleSolver(sc)
+    g = PML_WaveSolver(sc)
+    yo, yg = o.step(sc.steps), g.step(sc.steps)
+    assert np.abs(yo).max() > 0
+    assert rel_l2(yg, yo) <= TOL_FP64
+    fo, go = o.classification()
+    fg, gg = g.GetGrid()
+    assert np.array_equal(fo, fg)
+    assert np.array_equal(go, gg)
+
+
+def test_accelerating_bodies_fp32(oracle_lib, fdtd_lib):
+    sc = small_config2()
+    yo = oracle_lib.OracleSolver(sc).step(sc.steps)
+    yg = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED).step(sc.steps)
+    assert rel_l2(yg, yo) <= TOL_FP32
+
+
+def test_plane_constraint_and_pml_overlap(oracle_lib, fdtd_lib):
+    sc = S.config1(divisions=(40, 40, 40), pml_width=6, radius=0.02)
+    sc.constraints.append(S.PlaneConstraint(1, 1, -0.05))       # floor at y = -5 cm
+    sc.objects.append(S.RigidObject(S.SHAPE_BOX, (0.07, 0.0, 0.0), (0.04, 0.02, 0.02)))  # reaches into the PML
+    o = oracle_lib.OracleSolver(sc)
+    g = PML_WaveSolver(sc)
+    yo, yg = o.step(120), g.step(120)
+    fo, go = o.classification()
+    fg, gg = g.GetGrid()
+    assert np.array_equal(fo, fg)
+    assert np.array_equal(go, gg)
+    assert rel_l2(yg, yo) <= TOL_FP64
+    assert rel_l2(g.field(S.FIELD_PRESSURE), o.field(S.FIELD_PRESSURE)) <= TOL_FP64
+
+
+def moving_scene(steps=160):
+    sc = S.Scene(cell_size=0.004, divisions=(48, 40, 40), time_step=S.reference_time_step(0.004), pml_width=6,
+                 steps=steps, name="moving_small")
+    k = sc.time_step
+    # two spheres approaching at ~30 m/s (0.013 cells per step)
+    sc.objects.append(S.RigidObject(S.SHAPE_SPHERE, (-0.03, 0.0, 0.0), (0.012, 0, 0), motion=S.MOTION_BALLISTIC,
+                                    velocity=(60.0, 0, 0), gravity=(0, 0, -9.81)))
+    sc.objects.append(S.RigidObject(S.SHAPE_BOX, (0.035, 0.005, 0.0), (0.01, 0.008, 0.008), motion=S.MOTION_BALLISTIC,
+                                    velocity=(-60.0, 0, 0), accel_kind=S.ACCEL_GAUSSIAN_TRANSLATION,
+                                    accel_amplitude=1e3, accel_t0=40 * k, accel_tau=10 * k, accel_dir=(1, 0, 0)))
+    sc.sources.append(S.GaussianSource((0.0, 0.04, 0.0), 5e-5))
+    sc.listeners = np.array([[0.0, -0.03, 0.01], [0.02, 0.02, -0.02], [-0.04, 0.0, 0.03]])
+    return sc
+
+
+@pytest.mark.parametrize("precision,tol", [(S.PRECISION_FP64, TOL_FP64), (S.PRECISION_FP32_COMPENSATED, TOL_FP32)])
+def test_moving_bodies(oracle_lib, fdtd_lib, precision, tol):
+    sc = moving_scene()
+    o = oracle_lib.OracleSolver(sc)
+    g = PML_WaveSolver(sc, precision=precision)
+    for chunk in range(4):
+        yo, yg = o.step(40), g.step(40)
+        assert rel_l2(yg, yo) <= tol, chunk
+        fo, go = o.classification()
+        fg, gg = g.GetGrid()
+        assert np.array_equal(fo, fg), chunk
+        assert np.array_equal(go, gg), chunk
