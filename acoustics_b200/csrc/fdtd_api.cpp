@@ -216,6 +216,39 @@ fdtd_status run_classification(fdtd_solver* s) {
 // ---------------------------------------------------------------------------
 namespace fdtd {
 
+// PML shell boxes for a given number of x planes per thread (xs).
+void build_shell_boxes(fdtd_solver* s, int xs) {
+    ShellBoxes& B = s->shell;
+    std::memset(&B, 0, sizeof(B));
+    B.xs = xs;
+    const int* N = s->N;
+    const int* lo = s->interior.lo;
+    const int* hi = s->interior.hi;
+    auto add = [&](int x0, int x1, int y0, int y1, int za0, int za1, int zb0, int zb1) {
+        const int nz = (za1 - za0) + (zb1 - zb0);
+        if (x1 <= x0 || y1 <= y0 || nz <= 0) return;
+        const int b = B.n;
+        B.x0[b] = x0; B.nx[b] = x1 - x0;
+        B.y0[b] = y0; B.ny[b] = y1 - y0;
+        B.z0a[b] = za0; B.nza[b] = za1 - za0; B.z0b[b] = zb0; B.nz[b] = nz;
+        B.tz[b] = (nz + 31) / 32;
+        B.ty[b] = (B.ny[b] + 7) / 8;
+        B.tx[b] = (B.nx[b] + xs - 1) / xs;
+        B.block_first[b + 1] = B.block_first[b] + B.tz[b] * B.ty[b] * B.tx[b];
+        B.cells += (long long)B.nx[b] * B.ny[b] * nz;
+        ++B.n;
+    };
+    if (hi[0] <= lo[0] || hi[1] <= lo[1] || hi[2] <= lo[2]) {
+        add(0, N[0], 0, N[1], 0, N[2], N[2], N[2]);  // every cell is a PML cell
+        return;
+    }
+    add(0, lo[0], 0, N[1], 0, N[2], N[2], N[2]);
+    add(hi[0], N[0], 0, N[1], 0, N[2], N[2], N[2]);
+    add(lo[0], hi[0], 0, lo[1], 0, N[2], N[2], N[2]);
+    add(lo[0], hi[0], hi[1], N[1], 0, N[2], N[2], N[2]);
+    add(lo[0], hi[0], lo[1], hi[1], 0, lo[2], hi[2], N[2]);
+}
+
 fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
     s->h = sc->cell_size;
     s->c = sc->sound_speed;
@@ -291,27 +324,11 @@ fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
         s->interior.lo[d] = lo[d];
         s->interior.hi[d] = hi[d];
     }
-    ShellBoxes& B = s->shell;
-    std::memset(&B, 0, sizeof(B));
-    auto add = [&](int x0, int x1, int y0, int y1, int z0, int z1) {
-        if (x1 <= x0 || y1 <= y0 || z1 <= z0) return;
-        B.start[B.n][0] = x0; B.start[B.n][1] = y0; B.start[B.n][2] = z0;
-        B.size[B.n][0] = x1 - x0; B.size[B.n][1] = y1 - y0; B.size[B.n][2] = z1 - z0;
-        B.first[B.n + 1] = B.first[B.n] + (long long)(x1 - x0) * (y1 - y0) * (z1 - z0);
-        ++B.n;
-    };
     const int* N = s->N;
-    if (lo[0] >= hi[0] || lo[1] >= hi[1] || lo[2] >= hi[2]) {
-        add(0, N[0], 0, N[1], 0, N[2]);  // every cell is a PML cell
+    if (lo[0] >= hi[0] || lo[1] >= hi[1] || lo[2] >= hi[2])
         for (int d = 0; d < 3; ++d) s->interior.lo[d] = s->interior.hi[d] = 0;
-    } else {
-        add(0, lo[0], 0, N[1], 0, N[2]);
-        add(hi[0], N[0], 0, N[1], 0, N[2]);
-        add(lo[0], hi[0], 0, lo[1], 0, N[2]);
-        add(lo[0], hi[0], hi[1], N[1], 0, N[2]);
-        add(lo[0], hi[0], lo[1], hi[1], 0, lo[2]);
-        add(lo[0], hi[0], lo[1], hi[1], hi[2], N[2]);
-    }
+    build_shell_boxes(s, 1);
+    (void)N;
     return FDTD_OK;
 }
 
@@ -448,7 +465,7 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         const long long nf = (long long)(N[0] + (d == 0)) * (N[1] + (d == 1)) * (N[2] + (d == 2));
         s->vcount[d] = nf;
         cv.add(&P.v[0][d], nf * w);
-        if (o.kernel == FDTD_KERNEL_FUSED) cv.add(&P.v[1][d], nf * w);
+        if (o.kernel != FDTD_KERNEL_PHASED) cv.add(&P.v[1][d], nf * w);  // double-buffered faces
     }
     if (o.kernel == FDTD_KERNEL_PHASED) cv.add((void**)&s->d_lap, n * 8);
     cv.add((void**)&P.clock, 8);
@@ -597,6 +614,9 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     s->tile_y = o.tile_y > 0 ? o.tile_y : 8;
     s->xb = (o.x_chunk == 2 || o.x_chunk == 4 || o.x_chunk == 8) ? o.x_chunk : 4;
     s->region.xb = s->xb;
+    // tile_y selects the PML-shell planes per thread (1 or 2) of the fused path
+    if (o.kernel == FDTD_KERNEL_FUSED && (o.tile_y == 1 || o.tile_y == 2)) build_shell_boxes(s.get(), o.tile_y);
+    s->region.shell = s->shell;
     if (o.x_chunk > 0) s->xchunk = o.x_chunk;
     else {
         const long long cols = (long long)((N[2] + 31) / 32) * ((N[1] + s->tile_y - 1) / s->tile_y);

@@ -60,12 +60,17 @@ struct Box3 {
     int hi[3];
 };
 
-// The PML shell as up to six disjoint boxes; first[] holds prefix sums of cell counts.
+// The PML shell as up to five disjoint boxes (x slabs, y slabs, the merged z-slab
+// pair).  Box b covers x in [x0, x0+nx), y in [y0, y0+ny) and nz z indices:
+// z = zz < nza ? z0a + zz : z0b + (zz - nza).  Tiles are 32 z x 8 y x xs x;
+// block_first[] is the prefix sum of tiles per box.
 struct ShellBoxes {
-    int n;
-    int start[6][3];
-    int size[6][3];
-    long long first[7];
+    int n, xs;
+    int x0[5], nx[5], y0[5], ny[5];
+    int z0a[5], nza[5], z0b[5], nz[5];
+    int tz[5], ty[5], tx[5];
+    int block_first[6];
+    long long cells;
 };
 
 // Launch description of one region-split step.

@@ -35,7 +35,7 @@ cudaError_t launch_step_fused_fp32(const SolveParams* dP, const int N[3], int cu
 
 }  // namespace fdtd
 
-#include "fdtd_region.cuh"
+#include "fdtd_shell.cuh"
 namespace fdtd {
 cudaError_t launch_step_regions_fp32(const SolveParams* dP, const RegionLaunch& R, int cur, cudaStream_t s,
                                      int* launches) {

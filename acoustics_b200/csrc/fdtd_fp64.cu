@@ -8,6 +8,7 @@
 #include "fdtd_device.cuh"
 #include "fdtd_geometry.cuh"
 #include "fdtd_launch.hpp"
+#include "fdtd_listeners.cuh"
 #include "fdtd_stencil.cuh"
 
 namespace fdtd {
@@ -93,90 +94,7 @@ __global__ void k_cls_ghost(const SolveParams* __restrict__ Pp, long long n) {
     }
 }
 
-// ---------------------------------------------------------------------------
-// Listener sampling (PML_WaveSolver::FetchScalarData, PML_WaveSolver.cpp:210-317)
-// ---------------------------------------------------------------------------
-constexpr int MAX_MLS_POINTS = 8 * 6;
-
-// Gather the MLS stencil of point pt: enclosing cells (ascending flat index),
-// NaN cells dropped, ghost cells replaced by their ghost faces in key order
-// (neighbour flat index ascending: -x, -y, -z, +z, +y, +x).
-template <typename T>
-__device__ double sample_point(const SolveParams& P, const T* __restrict__ pnew, const T* __restrict__ pold,
-                               double t, const double pt[3], int* bad) {
-    int cells[8];
-    const int nc = enclosing_neighbours(P, pt, cells);
-    const long long sx = (long long)P.N[1] * P.N[2];
-    double A[MAX_MLS_POINTS * 4];
-    double b[MAX_MLS_POINTS];
-    int np = 0;
-    int kept[8];
-    int nk = 0;
-    for (int q = 0; q < nc; ++q) {
-        const int cell = cells[q];
-        const double v = (double)pnew[cell];
-        if (isnan(v)) continue;
-        kept[nk++] = cell;
-        const uint8_t code = P.cls[cell];
-        const int i = (int)(cell / sx), j = (int)((cell / P.N[2]) % P.N[1]), k = (int)(cell % P.N[2]);
-        const double cp[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
-        const unsigned mask = code & CLS_MASK;
-        if ((code & CLS_BULK) || mask == 0) {
-            mls_row(pt, cp, v, &A[np * 4], b[np]);
-            ++np;
-        } else {
-            const int order_dim[6] = {0, 1, 2, 2, 1, 0};
-            const int order_sgn[6] = {-1, -1, -1, +1, +1, +1};
-            const long long strides[3] = {sx, P.N[2], 1};
-            for (int f = 0; f < 6; ++f) {
-                const int d = order_dim[f], s = order_sgn[f];
-                if (!((mask >> (2 * d + (s > 0 ? 1 : 0))) & 1u)) continue;
-                const long long nbr = cell + s * strides[d];
-                const double pg = ghost_pressure(P, P.gobj[cell], cp, d, s, (double)pold[nbr], t);
-                double fp[3] = {cp[0], cp[1], cp[2]};
-                fp[d] += (s > 0 ? 1.0 : -1.0) * 0.25 * P.h;
-                mls_row(pt, fp, pg, &A[np * 4], b[np]);
-                ++np;
-            }
-        }
-    }
-    if (nk == 0) {
-        *bad = 1;
-        return 0.0;
-    }
-    if (nk < 4) {  // nearest cell (PML_WaveSolver.cpp:294-309)
-        int best = -1;
-        double bestD = DBL_MAX;
-        for (int q = 0; q < nk; ++q) {
-            const int cell = kept[q];
-            const int i = (int)(cell / sx), j = (int)((cell / P.N[2]) % P.N[1]), k = (int)(cell % P.N[2]);
-            const double dx = P.cpos[0][i] - pt[0], dy = P.cpos[1][j] - pt[1], dz = P.cpos[2][k] - pt[2];
-            const double d2 = dx * dx + dy * dy + dz * dz;
-            if (d2 < bestD) { best = cell; bestD = d2; }
-        }
-        return (double)pnew[best];
-    }
-    double c0 = 0.0;
-    if (!householder_ls4(A, b, np, c0)) {
-        *bad = 1;
-        c0 = 0.0;
-    }
-    return c0;
-}
-
-template <typename T>
-__global__ void k_listeners(const SolveParams* __restrict__ Pp, int newp, double* __restrict__ out_row) {
-    const SolveParams& P = *Pp;
-    const int li = blockIdx.x * blockDim.x + threadIdx.x;
-    if (li >= P.n_lis) return;
-    const T* pnew = (const T*)P.p[newp];
-    const T* pold = (const T*)P.p[newp ^ 1];
-    const double pt[3] = {P.listeners[3 * li], P.listeners[3 * li + 1], P.listeners[3 * li + 2]};
-    int bad = 0;
-    const double v = sample_point<T>(P, pnew, pold, P.consts->t, pt, &bad);
-    out_row[li] = v;
-    if (bad) atomicOr(&P.consts->error, 1);
-}
+// Listener sampling: fdtd_listeners.cuh (one warp per listener)
 
 // ---------------------------------------------------------------------------
 // Fresh-cell interpolation (MAC_Grid::InterpolateFreshPressureCell, MLS branch,
@@ -427,10 +345,10 @@ cudaError_t launch_step_fused_fp64(const SolveParams* dP, const int N[3], int cu
 cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int n_lis, double* out_row,
                              cudaStream_t s) {
     if (n_lis <= 0) return cudaSuccess;
-    const int block = 64;
-    const int grid = (n_lis + block - 1) / block;
-    if (precision == 0) k_listeners<double><<<grid, block, 0, s>>>(dP, newp, out_row);
-    else k_listeners<float><<<grid, block, 0, s>>>(dP, newp, out_row);
+    const int warps_per_block = 4;
+    const int grid = (n_lis + warps_per_block - 1) / warps_per_block;
+    if (precision == 0) k_listeners_warp<double><<<grid, 32 * warps_per_block, 0, s>>>(dP, newp, out_row);
+    else k_listeners_warp<float><<<grid, 32 * warps_per_block, 0, s>>>(dP, newp, out_row);
     return cudaGetLastError();
 }
 
@@ -476,7 +394,7 @@ cudaError_t launch_phased_fp64(const SolveParams* dP, const int N[3], int cur, d
 // ---------------------------------------------------------------------------
 // region-split step, FP64
 // ---------------------------------------------------------------------------
-#include "fdtd_region.cuh"
+#include "fdtd_shell.cuh"
 namespace fdtd {
 cudaError_t launch_step_regions_fp64(const SolveParams* dP, const RegionLaunch& R, int cur, cudaStream_t s,
                                      int* launches) {

@@ -1,0 +1,197 @@
+// fdtd_listeners.cuh — listener sampling, one warp per listener
+// (PML_WaveSolver::FetchScalarData, PML_WaveSolver.cpp:210-317, with the order-1
+// MLS of MLSModeInterpolator::lookup, MLSModeInterpolator.hpp:282-431).
+//
+// Lanes 0..7 read the (up to) eight enclosing cells; a warp scan turns their
+// point counts (0 for NaN, 1 for a bulk or plain solid cell, one per ghost face
+// for a ghost cell) into the row index of every MLS sample, so lane j builds
+// rows j and j+32.  The weighted least-squares fit is a Householder QR whose
+// column norms and dot products are warp reductions; its solution is the unique
+// minimiser for a full-rank stencil, as with the reference's JacobiSVD.
+#pragma once
+#include "fdtd_device.cuh"
+#include "fdtd_geometry.cuh"
+
+namespace fdtd {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// The k-th (0-based) set direction of a ghost mask in key order
+// (-x, -y, -z, +z, +y, +x) as (dim, sign).
+__device__ __forceinline__ void kth_face(unsigned mask, int k, int& d, int& s) {
+    const int od[6] = {0, 1, 2, 2, 1, 0};
+    const int os[6] = {-1, -1, -1, +1, +1, +1};
+    d = 0;
+    s = -1;
+    int seen = 0;
+    for (int f = 0; f < 6; ++f) {
+        if ((mask >> (2 * od[f] + (os[f] > 0 ? 1 : 0))) & 1u) {
+            if (seen == k) { d = od[f]; s = os[f]; return; }
+            ++seen;
+        }
+    }
+}
+
+template <typename T>
+__device__ void build_row(const SolveParams& P, const T* __restrict__ pold, double t, const double pt[3], int cell,
+                          uint8_t code, double v, int k, double A[4], double& b) {
+    const int Nz = P.N[2], Ny = P.N[1];
+    const long long sx = (long long)Ny * Nz;
+    const int i = (int)(cell / sx), j = (int)((cell / Nz) % Ny), kk = (int)(cell % Nz);
+    const double cp[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][kk]};
+    const unsigned mask = code & CLS_MASK;
+    if ((code & CLS_BULK) || mask == 0) {
+        mls_row(pt, cp, v, A, b);
+        return;
+    }
+    int d, s;
+    kth_face(mask, k, d, s);
+    const long long strides[3] = {sx, Nz, 1};
+    const long long nbr = cell + s * strides[d];
+    const double pg = ghost_pressure(P, P.gobj[cell], cp, d, s, (double)pold[nbr], t);
+    double fp[3] = {cp[0], cp[1], cp[2]};
+    fp[d] += (s > 0 ? 1.0 : -1.0) * 0.25 * P.h;
+    mls_row(pt, fp, pg, A, b);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_listeners_warp(const SolveParams* __restrict__ Pp, int newp,
+                                                        double* __restrict__ out_row) {
+    const SolveParams& P = *Pp;
+    const int lane = threadIdx.x & 31;
+    const int li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (li >= P.n_lis) return;  // the whole warp leaves together
+    const T* __restrict__ pnew = (const T*)P.p[newp];
+    const T* __restrict__ pold = (const T*)P.p[newp ^ 1];
+    const double t = P.consts->t;
+    const double pt[3] = {P.listeners[3 * li], P.listeners[3 * li + 1], P.listeners[3 * li + 2]};
+    int cells[8];
+    const int nc = enclosing_neighbours(P, pt, cells);
+
+    // ---- per-cell value, class and point count (lanes 0..nc-1) ----
+    int cellq = lane < nc ? cells[lane < 8 ? lane : 0] : 0;
+    double v = 0.0;
+    uint8_t code = 0;
+    if (lane < nc) {
+        v = (double)pnew[cellq];
+        code = P.cls[cellq];
+    }
+    const bool kept = lane < nc && !isnan(v);
+    int cnt = 0;
+    if (kept) cnt = ((code & CLS_BULK) || !(code & CLS_MASK)) ? 1 : __popc(code & CLS_MASK);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int n = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += n;
+    }
+    const int excl = incl - cnt;
+    const int total = __shfl_sync(0xffffffffu, incl, nc - 1);
+    const unsigned keptmask = __ballot_sync(0xffffffffu, kept);
+    const int nk = __popc(keptmask);
+    if (nk == 0) {
+        if (lane == 0) {
+            out_row[li] = 0.0;
+            atomicOr(&P.consts->error, 1);
+        }
+        return;
+    }
+    if (nk < 4) {  // nearest kept cell centre (PML_WaveSolver.cpp:294-309)
+        double d2 = DBL_MAX;
+        if (kept) {
+            const int Nz = P.N[2], Ny = P.N[1];
+            const long long sx = (long long)Ny * Nz;
+            const int i = (int)(cellq / sx), j = (int)((cellq / Nz) % Ny), k = (int)(cellq % Nz);
+            const double dx = P.cpos[0][i] - pt[0], dy = P.cpos[1][j] - pt[1], dz = P.cpos[2][k] - pt[2];
+            d2 = dx * dx + dy * dy + dz * dz;
+        }
+        // first minimum in ascending cell order (strict <)
+        double best = DBL_MAX;
+        int bl = -1;
+        for (int q = 0; q < nc; ++q) {
+            const double dq = __shfl_sync(0xffffffffu, d2, q);
+            if (dq < best) { best = dq; bl = q; }
+        }
+        const double val = __shfl_sync(0xffffffffu, v, bl < 0 ? 0 : bl);
+        if (lane == 0) out_row[li] = val;
+        return;
+    }
+
+    // ---- rows: lane j owns sample rows j and j + 32 ----
+    double A0[4] = {0, 0, 0, 0}, A1[4] = {0, 0, 0, 0};
+    double b0 = 0.0, b1 = 0.0;
+    const bool has0 = lane < total, has1 = lane + 32 < total;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        const int r = lane + 32 * half;
+        // owner cell q: excl[q] <= r < excl[q] + cnt[q]
+        int owner = 0, first = 0;
+        for (int q = 0; q < nc; ++q) {
+            const int eq = __shfl_sync(0xffffffffu, excl, q);
+            const int cq = __shfl_sync(0xffffffffu, cnt, q);
+            if (cq > 0 && r >= eq && r < eq + cq) { owner = q; first = eq; }
+        }
+        const double vq = __shfl_sync(0xffffffffu, v, owner);
+        const int codeq = __shfl_sync(0xffffffffu, (int)code, owner);
+        const int cellqq = __shfl_sync(0xffffffffu, cellq, owner);
+        if (half == 0 && has0) build_row<T>(P, pold, t, pt, cellqq, (uint8_t)codeq, vq, r - first, A0, b0);
+        if (half == 1 && has1) build_row<T>(P, pold, t, pt, cellqq, (uint8_t)codeq, vq, r - first, A1, b1);
+    }
+
+    // ---- Householder QR, warp-parallel ----
+    double R[4][4];
+    bool ok = true;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const bool a0 = has0 && lane >= j;          // row index lane >= j
+        const bool a1 = has1;                        // rows >= 32 are always >= j
+        double s = (a0 ? A0[j] * A0[j] : 0.0) + (a1 ? A1[j] * A1[j] : 0.0);
+        s = warp_sum(s);
+        const double norm = sqrt(s);
+        if (!(norm > 0.0)) ok = false;
+        const double x0 = __shfl_sync(0xffffffffu, A0[j], j);
+        const double alpha = x0 > 0.0 ? -norm : norm;
+        if (lane == j) A0[j] = x0 - alpha;
+        double vn = (a0 ? A0[j] * A0[j] : 0.0) + (a1 ? A1[j] * A1[j] : 0.0);
+        vn = warp_sum(vn);
+#pragma unroll
+        for (int cc = j + 1; cc < 4; ++cc) {
+            double dot = (a0 ? A0[j] * A0[cc] : 0.0) + (a1 ? A1[j] * A1[cc] : 0.0);
+            dot = warp_sum(dot);
+            const double f = 2.0 * dot / vn;
+            if (a0) A0[cc] -= f * A0[j];
+            if (a1) A1[cc] -= f * A1[j];
+        }
+        {
+            double dot = (a0 ? A0[j] * b0 : 0.0) + (a1 ? A1[j] * b1 : 0.0);
+            dot = warp_sum(dot);
+            const double f = 2.0 * dot / vn;
+            if (a0) b0 -= f * A0[j];
+            if (a1) b1 -= f * A1[j];
+        }
+        R[j][j] = alpha;
+#pragma unroll
+        for (int cc = j + 1; cc < 4; ++cc) R[j][cc] = __shfl_sync(0xffffffffu, A0[cc], j);
+    }
+    double bt[4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) bt[j] = __shfl_sync(0xffffffffu, b0, j);
+    if (lane != 0) return;
+    const double rmax = dmax(dmax(fabs(R[0][0]), fabs(R[1][1])), dmax(fabs(R[2][2]), fabs(R[3][3])));
+    for (int j = 0; j < 4; ++j)
+        if (fabs(R[j][j]) <= (double)(total > 4 ? total : 4) * 2.220446049250313e-16 * rmax) ok = false;
+    double x[4];
+    for (int j = 3; j >= 0; --j) {
+        double s = bt[j];
+        for (int cc = j + 1; cc < 4; ++cc) s -= R[j][cc] * x[cc];
+        x[j] = s / R[j][j];
+    }
+    out_row[li] = ok ? x[0] : 0.0;
+    if (!ok) atomicOr(&P.consts->error, 1);
+}
+
+}  // namespace fdtd

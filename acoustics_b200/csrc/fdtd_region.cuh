@@ -199,105 +199,4 @@ __global__ void __launch_bounds__(256) k_interior(const SolveParams* __restrict_
     }
 }
 
-// One PML cell per thread over the concatenated shell boxes (z fastest).
-template <typename T>
-__global__ void __launch_bounds__(256) k_pml_shell(const SolveParams* __restrict__ Pp, int cur, ShellBoxes B) {
-    const SolveParams& P = *Pp;
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= B.first[B.n]) return;
-    int b = 0;
-    while (t >= B.first[b + 1]) ++b;
-    long long r = t - B.first[b];
-    const int z = B.start[b][2] + (int)(r % B.size[b][2]);
-    r /= B.size[b][2];
-    const int y = B.start[b][1] + (int)(r % B.size[b][1]);
-    const int x = B.start[b][0] + (int)(r / B.size[b][1]);
-    const int N[3] = {P.N[0], P.N[1], P.N[2]};
-    const long long sx = (long long)N[1] * N[2];
-    const long long c = (long long)x * sx + (long long)y * N[2] + z;
-    const T* __restrict__ pc = (const T*)P.p[cur];
-    T* __restrict__ pn = (T*)P.p[cur ^ 1];
-    const T p0 = pc[c];
-    const int idx[3] = {x, y, z};
-    const long long pstride[3] = {sx, N[2], 1};
-    const long long fl[3] = {c, ((long long)x * (N[1] + 1) + y) * N[2] + z, ((long long)x * N[1] + y) * (N[2] + 1) + z};
-    const long long fstride[3] = {sx, N[2], 1};
-    const bool pmlc[3] = {P.pml_cell[0][x] != 0, P.pml_cell[1][y] != 0, P.pml_cell[2][z] != 0};
-    const T inv_h = (T)P.inv_h;
-    T acc = 0;
-    T pdn[3];
-#pragma unroll
-    for (int d = 0; d < 3; ++d) {
-        const int d1 = (d + 1) % 3, d2 = (d + 2) % 3;
-        const bool other = pmlc[d1] || pmlc[d2];
-        const int i = idx[d];
-        const T* __restrict__ vo = (const T*)P.v[cur][d];
-        T* __restrict__ vn = (T*)P.v[cur ^ 1][d];
-        const T* __restrict__ vupd = Coef<T>::vupd(P, d);
-        const T* __restrict__ vgrad = Coef<T>::vgrad(P, d);
-        // left face (owned)
-        T vl = vo[fl[d]];
-        if (i > 0 && (P.pml_face[d][i] != 0 || other)) {
-            vl = vel_update<T>(vl, vupd[i], vgrad[i], p0, pc[c - pstride[d]]);
-            vn[fl[d]] = vl;
-        }
-        // right face (owned only when the right cell is not in the PML)
-        const long long fr = fl[d] + fstride[d];
-        T vr = vo[fr];
-        if (i + 1 < N[d] && (P.pml_face[d][i + 1] != 0 || other)) {
-            vr = vel_update<T>(vr, vupd[i + 1], vgrad[i + 1], pc[c + pstride[d]], p0);
-            const bool right_pml = P.pml_cell[d][i + 1] != 0 || other;
-            if (!right_pml) vn[fr] = vr;
-        }
-        T* __restrict__ pd = (T*)P.pd[d];
-        const T a = pd_update<T>(pd[c], Coef<T>::pupd(P, d)[i], Coef<T>::pdiv(P, d)[i], vr, vl, inv_h);
-        pd[c] = a;
-        pdn[d] = a;
-    }
-    acc = pdn[0] + pdn[1] + pdn[2];
-    pn[c] = acc;
-}
-
-}  // namespace fdtd
-
-namespace fdtd {
-
-// Host side: one step of the region-split path on `s`.
-template <typename T>
-cudaError_t launch_regions(const SolveParams* dP, const RegionLaunch& R, int cur, cudaStream_t s, int* launches) {
-    int l = 0;
-    const long long n = R.shell.first[R.shell.n];
-    if (n > 0) {
-        k_pml_shell<T><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(dP, cur, R.shell);
-        ++l;
-    }
-    const Box3& b = R.interior;
-    const int nx = b.hi[0] - b.lo[0], ny = b.hi[1] - b.lo[1], nz = b.hi[2] - b.lo[2];
-    if (nx > 0 && ny > 0 && nz > 0) {
-        dim3 block(32, 8);
-        const int xb = (R.xb == 2 || R.xb == 8) ? R.xb : 4;
-        dim3 grid((nz + 31) / 32, (ny + 7) / 8, (nx + xb - 1) / xb);
-        if (xb == 2) k_interior<T, 2><<<grid, block, 0, s>>>(dP, cur, b);
-        else if (xb == 8) k_interior<T, 8><<<grid, block, 0, s>>>(dP, cur, b);
-        else k_interior<T, 4><<<grid, block, 0, s>>>(dP, cur, b);
-        ++l;
-    }
-    if (R.ghost_cap > 0) {
-        const int blocks = (R.ghost_cap + 127) / 128 < 1184 ? (R.ghost_cap + 127) / 128 : 1184;
-        k_ghost_cells<T><<<blocks, 128, 0, s>>>(dP, cur);
-        ++l;
-    }
-    if (R.sources) {
-        const Box3& r = R.src_region;
-        const long long total = (long long)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);
-        if (total > 0) {
-            const long long g = (total + 255) / 256;
-            k_sources<T><<<(unsigned)(g < 148 * 16 ? g : 148 * 16), 256, 0, s>>>(dP, cur, r);
-            ++l;
-        }
-    }
-    if (launches) *launches += l;
-    return cudaGetLastError();
-}
-
 }  // namespace fdtd

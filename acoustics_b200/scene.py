@@ -272,18 +272,19 @@ def config1(seed_src: int = 1, seed_lis: int = 2, divisions=(64, 64, 64), pml_wi
     return sc
 
 
-def config2(seed_pose: int = 3, seed_lis: int = 4, steps: int = 4000) -> Scene:
+def config2(seed_pose: int = 3, seed_lis: int = 4, steps: int = 4000, n: int = 256) -> Scene:
     """256^3, h=2.5 mm, 16-cell PML, sphere r=3 cm + axis-aligned box 4x2x1 cm +
     ellipsoid 3/2/1 cm at seeded non-overlapping poses, Gaussian-in-time
     translational boundary acceleration of amplitude 1e3 m/s^2, 64 listeners on a
-    seeded sphere shell."""
-    h = 0.0025
+    seeded sphere shell.  n != 256 keeps the 64 cm domain and PML thickness with
+    h = 0.64/n."""
+    h = 0.0025 * 256 / n
     k = reference_time_step(h)
-    sc = Scene(cell_size=h, divisions=(256, 256, 256), time_step=k, pml_width=16, steps=steps,
-               name="cfg2_256cube_3objects")
+    sc = Scene(cell_size=h, divisions=(n, n, n), time_step=k, pml_width=16 * n / 256, steps=steps,
+               name="cfg2_256cube_3objects" if n == 256 else f"cfg2_{n}cube_3objects")
     rng = np.random.default_rng(seed_pose)
     half_ext = [np.array([0.03, 0.03, 0.03]), np.array([0.02, 0.01, 0.005]), np.array([0.03, 0.02, 0.01])]
-    lo, hi = _non_pml_box(sc, 12.0)
+    lo, hi = _non_pml_box(sc, 12.0 * n / 256)
     centers = []
     while len(centers) < 3:
         e = half_ext[len(centers)]
