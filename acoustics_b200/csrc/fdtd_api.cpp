@@ -428,6 +428,9 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     s->precision = o.precision;
     CUDA_TRY(nullptr, cudaSetDevice(o.device));
     CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
+    CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
+    CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
     solver_init_geometry(s.get(), sc);
     for (int i = 0; i < sc->n_objects; ++i) {
         HostObject h;
@@ -468,8 +471,8 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         if (o.kernel != FDTD_KERNEL_PHASED) cv.add(&P.v[1][d], nf * w);  // double-buffered faces
     }
     if (o.kernel == FDTD_KERNEL_PHASED) cv.add((void**)&s->d_lap, n * 8);
-    cv.add((void**)&P.clock, 8);
-    cv.add((void**)&P.consts, sizeof(StepConsts));
+    cv.add((void**)&P.consts, 2 * sizeof(StepConsts));
+    cv.add((void**)&P.dev_error, 16);
     cv.add((void**)&s->d_status, 16);
     cv.add((void**)&P.listeners, std::max<size_t>(1, s->listeners.size()) * 8);
     for (int d = 0; d < 3; ++d) {
@@ -640,6 +643,10 @@ fdtd_status fdtd_solver_destroy(fdtd_solver* s) {
         if (s->graph_exec[i]) cudaGraphExecDestroy(s->graph_exec[i]);
     if (s->arena) cudaFree(s->arena);
     if (s->h_lis_stage) cudaFreeHost(s->h_lis_stage);
+    cudaStreamSynchronize(s->stream2);
+    cudaEventDestroy(s->ev_fork);
+    cudaEventDestroy(s->ev_join);
+    cudaStreamDestroy(s->stream2);
     cudaStreamDestroy(s->stream);
     delete s;
     return FDTD_OK;
@@ -664,7 +671,8 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     // initFieldRasterized: every cell bulk with valid history (MAC_Grid.cpp:2459-2470, :4170-4180)
     CUDA_TRY(s, cudaMemsetAsync(P.cls, CLS_BULK | CLS_VALID, s->ncell, s->stream));
     CUDA_TRY(s, cudaMemsetAsync(P.gobj, GOBJ_NONE, s->ncell, s->stream));
-    CUDA_TRY(s, cudaMemsetAsync(P.consts, 0, sizeof(StepConsts), s->stream));
+    CUDA_TRY(s, cudaMemsetAsync(P.consts, 0, 2 * sizeof(StepConsts), s->stream));
+    CUDA_TRY(s, cudaMemsetAsync(P.dev_error, 0, sizeof(int), s->stream));
     CUDA_TRY(s, cudaMemsetAsync(s->d_status, 0, 16, s->stream));
     s->time = t0;
     s->state_time = t0;
@@ -681,7 +689,7 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     P.n_solid_pml = 0;
     fdtd_status st = upload_params(s);
     if (st != FDTD_OK) return st;
-    CUDA_TRY(s, cudaMemcpyAsync(P.clock, &s->time, 8, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, launch_consts_init(s->dP, t0, s->stream));
     s->launches = 0;
     st = run_classification(s);
     if (st != FDTD_OK) return st;

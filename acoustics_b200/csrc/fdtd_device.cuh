@@ -73,6 +73,33 @@ struct ShellBoxes {
     long long cells;
 };
 
+struct SolveParams;
+
+// Pointers and scalars of the hot kernels, passed by value (kernel parameters
+// live in the constant bank, so the kernels issue no loads to fetch them).
+template <typename T>
+struct KArgs {
+    int N0, N1, N2;
+    unsigned sx;                  // N1*N2
+    const T* pc;                  // p^n
+    T* pn;                        // p^{n+1} (FP64: also p^{n-1} in place)
+    float* dinc;                  // FP32 increment
+    const uint8_t* cls;
+    T* pd[3];
+    const T* vo[3];
+    T* vn[3];
+    const uint8_t* pml_cell[3];
+    const uint8_t* pml_face[3];
+    const T* pupd[3];
+    const T* pdiv[3];
+    const T* vupd[3];
+    const T* vgrad[3];
+    T inv_h, c2k2, lap_scale;
+    SolveParams* P;               // device copy (for the step-constant advance)
+    int cur;
+    int advance;                  // the shell kernel advances consts[cur^1]
+};
+
 // Launch description of one region-split step.
 struct RegionLaunch {
     Box3 interior;
@@ -83,13 +110,12 @@ struct RegionLaunch {
     int xb;            // x planes per interior thread
 };
 
-// Written by the step prologue, read by the rest of the step.
+// Two copies indexed by the step parity: the kernels of a step read
+// consts[cur]; one thread of the step writes consts[cur^1] for the next step.
 struct StepConsts {
     double t;                       // simulation time at the start of the step
     double src_tf[FDTD_MAX_SOURCES];  // exp(-((t+k/2 - t0)/wt)^2/2)
     int64_t step;
-    int32_t error;                  // sticky device-side error flags
-    int32_t _pad;
 };
 
 struct SolveParams {
@@ -127,8 +153,8 @@ struct SolveParams {
     float* dinc;
     void* pd[3];
     void* v[2][3];
-    double* clock;                // simulation time of the next step
-    StepConsts* consts;
+    StepConsts* consts;           // [2], indexed by the step parity
+    int* dev_error;               // sticky device-side error flags
     const double* listeners;      // 3*n_lis
     int* solid_pml;               // solid cells inside the PML (re-zeroed every step)
     int n_solid_pml;
@@ -137,6 +163,25 @@ struct SolveParams {
     int ghost_cap;
     int precision;                // 0 fp64, 1 fp32 compensated
 };
+
+// consts[cur^1] <- the next step's constants (PML_WaveSolver.cpp:825,
+// _currentTime += _timeStep; source time factors at t + k/2).
+__device__ inline void advance_consts(const SolveParams& P, int cur) {
+    const StepConsts& c = P.consts[cur];
+    StepConsts& n = P.consts[cur ^ 1];
+    const double t = c.t + P.k;
+    n.t = t;
+    const double ts = t + 0.5 * P.k;
+    for (int s = 0; s < FDTD_MAX_SOURCES; ++s) {
+        double tf = 0.0;
+        if (s < P.n_src) {
+            const double u = (ts - P.src[s].t0) / P.src[s].wt;
+            tf = exp(-(u * u) / 2.0);
+        }
+        n.src_tf[s] = tf;
+    }
+    n.step = c.step + 1;
+}
 
 // Szudzik pairing of two cell indices (MAC_Grid.h:108-116)
 __host__ __device__ inline unsigned long long szudzik(int a_, int b_) {

@@ -8,10 +8,10 @@
 
 namespace fdtd {
 
-cudaError_t launch_prologue_fp32(const SolveParams* dP, int n_solid_pml, cudaStream_t s) {
+cudaError_t launch_prologue_fp32(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s) {
     int blocks = 1;
     if (n_solid_pml > 0) blocks = (n_solid_pml + 255) / 256 > 2368 ? 2368 : (n_solid_pml + 255) / 256;
-    k_prologue<float><<<blocks, 256, 0, s>>>(dP);
+    k_prologue<float><<<blocks, 256, 0, s>>>(dP, cur, advance);
     return cudaGetLastError();
 }
 
@@ -35,10 +35,11 @@ cudaError_t launch_step_fused_fp32(const SolveParams* dP, const int N[3], int cu
 
 }  // namespace fdtd
 
-#include "fdtd_shell.cuh"
+#include "fdtd_hot.cuh"
 namespace fdtd {
-cudaError_t launch_step_regions_fp32(const SolveParams* dP, const RegionLaunch& R, int cur, cudaStream_t s,
+cudaError_t launch_step_regions_fp32(const SolveParams* dP, const SolveParams& hP, const RegionLaunch& R, int cur,
+                                     cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
                                      int* launches) {
-    return launch_regions<float>(dP, R, cur, s, launches);
+    return launch_regions<float>(dP, hP, R, cur, s, s2, fork, join, launches);
 }
 }  // namespace fdtd

@@ -165,7 +165,7 @@ __device__ double fresh_value(const SolveParams& P, const T* __restrict__ pa, co
 template <typename T>
 __global__ void k_fresh_cells(const SolveParams* __restrict__ Pp, int cur, long long n, int* status) {
     const SolveParams& P = *Pp;
-    const double t = *P.clock;  // runs before the prologue: the clock holds t_n
+    const double t = P.consts[cur].t;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
         const uint8_t code = P.cls[c];
         if (!(code & CLS_BULK) || (code & CLS_VALID)) continue;
@@ -220,7 +220,7 @@ __global__ void k_phase_laplacian(const SolveParams* __restrict__ Pp, int cur, d
     const SolveParams& P = *Pp;
     const double* p = (const double*)P.p[cur];
     const long long sx = (long long)P.N[1] * P.N[2];
-    const double t = P.consts->t;
+    const double t = P.consts[cur].t;
     for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.ncell; c += (long long)gridDim.x * blockDim.x) {
         const uint8_t code = P.cls[c];
         if (!(code & CLS_BULK)) { lap[c] = 0.0; continue; }
@@ -266,7 +266,7 @@ __global__ void k_phase_pressure(const SolveParams* __restrict__ Pp, int cur, co
     const double* pc = (const double*)P.p[cur];
     double* pn = (double*)P.p[cur ^ 1];
     const long long sx = (long long)P.N[1] * P.N[2];
-    const StepConsts sc = *P.consts;
+    const StepConsts sc = P.consts[cur];
     bool any_src = false;
     for (int s = 0; s < P.n_src; ++s) any_src |= (sc.src_tf[s] != 0.0);
     const double* v0 = (const double*)P.v[0][0];
@@ -318,9 +318,14 @@ static int grid_for(long long n, int block) {
     return (int)g;
 }
 
-cudaError_t launch_prologue_fp64(const SolveParams* dP, int n_solid_pml, cudaStream_t s) {
+cudaError_t launch_prologue_fp64(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s) {
     const int blocks = n_solid_pml > 0 ? grid_for(n_solid_pml, 256) : 1;
-    k_prologue<double><<<blocks, 256, 0, s>>>(dP);
+    k_prologue<double><<<blocks, 256, 0, s>>>(dP, cur, advance);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_consts_init(const SolveParams* dP, double t0, cudaStream_t s) {
+    k_consts_init<<<1, 32, 0, s>>>(dP, t0);
     return cudaGetLastError();
 }
 
@@ -394,10 +399,11 @@ cudaError_t launch_phased_fp64(const SolveParams* dP, const int N[3], int cur, d
 // ---------------------------------------------------------------------------
 // region-split step, FP64
 // ---------------------------------------------------------------------------
-#include "fdtd_shell.cuh"
+#include "fdtd_hot.cuh"
 namespace fdtd {
-cudaError_t launch_step_regions_fp64(const SolveParams* dP, const RegionLaunch& R, int cur, cudaStream_t s,
+cudaError_t launch_step_regions_fp64(const SolveParams* dP, const SolveParams& hP, const RegionLaunch& R, int cur,
+                                     cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
                                      int* launches) {
-    return launch_regions<double>(dP, R, cur, s, launches);
+    return launch_regions<double>(dP, hP, R, cur, s, s2, fork, join, launches);
 }
 }  // namespace fdtd

@@ -33,6 +33,8 @@ struct fdtd_solver {
     fdtd_options opt{};
     int precision = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;   // second stream: interior kernel concurrent with the shell
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     // geometry
     double h = 0, c = 0, rho = 0, k = 0, end_time = 0, start_time = 0;
     int N[3] = {0, 0, 0};

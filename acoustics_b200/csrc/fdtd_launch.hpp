@@ -7,13 +7,16 @@
 namespace fdtd {
 
 // region-split step: PML shell, interior, ghost-neighbour list and (while active) sources
-cudaError_t launch_step_regions_fp64(const SolveParams* dP, const RegionLaunch& R, int cur, cudaStream_t s,
+cudaError_t launch_step_regions_fp64(const SolveParams* dP, const SolveParams& hP, const RegionLaunch& R, int cur,
+                                     cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
                                      int* launches);
-cudaError_t launch_step_regions_fp32(const SolveParams* dP, const RegionLaunch& R, int cur, cudaStream_t s,
+cudaError_t launch_step_regions_fp32(const SolveParams* dP, const SolveParams& hP, const RegionLaunch& R, int cur,
+                                     cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
                                      int* launches);
 
 // fdtd_fp64.cu (compiled with -fmad=false)
-cudaError_t launch_prologue_fp64(const SolveParams* dP, int n_solid_pml, cudaStream_t s);
+cudaError_t launch_prologue_fp64(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s);
+cudaError_t launch_consts_init(const SolveParams* dP, double t0, cudaStream_t s);
 cudaError_t launch_step_fused_fp64(const SolveParams* dP, const int N[3], int cur, int tile_y, int xchunk,
                                    cudaStream_t s);
 cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int n_lis, double* out_row,
@@ -29,7 +32,7 @@ cudaError_t launch_phased_fp64(const SolveParams* dP, const int N[3], int cur, d
                                int* launches);
 
 // fdtd_fp32.cu
-cudaError_t launch_prologue_fp32(const SolveParams* dP, int n_solid_pml, cudaStream_t s);
+cudaError_t launch_prologue_fp32(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s);
 cudaError_t launch_step_fused_fp32(const SolveParams* dP, const int N[3], int cur, int tile_y, int xchunk,
                                    cudaStream_t s);
 

@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(128) k_listeners_warp(const SolveParams* __res
     if (li >= P.n_lis) return;  // the whole warp leaves together
     const T* __restrict__ pnew = (const T*)P.p[newp];
     const T* __restrict__ pold = (const T*)P.p[newp ^ 1];
-    const double t = P.consts->t;
+    const double t = P.consts[newp ^ 1].t;
     const double pt[3] = {P.listeners[3 * li], P.listeners[3 * li + 1], P.listeners[3 * li + 2]};
     int cells[8];
     const int nc = enclosing_neighbours(P, pt, cells);
@@ -96,7 +96,7 @@ __global__ void __launch_bounds__(128) k_listeners_warp(const SolveParams* __res
     if (nk == 0) {
         if (lane == 0) {
             out_row[li] = 0.0;
-            atomicOr(&P.consts->error, 1);
+            atomicOr(P.dev_error, 1);
         }
         return;
     }
@@ -191,7 +191,7 @@ __global__ void __launch_bounds__(128) k_listeners_warp(const SolveParams* __res
         x[j] = s / R[j][j];
     }
     out_row[li] = ok ? x[0] : 0.0;
-    if (!ok) atomicOr(&P.consts->error, 1);
+    if (!ok) atomicOr(P.dev_error, 1);
 }
 
 }  // namespace fdtd

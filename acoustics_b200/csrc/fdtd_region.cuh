@@ -79,7 +79,7 @@ __global__ void __launch_bounds__(128) k_ghost_cells(const SolveParams* __restri
     const long long sx = (long long)Ny * Nz;
     const T* __restrict__ pc = (const T*)P.p[cur];
     T* __restrict__ pn = (T*)P.p[cur ^ 1];
-    const double t = P.consts->t;
+    const double t = P.consts[cur].t;
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n && g < P.ghost_cap; g += gridDim.x * blockDim.x) {
         const long long c = P.ghost_list[g];
         const int x = (int)(c / sx), y = (int)((c / Nz) % Ny), z = (int)(c % Nz);
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(128) k_ghost_cells(const SolveParams* __restri
 template <typename T>
 __global__ void __launch_bounds__(256) k_sources(const SolveParams* __restrict__ Pp, int cur, Box3 region) {
     const SolveParams& P = *Pp;
-    const StepConsts& sc = *P.consts;
+    const StepConsts& sc = P.consts[cur];
     bool any_src = false;
     for (int s = 0; s < P.n_src; ++s) any_src |= (sc.src_tf[s] != 0.0);
     if (!any_src) return;
@@ -129,72 +129,6 @@ __global__ void __launch_bounds__(256) k_sources(const SolveParams* __restrict__
             const float d = P.dinc[c] + (float)(src * P.k);
             P.dinc[c] = d;
             pn[c] = pc[c] + d;
-        }
-    }
-}
-
-template <typename T, int XB>
-__global__ void __launch_bounds__(256) k_interior(const SolveParams* __restrict__ Pp, int cur, Box3 box) {
-    const SolveParams& P = *Pp;
-    constexpr bool COMP = sizeof(T) == 4;
-    const int lane = threadIdx.x;
-    const int z = box.lo[2] + blockIdx.x * 32 + lane;
-    const int y = box.lo[1] + blockIdx.y * 8 + threadIdx.y;
-    const int x0 = box.lo[0] + blockIdx.z * XB;
-    const bool active = (z < box.hi[2]) && (y < box.hi[1]);
-    const int zc = min(z, box.hi[2] - 1);
-    const int yc = min(y, box.hi[1] - 1);
-    const int nx = min(XB, box.hi[0] - x0);
-    const int Nz = P.N[2];
-    const int sx = P.N[1] * Nz;
-    const long long off = (long long)x0 * sx + (long long)yc * Nz + zc;
-    const T* __restrict__ pc = (const T*)P.p[cur] + off;
-    T* __restrict__ pn = (T*)P.p[cur ^ 1] + off;
-    float* __restrict__ dinc = P.dinc + off;
-    const uint8_t* __restrict__ cls = P.cls + off;
-
-    // ---- issue every load of the XB planes before any arithmetic ----
-    T pcol[XB + 2];
-    T ym[XB], yp[XB], prev[XB];
-    uint8_t code[XB];
-    pcol[0] = pc[-sx];
-#pragma unroll
-    for (int i = 0; i < XB + 1; ++i)
-        if (i <= nx) pcol[i + 1] = pc[i * sx];
-#pragma unroll
-    for (int i = 0; i < XB; ++i) {
-        if (i < nx) {
-            ym[i] = pc[i * sx - Nz];
-            yp[i] = pc[i * sx + Nz];
-            if constexpr (COMP) prev[i] = (T)dinc[i * sx];
-            else prev[i] = pn[i * sx];
-            code[i] = cls[i * sx];
-        }
-    }
-    const T c2k2 = (T)P.c2k2;
-    const T lap_scale = (T)P.lap_scale;
-
-#pragma unroll
-    for (int i = 0; i < XB; ++i) {
-        if (i >= nx) break;
-        const T p0 = pcol[i + 1];
-        T zm = __shfl_up_sync(0xffffffffu, p0, 1);
-        T zp = __shfl_down_sync(0xffffffffu, p0, 1);
-        if (lane == 0) zm = pc[i * sx - 1];
-        if (lane == 31 || z + 1 >= box.hi[2]) zp = pc[i * sx + 1];
-        // solid cells stay untouched; cells next to a solid go to k_ghost_cells
-        if (!active || (code[i] & (CLS_BULK | CLS_MASK)) != CLS_BULK) continue;
-        T lap = 0.0;
-        lap = lap + (pcol[i + 2] + pcol[i] - (T)2.0 * p0);
-        lap = lap + (yp[i] + ym[i] - (T)2.0 * p0);
-        lap = lap + (zp + zm - (T)2.0 * p0);
-        lap = lap * lap_scale;
-        if constexpr (!COMP) {
-            pn[i * sx] = (T)2.0 * p0 - prev[i] + lap * c2k2;
-        } else {
-            const float d = (float)prev[i] + (float)(lap * c2k2);
-            dinc[i * sx] = d;
-            pn[i * sx] = p0 + d;
         }
     }
 }

@@ -111,7 +111,7 @@ __global__ void __launch_bounds__(32 * BY) k_step_fused(const SolveParams* __res
     T* __restrict__ vny = (T*)P.v[cur ^ 1][1];
     T* __restrict__ vnz = (T*)P.v[cur ^ 1][2];
     const uint8_t* __restrict__ cls = P.cls;
-    const StepConsts sc = *P.consts;
+    const StepConsts sc = P.consts[cur];
     const T inv_h = (T)P.inv_h;
     const T c2k2 = (T)P.c2k2;
     const T lap_scale = (T)P.lap_scale;
@@ -277,29 +277,13 @@ __global__ void __launch_bounds__(32 * BY) k_step_fused(const SolveParams* __res
     }
 }
 
-// Step prologue: publishes the step time and source time factors, advances
-// the device clock (PML_WaveSolver.cpp:825 _currentTime += _timeStep) and
-// re-zeroes solid cells inside the PML, which classifyCells_FAST zeroes at
-// the start of every step (MAC_Grid.cpp:3796-3798).
+// Step prologue: advances the step constants (PML_WaveSolver.cpp:825
+// _currentTime += _timeStep) and re-zeroes solid cells inside the PML, which
+// classifyCells_FAST zeroes at the start of every step (MAC_Grid.cpp:3796-3798).
 template <typename T>
-__global__ void k_prologue(const SolveParams* __restrict__ Pp) {
+__global__ void k_prologue(const SolveParams* __restrict__ Pp, int cur, int advance) {
     const SolveParams& P = *Pp;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        const double t = *P.clock;
-        StepConsts* sc = P.consts;
-        sc->t = t;
-        const double ts = t + 0.5 * P.k;
-        for (int s = 0; s < FDTD_MAX_SOURCES; ++s) {
-            double tf = 0.0;
-            if (s < P.n_src) {
-                const double u = (ts - P.src[s].t0) / P.src[s].wt;
-                tf = exp(-(u * u) / 2.0);
-            }
-            sc->src_tf[s] = tf;
-        }
-        sc->step = sc->step + 1;
-        *P.clock = t + P.k;
-    }
+    if (advance && blockIdx.x == 0 && threadIdx.x == 0) advance_consts(P, cur);
     T* p0 = (T*)P.p[0];
     T* p1 = (T*)P.p[1];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n_solid_pml; i += gridDim.x * blockDim.x) {
@@ -307,6 +291,18 @@ __global__ void k_prologue(const SolveParams* __restrict__ Pp) {
         p0[c] = (T)0;
         p1[c] = (T)0;
         if (P.dinc) P.dinc[c] = 0.0f;
+    }
+}
+
+// consts[0] <- the constants of the first step at time t0.
+static __global__ void k_consts_init(const SolveParams* __restrict__ Pp, double t0) {
+    const SolveParams& P = *Pp;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        P.consts[1].t = t0 - P.k;
+        P.consts[1].step = -1;
+        advance_consts(P, 1);
+        P.consts[0].t = t0;
+        P.consts[0].step = 0;
     }
 }
 

@@ -78,9 +78,14 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
             s->launches++;
         }
     }
+    // the region-split path advances the step constants inside its shell kernel;
+    // the prologue then only runs to re-zero solid cells inside the PML
+    const bool fused = s->opt.kernel == FDTD_KERNEL_FUSED;
     if (s->precision == FDTD_PRECISION_FP64) {
-        CUDA_TRY(s, launch_prologue_fp64(s->dP, s->n_solid_pml, s->stream));
-        s->launches++;
+        if (!fused || s->n_solid_pml > 0) {
+            CUDA_TRY(s, launch_prologue_fp64(s->dP, cur, fused ? 0 : 1, s->n_solid_pml, s->stream));
+            s->launches++;
+        }
         int l = 0;
         if (s->opt.kernel == FDTD_KERNEL_PHASED) {
             CUDA_TRY(s, launch_phased_fp64(s->dP, s->N, cur, s->d_lap, s->stream, &l));
@@ -88,18 +93,20 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
             CUDA_TRY(s, launch_step_fused_fp64(s->dP, s->N, cur, s->tile_y, s->xchunk, s->stream));
             l = 1;
         } else {
-            CUDA_TRY(s, launch_step_regions_fp64(s->dP, s->region, cur, s->stream, &l));
+            CUDA_TRY(s, launch_step_regions_fp64(s->dP, s->hP, s->region, cur, s->stream, s->stream2, s->ev_fork, s->ev_join, &l));
         }
         s->launches += l;
     } else {
-        CUDA_TRY(s, launch_prologue_fp32(s->dP, s->n_solid_pml, s->stream));
-        s->launches++;
+        if (!fused || s->n_solid_pml > 0) {
+            CUDA_TRY(s, launch_prologue_fp32(s->dP, cur, fused ? 0 : 1, s->n_solid_pml, s->stream));
+            s->launches++;
+        }
         int l = 0;
         if (s->opt.kernel == FDTD_KERNEL_STREAMING) {
             CUDA_TRY(s, launch_step_fused_fp32(s->dP, s->N, cur, s->tile_y, s->xchunk, s->stream));
             l = 1;
         } else {
-            CUDA_TRY(s, launch_step_regions_fp32(s->dP, s->region, cur, s->stream, &l));
+            CUDA_TRY(s, launch_step_regions_fp32(s->dP, s->hP, s->region, cur, s->stream, s->stream2, s->ev_fork, s->ev_join, &l));
         }
         s->launches += l;
     }
@@ -133,9 +140,9 @@ fdtd_status after_step(fdtd_solver* s) {
 }
 
 fdtd_status check_device_errors(fdtd_solver* s) {
-    StepConsts sc;
+    int dev_error = 0;
     int status[4] = {0, 0, 0, 0};
-    CUDA_TRY(s, cudaMemcpyAsync(&sc, s->hP.consts, sizeof(sc), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(&dev_error, s->hP.dev_error, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaMemcpyAsync(status, s->d_status, sizeof(status), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     int ghosts = 0;
@@ -149,7 +156,7 @@ fdtd_status check_device_errors(fdtd_solver* s) {
         set_error(s, "fresh cell inside an object (MAC_Grid.cpp:2050-2053)");
         return FDTD_ERR_GEOMETRY;
     }
-    if (sc.error & 1) {
+    if (dev_error & 1) {
         set_error(s, "degenerate listener stencil (no cell or rank-deficient MLS)");
         return FDTD_ERR_NUMERIC;
     }
@@ -295,11 +302,11 @@ fdtd_status fdtd_solver_time_stencil(fdtd_solver* s, int32_t n_launches, float* 
             if (s->opt.kernel == FDTD_KERNEL_PHASED) e = launch_phased_fp64(s->dP, s->N, c, s->d_lap, s->stream, nullptr);
             else if (s->opt.kernel == FDTD_KERNEL_STREAMING)
                 e = launch_step_fused_fp64(s->dP, s->N, c, s->tile_y, s->xchunk, s->stream);
-            else e = launch_step_regions_fp64(s->dP, s->region, c, s->stream, nullptr);
+            else e = launch_step_regions_fp64(s->dP, s->hP, s->region, c, s->stream, s->stream2, s->ev_fork, s->ev_join, nullptr);
         } else {
             if (s->opt.kernel == FDTD_KERNEL_STREAMING)
                 e = launch_step_fused_fp32(s->dP, s->N, c, s->tile_y, s->xchunk, s->stream);
-            else e = launch_step_regions_fp32(s->dP, s->region, c, s->stream, nullptr);
+            else e = launch_step_regions_fp32(s->dP, s->hP, s->region, c, s->stream, s->stream2, s->ev_fork, s->ev_join, nullptr);
         }
         if (e != cudaSuccess) {
             set_error(s, std::string("stencil launch: ") + cudaGetErrorString(e));
@@ -456,8 +463,8 @@ std::vector<std::pair<void*, size_t>> snap_regions(fdtd_solver* s) {
             if (P.v[b][d]) r.push_back({P.v[b][d], s->vcount[d] * w});
     r.push_back({P.cls, (size_t)s->ncell});
     r.push_back({P.gobj, (size_t)s->ncell});
-    r.push_back({P.clock, 8});
-    r.push_back({P.consts, sizeof(StepConsts)});
+    r.push_back({P.consts, 2 * sizeof(StepConsts)});
+    r.push_back({P.dev_error, sizeof(int)});
     return r;
 }
 }  // namespace
