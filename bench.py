@@ -99,36 +99,6 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def dist_setup():
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
-    pg = None
-    if world > 1:
-        import datetime
-
-        import torch
-        import torch.distributed as dist
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
-        pg = dist
-    return world, rank, local, pg
-
-
-def max_over_ranks(x: float, pg) -> float:
-    if pg is None:
-        return x
-    import torch
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    pg.all_reduce(t, op=pg.ReduceOp.MAX)
-    return float(t.item())
-
-
-def barrier(pg):
-    if pg is not None:
-        pg.barrier()
-
-
 def bench_scene(steps_for_accuracy=None):
     from acoustics_b200.scene import config2
     return config2()
@@ -152,7 +122,7 @@ def cpu_baseline(scene, budget_s: float, max_steps: int):
     return scene.n_cells * n / dt / 1e9, n, threads, dt
 
 
-def run_reference(args, world, rank, pg):
+def run_reference(args, world, rank):
     if rank != 0:
         return 0
     sc = bench_scene()
@@ -174,15 +144,34 @@ def run_reference(args, world, rank, pg):
     return 0
 
 
-def read_traffic(name: str):
-    """DRAM bytes per launch from the committed ncu summary, if one exists."""
-    p = os.path.join(ROOT, "profiles", "traffic.json")
+def read_traffic(precision: str, n: int):
+    """DRAM bytes per step of the step-kernel group from the committed ncu summary
+    (profiles/kernel_traffic.txt: `precision cells bytes` per line)."""
+    p = os.path.join(ROOT, "profiles", "kernel_traffic.txt")
     if not os.path.exists(p):
         return None
     with open(p) as f:
-        d = json.load(f)
-    v = d.get(name)
-    return v.get("dram_bytes_per_launch") if isinstance(v, dict) else None
+        for line in f:
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#") and parts[0] == precision and int(parts[1]) == n:
+                return float(parts[2])
+    return None
+
+
+def profile_run(args):
+    """Create the bench solve and run a few steps, nothing else: the command the
+    committed ncu summaries under profiles/ were captured with."""
+    from acoustics_b200 import scene as S
+    from acoustics_b200.solver import PML_WaveSolver
+    sc = S.config2(n=args.profile_n)
+    prec = S.PRECISION_FP32_COMPENSATED if args.precision == "fp32" else S.PRECISION_FP64
+    kern = S.KERNEL_PHASED if args.precision == "fp64-plain" else S.KERNEL_FUSED
+    g = PML_WaveSolver(sc, precision=prec, kernel=kern)
+    y = g.step(3 + args.steps)
+    g.close()
+    print(json.dumps({"profile_run": sc.name, "cells": sc.n_cells, "steps": 3 + args.steps,
+                      "max_abs_listener": float(np.abs(y).max())}))
+    return 0
 
 
 def main():
@@ -197,11 +186,19 @@ def main():
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--accuracy-steps", type=int, default=4000)
     ap.add_argument("--cpu-budget", type=float, default=15.0)
+    ap.add_argument("--profile", action="store_true", help="only run --steps steps of the bench solve (for ncu)")
+    ap.add_argument("--profile-n", type=int, default=256, help="grid edge of the --profile solve")
     args = ap.parse_args()
+    if args.profile:
+        return profile_run(args)
     args.warmup = max(3, args.warmup)
-    world, rank, local, pg = dist_setup()
+    from acoustics_b200 import dist
+    ranks = dist.init_from_env()
+    world, rank, local = ranks.world, ranks.rank, ranks.local
     if args.impl == "reference":
-        return run_reference(args, world, rank, pg)
+        rc = run_reference(args, world, rank)
+        dist.shutdown(ranks)
+        return rc
 
     import torch
 
@@ -221,7 +218,7 @@ def main():
     ext = torch.cuda.ExternalStream(solver.stream)
     solver.step_device(W, dev_out.data_ptr())
     solver.synchronize()
-    barrier(pg)
+    dist.barrier(ranks)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(torch.cuda.current_device()) as clk:
         torch.cuda.synchronize()
@@ -234,15 +231,17 @@ def main():
         # kernel-only timing of the dominant step kernel (same stream)
         kernel_ms = solver.time_stencil(K) / K
     ms = e0.elapsed_time(e1)
-    barrier(pg)
-    ms_max = max_over_ranks(ms, pg)
+    dist.barrier(ranks)
+    ms_max = dist.max_over_ranks(ms, ranks)
     ms_step = ms_max / K
     value = world * sc.n_cells * K / (ms_max / 1e3) / 1e9
     alg_bytes = float(info.algorithmic_bytes_per_step)
     peak, peak_kind = measured_peaks()
     achieved = alg_bytes / (kernel_ms / 1e3) / 1e9
-    kname = {"fp32": "k_step_fused<float,8>", "fp64": "k_step_fused<double,8>", "fp64-plain": "phased fp64"}[args.precision]
-    traffic = read_traffic(kname)
+    kname = {"fp32": "k_pml_shell<float> || k_interior<float> -> k_ghost_cells<float>",
+             "fp64": "k_pml_shell<double> || k_interior<double> -> k_ghost_cells<double>",
+             "fp64-plain": "phased fp64 (velocity x3, laplacian, pressure)"}[args.precision]
+    traffic = read_traffic(args.precision, sc.n_cells)
     clocks = clk.summary()
     y_ours = dev_out[W * L:(W + K) * L].cpu().numpy().reshape(K, L)
     solver.close()
@@ -250,13 +249,13 @@ def main():
     # end to end through the public API: create (scene upload + classification),
     # K steps with listener rows read back to host memory every chunk, destroy
     torch.cuda.synchronize()
-    barrier(pg)
+    dist.barrier(ranks)
     t0 = time.perf_counter()
     s2 = PML_WaveSolver(sc, precision=prec, kernel=kern, graph_steps=G, device=local)
     y_e2e = s2.step(K)
     s2.close()
     e2e_s = time.perf_counter() - t0
-    e2e_s = max_over_ranks(e2e_s, pg)
+    e2e_s = dist.max_over_ranks(e2e_s, ranks)
     e2e_val = world * sc.n_cells * K / e2e_s / 1e9
     scene_bytes = 4096 + 8 * 3 * L
 
@@ -324,8 +323,7 @@ def main():
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)
-    if pg is not None:
-        pg.destroy_process_group()
+    dist.shutdown(ranks)
     return 0
 
 
