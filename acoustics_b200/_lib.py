@@ -22,7 +22,7 @@ EXPORTS = [
     "fdtd_solver_stream", "fdtd_solver_last_error", "fdtd_solver_last_launch_count",
     "fdtd_solver_snapshot", "fdtd_solver_restore", "fdtd_scene_from_xml", "fdtd_scene_desc_get",
     "fdtd_scene_number_of_steps", "fdtd_scene_output_pattern", "fdtd_scene_free", "fdtd_audio_append",
-    "fdtd_solver_time_stencil",
+    "fdtd_solver_time_stencil", "fdtd_interior_step_noalloc",
 ]
 
 _lib = None
@@ -74,6 +74,8 @@ def load(build_if_missing: bool = False):
         "fdtd_scene_free": ([vp], None),
         "fdtd_audio_append": ([C.c_char_p, vp, i64], i32),
         "fdtd_solver_time_stencil": ([vp, i32, C.POINTER(C.c_float)], i32),
+        "fdtd_interior_step_noalloc": ([vp, vp, vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), dbl, dbl, vp],
+                                       i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -232,6 +232,30 @@ int64_t fdtd_solver_last_launch_count(fdtd_solver* s);
  * created for measurement. */
 fdtd_status fdtd_solver_time_stencil(fdtd_solver* s, int32_t n_launches, float* elapsed_ms);
 
+/* Interior leapfrog step that allocates nothing.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc where they step
+ * the field — code being captured into a CUDA graph (allocation is not
+ * capturable), real-time callbacks that must not block on the allocator, hosts
+ * whose own memory pool already holds the GPU's free memory.
+ * One step of the plain path's Laplacian + leapfrog (MAC_Grid.cpp:187-299,
+ * :921-935) on the box lo <= (i,j,k) < hi of a dims[0] x dims[1] x dims[2] FP64
+ * grid (flat index i*dims[1]*dims[2] + j*dims[2] + k, device pointers), every box
+ * cell treated as a bulk, non-PML cell with no solid neighbour:
+ *   p_next = 2 p_curr - p_prev + c2k2 * lap_scale * sum_d (p_+ + p_- - 2 p_curr)
+ * p_next may equal p_prev (in place); cells outside the box are not written.
+ * Requires 1 <= lo < hi <= dims-1 per axis and at most FDTD_NOALLOC_MAX_CELLS
+ * box cells (FDTD_ERR_INVALID_ARG otherwise).  The Laplacian scratch is one
+ * static device array of FDTD_NOALLOC_MAX_CELLS doubles (8 MiB) that every GPU
+ * loading the library keeps until exit.  The first call on a device looks up
+ * that array's device address (cudaGetSymbolAddress) with the device current:
+ * make it before any stream capture.  Calls share the array, so calls that
+ * overlap on the GPU race; serialise them on one stream.  `stream` is a
+ * cudaStream_t (NULL: the legacy default stream); the call only enqueues work. */
+#define FDTD_NOALLOC_MAX_CELLS (1 << 20)
+fdtd_status fdtd_interior_step_noalloc(const double* p_curr, const double* p_prev, double* p_next,
+                                       const int32_t dims[3], const int32_t lo[3], const int32_t hi[3],
+                                       double c2k2, double lap_scale, void* stream);
+
 /* Snapshot / restore of the resident state (_SaveSimulationSnapshot,
  * FDTD_AcousticSimulator.cpp:381-415).  bytes: query with buffer NULL. */
 fdtd_status fdtd_solver_snapshot(fdtd_solver* s, void* buffer, int64_t* bytes);
