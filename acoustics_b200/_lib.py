@@ -23,6 +23,9 @@ EXPORTS = [
     "fdtd_solver_snapshot", "fdtd_solver_restore", "fdtd_scene_from_xml", "fdtd_scene_desc_get",
     "fdtd_scene_number_of_steps", "fdtd_scene_output_pattern", "fdtd_scene_free", "fdtd_audio_append",
     "fdtd_solver_time_stencil", "fdtd_interior_step_noalloc",
+    "fdtd_batch_create", "fdtd_batch_add", "fdtd_batch_step", "fdtd_batch_run", "fdtd_batch_member_info",
+    "fdtd_batch_output", "fdtd_batch_release", "fdtd_batch_destroy", "fdtd_batch_stream",
+    "fdtd_batch_last_launch_count", "fdtd_batch_device_bytes", "fdtd_scene_device_bytes",
 ]
 
 _lib = None
@@ -76,6 +79,18 @@ def load(build_if_missing: bool = False):
         "fdtd_solver_time_stencil": ([vp, i32, C.POINTER(C.c_float)], i32),
         "fdtd_interior_step_noalloc": ([vp, vp, vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), dbl, dbl, vp],
                                        i32),
+        "fdtd_batch_create": ([i32, C.POINTER(SceneDesc), C.POINTER(i32), C.POINTER(Options), C.POINTER(vp)], i32),
+        "fdtd_batch_add": ([vp, C.POINTER(SceneDesc), i32, C.POINTER(i32)], i32),
+        "fdtd_batch_step": ([vp, i32, C.POINTER(i32)], i32),
+        "fdtd_batch_run": ([vp], i32),
+        "fdtd_batch_member_info": ([vp, i32, C.POINTER(i64), C.POINTER(i64), C.POINTER(i32), C.POINTER(i32)], i32),
+        "fdtd_batch_output": ([vp, i32, vp, i64], i32),
+        "fdtd_batch_release": ([vp, i32], i32),
+        "fdtd_batch_destroy": ([vp], i32),
+        "fdtd_batch_stream": ([vp], vp),
+        "fdtd_batch_last_launch_count": ([vp], i64),
+        "fdtd_batch_device_bytes": ([vp], i64),
+        "fdtd_scene_device_bytes": ([C.POINTER(SceneDesc), C.POINTER(Options)], i64),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -18,8 +18,8 @@ LIB = os.path.join(OUT_DIR, "libfdtd_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 CU_FP64 = ["fdtd_fp64.cu", "fdtd_noalloc.cu"]
-CU_FAST = ["fdtd_fp32.cu", "fdtd_batch.cu"]
-CPP = ["fdtd_api.cpp", "fdtd_step.cpp", "fdtd_xml.cpp", "fdtd_server.cpp"]
+CU_FAST = ["fdtd_fp32.cu"]
+CPP = ["fdtd_api.cpp", "fdtd_step.cpp", "fdtd_xml.cpp", "fdtd_batch.cpp", "fdtd_server.cpp"]
 
 
 def _nvcc() -> str:

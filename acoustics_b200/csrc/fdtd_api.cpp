@@ -378,6 +378,72 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
     return FDTD_OK;
 }
 
+// Offsets of every device array of a solver inside its one arena allocation;
+// needs the geometry (solver_init_geometry) and the listener list.
+static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_options& o, Carver& cv) {
+    const size_t w = s->precision == FDTD_PRECISION_FP64 ? 8 : 4;
+    const long long n = s->ncell;
+    const int* N = s->N;
+    SolveParams& P = s->hP;
+    std::memset(&P, 0, sizeof(P));
+    cv.add((void**)&s->dP, sizeof(SolveParams));
+    cv.add((void**)&P.cls, n);
+    cv.add((void**)&P.gobj, n);
+    cv.add(&P.p[0], n * w);
+    cv.add(&P.p[1], n * w);
+    if (s->precision != FDTD_PRECISION_FP64) cv.add((void**)&P.dinc, n * 4);
+    for (int d = 0; d < 3; ++d) cv.add(&P.pd[d], n * w);
+    for (int d = 0; d < 3; ++d) {
+        const long long nf = (long long)(N[0] + (d == 0)) * (N[1] + (d == 1)) * (N[2] + (d == 2));
+        s->vcount[d] = nf;
+        cv.add(&P.v[0][d], nf * w);
+        if (o.kernel != FDTD_KERNEL_PHASED) cv.add(&P.v[1][d], nf * w);  // double-buffered faces
+    }
+    if (o.kernel == FDTD_KERNEL_PHASED) cv.add((void**)&s->d_lap, n * 8);
+    cv.add((void**)&P.consts, 2 * sizeof(StepConsts));
+    cv.add((void**)&P.dev_error, 16);
+    cv.add((void**)&s->d_status, 16);
+    cv.add((void**)&P.listeners, std::max<size_t>(1, s->listeners.size()) * 8);
+    for (int d = 0; d < 3; ++d) {
+        cv.add((void**)&P.pml_cell[d], N[d]);
+        cv.add((void**)&P.pml_face[d], N[d] + 1);
+        cv.add((void**)&P.cpos[d], N[d] * 8);
+        cv.add((void**)&P.fpos[d], (N[d] + 1) * 8);
+        cv.add((void**)&P.pupd[d], N[d] * 8);
+        cv.add((void**)&P.pdiv[d], N[d] * 8);
+        cv.add((void**)&P.vupd[d], (N[d] + 1) * 8);
+        cv.add((void**)&P.vgrad[d], (N[d] + 1) * 8);
+        cv.add((void**)&P.pupd_f[d], N[d] * 4);
+        cv.add((void**)&P.pdiv_f[d], N[d] * 4);
+        cv.add((void**)&P.vupd_f[d], (N[d] + 1) * 4);
+        cv.add((void**)&P.vgrad_f[d], (N[d] + 1) * 4);
+    }
+    s->lis_cap_steps = std::max(256, o.graph_steps);
+    cv.add((void**)&s->d_lis, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8);
+    // ghost-neighbour list: at most 6 bulk neighbours per solid cell; solid cells lie
+    // in the object boxes (dilated by 2 cells, and by the travel of moving bodies)
+    {
+        double cells = 4096;
+        for (int i = 0; i < sc->n_objects; ++i) {
+            HostObject tmp;
+            tmp.d = sc->objects[i];
+            host_object_pose(tmp, sc->start_time);
+            host_update_bbox(tmp);
+            double vol = 1.0;
+            for (int d = 0; d < 3; ++d) {
+                double ext = (tmp.bmax[d] - tmp.bmin[d]) / s->h + 4.0;
+                if (tmp.d.motion != FDTD_MOTION_STATIC) ext *= 2.0;
+                vol *= std::min(ext, (double)N[d]);
+            }
+            cells += 6.0 * vol;
+        }
+        cells += 2.0 * sc->n_constraints * ((double)N[0] * N[1] + (double)N[1] * N[2] + (double)N[0] * N[2]);
+        s->region.ghost_cap = (int)std::min<double>(cells, (double)n);
+        cv.add((void**)&s->d_ghost_list, (size_t)s->region.ghost_cap * 4);
+        cv.add((void**)&s->d_ghost_count, 16);
+    }
+}
+
 extern "C" {
 
 int32_t fdtd_abi_version(void) { return FDTD_ABI_VERSION; }
@@ -449,72 +515,11 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     s->start_time = sc->start_time;
 
     // ---- device arena ----
-    const size_t w = s->precision == FDTD_PRECISION_FP64 ? 8 : 4;
+    Carver cv;
+    carve_arena(s.get(), sc, o, cv);
     const long long n = s->ncell;
     const int* N = s->N;
     SolveParams& P = s->hP;
-    std::memset(&P, 0, sizeof(P));
-    Carver cv;
-    void* dummy[64];
-    int di = 0;
-    cv.add((void**)&s->dP, sizeof(SolveParams));
-    cv.add((void**)&P.cls, n);
-    cv.add((void**)&P.gobj, n);
-    cv.add(&P.p[0], n * w);
-    cv.add(&P.p[1], n * w);
-    if (s->precision != FDTD_PRECISION_FP64) cv.add((void**)&P.dinc, n * 4);
-    for (int d = 0; d < 3; ++d) cv.add(&P.pd[d], n * w);
-    for (int d = 0; d < 3; ++d) {
-        const long long nf = (long long)(N[0] + (d == 0)) * (N[1] + (d == 1)) * (N[2] + (d == 2));
-        s->vcount[d] = nf;
-        cv.add(&P.v[0][d], nf * w);
-        if (o.kernel != FDTD_KERNEL_PHASED) cv.add(&P.v[1][d], nf * w);  // double-buffered faces
-    }
-    if (o.kernel == FDTD_KERNEL_PHASED) cv.add((void**)&s->d_lap, n * 8);
-    cv.add((void**)&P.consts, 2 * sizeof(StepConsts));
-    cv.add((void**)&P.dev_error, 16);
-    cv.add((void**)&s->d_status, 16);
-    cv.add((void**)&P.listeners, std::max<size_t>(1, s->listeners.size()) * 8);
-    for (int d = 0; d < 3; ++d) {
-        cv.add((void**)&P.pml_cell[d], N[d]);
-        cv.add((void**)&P.pml_face[d], N[d] + 1);
-        cv.add((void**)&P.cpos[d], N[d] * 8);
-        cv.add((void**)&P.fpos[d], (N[d] + 1) * 8);
-        cv.add((void**)&P.pupd[d], N[d] * 8);
-        cv.add((void**)&P.pdiv[d], N[d] * 8);
-        cv.add((void**)&P.vupd[d], (N[d] + 1) * 8);
-        cv.add((void**)&P.vgrad[d], (N[d] + 1) * 8);
-        cv.add((void**)&P.pupd_f[d], N[d] * 4);
-        cv.add((void**)&P.pdiv_f[d], N[d] * 4);
-        cv.add((void**)&P.vupd_f[d], (N[d] + 1) * 4);
-        cv.add((void**)&P.vgrad_f[d], (N[d] + 1) * 4);
-    }
-    (void)dummy;
-    (void)di;
-    s->lis_cap_steps = std::max(256, o.graph_steps);
-    cv.add((void**)&s->d_lis, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8);
-    // ghost-neighbour list: at most 6 bulk neighbours per solid cell; solid cells lie
-    // in the object boxes (dilated by 2 cells, and by the travel of moving bodies)
-    {
-        double cells = 4096;
-        for (int i = 0; i < sc->n_objects; ++i) {
-            HostObject tmp;
-            tmp.d = sc->objects[i];
-            host_object_pose(tmp, sc->start_time);
-            host_update_bbox(tmp);
-            double vol = 1.0;
-            for (int d = 0; d < 3; ++d) {
-                double ext = (tmp.bmax[d] - tmp.bmin[d]) / s->h + 4.0;
-                if (tmp.d.motion != FDTD_MOTION_STATIC) ext *= 2.0;
-                vol *= std::min(ext, (double)N[d]);
-            }
-            cells += 6.0 * vol;
-        }
-        cells += 2.0 * sc->n_constraints * ((double)N[0] * N[1] + (double)N[1] * N[2] + (double)N[0] * N[2]);
-        s->region.ghost_cap = (int)std::min<double>(cells, (double)n);
-        cv.add((void**)&s->d_ghost_list, (size_t)s->region.ghost_cap * 4);
-        cv.add((void**)&s->d_ghost_count, 16);
-    }
     void* base = nullptr;
     cudaError_t e = cudaMalloc(&base, cv.off);
     if (e != cudaSuccess) {
@@ -728,6 +733,21 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
         s->graph_exec[i] = nullptr;
     }
     return FDTD_OK;
+}
+
+int64_t fdtd_scene_device_bytes(const fdtd_scene_desc* sc, const fdtd_options* opt) {
+    if (validate_scene(sc) != FDTD_OK) return -1;
+    fdtd_options o{};
+    if (opt) o = *opt;
+    fdtd_solver s;
+    s.opt = o;
+    s.precision = o.precision;
+    solver_init_geometry(&s, sc);
+    s.listeners.assign(sc->listeners, sc->listeners + 3 * (size_t)sc->n_listeners);
+    s.L = sc->n_listeners;
+    Carver cv;
+    carve_arena(&s, sc, o, cv);
+    return (int64_t)cv.off;
 }
 
 }  // extern "C"

@@ -1,0 +1,484 @@
+// fdtd_batch.cpp — many independent static solves stepped together.
+//
+// Each member is a complete fdtd_solver (own device arrays, classification,
+// ghost list, sources, listeners).  Its first step runs through the solver's
+// own path (it classifies the cells); afterwards every step of all active
+// members is one call of launch_batch_*: persistent shell and interior kernels
+// over tile tables of all members, then batched ghost-list, source, listener
+// and advance kernels (fdtd_batch.cuh).  Members finish at their own step
+// counts and leave the tables; a captured graph of graph_steps batched steps is
+// replayed while the membership is unchanged.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/fdtd_c.h"
+#include "fdtd_device.cuh"
+#include "fdtd_internal.hpp"
+#include "fdtd_launch.hpp"
+
+using namespace fdtd;
+
+namespace fdtd {
+void build_shell_boxes(fdtd_solver* s, int xs);
+}
+
+namespace {
+
+struct Member {
+    fdtd_solver* s = nullptr;
+    int64_t total = 0;
+    int64_t done = 0;
+    bool active = false;
+    bool released = false;  // slot free for a later fdtd_batch_add
+    fdtd_status status = FDTD_OK;
+    int L = 0;
+    std::vector<double> rows;
+};
+
+}  // namespace
+
+struct fdtd_batch {
+    fdtd_options opt{};
+    int precision = 0;
+    cudaStream_t stream = nullptr, stream2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    std::vector<Member> members;
+    // device tables
+    void* d_descs = nullptr;
+    size_t desc_cap = 0;
+    BatchTile* d_int = nullptr;
+    size_t int_cap = 0;
+    BatchTile* d_shell = nullptr;
+    size_t shell_cap = 0;
+    ListenerRef* d_refs = nullptr;
+    size_t refs_cap = 0;
+    BatchLaunch L{};
+    bool dirty = true;
+    cudaGraphExec_t graph = nullptr;
+    long long launches = 0, last_launches = 0, graph_launches = 0;
+    std::string err;
+};
+
+namespace {
+
+fdtd_status batch_fail(fdtd_batch* b, fdtd_status st, const std::string& m) {
+    fdtd::set_error(nullptr, m);
+    if (b) b->err = m;
+    return st;
+}
+
+fdtd_status batch_cuda_fail(fdtd_batch* b, cudaError_t e, const char* what) {
+    return batch_fail(b, e == cudaErrorMemoryAllocation ? FDTD_ERR_OOM : FDTD_ERR_CUDA,
+                      std::string("CUDA: ") + cudaGetErrorString(e) + " at " + what);
+}
+
+}  // namespace
+
+#define BATCH_TRY(b, expr)                                             \
+    do {                                                               \
+        cudaError_t _e = (expr);                                       \
+        if (_e != cudaSuccess) return batch_cuda_fail((b), _e, #expr); \
+    } while (0)
+
+namespace {
+
+template <typename T>
+void fill_desc(BatchDesc<T>& d, fdtd_solver* s, bool active) {
+    std::memset(&d, 0, sizeof(d));
+    d.a[0] = make_kargs<T>(s->dP, s->hP, 0);
+    d.a[1] = make_kargs<T>(s->dP, s->hP, 1);
+    d.P = s->dP;
+    d.interior = s->region.interior;
+    d.src_region = s->region.src_region;
+    d.shell = s->shell;
+    d.ring = s->d_lis;
+    d.ring_cap = s->lis_cap_steps;
+    d.n_lis = s->L;
+    d.cur = s->cur;
+    d.active = active ? 1 : 0;
+    d.has_src = s->hP.n_src > 0 ? 1 : 0;
+    d.ghost_cap = s->region.ghost_cap;
+}
+
+template <typename T>
+size_t desc_bytes() {
+    return sizeof(BatchDesc<T>);
+}
+
+template <typename T>
+fdtd_status grow(fdtd_batch* b, T** ptr, size_t* cap, size_t need) {
+    if (need <= *cap) return FDTD_OK;
+    if (*ptr) cudaFree(*ptr);
+    *ptr = nullptr;
+    *cap = 0;
+    const size_t n = std::max<size_t>(need, 64);
+    BATCH_TRY(b, cudaMalloc((void**)ptr, n * sizeof(T)));
+    *cap = n;
+    return FDTD_OK;
+}
+
+// Rebuild descriptors and tile tables after a membership change.
+fdtd_status rebuild(fdtd_batch* b) {
+    const bool f64 = b->precision == FDTD_PRECISION_FP64;
+    const int xb = (b->opt.x_chunk == 2 || b->opt.x_chunk == 8) ? b->opt.x_chunk : 4;
+    const int xs = (b->opt.tile_y == 2) ? 2 : 1;
+    const size_t dsz = f64 ? desc_bytes<double>() : desc_bytes<float>();
+    const size_t nm = b->members.size();
+    std::vector<char> descs(std::max<size_t>(nm, 1) * dsz, 0);
+    std::vector<BatchTile> it, st;
+    std::vector<ListenerRef> refs;
+    int max_ghost = 0, max_src = 0;
+    for (size_t m = 0; m < nm; ++m) {
+        Member& mb = b->members[m];
+        if (!mb.s) continue;
+        if (mb.s->shell.xs != xs) build_shell_boxes(mb.s, xs);
+        mb.s->region.shell = mb.s->shell;
+        if (f64) fill_desc<double>(*reinterpret_cast<BatchDesc<double>*>(&descs[m * dsz]), mb.s, mb.active);
+        else fill_desc<float>(*reinterpret_cast<BatchDesc<float>*>(&descs[m * dsz]), mb.s, mb.active);
+        if (!mb.active) continue;
+        const Box3& I = mb.s->region.interior;
+        const int nx = I.hi[0] - I.lo[0], ny = I.hi[1] - I.lo[1], nz = I.hi[2] - I.lo[2];
+        if (nx > 0 && ny > 0 && nz > 0) {
+            const int tz = (nz + 31) / 32, ty = (ny + 7) / 8, tx = (nx + xb - 1) / xb;
+            for (int x = 0; x < tx; ++x)
+                for (int y = 0; y < ty; ++y)
+                    for (int z = 0; z < tz; ++z) it.push_back({(int)m, 0, z, y, x});
+        }
+        const ShellBoxes& B = mb.s->shell;
+        for (int bx = 0; bx < B.n; ++bx)
+            for (int x = 0; x < B.tx[bx]; ++x)
+                for (int y = 0; y < B.ty[bx]; ++y)
+                    for (int z = 0; z < B.tz[bx]; ++z) st.push_back({(int)m, bx, z, y, x});
+        for (int li = 0; li < mb.s->L; ++li) refs.push_back({(int)m, li});
+        max_ghost = std::max(max_ghost, (mb.s->region.ghost_cap + 127) / 128);
+        if (mb.s->hP.n_src > 0) {
+            const Box3& r = mb.s->region.src_region;
+            const long long cells = (long long)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);
+            max_src = std::max<int>(max_src, (int)std::min<long long>((cells + 255) / 256, 64));
+        }
+    }
+    fdtd_status st_ = FDTD_OK;
+    char* dd = static_cast<char*>(b->d_descs);
+    if (b->desc_cap < descs.size()) {
+        if (b->d_descs) cudaFree(b->d_descs);
+        b->d_descs = nullptr;
+        b->desc_cap = 0;
+        BATCH_TRY(b, cudaMalloc(&b->d_descs, descs.size() * 2));
+        b->desc_cap = descs.size() * 2;
+        dd = static_cast<char*>(b->d_descs);
+    }
+    if ((st_ = grow(b, &b->d_int, &b->int_cap, it.size())) != FDTD_OK) return st_;
+    if ((st_ = grow(b, &b->d_shell, &b->shell_cap, st.size())) != FDTD_OK) return st_;
+    if ((st_ = grow(b, &b->d_refs, &b->refs_cap, refs.size())) != FDTD_OK) return st_;
+    BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+    BATCH_TRY(b, cudaMemcpy(dd, descs.data(), descs.size(), cudaMemcpyHostToDevice));
+    if (!it.empty()) BATCH_TRY(b, cudaMemcpy(b->d_int, it.data(), it.size() * sizeof(BatchTile), cudaMemcpyHostToDevice));
+    if (!st.empty()) BATCH_TRY(b, cudaMemcpy(b->d_shell, st.data(), st.size() * sizeof(BatchTile), cudaMemcpyHostToDevice));
+    if (!refs.empty())
+        BATCH_TRY(b, cudaMemcpy(b->d_refs, refs.data(), refs.size() * sizeof(ListenerRef), cudaMemcpyHostToDevice));
+    BatchLaunch& L = b->L;
+    L.descs = b->d_descs;
+    L.int_tiles = b->d_int;
+    L.n_int = (int)it.size();
+    L.shell_tiles = b->d_shell;
+    L.n_shell = (int)st.size();
+    L.refs = b->d_refs;
+    L.n_refs = (int)refs.size();
+    L.n_members = (int)nm;
+    L.xb = xb;
+    L.xs = xs;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->opt.device);
+    const int occ_i = batch_blocks_per_sm(b->precision, 0, xb);
+    const int occ_s = batch_blocks_per_sm(b->precision, 1, xs);
+    L.ctas_int = b->opt.persistent_ctas > 0 ? b->opt.persistent_ctas : sms * occ_i;
+    L.ctas_shell = b->opt.persistent_ctas > 0 ? b->opt.persistent_ctas : sms * occ_s;
+    L.ctas_int = std::max(1, std::min(L.ctas_int, std::max(1, L.n_int)));
+    L.ctas_shell = std::max(1, std::min(L.ctas_shell, std::max(1, L.n_shell)));
+    L.ghost_blocks = std::min(max_ghost, 32);
+    L.src_blocks = max_src;
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    b->dirty = false;
+    return FDTD_OK;
+}
+
+fdtd_status enqueue(fdtd_batch* b) {
+    int l = 0;
+    cudaError_t e = b->precision == FDTD_PRECISION_FP64
+                        ? launch_batch_fp64(b->L, b->stream, b->stream2, b->ev_fork, b->ev_join, &l)
+                        : launch_batch_fp32(b->L, b->stream, b->stream2, b->ev_fork, b->ev_join, &l);
+    if (e == cudaSuccess) e = launch_batch_tail_any(b->precision, b->L, b->stream, &l);
+    b->launches += l;
+    if (e != cudaSuccess) return batch_fail(b, FDTD_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+    return FDTD_OK;
+}
+
+fdtd_status capture(fdtd_batch* b, int n) {
+    cudaGraph_t g = nullptr;
+    BATCH_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    const long long l0 = b->launches;
+    fdtd_status st = FDTD_OK;
+    for (int i = 0; i < n && st == FDTD_OK; ++i) st = enqueue(b);
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    b->graph_launches = b->launches - l0;
+    b->launches = l0;
+    if (st != FDTD_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return batch_fail(b, FDTD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return batch_fail(b, FDTD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+    return FDTD_OK;
+}
+
+// Copy listener rows of steps [first, first+count) of a member from its ring.
+fdtd_status collect_rows(fdtd_batch* b, Member& mb, int64_t first, int64_t count) {
+    if (mb.L == 0 || count <= 0) return FDTD_OK;
+    const int cap = mb.s->lis_cap_steps;
+    const size_t old = mb.rows.size();
+    mb.rows.resize(old + (size_t)count * mb.L);
+    int64_t k = 0;
+    while (k < count) {
+        const int64_t pos = (first + k) % cap;
+        const int64_t run = std::min<int64_t>(count - k, cap - pos);
+        BATCH_TRY(b, cudaMemcpyAsync(mb.rows.data() + old + (size_t)k * mb.L, mb.s->d_lis + (size_t)pos * mb.L,
+                                     (size_t)run * mb.L * sizeof(double), cudaMemcpyDeviceToHost, b->stream));
+        k += run;
+    }
+    return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fdtd_status fdtd_batch_create(int32_t n, const fdtd_scene_desc* scenes, const int32_t* steps,
+                              const fdtd_options* options, fdtd_batch** out) {
+    if (!out || n < 0 || (n > 0 && (!scenes || !steps)))
+        return batch_fail(nullptr, FDTD_ERR_INVALID_ARG, "fdtd_batch_create: invalid arguments");
+    *out = nullptr;
+    std::unique_ptr<fdtd_batch> b(new fdtd_batch());
+    if (options) b->opt = *options;
+    if (b->opt.kernel != FDTD_KERNEL_FUSED)
+        return batch_fail(nullptr, FDTD_ERR_INVALID_ARG, "batches use the fused kernel path");
+    if (b->opt.graph_steps < 0 || (b->opt.graph_steps % 2) != 0 || b->opt.graph_steps > 256)
+        return batch_fail(nullptr, FDTD_ERR_INVALID_ARG, "graph_steps must be an even number in [0, 256]");
+    b->precision = b->opt.precision;
+    BATCH_TRY(nullptr, cudaSetDevice(b->opt.device));
+    BATCH_TRY(nullptr, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    BATCH_TRY(nullptr, cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking));
+    BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
+    BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+    for (int i = 0; i < n; ++i) {
+        int32_t id;
+        fdtd_status st = fdtd_batch_add(b.get(), &scenes[i], steps[i], &id);
+        if (st != FDTD_OK) {
+            fdtd_batch_destroy(b.release());
+            return st;
+        }
+    }
+    *out = b.release();
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_batch_add(fdtd_batch* b, const fdtd_scene_desc* scene, int32_t steps, int32_t* member) {
+    if (!b || !scene || steps < 0) return batch_fail(b, FDTD_ERR_INVALID_ARG, "fdtd_batch_add: invalid arguments");
+    fdtd_options o = b->opt;
+    o.graph_steps = 0;
+    fdtd_solver* s = nullptr;
+    fdtd_status st = fdtd_solver_create(scene, &o, &s);
+    if (st != FDTD_OK) return batch_fail(b, st, fdtd_last_error());
+    if (s->moving) {
+        fdtd_solver_destroy(s);
+        return batch_fail(b, FDTD_ERR_UNSUPPORTED, "moving bodies are stepped by fdtd_solver, not in batches");
+    }
+    Member mb;
+    mb.s = s;
+    mb.total = steps;
+    mb.L = s->L;
+    if (steps > 0) {
+        // the first step classifies the cells (MAC_Grid::classifyCells_FAST)
+        mb.rows.resize(mb.L);
+        st = fdtd_solver_step(s, 1, mb.L ? mb.rows.data() : nullptr);
+        if (st < 0) {
+            std::string m = fdtd_solver_last_error(s);
+            fdtd_solver_destroy(s);
+            return batch_fail(b, st, m);
+        }
+        mb.done = 1;
+    }
+    mb.active = mb.done < mb.total;
+    size_t slot = b->members.size();
+    for (size_t i = 0; i < b->members.size(); ++i)
+        if (b->members[i].released) {
+            slot = i;
+            break;
+        }
+    if (slot == b->members.size()) b->members.push_back(std::move(mb));
+    else b->members[slot] = std::move(mb);
+    b->dirty = true;
+    if (member) *member = (int32_t)slot;
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_batch_step(fdtd_batch* b, int32_t n_steps, int32_t* n_active) {
+    if (!b || n_steps < 0) return batch_fail(b, FDTD_ERR_INVALID_ARG, "fdtd_batch_step: invalid arguments");
+    BATCH_TRY(b, cudaSetDevice(b->opt.device));
+    const long long l0 = b->launches;
+    int64_t left = n_steps;
+    const int G = b->opt.graph_steps;
+    while (left > 0) {
+        int64_t chunk = left;
+        bool any = false;
+        for (auto& mb : b->members)
+            if (mb.active) {
+                any = true;
+                chunk = std::min(chunk, mb.total - mb.done);
+                chunk = std::min<int64_t>(chunk, mb.s->lis_cap_steps);
+            }
+        if (!any) break;
+        if (b->dirty) {
+            fdtd_status st = rebuild(b);
+            if (st != FDTD_OK) return st;
+        }
+        if (G > 0 && chunk >= G) {
+            chunk = (chunk / G) * G;
+            if (!b->graph) {
+                fdtd_status st = capture(b, G);
+                if (st != FDTD_OK) return st;
+            }
+            for (int64_t i = 0; i < chunk / G; ++i) {
+                BATCH_TRY(b, cudaGraphLaunch(b->graph, b->stream));
+                b->launches += b->graph_launches;
+            }
+        } else {
+            for (int64_t i = 0; i < chunk; ++i) {
+                fdtd_status st = enqueue(b);
+                if (st != FDTD_OK) return st;
+            }
+        }
+        // rows, host mirrors, retirement
+        std::vector<int> errs(b->members.size(), 0);
+        for (size_t m = 0; m < b->members.size(); ++m) {
+            Member& mb = b->members[m];
+            if (!mb.active) continue;
+            fdtd_status st = collect_rows(b, mb, mb.done, chunk);
+            if (st != FDTD_OK) return st;
+            BATCH_TRY(b, cudaMemcpyAsync(&errs[m], mb.s->hP.dev_error, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+        }
+        BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+        for (size_t m = 0; m < b->members.size(); ++m) {
+            Member& mb = b->members[m];
+            if (!mb.active) continue;
+            fdtd_solver* s = mb.s;
+            s->cur ^= (int)(chunk & 1);
+            s->step_index += chunk;
+            for (int64_t i = 0; i < chunk; ++i) s->time += s->k;
+            mb.done += chunk;
+            if (errs[m] & 1) mb.status = FDTD_ERR_NUMERIC;
+            if (mb.done >= mb.total) {
+                mb.active = false;
+                b->dirty = true;
+            }
+        }
+        left -= chunk;
+    }
+    b->last_launches = b->launches - l0;
+    if (n_active) {
+        int a = 0;
+        for (auto& mb : b->members) a += mb.active ? 1 : 0;
+        *n_active = a;
+    }
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_batch_run(fdtd_batch* b) {
+    if (!b) return FDTD_ERR_INVALID_ARG;
+    int32_t active = 1;
+    while (active > 0) {
+        fdtd_status st = fdtd_batch_step(b, 1 << 20, &active);
+        if (st != FDTD_OK) return st;
+    }
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_batch_member_info(fdtd_batch* b, int32_t member, int64_t* steps_done, int64_t* steps_total,
+                                   int32_t* n_listeners, int32_t* status) {
+    if (!b || member < 0 || member >= (int32_t)b->members.size() || b->members[member].released)
+        return batch_fail(b, FDTD_ERR_INVALID_ARG, "no such member (out of range or released)");
+    const Member& mb = b->members[member];
+    if (steps_done) *steps_done = mb.done;
+    if (steps_total) *steps_total = mb.total;
+    if (n_listeners) *n_listeners = mb.L;
+    if (status) *status = mb.status;
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_batch_output(fdtd_batch* b, int32_t member, double* out, int64_t count) {
+    if (!b || member < 0 || member >= (int32_t)b->members.size() || b->members[member].released)
+        return batch_fail(b, FDTD_ERR_INVALID_ARG, "no such member (out of range or released)");
+    const Member& mb = b->members[member];
+    if (count < (int64_t)mb.rows.size() || (!out && !mb.rows.empty()))
+        return batch_fail(b, FDTD_ERR_INVALID_ARG, "output buffer smaller than steps_done * n_listeners");
+    if (!mb.rows.empty()) std::memcpy(out, mb.rows.data(), mb.rows.size() * sizeof(double));
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_batch_release(fdtd_batch* b, int32_t member) {
+    if (!b || member < 0 || member >= (int32_t)b->members.size())
+        return batch_fail(b, FDTD_ERR_INVALID_ARG, "member index out of range");
+    Member& mb = b->members[member];
+    if (mb.released) return FDTD_OK;
+    if (mb.active) return batch_fail(b, FDTD_ERR_BUSY, "member still running");
+    if (mb.s) {
+        BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+        fdtd_solver_destroy(mb.s);
+        mb.s = nullptr;
+    }
+    mb = Member();
+    mb.released = true;
+    b->dirty = true;
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_batch_destroy(fdtd_batch* b) {
+    if (!b) return FDTD_OK;
+    cudaSetDevice(b->opt.device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (auto& mb : b->members)
+        if (mb.s) fdtd_solver_destroy(mb.s);
+    if (b->d_descs) cudaFree(b->d_descs);
+    if (b->d_int) cudaFree(b->d_int);
+    if (b->d_shell) cudaFree(b->d_shell);
+    if (b->d_refs) cudaFree(b->d_refs);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->stream2) cudaStreamDestroy(b->stream2);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return FDTD_OK;
+}
+
+void* fdtd_batch_stream(fdtd_batch* b) { return b ? (void*)b->stream : nullptr; }
+int64_t fdtd_batch_last_launch_count(fdtd_batch* b) { return b ? b->last_launches : 0; }
+
+int64_t fdtd_batch_device_bytes(fdtd_batch* b) {
+    if (!b) return 0;
+    int64_t t = 0;
+    for (auto& mb : b->members)
+        if (mb.s) t += (int64_t)mb.s->arena_bytes;
+    return t;
+}
+
+}  // extern "C"

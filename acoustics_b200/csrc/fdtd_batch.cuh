@@ -1,0 +1,173 @@
+// fdtd_batch.cuh — one step of many independent solves of uneven sizes in a
+// fixed number of launches, whatever the number of solves.
+//
+// Every member keeps its own device state (the arrays of its fdtd_solver); a
+// descriptor per member holds its kernel arguments for both buffer parities,
+// its boxes, its listener ring and its current parity, which the last kernel
+// of a step flips on the device.  Because parity and step constants live on
+// the device, a captured graph of N batched steps replays for any step index.
+//
+// Per step:  k_batch_shell (PML tiles of all members)  ||  k_batch_interior ->
+//            k_batch_ghost  (second stream), then k_batch_sources (launch_batch),
+//            k_batch_listeners, k_batch_advance (launch_batch_tail).
+// The shell and interior kernels are persistent: gridDim CTAs each take one
+// contiguous range of a tile table sorted by member, reload the member's
+// arguments into shared memory only when the member changes, and call the
+// same tile functions as the single-solve kernels.
+#pragma once
+#include "fdtd_device.cuh"
+#include "fdtd_hot.cuh"
+#include "fdtd_listeners.cuh"
+#include "fdtd_region.cuh"
+
+namespace fdtd {
+
+template <typename T, int XB>
+__global__ void __launch_bounds__(256) k_batch_interior(const BatchDesc<T>* __restrict__ D,
+                                                        const BatchTile* __restrict__ tiles, int n) {
+    __shared__ KArgs<T> sA;
+    __shared__ Box3 sBox;
+    const int per = (n + gridDim.x - 1) / gridDim.x;
+    const int t0 = blockIdx.x * per;
+    const int t1 = min(n, t0 + per);
+    int prev = -1;
+    for (int t = t0; t < t1; ++t) {
+        const BatchTile tile = tiles[t];
+        if (tile.m != prev) {
+            __syncthreads();
+            if (threadIdx.x == 0 && threadIdx.y == 0) {
+                const BatchDesc<T>& d = D[tile.m];
+                sA = d.a[d.cur];
+                sBox = d.interior;
+            }
+            __syncthreads();
+            prev = tile.m;
+        }
+        interior_tile<T, XB>(sA, sBox, tile.tz, tile.ty, tile.tx);
+    }
+}
+
+template <typename T, int XS>
+__global__ void __launch_bounds__(256, FDTD_SHELL_MINB) k_batch_shell(const BatchDesc<T>* __restrict__ D,
+                                                                      const BatchTile* __restrict__ tiles, int n) {
+    __shared__ KArgs<T> sA;
+    __shared__ ShellBoxes sB;
+    const int per = (n + gridDim.x - 1) / gridDim.x;
+    const int t0 = blockIdx.x * per;
+    const int t1 = min(n, t0 + per);
+    int prev = -1;
+    for (int t = t0; t < t1; ++t) {
+        const BatchTile tile = tiles[t];
+        if (tile.m != prev) {
+            __syncthreads();
+            if (threadIdx.x == 0 && threadIdx.y == 0) {
+                const BatchDesc<T>& d = D[tile.m];
+                sA = d.a[d.cur];
+                sB = d.shell;
+            }
+            __syncthreads();
+            prev = tile.m;
+        }
+        shell_tile<T, XS>(sA, sB, tile.box, tile.tz, tile.ty, tile.tx);
+    }
+}
+
+// grid (ghost_blocks, members)
+template <typename T>
+__global__ void __launch_bounds__(128) k_batch_ghost(const BatchDesc<T>* __restrict__ D) {
+    const BatchDesc<T>& d = D[blockIdx.y];
+    if (!d.active || d.ghost_cap == 0) return;
+    ghost_cells_body<T>(*d.P, d.cur, blockIdx.x, gridDim.x);
+}
+
+// grid (src_blocks, members)
+template <typename T>
+__global__ void __launch_bounds__(256) k_batch_sources(const BatchDesc<T>* __restrict__ D) {
+    const BatchDesc<T>& d = D[blockIdx.y];
+    if (!d.active || !d.has_src) return;
+    // a source whose time factor underflowed to zero adds nothing (the single-solve
+    // path skips the launch then); the whole block leaves together
+    const StepConsts& c = d.P->consts[d.cur];
+    bool any = false;
+    for (int s = 0; s < d.P->n_src; ++s) any |= c.src_tf[s] != 0.0;
+    if (!any) return;
+    sources_body<T>(*d.P, d.cur, d.src_region, blockIdx.x, gridDim.x);
+}
+
+// one warp per (member, listener)
+template <typename T>
+__global__ void __launch_bounds__(128) k_batch_listeners(const BatchDesc<T>* __restrict__ D,
+                                                         const ListenerRef* __restrict__ refs, int n) {
+    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (w >= n) return;
+    const ListenerRef r = refs[w];
+    const BatchDesc<T>& d = D[r.m];
+    if (!d.active) return;
+    const long long step = d.P->consts[d.cur].step;
+    double* row = d.ring + (size_t)(step % d.ring_cap) * d.n_lis;
+    listener_body<T>(*d.P, d.cur ^ 1, r.li, row);
+}
+
+// end of step: advance every active member's constants and flip its parity
+template <typename T>
+__global__ void k_batch_advance(BatchDesc<T>* __restrict__ D, int n) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n || !D[m].active) return;
+    advance_consts(*D[m].P, D[m].cur);
+    D[m].cur ^= 1;
+}
+
+template <typename T>
+cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, cudaEvent_t fork,
+                         cudaEvent_t join, int* launches) {
+    BatchDesc<T>* D = static_cast<BatchDesc<T>*>(L.descs);
+    int l = 0;
+    cudaError_t e = cudaEventRecord(fork, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, fork, 0);
+    if (e != cudaSuccess) return e;
+    if (L.n_int > 0) {
+        const dim3 block(32, 8);
+        if (L.xb == 2) k_batch_interior<T, 2><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int);
+        else if (L.xb == 8) k_batch_interior<T, 8><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int);
+        else k_batch_interior<T, 4><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int);
+        ++l;
+    }
+    if (L.ghost_blocks > 0) {
+        k_batch_ghost<T><<<dim3(L.ghost_blocks, L.n_members), 128, 0, s2>>>(D);
+        ++l;
+    }
+    if (L.n_shell > 0) {
+        if (L.xs == 2) k_batch_shell<T, 2><<<L.ctas_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles, L.n_shell);
+        else k_batch_shell<T, 1><<<L.ctas_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles, L.n_shell);
+        ++l;
+    }
+    e = cudaEventRecord(join, s2);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
+    if (e != cudaSuccess) return e;
+    if (L.src_blocks > 0) {
+        k_batch_sources<T><<<dim3(L.src_blocks, L.n_members), 256, 0, s>>>(D);
+        ++l;
+    }
+    if (launches) *launches += l;
+    return cudaGetLastError();
+}
+
+// Listener rows and the end-of-step advance.  Instantiated in the FP64
+// translation unit for both field types, like the single-solve listener
+// kernel, so the double-precision MLS arithmetic is compiled the same way
+// (no FMA contraction) and batch rows equal single-solve rows bit for bit.
+template <typename T>
+cudaError_t launch_batch_tail(const BatchLaunch& L, cudaStream_t s, int* launches) {
+    BatchDesc<T>* D = static_cast<BatchDesc<T>*>(L.descs);
+    int l = 0;
+    if (L.n_refs > 0) {
+        k_batch_listeners<T><<<(L.n_refs * 32 + 127) / 128, 128, 0, s>>>(D, L.refs, L.n_refs);
+        ++l;
+    }
+    k_batch_advance<T><<<(L.n_members + 127) / 128, 128, 0, s>>>(D, L.n_members);
+    ++l;
+    if (launches) *launches += l;
+    return cudaGetLastError();
+}
+
+}  // namespace fdtd

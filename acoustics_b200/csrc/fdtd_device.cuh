@@ -15,6 +15,7 @@
 // (MAC_Grid.cpp:2495-2523, :2653-2677): every coefficient depends on one
 // coordinate only.
 #pragma once
+#include <cmath>
 #include <cstdint>
 
 #ifndef FDTD_MAX_OBJECTS
@@ -162,6 +163,101 @@ struct SolveParams {
     int* ghost_count;
     int ghost_cap;
     int precision;                // 0 fp64, 1 fp32 compensated
+};
+
+template <typename T>
+KArgs<T> make_kargs(SolveParams* dP, const SolveParams& P, int cur);
+
+template <>
+inline KArgs<double> make_kargs<double>(SolveParams* dP, const SolveParams& P, int cur) {
+    KArgs<double> A;
+    A.P = dP;
+    A.cur = cur;
+    A.advance = 1;
+    A.N0 = P.N[0]; A.N1 = P.N[1]; A.N2 = P.N[2];
+    A.sx = (unsigned)P.N[1] * P.N[2];
+    A.pc = (const double*)P.p[cur];
+    A.pn = (double*)P.p[cur ^ 1];
+    A.dinc = P.dinc;
+    A.cls = P.cls;
+    for (int d = 0; d < 3; ++d) {
+        A.pd[d] = (double*)P.pd[d];
+        A.vo[d] = (const double*)P.v[cur][d];
+        A.vn[d] = (double*)P.v[cur ^ 1][d];
+        A.pml_cell[d] = P.pml_cell[d];
+        A.pml_face[d] = P.pml_face[d];
+        A.pupd[d] = P.pupd[d]; A.pdiv[d] = P.pdiv[d]; A.vupd[d] = P.vupd[d]; A.vgrad[d] = P.vgrad[d];
+    }
+    A.inv_h = P.inv_h; A.c2k2 = P.c2k2; A.lap_scale = P.lap_scale;
+    return A;
+}
+
+template <>
+inline KArgs<float> make_kargs<float>(SolveParams* dP, const SolveParams& P, int cur) {
+    KArgs<float> A;
+    A.P = dP;
+    A.cur = cur;
+    A.advance = 1;
+    A.N0 = P.N[0]; A.N1 = P.N[1]; A.N2 = P.N[2];
+    A.sx = (unsigned)P.N[1] * P.N[2];
+    A.pc = (const float*)P.p[cur];
+    A.pn = (float*)P.p[cur ^ 1];
+    A.dinc = P.dinc;
+    A.cls = P.cls;
+    for (int d = 0; d < 3; ++d) {
+        A.pd[d] = (float*)P.pd[d];
+        A.vo[d] = (const float*)P.v[cur][d];
+        A.vn[d] = (float*)P.v[cur ^ 1][d];
+        A.pml_cell[d] = P.pml_cell[d];
+        A.pml_face[d] = P.pml_face[d];
+        A.pupd[d] = P.pupd_f[d]; A.pdiv[d] = P.pdiv_f[d]; A.vupd[d] = P.vupd_f[d]; A.vgrad[d] = P.vgrad_f[d];
+    }
+    A.inv_h = (float)P.inv_h; A.c2k2 = (float)P.c2k2; A.lap_scale = (float)P.lap_scale;
+    return A;
+}
+
+
+// ---- batches of independent solves (fdtd_batch.cuh, fdtd_batch.cpp) ----
+
+template <typename T>
+struct BatchDesc {
+    KArgs<T> a[2];       // kernel arguments by parity
+    SolveParams* P;      // the member's device parameters
+    Box3 interior;
+    Box3 src_region;
+    ShellBoxes shell;
+    double* ring;        // listener rows: row (step % ring_cap) of n_lis doubles
+    int ring_cap;
+    int n_lis;
+    int cur;             // buffer parity of the member's next step
+    int active;
+    int has_src;
+    int ghost_cap;
+};
+
+struct BatchTile {
+    int m;       // member
+    int box;     // shell box (shell tiles)
+    int tz, ty, tx;
+};
+
+struct ListenerRef {
+    int m, li;
+};
+
+struct BatchLaunch {
+    void* descs;                 // BatchDesc<T>[n_members] on the device
+    const BatchTile* int_tiles;
+    int n_int;
+    const BatchTile* shell_tiles;
+    int n_shell;
+    const ListenerRef* refs;
+    int n_refs;
+    int n_members;
+    int xb, xs;
+    int ctas_int, ctas_shell;    // persistent grid sizes
+    int ghost_blocks;            // per member
+    int src_blocks;              // per member (0: no member has a source)
 };
 
 // consts[cur^1] <- the next step's constants (PML_WaveSolver.cpp:825,

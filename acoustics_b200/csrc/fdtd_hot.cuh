@@ -34,13 +34,16 @@
 
 namespace fdtd {
 
+// One interior tile: 32 z x 8 y columns, XB x planes, starting at tile
+// coordinates (tz, ty, tx) of the box.  Every thread of the CTA must call it
+// (z neighbours are exchanged by warp shuffles).
 template <typename T, int XB>
-__global__ void __launch_bounds__(256) k_interior(const KArgs<T> A, Box3 box) {
+__device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box, int tz, int ty, int tx) {
     constexpr bool COMP = sizeof(T) == 4;
     const int lane = threadIdx.x;
-    const int z = box.lo[2] + blockIdx.x * 32 + lane;
-    const int y = box.lo[1] + blockIdx.y * 8 + threadIdx.y;
-    const int x0 = box.lo[0] + blockIdx.z * XB;
+    const int z = box.lo[2] + tz * 32 + lane;
+    const int y = box.lo[1] + ty * 8 + threadIdx.y;
+    const int x0 = box.lo[0] + tx * XB;
     const bool active = (z < box.hi[2]) && (y < box.hi[1]);
     const int zc = min(z, box.hi[2] - 1);
     const int yc = min(y, box.hi[1] - 1);
@@ -95,20 +98,14 @@ __global__ void __launch_bounds__(256) k_interior(const KArgs<T> A, Box3 box) {
     }
 }
 
+template <typename T, int XB>
+__global__ void __launch_bounds__(256) k_interior(const KArgs<T> A, Box3 box) {
+    interior_tile<T, XB>(A, box, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+// One PML-shell tile of box b at tile coordinates (tz, ty, tx).
 template <typename T, int XS>
-__global__ void __launch_bounds__(256, FDTD_SHELL_MINB) k_pml_shell(const KArgs<T> A, const ShellBoxes B) {
-    if (A.advance && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) advance_consts(*A.P, A.cur);
-    // ---- CTA -> (box, tile) ----
-    const int blk = blockIdx.x;
-    int b = 0;
-#pragma unroll
-    for (int q = 1; q < 5; ++q)
-        if (q < B.n && blk >= B.block_first[q]) b = q;
-    int local = blk - B.block_first[b];
-    const int tz = local % B.tz[b];
-    local /= B.tz[b];
-    const int ty = local % B.ty[b];
-    const int tx = local / B.ty[b];
+__device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& B, int b, int tz, int ty, int tx) {
     const int zz = tz * 32 + threadIdx.x;
     const int yy = ty * 8 + threadIdx.y;
     if (zz >= B.nz[b] || yy >= B.ny[b]) return;
@@ -186,55 +183,25 @@ __global__ void __launch_bounds__(256, FDTD_SHELL_MINB) k_pml_shell(const KArgs<
     }
 }
 
-template <typename T>
-KArgs<T> make_kargs(SolveParams* dP, const SolveParams& P, int cur);
-
-template <>
-inline KArgs<double> make_kargs<double>(SolveParams* dP, const SolveParams& P, int cur) {
-    KArgs<double> A;
-    A.P = dP;
-    A.cur = cur;
-    A.advance = 1;
-    A.N0 = P.N[0]; A.N1 = P.N[1]; A.N2 = P.N[2];
-    A.sx = (unsigned)P.N[1] * P.N[2];
-    A.pc = (const double*)P.p[cur];
-    A.pn = (double*)P.p[cur ^ 1];
-    A.dinc = P.dinc;
-    A.cls = P.cls;
-    for (int d = 0; d < 3; ++d) {
-        A.pd[d] = (double*)P.pd[d];
-        A.vo[d] = (const double*)P.v[cur][d];
-        A.vn[d] = (double*)P.v[cur ^ 1][d];
-        A.pml_cell[d] = P.pml_cell[d];
-        A.pml_face[d] = P.pml_face[d];
-        A.pupd[d] = P.pupd[d]; A.pdiv[d] = P.pdiv[d]; A.vupd[d] = P.vupd[d]; A.vgrad[d] = P.vgrad[d];
-    }
-    A.inv_h = P.inv_h; A.c2k2 = P.c2k2; A.lap_scale = P.lap_scale;
-    return A;
+// CTA -> (box, tile) through the prefix table of the shell boxes
+__device__ __forceinline__ void shell_decode(const ShellBoxes& B, int blk, int& b, int& tz, int& ty, int& tx) {
+    b = 0;
+#pragma unroll
+    for (int q = 1; q < 5; ++q)
+        if (q < B.n && blk >= B.block_first[q]) b = q;
+    int local = blk - B.block_first[b];
+    tz = local % B.tz[b];
+    local /= B.tz[b];
+    ty = local % B.ty[b];
+    tx = local / B.ty[b];
 }
 
-template <>
-inline KArgs<float> make_kargs<float>(SolveParams* dP, const SolveParams& P, int cur) {
-    KArgs<float> A;
-    A.P = dP;
-    A.cur = cur;
-    A.advance = 1;
-    A.N0 = P.N[0]; A.N1 = P.N[1]; A.N2 = P.N[2];
-    A.sx = (unsigned)P.N[1] * P.N[2];
-    A.pc = (const float*)P.p[cur];
-    A.pn = (float*)P.p[cur ^ 1];
-    A.dinc = P.dinc;
-    A.cls = P.cls;
-    for (int d = 0; d < 3; ++d) {
-        A.pd[d] = (float*)P.pd[d];
-        A.vo[d] = (const float*)P.v[cur][d];
-        A.vn[d] = (float*)P.v[cur ^ 1][d];
-        A.pml_cell[d] = P.pml_cell[d];
-        A.pml_face[d] = P.pml_face[d];
-        A.pupd[d] = P.pupd_f[d]; A.pdiv[d] = P.pdiv_f[d]; A.vupd[d] = P.vupd_f[d]; A.vgrad[d] = P.vgrad_f[d];
-    }
-    A.inv_h = (float)P.inv_h; A.c2k2 = (float)P.c2k2; A.lap_scale = (float)P.lap_scale;
-    return A;
+template <typename T, int XS>
+__global__ void __launch_bounds__(256, FDTD_SHELL_MINB) k_pml_shell(const KArgs<T> A, const ShellBoxes B) {
+    if (A.advance && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) advance_consts(*A.P, A.cur);
+    int b, tz, ty, tx;
+    shell_decode(B, blockIdx.x, b, tz, ty, tx);
+    shell_tile<T, XS>(A, B, b, tz, ty, tx);
 }
 
 // Host side: one region-split step.  The shell kernel runs on s, the interior

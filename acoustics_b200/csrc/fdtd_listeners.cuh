@@ -58,13 +58,10 @@ __device__ void build_row(const SolveParams& P, const T* __restrict__ pold, doub
     mls_row(pt, fp, pg, A, b);
 }
 
+// Listener li of solve P into out_row[li]; called by a whole warp.
 template <typename T>
-__global__ void __launch_bounds__(128) k_listeners_warp(const SolveParams* __restrict__ Pp, int newp,
-                                                        double* __restrict__ out_row) {
-    const SolveParams& P = *Pp;
+__device__ void listener_body(const SolveParams& P, int newp, int li, double* __restrict__ out_row) {
     const int lane = threadIdx.x & 31;
-    const int li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (li >= P.n_lis) return;  // the whole warp leaves together
     const T* __restrict__ pnew = (const T*)P.p[newp];
     const T* __restrict__ pold = (const T*)P.p[newp ^ 1];
     const double t = P.consts[newp ^ 1].t;
@@ -192,6 +189,14 @@ __global__ void __launch_bounds__(128) k_listeners_warp(const SolveParams* __res
     }
     out_row[li] = ok ? x[0] : 0.0;
     if (!ok) atomicOr(P.dev_error, 1);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_listeners_warp(const SolveParams* __restrict__ Pp, int newp,
+                                                        double* __restrict__ out_row) {
+    const int li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (li >= Pp->n_lis) return;  // the whole warp leaves together
+    listener_body<T>(*Pp, newp, li, out_row);
 }
 
 }  // namespace fdtd

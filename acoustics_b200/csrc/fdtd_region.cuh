@@ -72,15 +72,14 @@ __device__ __noinline__ T ghost_laplacian(const SolveParams& P, long long c, con
 // k_sources afterwards, as the reference adds them after the update
 // (MAC_Grid.cpp:938-944).
 template <typename T>
-__global__ void __launch_bounds__(128) k_ghost_cells(const SolveParams* __restrict__ Pp, int cur) {
-    const SolveParams& P = *Pp;
+__device__ __forceinline__ void ghost_cells_body(const SolveParams& P, int cur, int bid, int nblocks) {
     const int n = *P.ghost_count;
     const int Ny = P.N[1], Nz = P.N[2];
     const long long sx = (long long)Ny * Nz;
     const T* __restrict__ pc = (const T*)P.p[cur];
     T* __restrict__ pn = (T*)P.p[cur ^ 1];
     const double t = P.consts[cur].t;
-    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < n && g < P.ghost_cap; g += gridDim.x * blockDim.x) {
+    for (int g = bid * blockDim.x + threadIdx.x; g < n && g < P.ghost_cap; g += nblocks * blockDim.x) {
         const long long c = P.ghost_list[g];
         const int x = (int)(c / sx), y = (int)((c / Nz) % Ny), z = (int)(c % Nz);
         const uint8_t code = P.cls[c];
@@ -105,8 +104,7 @@ __global__ void __launch_bounds__(128) k_ghost_cells(const SolveParams* __restri
 // pNext += k * sum_s G_s(x, t + k/2) over the bounding box of the source
 // supports clipped to the non-PML box (GaussianPressureSource.cpp:6-30).
 template <typename T>
-__global__ void __launch_bounds__(256) k_sources(const SolveParams* __restrict__ Pp, int cur, Box3 region) {
-    const SolveParams& P = *Pp;
+__device__ __forceinline__ void sources_body(const SolveParams& P, int cur, const Box3& region, int bid, int nblocks) {
     const StepConsts& sc = P.consts[cur];
     bool any_src = false;
     for (int s = 0; s < P.n_src; ++s) any_src |= (sc.src_tf[s] != 0.0);
@@ -116,7 +114,7 @@ __global__ void __launch_bounds__(256) k_sources(const SolveParams* __restrict__
     const int Ny = P.N[1], Nz = P.N[2];
     const T* __restrict__ pc = (const T*)P.p[cur];
     T* __restrict__ pn = (T*)P.p[cur ^ 1];
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)gridDim.x * blockDim.x) {
+    for (long long t = bid * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)nblocks * blockDim.x) {
         const int z = region.lo[2] + (int)(t % nz);
         const int y = region.lo[1] + (int)((t / nz) % ny);
         const int x = region.lo[0] + (int)(t / ((long long)nz * ny));
@@ -131,6 +129,16 @@ __global__ void __launch_bounds__(256) k_sources(const SolveParams* __restrict__
             pn[c] = pc[c] + d;
         }
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(128) k_ghost_cells(const SolveParams* __restrict__ Pp, int cur) {
+    ghost_cells_body<T>(*Pp, cur, blockIdx.x, gridDim.x);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_sources(const SolveParams* __restrict__ Pp, int cur, Box3 region) {
+    sources_body<T>(*Pp, cur, region, blockIdx.x, gridDim.x);
 }
 
 }  // namespace fdtd

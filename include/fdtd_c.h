@@ -129,8 +129,10 @@ typedef struct {
     int32_t device;           /* CUDA ordinal                                            */
     int32_t kernel;           /* FDTD_KERNEL_*                                           */
     int32_t graph_steps;      /* >0: capture this many steps per CUDA graph launch       */
-    int32_t tile_y;           /* 0: autotuned/default                                    */
-    int32_t x_chunk;          /* 0: autotuned/default                                    */
+    int32_t tile_y;           /* fused path: PML-shell x planes per thread (1, 2); 0: default */
+    int32_t x_chunk;          /* fused path: interior x planes per thread (2, 4, 8); 0: default */
+    int32_t persistent_ctas;  /* batches: CTAs of the persistent kernels; 0: from occupancy    */
+    int32_t _pad;
 } fdtd_options;
 
 typedef struct {
@@ -260,6 +262,37 @@ fdtd_status fdtd_interior_step_noalloc(const double* p_curr, const double* p_pre
  * FDTD_AcousticSimulator.cpp:381-415).  bytes: query with buffer NULL. */
 fdtd_status fdtd_solver_snapshot(fdtd_solver* s, void* buffer, int64_t* bytes);
 fdtd_status fdtd_solver_restore(fdtd_solver* s, const void* buffer, int64_t bytes);
+
+/* ------------------------------------------------------------------------ */
+/* Batches of independent static solves stepped together.  No counterpart in
+ * the reference, which steps its sim units one after the other
+ * (SimWorld.cpp:517-590); each member produces exactly what an fdtd_solver of
+ * the same scene and options produces.  Per step the whole batch costs a fixed
+ * number of kernel launches; members may have different grids, step counts,
+ * objects, sources and listeners, and retire when their steps are done. */
+typedef struct fdtd_batch fdtd_batch;
+fdtd_status fdtd_batch_create(int32_t n, const fdtd_scene_desc* scenes, const int32_t* steps,
+                              const fdtd_options* options, fdtd_batch** out);
+/* add a member (its first, classifying step runs at once); returns its index,
+ * which may be the index of a released member */
+fdtd_status fdtd_batch_add(fdtd_batch* b, const fdtd_scene_desc* scene, int32_t steps, int32_t* member);
+/* advance every active member by up to n_steps; *n_active: members still running */
+fdtd_status fdtd_batch_step(fdtd_batch* b, int32_t n_steps, int32_t* n_active);
+/* run until every member has finished */
+fdtd_status fdtd_batch_run(fdtd_batch* b);
+fdtd_status fdtd_batch_member_info(fdtd_batch* b, int32_t member, int64_t* steps_done, int64_t* steps_total,
+                                   int32_t* n_listeners, int32_t* status);
+/* listener series of a member so far: steps_done x n_listeners doubles */
+fdtd_status fdtd_batch_output(fdtd_batch* b, int32_t member, double* out, int64_t count);
+/* free the device memory and the series of a finished member; its index becomes free */
+fdtd_status fdtd_batch_release(fdtd_batch* b, int32_t member);
+fdtd_status fdtd_batch_destroy(fdtd_batch* b);
+void* fdtd_batch_stream(fdtd_batch* b);
+int64_t fdtd_batch_last_launch_count(fdtd_batch* b);
+int64_t fdtd_batch_device_bytes(fdtd_batch* b);
+/* Device bytes of the arena a solver of this scene and options allocates (admission by
+ * HBM footprint); -1 when the scene is invalid. */
+int64_t fdtd_scene_device_bytes(const fdtd_scene_desc* scene, const fdtd_options* options);
 
 /* ------------------------------------------------------------------------ */
 /* XML scene reader (ImpulseResponseParser subset, ImpulseResponseParser.cpp:55-751) */
