@@ -8,7 +8,7 @@ from __future__ import annotations
 import ctypes as C
 import os
 
-from .scene import GhostFace, Options, SceneDesc, SolverInfo, GaussianSourceDesc
+from .scene import GaussianSourceDesc, GhostFace, Options, SceneDesc, ServerConfig, ServerStats, SolverInfo
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_lib", "libfdtd_b200.so")
@@ -26,6 +26,8 @@ EXPORTS = [
     "fdtd_batch_create", "fdtd_batch_add", "fdtd_batch_step", "fdtd_batch_run", "fdtd_batch_member_info",
     "fdtd_batch_output", "fdtd_batch_release", "fdtd_batch_destroy", "fdtd_batch_stream",
     "fdtd_batch_last_launch_count", "fdtd_batch_device_bytes", "fdtd_scene_device_bytes",
+    "fdtd_server_create", "fdtd_server_submit", "fdtd_server_poll", "fdtd_server_wait", "fdtd_server_result",
+    "fdtd_server_drain", "fdtd_server_stats_get", "fdtd_server_request_error", "fdtd_server_destroy",
 ]
 
 _lib = None
@@ -91,6 +93,15 @@ def load(build_if_missing: bool = False):
         "fdtd_batch_last_launch_count": ([vp], i64),
         "fdtd_batch_device_bytes": ([vp], i64),
         "fdtd_scene_device_bytes": ([C.POINTER(SceneDesc), C.POINTER(Options)], i64),
+        "fdtd_server_create": ([C.POINTER(Options), C.POINTER(ServerConfig), C.POINTER(vp)], i32),
+        "fdtd_server_submit": ([vp, C.POINTER(SceneDesc), i32, C.POINTER(i64)], i32),
+        "fdtd_server_poll": ([vp, i64, C.POINTER(i32), C.POINTER(i64), C.POINTER(i32)], i32),
+        "fdtd_server_wait": ([vp, i64, dbl], i32),
+        "fdtd_server_result": ([vp, i64, vp, i64, C.POINTER(i64), C.POINTER(i32), C.POINTER(dbl)], i32),
+        "fdtd_server_drain": ([vp, dbl], i32),
+        "fdtd_server_stats_get": ([vp, C.POINTER(ServerStats)], i32),
+        "fdtd_server_request_error": ([vp, i64], C.c_char_p),
+        "fdtd_server_destroy": ([vp], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -439,7 +439,6 @@ fdtd_status fdtd_batch_release(fdtd_batch* b, int32_t member) {
         return batch_fail(b, FDTD_ERR_INVALID_ARG, "member index out of range");
     Member& mb = b->members[member];
     if (mb.released) return FDTD_OK;
-    if (mb.active) return batch_fail(b, FDTD_ERR_BUSY, "member still running");
     if (mb.s) {
         BATCH_TRY(b, cudaStreamSynchronize(b->stream));
         fdtd_solver_destroy(mb.s);

@@ -77,6 +77,21 @@ class Options(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_members", C.c_int32), ("chunk_steps", C.c_int32),
+                ("_pad", C.c_int32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("submitted", "completed", "failed", "queued", "running", "peak_members",
+                                         "peak_device_bytes")] + \
+               [(n, C.c_double) for n in ("p50_latency_s", "p99_latency_s", "mean_latency_s", "span_s",
+                                          "solves_per_s", "cell_steps_per_s")]
+
+
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+
+
 class SolverInfo(C.Structure):
     _fields_ = [
         ("divisions", C.c_int32 * 3), ("n_listeners", C.c_int32), ("n_cells", C.c_int64),

@@ -284,7 +284,7 @@ fdtd_status fdtd_batch_member_info(fdtd_batch* b, int32_t member, int64_t* steps
                                    int32_t* n_listeners, int32_t* status);
 /* listener series of a member so far: steps_done x n_listeners doubles */
 fdtd_status fdtd_batch_output(fdtd_batch* b, int32_t member, double* out, int64_t count);
-/* free the device memory and the series of a finished member; its index becomes free */
+/* stop a member if it still runs, free its device memory and series; its index becomes free */
 fdtd_status fdtd_batch_release(fdtd_batch* b, int32_t member);
 fdtd_status fdtd_batch_destroy(fdtd_batch* b);
 void* fdtd_batch_stream(fdtd_batch* b);
@@ -293,6 +293,54 @@ int64_t fdtd_batch_device_bytes(fdtd_batch* b);
 /* Device bytes of the arena a solver of this scene and options allocates (admission by
  * HBM footprint); -1 when the scene is invalid. */
 int64_t fdtd_scene_device_bytes(const fdtd_scene_desc* scene, const fdtd_options* options);
+
+/* ------------------------------------------------------------------------ */
+/* Solve server: continuous batching of submitted scenes.  No counterpart in the
+ * reference.  A worker thread owns one fdtd_batch; between chunks of batched
+ * steps it admits queued requests in arrival order while their device bytes
+ * (fdtd_scene_device_bytes) fit the budget and a member slot is free, and
+ * retires finished ones, whose series stay on the host until collected.  A
+ * request's series equals that of an fdtd_solver of the same scene and
+ * options, whatever else runs beside it. */
+typedef struct fdtd_server fdtd_server;
+
+typedef struct {
+    int64_t hbm_budget_bytes;  /* device bytes the members may hold; 0: 90% of free memory at create */
+    int32_t max_members;       /* members stepped together; 0: 256; 1 gives FIFO service           */
+    int32_t chunk_steps;       /* batched steps between admissions; 0: max(graph_steps, 32)       */
+    int32_t _pad;
+} fdtd_server_config;
+
+enum { FDTD_REQ_QUEUED = 0, FDTD_REQ_RUNNING = 1, FDTD_REQ_DONE = 2, FDTD_REQ_FAILED = 3 };
+
+typedef struct {
+    int64_t submitted, completed, failed, queued, running;
+    int64_t peak_members;
+    int64_t peak_device_bytes;      /* sum of admitted footprints                               */
+    double p50_latency_s, p99_latency_s, mean_latency_s;  /* submit -> done, completed requests */
+    double span_s;                  /* first submit -> last completion                         */
+    double solves_per_s;            /* completed / span_s                                      */
+    double cell_steps_per_s;        /* sum of cells x steps of completed requests / span_s     */
+} fdtd_server_stats;
+
+fdtd_status fdtd_server_create(const fdtd_options* options, const fdtd_server_config* config, fdtd_server** out);
+/* queue a copy of the scene for `steps` steps; FDTD_ERR_INVALID_ARG for an invalid scene or
+ * one whose footprint exceeds the budget */
+fdtd_status fdtd_server_submit(fdtd_server* srv, const fdtd_scene_desc* scene, int32_t steps, int64_t* request);
+/* state (FDTD_REQ_*), steps done, and for failed requests the status */
+fdtd_status fdtd_server_poll(fdtd_server* srv, int64_t request, int32_t* state, int64_t* steps_done,
+                             int32_t* status);
+/* block until the request is done or failed; FDTD_ERR_TIMEOUT after timeout_s (< 0: no limit) */
+fdtd_status fdtd_server_wait(fdtd_server* srv, int64_t request, double timeout_s);
+/* steps x n_listeners doubles and the latency; the request is forgotten afterwards */
+fdtd_status fdtd_server_result(fdtd_server* srv, int64_t request, double* out, int64_t count, int64_t* steps,
+                               int32_t* n_listeners, double* latency_s);
+/* block until every submitted request is done or failed */
+fdtd_status fdtd_server_drain(fdtd_server* srv, double timeout_s);
+fdtd_status fdtd_server_stats_get(fdtd_server* srv, fdtd_server_stats* stats);
+/* the error text of a failed request */
+const char* fdtd_server_request_error(fdtd_server* srv, int64_t request);
+fdtd_status fdtd_server_destroy(fdtd_server* srv);
 
 /* ------------------------------------------------------------------------ */
 /* XML scene reader (ImpulseResponseParser subset, ImpulseResponseParser.cpp:55-751) */

@@ -43,9 +43,10 @@ def test_struct_layouts_match_header(tmp_path):
 #include <stddef.h>
 #include "fdtd_c.h"
 int main(void) {
-  printf("%zu %zu %zu %zu %zu %zu %zu\\n", sizeof(fdtd_object_desc), sizeof(fdtd_plane_desc),
+  printf("%zu %zu %zu %zu %zu %zu %zu %zu %zu\\n", sizeof(fdtd_object_desc), sizeof(fdtd_plane_desc),
          sizeof(fdtd_gaussian_source_desc), sizeof(fdtd_scene_desc), sizeof(fdtd_options),
-         sizeof(fdtd_solver_info), sizeof(fdtd_ghost_face));
+         sizeof(fdtd_solver_info), sizeof(fdtd_ghost_face), sizeof(fdtd_server_config),
+         sizeof(fdtd_server_stats));
   printf("%zu %zu %zu %zu\\n", offsetof(fdtd_scene_desc, objects), offsetof(fdtd_scene_desc, listeners),
          offsetof(fdtd_object_desc, gravity), offsetof(fdtd_solver_info, algorithmic_bytes_per_step));
   return 0;
@@ -57,7 +58,8 @@ int main(void) {
     sizes = [int(x) for x in out[0].split()]
     offs = [int(x) for x in out[1].split()]
     assert sizes == [C.sizeof(S.ObjectDesc), C.sizeof(S.PlaneDesc), C.sizeof(S.GaussianSourceDesc),
-                     C.sizeof(S.SceneDesc), C.sizeof(S.Options), C.sizeof(S.SolverInfo), C.sizeof(S.GhostFace)]
+                     C.sizeof(S.SceneDesc), C.sizeof(S.Options), C.sizeof(S.SolverInfo), C.sizeof(S.GhostFace),
+                     C.sizeof(S.ServerConfig), C.sizeof(S.ServerStats)]
     assert offs == [S.SceneDesc.objects.offset, S.SceneDesc.listeners.offset, S.ObjectDesc.gravity.offset,
                     S.SolverInfo.algorithmic_bytes_per_step.offset]
     assert S.GHOST_FACE_DTYPE.itemsize == C.sizeof(S.GhostFace)
@@ -167,3 +169,30 @@ def test_invalid_scenes_are_rejected_before_device_use(fdtd_lib):
         h = C.c_void_p()
         assert fdtd_lib.fdtd_solver_create(C.byref(desc), None, C.byref(h)) == status
         assert h.value is None
+
+
+def test_server_and_batch_without_device_fail_cleanly(fdtd_lib):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is visible")
+    from acoustics_b200._lib import FDTDError
+    from acoustics_b200.batch import SolveBatch
+    from acoustics_b200.server import SolveServer
+    with pytest.raises(FDTDError):
+        SolveServer()
+    with pytest.raises(FDTDError):
+        SolveBatch()
+
+
+def test_scene_device_bytes_follows_the_arena_layout(fdtd_lib):
+    from acoustics_b200.batch import scene_device_bytes
+    small = S.config1(divisions=(40, 36, 32), pml_width=6, radius=0.02)
+    big = S.config1()
+    a32, a64 = scene_device_bytes(small), scene_device_bytes(small, precision=S.PRECISION_FP64)
+    assert 0 < a32 < a64 < scene_device_bytes(big, precision=S.PRECISION_FP64)
+    n = 40 * 36 * 32
+    # per cell: flags 2 B, p[2] + dinc + pd[3] + 2 x 3 faces = 12 words (FP32)
+    assert 12 * 4 * n < a32 < 12 * 4 * n + 2 * n + (1 << 20)
+    bad = S.config1(); bad.cell_size = -1.0
+    with pytest.raises(Exception):
+        scene_device_bytes(bad)
