@@ -25,7 +25,7 @@ EXPORTS = [
     "fdtd_solver_time_stencil", "fdtd_interior_step_noalloc",
     "fdtd_batch_create", "fdtd_batch_add", "fdtd_batch_step", "fdtd_batch_run", "fdtd_batch_member_info",
     "fdtd_batch_output", "fdtd_batch_release", "fdtd_batch_destroy", "fdtd_batch_stream",
-    "fdtd_batch_last_launch_count", "fdtd_batch_device_bytes", "fdtd_scene_device_bytes",
+    "fdtd_batch_last_launch_count", "fdtd_batch_device_bytes", "fdtd_scene_device_bytes", "fdtd_scene_info",
     "fdtd_server_create", "fdtd_server_submit", "fdtd_server_poll", "fdtd_server_wait", "fdtd_server_result",
     "fdtd_server_drain", "fdtd_server_stats_get", "fdtd_server_request_error", "fdtd_server_destroy",
 ]
@@ -93,6 +93,7 @@ def load(build_if_missing: bool = False):
         "fdtd_batch_last_launch_count": ([vp], i64),
         "fdtd_batch_device_bytes": ([vp], i64),
         "fdtd_scene_device_bytes": ([C.POINTER(SceneDesc), C.POINTER(Options)], i64),
+        "fdtd_scene_info": ([C.POINTER(SceneDesc), C.POINTER(Options), C.POINTER(SolverInfo)], i32),
         "fdtd_server_create": ([C.POINTER(Options), C.POINTER(ServerConfig), C.POINTER(vp)], i32),
         "fdtd_server_submit": ([vp, C.POINTER(SceneDesc), i32, C.POINTER(i64)], i32),
         "fdtd_server_poll": ([vp, i64, C.POINTER(i32), C.POINTER(i64), C.POINTER(i32)], i32),

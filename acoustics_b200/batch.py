@@ -30,6 +30,18 @@ def scene_device_bytes(scene: Scene, precision: int = PRECISION_FP32_COMPENSATED
     return n
 
 
+def scene_info(scene: Scene, precision: int = PRECISION_FP32_COMPENSATED, kernel: int = KERNEL_FUSED):
+    """SolverInfo of a solver of `scene` (cell counts, device and algorithmic bytes), host only."""
+    from .scene import SolverInfo
+    L = load()
+    desc, keep = scene.to_c()
+    opt = Options(precision=precision, kernel=kernel)
+    info = SolverInfo()
+    check(L.fdtd_scene_info(C.byref(desc), C.byref(opt), C.byref(info)))
+    del keep
+    return info
+
+
 class SolveBatch:
     def __init__(self, scenes: Sequence[Scene] = (), steps: Optional[Sequence[int]] = None,
                  precision: int = PRECISION_FP32_COMPENSATED, graph_steps: int = 16, device: int = 0,

@@ -735,8 +735,10 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     return FDTD_OK;
 }
 
-int64_t fdtd_scene_device_bytes(const fdtd_scene_desc* sc, const fdtd_options* opt) {
-    if (validate_scene(sc) != FDTD_OK) return -1;
+fdtd_status fdtd_scene_info(const fdtd_scene_desc* sc, const fdtd_options* opt, fdtd_solver_info* info) {
+    if (!info) return (set_error(nullptr, "info is NULL"), FDTD_ERR_INVALID_ARG);
+    fdtd_status st = validate_scene(sc);
+    if (st != FDTD_OK) return st;
     fdtd_options o{};
     if (opt) o = *opt;
     fdtd_solver s;
@@ -747,7 +749,24 @@ int64_t fdtd_scene_device_bytes(const fdtd_scene_desc* sc, const fdtd_options* o
     s.L = sc->n_listeners;
     Carver cv;
     carve_arena(&s, sc, o, cv);
-    return (int64_t)cv.off;
+    std::memset(info, 0, sizeof(*info));
+    for (int d = 0; d < 3; ++d) info->divisions[d] = s.N[d];
+    info->n_listeners = s.L;
+    info->n_cells = s.ncell;
+    info->n_pml_cells = s.n_pml;
+    info->n_interior_cells = s.n_interior;
+    info->device_bytes = (int64_t)cv.off;
+    info->time = sc->start_time;
+    info->time_step = s.k;
+    const double w = s.precision == FDTD_PRECISION_FP64 ? 8.0 : 4.0;
+    info->algorithmic_bytes_per_step = w * (3.0 * (double)s.n_interior + 14.0 * (double)s.n_pml);
+    return FDTD_OK;
+}
+
+int64_t fdtd_scene_device_bytes(const fdtd_scene_desc* sc, const fdtd_options* opt) {
+    fdtd_solver_info info;
+    if (fdtd_scene_info(sc, opt, &info) != FDTD_OK) return -1;
+    return info.device_bytes;
 }
 
 }  // extern "C"

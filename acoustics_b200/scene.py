@@ -370,6 +370,19 @@ def config3(seed: int = 5, n_scenes: int = 64) -> List[Scene]:
     return [random_scene(rng, 48, 160, 3, 8, 1000, 3000, f"cfg3_scene{i}") for i in range(n_scenes)]
 
 
+def config4(seed: int = 9, n_requests: int = 16, rate_per_s: float = 2.0):
+    """Serving stream: Poisson arrivals at `rate_per_s` (seeded), each request a scene
+    with grid edges log-uniform in [64, 256], 1000-8000 steps, 1-4 rigid
+    spheres/boxes, a random source and 16 listeners.  Returns [(arrival_s, Scene)]."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for i in range(n_requests):
+        t += float(rng.exponential(1.0 / rate_per_s))
+        out.append((t, random_scene(rng, 64, 256, 4, 16, 1000, 8000, f"cfg4_req{i}")))
+    return out
+
+
 def config5(seed: int = 7, steps: int = 6000) -> Scene:
     """384x384x256, h=2 mm, two spheres r=2.5 cm on seeded ballistic paths that
     meet mid-run, a Gaussian pulse to scatter, 32 listeners; PML width 10."""

@@ -174,6 +174,109 @@ def profile_run(args):
     return 0
 
 
+def bench_batched(peak: float, fp64_check: bool = True):
+    """64 uneven scenes (grid edges log-uniform in [48, 160], 1000-3000 steps, 1-3
+    bodies) stepped as one batch, FP32 compensated, against the same scenes run one
+    by one through PML_WaveSolver.  Cell-steps count every step after the first
+    (classifying) one, which fdtd_batch_add runs per member before the timed loop."""
+    import torch
+
+    from acoustics_b200 import scene as S
+    from acoustics_b200.batch import SolveBatch, scene_info
+    from acoustics_b200.solver import PML_WaveSolver
+    scenes = S.config3()
+    P32 = S.PRECISION_FP32_COMPENSATED
+    infos = [scene_info(sc, precision=P32) for sc in scenes]
+    cell_steps = sum(i.n_cells * (sc.steps - 1) for i, sc in zip(infos, scenes))
+    alg = sum(i.algorithmic_bytes_per_step * (sc.steps - 1) for i, sc in zip(infos, scenes))
+    out = {"workload": "config3: 64 uneven scenes, edges log-uniform [48,160], 1000-3000 steps",
+           "scenes": len(scenes), "cells": int(sum(i.n_cells for i in infos)),
+           "cell_steps": int(cell_steps), "graph_steps": 16}
+    b = SolveBatch(scenes, precision=P32, graph_steps=16)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.run()
+    torch.cuda.synchronize()
+    dt = time.perf_counter() - t0
+    y32 = [b.output(m) for m in range(len(scenes))]
+    b.close()
+    out.update({"seconds": dt, "gcell_steps_s": cell_steps / dt / 1e9,
+                "achieved_gbs": alg / dt / 1e9, "hbm_frac": alg / dt / 1e9 / peak})
+    # one by one, same scenes and options, stepping only (creation outside)
+    solvers = [PML_WaveSolver(sc, precision=P32, graph_steps=16) for sc in scenes]
+    for g in solvers:
+        g.step(1)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for g, sc in zip(solvers, scenes):
+        g.step(sc.steps - 1)
+    torch.cuda.synchronize()
+    dt1 = time.perf_counter() - t0
+    for g in solvers:
+        g.close()
+    out.update({"one_by_one_seconds": dt1, "one_by_one_gcell_steps_s": cell_steps / dt1 / 1e9,
+                "speedup_vs_one_by_one": dt1 / dt})
+    if fp64_check:
+        b64 = SolveBatch(scenes, precision=S.PRECISION_FP64, graph_steps=16)
+        b64.run()
+        y64 = [b64.output(m) for m in range(len(scenes))]
+        b64.close()
+        errs = [float(np.linalg.norm(a - c) / np.linalg.norm(c)) for a, c in zip(y32, y64)]
+        out["listener_rel_l2_vs_fp64_max"] = max(errs)
+        out["listener_rel_l2_vs_fp64_median"] = float(np.median(errs))
+    return out
+
+
+def bench_served(peak: float, rate: float, n_requests: int, fifo_baseline: bool = True):
+    """Poisson request stream (config4) into the solve server (FP32, continuous
+    batching) and, as the baseline, served first-in first-out by the plain FP64
+    GPU path (one kernel per reference phase), one request at a time."""
+    from acoustics_b200 import scene as S
+    from acoustics_b200.batch import scene_info
+    from acoustics_b200.server import SolveServer
+    from acoustics_b200.solver import PML_WaveSolver
+    reqs = S.config4(n_requests=n_requests, rate_per_s=rate)
+    P32 = S.PRECISION_FP32_COMPENSATED
+    infos = [scene_info(sc, precision=P32) for _, sc in reqs]
+    cell_steps = sum(i.n_cells * sc.steps for i, (_, sc) in zip(infos, reqs))
+    alg = sum(i.algorithmic_bytes_per_step * sc.steps for i, (_, sc) in zip(infos, reqs))
+    out = {"workload": f"config4: {n_requests} Poisson arrivals at {rate}/s, edges log-uniform [64,256], "
+                       f"1000-8000 steps, 16 listeners", "requests": n_requests, "cell_steps": int(cell_steps)}
+    with SolveServer(precision=P32, graph_steps=16, chunk_steps=32) as srv:
+        t0 = time.perf_counter()
+        ids = []
+        for t_arr, sc in reqs:
+            d = t0 + t_arr - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            ids.append(srv.submit(sc))
+        lat = [srv.result(i)[1] for i in ids]
+        st = srv.stats()
+    out.update({"p50_latency_s": float(np.percentile(lat, 50)), "p99_latency_s": float(np.percentile(lat, 99)),
+                "solves_per_s": st["solves_per_s"], "gcell_steps_s": st["cell_steps_per_s"] / 1e9,
+                "hbm_frac": alg / st["span_s"] / 1e9 / peak if st["span_s"] > 0 else None,
+                "span_s": st["span_s"], "peak_members": st["peak_members"],
+                "peak_device_gb": st["peak_device_bytes"] / 1e9})
+    if fifo_baseline:
+        t0 = time.perf_counter()
+        lat64 = []
+        for t_arr, sc in reqs:
+            d = t0 + t_arr - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            g = PML_WaveSolver(sc, precision=S.PRECISION_FP64, kernel=S.KERNEL_PHASED)
+            g.step(sc.steps)
+            g.close()
+            lat64.append(time.perf_counter() - (t0 + t_arr))
+        span = time.perf_counter() - (t0 + reqs[0][0])
+        out["fifo_fp64_plain"] = {"p50_latency_s": float(np.percentile(lat64, 50)),
+                                  "p99_latency_s": float(np.percentile(lat64, 99)),
+                                  "solves_per_s": n_requests / span, "gcell_steps_s": cell_steps / span / 1e9}
+        out["solves_per_s_vs_fifo_fp64"] = out["solves_per_s"] / out["fifo_fp64_plain"]["solves_per_s"]
+        out["p99_vs_fifo_fp64"] = out["p99_latency_s"] / out["fifo_fp64_plain"]["p99_latency_s"]
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -188,6 +291,10 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--profile", action="store_true", help="only run --steps steps of the bench solve (for ncu)")
     ap.add_argument("--profile-n", type=int, default=256, help="grid edge of the --profile solve")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 64-scene batch (config 3)")
+    ap.add_argument("--no-served", action="store_true", help="skip the serving stream (config 4)")
+    ap.add_argument("--serve-rate", type=float, default=4.0)
+    ap.add_argument("--serve-requests", type=int, default=16)
     args = ap.parse_args()
     if args.profile:
         return profile_run(args)
@@ -293,6 +400,12 @@ def main():
         if "fp64_plain" in variants and "fp32_compensated" in variants:
             variants["fp32_over_fp64_plain"] = variants["fp32_compensated"]["gcell_steps_s"] / variants["fp64_plain"]["gcell_steps_s"]
 
+    batched = served = None
+    if rank == 0 and world == 1 and not args.no_batched:
+        batched = bench_batched(peak)
+    if rank == 0 and world == 1 and not args.no_served:
+        served = bench_served(peak, args.serve_rate, args.serve_requests)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         val, n, threads, dt = cpu_baseline(sc, args.cpu_budget, 1000)
@@ -320,6 +433,10 @@ def main():
             "clocks": clocks,
             "variants": variants,
         }
+        if batched:
+            line["batched"] = batched
+        if served:
+            line["served"] = served
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)

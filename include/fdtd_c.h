@@ -293,6 +293,10 @@ int64_t fdtd_batch_device_bytes(fdtd_batch* b);
 /* Device bytes of the arena a solver of this scene and options allocates (admission by
  * HBM footprint); -1 when the scene is invalid. */
 int64_t fdtd_scene_device_bytes(const fdtd_scene_desc* scene, const fdtd_options* options);
+/* The fdtd_solver_info a solver of this scene would report at creation (grid,
+ * PML / interior cell counts, device and algorithmic bytes), computed on the
+ * host without a device. */
+fdtd_status fdtd_scene_info(const fdtd_scene_desc* scene, const fdtd_options* options, fdtd_solver_info* info);
 
 /* ------------------------------------------------------------------------ */
 /* Solve server: continuous batching of submitted scenes.  No counterpart in the

@@ -196,3 +196,13 @@ def test_scene_device_bytes_follows_the_arena_layout(fdtd_lib):
     bad = S.config1(); bad.cell_size = -1.0
     with pytest.raises(Exception):
         scene_device_bytes(bad)
+
+
+def test_scene_info_on_the_host(fdtd_lib):
+    from acoustics_b200.batch import scene_info
+    sc = S.config2(n=256)
+    i32, i64 = scene_info(sc), scene_info(sc, precision=S.PRECISION_FP64)
+    assert tuple(i32.divisions) == (256, 256, 256)
+    assert i32.n_interior_cells == 11239424 and i32.n_pml_cells == 5537792
+    assert i32.algorithmic_bytes_per_step == 444989440.0
+    assert i64.algorithmic_bytes_per_step == 2 * i32.algorithmic_bytes_per_step
