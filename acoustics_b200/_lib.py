@@ -11,7 +11,9 @@ import os
 from .scene import GaussianSourceDesc, GhostFace, Options, SceneDesc, ServerConfig, ServerStats, SolverInfo
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "_lib", "libfdtd_b200.so")
+# FDTD_B200_LIB: load another build of the same library (same ABI), e.g. one with
+# other compile-time tile shapes
+LIB_PATH = os.environ.get("FDTD_B200_LIB") or os.path.join(HERE, "_lib", "libfdtd_b200.so")
 
 # every symbol include/fdtd_c.h declares
 EXPORTS = [
@@ -22,7 +24,7 @@ EXPORTS = [
     "fdtd_solver_stream", "fdtd_solver_last_error", "fdtd_solver_last_launch_count",
     "fdtd_solver_snapshot", "fdtd_solver_restore", "fdtd_scene_from_xml", "fdtd_scene_desc_get",
     "fdtd_scene_number_of_steps", "fdtd_scene_output_pattern", "fdtd_scene_free", "fdtd_audio_append",
-    "fdtd_solver_time_stencil", "fdtd_interior_step_noalloc",
+    "fdtd_solver_time_stencil", "fdtd_solver_time_kernel", "fdtd_interior_step_noalloc",
     "fdtd_batch_create", "fdtd_batch_add", "fdtd_batch_step", "fdtd_batch_run", "fdtd_batch_member_info",
     "fdtd_batch_output", "fdtd_batch_release", "fdtd_batch_destroy", "fdtd_batch_stream",
     "fdtd_batch_last_launch_count", "fdtd_batch_device_bytes", "fdtd_scene_device_bytes", "fdtd_scene_info",
@@ -79,6 +81,7 @@ def load(build_if_missing: bool = False):
         "fdtd_scene_free": ([vp], None),
         "fdtd_audio_append": ([C.c_char_p, vp, i64], i32),
         "fdtd_solver_time_stencil": ([vp, i32, C.POINTER(C.c_float)], i32),
+        "fdtd_solver_time_kernel": ([vp, i32, i32, C.POINTER(C.c_float)], i32),
         "fdtd_interior_step_noalloc": ([vp, vp, vp, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), dbl, dbl, vp],
                                        i32),
         "fdtd_batch_create": ([i32, C.POINTER(SceneDesc), C.POINTER(i32), C.POINTER(Options), C.POINTER(vp)], i32),

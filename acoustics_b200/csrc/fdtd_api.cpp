@@ -417,6 +417,9 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
         cv.add((void**)&P.pdiv_f[d], N[d] * 4);
         cv.add((void**)&P.vupd_f[d], (N[d] + 1) * 4);
         cv.add((void**)&P.vgrad_f[d], (N[d] + 1) * 4);
+        cv.add((void**)&P.axflag[d], N[d] + 1);
+        cv.add((void**)&P.coef_d[d], (N[d] + 1) * sizeof(AxisCoef<double>));
+        cv.add((void**)&P.coef_f[d], (N[d] + 1) * sizeof(AxisCoef<float>));
     }
     s->lis_cap_steps = std::max(256, o.graph_steps);
     cv.add((void**)&s->d_lis, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8);
@@ -614,6 +617,33 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         CUDA_TRY(s.get(), cudaMemcpy((void*)P.pdiv_f[d], f2.data(), N[d] * 4, cudaMemcpyHostToDevice));
         CUDA_TRY(s.get(), cudaMemcpy((void*)P.vupd_f[d], f3.data(), (N[d] + 1) * 4, cudaMemcpyHostToDevice));
         CUDA_TRY(s.get(), cudaMemcpy((void*)P.vgrad_f[d], f4.data(), (N[d] + 1) * 4, cudaMemcpyHostToDevice));
+        // packed flags and coefficient quads of the shell kernel
+        std::vector<uint8_t> fl(N[d] + 1, 0);
+        std::vector<AxisCoef<double>> cd(N[d] + 1);
+        std::vector<AxisCoef<float>> cf(N[d] + 1);
+        for (int i = 0; i <= N[d]; ++i) {
+            uint8_t f = 0;
+            if (i < N[d]) {
+                if (T.pml_cell[i]) f |= AXF_PML;
+                if (i > 0 && T.pml_face[i]) f |= AXF_FACE_LO;
+                if (i + 1 < N[d] && T.pml_face[i + 1]) f |= AXF_FACE_HI;
+                if (i + 1 < N[d] && T.pml_cell[i + 1]) f |= AXF_NEXT_PML;
+                if (i > 0) f |= AXF_HAS_LO;
+                if (i + 1 < N[d]) f |= AXF_HAS_HI;
+            }
+            fl[i] = f;
+            cd[i].vupd = T.vupd[i];
+            cd[i].vgrad = T.vgrad[i];
+            cd[i].pupd = i < N[d] ? T.pupd[i] : 0.0;
+            cd[i].pdiv = i < N[d] ? T.pdiv[i] : 0.0;
+            cf[i].vupd = (float)cd[i].vupd;
+            cf[i].vgrad = (float)cd[i].vgrad;
+            cf[i].pupd = (float)cd[i].pupd;
+            cf[i].pdiv = (float)cd[i].pdiv;
+        }
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.axflag[d], fl.data(), N[d] + 1, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.coef_d[d], cd.data(), cd.size() * sizeof(cd[0]), cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.coef_f[d], cf.data(), cf.size() * sizeof(cf[0]), cudaMemcpyHostToDevice));
     }
     if (s->L > 0)
         CUDA_TRY(s.get(), cudaMemcpy((void*)P.listeners, s->listeners.data(), s->listeners.size() * 8, cudaMemcpyHostToDevice));
@@ -623,7 +653,8 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     s->xb = (o.x_chunk == 2 || o.x_chunk == 4 || o.x_chunk == 8) ? o.x_chunk : 4;
     s->region.xb = s->xb;
     // tile_y selects the PML-shell planes per thread (1 or 2) of the fused path
-    if (o.kernel == FDTD_KERNEL_FUSED && (o.tile_y == 1 || o.tile_y == 2)) build_shell_boxes(s.get(), o.tile_y);
+    if (o.kernel == FDTD_KERNEL_FUSED && (o.tile_y == 1 || o.tile_y == 2 || o.tile_y == 4))
+        build_shell_boxes(s.get(), o.tile_y);
     s->region.shell = s->shell;
     if (o.x_chunk > 0) s->xchunk = o.x_chunk;
     else {

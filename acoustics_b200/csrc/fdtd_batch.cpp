@@ -126,7 +126,7 @@ fdtd_status grow(fdtd_batch* b, T** ptr, size_t* cap, size_t need) {
 fdtd_status rebuild(fdtd_batch* b) {
     const bool f64 = b->precision == FDTD_PRECISION_FP64;
     const int xb = (b->opt.x_chunk == 2 || b->opt.x_chunk == 8) ? b->opt.x_chunk : 4;
-    const int xs = (b->opt.tile_y == 2) ? 2 : 1;
+    const int xs = (b->opt.tile_y == 2 || b->opt.tile_y == 4) ? b->opt.tile_y : 1;
     const size_t dsz = f64 ? desc_bytes<double>() : desc_bytes<float>();
     const size_t nm = b->members.size();
     std::vector<char> descs(std::max<size_t>(nm, 1) * dsz, 0);

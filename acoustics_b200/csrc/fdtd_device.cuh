@@ -76,6 +76,25 @@ struct ShellBoxes {
 
 struct SolveParams;
 
+// Per-axis PML flags of index i (one byte, read once per thread and axis by the
+// shell kernel instead of four table lookups).
+enum : uint8_t {
+    AXF_PML = 1,        // cell i inside the PML
+    AXF_FACE_LO = 2,    // face i inside the PML and not the outer face (i > 0)
+    AXF_FACE_HI = 4,    // face i+1 inside the PML and not the outer face (i+1 < N)
+    AXF_NEXT_PML = 8,   // cell i+1 inside the PML
+    AXF_HAS_LO = 16,    // i > 0
+    AXF_HAS_HI = 32     // i + 1 < N
+};
+
+// Coefficients of index i in one aligned quad: face i (velocity update and
+// gradient factor) and cell i (split-pressure update and divergence factor;
+// zero for i = N).  One vector load per face instead of two scalar ones.
+template <typename T>
+struct alignas(4 * sizeof(T)) AxisCoef {
+    T vupd, vgrad, pupd, pdiv;
+};
+
 // Pointers and scalars of the hot kernels, passed by value (kernel parameters
 // live in the constant bank, so the kernels issue no loads to fetch them).
 template <typename T>
@@ -89,12 +108,8 @@ struct KArgs {
     T* pd[3];
     const T* vo[3];
     T* vn[3];
-    const uint8_t* pml_cell[3];
-    const uint8_t* pml_face[3];
-    const T* pupd[3];
-    const T* pdiv[3];
-    const T* vupd[3];
-    const T* vgrad[3];
+    const uint8_t* axflag[3];     // AXF_* per index, [N_d + 1]
+    const AxisCoef<T>* coef[3];   // [N_d + 1]
     T inv_h, c2k2, lap_scale;
     SolveParams* P;               // device copy (for the step-constant advance)
     int cur;
@@ -109,6 +124,7 @@ struct RegionLaunch {
     int sources;       // launch the source kernel this step
     int ghost_cap;     // capacity of the ghost-neighbour list (0: no list kernel)
     int xb;            // x planes per interior thread
+    int skip;          // kernels left out (timing of single kernels): 1 interior, 2 shell, 4 ghost list
 };
 
 // Two copies indexed by the step parity: the kernels of a step read
@@ -147,6 +163,9 @@ struct SolveParams {
     const float* pdiv_f[3];
     const float* vupd_f[3];
     const float* vgrad_f[3];
+    const uint8_t* axflag[3];     // [N_d+1] AXF_* flags
+    const AxisCoef<double>* coef_d[3];  // [N_d+1]
+    const AxisCoef<float>* coef_f[3];   // [N_d+1] (the same values rounded to float)
     // state
     uint8_t* cls;
     uint8_t* gobj;
@@ -184,9 +203,8 @@ inline KArgs<double> make_kargs<double>(SolveParams* dP, const SolveParams& P, i
         A.pd[d] = (double*)P.pd[d];
         A.vo[d] = (const double*)P.v[cur][d];
         A.vn[d] = (double*)P.v[cur ^ 1][d];
-        A.pml_cell[d] = P.pml_cell[d];
-        A.pml_face[d] = P.pml_face[d];
-        A.pupd[d] = P.pupd[d]; A.pdiv[d] = P.pdiv[d]; A.vupd[d] = P.vupd[d]; A.vgrad[d] = P.vgrad[d];
+        A.axflag[d] = P.axflag[d];
+        A.coef[d] = P.coef_d[d];
     }
     A.inv_h = P.inv_h; A.c2k2 = P.c2k2; A.lap_scale = P.lap_scale;
     return A;
@@ -208,9 +226,8 @@ inline KArgs<float> make_kargs<float>(SolveParams* dP, const SolveParams& P, int
         A.pd[d] = (float*)P.pd[d];
         A.vo[d] = (const float*)P.v[cur][d];
         A.vn[d] = (float*)P.v[cur ^ 1][d];
-        A.pml_cell[d] = P.pml_cell[d];
-        A.pml_face[d] = P.pml_face[d];
-        A.pupd[d] = P.pupd_f[d]; A.pdiv[d] = P.pdiv_f[d]; A.vupd[d] = P.vupd_f[d]; A.vgrad[d] = P.vgrad_f[d];
+        A.axflag[d] = P.axflag[d];
+        A.coef[d] = P.coef_f[d];
     }
     A.inv_h = (float)P.inv_h; A.c2k2 = (float)P.c2k2; A.lap_scale = (float)P.lap_scale;
     return A;

@@ -28,9 +28,11 @@
 #include "fdtd_region.cuh"
 #include "fdtd_stencil.cuh"
 
-#ifndef FDTD_SHELL_MINB
-#define FDTD_SHELL_MINB 4
-#endif
+// resident CTAs of 256 threads the shell kernels are compiled for (register
+// budget per thread): FP32 64 / 80 / 128, FP64 80 / 128 / 255 for 1 / 2 / 4 x planes
+__host__ __device__ constexpr int shell_min_blocks(int xs, int word) {
+    return word == 4 ? (xs == 1 ? 4 : (xs == 2 ? 3 : 2)) : (xs == 1 ? 3 : (xs == 2 ? 2 : 1));
+}
 
 namespace fdtd {
 
@@ -91,7 +93,7 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
         if constexpr (!COMP) {
             pn[i * sx] = (T)2.0 * p0 - prev[i] + lap * A.c2k2;
         } else {
-            const float d = (float)prev[i] + (float)(lap * A.c2k2);
+            const float d = fmaf(lap, A.c2k2, prev[i]);
             dinc[i * sx] = d;
             pn[i * sx] = p0 + d;
         }
@@ -103,7 +105,13 @@ __global__ void __launch_bounds__(256) k_interior(const KArgs<T> A, Box3 box) {
     interior_tile<T, XB>(A, box, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
-// One PML-shell tile of box b at tile coordinates (tz, ty, tx).
+// One PML-shell tile of box b at tile coordinates (tz, ty, tx): XS x planes of
+// one (y, z) column per thread.  Every global load of the XS planes (pressure
+// and its six neighbours, six face velocities, three split pressures) is
+// issued before the first use, with neighbour offsets clamped at the domain
+// edge instead of branched on, so a thread keeps ~13*XS independent loads in
+// flight; the face flags and coefficients come from the packed per-axis
+// tables (L1-resident).  Arithmetic order per cell is unchanged.
 template <typename T, int XS>
 __device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& B, int b, int tz, int ty, int tx) {
     const int zz = tz * 32 + threadIdx.x;
@@ -112,70 +120,100 @@ __device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& 
     const int z = zz < B.nza[b] ? B.z0a[b] + zz : B.z0b[b] + (zz - B.nza[b]);
     const int y = B.y0[b] + yy;
     const int xbeg = B.x0[b] + tx * XS;
-    const int xend = min(xbeg + XS, B.x0[b] + B.nx[b]);
-    const int N0 = A.N0, N1 = A.N1, N2 = A.N2;
+    const int nxh = min(XS, B.x0[b] + B.nx[b] - xbeg);
+    const int N1 = A.N1, N2 = A.N2;
+    const unsigned sx = A.sx;
     const unsigned sy1 = (unsigned)(N1 + 1) * N2;  // x stride of the y-face grid
     const unsigned sz2 = (unsigned)N1 * (N2 + 1);  // x stride of the z-face grid
-    const bool pmly = A.pml_cell[1][y] != 0;
-    const bool pmlz = A.pml_cell[2][z] != 0;
+    const unsigned c0 = (unsigned)xbeg * sx + (unsigned)y * N2 + z;
+    const unsigned fy0 = (unsigned)xbeg * sy1 + (unsigned)y * N2 + z;
+    const unsigned fz0 = (unsigned)xbeg * sz2 + (unsigned)y * (N2 + 1) + z;
+    const uint8_t gy = __ldg(A.axflag[1] + y), gz = __ldg(A.axflag[2] + z);
+    const bool pmly = gy & AXF_PML, pmlz = gz & AXF_PML;
+    const unsigned oym = (gy & AXF_HAS_LO) ? (unsigned)N2 : 0u, oyp = (gy & AXF_HAS_HI) ? (unsigned)N2 : 0u;
+    const unsigned ozm = (gz & AXF_HAS_LO) ? 1u : 0u, ozp = (gz & AXF_HAS_HI) ? 1u : 0u;
 
+    // ---- loads of all XS planes ----
+    T p0v[XS], xm[XS], xp[XS], ym[XS], yp[XS], zm[XS], zp[XS];
+    T vxl[XS], vxr[XS], vyl[XS], vyr[XS], vzl[XS], vzr[XS], a0[XS], a1[XS], a2[XS];
+    uint8_t gx[XS];
 #pragma unroll
     for (int i = 0; i < XS; ++i) {
+        if (i < nxh) {
+            const int x = xbeg + i;
+            const unsigned c = c0 + i * sx;
+            gx[i] = __ldg(A.axflag[0] + x);
+            p0v[i] = A.pc[c];
+            xm[i] = A.pc[c - (x > 0 ? sx : 0u)];
+            xp[i] = A.pc[c + (x + 1 < A.N0 ? sx : 0u)];
+            ym[i] = A.pc[c - oym];
+            yp[i] = A.pc[c + oyp];
+            zm[i] = A.pc[c - ozm];
+            zp[i] = A.pc[c + ozp];
+            vxl[i] = A.vo[0][c];
+            vxr[i] = A.vo[0][c + sx];
+            vyl[i] = A.vo[1][fy0 + i * sy1];
+            vyr[i] = A.vo[1][fy0 + i * sy1 + N2];
+            vzl[i] = A.vo[2][fz0 + i * sz2];
+            vzr[i] = A.vo[2][fz0 + i * sz2 + 1];
+            a0[i] = A.pd[0][c];
+            a1[i] = A.pd[1][c];
+            a2[i] = A.pd[2][c];
+        }
+    }
+    const AxisCoef<T> cyl = A.coef[1][y], cyr = A.coef[1][y + 1];
+    const AxisCoef<T> czl = A.coef[2][z], czr = A.coef[2][z + 1];
+
+    // ---- face velocities, split pressures, pressure ----
+#pragma unroll
+    for (int i = 0; i < XS; ++i) {
+        if (i >= nxh) break;
         const int x = xbeg + i;
-        if (x >= xend) break;
-        const unsigned c = (unsigned)x * A.sx + (unsigned)y * N2 + z;
-        const unsigned fy = (unsigned)x * sy1 + (unsigned)y * N2 + z;
-        const unsigned fz = (unsigned)x * sz2 + (unsigned)y * (N2 + 1) + z;
-        const bool pmlx = A.pml_cell[0][x] != 0;
+        const unsigned c = c0 + i * sx;
+        const unsigned fy = fy0 + i * sy1, fz = fz0 + i * sz2;
+        const uint8_t g = gx[i];
+        const bool pmlx = g & AXF_PML;
         // faces inside the PML (InsidePML at the face position, MAC_Grid.cpp:2631-2633),
-        // outer faces excluded (:2568-2575)
-        const bool fxl = x > 0 && (A.pml_face[0][x] != 0 || pmly || pmlz);
-        const bool fxr = x + 1 < N0 && (A.pml_face[0][x + 1] != 0 || pmly || pmlz);
-        const bool fyl = y > 0 && (A.pml_face[1][y] != 0 || pmlx || pmlz);
-        const bool fyr = y + 1 < N1 && (A.pml_face[1][y + 1] != 0 || pmlx || pmlz);
-        const bool fzl = z > 0 && (A.pml_face[2][z] != 0 || pmlx || pmly);
-        const bool fzr = z + 1 < N2 && (A.pml_face[2][z + 1] != 0 || pmlx || pmly);
-        // ---- loads ----
-        const T p0 = A.pc[c];
-        const T pxm = fxl ? A.pc[c - A.sx] : p0;
-        const T pxp = fxr ? A.pc[c + A.sx] : p0;
-        const T pym = fyl ? A.pc[c - N2] : p0;
-        const T pyp = fyr ? A.pc[c + N2] : p0;
-        const T pzm = fzl ? A.pc[c - 1] : p0;
-        const T pzp = fzr ? A.pc[c + 1] : p0;
-        T vxl = A.vo[0][c], vxr = A.vo[0][c + A.sx];
-        T vyl = A.vo[1][fy], vyr = A.vo[1][fy + N2];
-        T vzl = A.vo[2][fz], vzr = A.vo[2][fz + 1];
-        const T ax0 = A.pd[0][c], ay0 = A.pd[1][c], az0 = A.pd[2][c];
-        // ---- face velocities ----
+        // outer faces excluded (:2568-2575); a high face is written here only when the
+        // cell beyond it is not a PML cell
+        const bool oyz = pmly || pmlz, oxz = pmlx || pmlz, oxy = pmlx || pmly;
+        const bool fxl = (g & AXF_FACE_LO) || ((g & AXF_HAS_LO) && oyz);
+        const bool fxr = (g & AXF_FACE_HI) || ((g & AXF_HAS_HI) && oyz);
+        const bool fyl = (gy & AXF_FACE_LO) || ((gy & AXF_HAS_LO) && oxz);
+        const bool fyr = (gy & AXF_FACE_HI) || ((gy & AXF_HAS_HI) && oxz);
+        const bool fzl = (gz & AXF_FACE_LO) || ((gz & AXF_HAS_LO) && oxy);
+        const bool fzr = (gz & AXF_FACE_HI) || ((gz & AXF_HAS_HI) && oxy);
+        const T p0 = p0v[i];
+        T vxl_ = vxl[i], vxr_ = vxr[i];
+        T vyl_ = vyl[i], vyr_ = vyr[i], vzl_ = vzl[i], vzr_ = vzr[i];
+        const AxisCoef<T> cxl = A.coef[0][x], cxr = A.coef[0][x + 1];
         if (fxl) {
-            vxl = vel_update<T>(vxl, A.vupd[0][x], A.vgrad[0][x], p0, pxm);
-            A.vn[0][c] = vxl;
+            vxl_ = vel_update<T>(vxl_, cxl.vupd, cxl.vgrad, p0, xm[i]);
+            A.vn[0][c] = vxl_;
         }
         if (fxr) {
-            vxr = vel_update<T>(vxr, A.vupd[0][x + 1], A.vgrad[0][x + 1], pxp, p0);
-            if (!(A.pml_cell[0][x + 1] != 0 || pmly || pmlz)) A.vn[0][c + A.sx] = vxr;
+            vxr_ = vel_update<T>(vxr_, cxr.vupd, cxr.vgrad, xp[i], p0);
+            if (!((g & AXF_NEXT_PML) || oyz)) A.vn[0][c + sx] = vxr_;
         }
         if (fyl) {
-            vyl = vel_update<T>(vyl, A.vupd[1][y], A.vgrad[1][y], p0, pym);
-            A.vn[1][fy] = vyl;
+            vyl_ = vel_update<T>(vyl_, cyl.vupd, cyl.vgrad, p0, ym[i]);
+            A.vn[1][fy] = vyl_;
         }
         if (fyr) {
-            vyr = vel_update<T>(vyr, A.vupd[1][y + 1], A.vgrad[1][y + 1], pyp, p0);
-            if (!(A.pml_cell[1][y + 1] != 0 || pmlx || pmlz)) A.vn[1][fy + N2] = vyr;
+            vyr_ = vel_update<T>(vyr_, cyr.vupd, cyr.vgrad, yp[i], p0);
+            if (!((gy & AXF_NEXT_PML) || oxz)) A.vn[1][fy + N2] = vyr_;
         }
         if (fzl) {
-            vzl = vel_update<T>(vzl, A.vupd[2][z], A.vgrad[2][z], p0, pzm);
-            A.vn[2][fz] = vzl;
+            vzl_ = vel_update<T>(vzl_, czl.vupd, czl.vgrad, p0, zm[i]);
+            A.vn[2][fz] = vzl_;
         }
         if (fzr) {
-            vzr = vel_update<T>(vzr, A.vupd[2][z + 1], A.vgrad[2][z + 1], pzp, p0);
-            if (!(A.pml_cell[2][z + 1] != 0 || pmlx || pmly)) A.vn[2][fz + 1] = vzr;
+            vzr_ = vel_update<T>(vzr_, czr.vupd, czr.vgrad, zp[i], p0);
+            if (!((gz & AXF_NEXT_PML) || oxy)) A.vn[2][fz + 1] = vzr_;
         }
-        // ---- split-field pressures ----
-        const T ax = pd_update<T>(ax0, A.pupd[0][x], A.pdiv[0][x], vxr, vxl, A.inv_h);
-        const T ay = pd_update<T>(ay0, A.pupd[1][y], A.pdiv[1][y], vyr, vyl, A.inv_h);
-        const T az = pd_update<T>(az0, A.pupd[2][z], A.pdiv[2][z], vzr, vzl, A.inv_h);
+        const T ax = pd_update<T>(a0[i], cxl.pupd, cxl.pdiv, vxr_, vxl_, A.inv_h);
+        const T ay = pd_update<T>(a1[i], cyl.pupd, cyl.pdiv, vyr_, vyl_, A.inv_h);
+        const T az = pd_update<T>(a2[i], czl.pupd, czl.pdiv, vzr_, vzl_, A.inv_h);
         A.pd[0][c] = ax;
         A.pd[1][c] = ay;
         A.pd[2][c] = az;
@@ -197,7 +235,7 @@ __device__ __forceinline__ void shell_decode(const ShellBoxes& B, int blk, int& 
 }
 
 template <typename T, int XS>
-__global__ void __launch_bounds__(256, FDTD_SHELL_MINB) k_pml_shell(const KArgs<T> A, const ShellBoxes B) {
+__global__ void __launch_bounds__(256, shell_min_blocks(XS, sizeof(T))) k_pml_shell(const KArgs<T> A, const ShellBoxes B) {
     if (A.advance && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) advance_consts(*A.P, A.cur);
     int b, tz, ty, tx;
     shell_decode(B, blockIdx.x, b, tz, ty, tx);
@@ -214,7 +252,7 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     const KArgs<T> A = make_kargs<T>(const_cast<SolveParams*>(dP), hP, cur);
     const Box3& b = R.interior;
     const int nx = b.hi[0] - b.lo[0], ny = b.hi[1] - b.lo[1], nz = b.hi[2] - b.lo[2];
-    const bool has_interior = nx > 0 && ny > 0 && nz > 0;
+    const bool has_interior = nx > 0 && ny > 0 && nz > 0 && !(R.skip & 1);
     const bool concurrent = has_interior && s2 != nullptr;
     cudaError_t e = cudaSuccess;
     if (concurrent) {
@@ -232,13 +270,14 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
         else k_interior<T, 4><<<grid, block, 0, si>>>(A, b);
         ++l;
     }
-    const int nblk = R.shell.block_first[R.shell.n];
+    const int nblk = (R.skip & 2) ? 0 : R.shell.block_first[R.shell.n];
     if (nblk > 0) {
         if (R.shell.xs == 2) k_pml_shell<T, 2><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
+        else if (R.shell.xs == 4) k_pml_shell<T, 4><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
         else k_pml_shell<T, 1><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
         ++l;
     }
-    if (R.ghost_cap > 0) {
+    if (R.ghost_cap > 0 && !(R.skip & 4)) {
         // cells next to a solid: disjoint from the interior and shell cells
         const int blocks = (R.ghost_cap + 127) / 128 < 1184 ? (R.ghost_cap + 127) / 128 : 1184;
         k_ghost_cells<T><<<blocks, 128, 0, concurrent ? s2 : s>>>(dP, cur);

@@ -46,22 +46,34 @@ struct Coef<float> {
     __device__ static const float* vgrad(const SolveParams& P, int d) { return P.vgrad_f[d]; }
 };
 
-// v <- v*upd + grad*pR - grad*pL   (three roundings, MAC_Grid.cpp:471-474)
+// v <- v*upd + grad*pR - grad*pL   (MAC_Grid.cpp:471-474).  FP64: the reference's
+// roundings in its order (the unit is compiled without FMA contraction).  FP32:
+// two explicit FMAs, so the result does not depend on how the compiler
+// contracts a given instantiation (every device unit is built with -fmad=false).
 template <typename T>
 __device__ __forceinline__ T vel_update(T v, T upd, T grad, T pR, T pL) {
-    T r = v * upd;
-    r = r + grad * pR;
-    r = r - grad * pL;
-    return r;
+    if constexpr (sizeof(T) == 4) {
+        return fmaf(-grad, pL, fmaf(grad, pR, v * upd));
+    } else {
+        T r = v * upd;
+        r = r + grad * pR;
+        r = r - grad * pL;
+        return r;
+    }
 }
 
-// p_d <- p_d*upd + div*vR/h - div*vL/h   (MAC_Grid.cpp:500-505)
+// p_d <- p_d*upd + div*vR/h - div*vL/h   (MAC_Grid.cpp:500-505); FP32 as above
 template <typename T>
 __device__ __forceinline__ T pd_update(T pd, T upd, T div, T vR, T vL, T inv_h) {
-    T r = pd * upd;
-    r = r + div * vR * inv_h;
-    r = r - div * vL * inv_h;
-    return r;
+    if constexpr (sizeof(T) == 4) {
+        const float dv = div * inv_h;
+        return fmaf(-dv, vL, fmaf(dv, vR, pd * upd));
+    } else {
+        T r = pd * upd;
+        r = r + div * vR * inv_h;
+        r = r - div * vL * inv_h;
+        return r;
+    }
 }
 
 // Sum of the Gaussian pressure sources at a cell centre (GaussianPressureSource.cpp:6-30,

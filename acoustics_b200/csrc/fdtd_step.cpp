@@ -288,31 +288,41 @@ fdtd_status fdtd_solver_fetch_listeners(fdtd_solver* s, double* out) {
     return FDTD_OK;
 }
 
-fdtd_status fdtd_solver_time_stencil(fdtd_solver* s, int32_t n_launches, float* elapsed_ms) {
-    if (!s || n_launches <= 0 || !elapsed_ms) return (set_error(s, "invalid arguments"), FDTD_ERR_INVALID_ARG);
+fdtd_status fdtd_solver_time_kernel(fdtd_solver* s, int32_t which, int32_t n_launches, float* elapsed_ms) {
+    if (!s || n_launches <= 0 || !elapsed_ms || which < 0 || which > 4)
+        return (set_error(s, "invalid arguments"), FDTD_ERR_INVALID_ARG);
+    if (which > 0 && s->opt.kernel != FDTD_KERNEL_FUSED)
+        return (set_error(s, "single-kernel timing needs the region-split (fused) path"), FDTD_ERR_INVALID_ARG);
     CUDA_TRY(s, cudaSetDevice(s->opt.device));
     cudaEvent_t e0, e1;
     CUDA_TRY(s, cudaEventCreate(&e0));
     CUDA_TRY(s, cudaEventCreate(&e1));
+    RegionLaunch R = s->region;
+    R.sources = 0;
+    if (which == 1) R.skip = 2 | 4;
+    if (which == 2) R.skip = 1 | 4;
+    if (which == 3) R.skip = 1 | 2;
     CUDA_TRY(s, cudaEventRecord(e0, s->stream));
     int c = s->cur;
     for (int i = 0; i < n_launches; ++i) {
         cudaError_t e;
-        if (s->precision == FDTD_PRECISION_FP64) {
+        if (which == 4) {
+            e = launch_listeners(s->dP, s->precision, c, s->L, s->d_lis, s->stream);
+        } else if (s->precision == FDTD_PRECISION_FP64) {
             if (s->opt.kernel == FDTD_KERNEL_PHASED) e = launch_phased_fp64(s->dP, s->N, c, s->d_lap, s->stream, nullptr);
             else if (s->opt.kernel == FDTD_KERNEL_STREAMING)
                 e = launch_step_fused_fp64(s->dP, s->N, c, s->tile_y, s->xchunk, s->stream);
-            else e = launch_step_regions_fp64(s->dP, s->hP, s->region, c, s->stream, s->stream2, s->ev_fork, s->ev_join, nullptr);
+            else e = launch_step_regions_fp64(s->dP, s->hP, R, c, s->stream, s->stream2, s->ev_fork, s->ev_join, nullptr);
         } else {
             if (s->opt.kernel == FDTD_KERNEL_STREAMING)
                 e = launch_step_fused_fp32(s->dP, s->N, c, s->tile_y, s->xchunk, s->stream);
-            else e = launch_step_regions_fp32(s->dP, s->hP, s->region, c, s->stream, s->stream2, s->ev_fork, s->ev_join, nullptr);
+            else e = launch_step_regions_fp32(s->dP, s->hP, R, c, s->stream, s->stream2, s->ev_fork, s->ev_join, nullptr);
         }
         if (e != cudaSuccess) {
             set_error(s, std::string("stencil launch: ") + cudaGetErrorString(e));
             return FDTD_ERR_CUDA;
         }
-        c ^= 1;
+        if (which != 4) c ^= 1;
     }
     CUDA_TRY(s, cudaEventRecord(e1, s->stream));
     CUDA_TRY(s, cudaEventSynchronize(e1));
@@ -321,6 +331,10 @@ fdtd_status fdtd_solver_time_stencil(fdtd_solver* s, int32_t n_launches, float* 
     cudaEventDestroy(e1);
     s->cur = c;
     return FDTD_OK;
+}
+
+fdtd_status fdtd_solver_time_stencil(fdtd_solver* s, int32_t n_launches, float* elapsed_ms) {
+    return fdtd_solver_time_kernel(s, 0, n_launches, elapsed_ms);
 }
 
 fdtd_status fdtd_solver_synchronize(fdtd_solver* s) {

@@ -100,6 +100,13 @@ class PML_WaveSolver:
         check(self._L.fdtd_solver_time_stencil(self._h, int(n_launches), C.byref(ms)), self._h)
         return float(ms.value)
 
+    def time_kernel(self, which: int, n_launches: int) -> float:
+        """Milliseconds for n launches of one part of the step: 0 step kernels,
+        1 interior, 2 PML shell, 3 ghost-cell list, 4 listeners (timing only)."""
+        ms = C.c_float(0.0)
+        check(self._L.fdtd_solver_time_kernel(self._h, int(which), int(n_launches), C.byref(ms)), self._h)
+        return float(ms.value)
+
     # ---- introspection ----
     def info(self) -> SolverInfo:
         info = SolverInfo()

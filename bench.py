@@ -166,7 +166,7 @@ def profile_run(args):
     sc = S.config2(n=args.profile_n)
     prec = S.PRECISION_FP32_COMPENSATED if args.precision == "fp32" else S.PRECISION_FP64
     kern = S.KERNEL_PHASED if args.precision == "fp64-plain" else S.KERNEL_FUSED
-    g = PML_WaveSolver(sc, precision=prec, kernel=kern)
+    g = PML_WaveSolver(sc, precision=prec, kernel=kern, tile_y=args.tile_y, x_chunk=args.x_chunk)
     y = g.step(3 + args.steps)
     g.close()
     print(json.dumps({"profile_run": sc.name, "cells": sc.n_cells, "steps": 3 + args.steps,
@@ -291,6 +291,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--profile", action="store_true", help="only run --steps steps of the bench solve (for ncu)")
     ap.add_argument("--profile-n", type=int, default=256, help="grid edge of the --profile solve")
+    ap.add_argument("--tile-y", type=int, default=0, help="PML-shell x planes per thread (1, 2, 4; 0 default)")
+    ap.add_argument("--x-chunk", type=int, default=0, help="interior x planes per thread (2, 4, 8; 0 default)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-scene batch (config 3)")
     ap.add_argument("--no-served", action="store_true", help="skip the serving stream (config 4)")
     ap.add_argument("--serve-rate", type=float, default=4.0)

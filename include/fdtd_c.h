@@ -129,7 +129,7 @@ typedef struct {
     int32_t device;           /* CUDA ordinal                                            */
     int32_t kernel;           /* FDTD_KERNEL_*                                           */
     int32_t graph_steps;      /* >0: capture this many steps per CUDA graph launch       */
-    int32_t tile_y;           /* fused path: PML-shell x planes per thread (1, 2); 0: default */
+    int32_t tile_y;           /* fused path: PML-shell x planes per thread (1, 2, 4); 0: default */
     int32_t x_chunk;          /* fused path: interior x planes per thread (2, 4, 8); 0: default */
     int32_t persistent_ctas;  /* batches: CTAs of the persistent kernels; 0: from occupancy    */
     int32_t _pad;
@@ -233,6 +233,12 @@ int64_t fdtd_solver_last_launch_count(fdtd_solver* s);
  * milliseconds.  The solver state is left advanced by those launches; use a solver
  * created for measurement. */
 fdtd_status fdtd_solver_time_stencil(fdtd_solver* s, int32_t n_launches, float* elapsed_ms);
+/* CUDA-event time of n back-to-back launches of one part of the step on the
+ * solver stream: which = 0 the step kernels (as fdtd_solver_time_stencil),
+ * 1 the interior kernel, 2 the PML-shell kernel, 3 the ghost-cell list kernel,
+ * 4 the listener kernel.  Parts 1-4 need FDTD_KERNEL_FUSED.  The fields are
+ * left in an unspecified state (timing only). */
+fdtd_status fdtd_solver_time_kernel(fdtd_solver* s, int32_t which, int32_t n_launches, float* elapsed_ms);
 
 /* Interior leapfrog step that allocates nothing.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc where they step
