@@ -265,6 +265,11 @@ fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
         s->bmax[d] += s->h * (double)s->N[d];
     }
     s->ncell = (long long)s->N[0] * s->N[1] * s->N[2];
+    // padded layout shared by cells and the three face grids: rows of Nz+1
+    // rounded up to 8 elements, Ny+1 rows per plane, Nx+1 planes
+    s->SY = ((long long)s->N[2] + 1 + 7) / 8 * 8;
+    s->SX = ((long long)s->N[1] + 1) * s->SY;
+    s->np = ((long long)s->N[0] + 1) * s->SX;
     const double w = sc->pml_width * s->h;  // setPMLBoundaryWidth (MAC_Grid.cpp:146-150)
     const double S = sc->pml_strength;
     const double one_over_k = 1.0 / s->k;
@@ -382,7 +387,7 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
 // needs the geometry (solver_init_geometry) and the listener list.
 static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_options& o, Carver& cv) {
     const size_t w = s->precision == FDTD_PRECISION_FP64 ? 8 : 4;
-    const long long n = s->ncell;
+    const long long n = s->np;  // every array uses the padded layout
     const int* N = s->N;
     SolveParams& P = s->hP;
     std::memset(&P, 0, sizeof(P));
@@ -394,10 +399,9 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
     if (s->precision != FDTD_PRECISION_FP64) cv.add((void**)&P.dinc, n * 4);
     for (int d = 0; d < 3; ++d) cv.add(&P.pd[d], n * w);
     for (int d = 0; d < 3; ++d) {
-        const long long nf = (long long)(N[0] + (d == 0)) * (N[1] + (d == 1)) * (N[2] + (d == 2));
-        s->vcount[d] = nf;
-        cv.add(&P.v[0][d], nf * w);
-        if (o.kernel != FDTD_KERNEL_PHASED) cv.add(&P.v[1][d], nf * w);  // double-buffered faces
+        s->vcount[d] = (long long)(N[0] + (d == 0)) * (N[1] + (d == 1)) * (N[2] + (d == 2));  // dense face count
+        cv.add(&P.v[0][d], n * w);
+        if (o.kernel != FDTD_KERNEL_PHASED) cv.add(&P.v[1][d], n * w);  // double-buffered faces
     }
     if (o.kernel == FDTD_KERNEL_PHASED) cv.add((void**)&s->d_lap, n * 8);
     cv.add((void**)&P.consts, 2 * sizeof(StepConsts));
@@ -483,6 +487,8 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     if (opt) o = *opt;
     if (o.precision != FDTD_PRECISION_FP64 && o.precision != FDTD_PRECISION_FP32_COMPENSATED)
         return (set_error(nullptr, "unknown precision"), FDTD_ERR_INVALID_ARG);
+    if (o.kernel != FDTD_KERNEL_FUSED && o.kernel != FDTD_KERNEL_PHASED)
+        return (set_error(nullptr, "unknown kernel path"), FDTD_ERR_INVALID_ARG);
     if (o.kernel == FDTD_KERNEL_PHASED && o.precision != FDTD_PRECISION_FP64)
         return (set_error(nullptr, "the phased kernel path is FP64 only"), FDTD_ERR_INVALID_ARG);
     if (o.graph_steps < 0 || (o.graph_steps % 2) != 0)
@@ -501,6 +507,12 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
     solver_init_geometry(s.get(), sc);
+    if (s->np >= (1LL << 31)) {
+        set_error(nullptr, "grid too large: cell indices are 32-bit (padded cells >= 2^31)");
+        cudaStreamDestroy(s->stream);
+        cudaStreamDestroy(s->stream2);
+        return FDTD_ERR_UNSUPPORTED;
+    }
     for (int i = 0; i < sc->n_objects; ++i) {
         HostObject h;
         h.d = sc->objects[i];
@@ -533,6 +545,7 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     s->arena = base;
     s->arena_bytes = cv.off;
     for (auto& r : cv.req) *r.first = (char*)base + r.second;
+    const long long ncell = s->ncell;
 
     // ---- constants ----
     for (int d = 0; d < 3; ++d) {
@@ -541,7 +554,10 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         for (int e2 = 0; e2 < 3; ++e2) P.vN[d][e2] = N[e2] + (d == e2 ? 1 : 0);
         P.vcount[d] = s->vcount[d];
     }
-    P.ncell = n;
+    P.ncell = ncell;
+    P.SX = s->SX;
+    P.SY = s->SY;
+    P.np = s->np;
     P.h = s->h;
     P.inv_h = 1.0 / s->h;
     P.rho = s->rho;
@@ -648,23 +664,12 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     if (s->L > 0)
         CUDA_TRY(s.get(), cudaMemcpy((void*)P.listeners, s->listeners.data(), s->listeners.size() * 8, cudaMemcpyHostToDevice));
     CUDA_TRY(s.get(), cudaMallocHost((void**)&s->h_lis_stage, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8));
-    // tile choice: 8 rows; x chunk so that the grid has >= 4 waves on 148 SMs
-    s->tile_y = o.tile_y > 0 ? o.tile_y : 8;
     s->xb = (o.x_chunk == 2 || o.x_chunk == 4 || o.x_chunk == 8) ? o.x_chunk : 4;
     s->region.xb = s->xb;
-    // tile_y selects the PML-shell planes per thread (1 or 2) of the fused path
+    // tile_y selects the PML-shell planes per thread (1, 2 or 4) of the fused path
     if (o.kernel == FDTD_KERNEL_FUSED && (o.tile_y == 1 || o.tile_y == 2 || o.tile_y == 4))
         build_shell_boxes(s.get(), o.tile_y);
     s->region.shell = s->shell;
-    if (o.x_chunk > 0) s->xchunk = o.x_chunk;
-    else {
-        const long long cols = (long long)((N[2] + 31) / 32) * ((N[1] + s->tile_y - 1) / s->tile_y);
-        long long chunks = (148LL * 8 + cols - 1) / cols;
-        if (chunks < 1) chunks = 1;
-        int xc = (int)((N[0] + chunks - 1) / chunks);
-        if (xc < 4) xc = 4;
-        s->xchunk = xc;
-    }
     st = fdtd_solver_reset(s.get(), sc->start_time);
     if (st != FDTD_OK) return st;
     *out = s.release();
@@ -695,18 +700,19 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     CUDA_TRY(s, cudaSetDevice(s->opt.device));
     SolveParams& P = s->hP;
     const size_t w = s->precision == FDTD_PRECISION_FP64 ? 8 : 4;
-    // zero all state (fields, velocities, split pressures, flags)
-    CUDA_TRY(s, cudaMemsetAsync(P.p[0], 0, s->ncell * w, s->stream));
-    CUDA_TRY(s, cudaMemsetAsync(P.p[1], 0, s->ncell * w, s->stream));
-    if (P.dinc) CUDA_TRY(s, cudaMemsetAsync(P.dinc, 0, s->ncell * 4, s->stream));
+    // zero all state (fields, velocities, split pressures, flags; padding included)
+    const long long np = s->np;
+    CUDA_TRY(s, cudaMemsetAsync(P.p[0], 0, np * w, s->stream));
+    CUDA_TRY(s, cudaMemsetAsync(P.p[1], 0, np * w, s->stream));
+    if (P.dinc) CUDA_TRY(s, cudaMemsetAsync(P.dinc, 0, np * 4, s->stream));
     for (int d = 0; d < 3; ++d) {
-        CUDA_TRY(s, cudaMemsetAsync(P.pd[d], 0, s->ncell * w, s->stream));
-        CUDA_TRY(s, cudaMemsetAsync(P.v[0][d], 0, s->vcount[d] * w, s->stream));
-        if (P.v[1][d]) CUDA_TRY(s, cudaMemsetAsync(P.v[1][d], 0, s->vcount[d] * w, s->stream));
+        CUDA_TRY(s, cudaMemsetAsync(P.pd[d], 0, np * w, s->stream));
+        CUDA_TRY(s, cudaMemsetAsync(P.v[0][d], 0, np * w, s->stream));
+        if (P.v[1][d]) CUDA_TRY(s, cudaMemsetAsync(P.v[1][d], 0, np * w, s->stream));
     }
     // initFieldRasterized: every cell bulk with valid history (MAC_Grid.cpp:2459-2470, :4170-4180)
-    CUDA_TRY(s, cudaMemsetAsync(P.cls, CLS_BULK | CLS_VALID, s->ncell, s->stream));
-    CUDA_TRY(s, cudaMemsetAsync(P.gobj, GOBJ_NONE, s->ncell, s->stream));
+    CUDA_TRY(s, cudaMemsetAsync(P.cls, CLS_BULK | CLS_VALID, np, s->stream));
+    CUDA_TRY(s, cudaMemsetAsync(P.gobj, GOBJ_NONE, np, s->stream));
     CUDA_TRY(s, cudaMemsetAsync(P.consts, 0, 2 * sizeof(StepConsts), s->stream));
     CUDA_TRY(s, cudaMemsetAsync(P.dev_error, 0, sizeof(int), s->stream));
     CUDA_TRY(s, cudaMemsetAsync(s->d_status, 0, 16, s->stream));
@@ -731,20 +737,20 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     if (st != FDTD_OK) return st;
     // ResetCellHistory(true): every cell has a valid history after reset
     // (the classification kernels keep it in bit 6; re-set it on all cells)
-    std::vector<uint8_t> cls(s->ncell);
-    CUDA_TRY(s, cudaMemcpyAsync(cls.data(), P.cls, s->ncell, cudaMemcpyDeviceToHost, s->stream));
+    std::vector<uint8_t> cls(np);
+    CUDA_TRY(s, cudaMemcpyAsync(cls.data(), P.cls, np, cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     std::vector<int> solid_pml;
-    for (long long c = 0; c < s->ncell; ++c) {
-        cls[c] |= CLS_VALID;
-        if (!(cls[c] & CLS_BULK)) {
-            const int i = (int)(c / ((long long)s->N[1] * s->N[2]));
-            const int j = (int)((c / s->N[2]) % s->N[1]);
-            const int k = (int)(c % s->N[2]);
-            if (s->tab[0].pml_cell[i] || s->tab[1].pml_cell[j] || s->tab[2].pml_cell[k]) solid_pml.push_back((int)c);
-        }
-    }
-    CUDA_TRY(s, cudaMemcpy(P.cls, cls.data(), s->ncell, cudaMemcpyHostToDevice));
+    for (int i = 0; i < s->N[0]; ++i)
+        for (int j = 0; j < s->N[1]; ++j)
+            for (int k = 0; k < s->N[2]; ++k) {
+                const long long c = i * s->SX + j * s->SY + k;
+                cls[c] |= CLS_VALID;
+                if (!(cls[c] & CLS_BULK) &&
+                    (s->tab[0].pml_cell[i] || s->tab[1].pml_cell[j] || s->tab[2].pml_cell[k]))
+                    solid_pml.push_back((int)c);
+            }
+    CUDA_TRY(s, cudaMemcpy(P.cls, cls.data(), np, cudaMemcpyHostToDevice));
     if (s->d_solid_pml) {
         cudaFree(s->d_solid_pml);
         s->d_solid_pml = nullptr;

@@ -1,8 +1,14 @@
 // fdtd_device.cuh — device-side data layout and helpers shared by the FP64 and
 // FP32 kernel translation units.
 //
-// HBM layout of one solve (all arrays 256-byte aligned, flat index
-// i*Ny*Nz + j*Nz + k, z contiguous as in ScalarField.cpp:86-97):
+// HBM layout of one solve.  Every array (cells and the three face grids) uses
+// one padded index  i*SX + j*SY + k  with z contiguous (the reference's order,
+// ScalarField.cpp:86-97), SY = Nz+1 rounded up to 8 elements and
+// SX = (Ny+1)*SY, over Nx+1 planes: a cell and its three low faces share an
+// index, the high faces are +SX, +SY, +1, rows start on 32-byte boundaries and
+// 16-byte vector accesses along z are aligned at k = 0 mod 4 (FP32) / 2 (FP64).
+// Arrays are 256-byte aligned; indices returned through the C-ABI are the
+// reference's dense i*Ny*Nz + j*Nz + k.
 //   cls[N]      u8   bit7 bulk, bit6 valid history, bits0-5 solid-neighbour mask
 //                    (bit 2d: -d side, bit 2d+1: +d side)
 //   gobj[N]     u8   for solid cells: closest object (LowestObjectDistance) | 0x80 constraint
@@ -100,7 +106,7 @@ struct alignas(4 * sizeof(T)) AxisCoef {
 template <typename T>
 struct KArgs {
     int N0, N1, N2;
-    unsigned sx;                  // N1*N2
+    unsigned sx, sy;              // padded plane and row strides (elements)
     const T* pc;                  // p^n
     T* pn;                        // p^{n+1} (FP64: also p^{n-1} in place)
     float* dinc;                  // FP32 increment
@@ -138,7 +144,9 @@ struct StepConsts {
 struct SolveParams {
     int N[3];
     int vN[3][3];         // velocity grid divisions per face orientation
-    long long ncell;
+    long long ncell;      // Nx*Ny*Nz
+    long long SX, SY;     // padded strides of every array (elements)
+    long long np;         // elements per array: (Nx+1)*SX
     long long vcount[3];
     double h, inv_h, rho, c, k;
     double c2k2;          // (c k)^2
@@ -194,7 +202,8 @@ inline KArgs<double> make_kargs<double>(SolveParams* dP, const SolveParams& P, i
     A.cur = cur;
     A.advance = 1;
     A.N0 = P.N[0]; A.N1 = P.N[1]; A.N2 = P.N[2];
-    A.sx = (unsigned)P.N[1] * P.N[2];
+    A.sx = (unsigned)P.SX;
+    A.sy = (unsigned)P.SY;
     A.pc = (const double*)P.p[cur];
     A.pn = (double*)P.p[cur ^ 1];
     A.dinc = P.dinc;
@@ -217,7 +226,8 @@ inline KArgs<float> make_kargs<float>(SolveParams* dP, const SolveParams& P, int
     A.cur = cur;
     A.advance = 1;
     A.N0 = P.N[0]; A.N1 = P.N[1]; A.N2 = P.N[2];
-    A.sx = (unsigned)P.N[1] * P.N[2];
+    A.sx = (unsigned)P.SX;
+    A.sy = (unsigned)P.SY;
     A.pc = (const float*)P.p[cur];
     A.pn = (float*)P.p[cur ^ 1];
     A.dinc = P.dinc;
@@ -276,6 +286,26 @@ struct BatchLaunch {
     int ghost_blocks;            // per member
     int src_blocks;              // per member (0: no member has a source)
 };
+
+// padded index of cell (or low face) (i, j, k)
+__host__ __device__ __forceinline__ long long cidx(const SolveParams& P, int i, int j, int k) {
+    return i * P.SX + j * P.SY + k;
+}
+// (i, j, k) of a padded index
+__host__ __device__ __forceinline__ void cell_ijk(const SolveParams& P, long long c, int& i, int& j, int& k) {
+    i = (int)(c / P.SX);
+    const long long r = c - i * P.SX;
+    j = (int)(r / P.SY);
+    k = (int)(r - j * P.SY);
+}
+// (i, j, k) of the dense (reference) index t
+__host__ __device__ __forceinline__ void dense_ijk(const SolveParams& P, long long t, int& i, int& j, int& k) {
+    const long long yz = (long long)P.N[1] * P.N[2];
+    i = (int)(t / yz);
+    const long long r = t - i * yz;
+    j = (int)(r / P.N[2]);
+    k = (int)(r - (long long)j * P.N[2]);
+}
 
 // consts[cur^1] <- the next step's constants (PML_WaveSolver.cpp:825,
 // _currentTime += _timeStep; source time factors at t + k/2).

@@ -15,24 +15,6 @@ cudaError_t launch_prologue_fp32(const SolveParams* dP, int cur, int advance, in
     return cudaGetLastError();
 }
 
-template <int BY>
-static cudaError_t launch_fused_by(const SolveParams* dP, const int N[3], int cur, int xchunk, cudaStream_t s) {
-    dim3 block(32, BY);
-    dim3 grid((N[2] + 31) / 32, (N[1] + BY - 1) / BY, (N[0] + xchunk - 1) / xchunk);
-    k_step_fused<float, BY><<<grid, block, 0, s>>>(dP, cur, xchunk);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_step_fused_fp32(const SolveParams* dP, const int N[3], int cur, int tile_y, int xchunk,
-                                   cudaStream_t s) {
-    switch (tile_y) {
-        case 2: return launch_fused_by<2>(dP, N, cur, xchunk, s);
-        case 4: return launch_fused_by<4>(dP, N, cur, xchunk, s);
-        case 16: return launch_fused_by<16>(dP, N, cur, xchunk, s);
-        default: return launch_fused_by<8>(dP, N, cur, xchunk, s);
-    }
-}
-
 }  // namespace fdtd
 
 #include "fdtd_hot.cuh"

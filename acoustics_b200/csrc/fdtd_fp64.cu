@@ -19,9 +19,13 @@ namespace fdtd {
 
 // validHistory <- isBulk; isBulk <- true (MAC_Grid.cpp:3464-3472)
 __global__ void k_cls_reset(const SolveParams* __restrict__ Pp, long long n) {
-    uint8_t* cls = Pp->cls;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *Pp->ghost_count = 0;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    const SolveParams& P = *Pp;
+    uint8_t* cls = P.cls;
+    if (blockIdx.x == 0 && threadIdx.x == 0) *P.ghost_count = 0;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        dense_ijk(P, t, i, j, k);
+        const long long c = cidx(P, i, j, k);
         const uint8_t code = cls[c];
         cls[c] = CLS_BULK | ((code & CLS_BULK) ? CLS_VALID : 0);
     }
@@ -37,7 +41,7 @@ __global__ void k_cls_solid(const SolveParams* __restrict__ Pp, int s0, int s1, 
         const int i = s0 + (int)(t / ((long long)r1 * r2));
         const int j = s1 + (int)((t / r2) % r1);
         const int k = s2 + (int)(t % r2);
-        const long long c = ((long long)i * P.N[1] + j) * P.N[2] + k;
+        const long long c = cidx(P, i, j, k);
         const double pos[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
         int type = 0;
         if (!is_fluid(P, pos, type)) {
@@ -61,13 +65,12 @@ __global__ void k_cls_solid(const SolveParams* __restrict__ Pp, int s0, int s1, 
 // directions of its solid (ghost) neighbours, read by the Laplacian.
 __global__ void k_cls_ghost(const SolveParams* __restrict__ Pp, long long n) {
     const SolveParams& P = *Pp;
-    const long long sx = (long long)P.N[1] * P.N[2];
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(c / sx);
-        const int j = (int)((c / P.N[2]) % P.N[1]);
-        const int k = (int)(c % P.N[2]);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        dense_ijk(P, t, i, j, k);
+        const long long c = cidx(P, i, j, k);
         const int idx[3] = {i, j, k};
-        const long long strides[3] = {sx, P.N[2], 1};
+        const long long strides[3] = {P.SX, P.SY, 1};
         const uint8_t code = P.cls[c];
         const bool bulk = code & CLS_BULK;
         unsigned mask = 0;
@@ -106,8 +109,8 @@ __device__ double fresh_value(const SolveParams& P, const T* __restrict__ pa, co
                               long long c, double t, int* status) {
     // value of buffer "a" (or a - b when diff) at cell n
     auto val = [&](long long n) -> double { return diff ? (double)pa[n] - (double)pb[n] : (double)pa[n]; };
-    const long long sx = (long long)P.N[1] * P.N[2];
-    const int i = (int)(c / sx), j = (int)((c / P.N[2]) % P.N[1]), k = (int)(c % P.N[2]);
+    int i, j, k;
+    cell_ijk(P, c, i, j, k);
     const double cp[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
     double distance = DBL_MAX;
     const int oid = lowest_object(P, cp, &distance);
@@ -126,7 +129,8 @@ __device__ double fresh_value(const SolveParams& P, const T* __restrict__ pa, co
     for (int q = 0; q < nc; ++q) {
         const int n = cells[q];
         if (!(P.cls[n] & CLS_VALID)) continue;
-        const int ni = n / (int)sx, nj = (n / P.N[2]) % P.N[1], nn = n % P.N[2];
+        int ni, nj, nn;
+        cell_ijk(P, n, ni, nj, nn);
         const double np_[3] = {P.cpos[0][ni], P.cpos[1][nj], P.cpos[2][nn]};
         mls_row(image, np_, val(n), &A[nk * 4], b[nk]);
         kept[nk++] = n;
@@ -137,7 +141,8 @@ __device__ double fresh_value(const SolveParams& P, const T* __restrict__ pa, co
             int mid = -1;
             for (int q = 0; q < nk; ++q) {
                 const int n = kept[q];
-                const int ni = n / (int)sx, nj = (n / P.N[2]) % P.N[1], nn = n % P.N[2];
+                int ni, nj, nn;
+                cell_ijk(P, n, ni, nj, nn);
                 const double dx = image[0] - P.cpos[0][ni], dy = image[1] - P.cpos[1][nj], dz = image[2] - P.cpos[2][nn];
                 const double d2 = dx * dx + dy * dy + dz * dz;
                 if (d2 < md) { md = d2; mid = n; }
@@ -145,7 +150,7 @@ __device__ double fresh_value(const SolveParams& P, const T* __restrict__ pa, co
             return val(mid);
         }
         const int idx[3] = {i, j, k};
-        const long long strides[3] = {sx, P.N[2], 1};
+        const long long strides[3] = {P.SX, P.SY, 1};
         for (int d = 0; d < 3; ++d)
             for (int s = 1; s >= -1; s -= 2) {
                 if (idx[d] + s < 0 || idx[d] + s >= P.N[d]) continue;
@@ -166,7 +171,10 @@ template <typename T>
 __global__ void k_fresh_cells(const SolveParams* __restrict__ Pp, int cur, long long n, int* status) {
     const SolveParams& P = *Pp;
     const double t = P.consts[cur].t;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        dense_ijk(P, q, i, j, k);
+        const long long c = cidx(P, i, j, k);
         const uint8_t code = P.cls[c];
         if (!(code & CLS_BULK) || (code & CLS_VALID)) continue;
         int st = 0;
@@ -209,23 +217,23 @@ __global__ void k_phase_velocity(const SolveParams* __restrict__ Pp, int cur, in
         for (int d = 0; d < 3; ++d)
             if (d != dim) inpml = inpml || P.pml_cell[d][a[d]] != 0;
         if (!inpml) continue;
-        const long long pr = ((long long)a[0] * P.N[1] + a[1]) * P.N[2] + a[2];
-        a[dim] -= 1;
-        const long long pl = ((long long)a[0] * P.N[1] + a[1]) * P.N[2] + a[2];
-        v[f] = vel_update<double>(v[f], P.vupd[dim][a[dim] + 1], P.vgrad[dim][a[dim] + 1], p[pr], p[pl]);
+        const long long pr = cidx(P, a[0], a[1], a[2]);  // also the face index
+        const long long pl = pr - (dim == 0 ? P.SX : (dim == 1 ? P.SY : 1));
+        v[pr] = vel_update<double>(v[pr], P.vupd[dim][a[dim]], P.vgrad[dim][a[dim]], p[pr], p[pl]);
     }
 }
 
 __global__ void k_phase_laplacian(const SolveParams* __restrict__ Pp, int cur, double* __restrict__ lap) {
     const SolveParams& P = *Pp;
     const double* p = (const double*)P.p[cur];
-    const long long sx = (long long)P.N[1] * P.N[2];
     const double t = P.consts[cur].t;
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.ncell; c += (long long)gridDim.x * blockDim.x) {
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P.ncell; q += (long long)gridDim.x * blockDim.x) {
+        int idx[3];
+        dense_ijk(P, q, idx[0], idx[1], idx[2]);
+        const long long c = cidx(P, idx[0], idx[1], idx[2]);
         const uint8_t code = P.cls[c];
         if (!(code & CLS_BULK)) { lap[c] = 0.0; continue; }
-        const int idx[3] = {(int)(c / sx), (int)((c / P.N[2]) % P.N[1]), (int)(c % P.N[2])};
-        const long long strides[3] = {sx, P.N[2], 1};
+        const long long strides[3] = {P.SX, P.SY, 1};
         const unsigned mask = code & CLS_MASK;
         double L = 0.0;
         int surrounded = 0;
@@ -265,7 +273,6 @@ __global__ void k_phase_pressure(const SolveParams* __restrict__ Pp, int cur, co
     const SolveParams& P = *Pp;
     const double* pc = (const double*)P.p[cur];
     double* pn = (double*)P.p[cur ^ 1];
-    const long long sx = (long long)P.N[1] * P.N[2];
     const StepConsts sc = P.consts[cur];
     bool any_src = false;
     for (int s = 0; s < P.n_src; ++s) any_src |= (sc.src_tf[s] != 0.0);
@@ -275,15 +282,15 @@ __global__ void k_phase_pressure(const SolveParams* __restrict__ Pp, int cur, co
     double* pd0 = (double*)P.pd[0];
     double* pd1 = (double*)P.pd[1];
     double* pd2 = (double*)P.pd[2];
-    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < P.ncell; c += (long long)gridDim.x * blockDim.x) {
-        const int i = (int)(c / sx), j = (int)((c / P.N[2]) % P.N[1]), k = (int)(c % P.N[2]);
+    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < P.ncell; q += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        dense_ijk(P, q, i, j, k);
+        const long long c = cidx(P, i, j, k);  // the cell and its three low faces
         const bool pml = P.pml_cell[0][i] || P.pml_cell[1][j] || P.pml_cell[2][k];
         if (pml) {
-            const long long f0 = c, f1 = ((long long)i * (P.N[1] + 1) + j) * P.N[2] + k,
-                            f2 = ((long long)i * P.N[1] + j) * (P.N[2] + 1) + k;
-            const double a = pd_update<double>(pd0[c], P.pupd[0][i], P.pdiv[0][i], v0[f0 + sx], v0[f0], P.inv_h);
-            const double b = pd_update<double>(pd1[c], P.pupd[1][j], P.pdiv[1][j], v1[f1 + P.N[2]], v1[f1], P.inv_h);
-            const double d = pd_update<double>(pd2[c], P.pupd[2][k], P.pdiv[2][k], v2[f2 + 1], v2[f2], P.inv_h);
+            const double a = pd_update<double>(pd0[c], P.pupd[0][i], P.pdiv[0][i], v0[c + P.SX], v0[c], P.inv_h);
+            const double b = pd_update<double>(pd1[c], P.pupd[1][j], P.pdiv[1][j], v1[c + P.SY], v1[c], P.inv_h);
+            const double d = pd_update<double>(pd2[c], P.pupd[2][k], P.pdiv[2][k], v2[c + 1], v2[c], P.inv_h);
             pd0[c] = a;
             pd1[c] = b;
             pd2[c] = d;
@@ -327,24 +334,6 @@ cudaError_t launch_prologue_fp64(const SolveParams* dP, int cur, int advance, in
 cudaError_t launch_consts_init(const SolveParams* dP, double t0, cudaStream_t s) {
     k_consts_init<<<1, 32, 0, s>>>(dP, t0);
     return cudaGetLastError();
-}
-
-template <int BY>
-static cudaError_t launch_fused_by(const SolveParams* dP, const int N[3], int cur, int xchunk, cudaStream_t s) {
-    dim3 block(32, BY);
-    dim3 grid((N[2] + 31) / 32, (N[1] + BY - 1) / BY, (N[0] + xchunk - 1) / xchunk);
-    k_step_fused<double, BY><<<grid, block, 0, s>>>(dP, cur, xchunk);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_step_fused_fp64(const SolveParams* dP, const int N[3], int cur, int tile_y, int xchunk,
-                                   cudaStream_t s) {
-    switch (tile_y) {
-        case 2: return launch_fused_by<2>(dP, N, cur, xchunk, s);
-        case 4: return launch_fused_by<4>(dP, N, cur, xchunk, s);
-        case 16: return launch_fused_by<16>(dP, N, cur, xchunk, s);
-        default: return launch_fused_by<8>(dP, N, cur, xchunk, s);
-    }
 }
 
 cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int n_lis, double* out_row,

@@ -151,7 +151,7 @@ FDTD_HD int enclosing_neighbours(const SolveParams& P, const double x[3], int ou
     for (int i = 0; i < 2; ++i)
         for (int j = 0; j < 2; ++j)
             for (int l = 0; l < 2; ++l) {
-                const int ci = (i ? a1[0] : a0[0]) * (P.N[1] * P.N[2]) + (j ? a1[1] : a0[1]) * P.N[2] + (l ? a1[2] : a0[2]);
+                const int ci = (int)cidx(P, i ? a1[0] : a0[0], j ? a1[1] : a0[1], l ? a1[2] : a0[2]);
                 int pos = 0;
                 while (pos < n && out[pos] < ci) ++pos;
                 if (pos < n && out[pos] == ci) continue;

@@ -50,9 +50,9 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
     const int zc = min(z, box.hi[2] - 1);
     const int yc = min(y, box.hi[1] - 1);
     const int nx = min(XB, box.hi[0] - x0);
-    const int Nz = A.N2;
+    const int sy = (int)A.sy;
     const int sx = (int)A.sx;
-    const unsigned off = (unsigned)x0 * A.sx + (unsigned)yc * Nz + zc;
+    const unsigned off = (unsigned)x0 * A.sx + (unsigned)yc * A.sy + zc;
     const T* __restrict__ pc = A.pc + off;
     T* __restrict__ pn = A.pn + off;
     float* __restrict__ dinc = A.dinc + off;
@@ -68,8 +68,8 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
 #pragma unroll
     for (int i = 0; i < XB; ++i) {
         if (i < nx) {
-            ym[i] = pc[i * sx - Nz];
-            yp[i] = pc[i * sx + Nz];
+            ym[i] = pc[i * sx - sy];
+            yp[i] = pc[i * sx + sy];
             if constexpr (COMP) prev[i] = (T)dinc[i * sx];
             else prev[i] = pn[i * sx];
             code[i] = cls[i * sx];
@@ -121,16 +121,11 @@ __device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& 
     const int y = B.y0[b] + yy;
     const int xbeg = B.x0[b] + tx * XS;
     const int nxh = min(XS, B.x0[b] + B.nx[b] - xbeg);
-    const int N1 = A.N1, N2 = A.N2;
-    const unsigned sx = A.sx;
-    const unsigned sy1 = (unsigned)(N1 + 1) * N2;  // x stride of the y-face grid
-    const unsigned sz2 = (unsigned)N1 * (N2 + 1);  // x stride of the z-face grid
-    const unsigned c0 = (unsigned)xbeg * sx + (unsigned)y * N2 + z;
-    const unsigned fy0 = (unsigned)xbeg * sy1 + (unsigned)y * N2 + z;
-    const unsigned fz0 = (unsigned)xbeg * sz2 + (unsigned)y * (N2 + 1) + z;
+    const unsigned sx = A.sx, sy = A.sy;
+    const unsigned c0 = (unsigned)xbeg * sx + (unsigned)y * sy + z;  // cell and its three low faces
     const uint8_t gy = __ldg(A.axflag[1] + y), gz = __ldg(A.axflag[2] + z);
     const bool pmly = gy & AXF_PML, pmlz = gz & AXF_PML;
-    const unsigned oym = (gy & AXF_HAS_LO) ? (unsigned)N2 : 0u, oyp = (gy & AXF_HAS_HI) ? (unsigned)N2 : 0u;
+    const unsigned oym = (gy & AXF_HAS_LO) ? sy : 0u, oyp = (gy & AXF_HAS_HI) ? sy : 0u;
     const unsigned ozm = (gz & AXF_HAS_LO) ? 1u : 0u, ozp = (gz & AXF_HAS_HI) ? 1u : 0u;
 
     // ---- loads of all XS planes ----
@@ -152,10 +147,10 @@ __device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& 
             zp[i] = A.pc[c + ozp];
             vxl[i] = A.vo[0][c];
             vxr[i] = A.vo[0][c + sx];
-            vyl[i] = A.vo[1][fy0 + i * sy1];
-            vyr[i] = A.vo[1][fy0 + i * sy1 + N2];
-            vzl[i] = A.vo[2][fz0 + i * sz2];
-            vzr[i] = A.vo[2][fz0 + i * sz2 + 1];
+            vyl[i] = A.vo[1][c];
+            vyr[i] = A.vo[1][c + sy];
+            vzl[i] = A.vo[2][c];
+            vzr[i] = A.vo[2][c + 1];
             a0[i] = A.pd[0][c];
             a1[i] = A.pd[1][c];
             a2[i] = A.pd[2][c];
@@ -170,7 +165,6 @@ __device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& 
         if (i >= nxh) break;
         const int x = xbeg + i;
         const unsigned c = c0 + i * sx;
-        const unsigned fy = fy0 + i * sy1, fz = fz0 + i * sz2;
         const uint8_t g = gx[i];
         const bool pmlx = g & AXF_PML;
         // faces inside the PML (InsidePML at the face position, MAC_Grid.cpp:2631-2633),
@@ -197,19 +191,19 @@ __device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& 
         }
         if (fyl) {
             vyl_ = vel_update<T>(vyl_, cyl.vupd, cyl.vgrad, p0, ym[i]);
-            A.vn[1][fy] = vyl_;
+            A.vn[1][c] = vyl_;
         }
         if (fyr) {
             vyr_ = vel_update<T>(vyr_, cyr.vupd, cyr.vgrad, yp[i], p0);
-            if (!((gy & AXF_NEXT_PML) || oxz)) A.vn[1][fy + N2] = vyr_;
+            if (!((gy & AXF_NEXT_PML) || oxz)) A.vn[1][c + sy] = vyr_;
         }
         if (fzl) {
             vzl_ = vel_update<T>(vzl_, czl.vupd, czl.vgrad, p0, zm[i]);
-            A.vn[2][fz] = vzl_;
+            A.vn[2][c] = vzl_;
         }
         if (fzr) {
             vzr_ = vel_update<T>(vzr_, czr.vupd, czr.vgrad, zp[i], p0);
-            if (!((gz & AXF_NEXT_PML) || oxy)) A.vn[2][fz + 1] = vzr_;
+            if (!((gz & AXF_NEXT_PML) || oxy)) A.vn[2][c + 1] = vzr_;
         }
         const T ax = pd_update<T>(a0[i], cxl.pupd, cxl.pdiv, vxr_, vxl_, A.inv_h);
         const T ay = pd_update<T>(a1[i], cyl.pupd, cyl.pdiv, vyr_, vyl_, A.inv_h);

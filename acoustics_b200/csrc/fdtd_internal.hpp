@@ -39,6 +39,7 @@ struct fdtd_solver {
     double h = 0, c = 0, rho = 0, k = 0, end_time = 0, start_time = 0;
     int N[3] = {0, 0, 0};
     long long ncell = 0, n_pml = 0, n_interior = 0;
+    long long SX = 0, SY = 0, np = 0;  // padded strides and elements per device array
     long long vcount[3] = {0, 0, 0};
     double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};
     fdtd::AxisTables tab[3];
@@ -60,7 +61,6 @@ struct fdtd_solver {
     double* d_lis = nullptr;
     double* h_lis_stage = nullptr;
     int lis_cap_steps = 0;
-    int tile_y = 8, xchunk = 16;
     int xb = 4;                       // planes per thread of the interior kernel
     fdtd::Box3 interior{};            // non-PML box
     fdtd::ShellBoxes shell{};         // PML shell boxes

@@ -27,8 +27,6 @@ int batch_blocks_per_sm(int precision, int which, int shape);
 // fdtd_fp64.cu (compiled with -fmad=false)
 cudaError_t launch_prologue_fp64(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s);
 cudaError_t launch_consts_init(const SolveParams* dP, double t0, cudaStream_t s);
-cudaError_t launch_step_fused_fp64(const SolveParams* dP, const int N[3], int cur, int tile_y, int xchunk,
-                                   cudaStream_t s);
 cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int n_lis, double* out_row,
                              cudaStream_t s);
 cudaError_t launch_cls_reset(const SolveParams* dP, long long ncell, cudaStream_t s);
@@ -43,7 +41,5 @@ cudaError_t launch_phased_fp64(const SolveParams* dP, const int N[3], int cur, d
 
 // fdtd_fp32.cu
 cudaError_t launch_prologue_fp32(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s);
-cudaError_t launch_step_fused_fp32(const SolveParams* dP, const int N[3], int cur, int tile_y, int xchunk,
-                                   cudaStream_t s);
 
 }  // namespace fdtd

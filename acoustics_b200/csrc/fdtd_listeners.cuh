@@ -39,9 +39,8 @@ __device__ __forceinline__ void kth_face(unsigned mask, int k, int& d, int& s) {
 template <typename T>
 __device__ void build_row(const SolveParams& P, const T* __restrict__ pold, double t, const double pt[3], int cell,
                           uint8_t code, double v, int k, double A[4], double& b) {
-    const int Nz = P.N[2], Ny = P.N[1];
-    const long long sx = (long long)Ny * Nz;
-    const int i = (int)(cell / sx), j = (int)((cell / Nz) % Ny), kk = (int)(cell % Nz);
+    int i, j, kk;
+    cell_ijk(P, cell, i, j, kk);
     const double cp[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][kk]};
     const unsigned mask = code & CLS_MASK;
     if ((code & CLS_BULK) || mask == 0) {
@@ -50,7 +49,7 @@ __device__ void build_row(const SolveParams& P, const T* __restrict__ pold, doub
     }
     int d, s;
     kth_face(mask, k, d, s);
-    const long long strides[3] = {sx, Nz, 1};
+    const long long strides[3] = {P.SX, P.SY, 1};
     const long long nbr = cell + s * strides[d];
     const double pg = ghost_pressure(P, P.gobj[cell], cp, d, s, (double)pold[nbr], t);
     double fp[3] = {cp[0], cp[1], cp[2]};
@@ -100,9 +99,8 @@ __device__ void listener_body(const SolveParams& P, int newp, int li, double* __
     if (nk < 4) {  // nearest kept cell centre (PML_WaveSolver.cpp:294-309)
         double d2 = DBL_MAX;
         if (kept) {
-            const int Nz = P.N[2], Ny = P.N[1];
-            const long long sx = (long long)Ny * Nz;
-            const int i = (int)(cellq / sx), j = (int)((cellq / Nz) % Ny), k = (int)(cellq % Nz);
+            int i, j, k;
+            cell_ijk(P, cellq, i, j, k);
             const double dx = P.cpos[0][i] - pt[0], dy = P.cpos[1][j] - pt[1], dz = P.cpos[2][k] - pt[2];
             d2 = dx * dx + dy * dy + dz * dz;
         }

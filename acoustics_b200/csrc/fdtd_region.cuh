@@ -34,7 +34,7 @@ namespace fdtd {
 template <typename T>
 __device__ __noinline__ T ghost_laplacian(const SolveParams& P, long long c, const int idx[3], unsigned mask, T p0,
                                           const T nbp[3], const T nbm[3], double t, int* surrounded) {
-    const long long strides[3] = {(long long)P.N[1] * P.N[2], P.N[2], 1};
+    const long long strides[3] = {P.SX, P.SY, 1};
     T lap = 0.0;
     int s = 0;
     for (int d = 0; d < 3; ++d) {
@@ -74,18 +74,18 @@ __device__ __noinline__ T ghost_laplacian(const SolveParams& P, long long c, con
 template <typename T>
 __device__ __forceinline__ void ghost_cells_body(const SolveParams& P, int cur, int bid, int nblocks) {
     const int n = *P.ghost_count;
-    const int Ny = P.N[1], Nz = P.N[2];
-    const long long sx = (long long)Ny * Nz;
+    const long long sx = P.SX, sy = P.SY;
     const T* __restrict__ pc = (const T*)P.p[cur];
     T* __restrict__ pn = (T*)P.p[cur ^ 1];
     const double t = P.consts[cur].t;
     for (int g = bid * blockDim.x + threadIdx.x; g < n && g < P.ghost_cap; g += nblocks * blockDim.x) {
         const long long c = P.ghost_list[g];
-        const int x = (int)(c / sx), y = (int)((c / Nz) % Ny), z = (int)(c % Nz);
+        int x, y, z;
+        cell_ijk(P, c, x, y, z);
         const uint8_t code = P.cls[c];
         const T p0 = pc[c];
-        const T nbp[3] = {pc[c + sx], pc[c + Nz], pc[c + 1]};
-        const T nbm[3] = {pc[c - sx], pc[c - Nz], pc[c - 1]};
+        const T nbp[3] = {pc[c + sx], pc[c + sy], pc[c + 1]};
+        const T nbm[3] = {pc[c - sx], pc[c - sy], pc[c - 1]};
         const int idx[3] = {x, y, z};
         int surrounded = 0;
         T lap = ghost_laplacian<T>(P, c, idx, code & CLS_MASK, p0, nbp, nbm, t, &surrounded);
@@ -111,14 +111,13 @@ __device__ __forceinline__ void sources_body(const SolveParams& P, int cur, cons
     if (!any_src) return;
     const int nx = region.hi[0] - region.lo[0], ny = region.hi[1] - region.lo[1], nz = region.hi[2] - region.lo[2];
     const long long total = (long long)nx * ny * nz;
-    const int Ny = P.N[1], Nz = P.N[2];
     const T* __restrict__ pc = (const T*)P.p[cur];
     T* __restrict__ pn = (T*)P.p[cur ^ 1];
     for (long long t = bid * (long long)blockDim.x + threadIdx.x; t < total; t += (long long)nblocks * blockDim.x) {
         const int z = region.lo[2] + (int)(t % nz);
         const int y = region.lo[1] + (int)((t / nz) % ny);
         const int x = region.lo[0] + (int)(t / ((long long)nz * ny));
-        const long long c = ((long long)x * Ny + y) * Nz + z;
+        const long long c = cidx(P, x, y, z);
         if (!(P.cls[c] & CLS_BULK)) continue;
         const double src = source_sum(P, sc, P.cpos[0][x], P.cpos[1][y], P.cpos[2][z]);
         if constexpr (sizeof(T) == 8) {

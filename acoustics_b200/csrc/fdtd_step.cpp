@@ -89,9 +89,6 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         int l = 0;
         if (s->opt.kernel == FDTD_KERNEL_PHASED) {
             CUDA_TRY(s, launch_phased_fp64(s->dP, s->N, cur, s->d_lap, s->stream, &l));
-        } else if (s->opt.kernel == FDTD_KERNEL_STREAMING) {
-            CUDA_TRY(s, launch_step_fused_fp64(s->dP, s->N, cur, s->tile_y, s->xchunk, s->stream));
-            l = 1;
         } else {
             CUDA_TRY(s, launch_step_regions_fp64(s->dP, s->hP, s->region, cur, s->stream, s->stream2, s->ev_fork, s->ev_join, &l));
         }
@@ -102,12 +99,7 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
             s->launches++;
         }
         int l = 0;
-        if (s->opt.kernel == FDTD_KERNEL_STREAMING) {
-            CUDA_TRY(s, launch_step_fused_fp32(s->dP, s->N, cur, s->tile_y, s->xchunk, s->stream));
-            l = 1;
-        } else {
-            CUDA_TRY(s, launch_step_regions_fp32(s->dP, s->hP, s->region, cur, s->stream, s->stream2, s->ev_fork, s->ev_join, &l));
-        }
+        CUDA_TRY(s, launch_step_regions_fp32(s->dP, s->hP, s->region, cur, s->stream, s->stream2, s->ev_fork, s->ev_join, &l));
         s->launches += l;
     }
     if (s->L > 0 && dev_row) {
@@ -310,13 +302,9 @@ fdtd_status fdtd_solver_time_kernel(fdtd_solver* s, int32_t which, int32_t n_lau
             e = launch_listeners(s->dP, s->precision, c, s->L, s->d_lis, s->stream);
         } else if (s->precision == FDTD_PRECISION_FP64) {
             if (s->opt.kernel == FDTD_KERNEL_PHASED) e = launch_phased_fp64(s->dP, s->N, c, s->d_lap, s->stream, nullptr);
-            else if (s->opt.kernel == FDTD_KERNEL_STREAMING)
-                e = launch_step_fused_fp64(s->dP, s->N, c, s->tile_y, s->xchunk, s->stream);
             else e = launch_step_regions_fp64(s->dP, s->hP, R, c, s->stream, s->stream2, s->ev_fork, s->ev_join, nullptr);
         } else {
-            if (s->opt.kernel == FDTD_KERNEL_STREAMING)
-                e = launch_step_fused_fp32(s->dP, s->N, c, s->tile_y, s->xchunk, s->stream);
-            else e = launch_step_regions_fp32(s->dP, s->hP, R, c, s->stream, s->stream2, s->ev_fork, s->ev_join, nullptr);
+            e = launch_step_regions_fp32(s->dP, s->hP, R, c, s->stream, s->stream2, s->ev_fork, s->ev_join, nullptr);
         }
         if (e != cudaSuccess) {
             set_error(s, std::string("stencil launch: ") + cudaGetErrorString(e));
@@ -369,10 +357,21 @@ fdtd_status fdtd_solver_info_get(fdtd_solver* s, fdtd_solver_info* info) {
 fdtd_status fdtd_solver_get_classification(fdtd_solver* s, uint8_t* flags, fdtd_ghost_face* faces, int64_t* n_faces) {
     if (!s) return FDTD_ERR_INVALID_ARG;
     CUDA_TRY(s, cudaSetDevice(s->opt.device));
-    std::vector<uint8_t> cls(s->ncell), gobj(s->ncell);
-    CUDA_TRY(s, cudaMemcpyAsync(cls.data(), s->hP.cls, s->ncell, cudaMemcpyDeviceToHost, s->stream));
-    CUDA_TRY(s, cudaMemcpyAsync(gobj.data(), s->hP.gobj, s->ncell, cudaMemcpyDeviceToHost, s->stream));
+    std::vector<uint8_t> pcls(s->np), pgobj(s->np);
+    CUDA_TRY(s, cudaMemcpyAsync(pcls.data(), s->hP.cls, s->np, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(pgobj.data(), s->hP.gobj, s->np, cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    // dense (reference) order and indices
+    std::vector<uint8_t> cls(s->ncell), gobj(s->ncell);
+    {
+        long long c = 0;
+        for (int i = 0; i < s->N[0]; ++i)
+            for (int j = 0; j < s->N[1]; ++j)
+                for (int k = 0; k < s->N[2]; ++k, ++c) {
+                    cls[c] = pcls[i * s->SX + j * s->SY + k];
+                    gobj[c] = pgobj[i * s->SX + j * s->SY + k];
+                }
+    }
     const long long sx = (long long)s->N[1] * s->N[2];
     int64_t count = 0;
     const int64_t cap = (faces && n_faces) ? *n_faces : 0;
@@ -435,19 +434,28 @@ fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, in
         default: return (set_error(s, "unknown field"), FDTD_ERR_INVALID_ARG);
     }
     if (count != n) return (set_error(s, "count does not match the field size"), FDTD_ERR_INVALID_ARG);
-    if (f64) {
-        CUDA_TRY(s, cudaMemcpyAsync(out, src, n * 8, cudaMemcpyDeviceToHost, s->stream));
-        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-        return FDTD_OK;
-    }
-    std::vector<float> tmp(n), inc;
-    CUDA_TRY(s, cudaMemcpyAsync(tmp.data(), src, n * w, cudaMemcpyDeviceToHost, s->stream));
-    if (which == FDTD_FIELD_PRESSURE_PREV) {
-        inc.resize(n);
-        CUDA_TRY(s, cudaMemcpyAsync(inc.data(), P.dinc, n * 4, cudaMemcpyDeviceToHost, s->stream));
+    // extent of the requested grid (cells, or faces of one orientation)
+    int ext[3] = {s->N[0], s->N[1], s->N[2]};
+    if (which >= FDTD_FIELD_VX) ext[which - FDTD_FIELD_VX] += 1;
+    const long long np = s->np;
+    std::vector<char> raw(np * w);
+    std::vector<float> inc;
+    CUDA_TRY(s, cudaMemcpyAsync(raw.data(), src, np * w, cudaMemcpyDeviceToHost, s->stream));
+    if (!f64 && which == FDTD_FIELD_PRESSURE_PREV) {
+        inc.resize(np);
+        CUDA_TRY(s, cudaMemcpyAsync(inc.data(), P.dinc, np * 4, cudaMemcpyDeviceToHost, s->stream));
     }
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-    for (long long i = 0; i < n; ++i) out[i] = inc.empty() ? (double)tmp[i] : (double)tmp[i] - (double)inc[i];
+    const double* r64 = (const double*)raw.data();
+    const float* r32 = (const float*)raw.data();
+    long long o = 0;
+    for (int i = 0; i < ext[0]; ++i)
+        for (int j = 0; j < ext[1]; ++j)
+            for (int k = 0; k < ext[2]; ++k, ++o) {
+                const long long c = i * s->SX + j * s->SY + k;
+                if (f64) out[o] = r64[c];
+                else out[o] = inc.empty() ? (double)r32[c] : (double)r32[c] - (double)inc[c];
+            }
     return FDTD_OK;
 }
 
@@ -468,15 +476,16 @@ std::vector<std::pair<void*, size_t>> snap_regions(fdtd_solver* s) {
     const SolveParams& P = s->hP;
     const size_t w = s->precision == FDTD_PRECISION_FP64 ? 8 : 4;
     std::vector<std::pair<void*, size_t>> r;
-    r.push_back({P.p[0], s->ncell * w});
-    r.push_back({P.p[1], s->ncell * w});
-    if (P.dinc) r.push_back({P.dinc, s->ncell * 4});
-    for (int d = 0; d < 3; ++d) r.push_back({P.pd[d], s->ncell * w});
+    const size_t np = (size_t)s->np;  // the padded arrays as they are
+    r.push_back({P.p[0], np * w});
+    r.push_back({P.p[1], np * w});
+    if (P.dinc) r.push_back({P.dinc, np * 4});
+    for (int d = 0; d < 3; ++d) r.push_back({P.pd[d], np * w});
     for (int b = 0; b < 2; ++b)
         for (int d = 0; d < 3; ++d)
-            if (P.v[b][d]) r.push_back({P.v[b][d], s->vcount[d] * w});
-    r.push_back({P.cls, (size_t)s->ncell});
-    r.push_back({P.gobj, (size_t)s->ncell});
+            if (P.v[b][d]) r.push_back({P.v[b][d], np * w});
+    r.push_back({P.cls, np});
+    r.push_back({P.gobj, np});
     r.push_back({P.consts, 2 * sizeof(StepConsts)});
     r.push_back({P.dev_error, sizeof(int)});
     return r;

@@ -22,7 +22,7 @@ SHAPE_SPHERE, SHAPE_BOX, SHAPE_ELLIPSOID = 0, 1, 2
 ACCEL_NONE, ACCEL_GAUSSIAN_TRANSLATION, ACCEL_GAUSSIAN_PULSATION = 0, 1, 2
 MOTION_STATIC, MOTION_BALLISTIC = 0, 1
 PRECISION_FP64, PRECISION_FP32_COMPENSATED = 0, 1
-KERNEL_FUSED, KERNEL_PHASED, KERNEL_STREAMING = 0, 1, 2
+KERNEL_FUSED, KERNEL_PHASED = 0, 1
 
 CELL_BULK, CELL_GHOST, CELL_VALID_HISTORY, CELL_PML, CELL_CONSTRAINT = 1, 2, 4, 8, 16
 (FIELD_PRESSURE, FIELD_PRESSURE_PREV, FIELD_PML_PX, FIELD_PML_PY, FIELD_PML_PZ,

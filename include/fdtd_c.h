@@ -120,8 +120,7 @@ enum {
 
 enum {
     FDTD_KERNEL_FUSED = 0,    /* region-split fused step: interior kernel + PML-shell kernel */
-    FDTD_KERNEL_PHASED = 1,   /* plain path: one kernel per reference phase (FP64 only)      */
-    FDTD_KERNEL_STREAMING = 2 /* single kernel, one thread per column marching along x       */
+    FDTD_KERNEL_PHASED = 1    /* plain path: one kernel per reference phase (FP64 only)      */
 };
 
 typedef struct {
