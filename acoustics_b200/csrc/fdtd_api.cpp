@@ -664,7 +664,7 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     if (s->L > 0)
         CUDA_TRY(s.get(), cudaMemcpy((void*)P.listeners, s->listeners.data(), s->listeners.size() * 8, cudaMemcpyHostToDevice));
     CUDA_TRY(s.get(), cudaMallocHost((void**)&s->h_lis_stage, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8));
-    s->xb = (o.x_chunk == 2 || o.x_chunk == 4 || o.x_chunk == 8) ? o.x_chunk : 4;
+    s->xb = (o.x_chunk == 2 || o.x_chunk == 4 || o.x_chunk == 8) ? o.x_chunk : 2;
     s->region.xb = s->xb;
     // tile_y selects the PML-shell planes per thread (1, 2 or 4) of the fused path
     if (o.kernel == FDTD_KERNEL_FUSED && (o.tile_y == 1 || o.tile_y == 2 || o.tile_y == 4))

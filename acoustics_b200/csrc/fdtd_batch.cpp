@@ -125,7 +125,7 @@ fdtd_status grow(fdtd_batch* b, T** ptr, size_t* cap, size_t need) {
 // Rebuild descriptors and tile tables after a membership change.
 fdtd_status rebuild(fdtd_batch* b) {
     const bool f64 = b->precision == FDTD_PRECISION_FP64;
-    const int xb = (b->opt.x_chunk == 2 || b->opt.x_chunk == 8) ? b->opt.x_chunk : 4;
+    const int xb = (b->opt.x_chunk == 4 || b->opt.x_chunk == 8) ? b->opt.x_chunk : 2;
     const int xs = (b->opt.tile_y == 2 || b->opt.tile_y == 4) ? b->opt.tile_y : 1;
     const size_t dsz = f64 ? desc_bytes<double>() : desc_bytes<float>();
     const size_t nm = b->members.size();
@@ -144,7 +144,7 @@ fdtd_status rebuild(fdtd_batch* b) {
         const Box3& I = mb.s->region.interior;
         const int nx = I.hi[0] - I.lo[0], ny = I.hi[1] - I.lo[1], nz = I.hi[2] - I.lo[2];
         if (nx > 0 && ny > 0 && nz > 0) {
-            const int tz = (nz + 31) / 32, ty = (ny + 7) / 8, tx = (nx + xb - 1) / xb;
+            const int tz = interior_strips_z(I, f64 ? 2 : 4), ty = (ny + 7) / 8, tx = (nx + xb - 1) / xb;
             for (int x = 0; x < tx; ++x)
                 for (int y = 0; y < ty; ++y)
                     for (int z = 0; z < tz; ++z) it.push_back({(int)m, 0, z, y, x});

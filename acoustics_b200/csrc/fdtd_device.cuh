@@ -287,6 +287,13 @@ struct BatchLaunch {
     int src_blocks;              // per member (0: no member has a source)
 };
 
+// z-vector groups of the interior box: groups start at multiples of V = 16 /
+// sizeof(T) (aligned in the padded layout); number of 32-group CTA strips
+__host__ __device__ inline int interior_groups_z(const Box3& b, int V) {
+    return b.hi[2] > b.lo[2] ? (b.hi[2] - 1) / V - b.lo[2] / V + 1 : 0;
+}
+__host__ __device__ inline int interior_strips_z(const Box3& b, int V) { return (interior_groups_z(b, V) + 31) / 32; }
+
 // padded index of cell (or low face) (i, j, k)
 __host__ __device__ __forceinline__ long long cidx(const SolveParams& P, int i, int j, int k) {
     return i * P.SX + j * P.SY + k;

@@ -36,66 +36,121 @@ __host__ __device__ constexpr int shell_min_blocks(int xs, int word) {
 
 namespace fdtd {
 
-// One interior tile: 32 z x 8 y columns, XB x planes, starting at tile
-// coordinates (tz, ty, tx) of the box.  Every thread of the CTA must call it
-// (z neighbours are exchanged by warp shuffles).
+// 16-byte vector of T (4 floats or 2 doubles) for aligned z-vector accesses
+template <typename T>
+struct alignas(16) Vec16 {
+    T e[16 / sizeof(T)];
+};
+template <typename T>
+__device__ __forceinline__ Vec16<T> ldv(const T* p) {
+    return *reinterpret_cast<const Vec16<T>*>(p);
+}
+template <typename T>
+__device__ __forceinline__ void stv(T* p, const Vec16<T>& v) {
+    *reinterpret_cast<Vec16<T>*>(p) = v;
+}
+
+// One interior tile: 32 z-vector groups (128 FP32 / 64 FP64 cells) x 8 y rows
+// x XB x planes, at tile coordinates (tz, ty, tx) of the box.  Every access is
+// a 16-byte vector load or store (classification bytes: one 4- or 2-byte
+// word), z neighbours across vectors come from the adjacent lane by shuffles
+// and at the strip edges from memory.  Cells of a group outside the box or not
+// plain bulk are masked (scalar stores for partial groups).  Every thread of
+// the CTA must call it.
 template <typename T, int XB>
 __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box, int tz, int ty, int tx) {
     constexpr bool COMP = sizeof(T) == 4;
+    constexpr int V = 16 / (int)sizeof(T);
+    using VT = Vec16<T>;
     const int lane = threadIdx.x;
-    const int z = box.lo[2] + tz * 32 + lane;
+    const int zg0 = box.lo[2] / V * V;
+    const int zlast = (box.hi[2] - 1) / V * V;
+    const int zv = zg0 + (tz * 32 + lane) * V;
     const int y = box.lo[1] + ty * 8 + threadIdx.y;
     const int x0 = box.lo[0] + tx * XB;
-    const bool active = (z < box.hi[2]) && (y < box.hi[1]);
-    const int zc = min(z, box.hi[2] - 1);
+    const bool lane_on = (zv <= zlast) && (y < box.hi[1]);
+    const int zc = min(zv, zlast);  // inactive lanes shadow a valid group for the shuffles
     const int yc = min(y, box.hi[1] - 1);
     const int nx = min(XB, box.hi[0] - x0);
-    const int sy = (int)A.sy;
-    const int sx = (int)A.sx;
+    // signed strides: offsets below are formed relative to the tile's first cell
+    // and may be negative (pc[i*sx - 1] at i = 0)
+    const int sx = (int)A.sx, sy = (int)A.sy;
     const unsigned off = (unsigned)x0 * A.sx + (unsigned)yc * A.sy + zc;
     const T* __restrict__ pc = A.pc + off;
     T* __restrict__ pn = A.pn + off;
     float* __restrict__ dinc = A.dinc + off;
     const uint8_t* __restrict__ cls = A.cls + off;
+    // the z+V neighbour comes from memory where the next lane does not hold it
+    const bool zp_mem = (lane == 31) || (zv + V > zlast);
 
-    T pcol[XB + 2];
-    T ym[XB], yp[XB], prev[XB];
-    uint8_t code[XB];
-    pcol[0] = pc[-sx];
+    VT pcol[XB + 2], ym[XB], yp[XB], prev[XB];
+    uint32_t code[XB];
+    T zme[XB], zpe[XB];
+    pcol[0] = ldv(pc - sx);
 #pragma unroll
     for (int i = 0; i < XB + 1; ++i)
-        if (i <= nx) pcol[i + 1] = pc[i * sx];
+        if (i <= nx) pcol[i + 1] = ldv(pc + i * sx);
 #pragma unroll
     for (int i = 0; i < XB; ++i) {
         if (i < nx) {
-            ym[i] = pc[i * sx - sy];
-            yp[i] = pc[i * sx + sy];
-            if constexpr (COMP) prev[i] = (T)dinc[i * sx];
-            else prev[i] = pn[i * sx];
-            code[i] = cls[i * sx];
+            ym[i] = ldv(pc + i * sx - sy);
+            yp[i] = ldv(pc + i * sx + sy);
+            if constexpr (COMP) {
+                const Vec16<float> d = ldv(dinc + i * sx);
+#pragma unroll
+                for (int e = 0; e < V; ++e) prev[i].e[e] = d.e[e];
+            } else {
+                prev[i] = ldv(pn + i * sx);
+            }
+            if constexpr (V == 4) code[i] = *reinterpret_cast<const uint32_t*>(cls + i * sx);
+            else code[i] = *reinterpret_cast<const uint16_t*>(cls + i * sx);
+            zme[i] = (lane == 0) ? pc[i * sx - 1] : (T)0;
+            zpe[i] = zp_mem ? pc[i * sx + V] : (T)0;
         }
     }
 #pragma unroll
     for (int i = 0; i < XB; ++i) {
         if (i >= nx) break;
-        const T p0 = pcol[i + 1];
-        T zm = __shfl_up_sync(0xffffffffu, p0, 1);
-        T zp = __shfl_down_sync(0xffffffffu, p0, 1);
-        if (lane == 0) zm = pc[i * sx - 1];
-        if (lane == 31 || z + 1 >= box.hi[2]) zp = pc[i * sx + 1];
-        // solid cells are left untouched; cells next to a solid go to k_ghost_cells
-        if (!active || (code[i] & (CLS_BULK | CLS_MASK)) != CLS_BULK) continue;
-        T lap = 0.0;
-        lap = lap + (pcol[i + 2] + pcol[i] - (T)2.0 * p0);
-        lap = lap + (yp[i] + ym[i] - (T)2.0 * p0);
-        lap = lap + (zp + zm - (T)2.0 * p0);
-        lap = lap * A.lap_scale;
-        if constexpr (!COMP) {
-            pn[i * sx] = (T)2.0 * p0 - prev[i] + lap * A.c2k2;
-        } else {
-            const float d = fmaf(lap, A.c2k2, prev[i]);
-            dinc[i * sx] = d;
-            pn[i * sx] = p0 + d;
+        const VT& c0 = pcol[i + 1];
+        const T left = __shfl_up_sync(0xffffffffu, c0.e[V - 1], 1);
+        const T right = __shfl_down_sync(0xffffffffu, c0.e[0], 1);
+        const T zm_edge = lane == 0 ? zme[i] : left;
+        const T zp_edge = zp_mem ? zpe[i] : right;
+        VT outp, outd;
+        unsigned act = 0;
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            const T p0 = c0.e[e];
+            const T zm = e > 0 ? c0.e[e - 1] : zm_edge;
+            const T zp = e < V - 1 ? c0.e[e + 1] : zp_edge;
+            const int z = zc + e;
+            const uint8_t cb = (uint8_t)(code[i] >> (8 * e));
+            // solid cells are left untouched; cells next to a solid go to k_ghost_cells
+            const bool on = lane_on && z >= box.lo[2] && z < box.hi[2] && (cb & (CLS_BULK | CLS_MASK)) == CLS_BULK;
+            act |= (on ? 1u : 0u) << e;
+            T lap = 0.0;
+            lap = lap + (pcol[i + 2].e[e] + pcol[i].e[e] - (T)2.0 * p0);
+            lap = lap + (yp[i].e[e] + ym[i].e[e] - (T)2.0 * p0);
+            lap = lap + (zp + zm - (T)2.0 * p0);
+            lap = lap * A.lap_scale;
+            if constexpr (!COMP) {
+                outp.e[e] = (T)2.0 * p0 - prev[i].e[e] + lap * A.c2k2;
+            } else {
+                const float d = fmaf(lap, A.c2k2, prev[i].e[e]);
+                outd.e[e] = d;
+                outp.e[e] = p0 + d;
+            }
+        }
+        if (act == (1u << V) - 1u) {
+            stv(pn + i * sx, outp);
+            if constexpr (COMP) stv(dinc + i * sx, outd);
+        } else if (act) {
+#pragma unroll
+            for (int e = 0; e < V; ++e)
+                if ((act >> e) & 1u) {
+                    pn[i * sx + e] = outp.e[e];
+                    if constexpr (COMP) dinc[i * sx + e] = outd.e[e];
+                }
         }
     }
 }
@@ -257,8 +312,8 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     if (has_interior) {
         cudaStream_t si = concurrent ? s2 : s;
         dim3 block(32, 8);
-        const int xb = (R.xb == 2 || R.xb == 8) ? R.xb : 4;
-        dim3 grid((nz + 31) / 32, (ny + 7) / 8, (nx + xb - 1) / xb);
+        const int xb = (R.xb == 4 || R.xb == 8) ? R.xb : 2;
+        dim3 grid(interior_strips_z(b, 16 / (int)sizeof(T)), (ny + 7) / 8, (nx + xb - 1) / xb);
         if (xb == 2) k_interior<T, 2><<<grid, block, 0, si>>>(A, b);
         else if (xb == 8) k_interior<T, 8><<<grid, block, 0, si>>>(A, b);
         else k_interior<T, 4><<<grid, block, 0, si>>>(A, b);
