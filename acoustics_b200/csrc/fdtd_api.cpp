@@ -221,20 +221,25 @@ void build_shell_boxes(fdtd_solver* s, int xs) {
     ShellBoxes& B = s->shell;
     std::memset(&B, 0, sizeof(B));
     B.xs = xs;
+    B.zbox = -1;
+    const int V = shell_vz(s->precision == FDTD_PRECISION_FP64 ? 8 : 4);  // z cells per vector group
+    B.vz = V;
     const int* N = s->N;
     const int* lo = s->interior.lo;
     const int* hi = s->interior.hi;
+    auto groups = [&](int z0, int z1) { return z1 > z0 ? (z1 - 1) / V - z0 / V + 1 : 0; };
     auto add = [&](int x0, int x1, int y0, int y1, int za0, int za1, int zb0, int zb1) {
         const int nz = (za1 - za0) + (zb1 - zb0);
         if (x1 <= x0 || y1 <= y0 || nz <= 0) return;
         const int b = B.n;
         B.x0[b] = x0; B.nx[b] = x1 - x0;
         B.y0[b] = y0; B.ny[b] = y1 - y0;
-        B.z0a[b] = za0; B.nza[b] = za1 - za0; B.z0b[b] = zb0; B.nz[b] = nz;
-        B.tz[b] = (nz + 31) / 32;
-        B.ty[b] = (B.ny[b] + 7) / 8;
+        B.za[b] = za0; B.zae[b] = za1; B.zb[b] = zb0; B.zbe[b] = zb1;
+        B.gl[b] = groups(za0, za1);
+        B.ng[b] = B.gl[b] + groups(zb0, zb1);
+        B.tu[b] = (B.ny[b] * B.ng[b] + 255) / 256;
         B.tx[b] = (B.nx[b] + xs - 1) / xs;
-        B.block_first[b + 1] = B.block_first[b] + B.tz[b] * B.ty[b] * B.tx[b];
+        B.block_first[b + 1] = B.block_first[b] + B.tu[b] * B.tx[b];
         B.cells += (long long)B.nx[b] * B.ny[b] * nz;
         ++B.n;
     };
@@ -247,6 +252,10 @@ void build_shell_boxes(fdtd_solver* s, int xs) {
     add(lo[0], hi[0], 0, lo[1], 0, N[2], N[2], N[2]);
     add(lo[0], hi[0], hi[1], N[1], 0, N[2], N[2], N[2]);
     add(lo[0], hi[0], lo[1], hi[1], 0, lo[2], hi[2], N[2]);
+    if (B.n > 0 && B.x0[B.n - 1] == lo[0] && B.y0[B.n - 1] == lo[1] && B.zb[B.n - 1] == hi[2]) {
+        B.zbox = B.n - 1;
+        B.zrw = (B.ng[B.zbox] + 1) * V;
+    }
 }
 
 fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
@@ -332,7 +341,7 @@ fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
     const int* N = s->N;
     if (lo[0] >= hi[0] || lo[1] >= hi[1] || lo[2] >= hi[2])
         for (int d = 0; d < 3; ++d) s->interior.lo[d] = s->interior.hi[d] = 0;
-    build_shell_boxes(s, 1);
+    build_shell_boxes(s, FDTD_SHELL_PLANES);
     (void)N;
     return FDTD_OK;
 }
@@ -404,6 +413,16 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
         if (o.kernel != FDTD_KERNEL_PHASED) cv.add(&P.v[1][d], n * w);  // double-buffered faces
     }
     if (o.kernel == FDTD_KERNEL_PHASED) cv.add((void**)&s->d_lap, n * 8);
+    // compact storage of the z-slab box (region-split path)
+    const ShellBoxes& SB = s->shell;
+    if (o.kernel == FDTD_KERNEL_FUSED && SB.zbox >= 0) {
+        P.zcount = (long long)SB.nx[SB.zbox] * SB.ny[SB.zbox] * SB.zrw;
+        for (int d = 0; d < 3; ++d) {
+            cv.add(&P.zpd[d], P.zcount * w);
+            cv.add(&P.zv[0][d], P.zcount * w);
+            cv.add(&P.zv[1][d], P.zcount * w);
+        }
+    }
     cv.add((void**)&P.consts, 2 * sizeof(StepConsts));
     cv.add((void**)&P.dev_error, 16);
     cv.add((void**)&s->d_status, 16);
@@ -421,9 +440,10 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
         cv.add((void**)&P.pdiv_f[d], N[d] * 4);
         cv.add((void**)&P.vupd_f[d], (N[d] + 1) * 4);
         cv.add((void**)&P.vgrad_f[d], (N[d] + 1) * 4);
-        cv.add((void**)&P.axflag[d], N[d] + 1);
-        cv.add((void**)&P.coef_d[d], (N[d] + 1) * sizeof(AxisCoef<double>));
-        cv.add((void**)&P.coef_f[d], (N[d] + 1) * sizeof(AxisCoef<float>));
+        // N+8 entries: z-vector groups of the shell kernel read up to 7 past N (zeros)
+        cv.add((void**)&P.axflag[d], N[d] + 8);
+        cv.add((void**)&P.coef_d[d], (N[d] + 8) * sizeof(AxisCoef<double>));
+        cv.add((void**)&P.coef_f[d], (N[d] + 8) * sizeof(AxisCoef<float>));
     }
     s->lis_cap_steps = std::max(256, o.graph_steps);
     cv.add((void**)&s->d_lis, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8);
@@ -634,9 +654,9 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         CUDA_TRY(s.get(), cudaMemcpy((void*)P.vupd_f[d], f3.data(), (N[d] + 1) * 4, cudaMemcpyHostToDevice));
         CUDA_TRY(s.get(), cudaMemcpy((void*)P.vgrad_f[d], f4.data(), (N[d] + 1) * 4, cudaMemcpyHostToDevice));
         // packed flags and coefficient quads of the shell kernel
-        std::vector<uint8_t> fl(N[d] + 1, 0);
-        std::vector<AxisCoef<double>> cd(N[d] + 1);
-        std::vector<AxisCoef<float>> cf(N[d] + 1);
+        std::vector<uint8_t> fl(N[d] + 8, 0);
+        std::vector<AxisCoef<double>> cd(N[d] + 8, AxisCoef<double>{0.0, 0.0, 0.0, 0.0});
+        std::vector<AxisCoef<float>> cf(N[d] + 8, AxisCoef<float>{0.0f, 0.0f, 0.0f, 0.0f});
         for (int i = 0; i <= N[d]; ++i) {
             uint8_t f = 0;
             if (i < N[d]) {
@@ -657,7 +677,7 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
             cf[i].pupd = (float)cd[i].pupd;
             cf[i].pdiv = (float)cd[i].pdiv;
         }
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.axflag[d], fl.data(), N[d] + 1, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), cudaMemcpy((void*)P.axflag[d], fl.data(), fl.size(), cudaMemcpyHostToDevice));
         CUDA_TRY(s.get(), cudaMemcpy((void*)P.coef_d[d], cd.data(), cd.size() * sizeof(cd[0]), cudaMemcpyHostToDevice));
         CUDA_TRY(s.get(), cudaMemcpy((void*)P.coef_f[d], cf.data(), cf.size() * sizeof(cf[0]), cudaMemcpyHostToDevice));
     }
@@ -666,9 +686,8 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     CUDA_TRY(s.get(), cudaMallocHost((void**)&s->h_lis_stage, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8));
     s->xb = (o.x_chunk == 2 || o.x_chunk == 4 || o.x_chunk == 8) ? o.x_chunk : 2;
     s->region.xb = s->xb;
-    // tile_y selects the PML-shell planes per thread (1, 2 or 4) of the fused path
-    if (o.kernel == FDTD_KERNEL_FUSED && (o.tile_y == 1 || o.tile_y == 2 || o.tile_y == 4))
-        build_shell_boxes(s.get(), o.tile_y);
+    // tile_y: x planes each PML-shell thread marches over
+    if (o.kernel == FDTD_KERNEL_FUSED && o.tile_y > 0) build_shell_boxes(s.get(), std::min(o.tile_y, 256));
     s->region.shell = s->shell;
     st = fdtd_solver_reset(s.get(), sc->start_time);
     if (st != FDTD_OK) return st;
@@ -709,6 +728,11 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
         CUDA_TRY(s, cudaMemsetAsync(P.pd[d], 0, np * w, s->stream));
         CUDA_TRY(s, cudaMemsetAsync(P.v[0][d], 0, np * w, s->stream));
         if (P.v[1][d]) CUDA_TRY(s, cudaMemsetAsync(P.v[1][d], 0, np * w, s->stream));
+        if (P.zcount > 0) {
+            CUDA_TRY(s, cudaMemsetAsync(P.zpd[d], 0, P.zcount * w, s->stream));
+            CUDA_TRY(s, cudaMemsetAsync(P.zv[0][d], 0, P.zcount * w, s->stream));
+            CUDA_TRY(s, cudaMemsetAsync(P.zv[1][d], 0, P.zcount * w, s->stream));
+        }
     }
     // initFieldRasterized: every cell bulk with valid history (MAC_Grid.cpp:2459-2470, :4170-4180)
     CUDA_TRY(s, cudaMemsetAsync(P.cls, CLS_BULK | CLS_VALID, np, s->stream));

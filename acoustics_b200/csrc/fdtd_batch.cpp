@@ -126,7 +126,7 @@ fdtd_status grow(fdtd_batch* b, T** ptr, size_t* cap, size_t need) {
 fdtd_status rebuild(fdtd_batch* b) {
     const bool f64 = b->precision == FDTD_PRECISION_FP64;
     const int xb = (b->opt.x_chunk == 4 || b->opt.x_chunk == 8) ? b->opt.x_chunk : 2;
-    const int xs = (b->opt.tile_y == 2 || b->opt.tile_y == 4) ? b->opt.tile_y : 1;
+    const int xs = b->opt.tile_y > 0 ? std::min(b->opt.tile_y, 256) : FDTD_SHELL_PLANES;
     const size_t dsz = f64 ? desc_bytes<double>() : desc_bytes<float>();
     const size_t nm = b->members.size();
     std::vector<char> descs(std::max<size_t>(nm, 1) * dsz, 0);
@@ -152,8 +152,7 @@ fdtd_status rebuild(fdtd_batch* b) {
         const ShellBoxes& B = mb.s->shell;
         for (int bx = 0; bx < B.n; ++bx)
             for (int x = 0; x < B.tx[bx]; ++x)
-                for (int y = 0; y < B.ty[bx]; ++y)
-                    for (int z = 0; z < B.tz[bx]; ++z) st.push_back({(int)m, bx, z, y, x});
+                for (int u = 0; u < B.tu[bx]; ++u) st.push_back({(int)m, bx, u, 0, x});
         for (int li = 0; li < mb.s->L; ++li) refs.push_back({(int)m, li});
         max_ghost = std::max(max_ghost, (mb.s->region.ghost_cap + 127) / 128);
         if (mb.s->hP.n_src > 0) {

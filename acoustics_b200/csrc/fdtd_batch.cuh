@@ -47,8 +47,8 @@ __global__ void __launch_bounds__(256) k_batch_interior(const BatchDesc<T>* __re
     }
 }
 
-template <typename T, int XS>
-__global__ void __launch_bounds__(256, shell_min_blocks(XS, sizeof(T))) k_batch_shell(const BatchDesc<T>* __restrict__ D,
+template <typename T>
+__global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_batch_shell(const BatchDesc<T>* __restrict__ D,
                                                                       const BatchTile* __restrict__ tiles, int n) {
     __shared__ KArgs<T> sA;
     __shared__ ShellBoxes sB;
@@ -68,7 +68,7 @@ __global__ void __launch_bounds__(256, shell_min_blocks(XS, sizeof(T))) k_batch_
             __syncthreads();
             prev = tile.m;
         }
-        shell_tile<T, XS>(sA, sB, tile.box, tile.tz, tile.ty, tile.tx);
+        shell_tile<T>(sA, sB, tile.box, tile.tz, tile.tx);
     }
 }
 
@@ -137,9 +137,7 @@ cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, 
         ++l;
     }
     if (L.n_shell > 0) {
-        if (L.xs == 2) k_batch_shell<T, 2><<<L.ctas_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles, L.n_shell);
-        else if (L.xs == 4) k_batch_shell<T, 4><<<L.ctas_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles, L.n_shell);
-        else k_batch_shell<T, 1><<<L.ctas_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles, L.n_shell);
+        k_batch_shell<T><<<L.ctas_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles, L.n_shell);
         ++l;
     }
     e = cudaEventRecord(join, s2);

@@ -24,6 +24,13 @@
 #include <cmath>
 #include <cstdint>
 
+#ifndef FDTD_SHELL_VZ_F32
+#define FDTD_SHELL_VZ_F32 2
+#endif
+#ifndef FDTD_SHELL_PLANES
+#define FDTD_SHELL_PLANES 8  // x planes a PML-shell thread marches over (default)
+#endif
+
 #ifndef FDTD_MAX_OBJECTS
 #define FDTD_MAX_OBJECTS 8
 #endif
@@ -67,16 +74,37 @@ struct Box3 {
     int hi[3];
 };
 
+// z cells per vector group of the shell kernel for a word size (8-byte groups:
+// 2 FP32 or 2 FP64 cells... FP64 uses 16 bytes)
+__host__ __device__ constexpr int shell_vz(int word) { return word == 4 ? FDTD_SHELL_VZ_F32 : 2; }
+
 // The PML shell as up to five disjoint boxes (x slabs, y slabs, the merged z-slab
-// pair).  Box b covers x in [x0, x0+nx), y in [y0, y0+ny) and nz z indices:
-// z = zz < nza ? z0a + zz : z0b + (zz - nza).  Tiles are 32 z x 8 y x xs x;
-// block_first[] is the prefix sum of tiles per box.
+// pair).  Box b covers x in [x0, x0+nx), y in [y0, y0+ny) and z in
+// [za, zae) u [zb, zbe).  Along z it is cut into vector groups of vz cells
+// starting at multiples of vz: gl groups cover [za, zae), the next ng - gl
+// cover [zb, zbe) (groups may reach outside the ranges; those cells are
+// masked).  A thread owns one group of one row for xs x planes; a CTA owns 256
+// consecutive (row, group) units: tu unit tiles x tx plane tiles per box.
+// block_first[] is the prefix sum of CTAs per box.
+//
+// The z-slab pair (box zbox) keeps its split pressures and face velocities in
+// compact arrays: row (x, y) of the box at ((x - x0) * ny + (y - y0)) * zrw,
+// group gi of the row at gi * vz, plus one spare group at ng * vz holding the
+// high z face of the last group of each range (slot 0: first range, 1: second)
+// when that face is not the next group's first slot.  Its rows are then
+// contiguous instead of two short pieces per row of the grid.  Faces it
+// shares with other boxes stay in the grid arrays: it reads its high x / y
+// faces at the far box ends from there, and writes its low x / y faces at
+// x = x0 / y = y0 to both (the x / y slabs read them as their high faces).
 struct ShellBoxes {
-    int n, xs;
+    int n, xs, vz;
     int x0[5], nx[5], y0[5], ny[5];
-    int z0a[5], nza[5], z0b[5], nz[5];
-    int tz[5], ty[5], tx[5];
+    int za[5], zae[5], zb[5], zbe[5];
+    int gl[5], ng[5];
+    int tu[5], tx[5];
     int block_first[6];
+    int zbox;     // box with compact storage (-1: none)
+    int zrw;      // compact row width (elements): (ng + 1) * vz
     long long cells;
 };
 
@@ -114,8 +142,11 @@ struct KArgs {
     T* pd[3];
     const T* vo[3];
     T* vn[3];
-    const uint8_t* axflag[3];     // AXF_* per index, [N_d + 1]
-    const AxisCoef<T>* coef[3];   // [N_d + 1]
+    T* zpd[3];                    // compact z-slab storage (ShellBoxes::zbox)
+    const T* zvo[3];
+    T* zvn[3];
+    const uint8_t* axflag[3];     // AXF_* per index, [N_d + 8] (zero past N_d)
+    const AxisCoef<T>* coef[3];   // [N_d + 8]
     T inv_h, c2k2, lap_scale;
     SolveParams* P;               // device copy (for the step-constant advance)
     int cur;
@@ -171,9 +202,9 @@ struct SolveParams {
     const float* pdiv_f[3];
     const float* vupd_f[3];
     const float* vgrad_f[3];
-    const uint8_t* axflag[3];     // [N_d+1] AXF_* flags
-    const AxisCoef<double>* coef_d[3];  // [N_d+1]
-    const AxisCoef<float>* coef_f[3];   // [N_d+1] (the same values rounded to float)
+    const uint8_t* axflag[3];     // [N_d+8] AXF_* flags (zero past N_d)
+    const AxisCoef<double>* coef_d[3];  // [N_d+8]
+    const AxisCoef<float>* coef_f[3];   // [N_d+8] (the same values rounded to float)
     // state
     uint8_t* cls;
     uint8_t* gobj;
@@ -181,6 +212,9 @@ struct SolveParams {
     float* dinc;
     void* pd[3];
     void* v[2][3];
+    void* zpd[3];                 // compact z-slab split pressures and face velocities
+    void* zv[2][3];
+    long long zcount;             // elements per compact array
     StepConsts* consts;           // [2], indexed by the step parity
     int* dev_error;               // sticky device-side error flags
     const double* listeners;      // 3*n_lis
@@ -212,6 +246,9 @@ inline KArgs<double> make_kargs<double>(SolveParams* dP, const SolveParams& P, i
         A.pd[d] = (double*)P.pd[d];
         A.vo[d] = (const double*)P.v[cur][d];
         A.vn[d] = (double*)P.v[cur ^ 1][d];
+        A.zpd[d] = (double*)P.zpd[d];
+        A.zvo[d] = (const double*)P.zv[cur][d];
+        A.zvn[d] = (double*)P.zv[cur ^ 1][d];
         A.axflag[d] = P.axflag[d];
         A.coef[d] = P.coef_d[d];
     }
@@ -236,6 +273,9 @@ inline KArgs<float> make_kargs<float>(SolveParams* dP, const SolveParams& P, int
         A.pd[d] = (float*)P.pd[d];
         A.vo[d] = (const float*)P.v[cur][d];
         A.vn[d] = (float*)P.v[cur ^ 1][d];
+        A.zpd[d] = (float*)P.zpd[d];
+        A.zvo[d] = (const float*)P.zv[cur][d];
+        A.zvn[d] = (float*)P.zv[cur ^ 1][d];
         A.axflag[d] = P.axflag[d];
         A.coef[d] = P.coef_f[d];
     }

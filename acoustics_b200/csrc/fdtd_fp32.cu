@@ -41,9 +41,7 @@ int batch_blocks_per_sm(int precision, int which, int shape) {
         else if (shape == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_interior<float, 8>, 256, 0);
         else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_interior<float, 4>, 256, 0);
     } else {
-        if (shape == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_shell<float, 2>, 256, 0);
-        else if (shape == 4) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_shell<float, 4>, 256, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_shell<float, 1>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_shell<float>, 256, 0);
     }
     return n > 0 ? n : 1;
 }

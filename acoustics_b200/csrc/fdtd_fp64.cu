@@ -416,9 +416,7 @@ int batch_blocks_per_sm_fp64(int which, int shape) {
         else if (shape == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_interior<double, 8>, 256, 0);
         else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_interior<double, 4>, 256, 0);
     } else {
-        if (shape == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_shell<double, 2>, 256, 0);
-        else if (shape == 4) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_shell<double, 4>, 256, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_shell<double, 1>, 256, 0);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_shell<double>, 256, 0);
     }
     return n > 0 ? n : 1;
 }

@@ -17,9 +17,9 @@
 // issued before the arithmetic; z neighbours come from the warp by shuffles.
 //
 // Shell mapping: five boxes (two x slabs, two y slabs, the merged pair of z
-// slabs whose z index jumps from the low slab to the high one so warps stay
-// full); a CTA of 32 x 8 threads owns one tile of one box and XS x planes,
-// decoded once per CTA from a prefix table; offsets are 32-bit.
+// slabs); a thread owns one z-vector group of one row and marches along x; a
+// CTA of 256 threads owns 256 consecutive (row, group) units of one box, decoded
+// once per CTA from a prefix table; offsets are 32-bit.
 // Face ownership: a face is written by the cell to its right, or by its left
 // cell when the right one is not a PML cell (the x = W h layer on the low side),
 // so the interior kernel never touches velocities.
@@ -28,26 +28,27 @@
 #include "fdtd_region.cuh"
 #include "fdtd_stencil.cuh"
 
-// resident CTAs of 256 threads the shell kernels are compiled for (register
-// budget per thread): FP32 64 / 80 / 128, FP64 80 / 128 / 255 for 1 / 2 / 4 x planes
-__host__ __device__ constexpr int shell_min_blocks(int xs, int word) {
-    return word == 4 ? (xs == 1 ? 4 : (xs == 2 ? 3 : 2)) : (xs == 1 ? 3 : (xs == 2 ? 2 : 1));
-}
+// resident CTAs of 256 threads the shell kernels are compiled for: 3 (85
+// registers per thread) in FP32, 2 (128) in FP64
+__host__ __device__ constexpr int shell_min_blocks(int word) { return word == 4 ? 2 : 1; }
 
 namespace fdtd {
 
-// 16-byte vector of T (4 floats or 2 doubles) for aligned z-vector accesses
-template <typename T>
-struct alignas(16) Vec16 {
-    T e[16 / sizeof(T)];
+// Vector of V consecutive z cells (aligned to its size) for z-vector accesses;
+// Vec16<T> is the 16-byte one (4 floats or 2 doubles)
+template <typename T, int V>
+struct alignas(sizeof(T) * V) Vec {
+    T e[V];
 };
 template <typename T>
-__device__ __forceinline__ Vec16<T> ldv(const T* p) {
-    return *reinterpret_cast<const Vec16<T>*>(p);
+using Vec16 = Vec<T, 16 / sizeof(T)>;
+template <typename T, int V = 16 / sizeof(T)>
+__device__ __forceinline__ Vec<T, V> ldv(const T* p) {
+    return *reinterpret_cast<const Vec<T, V>*>(p);
 }
-template <typename T>
-__device__ __forceinline__ void stv(T* p, const Vec16<T>& v) {
-    *reinterpret_cast<Vec16<T>*>(p) = v;
+template <typename T, int V>
+__device__ __forceinline__ void stv(T* p, const Vec<T, V>& v) {
+    *reinterpret_cast<Vec<T, V>*>(p) = v;
 }
 
 // One interior tile: 32 z-vector groups (128 FP32 / 64 FP64 cells) x 8 y rows
@@ -160,135 +161,258 @@ __global__ void __launch_bounds__(256) k_interior(const KArgs<T> A, Box3 box) {
     interior_tile<T, XB>(A, box, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
-// One PML-shell tile of box b at tile coordinates (tz, ty, tx): XS x planes of
-// one (y, z) column per thread.  Every global load of the XS planes (pressure
-// and its six neighbours, six face velocities, three split pressures) is
-// issued before the first use, with neighbour offsets clamped at the domain
-// edge instead of branched on, so a thread keeps ~13*XS independent loads in
-// flight; the face flags and coefficients come from the packed per-axis
-// tables (L1-resident).  Arithmetic order per cell is unchanged.
-template <typename T, int XS>
-__device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& B, int b, int tz, int ty, int tx) {
-    const int zz = tz * 32 + threadIdx.x;
-    const int yy = ty * 8 + threadIdx.y;
-    if (zz >= B.nz[b] || yy >= B.ny[b]) return;
-    const int z = zz < B.nza[b] ? B.z0a[b] + zz : B.z0b[b] + (zz - B.nza[b]);
-    const int y = B.y0[b] + yy;
-    const int xbeg = B.x0[b] + tx * XS;
-    const int nxh = min(XS, B.x0[b] + B.nx[b] - xbeg);
-    const unsigned sx = A.sx, sy = A.sy;
-    const unsigned c0 = (unsigned)xbeg * sx + (unsigned)y * sy + z;  // cell and its three low faces
-    const uint8_t gy = __ldg(A.axflag[1] + y), gz = __ldg(A.axflag[2] + z);
-    const bool pmly = gy & AXF_PML, pmlz = gz & AXF_PML;
-    const unsigned oym = (gy & AXF_HAS_LO) ? sy : 0u, oyp = (gy & AXF_HAS_HI) ? sy : 0u;
-    const unsigned ozm = (gz & AXF_HAS_LO) ? 1u : 0u, ozp = (gz & AXF_HAS_HI) ? 1u : 0u;
-
-    // ---- loads of all XS planes ----
-    T p0v[XS], xm[XS], xp[XS], ym[XS], yp[XS], zm[XS], zp[XS];
-    T vxl[XS], vxr[XS], vyl[XS], vyr[XS], vzl[XS], vzr[XS], a0[XS], a1[XS], a2[XS];
-    uint8_t gx[XS];
+// Masked store of a z vector: one vector store when every cell is selected,
+// else the selected cells one by one.
+template <typename T, int V>
+__device__ __forceinline__ void st_masked(T* p, const Vec<T, V>& v, unsigned m) {
+    if (m == (1u << V) - 1u) {
+        stv(p, v);
+    } else if (m) {
 #pragma unroll
-    for (int i = 0; i < XS; ++i) {
-        if (i < nxh) {
-            const int x = xbeg + i;
-            const unsigned c = c0 + i * sx;
-            gx[i] = __ldg(A.axflag[0] + x);
-            p0v[i] = A.pc[c];
-            xm[i] = A.pc[c - (x > 0 ? sx : 0u)];
-            xp[i] = A.pc[c + (x + 1 < A.N0 ? sx : 0u)];
-            ym[i] = A.pc[c - oym];
-            yp[i] = A.pc[c + oyp];
-            zm[i] = A.pc[c - ozm];
-            zp[i] = A.pc[c + ozp];
-            vxl[i] = A.vo[0][c];
-            vxr[i] = A.vo[0][c + sx];
-            vyl[i] = A.vo[1][c];
-            vyr[i] = A.vo[1][c + sy];
-            vzl[i] = A.vo[2][c];
-            vzr[i] = A.vo[2][c + 1];
-            a0[i] = A.pd[0][c];
-            a1[i] = A.pd[1][c];
-            a2[i] = A.pd[2][c];
-        }
-    }
-    const AxisCoef<T> cyl = A.coef[1][y], cyr = A.coef[1][y + 1];
-    const AxisCoef<T> czl = A.coef[2][z], czr = A.coef[2][z + 1];
-
-    // ---- face velocities, split pressures, pressure ----
-#pragma unroll
-    for (int i = 0; i < XS; ++i) {
-        if (i >= nxh) break;
-        const int x = xbeg + i;
-        const unsigned c = c0 + i * sx;
-        const uint8_t g = gx[i];
-        const bool pmlx = g & AXF_PML;
-        // faces inside the PML (InsidePML at the face position, MAC_Grid.cpp:2631-2633),
-        // outer faces excluded (:2568-2575); a high face is written here only when the
-        // cell beyond it is not a PML cell
-        const bool oyz = pmly || pmlz, oxz = pmlx || pmlz, oxy = pmlx || pmly;
-        const bool fxl = (g & AXF_FACE_LO) || ((g & AXF_HAS_LO) && oyz);
-        const bool fxr = (g & AXF_FACE_HI) || ((g & AXF_HAS_HI) && oyz);
-        const bool fyl = (gy & AXF_FACE_LO) || ((gy & AXF_HAS_LO) && oxz);
-        const bool fyr = (gy & AXF_FACE_HI) || ((gy & AXF_HAS_HI) && oxz);
-        const bool fzl = (gz & AXF_FACE_LO) || ((gz & AXF_HAS_LO) && oxy);
-        const bool fzr = (gz & AXF_FACE_HI) || ((gz & AXF_HAS_HI) && oxy);
-        const T p0 = p0v[i];
-        T vxl_ = vxl[i], vxr_ = vxr[i];
-        T vyl_ = vyl[i], vyr_ = vyr[i], vzl_ = vzl[i], vzr_ = vzr[i];
-        const AxisCoef<T> cxl = A.coef[0][x], cxr = A.coef[0][x + 1];
-        if (fxl) {
-            vxl_ = vel_update<T>(vxl_, cxl.vupd, cxl.vgrad, p0, xm[i]);
-            A.vn[0][c] = vxl_;
-        }
-        if (fxr) {
-            vxr_ = vel_update<T>(vxr_, cxr.vupd, cxr.vgrad, xp[i], p0);
-            if (!((g & AXF_NEXT_PML) || oyz)) A.vn[0][c + sx] = vxr_;
-        }
-        if (fyl) {
-            vyl_ = vel_update<T>(vyl_, cyl.vupd, cyl.vgrad, p0, ym[i]);
-            A.vn[1][c] = vyl_;
-        }
-        if (fyr) {
-            vyr_ = vel_update<T>(vyr_, cyr.vupd, cyr.vgrad, yp[i], p0);
-            if (!((gy & AXF_NEXT_PML) || oxz)) A.vn[1][c + sy] = vyr_;
-        }
-        if (fzl) {
-            vzl_ = vel_update<T>(vzl_, czl.vupd, czl.vgrad, p0, zm[i]);
-            A.vn[2][c] = vzl_;
-        }
-        if (fzr) {
-            vzr_ = vel_update<T>(vzr_, czr.vupd, czr.vgrad, zp[i], p0);
-            if (!((gz & AXF_NEXT_PML) || oxy)) A.vn[2][c + 1] = vzr_;
-        }
-        const T ax = pd_update<T>(a0[i], cxl.pupd, cxl.pdiv, vxr_, vxl_, A.inv_h);
-        const T ay = pd_update<T>(a1[i], cyl.pupd, cyl.pdiv, vyr_, vyl_, A.inv_h);
-        const T az = pd_update<T>(a2[i], czl.pupd, czl.pdiv, vzr_, vzl_, A.inv_h);
-        A.pd[0][c] = ax;
-        A.pd[1][c] = ay;
-        A.pd[2][c] = az;
-        A.pn[c] = ax + ay + az;
+        for (int e = 0; e < V; ++e)
+            if ((m >> e) & 1u) p[e] = v.e[e];
     }
 }
 
-// CTA -> (box, tile) through the prefix table of the shell boxes
-__device__ __forceinline__ void shell_decode(const ShellBoxes& B, int blk, int& b, int& tz, int& ty, int& tx) {
+// V-bit mask of bit k of each of V flag bytes
+template <int V>
+__device__ __forceinline__ unsigned flag_mask(const uint8_t (&f)[V], int k) {
+    unsigned m = 0;
+#pragma unroll
+    for (int e = 0; e < V; ++e) m |= ((f[e] >> k) & 1u) << e;
+    return m;
+}
+
+// Where a shell column keeps its split pressures and face velocities: the grid
+// arrays, or the compact arrays of the z-slab box (ShellBoxes).
+template <typename T>
+struct ShellStore {
+    T* pd[3];
+    const T* vo[3];
+    T* vn[3];
+    int sx, sy;         // plane and row strides of that storage
+    bool compact;
+    bool x_hi_grid;     // compact: the last plane reads its high x face from the grid
+    bool y_hi_grid;     // compact: this row reads its high y face from the grid
+    bool y_lo_grid;     // compact: this row also writes its low y faces to the grid
+    int spare;          // compact: offset (from the group) of the spare high-z-face slot, 0: next slot
+};
+
+// Loads of one x plane of a shell column (everything but p(x-1), p(x) and the
+// low x face, which the previous plane carries).
+template <typename T, int V>
+struct ShellPlane {
+    Vec<T, V> pp, ym, yp, vxr, vyl, vyr, vzl, a0, a1, a2;
+    T zme, zpe, vze;
+    AxisCoef<T> cxr;
+    uint8_t g;
+};
+
+template <typename T, int V>
+__device__ __forceinline__ void shell_load(const KArgs<T>& A, const ShellStore<T>& S, ShellPlane<T, V>& L, int x,
+                                           bool last_plane, unsigned c, unsigned q, int oym, int oyp, int ozm) {
+    const int sx = (int)A.sx, sy = (int)A.sy;
+    const T* pc = A.pc + c;
+    L.g = __ldg(A.axflag[0] + x);
+    L.cxr = A.coef[0][x + 1];
+    L.pp = ldv<T, V>(pc + (x + 1 < A.N0 ? sx : 0));
+    L.ym = ldv<T, V>(pc - oym);
+    L.yp = ldv<T, V>(pc + oyp);
+    L.zme = pc[-ozm];
+    L.zpe = pc[V];
+    L.vxr = (S.x_hi_grid && last_plane) ? ldv<T, V>(A.vo[0] + c + sx) : ldv<T, V>(S.vo[0] + q + S.sx);
+    L.vyl = ldv<T, V>(S.vo[1] + q);
+    L.vyr = S.y_hi_grid ? ldv<T, V>(A.vo[1] + c + sy) : ldv<T, V>(S.vo[1] + q + S.sy);
+    L.vzl = ldv<T, V>(S.vo[2] + q);
+    L.vze = S.vo[2][q + (S.spare ? S.spare : V)];
+    L.a0 = ldv<T, V>(S.pd[0] + q);
+    L.a1 = ldv<T, V>(S.pd[1] + q);
+    L.a2 = ldv<T, V>(S.pd[2] + q);
+}
+
+// One PML-shell tile: unit tile tu (256 consecutive (row, z-group) units of box
+// b, one per thread) by x tile tx.  A thread owns one z group (a vector of
+// shell_vz cells starting at a multiple of its width; cells outside the
+// group's z range are masked) of one row and marches along x over B.xs planes:
+// p(x-1), p(x) and the low x face velocity are carried in registers, and the
+// loads of plane x+1 are issued before plane x is computed and stored.  Face
+// flags (MAC_Grid.cpp:2568-2575, :2631-2633) are V-bit masks from the packed
+// per-axis tables; the arithmetic per cell is the reference's, in its order.
+template <typename T>
+__device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& B, int b, int tu, int tx) {
+    constexpr int V = shell_vz(sizeof(T));
+    constexpr unsigned ALL = (1u << V) - 1u;
+    using VT = Vec<T, V>;
+    const int u = tu * 256 + threadIdx.x + 32 * threadIdx.y;
+    const int ng = B.ng[b];
+    if (u >= B.ny[b] * ng) return;
+    const int yl = u / ng;
+    const int gi = u - yl * ng;
+    const int y = B.y0[b] + yl;
+    // the group and its cells belong to the range they were enumerated from (a
+    // low and a high group may share a vector when the ranges are close)
+    const bool first = gi < B.gl[b];
+    const int zg = first ? (B.za[b] / V + gi) * V : (B.zb[b] / V + (gi - B.gl[b])) * V;
+    const int zr0 = first ? B.za[b] : B.zb[b], zr1 = first ? B.zae[b] : B.zbe[b];
+    unsigned inbox = 0;
+#pragma unroll
+    for (int e = 0; e < V; ++e) inbox |= (zg + e >= zr0 && zg + e < zr1 ? 1u : 0u) << e;
+    const int x0 = B.x0[b] + tx * B.xs;
+    const int x1 = min(x0 + B.xs, B.x0[b] + B.nx[b]);
+    const int xend = B.x0[b] + B.nx[b];
+    const int sx = (int)A.sx, sy = (int)A.sy;
+    const unsigned c0 = (unsigned)x0 * A.sx + (unsigned)y * A.sy + zg;  // cell and its three low faces
+
+    ShellStore<T> S;
+    S.compact = (b == B.zbox);
+    unsigned q0;
+    if (S.compact) {
+        S.sy = B.zrw;
+        S.sx = B.ny[b] * B.zrw;
+        q0 = (unsigned)(x0 - B.x0[b]) * S.sx + (unsigned)yl * S.sy + gi * V;
+        const bool last_group = first ? (gi == B.gl[b] - 1) : (gi == ng - 1);
+        S.spare = last_group ? (ng - gi) * V + (first ? 0 : 1) : 0;
+        S.x_hi_grid = true;
+        S.y_hi_grid = (y + 1 == B.y0[b] + B.ny[b]);
+        S.y_lo_grid = (yl == 0);
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            S.pd[d] = A.zpd[d];
+            S.vo[d] = A.zvo[d];
+            S.vn[d] = A.zvn[d];
+        }
+    } else {
+        S.sx = sx;
+        S.sy = sy;
+        q0 = c0;
+        S.spare = 0;
+        S.x_hi_grid = S.y_hi_grid = S.y_lo_grid = false;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            S.pd[d] = A.pd[d];
+            S.vo[d] = A.vo[d];
+            S.vn[d] = A.vn[d];
+        }
+    }
+
+    const uint8_t gy = __ldg(A.axflag[1] + y);
+    uint8_t gz[V];
+#pragma unroll
+    for (int e = 0; e < V; ++e) gz[e] = __ldg(A.axflag[2] + zg + e);
+    const unsigned zpml = flag_mask<V>(gz, 0), zflo = flag_mask<V>(gz, 1), zfhi = flag_mask<V>(gz, 2);
+    const unsigned znext = flag_mask<V>(gz, 3), zhlo = flag_mask<V>(gz, 4), zhhi = flag_mask<V>(gz, 5);
+    const unsigned mpy = (gy & AXF_PML) ? ALL : 0u;
+    const int oym = (gy & AXF_HAS_LO) ? sy : 0, oyp = (gy & AXF_HAS_HI) ? sy : 0;
+    const int ozm = zg > 0 ? 1 : 0;
+    const AxisCoef<T> cyl = A.coef[1][y], cyr = A.coef[1][y + 1];
+    AxisCoef<T> cz[V + 1];
+#pragma unroll
+    for (int e = 0; e <= V; ++e) cz[e] = A.coef[2][zg + e];
+
+    // carried along x
+    VT pm = ldv<T, V>(A.pc + c0 - (x0 > 0 ? sx : 0));
+    VT p0 = ldv<T, V>(A.pc + c0);
+    VT vxl = ldv<T, V>(S.vo[0] + q0);
+    AxisCoef<T> cxl = A.coef[0][x0];
+    ShellPlane<T, V> cur, nxt;
+    shell_load<T, V>(A, S, cur, x0, x0 + 1 == xend, c0, q0, oym, oyp, ozm);
+#pragma unroll 1
+    for (int x = x0; x < x1; ++x) {
+        const unsigned c = c0 + (unsigned)(x - x0) * A.sx;
+        const unsigned q = q0 + (unsigned)(x - x0) * S.sx;
+        if (x + 1 < x1) shell_load<T, V>(A, S, nxt, x + 1, x + 2 == xend, c + sx, q + S.sx, oym, oyp, ozm);
+        const uint8_t g = cur.g;
+        const unsigned mpx = (g & AXF_PML) ? ALL : 0u;
+        const unsigned oyz = mpy | zpml, oxz = mpx | zpml, oxy = mpx | mpy;
+        // faces inside the PML, outer faces excluded; a high face is written by
+        // this cell only when the cell beyond it is not a PML cell
+        const unsigned fxl = ((g & AXF_FACE_LO) ? ALL : 0u) | ((g & AXF_HAS_LO) ? oyz : 0u);
+        const unsigned fxr = ((g & AXF_FACE_HI) ? ALL : 0u) | ((g & AXF_HAS_HI) ? oyz : 0u);
+        const unsigned fyl = ((gy & AXF_FACE_LO) ? ALL : 0u) | ((gy & AXF_HAS_LO) ? oxz : 0u);
+        const unsigned fyr = ((gy & AXF_FACE_HI) ? ALL : 0u) | ((gy & AXF_HAS_HI) ? oxz : 0u);
+        const unsigned fzl = zflo | (zhlo & oxy);
+        const unsigned fzr = zfhi | (zhhi & oxy);
+        const unsigned m_xl = inbox & fxl;
+        const unsigned m_xr = inbox & fxr & ~(((g & AXF_NEXT_PML) ? ALL : 0u) | oyz);
+        const unsigned m_yl = inbox & fyl;
+        const unsigned m_yr = inbox & fyr & ~(((gy & AXF_NEXT_PML) ? ALL : 0u) | oxz);
+        const unsigned m_zl = inbox & fzl;
+        const unsigned m_zr = inbox & fzr & ~(znext | oxy);
+        const AxisCoef<T> cxr = cur.cxr;
+        VT nxl, nxr, nyl, nyr, nzl, ax, ay, az, pn;
+        T nzr[V];
+#pragma unroll
+        for (int e = 0; e < V; ++e) {
+            const T pz = p0.e[e];
+            const T pzm = e > 0 ? p0.e[e - 1] : cur.zme;
+            const T pzp = e < V - 1 ? p0.e[e + 1] : cur.zpe;
+            const T vx_l0 = vxl.e[e], vx_r0 = cur.vxr.e[e], vy_l0 = cur.vyl.e[e], vy_r0 = cur.vyr.e[e];
+            const T vz_l0 = cur.vzl.e[e], vz_r0 = e < V - 1 ? cur.vzl.e[e + 1] : cur.vze;
+            const T vx_l = ((fxl >> e) & 1u) ? vel_update<T>(vx_l0, cxl.vupd, cxl.vgrad, pz, pm.e[e]) : vx_l0;
+            const T vx_r = ((fxr >> e) & 1u) ? vel_update<T>(vx_r0, cxr.vupd, cxr.vgrad, cur.pp.e[e], pz) : vx_r0;
+            const T vy_l = ((fyl >> e) & 1u) ? vel_update<T>(vy_l0, cyl.vupd, cyl.vgrad, pz, cur.ym.e[e]) : vy_l0;
+            const T vy_r = ((fyr >> e) & 1u) ? vel_update<T>(vy_r0, cyr.vupd, cyr.vgrad, cur.yp.e[e], pz) : vy_r0;
+            const T vz_l = ((fzl >> e) & 1u) ? vel_update<T>(vz_l0, cz[e].vupd, cz[e].vgrad, pz, pzm) : vz_l0;
+            const T vz_r = ((fzr >> e) & 1u) ? vel_update<T>(vz_r0, cz[e + 1].vupd, cz[e + 1].vgrad, pzp, pz) : vz_r0;
+            nxl.e[e] = vx_l;
+            nxr.e[e] = vx_r;
+            nyl.e[e] = vy_l;
+            nyr.e[e] = vy_r;
+            nzl.e[e] = vz_l;
+            nzr[e] = vz_r;
+            ax.e[e] = pd_update<T>(cur.a0.e[e], cxl.pupd, cxl.pdiv, vx_r, vx_l, A.inv_h);
+            ay.e[e] = pd_update<T>(cur.a1.e[e], cyl.pupd, cyl.pdiv, vy_r, vy_l, A.inv_h);
+            az.e[e] = pd_update<T>(cur.a2.e[e], cz[e].pupd, cz[e].pdiv, vz_r, vz_l, A.inv_h);
+            pn.e[e] = ax.e[e] + ay.e[e] + az.e[e];
+        }
+        st_masked<T, V>(S.vn[0] + q, nxl, m_xl);
+        st_masked<T, V>(S.vn[1] + q, nyl, m_yl);
+        st_masked<T, V>(S.vn[2] + q, nzl, m_zl);
+        if (S.compact) {
+            // low x / y faces shared with the x / y slabs, high faces owned by them
+            if (x == B.x0[b]) st_masked<T, V>(A.vn[0] + c, nxl, m_xl);
+            if (S.y_lo_grid) st_masked<T, V>(A.vn[1] + c, nyl, m_yl);
+            st_masked<T, V>((x + 1 == xend ? A.vn[0] + c : S.vn[0] + q) + (x + 1 == xend ? sx : S.sx), nxr, m_xr);
+            st_masked<T, V>(S.y_hi_grid ? A.vn[1] + c + sy : S.vn[1] + q + S.sy, nyr, m_yr);
+        } else {
+            st_masked<T, V>(S.vn[0] + q + S.sx, nxr, m_xr);
+            st_masked<T, V>(S.vn[1] + q + S.sy, nyr, m_yr);
+        }
+        if (m_zr) {
+#pragma unroll
+            for (int e = 0; e < V; ++e)
+                if ((m_zr >> e) & 1u) S.vn[2][q + ((e == V - 1 && S.spare) ? S.spare : e + 1)] = nzr[e];
+        }
+        st_masked<T, V>(S.pd[0] + q, ax, inbox);
+        st_masked<T, V>(S.pd[1] + q, ay, inbox);
+        st_masked<T, V>(S.pd[2] + q, az, inbox);
+        st_masked<T, V>(A.pn + c, pn, inbox);
+        // carry to plane x+1
+        pm = p0;
+        p0 = cur.pp;
+        vxl = cur.vxr;
+        cxl = cxr;
+        cur = nxt;
+    }
+}
+
+// CTA -> (box, unit tile, plane tile) through the prefix table of the shell boxes
+__device__ __forceinline__ void shell_decode(const ShellBoxes& B, int blk, int& b, int& tu, int& tx) {
     b = 0;
 #pragma unroll
     for (int q = 1; q < 5; ++q)
         if (q < B.n && blk >= B.block_first[q]) b = q;
-    int local = blk - B.block_first[b];
-    tz = local % B.tz[b];
-    local /= B.tz[b];
-    ty = local % B.ty[b];
-    tx = local / B.ty[b];
+    const int local = blk - B.block_first[b];
+    tu = local % B.tu[b];
+    tx = local / B.tu[b];
 }
 
-template <typename T, int XS>
-__global__ void __launch_bounds__(256, shell_min_blocks(XS, sizeof(T))) k_pml_shell(const KArgs<T> A, const ShellBoxes B) {
+template <typename T>
+__global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_pml_shell(const KArgs<T> A, const ShellBoxes B) {
     if (A.advance && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) advance_consts(*A.P, A.cur);
-    int b, tz, ty, tx;
-    shell_decode(B, blockIdx.x, b, tz, ty, tx);
-    shell_tile<T, XS>(A, B, b, tz, ty, tx);
+    int b, tu, tx;
+    shell_decode(B, blockIdx.x, b, tu, tx);
+    shell_tile<T>(A, B, b, tu, tx);
 }
 
 // Host side: one region-split step.  The shell kernel runs on s, the interior
@@ -321,9 +445,7 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     }
     const int nblk = (R.skip & 2) ? 0 : R.shell.block_first[R.shell.n];
     if (nblk > 0) {
-        if (R.shell.xs == 2) k_pml_shell<T, 2><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
-        else if (R.shell.xs == 4) k_pml_shell<T, 4><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
-        else k_pml_shell<T, 1><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
+        k_pml_shell<T><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
         ++l;
     }
     if (R.ghost_cap > 0 && !(R.skip & 4)) {

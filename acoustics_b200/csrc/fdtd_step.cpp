@@ -445,7 +445,42 @@ fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, in
         inc.resize(np);
         CUDA_TRY(s, cudaMemcpyAsync(inc.data(), P.dinc, np * 4, cudaMemcpyDeviceToHost, s->stream));
     }
+    // the z-slab box keeps its PML state in compact arrays (ShellBoxes)
+    const ShellBoxes& B = s->shell;
+    const bool zc = P.zcount > 0 && which >= FDTD_FIELD_PML_PX;
+    std::vector<char> zraw;
+    if (zc) {
+        const void* zsrc = which <= FDTD_FIELD_PML_PZ ? P.zpd[which - FDTD_FIELD_PML_PX] : P.zv[vbuf][which - FDTD_FIELD_VX];
+        zraw.resize(P.zcount * w);
+        CUDA_TRY(s, cudaMemcpyAsync(zraw.data(), zsrc, P.zcount * w, cudaMemcpyDeviceToHost, s->stream));
+    }
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    if (zc) {
+        const int b = B.zbox, V = B.vz;
+        const int X0 = B.x0[b], Y0 = B.y0[b], nxb = B.nx[b], nyb = B.ny[b];
+        auto slot = [&](int z) -> long long {  // compact slot of the cell (or its low face) z in the row
+            if (z >= B.za[b] && z < B.zae[b]) return (long long)(z / V - B.za[b] / V) * V + z % V;
+            if (z >= B.zb[b] && z < B.zbe[b]) return (long long)(B.gl[b] + z / V - B.zb[b] / V) * V + z % V;
+            return -1;
+        };
+        const int dface = which >= FDTD_FIELD_VX ? which - FDTD_FIELD_VX : -1;
+        for (int x = X0; x < X0 + nxb; ++x)
+            for (int y = Y0; y < Y0 + nyb; ++y) {
+                const long long row = ((long long)(x - X0) * nyb + (y - Y0)) * B.zrw;
+                for (int z = 0; z <= s->N[2]; ++z) {
+                    long long q = slot(z);
+                    if (dface == 2 && q < 0 && z == B.zae[b] && z > 0) {
+                        // boundary face after the first range: high face of its last cell
+                        const long long qc = slot(z - 1);
+                        q = ((z - 1) % V != V - 1) ? qc + 1 : (long long)B.ng[b] * V;
+                    }
+                    if (q < 0 || (dface != 2 && z == s->N[2])) continue;
+                    const long long c = x * s->SX + y * s->SY + z;
+                    if (f64) std::memcpy(raw.data() + c * 8, zraw.data() + (row + q) * 8, 8);
+                    else std::memcpy(raw.data() + c * 4, zraw.data() + (row + q) * 4, 4);
+                }
+            }
+    }
     const double* r64 = (const double*)raw.data();
     const float* r32 = (const float*)raw.data();
     long long o = 0;
@@ -486,6 +521,12 @@ std::vector<std::pair<void*, size_t>> snap_regions(fdtd_solver* s) {
             if (P.v[b][d]) r.push_back({P.v[b][d], np * w});
     r.push_back({P.cls, np});
     r.push_back({P.gobj, np});
+    if (P.zcount > 0)
+        for (int d = 0; d < 3; ++d) {
+            r.push_back({P.zpd[d], (size_t)P.zcount * w});
+            r.push_back({P.zv[0][d], (size_t)P.zcount * w});
+            r.push_back({P.zv[1][d], (size_t)P.zcount * w});
+        }
     r.push_back({P.consts, 2 * sizeof(StepConsts)});
     r.push_back({P.dev_error, sizeof(int)});
     return r;

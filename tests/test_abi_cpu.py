@@ -190,9 +190,11 @@ def test_scene_device_bytes_follows_the_arena_layout(fdtd_lib):
     big = S.config1()
     a32, a64 = scene_device_bytes(small), scene_device_bytes(small, precision=S.PRECISION_FP64)
     assert 0 < a32 < a64 < scene_device_bytes(big, precision=S.PRECISION_FP64)
-    n = 40 * 36 * 32
-    # per cell: flags 2 B, p[2] + dinc + pd[3] + 2 x 3 faces = 12 words (FP32)
-    assert 12 * 4 * n < a32 < 12 * 4 * n + 2 * n + (1 << 20)
+    # padded layout: rows of Nz+1 rounded up to 8, Ny+1 rows, Nx+1 planes
+    npad = 41 * 37 * 40
+    # per padded cell: flags 2 B, p[2] + dinc + pd[3] + 2 x 3 faces = 12 words (FP32),
+    # plus the compact PML storage of the z-slab box and the small tables
+    assert 12 * 4 * npad < a32 < 16 * 4 * npad + (1 << 20)
     bad = S.config1(); bad.cell_size = -1.0
     with pytest.raises(Exception):
         scene_device_bytes(bad)
