@@ -392,6 +392,27 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
     return FDTD_OK;
 }
 
+// Bounding box of the Gaussian source supports (cells whose centre may lie
+// strictly inside a source's box) clipped to the non-PML box.
+static Box3 source_region(const fdtd_solver* s) {
+    Box3 r{};
+    bool any = false;
+    for (const auto& g : s->sources) {
+        for (int d = 0; d < 3; ++d) {
+            const double a = (g.position[d] - 2.0 * g.width_space - s->bmin[d]) / s->h - 0.5;
+            const double b = (g.position[d] + 2.0 * g.width_space - s->bmin[d]) / s->h - 0.5;
+            const int lo = std::max(s->interior.lo[d], (int)std::floor(a));
+            const int hi = std::min(s->interior.hi[d], (int)std::ceil(b) + 1);
+            if (!any) { r.lo[d] = lo; r.hi[d] = hi; }
+            else { r.lo[d] = std::min(r.lo[d], lo); r.hi[d] = std::max(r.hi[d], hi); }
+        }
+        any = true;
+    }
+    for (int d = 0; d < 3; ++d)
+        if (!any || r.hi[d] < r.lo[d]) r.hi[d] = r.lo[d];
+    return r;
+}
+
 // Offsets of every device array of a solver inside its one arena allocation;
 // needs the geometry (solver_init_geometry) and the listener list.
 static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_options& o, Carver& cv) {
@@ -413,6 +434,14 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
         if (o.kernel != FDTD_KERNEL_PHASED) cv.add(&P.v[1][d], n * w);  // double-buffered faces
     }
     if (o.kernel == FDTD_KERNEL_PHASED) cv.add((void**)&s->d_lap, n * 8);
+    // spatial factors of the sources over their region (one table per source)
+    s->region.src_region = source_region(s);
+    {
+        const Box3& r = s->region.src_region;
+        P.src_cells = (long long)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);
+        if (P.src_cells > 0 && !s->sources.empty())
+            cv.add((void**)&P.src_g, (size_t)P.src_cells * s->sources.size() * 8);
+    }
     // compact storage of the z-slab box (region-split path)
     const ShellBoxes& SB = s->shell;
     if (o.kernel == FDTD_KERNEL_FUSED && SB.zbox >= 0) {
@@ -598,25 +627,6 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     s->region.interior = s->interior;
     s->region.shell = s->shell;
     s->region.sources = 0;
-    // bounding box of the source supports (cells whose centre may lie strictly inside)
-    {
-        Box3 r{};
-        bool any = false;
-        for (const auto& g : s->sources) {
-            for (int d = 0; d < 3; ++d) {
-                const double a = (g.position[d] - 2.0 * g.width_space - s->bmin[d]) / s->h - 0.5;
-                const double b = (g.position[d] + 2.0 * g.width_space - s->bmin[d]) / s->h - 0.5;
-                const int lo = std::max(s->interior.lo[d], (int)std::floor(a));
-                const int hi = std::min(s->interior.hi[d], (int)std::ceil(b) + 1);
-                if (!any) { r.lo[d] = lo; r.hi[d] = hi; }
-                else { r.lo[d] = std::min(r.lo[d], lo); r.hi[d] = std::max(r.hi[d], hi); }
-            }
-            any = true;
-        }
-        for (int d = 0; d < 3; ++d)
-            if (!any || r.hi[d] < r.lo[d]) r.hi[d] = r.lo[d];
-        s->region.src_region = r;
-    }
     for (int i = 0; i < P.n_plane; ++i) {
         P.plane[i].dir = s->planes[i].normal_dir;
         P.plane[i].sign = s->planes[i].normal_sign;
@@ -756,6 +766,7 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     fdtd_status st = upload_params(s);
     if (st != FDTD_OK) return st;
     CUDA_TRY(s, launch_consts_init(s->dP, t0, s->stream));
+    if (P.src_g) CUDA_TRY(s, launch_source_factors(s->dP, s->region.src_region, P.n_src, P.src_cells, s->stream));
     s->launches = 0;
     st = run_classification(s);
     if (st != FDTD_OK) return st;
@@ -806,6 +817,11 @@ fdtd_status fdtd_scene_info(const fdtd_scene_desc* sc, const fdtd_options* opt, 
     s.opt = o;
     s.precision = o.precision;
     solver_init_geometry(&s, sc);
+    for (int i = 0; i < sc->n_sources; ++i) {
+        fdtd_gaussian_source_desc g = sc->sources[i];
+        fdtd_gaussian_source_defaults(&g, s.c);
+        s.sources.push_back(g);
+    }
     s.listeners.assign(sc->listeners, sc->listeners + 3 * (size_t)sc->n_listeners);
     s.L = sc->n_listeners;
     Carver cv;

@@ -50,6 +50,7 @@ struct fdtd_batch {
     std::vector<Member> members;
     // device tables
     void* d_descs = nullptr;
+    int* d_next = nullptr;  // tile counters of the persistent kernels
     size_t desc_cap = 0;
     BatchTile* d_int = nullptr;
     size_t int_cap = 0;
@@ -181,6 +182,9 @@ fdtd_status rebuild(fdtd_batch* b) {
     if (!refs.empty())
         BATCH_TRY(b, cudaMemcpy(b->d_refs, refs.data(), refs.size() * sizeof(ListenerRef), cudaMemcpyHostToDevice));
     BatchLaunch& L = b->L;
+    if (!b->d_next) BATCH_TRY(b, cudaMalloc((void**)&b->d_next, 2 * sizeof(int)));
+    BATCH_TRY(b, cudaMemset(b->d_next, 0, 2 * sizeof(int)));
+    L.next = b->d_next;
     L.descs = b->d_descs;
     L.int_tiles = b->d_int;
     L.n_int = (int)it.size();
@@ -457,6 +461,7 @@ fdtd_status fdtd_batch_destroy(fdtd_batch* b) {
     for (auto& mb : b->members)
         if (mb.s) fdtd_solver_destroy(mb.s);
     if (b->d_descs) cudaFree(b->d_descs);
+    if (b->d_next) cudaFree(b->d_next);
     if (b->d_int) cudaFree(b->d_int);
     if (b->d_shell) cudaFree(b->d_shell);
     if (b->d_refs) cudaFree(b->d_refs);

@@ -22,20 +22,27 @@
 
 namespace fdtd {
 
+// Persistent tile loop: each CTA takes the next tile from a device counter
+// (reset by k_batch_advance at the end of the step), so CTAs that drew cheap
+// tiles take more of them; the member's arguments are reloaded into shared
+// memory only when the member changes.
 template <typename T, int XB>
 __global__ void __launch_bounds__(256) k_batch_interior(const BatchDesc<T>* __restrict__ D,
-                                                        const BatchTile* __restrict__ tiles, int n) {
+                                                        const BatchTile* __restrict__ tiles, int n,
+                                                        int* __restrict__ next) {
     __shared__ KArgs<T> sA;
     __shared__ Box3 sBox;
-    const int per = (n + gridDim.x - 1) / gridDim.x;
-    const int t0 = blockIdx.x * per;
-    const int t1 = min(n, t0 + per);
+    __shared__ int s_t;
+    const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
     int prev = -1;
-    for (int t = t0; t < t1; ++t) {
+    for (;;) {
+        if (lead) s_t = atomicAdd(next, 1);
+        __syncthreads();
+        const int t = s_t;
+        if (t >= n) break;
         const BatchTile tile = tiles[t];
         if (tile.m != prev) {
-            __syncthreads();
-            if (threadIdx.x == 0 && threadIdx.y == 0) {
+            if (lead) {
                 const BatchDesc<T>& d = D[tile.m];
                 sA = d.a[d.cur];
                 sBox = d.interior;
@@ -44,23 +51,27 @@ __global__ void __launch_bounds__(256) k_batch_interior(const BatchDesc<T>* __re
             prev = tile.m;
         }
         interior_tile<T, XB>(sA, sBox, tile.tz, tile.ty, tile.tx);
+        __syncthreads();  // s_t and the arguments are rewritten next
     }
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_batch_shell(const BatchDesc<T>* __restrict__ D,
-                                                                      const BatchTile* __restrict__ tiles, int n) {
+                                                                      const BatchTile* __restrict__ tiles, int n,
+                                                                      int* __restrict__ next) {
     __shared__ KArgs<T> sA;
     __shared__ ShellBoxes sB;
-    const int per = (n + gridDim.x - 1) / gridDim.x;
-    const int t0 = blockIdx.x * per;
-    const int t1 = min(n, t0 + per);
+    __shared__ int s_t;
+    const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
     int prev = -1;
-    for (int t = t0; t < t1; ++t) {
+    for (;;) {
+        if (lead) s_t = atomicAdd(next, 1);
+        __syncthreads();
+        const int t = s_t;
+        if (t >= n) break;
         const BatchTile tile = tiles[t];
         if (tile.m != prev) {
-            __syncthreads();
-            if (threadIdx.x == 0 && threadIdx.y == 0) {
+            if (lead) {
                 const BatchDesc<T>& d = D[tile.m];
                 sA = d.a[d.cur];
                 sB = d.shell;
@@ -69,6 +80,7 @@ __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_batch_shel
             prev = tile.m;
         }
         shell_tile<T>(sA, sB, tile.box, tile.tz, tile.tx);
+        __syncthreads();
     }
 }
 
@@ -108,10 +120,15 @@ __global__ void __launch_bounds__(128) k_batch_listeners(const BatchDesc<T>* __r
     listener_body<T>(*d.P, d.cur ^ 1, r.li, row);
 }
 
-// end of step: advance every active member's constants and flip its parity
+// end of step: advance every active member's constants, flip its parity and
+// reset the tile counters of the persistent kernels
 template <typename T>
-__global__ void k_batch_advance(BatchDesc<T>* __restrict__ D, int n) {
+__global__ void k_batch_advance(BatchDesc<T>* __restrict__ D, int n, int* __restrict__ next) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m == 0) {
+        next[0] = 0;
+        next[1] = 0;
+    }
     if (m >= n || !D[m].active) return;
     advance_consts(*D[m].P, D[m].cur);
     D[m].cur ^= 1;
@@ -127,9 +144,9 @@ cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, 
     if (e != cudaSuccess) return e;
     if (L.n_int > 0) {
         const dim3 block(32, 8);
-        if (L.xb == 2) k_batch_interior<T, 2><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int);
-        else if (L.xb == 8) k_batch_interior<T, 8><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int);
-        else k_batch_interior<T, 4><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int);
+        if (L.xb == 2) k_batch_interior<T, 2><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int, L.next);
+        else if (L.xb == 8) k_batch_interior<T, 8><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int, L.next);
+        else k_batch_interior<T, 4><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int, L.next);
         ++l;
     }
     if (L.ghost_blocks > 0) {
@@ -137,7 +154,7 @@ cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, 
         ++l;
     }
     if (L.n_shell > 0) {
-        k_batch_shell<T><<<L.ctas_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles, L.n_shell);
+        k_batch_shell<T><<<L.ctas_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles, L.n_shell, L.next + 1);
         ++l;
     }
     e = cudaEventRecord(join, s2);
@@ -163,7 +180,7 @@ cudaError_t launch_batch_tail(const BatchLaunch& L, cudaStream_t s, int* launche
         k_batch_listeners<T><<<(L.n_refs * 32 + 127) / 128, 128, 0, s>>>(D, L.refs, L.n_refs);
         ++l;
     }
-    k_batch_advance<T><<<(L.n_members + 127) / 128, 128, 0, s>>>(D, L.n_members);
+    k_batch_advance<T><<<(L.n_members + 127) / 128, 128, 0, s>>>(D, L.n_members, L.next);
     ++l;
     if (launches) *launches += l;
     return cudaGetLastError();

@@ -220,6 +220,9 @@ struct SolveParams {
     const double* listeners;      // 3*n_lis
     int* solid_pml;               // solid cells inside the PML (re-zeroed every step)
     int n_solid_pml;
+    double* src_g;                // [n_src][src_cells] spatial factor exp(-r^2/2w^2)*scale of each
+                                  // source over the source region (zero outside its box)
+    long long src_cells;          // cells of the source region
     int* ghost_list;              // non-PML bulk cells with a solid neighbour
     int* ghost_count;
     int ghost_cap;
@@ -323,6 +326,7 @@ struct BatchLaunch {
     int n_members;
     int xb, xs;
     int ctas_int, ctas_shell;    // persistent grid sizes
+    int* next;                   // [2] tile counters of the persistent interior / shell kernels (zero)
     int ghost_blocks;            // per member
     int src_blocks;              // per member (0: no member has a source)
 };
