@@ -45,10 +45,10 @@ def scene_info(scene: Scene, precision: int = PRECISION_FP32_COMPENSATED, kernel
 class SolveBatch:
     def __init__(self, scenes: Sequence[Scene] = (), steps: Optional[Sequence[int]] = None,
                  precision: int = PRECISION_FP32_COMPENSATED, graph_steps: int = 16, device: int = 0,
-                 tile_y: int = 0, x_chunk: int = 0, persistent_ctas: int = 0):
+                 tile_y: int = 0, x_chunk: int = 0):
         self._L = load()
         opt = Options(precision=precision, device=device, kernel=KERNEL_FUSED, graph_steps=graph_steps,
-                      tile_y=tile_y, x_chunk=x_chunk, persistent_ctas=persistent_ctas)
+                      tile_y=tile_y, x_chunk=x_chunk)
         h = C.c_void_p()
         check(self._L.fdtd_batch_create(0, None, None, C.byref(opt), C.byref(h)))
         self._h = h

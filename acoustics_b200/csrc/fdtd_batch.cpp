@@ -3,8 +3,8 @@
 // Each member is a complete fdtd_solver (own device arrays, classification,
 // ghost list, sources, listeners).  Its first step runs through the solver's
 // own path (it classifies the cells); afterwards every step of all active
-// members is one call of launch_batch_*: persistent shell and interior kernels
-// over tile tables of all members, then batched ghost-list, source, listener
+// members is one call of launch_batch_*: shell and interior kernels over tile
+// tables of all members, then batched ghost-list, source, listener
 // and advance kernels (fdtd_batch.cuh).  Members finish at their own step
 // counts and leave the tables; a captured graph of graph_steps batched steps is
 // replayed while the membership is unchanged.
@@ -50,7 +50,6 @@ struct fdtd_batch {
     std::vector<Member> members;
     // device tables
     void* d_descs = nullptr;
-    int* d_next = nullptr;  // tile counters of the persistent kernels
     size_t desc_cap = 0;
     BatchTile* d_int = nullptr;
     size_t int_cap = 0;
@@ -182,9 +181,6 @@ fdtd_status rebuild(fdtd_batch* b) {
     if (!refs.empty())
         BATCH_TRY(b, cudaMemcpy(b->d_refs, refs.data(), refs.size() * sizeof(ListenerRef), cudaMemcpyHostToDevice));
     BatchLaunch& L = b->L;
-    if (!b->d_next) BATCH_TRY(b, cudaMalloc((void**)&b->d_next, 2 * sizeof(int)));
-    BATCH_TRY(b, cudaMemset(b->d_next, 0, 2 * sizeof(int)));
-    L.next = b->d_next;
     L.descs = b->d_descs;
     L.int_tiles = b->d_int;
     L.n_int = (int)it.size();
@@ -195,14 +191,6 @@ fdtd_status rebuild(fdtd_batch* b) {
     L.n_members = (int)nm;
     L.xb = xb;
     L.xs = xs;
-    int sms = 148;
-    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->opt.device);
-    const int occ_i = batch_blocks_per_sm(b->precision, 0, xb);
-    const int occ_s = batch_blocks_per_sm(b->precision, 1, xs);
-    L.ctas_int = b->opt.persistent_ctas > 0 ? b->opt.persistent_ctas : sms * occ_i;
-    L.ctas_shell = b->opt.persistent_ctas > 0 ? b->opt.persistent_ctas : sms * occ_s;
-    L.ctas_int = std::max(1, std::min(L.ctas_int, std::max(1, L.n_int)));
-    L.ctas_shell = std::max(1, std::min(L.ctas_shell, std::max(1, L.n_shell)));
     L.ghost_blocks = std::min(max_ghost, 32);
     L.src_blocks = max_src;
     if (b->graph) {
@@ -461,7 +449,6 @@ fdtd_status fdtd_batch_destroy(fdtd_batch* b) {
     for (auto& mb : b->members)
         if (mb.s) fdtd_solver_destroy(mb.s);
     if (b->d_descs) cudaFree(b->d_descs);
-    if (b->d_next) cudaFree(b->d_next);
     if (b->d_int) cudaFree(b->d_int);
     if (b->d_shell) cudaFree(b->d_shell);
     if (b->d_refs) cudaFree(b->d_refs);

@@ -10,10 +10,9 @@
 // Per step:  k_batch_shell (PML tiles of all members)  ||  k_batch_interior ->
 //            k_batch_ghost  (second stream), then k_batch_sources (launch_batch),
 //            k_batch_listeners, k_batch_advance (launch_batch_tail).
-// The shell and interior kernels are persistent: gridDim CTAs each take one
-// contiguous range of a tile table sorted by member, reload the member's
-// arguments into shared memory only when the member changes, and call the
-// same tile functions as the single-solve kernels.
+// The shell and interior kernels run one CTA per entry of a tile table that
+// lists the tiles of every member (sorted by member), and call the same tile
+// functions as the single-solve kernels.
 #pragma once
 #include "fdtd_device.cuh"
 #include "fdtd_hot.cuh"
@@ -22,66 +21,23 @@
 
 namespace fdtd {
 
-// Persistent tile loop: each CTA takes the next tile from a device counter
-// (reset by k_batch_advance at the end of the step), so CTAs that drew cheap
-// tiles take more of them; the member's arguments are reloaded into shared
-// memory only when the member changes.
+// One CTA per tile of the tables (all members in one launch).  The member's
+// arguments are read through references into its descriptor in global memory
+// (L1-resident after the first warp), so a CTA starts without a barrier.
 template <typename T, int XB>
 __global__ void __launch_bounds__(256) k_batch_interior(const BatchDesc<T>* __restrict__ D,
-                                                        const BatchTile* __restrict__ tiles, int n,
-                                                        int* __restrict__ next) {
-    __shared__ KArgs<T> sA;
-    __shared__ Box3 sBox;
-    __shared__ int s_t;
-    const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
-    int prev = -1;
-    for (;;) {
-        if (lead) s_t = atomicAdd(next, 1);
-        __syncthreads();
-        const int t = s_t;
-        if (t >= n) break;
-        const BatchTile tile = tiles[t];
-        if (tile.m != prev) {
-            if (lead) {
-                const BatchDesc<T>& d = D[tile.m];
-                sA = d.a[d.cur];
-                sBox = d.interior;
-            }
-            __syncthreads();
-            prev = tile.m;
-        }
-        interior_tile<T, XB>(sA, sBox, tile.tz, tile.ty, tile.tx);
-        __syncthreads();  // s_t and the arguments are rewritten next
-    }
+                                                        const BatchTile* __restrict__ tiles) {
+    const BatchTile tile = tiles[blockIdx.x];
+    const BatchDesc<T>& d = D[tile.m];
+    interior_tile<T, XB>(d.a[d.cur], d.interior, tile.tz, tile.ty, tile.tx);
 }
 
 template <typename T>
 __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_batch_shell(const BatchDesc<T>* __restrict__ D,
-                                                                      const BatchTile* __restrict__ tiles, int n,
-                                                                      int* __restrict__ next) {
-    __shared__ KArgs<T> sA;
-    __shared__ ShellBoxes sB;
-    __shared__ int s_t;
-    const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
-    int prev = -1;
-    for (;;) {
-        if (lead) s_t = atomicAdd(next, 1);
-        __syncthreads();
-        const int t = s_t;
-        if (t >= n) break;
-        const BatchTile tile = tiles[t];
-        if (tile.m != prev) {
-            if (lead) {
-                const BatchDesc<T>& d = D[tile.m];
-                sA = d.a[d.cur];
-                sB = d.shell;
-            }
-            __syncthreads();
-            prev = tile.m;
-        }
-        shell_tile<T>(sA, sB, tile.box, tile.tz, tile.tx);
-        __syncthreads();
-    }
+                                                                      const BatchTile* __restrict__ tiles) {
+    const BatchTile tile = tiles[blockIdx.x];
+    const BatchDesc<T>& d = D[tile.m];
+    shell_tile<T>(d.a[d.cur], d.shell, tile.box, tile.tz, tile.tx);
 }
 
 // grid (ghost_blocks, members)
@@ -120,15 +76,10 @@ __global__ void __launch_bounds__(128) k_batch_listeners(const BatchDesc<T>* __r
     listener_body<T>(*d.P, d.cur ^ 1, r.li, row);
 }
 
-// end of step: advance every active member's constants, flip its parity and
-// reset the tile counters of the persistent kernels
+// end of step: advance every active member's constants and flip its parity
 template <typename T>
-__global__ void k_batch_advance(BatchDesc<T>* __restrict__ D, int n, int* __restrict__ next) {
+__global__ void k_batch_advance(BatchDesc<T>* __restrict__ D, int n) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m == 0) {
-        next[0] = 0;
-        next[1] = 0;
-    }
     if (m >= n || !D[m].active) return;
     advance_consts(*D[m].P, D[m].cur);
     D[m].cur ^= 1;
@@ -144,9 +95,9 @@ cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, 
     if (e != cudaSuccess) return e;
     if (L.n_int > 0) {
         const dim3 block(32, 8);
-        if (L.xb == 2) k_batch_interior<T, 2><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int, L.next);
-        else if (L.xb == 8) k_batch_interior<T, 8><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int, L.next);
-        else k_batch_interior<T, 4><<<L.ctas_int, block, 0, s2>>>(D, L.int_tiles, L.n_int, L.next);
+        if (L.xb == 2) k_batch_interior<T, 2><<<L.n_int, block, 0, s2>>>(D, L.int_tiles);
+        else if (L.xb == 8) k_batch_interior<T, 8><<<L.n_int, block, 0, s2>>>(D, L.int_tiles);
+        else k_batch_interior<T, 4><<<L.n_int, block, 0, s2>>>(D, L.int_tiles);
         ++l;
     }
     if (L.ghost_blocks > 0) {
@@ -154,7 +105,7 @@ cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, 
         ++l;
     }
     if (L.n_shell > 0) {
-        k_batch_shell<T><<<L.ctas_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles, L.n_shell, L.next + 1);
+        k_batch_shell<T><<<L.n_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles);
         ++l;
     }
     e = cudaEventRecord(join, s2);
@@ -180,7 +131,7 @@ cudaError_t launch_batch_tail(const BatchLaunch& L, cudaStream_t s, int* launche
         k_batch_listeners<T><<<(L.n_refs * 32 + 127) / 128, 128, 0, s>>>(D, L.refs, L.n_refs);
         ++l;
     }
-    k_batch_advance<T><<<(L.n_members + 127) / 128, 128, 0, s>>>(D, L.n_members, L.next);
+    k_batch_advance<T><<<(L.n_members + 127) / 128, 128, 0, s>>>(D, L.n_members);
     ++l;
     if (launches) *launches += l;
     return cudaGetLastError();

@@ -325,8 +325,6 @@ struct BatchLaunch {
     int n_refs;
     int n_members;
     int xb, xs;
-    int ctas_int, ctas_shell;    // persistent grid sizes
-    int* next;                   // [2] tile counters of the persistent interior / shell kernels (zero)
     int ghost_blocks;            // per member
     int src_blocks;              // per member (0: no member has a source)
 };

@@ -32,17 +32,4 @@ cudaError_t launch_batch_fp32(const BatchLaunch& L, cudaStream_t s, cudaStream_t
                               cudaEvent_t join, int* launches) {
     return launch_batch<float>(L, s, s2, fork, join, launches);
 }
-int batch_blocks_per_sm_fp64(int which, int shape);
-int batch_blocks_per_sm(int precision, int which, int shape) {
-    if (precision == 0) return batch_blocks_per_sm_fp64(which, shape);
-    int n = 0;
-    if (which == 0) {
-        if (shape == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_interior<float, 2>, 256, 0);
-        else if (shape == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_interior<float, 8>, 256, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_interior<float, 4>, 256, 0);
-    } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_shell<float>, 256, 0);
-    }
-    return n > 0 ? n : 1;
-}
 }  // namespace fdtd

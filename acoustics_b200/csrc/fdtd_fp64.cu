@@ -442,15 +442,4 @@ cudaError_t launch_batch_fp64(const BatchLaunch& L, cudaStream_t s, cudaStream_t
 cudaError_t launch_batch_tail_any(int precision, const BatchLaunch& L, cudaStream_t s, int* launches) {
     return precision == 0 ? launch_batch_tail<double>(L, s, launches) : launch_batch_tail<float>(L, s, launches);
 }
-int batch_blocks_per_sm_fp64(int which, int shape) {
-    int n = 0;
-    if (which == 0) {
-        if (shape == 2) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_interior<double, 2>, 256, 0);
-        else if (shape == 8) cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_interior<double, 8>, 256, 0);
-        else cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_interior<double, 4>, 256, 0);
-    } else {
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_shell<double>, 256, 0);
-    }
-    return n > 0 ? n : 1;
-}
 }  // namespace fdtd

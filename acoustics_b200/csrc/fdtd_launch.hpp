@@ -14,15 +14,13 @@ cudaError_t launch_step_regions_fp32(const SolveParams* dP, const SolveParams& h
                                      cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
                                      int* launches);
 
-// batched step of many members (fdtd_batch.cuh); blocks_per_sm: occupancy of the
-// persistent interior (which = 0) or shell (which = 1) kernel for shape xb / xs
+// batched step of many members (fdtd_batch.cuh)
 cudaError_t launch_batch_fp64(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, cudaEvent_t fork,
                               cudaEvent_t join, int* launches);
 cudaError_t launch_batch_fp32(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, cudaEvent_t fork,
                               cudaEvent_t join, int* launches);
 // listener rows + advance of a batched step, for either field type (FP64 unit)
 cudaError_t launch_batch_tail_any(int precision, const BatchLaunch& L, cudaStream_t s, int* launches);
-int batch_blocks_per_sm(int precision, int which, int shape);
 
 // fdtd_fp64.cu (compiled with -fmad=false)
 cudaError_t launch_prologue_fp64(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s);

@@ -73,7 +73,7 @@ class Options(C.Structure):
     _fields_ = [
         ("precision", C.c_int32), ("device", C.c_int32), ("kernel", C.c_int32),
         ("graph_steps", C.c_int32), ("tile_y", C.c_int32), ("x_chunk", C.c_int32),
-        ("persistent_ctas", C.c_int32), ("_pad", C.c_int32),
+        ("_reserved0", C.c_int32), ("_reserved1", C.c_int32),
     ]
 
 

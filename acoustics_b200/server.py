@@ -21,10 +21,10 @@ from .scene import (KERNEL_FUSED, PRECISION_FP32_COMPENSATED, REQ_DONE, REQ_FAIL
 class SolveServer:
     def __init__(self, precision: int = PRECISION_FP32_COMPENSATED, graph_steps: int = 16, device: int = 0,
                  hbm_budget_bytes: int = 0, max_members: int = 0, chunk_steps: int = 0, tile_y: int = 0,
-                 x_chunk: int = 0, persistent_ctas: int = 0):
+                 x_chunk: int = 0):
         self._L = load()
         opt = Options(precision=precision, device=device, kernel=KERNEL_FUSED, graph_steps=graph_steps,
-                      tile_y=tile_y, x_chunk=x_chunk, persistent_ctas=persistent_ctas)
+                      tile_y=tile_y, x_chunk=x_chunk)
         cfg = ServerConfig(hbm_budget_bytes=int(hbm_budget_bytes), max_members=int(max_members),
                            chunk_steps=int(chunk_steps))
         h = C.c_void_p()

@@ -130,8 +130,8 @@ typedef struct {
     int32_t graph_steps;      /* >0: capture this many steps per CUDA graph launch       */
     int32_t tile_y;           /* fused path: x planes a PML-shell thread marches over; 0: 8   */
     int32_t x_chunk;          /* fused path: interior x planes per thread (2, 4, 8); 0: 2        */
-    int32_t persistent_ctas;  /* batches: CTAs of the persistent kernels; 0: from occupancy    */
-    int32_t _pad;
+    int32_t _reserved0;       /* 0 */
+    int32_t _reserved1;       /* 0 */
 } fdtd_options;
 
 typedef struct {

@@ -37,7 +37,7 @@ def test_batch_members_equal_standalone(fdtd_lib, precision, graph_steps):
             assert np.array_equal(y, alone(sc, precision, sc.steps)), f"member {m}"
 
 
-@pytest.mark.parametrize("tile", [dict(x_chunk=2, tile_y=2), dict(x_chunk=8, tile_y=1, persistent_ctas=7)])
+@pytest.mark.parametrize("tile", [dict(x_chunk=2, tile_y=2), dict(x_chunk=8, tile_y=1), dict(x_chunk=4, tile_y=16)])
 def test_batch_tile_shapes(fdtd_lib, tile):
     scenes = uneven_scenes(12, 4)
     with SolveBatch(scenes, precision=S.PRECISION_FP32_COMPENSATED, **tile) as b:
