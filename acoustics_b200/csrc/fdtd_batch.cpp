@@ -58,8 +58,10 @@ struct fdtd_batch {
     ListenerRef* d_refs = nullptr;
     size_t refs_cap = 0;
     BatchLaunch L{};
+    size_t table_bytes = 0;  // one descriptor table (the second, at this offset, has every parity flipped)
+    int flip = 0;            // table of the next step
     bool dirty = true;
-    cudaGraphExec_t graph = nullptr;
+    cudaGraphExec_t graph[2] = {nullptr, nullptr};  // G steps starting at table 0 / 1
     long long launches = 0, last_launches = 0, graph_launches = 0;
     std::string err;
 };
@@ -129,7 +131,8 @@ fdtd_status rebuild(fdtd_batch* b) {
     const int xs = b->opt.tile_y > 0 ? std::min(b->opt.tile_y, 256) : FDTD_SHELL_PLANES;
     const size_t dsz = f64 ? desc_bytes<double>() : desc_bytes<float>();
     const size_t nm = b->members.size();
-    std::vector<char> descs(std::max<size_t>(nm, 1) * dsz, 0);
+    const size_t tbytes = std::max<size_t>(nm, 1) * dsz;
+    std::vector<char> descs(2 * tbytes, 0);
     std::vector<BatchTile> it, st;
     std::vector<ListenerRef> refs;
     int max_ghost = 0, max_src = 0;
@@ -138,8 +141,16 @@ fdtd_status rebuild(fdtd_batch* b) {
         if (!mb.s) continue;
         if (mb.s->shell.xs != xs) build_shell_boxes(mb.s, xs);
         mb.s->region.shell = mb.s->shell;
-        if (f64) fill_desc<double>(*reinterpret_cast<BatchDesc<double>*>(&descs[m * dsz]), mb.s, mb.active);
-        else fill_desc<float>(*reinterpret_cast<BatchDesc<float>*>(&descs[m * dsz]), mb.s, mb.active);
+        for (int par = 0; par < 2; ++par) {
+            char* dst = &descs[par * tbytes + m * dsz];
+            if (f64) {
+                fill_desc<double>(*reinterpret_cast<BatchDesc<double>*>(dst), mb.s, mb.active);
+                reinterpret_cast<BatchDesc<double>*>(dst)->cur ^= par;
+            } else {
+                fill_desc<float>(*reinterpret_cast<BatchDesc<float>*>(dst), mb.s, mb.active);
+                reinterpret_cast<BatchDesc<float>*>(dst)->cur ^= par;
+            }
+        }
         if (!mb.active) continue;
         const Box3& I = mb.s->region.interior;
         const int nx = I.hi[0] - I.lo[0], ny = I.hi[1] - I.lo[1], nz = I.hi[2] - I.lo[2];
@@ -150,9 +161,11 @@ fdtd_status rebuild(fdtd_batch* b) {
                     for (int z = 0; z < tz; ++z) it.push_back({(int)m, 0, z, y, x});
         }
         const ShellBoxes& B = mb.s->shell;
+        // the member's first shell tile (ty = 1) advances its step constants
+        const size_t first_tile = st.size();
         for (int bx = 0; bx < B.n; ++bx)
             for (int x = 0; x < B.tx[bx]; ++x)
-                for (int u = 0; u < B.tu[bx]; ++u) st.push_back({(int)m, bx, u, 0, x});
+                for (int u = 0; u < B.tu[bx]; ++u) st.push_back({(int)m, bx, u, st.size() == first_tile ? 1 : 0, x});
         for (int li = 0; li < mb.s->L; ++li) refs.push_back({(int)m, li});
         max_ghost = std::max(max_ghost, (mb.s->region.ghost_cap + 127) / 128);
         if (mb.s->hP.n_src > 0) {
@@ -182,6 +195,8 @@ fdtd_status rebuild(fdtd_batch* b) {
         BATCH_TRY(b, cudaMemcpy(b->d_refs, refs.data(), refs.size() * sizeof(ListenerRef), cudaMemcpyHostToDevice));
     BatchLaunch& L = b->L;
     L.descs = b->d_descs;
+    b->table_bytes = tbytes;
+    b->flip = 0;
     L.int_tiles = b->d_int;
     L.n_int = (int)it.size();
     L.shell_tiles = b->d_shell;
@@ -193,27 +208,33 @@ fdtd_status rebuild(fdtd_batch* b) {
     L.xs = xs;
     L.ghost_blocks = std::min(max_ghost, 32);
     L.src_blocks = max_src;
-    if (b->graph) {
-        cudaGraphExecDestroy(b->graph);
-        b->graph = nullptr;
-    }
+    for (int i = 0; i < 2; ++i)
+        if (b->graph[i]) {
+            cudaGraphExecDestroy(b->graph[i]);
+            b->graph[i] = nullptr;
+        }
     b->dirty = false;
     return FDTD_OK;
 }
 
 fdtd_status enqueue(fdtd_batch* b) {
     int l = 0;
+    BatchLaunch L = b->L;
+    L.descs = static_cast<char*>(b->d_descs) + b->flip * b->table_bytes;
+    b->flip ^= 1;
     cudaError_t e = b->precision == FDTD_PRECISION_FP64
-                        ? launch_batch_fp64(b->L, b->stream, b->stream2, b->ev_fork, b->ev_join, &l)
-                        : launch_batch_fp32(b->L, b->stream, b->stream2, b->ev_fork, b->ev_join, &l);
-    if (e == cudaSuccess) e = launch_batch_tail_any(b->precision, b->L, b->stream, &l);
+                        ? launch_batch_fp64(L, b->stream, b->stream2, b->ev_fork, b->ev_join, &l)
+                        : launch_batch_fp32(L, b->stream, b->stream2, b->ev_fork, b->ev_join, &l);
+    if (e == cudaSuccess) e = launch_batch_tail_any(b->precision, L, b->stream, &l);
     b->launches += l;
     if (e != cudaSuccess) return batch_fail(b, FDTD_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
     return FDTD_OK;
 }
 
+// Capture n (even) steps starting at the current table into graph[flip].
 fdtd_status capture(fdtd_batch* b, int n) {
     cudaGraph_t g = nullptr;
+    const int f0 = b->flip;
     BATCH_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     const long long l0 = b->launches;
     fdtd_status st = FDTD_OK;
@@ -221,12 +242,13 @@ fdtd_status capture(fdtd_batch* b, int n) {
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     b->graph_launches = b->launches - l0;
     b->launches = l0;
+    b->flip = f0;  // capturing launched nothing
     if (st != FDTD_OK) {
         if (g) cudaGraphDestroy(g);
         return st;
     }
     if (e != cudaSuccess) return batch_fail(b, FDTD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
-    e = cudaGraphInstantiate(&b->graph, g, 0);
+    e = cudaGraphInstantiate(&b->graph[f0], g, 0);
     cudaGraphDestroy(g);
     if (e != cudaSuccess) return batch_fail(b, FDTD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
     return FDTD_OK;
@@ -344,12 +366,13 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int32_t n_steps, int32_t* n_active) {
         }
         if (G > 0 && chunk >= G) {
             chunk = (chunk / G) * G;
-            if (!b->graph) {
+            if (!b->graph[b->flip]) {
                 fdtd_status st = capture(b, G);
                 if (st != FDTD_OK) return st;
             }
             for (int64_t i = 0; i < chunk / G; ++i) {
-                BATCH_TRY(b, cudaGraphLaunch(b->graph, b->stream));
+                // G is even: the graph leaves the table parity as it found it
+                BATCH_TRY(b, cudaGraphLaunch(b->graph[b->flip], b->stream));
                 b->launches += b->graph_launches;
             }
         } else {
@@ -445,7 +468,8 @@ fdtd_status fdtd_batch_destroy(fdtd_batch* b) {
     if (!b) return FDTD_OK;
     cudaSetDevice(b->opt.device);
     if (b->stream) cudaStreamSynchronize(b->stream);
-    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (int i = 0; i < 2; ++i)
+        if (b->graph[i]) cudaGraphExecDestroy(b->graph[i]);
     for (auto& mb : b->members)
         if (mb.s) fdtd_solver_destroy(mb.s);
     if (b->d_descs) cudaFree(b->d_descs);

@@ -4,12 +4,16 @@
 // Every member keeps its own device state (the arrays of its fdtd_solver); a
 // descriptor per member holds its kernel arguments for both buffer parities,
 // its boxes, its listener ring and its current parity, which the last kernel
-// of a step flips on the device.  Because parity and step constants live on
-// the device, a captured graph of N batched steps replays for any step index.
+// of a step flips.  Because the step constants live on the device, a captured
+// graph of an even number of batched steps replays for any step index.
 //
-// Per step:  k_batch_shell (PML tiles of all members)  ||  k_batch_interior ->
-//            k_batch_ghost  (second stream), then k_batch_sources (launch_batch),
-//            k_batch_listeners, k_batch_advance (launch_batch_tail).
+// Per step:  k_batch_shell (PML tiles of all members; its first tile of a
+//            member writes the member's next-step constants)  ||
+//            k_batch_interior -> k_batch_ghost -> k_batch_sources (second
+//            stream), then k_batch_listeners (launch_batch_tail).
+// The descriptors come in two tables, one per step parity (every member's
+// parity flips each step), so consecutive steps alternate tables and no kernel
+// flips parities on the device.
 // The shell and interior kernels run one CTA per entry of a tile table that
 // lists the tiles of every member (sorted by member), and call the same tile
 // functions as the single-solve kernels.
@@ -32,11 +36,14 @@ __global__ void __launch_bounds__(256) k_batch_interior(const BatchDesc<T>* __re
     interior_tile<T, XB>(d.a[d.cur], d.interior, tile.tz, tile.ty, tile.tx);
 }
 
+// The first shell tile of a member (tile.ty = 1) also writes the member's
+// constants of the next step (consts[cur ^ 1]; this step reads consts[cur]).
 template <typename T>
 __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_batch_shell(const BatchDesc<T>* __restrict__ D,
                                                                       const BatchTile* __restrict__ tiles) {
     const BatchTile tile = tiles[blockIdx.x];
     const BatchDesc<T>& d = D[tile.m];
+    if (tile.ty && threadIdx.x == 0 && threadIdx.y == 0) advance_consts(*d.P, d.cur);
     shell_tile<T>(d.a[d.cur], d.shell, tile.box, tile.tz, tile.tx);
 }
 
@@ -76,15 +83,6 @@ __global__ void __launch_bounds__(128) k_batch_listeners(const BatchDesc<T>* __r
     listener_body<T>(*d.P, d.cur ^ 1, r.li, row);
 }
 
-// end of step: advance every active member's constants and flip its parity
-template <typename T>
-__global__ void k_batch_advance(BatchDesc<T>* __restrict__ D, int n) {
-    const int m = blockIdx.x * blockDim.x + threadIdx.x;
-    if (m >= n || !D[m].active) return;
-    advance_consts(*D[m].P, D[m].cur);
-    D[m].cur ^= 1;
-}
-
 template <typename T>
 cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, cudaEvent_t fork,
                          cudaEvent_t join, int* launches) {
@@ -104,6 +102,12 @@ cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, 
         k_batch_ghost<T><<<dim3(L.ghost_blocks, L.n_members), 128, 0, s2>>>(D);
         ++l;
     }
+    if (L.src_blocks > 0) {
+        // source cells are non-PML cells: ordered after the interior and ghost updates
+        // of their cells, concurrent with the shell
+        k_batch_sources<T><<<dim3(L.src_blocks, L.n_members), 256, 0, s2>>>(D);
+        ++l;
+    }
     if (L.n_shell > 0) {
         k_batch_shell<T><<<L.n_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles);
         ++l;
@@ -111,29 +115,21 @@ cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, 
     e = cudaEventRecord(join, s2);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
     if (e != cudaSuccess) return e;
-    if (L.src_blocks > 0) {
-        k_batch_sources<T><<<dim3(L.src_blocks, L.n_members), 256, 0, s>>>(D);
-        ++l;
-    }
     if (launches) *launches += l;
     return cudaGetLastError();
 }
 
-// Listener rows and the end-of-step advance.  Instantiated in the FP64
-// translation unit for both field types, like the single-solve listener
-// kernel, so the double-precision MLS arithmetic is compiled the same way
-// (no FMA contraction) and batch rows equal single-solve rows bit for bit.
+// Listener rows of a batched step.  Instantiated in the FP64 translation unit
+// for both field types, like the single-solve listener kernel, so the
+// double-precision MLS arithmetic is compiled the same way (no FMA
+// contraction) and batch rows equal single-solve rows bit for bit.
 template <typename T>
 cudaError_t launch_batch_tail(const BatchLaunch& L, cudaStream_t s, int* launches) {
     BatchDesc<T>* D = static_cast<BatchDesc<T>*>(L.descs);
-    int l = 0;
     if (L.n_refs > 0) {
         k_batch_listeners<T><<<(L.n_refs * 32 + 127) / 128, 128, 0, s>>>(D, L.refs, L.n_refs);
-        ++l;
+        if (launches) *launches += 1;
     }
-    k_batch_advance<T><<<(L.n_members + 127) / 128, 128, 0, s>>>(D, L.n_members);
-    ++l;
-    if (launches) *launches += l;
     return cudaGetLastError();
 }
 

@@ -454,19 +454,21 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
         k_ghost_cells<T><<<blocks, 128, 0, concurrent ? s2 : s>>>(dP, cur);
         ++l;
     }
-    if (concurrent) {
-        e = cudaEventRecord(join, s2);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
-        if (e != cudaSuccess) return e;
-    }
     if (R.sources) {
+        // source cells are non-PML cells: after the interior and ghost updates of
+        // their cells (same stream), concurrent with the shell
         const Box3& r = R.src_region;
         const long long total = (long long)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);
         if (total > 0) {
             const long long g = (total + 255) / 256;
-            k_sources<T><<<(unsigned)(g < 148 * 16 ? g : 148 * 16), 256, 0, s>>>(dP, cur, r);
+            k_sources<T><<<(unsigned)(g < 148 * 16 ? g : 148 * 16), 256, 0, concurrent ? s2 : s>>>(dP, cur, r);
             ++l;
         }
+    }
+    if (concurrent) {
+        e = cudaEventRecord(join, s2);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
+        if (e != cudaSuccess) return e;
     }
     if (launches) *launches += l;
     return cudaGetLastError();
