@@ -456,6 +456,8 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
     cv.add((void**)&P.dev_error, 16);
     cv.add((void**)&s->d_status, 16);
     cv.add((void**)&P.listeners, std::max<size_t>(1, s->listeners.size()) * 8);
+    cv.add((void**)&P.lis_rows, (size_t)std::max(1, s->L) * 64 * sizeof(LisRow));
+    cv.add((void**)&P.lis_plan, (size_t)std::max(1, s->L) * sizeof(LisPlan));
     for (int d = 0; d < 3; ++d) {
         cv.add((void**)&P.pml_cell[d], N[d]);
         cv.add((void**)&P.pml_face[d], N[d] + 1);
@@ -763,6 +765,7 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     s->n_solid_pml = 0;
     P.solid_pml = nullptr;
     P.n_solid_pml = 0;
+    P.lis_ready = 0;  // the first step classifies and rebuilds the listener fits
     fdtd_status st = upload_params(s);
     if (st != FDTD_OK) return st;
     CUDA_TRY(s, launch_consts_init(s->dP, t0, s->stream));

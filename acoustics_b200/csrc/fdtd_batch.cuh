@@ -80,7 +80,8 @@ __global__ void __launch_bounds__(128) k_batch_listeners(const BatchDesc<T>* __r
     if (!d.active) return;
     const long long step = d.P->consts[d.cur].step;
     double* row = d.ring + (size_t)(step % d.ring_cap) * d.n_lis;
-    listener_body<T>(*d.P, d.cur ^ 1, r.li, row);
+    if (d.P->lis_ready) listener_plan<T>(*d.P, d.cur ^ 1, r.li, row);
+    else listener_body<T>(*d.P, d.cur ^ 1, r.li, row);
 }
 
 template <typename T>

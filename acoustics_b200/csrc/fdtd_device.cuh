@@ -110,6 +110,23 @@ struct ShellBoxes {
 
 struct SolveParams;
 
+// Precomputed order-1 MLS of one listener (static classification): the sample
+// value is sum_r w_r * value_r over its rows.  A row is the pressure of a cell
+// (kind 0) or the ghost pressure of one ghost face of a solid cell
+// (kind 1 + 2*dim + (sign > 0)).  mode 1: the value of one cell (fewer than
+// four samples); mode 2: no sample or a rank-deficient fit (0 and the error
+// flag).  cells[] are the enclosing cells whose NaN test the reference's
+// fit applies; a NaN there sends the listener back to the full fit.
+struct LisRow {
+    int cell;
+    int kind;
+    double w;
+};
+struct LisPlan {
+    int mode, n, nc, cell;
+    int cells[8];
+};
+
 // Per-axis PML flags of index i (one byte, read once per thread and axis by the
 // shell kernel instead of four table lookups).
 enum : uint8_t {
@@ -218,6 +235,9 @@ struct SolveParams {
     StepConsts* consts;           // [2], indexed by the step parity
     int* dev_error;               // sticky device-side error flags
     const double* listeners;      // 3*n_lis
+    LisRow* lis_rows;             // [n_lis][64] precomputed MLS rows (static scenes)
+    LisPlan* lis_plan;            // [n_lis]
+    int lis_ready;                // plans valid for the current classification
     int* solid_pml;               // solid cells inside the PML (re-zeroed every step)
     int n_solid_pml;
     double* src_g;                // [n_src][src_cells] spatial factor exp(-r^2/2w^2)*scale of each

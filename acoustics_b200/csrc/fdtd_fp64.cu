@@ -379,6 +379,18 @@ cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int
     return cudaGetLastError();
 }
 
+// listener fit plans from the current classification (static scenes, once)
+__global__ void k_set_lis_ready(SolveParams* __restrict__ Pp) { Pp->lis_ready = 1; }
+
+cudaError_t launch_listener_prep(SolveParams* dP, int precision, int newp, int n_lis, cudaStream_t s) {
+    if (n_lis <= 0) return cudaSuccess;
+    const int grid = (n_lis + 3) / 4;
+    if (precision == 0) k_listener_prep<double><<<grid, 128, 0, s>>>(dP, newp);
+    else k_listener_prep<float><<<grid, 128, 0, s>>>(dP, newp);
+    k_set_lis_ready<<<1, 1, 0, s>>>(dP);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_cls_reset(const SolveParams* dP, long long ncell, cudaStream_t s) {
     k_cls_reset<<<grid_for(ncell, 256), 256, 0, s>>>(dP, ncell);
     return cudaGetLastError();

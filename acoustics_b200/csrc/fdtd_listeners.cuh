@@ -57,8 +57,11 @@ __device__ void build_row(const SolveParams& P, const T* __restrict__ pold, doub
     mls_row(pt, fp, pg, A, b);
 }
 
-// Listener li of solve P into out_row[li]; called by a whole warp.
-template <typename T>
+// Listener li of solve P into out_row[li]; called by a whole warp.  With PREP
+// the same fit is built from the classification alone and, instead of a value,
+// its plan is written: the weight of every sample row in the fitted value at
+// the listener (x0 = e0' R^-1 Q' b = (Q [R^-T e0; 0])' b, b_r = w_r value_r).
+template <typename T, bool PREP = false>
 __device__ void listener_body(const SolveParams& P, int newp, int li, double* __restrict__ out_row) {
     const int lane = threadIdx.x & 31;
     const T* __restrict__ pnew = (const T*)P.p[newp];
@@ -89,10 +92,21 @@ __device__ void listener_body(const SolveParams& P, int newp, int li, double* __
     const int total = __shfl_sync(0xffffffffu, incl, nc - 1);
     const unsigned keptmask = __ballot_sync(0xffffffffu, kept);
     const int nk = __popc(keptmask);
+    if constexpr (PREP) {
+        if (lane < 8) P.lis_plan[li].cells[lane] = lane < nc ? cellq : 0;
+        if (lane == 0) {
+            P.lis_plan[li].nc = nc;
+            P.lis_plan[li].n = 0;
+        }
+    }
     if (nk == 0) {
         if (lane == 0) {
-            out_row[li] = 0.0;
-            atomicOr(P.dev_error, 1);
+            if constexpr (PREP) {
+                P.lis_plan[li].mode = 2;
+            } else {
+                out_row[li] = 0.0;
+                atomicOr(P.dev_error, 1);
+            }
         }
         return;
     }
@@ -112,7 +126,15 @@ __device__ void listener_body(const SolveParams& P, int newp, int li, double* __
             if (dq < best) { best = dq; bl = q; }
         }
         const double val = __shfl_sync(0xffffffffu, v, bl < 0 ? 0 : bl);
-        if (lane == 0) out_row[li] = val;
+        if constexpr (PREP) {
+            const int cb = __shfl_sync(0xffffffffu, cellq, bl < 0 ? 0 : bl);
+            if (lane == 0) {
+                P.lis_plan[li].mode = 1;
+                P.lis_plan[li].cell = cb;
+            }
+        } else {
+            if (lane == 0) out_row[li] = val;
+        }
         return;
     }
 
@@ -135,6 +157,22 @@ __device__ void listener_body(const SolveParams& P, int newp, int li, double* __
         const int cellqq = __shfl_sync(0xffffffffu, cellq, owner);
         if (half == 0 && has0) build_row<T>(P, pold, t, pt, cellqq, (uint8_t)codeq, vq, r - first, A0, b0);
         if (half == 1 && has1) build_row<T>(P, pold, t, pt, cellqq, (uint8_t)codeq, vq, r - first, A1, b1);
+        if constexpr (PREP) {
+            if ((half == 0 && has0) || (half == 1 && has1)) {
+                // row source: the cell value, or the ghost face it stands for
+                int kind = 0;
+                const unsigned mask = (unsigned)codeq & CLS_MASK;
+                if (!(codeq & CLS_BULK) && mask != 0) {
+                    int dd, ss;
+                    kth_face(mask, r - first, dd, ss);
+                    kind = 1 + 2 * dd + (ss > 0 ? 1 : 0);
+                }
+                LisRow& row = P.lis_rows[(size_t)li * 64 + r];
+                row.cell = cellqq;
+                row.kind = kind;
+                row.w = half == 0 ? A0[0] : A1[0];  // the row weight (first column)
+            }
+        }
     }
 
     // ---- Householder QR, warp-parallel ----
@@ -172,6 +210,39 @@ __device__ void listener_body(const SolveParams& P, int newp, int li, double* __
 #pragma unroll
         for (int cc = j + 1; cc < 4; ++cc) R[j][cc] = __shfl_sync(0xffffffffu, A0[cc], j);
     }
+    if constexpr (PREP) {
+        const double rmax = dmax(dmax(fabs(R[0][0]), fabs(R[1][1])), dmax(fabs(R[2][2]), fabs(R[3][3])));
+        for (int j = 0; j < 4; ++j)
+            if (fabs(R[j][j]) <= (double)(total > 4 ? total : 4) * 2.220446049250313e-16 * rmax) ok = false;
+        if (!ok) {
+            if (lane == 0) P.lis_plan[li].mode = 2;
+            return;
+        }
+        // u = R^-T e0, then y = H0 H1 H2 H3 [u; 0] (reflectors in reverse order)
+        double u[4];
+        u[0] = 1.0 / R[0][0];
+        u[1] = -(R[0][1] * u[0]) / R[1][1];
+        u[2] = -(R[0][2] * u[0] + R[1][2] * u[1]) / R[2][2];
+        u[3] = -(R[0][3] * u[0] + R[1][3] * u[1] + R[2][3] * u[2]) / R[3][3];
+        double y0 = lane < 4 ? u[lane] : 0.0, y1 = 0.0;
+#pragma unroll
+        for (int j = 3; j >= 0; --j) {
+            const bool a0 = has0 && lane >= j;
+            const bool a1 = has1;
+            const double vv = warp_sum((a0 ? A0[j] * A0[j] : 0.0) + (a1 ? A1[j] * A1[j] : 0.0));
+            const double dot = warp_sum((a0 ? A0[j] * y0 : 0.0) + (a1 ? A1[j] * y1 : 0.0));
+            const double f = 2.0 * dot / vv;
+            if (a0) y0 -= f * A0[j];
+            if (a1) y1 -= f * A1[j];
+        }
+        if (has0) P.lis_rows[(size_t)li * 64 + lane].w *= y0;
+        if (has1) P.lis_rows[(size_t)li * 64 + lane + 32].w *= y1;
+        if (lane == 0) {
+            P.lis_plan[li].mode = 0;
+            P.lis_plan[li].n = total;
+        }
+        return;
+    }
     double bt[4];
 #pragma unroll
     for (int j = 0; j < 4; ++j) bt[j] = __shfl_sync(0xffffffffu, b0, j);
@@ -189,12 +260,70 @@ __device__ void listener_body(const SolveParams& P, int newp, int li, double* __
     if (!ok) atomicOr(P.dev_error, 1);
 }
 
+// Listener li from its plan: sum_r w_r value_r as a warp reduction.  A NaN
+// among the enclosing cells (which the full fit drops) falls back to it.
+template <typename T>
+__device__ __forceinline__ void listener_plan(const SolveParams& P, int newp, int li, double* __restrict__ out_row) {
+    const int lane = threadIdx.x & 31;
+    const LisPlan& pl = P.lis_plan[li];
+    const T* __restrict__ pnew = (const T*)P.p[newp];
+    const int nc = pl.nc;
+    const double vc = lane < nc ? (double)pnew[pl.cells[lane < 8 ? lane : 0]] : 0.0;
+    if (__ballot_sync(0xffffffffu, lane < nc && isnan(vc))) {
+        listener_body<T>(P, newp, li, out_row);
+        return;
+    }
+    if (pl.mode == 1) {
+        if (lane == 0) out_row[li] = (double)pnew[pl.cell];
+        return;
+    }
+    if (pl.mode == 2) {
+        if (lane == 0) {
+            out_row[li] = 0.0;
+            atomicOr(P.dev_error, 1);
+        }
+        return;
+    }
+    const T* __restrict__ pold = (const T*)P.p[newp ^ 1];
+    const double t = P.consts[newp ^ 1].t;
+    double acc = 0.0;
+#pragma unroll
+    for (int half = 0; half < 2; ++half) {
+        const int r = lane + 32 * half;
+        if (r >= pl.n) continue;
+        const LisRow row = P.lis_rows[(size_t)li * 64 + r];
+        double val;
+        if (row.kind == 0) {
+            val = (double)pnew[row.cell];
+        } else {
+            const int d = (row.kind - 1) >> 1, sgn = ((row.kind - 1) & 1) ? 1 : -1;
+            int i, j, k;
+            cell_ijk(P, row.cell, i, j, k);
+            const double cp[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
+            const long long strides[3] = {P.SX, P.SY, 1};
+            val = ghost_pressure(P, P.gobj[row.cell], cp, d, sgn, (double)pold[row.cell + sgn * strides[d]], t);
+        }
+        acc += row.w * val;
+    }
+    acc = warp_sum(acc);
+    if (lane == 0) out_row[li] = acc;
+}
+
+// Plans of every listener from the current classification (one warp each)
+template <typename T>
+__global__ void __launch_bounds__(128) k_listener_prep(const SolveParams* __restrict__ Pp, int newp) {
+    const int li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (li >= Pp->n_lis) return;
+    listener_body<T, true>(*Pp, newp, li, nullptr);
+}
+
 template <typename T>
 __global__ void __launch_bounds__(128) k_listeners_warp(const SolveParams* __restrict__ Pp, int newp,
                                                         double* __restrict__ out_row) {
     const int li = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (li >= Pp->n_lis) return;  // the whole warp leaves together
-    listener_body<T>(*Pp, newp, li, out_row);
+    if (Pp->lis_ready) listener_plan<T>(*Pp, newp, li, out_row);
+    else listener_body<T>(*Pp, newp, li, out_row);
 }
 
 }  // namespace fdtd

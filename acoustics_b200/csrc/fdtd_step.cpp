@@ -76,6 +76,11 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         if (s->moving) {
             CUDA_TRY(s, launch_fresh_cells(s->dP, s->precision, cur, s->ncell, s->d_status, s->stream));
             s->launches++;
+        } else if (s->L > 0) {
+            // static classification: the listener fits become fixed weights
+            CUDA_TRY(s, launch_listener_prep(s->dP, s->precision, cur ^ 1, s->L, s->stream));
+            s->launches += 2;
+            s->hP.lis_ready = 1;  // host mirror of the flag the prep sets (later uploads keep it)
         }
     }
     // the region-split path advances the step constants inside its shell kernel;
