@@ -48,17 +48,22 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False, lineinfo: bool = True) -> str:
-    if not force and not _stale():
+def build(force: bool = False, verbose: bool = False, lineinfo: bool = True, defines=(), lib: str = LIB) -> str:
+    """Compile and link the library.  `defines` (e.g. ["FDTD_SHELL_PLANES=4"])
+    and `lib` build another variant of the same ABI elsewhere; load it with
+    FDTD_B200_LIB=<path>."""
+    if not force and lib == LIB and not defines and not _stale():
         return LIB
-    os.makedirs(OUT_DIR, exist_ok=True)
-    obj_dir = os.path.join(OUT_DIR, "obj")
+    out_dir = os.path.dirname(os.path.abspath(lib))
+    os.makedirs(out_dir, exist_ok=True)
+    obj_dir = os.path.join(out_dir, "obj" if lib == LIB else "obj_" + os.path.basename(lib).replace(".so", ""))
     os.makedirs(obj_dir, exist_ok=True)
     nvcc = _nvcc()
     cxx = _host_cxx()
     common = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-ccbin", cxx]
     if lineinfo:
         common.append("-lineinfo")
+    common += ["-D" + d for d in defines]
     objs = []
     jobs = []
     for f in CU_FP64 + CU_FAST + CPP:
@@ -86,14 +91,14 @@ def build(force: bool = False, verbose: bool = False, lineinfo: bool = True) -> 
             failed = True
     if failed:
         raise RuntimeError("building libfdtd_b200.so failed")
-    tmp = LIB + ".tmp"
+    tmp = lib + ".tmp"
     link = [nvcc] + ARCH + ["-shared", "-cudart", "static", "-o", tmp] + objs + ["-lpthread"]
     r = subprocess.run(link, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)
     if r.returncode != 0:
         sys.stderr.write(" ".join(link) + "\n" + r.stdout.decode(errors="replace"))
         raise RuntimeError("linking libfdtd_b200.so failed")
-    os.replace(tmp, LIB)
-    return LIB
+    os.replace(tmp, lib)
+    return lib
 
 
 if __name__ == "__main__":

@@ -216,6 +216,27 @@ fdtd_status run_classification(fdtd_solver* s) {
 // ---------------------------------------------------------------------------
 namespace fdtd {
 
+// Whether a solve keeps the reduced PML state (k_pml_shell_red): FP32 fused
+// solves of static scenes with no solid PML cell, the five-box shell, and, along
+// every axis, unit decay factors on both faces of every cell outside that axis'
+// PML (the condition under which the plain axes of a PML cell telescope into one
+// leapfrog increment exactly).
+bool use_reduced_pml(const fdtd_solver* s, bool no_solid_pml) {
+    if (s->precision != FDTD_PRECISION_FP32_COMPENSATED || s->opt.kernel != FDTD_KERNEL_FUSED) return false;
+    if (s->opt.pml_state != FDTD_PML_STATE_AUTO || s->moving || !no_solid_pml) return false;
+    if (s->shell.n != 5 || s->shell.zbox != 4) return false;
+    for (int d = 0; d < 3; ++d) {
+        const auto& T = s->tab[d];
+        for (int i = 0; i < s->N[d]; ++i) {
+            if (T.pml_cell[i]) continue;
+            if (i == 0 || i + 1 >= s->N[d]) return false;
+            if (T.pupd[i] != 1.0 || T.vupd[i] != 1.0 || T.vupd[i + 1] != 1.0) return false;
+            if (T.vgrad[i] != T.vgrad[i + 1] || T.pdiv[i] != -1.0 * s->rho * s->c * s->c / (1.0 / s->k)) return false;
+        }
+    }
+    return true;
+}
+
 // PML shell boxes for a given number of x planes per thread (xs).
 void build_shell_boxes(fdtd_solver* s, int xs) {
     ShellBoxes& B = s->shell;
@@ -800,6 +821,7 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
         P.n_solid_pml = (int)solid_pml.size();
         s->n_solid_pml = P.n_solid_pml;
     }
+    s->region.red = use_reduced_pml(s, solid_pml.empty()) ? 1 : 0;
     st = upload_params(s);
     if (st != FDTD_OK) return st;
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));

@@ -133,9 +133,9 @@ fdtd_status rebuild(fdtd_batch* b) {
     const size_t nm = b->members.size();
     const size_t tbytes = std::max<size_t>(nm, 1) * dsz;
     std::vector<char> descs(2 * tbytes, 0);
-    std::vector<BatchTile> it, st;
+    std::vector<BatchTile> it, st, st_full;
     std::vector<ListenerRef> refs;
-    int max_ghost = 0, max_src = 0;
+    int max_ghost = 0, max_src = 0, max_solid = 0;
     for (size_t m = 0; m < nm; ++m) {
         Member& mb = b->members[m];
         if (!mb.s) continue;
@@ -161,19 +161,24 @@ fdtd_status rebuild(fdtd_batch* b) {
                     for (int z = 0; z < tz; ++z) it.push_back({(int)m, 0, z, y, x});
         }
         const ShellBoxes& B = mb.s->shell;
-        // the member's first shell tile (ty = 1) advances its step constants
-        const size_t first_tile = st.size();
+        // the member's first shell tile (ty = 1) advances its step constants;
+        // members with the reduced PML state come first in the table
+        std::vector<BatchTile>& tab = mb.s->region.red ? st : st_full;
+        const size_t first_tile = tab.size();
         for (int bx = 0; bx < B.n; ++bx)
             for (int x = 0; x < B.tx[bx]; ++x)
-                for (int u = 0; u < B.tu[bx]; ++u) st.push_back({(int)m, bx, u, st.size() == first_tile ? 1 : 0, x});
+                for (int u = 0; u < B.tu[bx]; ++u) tab.push_back({(int)m, bx, u, tab.size() == first_tile ? 1 : 0, x});
         for (int li = 0; li < mb.s->L; ++li) refs.push_back({(int)m, li});
         max_ghost = std::max(max_ghost, (mb.s->region.ghost_cap + 127) / 128);
+        max_solid = std::max(max_solid, (mb.s->n_solid_pml + 255) / 256);
         if (mb.s->hP.n_src > 0) {
             const Box3& r = mb.s->region.src_region;
             const long long cells = (long long)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);
             max_src = std::max<int>(max_src, (int)std::min<long long>((cells + 255) / 256, 64));
         }
     }
+    const int n_shell_red = (int)st.size();
+    st.insert(st.end(), st_full.begin(), st_full.end());
     fdtd_status st_ = FDTD_OK;
     char* dd = static_cast<char*>(b->d_descs);
     if (b->desc_cap < descs.size()) {
@@ -201,6 +206,7 @@ fdtd_status rebuild(fdtd_batch* b) {
     L.n_int = (int)it.size();
     L.shell_tiles = b->d_shell;
     L.n_shell = (int)st.size();
+    L.n_shell_red = b->precision == FDTD_PRECISION_FP64 ? 0 : n_shell_red;
     L.refs = b->d_refs;
     L.n_refs = (int)refs.size();
     L.n_members = (int)nm;
@@ -208,6 +214,7 @@ fdtd_status rebuild(fdtd_batch* b) {
     L.xs = xs;
     L.ghost_blocks = std::min(max_ghost, 32);
     L.src_blocks = max_src;
+    L.solid_blocks = std::min(max_solid, 64);
     for (int i = 0; i < 2; ++i)
         if (b->graph[i]) {
             cudaGraphExecDestroy(b->graph[i]);

@@ -7,8 +7,9 @@
 // of a step flips.  Because the step constants live on the device, a captured
 // graph of an even number of batched steps replays for any step index.
 //
-// Per step:  k_batch_shell (PML tiles of all members; its first tile of a
-//            member writes the member's next-step constants)  ||
+// Per step:  k_batch_shell_red / k_batch_shell (PML tiles of the members with
+//            the reduced / full PML state; the first tile of a member writes
+//            the member's next-step constants)  ||
 //            k_batch_interior -> k_batch_ghost -> k_batch_sources (second
 //            stream), then k_batch_listeners (launch_batch_tail).
 // The descriptors come in two tables, one per step parity (every member's
@@ -45,6 +46,35 @@ __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_batch_shel
     const BatchDesc<T>& d = D[tile.m];
     if (tile.ty && threadIdx.x == 0 && threadIdx.y == 0) advance_consts(*d.P, d.cur);
     shell_tile<T>(d.a[d.cur], d.shell, tile.box, tile.tz, tile.tx);
+}
+
+// Shell tiles of members that keep the reduced PML state (FP32 only).
+template <typename T>
+__global__ void __launch_bounds__(256, FDTD_SHELL_RED_MINB) k_batch_shell_red(const BatchDesc<T>* __restrict__ D,
+                                                                      const BatchTile* __restrict__ tiles) {
+    static_assert(sizeof(T) == 4, "the reduced PML state is an FP32 path");
+    const BatchTile tile = tiles[blockIdx.x];
+    const BatchDesc<T>& d = D[tile.m];
+    if (tile.ty && threadIdx.x == 0 && threadIdx.y == 0) advance_consts(*d.P, d.cur);
+    shell_tile_red(d.a[d.cur], d.shell, tile.box, tile.tz, tile.tx);
+}
+
+// grid (solid_blocks, members): re-zero the solid cells inside the PML of the
+// members that have some (the PML update writes every PML cell; classification
+// zeroes solid cells in every buffer at the start of a step, MAC_Grid.cpp:3566-3600)
+template <typename T>
+__global__ void __launch_bounds__(256) k_batch_solid_pml(const BatchDesc<T>* __restrict__ D) {
+    const BatchDesc<T>& d = D[blockIdx.y];
+    if (!d.active) return;
+    const SolveParams& P = *d.P;
+    T* p0 = (T*)P.p[0];
+    T* p1 = (T*)P.p[1];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < P.n_solid_pml; i += gridDim.x * blockDim.x) {
+        const int c = P.solid_pml[i];
+        p0[c] = (T)0;
+        p1[c] = (T)0;
+        if (P.dinc) P.dinc[c] = 0.0f;
+    }
 }
 
 // grid (ghost_blocks, members)
@@ -89,6 +119,10 @@ cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, 
                          cudaEvent_t join, int* launches) {
     BatchDesc<T>* D = static_cast<BatchDesc<T>*>(L.descs);
     int l = 0;
+    if (L.solid_blocks > 0) {
+        k_batch_solid_pml<T><<<dim3(L.solid_blocks, L.n_members), 256, 0, s>>>(D);
+        ++l;
+    }
     cudaError_t e = cudaEventRecord(fork, s);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, fork, 0);
     if (e != cudaSuccess) return e;
@@ -109,8 +143,16 @@ cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, 
         k_batch_sources<T><<<dim3(L.src_blocks, L.n_members), 256, 0, s2>>>(D);
         ++l;
     }
-    if (L.n_shell > 0) {
-        k_batch_shell<T><<<L.n_shell, dim3(32, 8), 0, s>>>(D, L.shell_tiles);
+    int n_red = 0;
+    if constexpr (sizeof(T) == 4) {
+        n_red = L.n_shell_red;
+        if (n_red > 0) {
+            k_batch_shell_red<float><<<n_red, dim3(32, 8), 0, s>>>(D, L.shell_tiles);
+            ++l;
+        }
+    }
+    if (L.n_shell > n_red) {
+        k_batch_shell<T><<<L.n_shell - n_red, dim3(32, 8), 0, s>>>(D, L.shell_tiles + n_red);
         ++l;
     }
     e = cudaEventRecord(join, s2);

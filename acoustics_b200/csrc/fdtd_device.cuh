@@ -179,6 +179,7 @@ struct RegionLaunch {
     int ghost_cap;     // capacity of the ghost-neighbour list (0: no list kernel)
     int xb;            // x planes per interior thread
     int skip;          // kernels left out (timing of single kernels): 1 interior, 2 shell, 4 ghost list
+    int red;           // FP32: the shell keeps the reduced PML state (k_pml_shell_red)
 };
 
 // Two copies indexed by the step parity: the kernels of a step read
@@ -341,12 +342,14 @@ struct BatchLaunch {
     int n_int;
     const BatchTile* shell_tiles;
     int n_shell;
+    int n_shell_red;             // FP32: the first n_shell_red shell tiles belong to members with the reduced PML state
     const ListenerRef* refs;
     int n_refs;
     int n_members;
     int xb, xs;
     int ghost_blocks;            // per member
     int src_blocks;              // per member (0: no member has a source)
+    int solid_blocks;            // per member (0: no member has a solid cell inside its PML)
 };
 
 // z-vector groups of the interior box: groups start at multiples of V = 16 /

@@ -28,9 +28,22 @@
 #include "fdtd_region.cuh"
 #include "fdtd_stencil.cuh"
 
-// resident CTAs of 256 threads the shell kernels are compiled for: 3 (85
-// registers per thread) in FP32, 2 (128) in FP64
-__host__ __device__ constexpr int shell_min_blocks(int word) { return word == 4 ? 2 : 1; }
+// resident CTAs of 256 threads the shell kernels are compiled for: 2 (128
+// registers per thread) in FP32, 1 (255) in FP64 by default
+#ifndef FDTD_SHELL_MINB_F32
+#define FDTD_SHELL_MINB_F32 2
+#endif
+#ifndef FDTD_SHELL_MINB_F64
+#define FDTD_SHELL_MINB_F64 1
+#endif
+// 1: a shell thread issues the loads of its next x plane before computing the
+// current one (two planes of registers); 0: one plane at a time, more warps
+#ifndef FDTD_SHELL_PREFETCH
+#define FDTD_SHELL_PREFETCH 1
+#endif
+__host__ __device__ constexpr int shell_min_blocks(int word) {
+    return word == 4 ? FDTD_SHELL_MINB_F32 : FDTD_SHELL_MINB_F64;
+}
 
 namespace fdtd {
 
@@ -184,18 +197,29 @@ __device__ __forceinline__ unsigned flag_mask(const uint8_t (&f)[V], int k) {
 }
 
 // Where a shell column keeps its split pressures and face velocities: the grid
-// arrays, or the compact arrays of the z-slab box (ShellBoxes).
-template <typename T>
+// arrays (CMP = false: offsets equal the cell offsets, strides the grid's), or
+// the compact arrays of the z-slab box (CMP = true, ShellBoxes).  The choice is
+// a template parameter, so the array pointers stay kernel parameters instead of
+// registers.
+template <typename T, bool CMP>
+__device__ __forceinline__ T* sh_pd(const KArgs<T>& A, int d) {
+    return CMP ? A.zpd[d] : A.pd[d];
+}
+template <typename T, bool CMP>
+__device__ __forceinline__ const T* sh_vo(const KArgs<T>& A, int d) {
+    return CMP ? A.zvo[d] : A.vo[d];
+}
+template <typename T, bool CMP>
+__device__ __forceinline__ T* sh_vn(const KArgs<T>& A, int d) {
+    return CMP ? A.zvn[d] : A.vn[d];
+}
+
+// Strides and edge flags of the compact storage (CMP only).
 struct ShellStore {
-    T* pd[3];
-    const T* vo[3];
-    T* vn[3];
     int sx, sy;         // plane and row strides of that storage
-    bool compact;
-    bool x_hi_grid;     // compact: the last plane reads its high x face from the grid
-    bool y_hi_grid;     // compact: this row reads its high y face from the grid
-    bool y_lo_grid;     // compact: this row also writes its low y faces to the grid
-    int spare;          // compact: offset (from the group) of the spare high-z-face slot, 0: next slot
+    bool y_hi_grid;     // this row reads its high y face from the grid
+    bool y_lo_grid;     // this row also writes its low y faces to the grid
+    int spare;          // offset (from the group) of the spare high-z-face slot, 0: next slot
 };
 
 // Loads of one x plane of a shell column (everything but p(x-1), p(x) and the
@@ -208,8 +232,8 @@ struct ShellPlane {
     uint8_t g;
 };
 
-template <typename T, int V>
-__device__ __forceinline__ void shell_load(const KArgs<T>& A, const ShellStore<T>& S, ShellPlane<T, V>& L, int x,
+template <typename T, int V, bool CMP>
+__device__ __forceinline__ void shell_load(const KArgs<T>& A, const ShellStore& S, ShellPlane<T, V>& L, int x,
                                            bool last_plane, unsigned c, unsigned q, int oym, int oyp, int ozm) {
     const int sx = (int)A.sx, sy = (int)A.sy;
     const T* pc = A.pc + c;
@@ -220,26 +244,35 @@ __device__ __forceinline__ void shell_load(const KArgs<T>& A, const ShellStore<T
     L.yp = ldv<T, V>(pc + oyp);
     L.zme = pc[-ozm];
     L.zpe = pc[V];
-    L.vxr = (S.x_hi_grid && last_plane) ? ldv<T, V>(A.vo[0] + c + sx) : ldv<T, V>(S.vo[0] + q + S.sx);
-    L.vyl = ldv<T, V>(S.vo[1] + q);
-    L.vyr = S.y_hi_grid ? ldv<T, V>(A.vo[1] + c + sy) : ldv<T, V>(S.vo[1] + q + S.sy);
-    L.vzl = ldv<T, V>(S.vo[2] + q);
-    L.vze = S.vo[2][q + (S.spare ? S.spare : V)];
-    L.a0 = ldv<T, V>(S.pd[0] + q);
-    L.a1 = ldv<T, V>(S.pd[1] + q);
-    L.a2 = ldv<T, V>(S.pd[2] + q);
+    if constexpr (CMP) {
+        L.vxr = last_plane ? ldv<T, V>(A.vo[0] + c + sx) : ldv<T, V>(A.zvo[0] + q + S.sx);
+        L.vyl = ldv<T, V>(A.zvo[1] + q);
+        L.vyr = S.y_hi_grid ? ldv<T, V>(A.vo[1] + c + sy) : ldv<T, V>(A.zvo[1] + q + S.sy);
+        L.vzl = ldv<T, V>(A.zvo[2] + q);
+        L.vze = A.zvo[2][q + (S.spare ? S.spare : V)];
+    } else {
+        L.vxr = ldv<T, V>(A.vo[0] + c + sx);
+        L.vyl = ldv<T, V>(A.vo[1] + c);
+        L.vyr = ldv<T, V>(A.vo[1] + c + sy);
+        L.vzl = ldv<T, V>(A.vo[2] + c);
+        L.vze = A.vo[2][c + V];
+    }
+    L.a0 = ldv<T, V>(sh_pd<T, CMP>(A, 0) + q);
+    L.a1 = ldv<T, V>(sh_pd<T, CMP>(A, 1) + q);
+    L.a2 = ldv<T, V>(sh_pd<T, CMP>(A, 2) + q);
 }
 
 // One PML-shell tile: unit tile tu (256 consecutive (row, z-group) units of box
 // b, one per thread) by x tile tx.  A thread owns one z group (a vector of
 // shell_vz cells starting at a multiple of its width; cells outside the
 // group's z range are masked) of one row and marches along x over B.xs planes:
-// p(x-1), p(x) and the low x face velocity are carried in registers, and the
-// loads of plane x+1 are issued before plane x is computed and stored.  Face
-// flags (MAC_Grid.cpp:2568-2575, :2631-2633) are V-bit masks from the packed
-// per-axis tables; the arithmetic per cell is the reference's, in its order.
-template <typename T>
-__device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& B, int b, int tu, int tx) {
+// p(x-1), p(x) and the low x face velocity are carried in registers, and (with
+// FDTD_SHELL_PREFETCH) the loads of plane x+1 are issued before plane x is
+// computed and stored.  Face flags (MAC_Grid.cpp:2568-2575, :2631-2633) are
+// V-bit masks from the packed per-axis tables; the arithmetic per cell is the
+// reference's, in its order.  CMP: box b is the z-slab pair with compact storage.
+template <typename T, bool CMP>
+__device__ __forceinline__ void shell_tile_impl(const KArgs<T>& A, const ShellBoxes& B, int b, int tu, int tx) {
     constexpr int V = shell_vz(sizeof(T));
     constexpr unsigned ALL = (1u << V) - 1u;
     using VT = Vec<T, V>;
@@ -263,36 +296,22 @@ __device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& 
     const int sx = (int)A.sx, sy = (int)A.sy;
     const unsigned c0 = (unsigned)x0 * A.sx + (unsigned)y * A.sy + zg;  // cell and its three low faces
 
-    ShellStore<T> S;
-    S.compact = (b == B.zbox);
+    ShellStore S;
     unsigned q0;
-    if (S.compact) {
+    if constexpr (CMP) {
         S.sy = B.zrw;
         S.sx = B.ny[b] * B.zrw;
         q0 = (unsigned)(x0 - B.x0[b]) * S.sx + (unsigned)yl * S.sy + gi * V;
         const bool last_group = first ? (gi == B.gl[b] - 1) : (gi == ng - 1);
         S.spare = last_group ? (ng - gi) * V + (first ? 0 : 1) : 0;
-        S.x_hi_grid = true;
         S.y_hi_grid = (y + 1 == B.y0[b] + B.ny[b]);
         S.y_lo_grid = (yl == 0);
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            S.pd[d] = A.zpd[d];
-            S.vo[d] = A.zvo[d];
-            S.vn[d] = A.zvn[d];
-        }
     } else {
         S.sx = sx;
         S.sy = sy;
         q0 = c0;
         S.spare = 0;
-        S.x_hi_grid = S.y_hi_grid = S.y_lo_grid = false;
-#pragma unroll
-        for (int d = 0; d < 3; ++d) {
-            S.pd[d] = A.pd[d];
-            S.vo[d] = A.vo[d];
-            S.vn[d] = A.vn[d];
-        }
+        S.y_hi_grid = S.y_lo_grid = false;
     }
 
     const uint8_t gy = __ldg(A.axflag[1] + y);
@@ -312,15 +331,19 @@ __device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& 
     // carried along x
     VT pm = ldv<T, V>(A.pc + c0 - (x0 > 0 ? sx : 0));
     VT p0 = ldv<T, V>(A.pc + c0);
-    VT vxl = ldv<T, V>(S.vo[0] + q0);
+    VT vxl = ldv<T, V>(sh_vo<T, CMP>(A, 0) + q0);
     AxisCoef<T> cxl = A.coef[0][x0];
     ShellPlane<T, V> cur, nxt;
-    shell_load<T, V>(A, S, cur, x0, x0 + 1 == xend, c0, q0, oym, oyp, ozm);
+    if constexpr (FDTD_SHELL_PREFETCH) shell_load<T, V, CMP>(A, S, cur, x0, x0 + 1 == xend, c0, q0, oym, oyp, ozm);
 #pragma unroll 1
     for (int x = x0; x < x1; ++x) {
         const unsigned c = c0 + (unsigned)(x - x0) * A.sx;
-        const unsigned q = q0 + (unsigned)(x - x0) * S.sx;
-        if (x + 1 < x1) shell_load<T, V>(A, S, nxt, x + 1, x + 2 == xend, c + sx, q + S.sx, oym, oyp, ozm);
+        const unsigned q = CMP ? q0 + (unsigned)(x - x0) * S.sx : c;
+        if constexpr (FDTD_SHELL_PREFETCH) {
+            if (x + 1 < x1) shell_load<T, V, CMP>(A, S, nxt, x + 1, x + 2 == xend, c + sx, q + S.sx, oym, oyp, ozm);
+        } else {
+            shell_load<T, V, CMP>(A, S, cur, x, x + 1 == xend, c, q, oym, oyp, ozm);
+        }
         const uint8_t g = cur.g;
         const unsigned mpx = (g & AXF_PML) ? ALL : 0u;
         const unsigned oyz = mpy | zpml, oxz = mpx | zpml, oxy = mpx | mpy;
@@ -365,35 +388,42 @@ __device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& 
             az.e[e] = pd_update<T>(cur.a2.e[e], cz[e].pupd, cz[e].pdiv, vz_r, vz_l, A.inv_h);
             pn.e[e] = ax.e[e] + ay.e[e] + az.e[e];
         }
-        st_masked<T, V>(S.vn[0] + q, nxl, m_xl);
-        st_masked<T, V>(S.vn[1] + q, nyl, m_yl);
-        st_masked<T, V>(S.vn[2] + q, nzl, m_zl);
-        if (S.compact) {
+        st_masked<T, V>(sh_vn<T, CMP>(A, 0) + q, nxl, m_xl);
+        st_masked<T, V>(sh_vn<T, CMP>(A, 1) + q, nyl, m_yl);
+        st_masked<T, V>(sh_vn<T, CMP>(A, 2) + q, nzl, m_zl);
+        if constexpr (CMP) {
             // low x / y faces shared with the x / y slabs, high faces owned by them
             if (x == B.x0[b]) st_masked<T, V>(A.vn[0] + c, nxl, m_xl);
             if (S.y_lo_grid) st_masked<T, V>(A.vn[1] + c, nyl, m_yl);
-            st_masked<T, V>((x + 1 == xend ? A.vn[0] + c : S.vn[0] + q) + (x + 1 == xend ? sx : S.sx), nxr, m_xr);
-            st_masked<T, V>(S.y_hi_grid ? A.vn[1] + c + sy : S.vn[1] + q + S.sy, nyr, m_yr);
+            st_masked<T, V>(x + 1 == xend ? A.vn[0] + c + sx : A.zvn[0] + q + S.sx, nxr, m_xr);
+            st_masked<T, V>(S.y_hi_grid ? A.vn[1] + c + sy : A.zvn[1] + q + S.sy, nyr, m_yr);
         } else {
-            st_masked<T, V>(S.vn[0] + q + S.sx, nxr, m_xr);
-            st_masked<T, V>(S.vn[1] + q + S.sy, nyr, m_yr);
+            st_masked<T, V>(A.vn[0] + c + sx, nxr, m_xr);
+            st_masked<T, V>(A.vn[1] + c + sy, nyr, m_yr);
         }
         if (m_zr) {
+            T* vz = sh_vn<T, CMP>(A, 2);
 #pragma unroll
             for (int e = 0; e < V; ++e)
-                if ((m_zr >> e) & 1u) S.vn[2][q + ((e == V - 1 && S.spare) ? S.spare : e + 1)] = nzr[e];
+                if ((m_zr >> e) & 1u) vz[q + ((e == V - 1 && S.spare) ? S.spare : e + 1)] = nzr[e];
         }
-        st_masked<T, V>(S.pd[0] + q, ax, inbox);
-        st_masked<T, V>(S.pd[1] + q, ay, inbox);
-        st_masked<T, V>(S.pd[2] + q, az, inbox);
+        st_masked<T, V>(sh_pd<T, CMP>(A, 0) + q, ax, inbox);
+        st_masked<T, V>(sh_pd<T, CMP>(A, 1) + q, ay, inbox);
+        st_masked<T, V>(sh_pd<T, CMP>(A, 2) + q, az, inbox);
         st_masked<T, V>(A.pn + c, pn, inbox);
         // carry to plane x+1
         pm = p0;
         p0 = cur.pp;
         vxl = cur.vxr;
         cxl = cxr;
-        cur = nxt;
+        if constexpr (FDTD_SHELL_PREFETCH) cur = nxt;
     }
+}
+
+template <typename T>
+__device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& B, int b, int tu, int tx) {
+    if (b == B.zbox) shell_tile_impl<T, true>(A, B, b, tu, tx);
+    else shell_tile_impl<T, false>(A, B, b, tu, tx);
 }
 
 // CTA -> (box, unit tile, plane tile) through the prefix table of the shell boxes
@@ -414,6 +444,12 @@ __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_pml_shell(
     shell_decode(B, blockIdx.x, b, tu, tx);
     shell_tile<T>(A, B, b, tu, tx);
 }
+
+}  // namespace fdtd
+
+#include "fdtd_shell_red.cuh"
+
+namespace fdtd {
 
 // Host side: one region-split step.  The shell kernel runs on s, the interior
 // kernel on s2 (forked and joined with the two events), then the ghost-cell
@@ -445,7 +481,12 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     }
     const int nblk = (R.skip & 2) ? 0 : R.shell.block_first[R.shell.n];
     if (nblk > 0) {
-        k_pml_shell<T><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
+        if constexpr (sizeof(T) == 4) {
+            if (R.red) k_pml_shell_red<float><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
+            else k_pml_shell<T><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
+        } else {
+            k_pml_shell<T><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
+        }
         ++l;
     }
     if (R.ghost_cap > 0 && !(R.skip & 4)) {

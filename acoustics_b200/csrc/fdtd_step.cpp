@@ -342,6 +342,10 @@ const char* fdtd_solver_last_error(fdtd_solver* s) { return s ? s->err.c_str() :
 
 int64_t fdtd_solver_last_launch_count(fdtd_solver* s) { return s ? s->last_launches : 0; }
 
+int32_t fdtd_solver_pml_state(fdtd_solver* s) {
+    return (s && s->region.red) ? FDTD_PML_STATE_AUTO : FDTD_PML_STATE_FULL;
+}
+
 fdtd_status fdtd_solver_info_get(fdtd_solver* s, fdtd_solver_info* info) {
     if (!s || !info) return FDTD_ERR_INVALID_ARG;
     std::memset(info, 0, sizeof(*info));
@@ -439,6 +443,11 @@ fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, in
         default: return (set_error(s, "unknown field"), FDTD_ERR_INVALID_ARG);
     }
     if (count != n) return (set_error(s, "count does not match the field size"), FDTD_ERR_INVALID_ARG);
+    if (s->region.red && which >= FDTD_FIELD_PML_PX)
+        return (set_error(s, "this FP32 solve keeps the reduced PML state (no split pressures or face velocities "
+                             "along axes without absorption); create it with pml_state = FDTD_PML_STATE_FULL to "
+                             "read them"),
+                FDTD_ERR_UNSUPPORTED);
     // extent of the requested grid (cells, or faces of one orientation)
     int ext[3] = {s->N[0], s->N[1], s->N[2]};
     if (which >= FDTD_FIELD_VX) ext[which - FDTD_FIELD_VX] += 1;

@@ -23,6 +23,7 @@ ACCEL_NONE, ACCEL_GAUSSIAN_TRANSLATION, ACCEL_GAUSSIAN_PULSATION = 0, 1, 2
 MOTION_STATIC, MOTION_BALLISTIC = 0, 1
 PRECISION_FP64, PRECISION_FP32_COMPENSATED = 0, 1
 KERNEL_FUSED, KERNEL_PHASED = 0, 1
+PML_STATE_AUTO, PML_STATE_FULL = 0, 1
 
 CELL_BULK, CELL_GHOST, CELL_VALID_HISTORY, CELL_PML, CELL_CONSTRAINT = 1, 2, 4, 8, 16
 (FIELD_PRESSURE, FIELD_PRESSURE_PREV, FIELD_PML_PX, FIELD_PML_PY, FIELD_PML_PZ,
@@ -73,7 +74,7 @@ class Options(C.Structure):
     _fields_ = [
         ("precision", C.c_int32), ("device", C.c_int32), ("kernel", C.c_int32),
         ("graph_steps", C.c_int32), ("tile_y", C.c_int32), ("x_chunk", C.c_int32),
-        ("_reserved0", C.c_int32), ("_reserved1", C.c_int32),
+        ("pml_state", C.c_int32), ("_reserved1", C.c_int32),
     ]
 
 

@@ -15,20 +15,21 @@ from typing import Optional
 import numpy as np
 
 from ._lib import FDTDError, check, load
-from .scene import (FIELD_PRESSURE, GHOST_FACE_DTYPE, KERNEL_FUSED, PRECISION_FP64, Options, Scene,
-                    SceneDesc, SolverInfo)
+from .scene import (FIELD_PRESSURE, GHOST_FACE_DTYPE, KERNEL_FUSED, PML_STATE_AUTO, PRECISION_FP64, Options,
+                    Scene, SceneDesc, SolverInfo)
 
 
 class PML_WaveSolver:
     """One resident solve on one GPU (PML_WaveSolver.h:122-255)."""
 
     def __init__(self, scene: Scene, precision: int = PRECISION_FP64, kernel: int = KERNEL_FUSED,
-                 graph_steps: int = 0, device: int = 0, tile_y: int = 0, x_chunk: int = 0):
+                 graph_steps: int = 0, device: int = 0, tile_y: int = 0, x_chunk: int = 0,
+                 pml_state: int = PML_STATE_AUTO):
         self._L = load()
         self.scene = scene
         desc, self._keep = scene.to_c()
         opt = Options(precision=precision, device=device, kernel=kernel, graph_steps=graph_steps,
-                      tile_y=tile_y, x_chunk=x_chunk)
+                      tile_y=tile_y, x_chunk=x_chunk, pml_state=pml_state)
         h = C.c_void_p()
         check(self._L.fdtd_solver_create(C.byref(desc), C.byref(opt), C.byref(h)))
         self._h = h
@@ -55,6 +56,10 @@ class PML_WaveSolver:
 
     def __exit__(self, *a):
         self.close()
+
+    def pml_state(self) -> int:
+        """PML_STATE_AUTO when this solve keeps the reduced PML state, else PML_STATE_FULL."""
+        return int(self._L.fdtd_solver_pml_state(self._h))
 
     def Reinitialize_PML_WaveSolver(self, start_time: float = 0.0):
         check(self._L.fdtd_solver_reset(self._h, float(start_time)), self._h)

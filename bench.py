@@ -163,8 +163,19 @@ def profile_run(args):
     committed ncu summaries under profiles/ were captured with."""
     from acoustics_b200 import scene as S
     from acoustics_b200.solver import PML_WaveSolver
-    sc = S.config2(n=args.profile_n)
     prec = S.PRECISION_FP32_COMPENSATED if args.precision == "fp32" else S.PRECISION_FP64
+    if args.profile_batch:
+        # the 64 uneven scenes stepped eagerly (no graphs), so every kernel is listed
+        from acoustics_b200.batch import SolveBatch
+        scenes = S.config3()
+        b = SolveBatch(scenes, precision=prec, graph_steps=0, tile_y=args.tile_y, x_chunk=args.x_chunk)
+        b.step(args.steps)
+        launches = b.last_launch_count()
+        b.close()
+        print(json.dumps({"profile_run": "config3_batch", "members": len(scenes), "steps": args.steps,
+                          "launches": launches}))
+        return 0
+    sc = S.config2(n=args.profile_n)
     kern = S.KERNEL_PHASED if args.precision == "fp64-plain" else S.KERNEL_FUSED
     g = PML_WaveSolver(sc, precision=prec, kernel=kern, tile_y=args.tile_y, x_chunk=args.x_chunk)
     y = g.step(3 + args.steps)
@@ -291,6 +302,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--profile", action="store_true", help="only run --steps steps of the bench solve (for ncu)")
     ap.add_argument("--profile-n", type=int, default=256, help="grid edge of the --profile solve")
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="with --profile: step the 64-scene batch (config 3) instead of the 256^3 solve")
     ap.add_argument("--tile-y", type=int, default=0, help="PML-shell x planes per thread (1, 2, 4; 0 default)")
     ap.add_argument("--x-chunk", type=int, default=0, help="interior x planes per thread (2, 4, 8; 0 default)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-scene batch (config 3)")

@@ -130,9 +130,20 @@ typedef struct {
     int32_t graph_steps;      /* >0: capture this many steps per CUDA graph launch       */
     int32_t tile_y;           /* fused path: x planes a PML-shell thread marches over; 0: 8   */
     int32_t x_chunk;          /* fused path: interior x planes per thread (2, 4, 8); 0: 2        */
-    int32_t _reserved0;       /* 0 */
+    int32_t pml_state;        /* FDTD_PML_STATE_*                                        */
     int32_t _reserved1;       /* 0 */
 } fdtd_options;
+
+enum {
+    /* FP32 fused solves of static scenes with no solid cell inside the PML keep the
+     * reduced PML state: along every axis without absorption at a PML cell the split
+     * pressure and its two face velocities are replaced by one leapfrog increment
+     * (exact in exact arithmetic; 8 instead of 14 words per slab cell and step).
+     * Split-pressure and velocity fields cannot be read back then.  Every other
+     * solve keeps the full state. */
+    FDTD_PML_STATE_AUTO = 0,
+    FDTD_PML_STATE_FULL = 1   /* always the reference's split pressures and face velocities */
+};
 
 typedef struct {
     int32_t divisions[3];
@@ -223,6 +234,9 @@ fdtd_status fdtd_solver_synchronize(fdtd_solver* s);
 /* The cudaStream_t every kernel of this solver is launched on (for event timing). */
 void* fdtd_solver_stream(fdtd_solver* s);
 const char* fdtd_solver_last_error(fdtd_solver* s);
+/* PML state in effect: FDTD_PML_STATE_FULL, or FDTD_PML_STATE_AUTO when the
+ * reduced state is used (no counterpart in the reference). */
+int32_t fdtd_solver_pml_state(fdtd_solver* s);
 /* Kernel launches issued by the most recent fdtd_solver_step* call. */
 int64_t fdtd_solver_last_launch_count(fdtd_solver* s);
 

@@ -97,3 +97,21 @@ def test_moving_scene_is_refused(fdtd_lib):
     with SolveBatch([], precision=S.PRECISION_FP32_COMPENSATED) as b:
         with pytest.raises(Exception, match="UNSUPPORTED|moving"):
             b.add(sc, 10)
+
+
+def test_batch_mixed_pml_states(fdtd_lib):
+    """FP32 members with the reduced PML state and one with the full state (a
+    box reaching into the PML) step in one batch; each equals its standalone solve."""
+    scenes = uneven_scenes(21, 3)
+    sc = S.config1(divisions=(40, 36, 44), pml_width=6, radius=0.02, steps=60)
+    sc.objects.append(S.RigidObject(S.SHAPE_BOX, (0.08, 0.0, 0.0), (0.04, 0.02, 0.02)))
+    scenes.insert(1, sc)
+    p = S.PRECISION_FP32_COMPENSATED
+    with PML_WaveSolver(sc, precision=p) as g:
+        assert g.pml_state() == S.PML_STATE_FULL
+    with PML_WaveSolver(scenes[0], precision=p) as g:
+        assert g.pml_state() == S.PML_STATE_AUTO
+    with SolveBatch(scenes, precision=p, graph_steps=8) as b:
+        b.run()
+        for m, s in enumerate(scenes):
+            assert np.array_equal(b.output(m), alone(s, p, s.steps)), f"member {m}"

@@ -113,3 +113,48 @@ def test_moving_bodies(oracle_lib, fdtd_lib, precision, tol):
         fg, gg = g.GetGrid()
         assert np.array_equal(fo, fg), chunk
         assert np.array_equal(go, gg), chunk
+
+
+def test_reduced_pml_state_fp32(oracle_lib, fdtd_lib):
+    """FP32 static solves keep the reduced PML state (one leapfrog increment for
+    the axes without absorption of a PML cell): listener series and pressure
+    field agree with the FP64 oracle and with the full split state."""
+    from acoustics_b200._lib import FDTDError
+    sc = small_config2()
+    o = oracle_lib.OracleSolver(sc)
+    yo = o.step(sc.steps)
+    red = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED)
+    full = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED, pml_state=S.PML_STATE_FULL)
+    assert red.pml_state() == S.PML_STATE_AUTO
+    assert full.pml_state() == S.PML_STATE_FULL
+    yr, yf = red.step(sc.steps), full.step(sc.steps)
+    print("reduced vs oracle", rel_l2(yr, yo), "full vs oracle", rel_l2(yf, yo), "reduced vs full", rel_l2(yr, yf))
+    assert rel_l2(yr, yo) <= TOL_FP32
+    assert rel_l2(yf, yo) <= TOL_FP32
+    assert rel_l2(yr, yf) <= 1e-5
+    assert rel_l2(red.field(S.FIELD_PRESSURE), o.field(S.FIELD_PRESSURE)) <= TOL_FP32
+    with pytest.raises(FDTDError):
+        red.field(S.FIELD_PML_PX)
+
+
+def test_reduced_pml_state_only_where_exact(fdtd_lib):
+    """The full state stays where the reduction would not be exact: FP64,
+    moving bodies, a solid cell inside the PML, and a PML width whose inner
+    faces carry absorption next to non-PML cells."""
+    f32 = S.PRECISION_FP32_COMPENSATED
+    assert PML_WaveSolver(S.config1(), precision=f32).pml_state() == S.PML_STATE_AUTO
+    assert PML_WaveSolver(S.config1()).pml_state() == S.PML_STATE_FULL
+    assert PML_WaveSolver(moving_scene(), precision=f32).pml_state() == S.PML_STATE_FULL
+    sc = S.config1(divisions=(40, 40, 40), pml_width=6, radius=0.02)
+    sc.objects.append(S.RigidObject(S.SHAPE_BOX, (0.07, 0.0, 0.0), (0.04, 0.02, 0.02)))  # reaches into the PML
+    assert PML_WaveSolver(sc, precision=f32).pml_state() == S.PML_STATE_FULL
+    assert PML_WaveSolver(S.config1(pml_width=6.5), precision=f32).pml_state() == S.PML_STATE_AUTO
+    assert PML_WaveSolver(S.config1(pml_width=6.2), precision=f32).pml_state() == S.PML_STATE_FULL
+
+
+@pytest.mark.parametrize("pml_width", [6.5, 6.2])
+def test_fp32_fractional_pml_width(oracle_lib, fdtd_lib, pml_width):
+    sc = S.config1(divisions=(40, 36, 44), pml_width=pml_width, radius=0.02)
+    yo = oracle_lib.OracleSolver(sc).step(150)
+    yg = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED).step(150)
+    assert rel_l2(yg, yo) <= TOL_FP32
