@@ -237,6 +237,13 @@ bool use_reduced_pml(const fdtd_solver* s, bool no_solid_pml) {
     return true;
 }
 
+// x planes per PML-shell thread: tile_y when given, else the default of the
+// solve's PML state.
+int shell_planes(const fdtd_solver* s, int tile_y) {
+    if (tile_y > 0) return std::min(tile_y, 256);
+    return s->region.red ? FDTD_SHELL_RED_PLANES : FDTD_SHELL_PLANES;
+}
+
 // PML shell boxes for a given number of x planes per thread (xs).
 void build_shell_boxes(fdtd_solver* s, int xs) {
     ShellBoxes& B = s->shell;
@@ -576,6 +583,7 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     CUDA_TRY(nullptr, cudaSetDevice(o.device));
     CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
+    if (s->precision == FDTD_PRECISION_FP32_COMPENSATED) CUDA_TRY(nullptr, prepare_fp32_kernels());
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
     solver_init_geometry(s.get(), sc);
@@ -822,6 +830,12 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
         s->n_solid_pml = P.n_solid_pml;
     }
     s->region.red = use_reduced_pml(s, solid_pml.empty()) ? 1 : 0;
+    // default x planes per shell thread of the state in effect (tile_y overrides)
+    if (s->opt.kernel == FDTD_KERNEL_FUSED) {
+        const int xs = shell_planes(s, s->opt.tile_y);
+        if (s->shell.xs != xs) build_shell_boxes(s, xs);
+        s->region.shell = s->shell;
+    }
     st = upload_params(s);
     if (st != FDTD_OK) return st;
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));

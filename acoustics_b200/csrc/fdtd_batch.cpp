@@ -25,6 +25,7 @@ using namespace fdtd;
 
 namespace fdtd {
 void build_shell_boxes(fdtd_solver* s, int xs);
+int shell_planes(const fdtd_solver* s, int tile_y);
 }
 
 namespace {
@@ -139,7 +140,8 @@ fdtd_status rebuild(fdtd_batch* b) {
     for (size_t m = 0; m < nm; ++m) {
         Member& mb = b->members[m];
         if (!mb.s) continue;
-        if (mb.s->shell.xs != xs) build_shell_boxes(mb.s, xs);
+        const int xs_m = shell_planes(mb.s, b->opt.tile_y);
+        if (mb.s->shell.xs != xs_m) build_shell_boxes(mb.s, xs_m);
         mb.s->region.shell = mb.s->shell;
         for (int par = 0; par < 2; ++par) {
             char* dst = &descs[par * tbytes + m * dsz];
@@ -297,6 +299,7 @@ fdtd_status fdtd_batch_create(int32_t n, const fdtd_scene_desc* scenes, const in
     BATCH_TRY(nullptr, cudaSetDevice(b->opt.device));
     BATCH_TRY(nullptr, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     BATCH_TRY(nullptr, cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking));
+    if (b->precision == FDTD_PRECISION_FP32_COMPENSATED) BATCH_TRY(nullptr, prepare_fp32_kernels());
     BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
     BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
     for (int i = 0; i < n; ++i) {

@@ -147,7 +147,7 @@ cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, 
     if constexpr (sizeof(T) == 4) {
         n_red = L.n_shell_red;
         if (n_red > 0) {
-            k_batch_shell_red<float><<<n_red, dim3(32, 8), 0, s>>>(D, L.shell_tiles);
+            k_batch_shell_red<float><<<n_red, dim3(32, 8), red_smem_bytes(), s>>>(D, L.shell_tiles);
             ++l;
         }
     }

@@ -30,6 +30,9 @@
 #ifndef FDTD_SHELL_PLANES
 #define FDTD_SHELL_PLANES 8  // x planes a PML-shell thread marches over (default)
 #endif
+#ifndef FDTD_SHELL_RED_PLANES
+#define FDTD_SHELL_RED_PLANES 8  // x planes per PML-shell thread of reduced-state solves (default)
+#endif
 
 #ifndef FDTD_MAX_OBJECTS
 #define FDTD_MAX_OBJECTS 8

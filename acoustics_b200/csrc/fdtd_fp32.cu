@@ -28,6 +28,19 @@ cudaError_t launch_step_regions_fp32(const SolveParams* dP, const SolveParams& h
 
 #include "fdtd_batch.cuh"
 namespace fdtd {
+// The reduced-state shell kernels stage their loads in more than the default
+// 48 KB of dynamic shared memory: raise their limit on the current device.
+cudaError_t prepare_fp32_kernels() {
+    cudaError_t e = cudaSuccess;
+    if (red_smem_bytes() > 0) {
+        e = cudaFuncSetAttribute(k_pml_shell_red<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, red_smem_bytes());
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_batch_shell_red<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     red_smem_bytes());
+    }
+    return e;
+}
+
 cudaError_t launch_batch_fp32(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, cudaEvent_t fork,
                               cudaEvent_t join, int* launches) {
     return launch_batch<float>(L, s, s2, fork, join, launches);

@@ -482,7 +482,7 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     const int nblk = (R.skip & 2) ? 0 : R.shell.block_first[R.shell.n];
     if (nblk > 0) {
         if constexpr (sizeof(T) == 4) {
-            if (R.red) k_pml_shell_red<float><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
+            if (R.red) k_pml_shell_red<float><<<nblk, dim3(32, 8), red_smem_bytes(), s>>>(A, R.shell);
             else k_pml_shell<T><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
         } else {
             k_pml_shell<T><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);

@@ -40,6 +40,7 @@ cudaError_t launch_phased_fp64(const SolveParams* dP, const int N[3], int cur, d
                                int* launches);
 
 // fdtd_fp32.cu
+cudaError_t prepare_fp32_kernels();
 cudaError_t launch_prologue_fp32(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s);
 
 }  // namespace fdtd

@@ -39,8 +39,35 @@
 #ifndef FDTD_SHELL_RED_PREFETCH
 #define FDTD_SHELL_RED_PREFETCH 1
 #endif
+// x planes whose loads a thread keeps in flight through a shared-memory ring
+// (cp.async); 0: the register prefetch of FDTD_SHELL_RED_PREFETCH instead
+#ifndef FDTD_SHELL_RED_STAGES
+#define FDTD_SHELL_RED_STAGES 3
+#endif
 
 namespace fdtd {
+
+// Shared-memory ring of the staged loads: per stage, RED_NVEC vector fields
+// (pp, ym, yp, vxr, vyl, vyr, vzl, a0, a1, a2) and RED_NSCA scalar fields (zme,
+// zpe, vze), each an array over the CTA's 256 threads, so a thread's slots are
+// consecutive words of its own (no bank conflict, no barrier: every thread
+// reads back only what it copied).
+constexpr int RED_NVEC = 10, RED_NSCA = 3;
+__device__ __forceinline__ int threadIdx_lin() { return threadIdx.x + 32 * threadIdx.y; }
+__host__ __device__ constexpr int red_stage_bytes() { return 256 * (RED_NVEC * 4 * shell_vz(4) + RED_NSCA * 4); }
+__host__ __device__ constexpr int red_smem_bytes() {
+    return FDTD_SHELL_RED_STAGES > 0 ? FDTD_SHELL_RED_STAGES * red_stage_bytes() : 0;
+}
+
+template <int BYTES>
+__device__ __forceinline__ void cpa(unsigned saddr, const void* g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(saddr), "l"(g), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
 
 // Loads of one x plane of a reduced-state shell column.
 template <int V>
@@ -82,6 +109,70 @@ __device__ __forceinline__ void red_load(const KArgs<float>& A, RedPlane<shell_v
     L.a0 = ldv<float, V>(pd[0] + q);
     if constexpr (KIND != 2) L.a1 = ldv<float, V>(pd[1] + q);
     if ((KIND == 0 && EY) || ezm) L.a2 = ldv<float, V>(pd[2] + q);
+}
+
+// The loads of red_load as asynchronous copies into ring stage `st` (a shared
+// address of this thread's slot 0 of the stage).
+template <int KIND, bool EY>
+__device__ __forceinline__ void red_stage(const KArgs<float>& A, unsigned st, int x, unsigned c, unsigned q, int spare,
+                                          unsigned ezm, int oym, int oyp, int ozm) {
+    constexpr int V = shell_vz(4);
+    constexpr int VB = 4 * V;
+    constexpr unsigned FV = 256 * VB, FS = 256 * 4, S0 = RED_NVEC * FV;
+    constexpr bool CMP = KIND == 2;
+    const int sx = (int)A.sx, sy = (int)A.sy;
+    const float* pc = A.pc + c;
+    cpa<VB>(st + 0 * FV, pc + (x + 1 < A.N0 ? sx : 0));
+    cpa<VB>(st + 1 * FV, pc - oym);
+    cpa<VB>(st + 2 * FV, pc + oyp);
+    cpa<4>(st + S0 + 0 * FS - (VB - 4) * threadIdx_lin(), pc - ozm);
+    cpa<4>(st + S0 + 1 * FS - (VB - 4) * threadIdx_lin(), pc + V);
+    if constexpr (KIND == 0) cpa<VB>(st + 3 * FV, A.vo[0] + c + sx);
+    if constexpr (EY) {
+        cpa<VB>(st + 4 * FV, A.vo[1] + c);
+        cpa<VB>(st + 5 * FV, A.vo[1] + c + sy);
+    }
+    if (ezm) {
+        const float* vz = CMP ? A.zvo[2] : A.vo[2];
+        cpa<VB>(st + 6 * FV, vz + q);
+        cpa<4>(st + S0 + 2 * FS - (VB - 4) * threadIdx_lin(), vz + q + (spare ? spare : V));
+    }
+    float* const* pd = CMP ? A.zpd : A.pd;
+    cpa<VB>(st + 7 * FV, pd[0] + q);
+    if constexpr (KIND != 2) cpa<VB>(st + 8 * FV, pd[1] + q);
+    if ((KIND == 0 && EY) || ezm) cpa<VB>(st + 9 * FV, pd[2] + q);
+}
+
+// Read back a completed stage (`sp`: generic pointer to this thread's slot 0).
+template <int KIND, bool EY>
+__device__ __forceinline__ void red_unstage(const KArgs<float>& A, RedPlane<shell_vz(4)>& L, const char* sp, int x,
+                                            unsigned ezm) {
+    constexpr int V = shell_vz(4);
+    constexpr int VB = 4 * V;
+    constexpr int FV = 256 * VB, FS = 256 * 4, S0 = RED_NVEC * FV;
+    using VT = Vec<float, V>;
+    const int sfix = (VB - 4) * threadIdx_lin();
+    L.pp = *reinterpret_cast<const VT*>(sp + 0 * FV);
+    L.ym = *reinterpret_cast<const VT*>(sp + 1 * FV);
+    L.yp = *reinterpret_cast<const VT*>(sp + 2 * FV);
+    L.zme = *reinterpret_cast<const float*>(sp + S0 + 0 * FS - sfix);
+    L.zpe = *reinterpret_cast<const float*>(sp + S0 + 1 * FS - sfix);
+    if constexpr (KIND == 0) {
+        L.g = __ldg(A.axflag[0] + x);
+        L.cxr = A.coef[0][x + 1];
+        L.vxr = *reinterpret_cast<const VT*>(sp + 3 * FV);
+    }
+    if constexpr (EY) {
+        L.vyl = *reinterpret_cast<const VT*>(sp + 4 * FV);
+        L.vyr = *reinterpret_cast<const VT*>(sp + 5 * FV);
+    }
+    if (ezm) {
+        L.vzl = *reinterpret_cast<const VT*>(sp + 6 * FV);
+        L.vze = *reinterpret_cast<const float*>(sp + S0 + 2 * FS - sfix);
+    }
+    L.a0 = *reinterpret_cast<const VT*>(sp + 7 * FV);
+    if constexpr (KIND != 2) L.a1 = *reinterpret_cast<const VT*>(sp + 8 * FV);
+    if ((KIND == 0 && EY) || ezm) L.a2 = *reinterpret_cast<const VT*>(sp + 9 * FV);
 }
 
 template <int KIND, bool EY, bool PF>
@@ -161,14 +252,42 @@ __device__ __forceinline__ void shell_tile_red_impl(const KArgs<float>& A, const
         cxl = A.coef[0][x0];
     }
     RedPlane<V> cur, nxt;
-    if constexpr (PF) red_load<KIND, EY>(A, cur, x0, c0, q0, spare, ezm, oym, oyp, ozm);
+    constexpr int NS = FDTD_SHELL_RED_STAGES;
+    extern __shared__ __align__(16) char red_ring[];
+    // this thread's slot 0 of stage 0 (vector fields are VB bytes per thread,
+    // scalar fields 4: red_stage/red_unstage correct the scalar offsets)
+    const int tl = threadIdx_lin();
+    char* const sp0 = red_ring + tl * 4 * V;
+    const unsigned ss0 = (unsigned)__cvta_generic_to_shared(sp0);
+    if constexpr (NS > 0) {
+#pragma unroll
+        for (int k = 0; k < NS - 1; ++k) {
+            if (x0 + k < x1)
+                red_stage<KIND, EY>(A, ss0 + k * red_stage_bytes(), x0 + k, c0 + (unsigned)k * A.sx,
+                                    q0 + (unsigned)(k * csx), spare, ezm, oym, oyp, ozm);
+            cpa_commit();
+        }
+    } else if constexpr (PF) {
+        red_load<KIND, EY>(A, cur, x0, c0, q0, spare, ezm, oym, oyp, ozm);
+    }
     float* const* pdst = CMP ? A.zpd : A.pd;
     T* const vzn = CMP ? A.zvn[2] : A.vn[2];
+    int ring = 0;  // stage of plane x
 #pragma unroll 1
     for (int x = x0; x < x1; ++x) {
         const unsigned c = c0 + (unsigned)(x - x0) * A.sx;
         const unsigned q = CMP ? q0 + (unsigned)(x - x0) * csx : c;
-        if constexpr (PF) {
+        if constexpr (NS > 0) {
+            // the stage of plane x + NS - 1 is the one plane x - 1 was read from
+            const int st = ring == 0 ? NS - 1 : ring - 1;
+            if (x + NS - 1 < x1)
+                red_stage<KIND, EY>(A, ss0 + st * red_stage_bytes(), x + NS - 1, c + (unsigned)(NS - 1) * A.sx,
+                                    q + (unsigned)((NS - 1) * csx), spare, ezm, oym, oyp, ozm);
+            cpa_commit();
+            cpa_wait<NS - 1>();
+            red_unstage<KIND, EY>(A, cur, sp0 + ring * red_stage_bytes(), x, ezm);
+            ring = ring == NS - 1 ? 0 : ring + 1;
+        } else if constexpr (PF) {
             if (x + 1 < x1) red_load<KIND, EY>(A, nxt, x + 1, c + sx, q + csx, spare, ezm, oym, oyp, ozm);
         } else {
             red_load<KIND, EY>(A, cur, x, c, q, spare, ezm, oym, oyp, ozm);
@@ -266,8 +385,9 @@ __device__ __forceinline__ void shell_tile_red_impl(const KArgs<float>& A, const
             vxl = cur.vxr;
             cxl = cur.cxr;
         }
-        if constexpr (PF) cur = nxt;
+        if constexpr (NS == 0 && PF) cur = nxt;
     }
+    if constexpr (NS > 0) cpa_wait<0>();  // no copy outlives the thread
 }
 
 // Box kind: the z-slab pair is B.zbox; an x slab absorbs along x on its first
