@@ -22,6 +22,7 @@ EXPORTS = [
     "fdtd_solver_step_device", "fdtd_solver_fetch_listeners", "fdtd_solver_info_get",
     "fdtd_solver_get_classification", "fdtd_solver_get_field", "fdtd_solver_synchronize",
     "fdtd_solver_stream", "fdtd_solver_last_error", "fdtd_solver_last_launch_count", "fdtd_solver_pml_state",
+    "fdtd_solver_prepare_graphs",
     "fdtd_solver_snapshot", "fdtd_solver_restore", "fdtd_scene_from_xml", "fdtd_scene_desc_get",
     "fdtd_scene_number_of_steps", "fdtd_scene_output_pattern", "fdtd_scene_free", "fdtd_audio_append",
     "fdtd_solver_time_stencil", "fdtd_solver_time_kernel", "fdtd_interior_step_noalloc",
@@ -73,6 +74,7 @@ def load(build_if_missing: bool = False):
         "fdtd_solver_last_error": ([vp], C.c_char_p),
         "fdtd_solver_last_launch_count": ([vp], i64),
         "fdtd_solver_pml_state": ([vp], i32),
+        "fdtd_solver_prepare_graphs": ([vp], i32),
         "fdtd_solver_snapshot": ([vp, vp, C.POINTER(i64)], i32),
         "fdtd_solver_restore": ([vp, vp, i64], i32),
         "fdtd_scene_from_xml": ([C.c_char_p, C.POINTER(vp)], i32),

@@ -583,6 +583,13 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     CUDA_TRY(nullptr, cudaSetDevice(o.device));
     CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
+    CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream3, cudaStreamNonBlocking));
+    CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_ghost, cudaEventDisableTiming));
+    CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream4, cudaStreamNonBlocking));
+    CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_step, cudaEventDisableTiming));
+    CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_lis[0], cudaEventDisableTiming));
+    CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_lis[1], cudaEventDisableTiming));
+    CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_lis_join, cudaEventDisableTiming));
     if (s->precision == FDTD_PRECISION_FP32_COMPENSATED) CUDA_TRY(nullptr, prepare_fp32_kernels());
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
@@ -591,6 +598,8 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         set_error(nullptr, "grid too large: cell indices are 32-bit (padded cells >= 2^31)");
         cudaStreamDestroy(s->stream);
         cudaStreamDestroy(s->stream2);
+        cudaStreamDestroy(s->stream3);
+        cudaStreamDestroy(s->stream4);
         return FDTD_ERR_UNSUPPORTED;
     }
     for (int i = 0; i < sc->n_objects; ++i) {
@@ -745,9 +754,15 @@ fdtd_status fdtd_solver_destroy(fdtd_solver* s) {
     if (s->arena) cudaFree(s->arena);
     if (s->h_lis_stage) cudaFreeHost(s->h_lis_stage);
     cudaStreamSynchronize(s->stream2);
+    if (s->stream3) cudaStreamSynchronize(s->stream3);
+    if (s->stream4) cudaStreamSynchronize(s->stream4);
     cudaEventDestroy(s->ev_fork);
     cudaEventDestroy(s->ev_join);
+    for (cudaEvent_t ev : {s->ev_ghost, s->ev_step, s->ev_lis[0], s->ev_lis[1], s->ev_lis_join})
+        if (ev) cudaEventDestroy(ev);
     cudaStreamDestroy(s->stream2);
+    if (s->stream3) cudaStreamDestroy(s->stream3);
+    if (s->stream4) cudaStreamDestroy(s->stream4);
     cudaStreamDestroy(s->stream);
     delete s;
     return FDTD_OK;

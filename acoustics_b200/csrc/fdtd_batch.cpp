@@ -46,8 +46,8 @@ struct Member {
 struct fdtd_batch {
     fdtd_options opt{};
     int precision = 0;
-    cudaStream_t stream = nullptr, stream2 = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t stream = nullptr, stream2 = nullptr, stream3 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_ghost = nullptr;
     std::vector<Member> members;
     // device tables
     void* d_descs = nullptr;
@@ -231,9 +231,10 @@ fdtd_status enqueue(fdtd_batch* b) {
     BatchLaunch L = b->L;
     L.descs = static_cast<char*>(b->d_descs) + b->flip * b->table_bytes;
     b->flip ^= 1;
+    const StepStreams SS{b->stream, b->stream2, b->stream3, b->ev_fork, b->ev_join, b->ev_ghost};
     cudaError_t e = b->precision == FDTD_PRECISION_FP64
-                        ? launch_batch_fp64(L, b->stream, b->stream2, b->ev_fork, b->ev_join, &l)
-                        : launch_batch_fp32(L, b->stream, b->stream2, b->ev_fork, b->ev_join, &l);
+                        ? launch_batch_fp64(L, SS, &l)
+                        : launch_batch_fp32(L, SS, &l);
     if (e == cudaSuccess) e = launch_batch_tail_any(b->precision, L, b->stream, &l);
     b->launches += l;
     if (e != cudaSuccess) return batch_fail(b, FDTD_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
@@ -299,6 +300,8 @@ fdtd_status fdtd_batch_create(int32_t n, const fdtd_scene_desc* scenes, const in
     BATCH_TRY(nullptr, cudaSetDevice(b->opt.device));
     BATCH_TRY(nullptr, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     BATCH_TRY(nullptr, cudaStreamCreateWithFlags(&b->stream2, cudaStreamNonBlocking));
+    BATCH_TRY(nullptr, cudaStreamCreateWithFlags(&b->stream3, cudaStreamNonBlocking));
+    BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_ghost, cudaEventDisableTiming));
     if (b->precision == FDTD_PRECISION_FP32_COMPENSATED) BATCH_TRY(nullptr, prepare_fp32_kernels());
     BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
     BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
@@ -488,7 +491,9 @@ fdtd_status fdtd_batch_destroy(fdtd_batch* b) {
     if (b->d_refs) cudaFree(b->d_refs);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
+    if (b->ev_ghost) cudaEventDestroy(b->ev_ghost);
     if (b->stream2) cudaStreamDestroy(b->stream2);
+    if (b->stream3) cudaStreamDestroy(b->stream3);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
     return FDTD_OK;

@@ -7,11 +7,12 @@
 // of a step flips.  Because the step constants live on the device, a captured
 // graph of an even number of batched steps replays for any step index.
 //
-// Per step:  k_batch_shell_red / k_batch_shell (PML tiles of the members with
+// Per step:  k_batch_ghost (third stream)  ||  k_batch_interior (second stream)
+//            ||  k_batch_shell_red / k_batch_shell (PML tiles of the members with
 //            the reduced / full PML state; the first tile of a member writes
-//            the member's next-step constants)  ||
-//            k_batch_interior -> k_batch_ghost -> k_batch_sources (second
-//            stream), then k_batch_listeners (launch_batch_tail).
+//            the member's next-step constants), then k_batch_sources (second
+//            stream, after the ghost list), then k_batch_listeners
+//            (launch_batch_tail).
 // The descriptors come in two tables, one per step parity (every member's
 // parity flips each step), so consecutive steps alternate tables and no kernel
 // flips parities on the device.
@@ -115,48 +116,52 @@ __global__ void __launch_bounds__(128) k_batch_listeners(const BatchDesc<T>* __r
 }
 
 template <typename T>
-cudaError_t launch_batch(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, cudaEvent_t fork,
-                         cudaEvent_t join, int* launches) {
+cudaError_t launch_batch(const BatchLaunch& L, const StepStreams& S, int* launches) {
     BatchDesc<T>* D = static_cast<BatchDesc<T>*>(L.descs);
     int l = 0;
     if (L.solid_blocks > 0) {
-        k_batch_solid_pml<T><<<dim3(L.solid_blocks, L.n_members), 256, 0, s>>>(D);
+        k_batch_solid_pml<T><<<dim3(L.solid_blocks, L.n_members), 256, 0, S.s>>>(D);
         ++l;
     }
-    cudaError_t e = cudaEventRecord(fork, s);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, fork, 0);
+    const bool gside = L.ghost_blocks > 0 && S.s3 != nullptr;
+    cudaError_t e = cudaEventRecord(S.fork, S.s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(S.s2, S.fork, 0);
+    if (e == cudaSuccess && gside) e = cudaStreamWaitEvent(S.s3, S.fork, 0);
     if (e != cudaSuccess) return e;
+    if (L.ghost_blocks > 0) {
+        // first: a few latency-bound CTAs that run beside the interior's
+        k_batch_ghost<T><<<dim3(L.ghost_blocks, L.n_members), 128, 0, gside ? S.s3 : S.s2>>>(D);
+        ++l;
+        if (gside && (e = cudaEventRecord(S.ghost, S.s3)) != cudaSuccess) return e;
+    }
     if (L.n_int > 0) {
         const dim3 block(32, 8);
-        if (L.xb == 2) k_batch_interior<T, 2><<<L.n_int, block, 0, s2>>>(D, L.int_tiles);
-        else if (L.xb == 8) k_batch_interior<T, 8><<<L.n_int, block, 0, s2>>>(D, L.int_tiles);
-        else k_batch_interior<T, 4><<<L.n_int, block, 0, s2>>>(D, L.int_tiles);
-        ++l;
-    }
-    if (L.ghost_blocks > 0) {
-        k_batch_ghost<T><<<dim3(L.ghost_blocks, L.n_members), 128, 0, s2>>>(D);
-        ++l;
-    }
-    if (L.src_blocks > 0) {
-        // source cells are non-PML cells: ordered after the interior and ghost updates
-        // of their cells, concurrent with the shell
-        k_batch_sources<T><<<dim3(L.src_blocks, L.n_members), 256, 0, s2>>>(D);
+        if (L.xb == 2) k_batch_interior<T, 2><<<L.n_int, block, 0, S.s2>>>(D, L.int_tiles);
+        else if (L.xb == 8) k_batch_interior<T, 8><<<L.n_int, block, 0, S.s2>>>(D, L.int_tiles);
+        else k_batch_interior<T, 4><<<L.n_int, block, 0, S.s2>>>(D, L.int_tiles);
         ++l;
     }
     int n_red = 0;
     if constexpr (sizeof(T) == 4) {
         n_red = L.n_shell_red;
         if (n_red > 0) {
-            k_batch_shell_red<float><<<n_red, dim3(32, 8), red_smem_bytes(), s>>>(D, L.shell_tiles);
+            k_batch_shell_red<float><<<n_red, dim3(32, 8), red_smem_bytes(), S.s>>>(D, L.shell_tiles);
             ++l;
         }
     }
     if (L.n_shell > n_red) {
-        k_batch_shell<T><<<L.n_shell - n_red, dim3(32, 8), 0, s>>>(D, L.shell_tiles + n_red);
+        k_batch_shell<T><<<L.n_shell - n_red, dim3(32, 8), 0, S.s>>>(D, L.shell_tiles + n_red);
         ++l;
     }
-    e = cudaEventRecord(join, s2);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
+    if (gside && (e = cudaStreamWaitEvent(S.s2, S.ghost, 0)) != cudaSuccess) return e;
+    if (L.src_blocks > 0) {
+        // source cells are non-PML cells: ordered after the interior and ghost updates
+        // of their cells, concurrent with the shell
+        k_batch_sources<T><<<dim3(L.src_blocks, L.n_members), 256, 0, S.s2>>>(D);
+        ++l;
+    }
+    e = cudaEventRecord(S.join, S.s2);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(S.s, S.join, 0);
     if (e != cudaSuccess) return e;
     if (launches) *launches += l;
     return cudaGetLastError();

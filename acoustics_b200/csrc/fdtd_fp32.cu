@@ -20,9 +20,8 @@ cudaError_t launch_prologue_fp32(const SolveParams* dP, int cur, int advance, in
 #include "fdtd_hot.cuh"
 namespace fdtd {
 cudaError_t launch_step_regions_fp32(const SolveParams* dP, const SolveParams& hP, const RegionLaunch& R, int cur,
-                                     cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
-                                     int* launches) {
-    return launch_regions<float>(dP, hP, R, cur, s, s2, fork, join, launches);
+                                     const StepStreams& S, int* launches) {
+    return launch_regions<float>(dP, hP, R, cur, S, launches);
 }
 }  // namespace fdtd
 
@@ -41,8 +40,7 @@ cudaError_t prepare_fp32_kernels() {
     return e;
 }
 
-cudaError_t launch_batch_fp32(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, cudaEvent_t fork,
-                              cudaEvent_t join, int* launches) {
-    return launch_batch<float>(L, s, s2, fork, join, launches);
+cudaError_t launch_batch_fp32(const BatchLaunch& L, const StepStreams& S, int* launches) {
+    return launch_batch<float>(L, S, launches);
 }
 }  // namespace fdtd

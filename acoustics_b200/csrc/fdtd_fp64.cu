@@ -436,9 +436,8 @@ cudaError_t launch_phased_fp64(const SolveParams* dP, const int N[3], int cur, d
 #include "fdtd_hot.cuh"
 namespace fdtd {
 cudaError_t launch_step_regions_fp64(const SolveParams* dP, const SolveParams& hP, const RegionLaunch& R, int cur,
-                                     cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
-                                     int* launches) {
-    return launch_regions<double>(dP, hP, R, cur, s, s2, fork, join, launches);
+                                     const StepStreams& S, int* launches) {
+    return launch_regions<double>(dP, hP, R, cur, S, launches);
 }
 }  // namespace fdtd
 
@@ -447,9 +446,8 @@ cudaError_t launch_step_regions_fp64(const SolveParams* dP, const SolveParams& h
 // ---------------------------------------------------------------------------
 #include "fdtd_batch.cuh"
 namespace fdtd {
-cudaError_t launch_batch_fp64(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, cudaEvent_t fork,
-                              cudaEvent_t join, int* launches) {
-    return launch_batch<double>(L, s, s2, fork, join, launches);
+cudaError_t launch_batch_fp64(const BatchLaunch& L, const StepStreams& S, int* launches) {
+    return launch_batch<double>(L, S, launches);
 }
 cudaError_t launch_batch_tail_any(int precision, const BatchLaunch& L, cudaStream_t s, int* launches) {
     return precision == 0 ? launch_batch_tail<double>(L, s, launches) : launch_batch_tail<float>(L, s, launches);

@@ -451,26 +451,36 @@ __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_pml_shell(
 
 namespace fdtd {
 
-// Host side: one region-split step.  The shell kernel runs on s, the interior
-// kernel on s2 (forked and joined with the two events), then the ghost-cell
-// list and the sources on s.
+// Host side: one region-split step (streams: StepStreams).  Launch order: the
+// ghost-cell list (s3), the interior (s2), the shell (s), then the sources (s2,
+// after the interior and the ghost list, whose cells they add to).
 template <typename T>
 cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const RegionLaunch& R, int cur,
-                           cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join, int* launches) {
+                           const StepStreams& S, int* launches) {
     int l = 0;
     const KArgs<T> A = make_kargs<T>(const_cast<SolveParams*>(dP), hP, cur);
     const Box3& b = R.interior;
     const int nx = b.hi[0] - b.lo[0], ny = b.hi[1] - b.lo[1], nz = b.hi[2] - b.lo[2];
     const bool has_interior = nx > 0 && ny > 0 && nz > 0 && !(R.skip & 1);
-    const bool concurrent = has_interior && s2 != nullptr;
+    const bool has_ghost = R.ghost_cap > 0 && !(R.skip & 4);
+    const bool split = has_interior && S.s2 != nullptr;
+    const bool gside = split && has_ghost && S.s3 != nullptr;
+    const cudaStream_t si = split ? S.s2 : S.s;
     cudaError_t e = cudaSuccess;
-    if (concurrent) {
-        e = cudaEventRecord(fork, s);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, fork, 0);
+    if (split) {
+        e = cudaEventRecord(S.fork, S.s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(S.s2, S.fork, 0);
+        if (e == cudaSuccess && gside) e = cudaStreamWaitEvent(S.s3, S.fork, 0);
         if (e != cudaSuccess) return e;
     }
+    if (has_ghost) {
+        // cells next to a solid: disjoint from the interior and shell cells
+        const int blocks = (R.ghost_cap + 127) / 128 < 1184 ? (R.ghost_cap + 127) / 128 : 1184;
+        k_ghost_cells<T><<<blocks, 128, 0, gside ? S.s3 : si>>>(dP, cur);
+        ++l;
+        if (gside && (e = cudaEventRecord(S.ghost, S.s3)) != cudaSuccess) return e;
+    }
     if (has_interior) {
-        cudaStream_t si = concurrent ? s2 : s;
         dim3 block(32, 8);
         const int xb = (R.xb == 4 || R.xb == 8) ? R.xb : 2;
         dim3 grid(interior_strips_z(b, 16 / (int)sizeof(T)), (ny + 7) / 8, (nx + xb - 1) / xb);
@@ -482,33 +492,28 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     const int nblk = (R.skip & 2) ? 0 : R.shell.block_first[R.shell.n];
     if (nblk > 0) {
         if constexpr (sizeof(T) == 4) {
-            if (R.red) k_pml_shell_red<float><<<nblk, dim3(32, 8), red_smem_bytes(), s>>>(A, R.shell);
-            else k_pml_shell<T><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
+            if (R.red) k_pml_shell_red<float><<<nblk, dim3(32, 8), red_smem_bytes(), S.s>>>(A, R.shell);
+            else k_pml_shell<T><<<nblk, dim3(32, 8), 0, S.s>>>(A, R.shell);
         } else {
-            k_pml_shell<T><<<nblk, dim3(32, 8), 0, s>>>(A, R.shell);
+            k_pml_shell<T><<<nblk, dim3(32, 8), 0, S.s>>>(A, R.shell);
         }
         ++l;
     }
-    if (R.ghost_cap > 0 && !(R.skip & 4)) {
-        // cells next to a solid: disjoint from the interior and shell cells
-        const int blocks = (R.ghost_cap + 127) / 128 < 1184 ? (R.ghost_cap + 127) / 128 : 1184;
-        k_ghost_cells<T><<<blocks, 128, 0, concurrent ? s2 : s>>>(dP, cur);
-        ++l;
-    }
+    if (gside && (e = cudaStreamWaitEvent(S.s2, S.ghost, 0)) != cudaSuccess) return e;
     if (R.sources) {
         // source cells are non-PML cells: after the interior and ghost updates of
-        // their cells (same stream), concurrent with the shell
+        // their cells, concurrent with the shell
         const Box3& r = R.src_region;
         const long long total = (long long)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);
         if (total > 0) {
             const long long g = (total + 255) / 256;
-            k_sources<T><<<(unsigned)(g < 148 * 16 ? g : 148 * 16), 256, 0, concurrent ? s2 : s>>>(dP, cur, r);
+            k_sources<T><<<(unsigned)(g < 148 * 16 ? g : 148 * 16), 256, 0, si>>>(dP, cur, r);
             ++l;
         }
     }
-    if (concurrent) {
-        e = cudaEventRecord(join, s2);
-        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
+    if (split) {
+        e = cudaEventRecord(S.join, S.s2);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(S.s, S.join, 0);
         if (e != cudaSuccess) return e;
     }
     if (launches) *launches += l;

@@ -34,7 +34,13 @@ struct fdtd_solver {
     int precision = 0;
     cudaStream_t stream = nullptr;
     cudaStream_t stream2 = nullptr;   // second stream: interior kernel concurrent with the shell
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    cudaStream_t stream3 = nullptr;   // third stream: ghost-cell list beside the interior
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_ghost = nullptr;
+    // listener rows of step n run on stream4 beside step n+1; step n+2, which
+    // overwrites the pressure they read, waits on ev_lis[parity of step n]
+    cudaStream_t stream4 = nullptr;
+    cudaEvent_t ev_step = nullptr, ev_lis[2] = {nullptr, nullptr}, ev_lis_join = nullptr;
+    bool lis_pending[2] = {false, false};
     // geometry
     double h = 0, c = 0, rho = 0, k = 0, end_time = 0, start_time = 0;
     int N[3] = {0, 0, 0};

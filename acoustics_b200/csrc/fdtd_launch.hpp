@@ -6,19 +6,24 @@
 
 namespace fdtd {
 
+// Streams of one step.  The step is enqueued on s and ends on s; in between the
+// ghost-cell list runs on s3 (launched first: a few latency-bound CTAs next to
+// the interior's), the interior and then the sources on s2, the PML shell on s.
+// s2 / s3 may be null (everything on s).
+struct StepStreams {
+    cudaStream_t s, s2, s3;
+    cudaEvent_t fork, join, ghost;
+};
+
 // region-split step: PML shell, interior, ghost-neighbour list and (while active) sources
 cudaError_t launch_step_regions_fp64(const SolveParams* dP, const SolveParams& hP, const RegionLaunch& R, int cur,
-                                     cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
-                                     int* launches);
+                                     const StepStreams& S, int* launches);
 cudaError_t launch_step_regions_fp32(const SolveParams* dP, const SolveParams& hP, const RegionLaunch& R, int cur,
-                                     cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
-                                     int* launches);
+                                     const StepStreams& S, int* launches);
 
 // batched step of many members (fdtd_batch.cuh)
-cudaError_t launch_batch_fp64(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, cudaEvent_t fork,
-                              cudaEvent_t join, int* launches);
-cudaError_t launch_batch_fp32(const BatchLaunch& L, cudaStream_t s, cudaStream_t s2, cudaEvent_t fork,
-                              cudaEvent_t join, int* launches);
+cudaError_t launch_batch_fp64(const BatchLaunch& L, const StepStreams& S, int* launches);
+cudaError_t launch_batch_fp32(const BatchLaunch& L, const StepStreams& S, int* launches);
 // listener rows + advance of a batched step, for either field type (FP64 unit)
 cudaError_t launch_batch_tail_any(int precision, const BatchLaunch& L, cudaStream_t s, int* launches);
 

@@ -65,10 +65,33 @@ bool sources_active_window(const fdtd_solver* s, double t, int n) {
     return false;
 }
 
+StepStreams step_streams(const fdtd_solver* s) {
+    return StepStreams{s->stream, s->stream2, s->stream3, s->ev_fork, s->ev_join, s->ev_ghost};
+}
+
+// Listener rows of static scenes run on stream4 beside the next step.  Not for
+// moving bodies or solid cells inside the PML: the next step's classification /
+// prologue rewrites cells of the pressure they read.
+bool listeners_aside(const fdtd_solver* s) { return s->stream4 && !s->moving && s->n_solid_pml == 0; }
+
+// Make the solver stream wait for every listener launch on stream4.
+fdtd_status join_listeners(fdtd_solver* s) {
+    if (!s->lis_pending[0] && !s->lis_pending[1]) return FDTD_OK;
+    CUDA_TRY(s, cudaEventRecord(s->ev_lis_join, s->stream4));
+    CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_lis_join, 0));
+    s->lis_pending[0] = s->lis_pending[1] = false;
+    return FDTD_OK;
+}
+
 // Enqueue one time step with the pressure parity `cur`; listener row to dev_row.
 fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify, bool src) {
     s->region.sources = src ? 1 : 0;
     fdtd_status st = FDTD_OK;
+    // this step writes the pressure slot the listeners of the step before last read
+    if (s->lis_pending[cur]) {
+        CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_lis[cur], 0));
+        s->lis_pending[cur] = false;
+    }
     if (classify) {
         // MAC_Grid::classifyCells_FAST + InterpolateFreshPressureCell (PML_WaveSolver.cpp:807-812)
         classification_launches(s, st);
@@ -95,7 +118,7 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         if (s->opt.kernel == FDTD_KERNEL_PHASED) {
             CUDA_TRY(s, launch_phased_fp64(s->dP, s->N, cur, s->d_lap, s->stream, &l));
         } else {
-            CUDA_TRY(s, launch_step_regions_fp64(s->dP, s->hP, s->region, cur, s->stream, s->stream2, s->ev_fork, s->ev_join, &l));
+            CUDA_TRY(s, launch_step_regions_fp64(s->dP, s->hP, s->region, cur, step_streams(s), &l));
         }
         s->launches += l;
     } else {
@@ -104,12 +127,20 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
             s->launches++;
         }
         int l = 0;
-        CUDA_TRY(s, launch_step_regions_fp32(s->dP, s->hP, s->region, cur, s->stream, s->stream2, s->ev_fork, s->ev_join, &l));
+        CUDA_TRY(s, launch_step_regions_fp32(s->dP, s->hP, s->region, cur, step_streams(s), &l));
         s->launches += l;
     }
     if (s->L > 0 && dev_row) {
         // the phased path keeps p^{n+1} in the same slot as the fused one
-        CUDA_TRY(s, launch_listeners(s->dP, s->precision, cur ^ 1, s->L, dev_row, s->stream));
+        if (listeners_aside(s) && !classify) {
+            CUDA_TRY(s, cudaEventRecord(s->ev_step, s->stream));
+            CUDA_TRY(s, cudaStreamWaitEvent(s->stream4, s->ev_step, 0));
+            CUDA_TRY(s, launch_listeners(s->dP, s->precision, cur ^ 1, s->L, dev_row, s->stream4));
+            CUDA_TRY(s, cudaEventRecord(s->ev_lis[cur], s->stream4));
+            s->lis_pending[cur] = true;
+        } else {
+            CUDA_TRY(s, launch_listeners(s->dP, s->precision, cur ^ 1, s->L, dev_row, s->stream));
+        }
         s->launches++;
     }
     return FDTD_OK;
@@ -163,13 +194,16 @@ fdtd_status check_device_errors(fdtd_solver* s) {
 // Capture `n` steps starting at parity `cur` into a graph (static scenes only).
 fdtd_status capture_graph(fdtd_solver* s, int cur, int n, bool src, cudaGraphExec_t* out) {
     cudaGraph_t g = nullptr;
+    fdtd_status st = join_listeners(s);  // no dependency on work outside the capture
+    if (st != FDTD_OK) return st;
     CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-    fdtd_status st = FDTD_OK;
     int c = cur;
     for (int i = 0; i < n && st == FDTD_OK; ++i) {
         st = enqueue_step(s, c, s->d_lis + (size_t)i * s->L, false, src);
         c ^= 1;
     }
+    if (st == FDTD_OK) st = join_listeners(s);  // the graph ends with every row written
+    s->lis_pending[0] = s->lis_pending[1] = false;
     cudaError_t e = cudaStreamEndCapture(s->stream, &g);
     if (st != FDTD_OK) {
         if (g) cudaGraphDestroy(g);
@@ -231,7 +265,9 @@ fdtd_status run_steps(fdtd_solver* s, int n, Sink sink) {
             st = after_step(s);
             if (st != FDTD_OK) return st;
         }
-        fdtd_status st = sink(done, m);
+        fdtd_status st = join_listeners(s);
+        if (st != FDTD_OK) return st;
+        st = sink(done, m);
         if (st != FDTD_OK) return st;
         done += m;
     }
@@ -307,9 +343,9 @@ fdtd_status fdtd_solver_time_kernel(fdtd_solver* s, int32_t which, int32_t n_lau
             e = launch_listeners(s->dP, s->precision, c, s->L, s->d_lis, s->stream);
         } else if (s->precision == FDTD_PRECISION_FP64) {
             if (s->opt.kernel == FDTD_KERNEL_PHASED) e = launch_phased_fp64(s->dP, s->N, c, s->d_lap, s->stream, nullptr);
-            else e = launch_step_regions_fp64(s->dP, s->hP, R, c, s->stream, s->stream2, s->ev_fork, s->ev_join, nullptr);
+            else e = launch_step_regions_fp64(s->dP, s->hP, R, c, step_streams(s), nullptr);
         } else {
-            e = launch_step_regions_fp32(s->dP, s->hP, R, c, s->stream, s->stream2, s->ev_fork, s->ev_join, nullptr);
+            e = launch_step_regions_fp32(s->dP, s->hP, R, c, step_streams(s), nullptr);
         }
         if (e != cudaSuccess) {
             set_error(s, std::string("stencil launch: ") + cudaGetErrorString(e));
@@ -341,6 +377,22 @@ void* fdtd_solver_stream(fdtd_solver* s) { return s ? (void*)s->stream : nullptr
 const char* fdtd_solver_last_error(fdtd_solver* s) { return s ? s->err.c_str() : ""; }
 
 int64_t fdtd_solver_last_launch_count(fdtd_solver* s) { return s ? s->last_launches : 0; }
+
+fdtd_status fdtd_solver_prepare_graphs(fdtd_solver* s) {
+    if (!s) return FDTD_ERR_INVALID_ARG;
+    const int G = s->opt.graph_steps;
+    if (G <= 0 || s->moving || s->step_index == 0) return FDTD_OK;
+    CUDA_TRY(s, cudaSetDevice(s->opt.device));
+    const bool src = sources_active_window(s, s->time, G);
+    const int key = s->cur + (src ? 2 : 0);
+    if (s->graph_exec[key]) return FDTD_OK;
+    const long long l0 = s->launches;
+    fdtd_status st = capture_graph(s, s->cur, G, src, &s->graph_exec[key]);
+    if (st != FDTD_OK) return st;
+    s->graph_launches_per_exec = s->launches - l0;
+    s->launches = l0;
+    return FDTD_OK;
+}
 
 int32_t fdtd_solver_pml_state(fdtd_solver* s) {
     return (s && s->region.red) ? FDTD_PML_STATE_AUTO : FDTD_PML_STATE_FULL;

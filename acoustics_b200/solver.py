@@ -98,6 +98,10 @@ class PML_WaveSolver:
     def last_launch_count(self) -> int:
         return int(self._L.fdtd_solver_last_launch_count(self._h))
 
+    def prepare_graphs(self):
+        """Capture the CUDA graph of the next graph_steps-long chunk now (nothing runs)."""
+        check(self._L.fdtd_solver_prepare_graphs(self._h), self._h)
+
     def time_stencil(self, n_launches: int) -> float:
         """Milliseconds for n back-to-back launches of the step kernel (CUDA events
         on the solver stream).  Advances the state without prologue/listeners."""

@@ -339,6 +339,7 @@ def main():
     info = solver.info()
     ext = torch.cuda.ExternalStream(solver.stream)
     solver.step_device(W, dev_out.data_ptr())
+    solver.prepare_graphs()  # one-time graph capture outside the timed region (runs nothing)
     solver.synchronize()
     dist.barrier(ranks)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -389,6 +390,7 @@ def main():
             sv = PML_WaveSolver(sc, precision=p2, kernel=k2, graph_steps=G if k2 == S.KERNEL_FUSED else 0, device=local)
             n = min(K, 200)
             sv.step_device(5, dev_out.data_ptr())
+            sv.prepare_graphs()
             sv.synchronize()
             ext2 = torch.cuda.ExternalStream(sv.stream)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

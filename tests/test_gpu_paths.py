@@ -38,6 +38,11 @@ def test_graph_replay_identical_to_eager(fdtd_lib, precision):
     a = PML_WaveSolver(sc, precision=precision).step(75)
     b = PML_WaveSolver(sc, precision=precision, graph_steps=10).step(75)
     assert np.array_equal(a, b)
+    # graphs captured ahead of time by prepare_graphs replay the same steps
+    c = PML_WaveSolver(sc, precision=precision, graph_steps=10)
+    y0 = c.step(5)
+    c.prepare_graphs()
+    assert np.array_equal(np.concatenate([y0, c.step(70)]), a)
 
 
 def test_snapshot_restore_roundtrip(fdtd_lib):
