@@ -157,10 +157,9 @@ fdtd_status rebuild(fdtd_batch* b) {
         const Box3& I = mb.s->region.interior;
         const int nx = I.hi[0] - I.lo[0], ny = I.hi[1] - I.lo[1], nz = I.hi[2] - I.lo[2];
         if (nx > 0 && ny > 0 && nz > 0) {
-            const int tz = interior_strips_z(I, f64 ? 2 : 4), ty = (ny + 7) / 8, tx = (nx + xb - 1) / xb;
+            const int tu = interior_unit_tiles(I, f64 ? 2 : 4), tx = (nx + xb - 1) / xb;
             for (int x = 0; x < tx; ++x)
-                for (int y = 0; y < ty; ++y)
-                    for (int z = 0; z < tz; ++z) it.push_back({(int)m, 0, z, y, x});
+                for (int u = 0; u < tu; ++u) it.push_back({(int)m, 0, u, 0, x});
         }
         const ShellBoxes& B = mb.s->shell;
         // the member's first shell tile (ty = 1) advances its step constants;

@@ -35,7 +35,7 @@ __global__ void __launch_bounds__(256) k_batch_interior(const BatchDesc<T>* __re
                                                         const BatchTile* __restrict__ tiles) {
     const BatchTile tile = tiles[blockIdx.x];
     const BatchDesc<T>& d = D[tile.m];
-    interior_tile<T, XB>(d.a[d.cur], d.interior, tile.tz, tile.ty, tile.tx);
+    interior_tile<T, XB>(d.a[d.cur], d.interior, tile.tz, tile.tx);
 }
 
 // The first shell tile of a member (tile.ty = 1) also writes the member's

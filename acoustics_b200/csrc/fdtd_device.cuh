@@ -360,7 +360,11 @@ struct BatchLaunch {
 __host__ __device__ inline int interior_groups_z(const Box3& b, int V) {
     return b.hi[2] > b.lo[2] ? (b.hi[2] - 1) / V - b.lo[2] / V + 1 : 0;
 }
-__host__ __device__ inline int interior_strips_z(const Box3& b, int V) { return (interior_groups_z(b, V) + 31) / 32; }
+// CTAs of 256 (row, z-group) units per x-plane tile of the interior box
+__host__ __device__ inline int interior_unit_tiles(const Box3& b, int V) {
+    const long long units = (long long)(b.hi[1] - b.lo[1]) * interior_groups_z(b, V);
+    return b.hi[1] > b.lo[1] ? (int)((units + 255) / 256) : 0;
+}
 
 // padded index of cell (or low face) (i, j, k)
 __host__ __device__ __forceinline__ long long cidx(const SolveParams& P, int i, int j, int k) {

@@ -12,9 +12,10 @@
 // the launcher runs them concurrently on two streams; cells next to a solid
 // (k_ghost_cells) and active sources (k_sources) follow on the first stream.
 //
-// Interior mapping: a CTA of 32 (z) x 8 (y) threads, each thread owns XB
-// consecutive x planes of one (y, z) column; every load of those planes is
-// issued before the arithmetic; z neighbours come from the warp by shuffles.
+// Interior mapping: a CTA of 256 threads owns 256 consecutive (row, z-group)
+// units of the non-PML box, each thread XB consecutive x planes of its unit;
+// every load of those planes is issued before the arithmetic; z neighbours come
+// from the warp by shuffles.
 //
 // Shell mapping: five boxes (two x slabs, two y slabs, the merged pair of z
 // slabs); a thread owns one z-vector group of one row and marches along x; a
@@ -64,27 +65,33 @@ __device__ __forceinline__ void stv(T* p, const Vec<T, V>& v) {
     *reinterpret_cast<Vec<T, V>*>(p) = v;
 }
 
-// One interior tile: 32 z-vector groups (128 FP32 / 64 FP64 cells) x 8 y rows
-// x XB x planes, at tile coordinates (tz, ty, tx) of the box.  Every access is
-// a 16-byte vector load or store (classification bytes: one 4- or 2-byte
-// word), z neighbours across vectors come from the adjacent lane by shuffles
-// and at the strip edges from memory.  Cells of a group outside the box or not
-// plain bulk are masked (scalar stores for partial groups).  Every thread of
-// the CTA must call it.
+// One interior tile: 256 consecutive (row, z-group) units of the box (one per
+// thread; a z group is a 16-byte vector of V = 4 FP32 / 2 FP64 cells starting
+// at a multiple of V) x XB x planes, at unit tile tu and plane tile tx.  Units
+// are packed densely across rows, so narrow boxes leave no lane idle.  Every
+// access is a 16-byte vector load or store (classification bytes: one 4- or
+// 2-byte word); the z neighbour across vectors comes from the adjacent lane by a
+// shuffle when that lane holds the neighbouring group of the same row, else
+// from memory.  Cells of a group outside the box or not plain bulk are masked
+// (scalar stores for partial groups).  Every thread of the CTA must call it.
 template <typename T, int XB>
-__device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box, int tz, int ty, int tx) {
+__device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box, int tu, int tx) {
     constexpr bool COMP = sizeof(T) == 4;
     constexpr int V = 16 / (int)sizeof(T);
     using VT = Vec16<T>;
     const int lane = threadIdx.x;
-    const int zg0 = box.lo[2] / V * V;
-    const int zlast = (box.hi[2] - 1) / V * V;
-    const int zv = zg0 + (tz * 32 + lane) * V;
-    const int y = box.lo[1] + ty * 8 + threadIdx.y;
+    const int ng = interior_groups_z(box, V);
+    const int ny = box.hi[1] - box.lo[1];
+    const int u = tu * 256 + threadIdx.x + 32 * threadIdx.y;
+    int row = u / ng, g = u - row * ng;
+    const bool lane_on = row < ny;
+    if (!lane_on) {  // inactive lanes shadow the box's last unit for the shuffles
+        row = ny - 1;
+        g = ng - 1;
+    }
+    const int zc = box.lo[2] / V * V + g * V;
+    const int yc = box.lo[1] + row;
     const int x0 = box.lo[0] + tx * XB;
-    const bool lane_on = (zv <= zlast) && (y < box.hi[1]);
-    const int zc = min(zv, zlast);  // inactive lanes shadow a valid group for the shuffles
-    const int yc = min(y, box.hi[1] - 1);
     const int nx = min(XB, box.hi[0] - x0);
     // signed strides: offsets below are formed relative to the tile's first cell
     // and may be negative (pc[i*sx - 1] at i = 0)
@@ -94,8 +101,9 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
     T* __restrict__ pn = A.pn + off;
     float* __restrict__ dinc = A.dinc + off;
     const uint8_t* __restrict__ cls = A.cls + off;
-    // the z+V neighbour comes from memory where the next lane does not hold it
-    const bool zp_mem = (lane == 31) || (zv + V > zlast);
+    // z neighbours from memory where the adjacent lane does not hold them
+    const bool zm_mem = (lane == 0) || (g == 0);
+    const bool zp_mem = (lane == 31) || (g == ng - 1);
 
     VT pcol[XB + 2], ym[XB], yp[XB], prev[XB];
     uint32_t code[XB];
@@ -118,7 +126,7 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
             }
             if constexpr (V == 4) code[i] = *reinterpret_cast<const uint32_t*>(cls + i * sx);
             else code[i] = *reinterpret_cast<const uint16_t*>(cls + i * sx);
-            zme[i] = (lane == 0) ? pc[i * sx - 1] : (T)0;
+            zme[i] = zm_mem ? pc[i * sx - 1] : (T)0;
             zpe[i] = zp_mem ? pc[i * sx + V] : (T)0;
         }
     }
@@ -128,7 +136,7 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
         const VT& c0 = pcol[i + 1];
         const T left = __shfl_up_sync(0xffffffffu, c0.e[V - 1], 1);
         const T right = __shfl_down_sync(0xffffffffu, c0.e[0], 1);
-        const T zm_edge = lane == 0 ? zme[i] : left;
+        const T zm_edge = zm_mem ? zme[i] : left;
         const T zp_edge = zp_mem ? zpe[i] : right;
         VT outp, outd;
         unsigned act = 0;
@@ -171,7 +179,7 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
 
 template <typename T, int XB>
 __global__ void __launch_bounds__(256) k_interior(const KArgs<T> A, Box3 box) {
-    interior_tile<T, XB>(A, box, blockIdx.x, blockIdx.y, blockIdx.z);
+    interior_tile<T, XB>(A, box, blockIdx.x, blockIdx.y);
 }
 
 // Masked store of a z vector: one vector store when every cell is selected,
@@ -483,7 +491,7 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     if (has_interior) {
         dim3 block(32, 8);
         const int xb = (R.xb == 4 || R.xb == 8) ? R.xb : 2;
-        dim3 grid(interior_strips_z(b, 16 / (int)sizeof(T)), (ny + 7) / 8, (nx + xb - 1) / xb);
+        dim3 grid(interior_unit_tiles(b, 16 / (int)sizeof(T)), (nx + xb - 1) / xb);
         if (xb == 2) k_interior<T, 2><<<grid, block, 0, si>>>(A, b);
         else if (xb == 8) k_interior<T, 8><<<grid, block, 0, si>>>(A, b);
         else k_interior<T, 4><<<grid, block, 0, si>>>(A, b);
