@@ -39,6 +39,7 @@ struct Member {
     fdtd_status status = FDTD_OK;
     int L = 0;
     std::vector<double> rows;
+    int64_t tiles = 0;      // interior + shell tiles of the member in the current tables
 };
 
 }  // namespace
@@ -62,6 +63,7 @@ struct fdtd_batch {
     size_t table_bytes = 0;  // one descriptor table (the second, at this offset, has every parity flipped)
     int flip = 0;            // table of the next step
     bool dirty = true;
+    int64_t table_tiles = 0;  // tiles in the current tables (finished members' included until the next rebuild)
     cudaGraphExec_t graph[2] = {nullptr, nullptr};  // G steps starting at table 0 / 1
     long long launches = 0, last_launches = 0, graph_launches = 0;
     std::string err;
@@ -91,7 +93,7 @@ fdtd_status batch_cuda_fail(fdtd_batch* b, cudaError_t e, const char* what) {
 namespace {
 
 template <typename T>
-void fill_desc(BatchDesc<T>& d, fdtd_solver* s, bool active) {
+void fill_desc(BatchDesc<T>& d, fdtd_solver* s, bool active, int64_t total, bool halted) {
     std::memset(&d, 0, sizeof(d));
     d.a[0] = make_kargs<T>(s->dP, s->hP, 0);
     d.a[1] = make_kargs<T>(s->dP, s->hP, 1);
@@ -106,6 +108,8 @@ void fill_desc(BatchDesc<T>& d, fdtd_solver* s, bool active) {
     d.active = active ? 1 : 0;
     d.has_src = s->hP.n_src > 0 ? 1 : 0;
     d.ghost_cap = s->region.ghost_cap;
+    d.total = total;
+    d.halted = halted ? 1 : 0;
 }
 
 template <typename T>
@@ -146,14 +150,16 @@ fdtd_status rebuild(fdtd_batch* b) {
         for (int par = 0; par < 2; ++par) {
             char* dst = &descs[par * tbytes + m * dsz];
             if (f64) {
-                fill_desc<double>(*reinterpret_cast<BatchDesc<double>*>(dst), mb.s, mb.active);
+                fill_desc<double>(*reinterpret_cast<BatchDesc<double>*>(dst), mb.s, mb.active, mb.total, mb.done >= mb.total);
                 reinterpret_cast<BatchDesc<double>*>(dst)->cur ^= par;
             } else {
-                fill_desc<float>(*reinterpret_cast<BatchDesc<float>*>(dst), mb.s, mb.active);
+                fill_desc<float>(*reinterpret_cast<BatchDesc<float>*>(dst), mb.s, mb.active, mb.total, mb.done >= mb.total);
                 reinterpret_cast<BatchDesc<float>*>(dst)->cur ^= par;
             }
         }
+        mb.tiles = 0;
         if (!mb.active) continue;
+        const size_t tiles0 = it.size() + st.size() + st_full.size();
         const Box3& I = mb.s->region.interior;
         const int nx = I.hi[0] - I.lo[0], ny = I.hi[1] - I.lo[1], nz = I.hi[2] - I.lo[2];
         if (nx > 0 && ny > 0 && nz > 0) {
@@ -162,13 +168,12 @@ fdtd_status rebuild(fdtd_batch* b) {
                 for (int u = 0; u < tu; ++u) it.push_back({(int)m, 0, u, 0, x});
         }
         const ShellBoxes& B = mb.s->shell;
-        // the member's first shell tile (ty = 1) advances its step constants;
-        // members with the reduced PML state come first in the table
+        // members with the reduced PML state come first in the shell table
         std::vector<BatchTile>& tab = mb.s->region.red ? st : st_full;
-        const size_t first_tile = tab.size();
         for (int bx = 0; bx < B.n; ++bx)
             for (int x = 0; x < B.tx[bx]; ++x)
-                for (int u = 0; u < B.tu[bx]; ++u) tab.push_back({(int)m, bx, u, tab.size() == first_tile ? 1 : 0, x});
+                for (int u = 0; u < B.tu[bx]; ++u) tab.push_back({(int)m, bx, u, 0, x});
+        mb.tiles = (int64_t)(it.size() + st.size() + st_full.size() - tiles0);
         for (int li = 0; li < mb.s->L; ++li) refs.push_back({(int)m, li});
         max_ghost = std::max(max_ghost, (mb.s->region.ghost_cap + 127) / 128);
         max_solid = std::max(max_solid, (mb.s->n_solid_pml + 255) / 256);
@@ -205,6 +210,7 @@ fdtd_status rebuild(fdtd_batch* b) {
     b->flip = 0;
     L.int_tiles = b->d_int;
     L.n_int = (int)it.size();
+    b->table_tiles = (int64_t)(it.size() + st.size());
     L.shell_tiles = b->d_shell;
     L.n_shell = (int)st.size();
     L.n_shell_red = b->precision == FDTD_PRECISION_FP64 ? 0 : n_shell_red;
@@ -229,6 +235,7 @@ fdtd_status enqueue(fdtd_batch* b) {
     int l = 0;
     BatchLaunch L = b->L;
     L.descs = static_cast<char*>(b->d_descs) + b->flip * b->table_bytes;
+    L.descs_other = static_cast<char*>(b->d_descs) + (b->flip ^ 1) * b->table_bytes;
     b->flip ^= 1;
     const StepStreams SS{b->stream, b->stream2, b->stream3, b->ev_fork, b->ev_join, b->ev_ghost};
     cudaError_t e = b->precision == FDTD_PRECISION_FP64
@@ -363,15 +370,18 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int32_t n_steps, int32_t* n_active) {
     int64_t left = n_steps;
     const int G = b->opt.graph_steps;
     while (left > 0) {
-        int64_t chunk = left;
+        // members stop on the device at their own last step (k_batch_advance), so a
+        // chunk runs until the longest member finishes, within the listener rings
+        int64_t chunk = left, longest = 0;
         bool any = false;
         for (auto& mb : b->members)
             if (mb.active) {
                 any = true;
-                chunk = std::min(chunk, mb.total - mb.done);
+                longest = std::max<int64_t>(longest, mb.total - mb.done);
                 chunk = std::min<int64_t>(chunk, mb.s->lis_cap_steps);
             }
         if (!any) break;
+        chunk = std::min(chunk, longest);
         if (b->dirty) {
             fdtd_status st = rebuild(b);
             if (st != FDTD_OK) return st;
@@ -398,25 +408,32 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int32_t n_steps, int32_t* n_active) {
         for (size_t m = 0; m < b->members.size(); ++m) {
             Member& mb = b->members[m];
             if (!mb.active) continue;
-            fdtd_status st = collect_rows(b, mb, mb.done, chunk);
+            fdtd_status st = collect_rows(b, mb, mb.done, std::min<int64_t>(chunk, mb.total - mb.done));
             if (st != FDTD_OK) return st;
             BATCH_TRY(b, cudaMemcpyAsync(&errs[m], mb.s->hP.dev_error, sizeof(int), cudaMemcpyDeviceToHost, b->stream));
         }
         BATCH_TRY(b, cudaStreamSynchronize(b->stream));
+        int64_t idle_tiles = 0;
         for (size_t m = 0; m < b->members.size(); ++m) {
             Member& mb = b->members[m];
-            if (!mb.active) continue;
+            if (!mb.active) {
+                idle_tiles += mb.tiles;
+                continue;
+            }
             fdtd_solver* s = mb.s;
-            s->cur ^= (int)(chunk & 1);
-            s->step_index += chunk;
-            for (int64_t i = 0; i < chunk; ++i) s->time += s->k;
-            mb.done += chunk;
+            const int64_t n = std::min<int64_t>(chunk, mb.total - mb.done);
+            s->cur ^= (int)(n & 1);
+            s->step_index += n;
+            for (int64_t i = 0; i < n; ++i) s->time += s->k;
+            mb.done += n;
             if (errs[m] & 1) mb.status = FDTD_ERR_NUMERIC;
             if (mb.done >= mb.total) {
                 mb.active = false;
-                b->dirty = true;
+                idle_tiles += mb.tiles;
             }
         }
+        // new tables (and graphs) only once a quarter of the tiles belong to finished members
+        if (idle_tiles * 4 > b->table_tiles) b->dirty = true;
         left -= chunk;
     }
     b->last_launches = b->launches - l0;

@@ -9,10 +9,9 @@
 //
 // Per step:  k_batch_ghost (third stream)  ||  k_batch_interior (second stream)
 //            ||  k_batch_shell_red / k_batch_shell (PML tiles of the members with
-//            the reduced / full PML state; the first tile of a member writes
-//            the member's next-step constants), then k_batch_sources (second
-//            stream, after the ghost list), then k_batch_listeners
-//            (launch_batch_tail).
+//            the reduced / full PML state), then k_batch_sources (second
+//            stream, after the ghost list), then k_batch_listeners and
+//            k_batch_advance (launch_batch_tail).
 // The descriptors come in two tables, one per step parity (every member's
 // parity flips each step), so consecutive steps alternate tables and no kernel
 // flips parities on the device.
@@ -35,17 +34,16 @@ __global__ void __launch_bounds__(256) k_batch_interior(const BatchDesc<T>* __re
                                                         const BatchTile* __restrict__ tiles) {
     const BatchTile tile = tiles[blockIdx.x];
     const BatchDesc<T>& d = D[tile.m];
+    if (d.halted) return;
     interior_tile<T, XB>(d.a[d.cur], d.interior, tile.tz, tile.tx);
 }
 
-// The first shell tile of a member (tile.ty = 1) also writes the member's
-// constants of the next step (consts[cur ^ 1]; this step reads consts[cur]).
 template <typename T>
 __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_batch_shell(const BatchDesc<T>* __restrict__ D,
                                                                       const BatchTile* __restrict__ tiles) {
     const BatchTile tile = tiles[blockIdx.x];
     const BatchDesc<T>& d = D[tile.m];
-    if (tile.ty && threadIdx.x == 0 && threadIdx.y == 0) advance_consts(*d.P, d.cur);
+    if (d.halted) return;
     shell_tile<T>(d.a[d.cur], d.shell, tile.box, tile.tz, tile.tx);
 }
 
@@ -56,7 +54,7 @@ __global__ void __launch_bounds__(256, FDTD_SHELL_RED_MINB) k_batch_shell_red(co
     static_assert(sizeof(T) == 4, "the reduced PML state is an FP32 path");
     const BatchTile tile = tiles[blockIdx.x];
     const BatchDesc<T>& d = D[tile.m];
-    if (tile.ty && threadIdx.x == 0 && threadIdx.y == 0) advance_consts(*d.P, d.cur);
+    if (d.halted) return;
     shell_tile_red(d.a[d.cur], d.shell, tile.box, tile.tz, tile.tx);
 }
 
@@ -66,7 +64,7 @@ __global__ void __launch_bounds__(256, FDTD_SHELL_RED_MINB) k_batch_shell_red(co
 template <typename T>
 __global__ void __launch_bounds__(256) k_batch_solid_pml(const BatchDesc<T>* __restrict__ D) {
     const BatchDesc<T>& d = D[blockIdx.y];
-    if (!d.active) return;
+    if (!d.active || d.halted) return;
     const SolveParams& P = *d.P;
     T* p0 = (T*)P.p[0];
     T* p1 = (T*)P.p[1];
@@ -82,7 +80,7 @@ __global__ void __launch_bounds__(256) k_batch_solid_pml(const BatchDesc<T>* __r
 template <typename T>
 __global__ void __launch_bounds__(128) k_batch_ghost(const BatchDesc<T>* __restrict__ D) {
     const BatchDesc<T>& d = D[blockIdx.y];
-    if (!d.active || d.ghost_cap == 0) return;
+    if (!d.active || d.halted || d.ghost_cap == 0) return;
     ghost_cells_body<T>(*d.P, d.cur, blockIdx.x, gridDim.x);
 }
 
@@ -90,7 +88,7 @@ __global__ void __launch_bounds__(128) k_batch_ghost(const BatchDesc<T>* __restr
 template <typename T>
 __global__ void __launch_bounds__(256) k_batch_sources(const BatchDesc<T>* __restrict__ D) {
     const BatchDesc<T>& d = D[blockIdx.y];
-    if (!d.active || !d.has_src) return;
+    if (!d.active || d.halted || !d.has_src) return;
     // a source whose time factor underflowed to zero adds nothing (the single-solve
     // path skips the launch then); the whole block leaves together
     const StepConsts& c = d.P->consts[d.cur];
@@ -108,7 +106,7 @@ __global__ void __launch_bounds__(128) k_batch_listeners(const BatchDesc<T>* __r
     if (w >= n) return;
     const ListenerRef r = refs[w];
     const BatchDesc<T>& d = D[r.m];
-    if (!d.active) return;
+    if (!d.active || d.halted) return;
     const long long step = d.P->consts[d.cur].step;
     double* row = d.ring + (size_t)(step % d.ring_cap) * d.n_lis;
     if (d.P->lis_ready) listener_plan<T>(*d.P, d.cur ^ 1, r.li, row);
@@ -167,6 +165,27 @@ cudaError_t launch_batch(const BatchLaunch& L, const StepStreams& S, int* launch
     return cudaGetLastError();
 }
 
+// Last kernel of a batched step, one thread per member: write the member's
+// constants of the next step (consts[cur ^ 1]) and, after its last step, mark
+// it halted in both descriptor tables, so its kernels leave at once from the
+// next step on whatever the parity of the table (the tables alternate every
+// step, a halted member's state no longer does).  Members retire without a new
+// tile table or graph.
+template <typename T>
+__global__ void __launch_bounds__(128) k_batch_advance(BatchDesc<T>* __restrict__ D, BatchDesc<T>* __restrict__ D2,
+                                                       int n) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= n) return;
+    const BatchDesc<T>& d = D[m];
+    if (!d.active || d.halted) return;
+    const long long step = d.P->consts[d.cur].step;
+    advance_consts(*d.P, d.cur);
+    if (step + 1 >= d.total) {
+        D[m].halted = 1;
+        D2[m].halted = 1;
+    }
+}
+
 // Listener rows of a batched step.  Instantiated in the FP64 translation unit
 // for both field types, like the single-solve listener kernel, so the
 // double-precision MLS arithmetic is compiled the same way (no FMA
@@ -176,6 +195,11 @@ cudaError_t launch_batch_tail(const BatchLaunch& L, cudaStream_t s, int* launche
     BatchDesc<T>* D = static_cast<BatchDesc<T>*>(L.descs);
     if (L.n_refs > 0) {
         k_batch_listeners<T><<<(L.n_refs * 32 + 127) / 128, 128, 0, s>>>(D, L.refs, L.n_refs);
+        if (launches) *launches += 1;
+    }
+    if (L.n_members > 0) {
+        k_batch_advance<T><<<(L.n_members + 127) / 128, 128, 0, s>>>(D, static_cast<BatchDesc<T>*>(L.descs_other),
+                                                                      L.n_members);
         if (launches) *launches += 1;
     }
     return cudaGetLastError();

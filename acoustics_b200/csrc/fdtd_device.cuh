@@ -327,6 +327,8 @@ struct BatchDesc {
     int active;
     int has_src;
     int ghost_cap;
+    long long total;     // steps the member runs in all (the first, classifying one included)
+    int halted;          // set in both tables by k_batch_advance after the member's last step
 };
 
 struct BatchTile {
@@ -340,7 +342,8 @@ struct ListenerRef {
 };
 
 struct BatchLaunch {
-    void* descs;                 // BatchDesc<T>[n_members] on the device
+    void* descs;                 // BatchDesc<T>[n_members] on the device (table of this step's parity)
+    void* descs_other;           // the other parity's table (k_batch_advance marks halted members in both)
     const BatchTile* int_tiles;
     int n_int;
     const BatchTile* shell_tiles;
