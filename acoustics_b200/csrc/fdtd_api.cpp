@@ -817,34 +817,29 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     s->launches = 0;
     st = run_classification(s);
     if (st != FDTD_OK) return st;
-    // ResetCellHistory(true): every cell has a valid history after reset
-    // (the classification kernels keep it in bit 6; re-set it on all cells)
-    std::vector<uint8_t> cls(np);
-    CUDA_TRY(s, cudaMemcpyAsync(cls.data(), P.cls, np, cudaMemcpyDeviceToHost, s->stream));
+    // ResetCellHistory(true): every cell has a valid history after reset (the
+    // classification kernels keep it in bit 6; set it on all cells), and the
+    // solid cells inside the PML, re-zeroed every step of a static scene
+    int* d_count = s->d_status + 3;
+    int n_solid = 0;
+    CUDA_TRY(s, cudaMemsetAsync(d_count, 0, sizeof(int), s->stream));
+    CUDA_TRY(s, launch_cls_history(s->dP, s->ncell, d_count, nullptr, 0, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(&n_solid, d_count, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-    std::vector<int> solid_pml;
-    for (int i = 0; i < s->N[0]; ++i)
-        for (int j = 0; j < s->N[1]; ++j)
-            for (int k = 0; k < s->N[2]; ++k) {
-                const long long c = i * s->SX + j * s->SY + k;
-                cls[c] |= CLS_VALID;
-                if (!(cls[c] & CLS_BULK) &&
-                    (s->tab[0].pml_cell[i] || s->tab[1].pml_cell[j] || s->tab[2].pml_cell[k]))
-                    solid_pml.push_back((int)c);
-            }
-    CUDA_TRY(s, cudaMemcpy(P.cls, cls.data(), np, cudaMemcpyHostToDevice));
     if (s->d_solid_pml) {
         cudaFree(s->d_solid_pml);
         s->d_solid_pml = nullptr;
     }
-    if (!solid_pml.empty() && !s->moving) {
-        CUDA_TRY(s, cudaMalloc((void**)&s->d_solid_pml, solid_pml.size() * sizeof(int)));
-        CUDA_TRY(s, cudaMemcpy(s->d_solid_pml, solid_pml.data(), solid_pml.size() * sizeof(int), cudaMemcpyHostToDevice));
+    if (n_solid > 0 && !s->moving) {
+        CUDA_TRY(s, cudaMalloc((void**)&s->d_solid_pml, (size_t)n_solid * sizeof(int)));
+        CUDA_TRY(s, cudaMemsetAsync(d_count, 0, sizeof(int), s->stream));
+        CUDA_TRY(s, launch_cls_history(s->dP, s->ncell, d_count, s->d_solid_pml, n_solid, s->stream));
         P.solid_pml = s->d_solid_pml;
-        P.n_solid_pml = (int)solid_pml.size();
+        P.n_solid_pml = n_solid;
         s->n_solid_pml = P.n_solid_pml;
     }
-    s->region.red = use_reduced_pml(s, solid_pml.empty()) ? 1 : 0;
+    CUDA_TRY(s, cudaMemsetAsync(d_count, 0, sizeof(int), s->stream));
+    s->region.red = use_reduced_pml(s, n_solid == 0) ? 1 : 0;
     // default x planes per shell thread of the state in effect (tile_y overrides)
     if (s->opt.kernel == FDTD_KERNEL_FUSED) {
         const int xs = shell_planes(s, s->opt.tile_y);

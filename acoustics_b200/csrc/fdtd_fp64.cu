@@ -403,6 +403,30 @@ cudaError_t launch_cls_solid(const SolveParams* dP, const int start[3], const in
     return cudaGetLastError();
 }
 
+// ResetCellHistory(true) after the classification of a reset: every cell gets a
+// valid history (bit 6).  Also counts the solid cells inside the PML into
+// *count and, when `list` is given, writes their padded indices (in no fixed
+// order: they are only re-zeroed each step).
+__global__ void k_cls_history(const SolveParams* __restrict__ Pp, long long n, int* count, int* list, int cap) {
+    const SolveParams& P = *Pp;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        int i, j, k;
+        dense_ijk(P, t, i, j, k);
+        const long long c = cidx(P, i, j, k);
+        const uint8_t code = P.cls[c];
+        if (!list) P.cls[c] = code | CLS_VALID;
+        if (!(code & CLS_BULK) && (P.pml_cell[0][i] || P.pml_cell[1][j] || P.pml_cell[2][k])) {
+            const int slot = atomicAdd(count, 1);
+            if (list && slot < cap) list[slot] = (int)c;
+        }
+    }
+}
+
+cudaError_t launch_cls_history(const SolveParams* dP, long long ncell, int* count, int* list, int cap, cudaStream_t s) {
+    k_cls_history<<<grid_for(ncell, 256), 256, 0, s>>>(dP, ncell, count, list, cap);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_cls_ghost(const SolveParams* dP, long long ncell, cudaStream_t s) {
     k_cls_ghost<<<grid_for(ncell, 256), 256, 0, s>>>(dP, ncell);
     return cudaGetLastError();

@@ -37,6 +37,7 @@ cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int
 cudaError_t launch_cls_reset(const SolveParams* dP, long long ncell, cudaStream_t s);
 cudaError_t launch_cls_solid(const SolveParams* dP, const int start[3], const int range[3], cudaStream_t s);
 cudaError_t launch_cls_ghost(const SolveParams* dP, long long ncell, cudaStream_t s);
+cudaError_t launch_cls_history(const SolveParams* dP, long long ncell, int* count, int* list, int cap, cudaStream_t s);
 cudaError_t launch_fresh_cells(const SolveParams* dP, int precision, int cur, long long ncell, int* d_status,
                                cudaStream_t s);
 
