@@ -475,13 +475,22 @@ fdtd_status fdtd_solver_get_classification(fdtd_solver* s, uint8_t* flags, fdtd_
     return FDTD_OK;
 }
 
-fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, int64_t count) {
-    if (!s || !out) return FDTD_ERR_INVALID_ARG;
+}  // extern "C"
+
+namespace {
+
+// Field `which` between the device layout (padded arrays, the compact z-slab
+// arrays of the PML state) and a dense host array in the reference's flat order
+// (cells, or faces of one orientation).  to_device: dense -> device.  FP32
+// PRESSURE_PREV is p^n - d (d the compensated increment); writing it sets d from
+// the p^n already on the device, so write PRESSURE first.
+fdtd_status field_transfer(fdtd_solver* s, int32_t which, double* dense, int64_t count, bool to_device) {
+    if (!s || !dense) return FDTD_ERR_INVALID_ARG;
     CUDA_TRY(s, cudaSetDevice(s->opt.device));
     const SolveParams& P = s->hP;
     const bool f64 = s->precision == FDTD_PRECISION_FP64;
     const size_t w = f64 ? 8 : 4;
-    const void* src = nullptr;
+    void* src = nullptr;
     long long n = s->ncell;
     int vbuf = s->opt.kernel == FDTD_KERNEL_PHASED ? 0 : s->cur;
     switch (which) {
@@ -498,7 +507,7 @@ fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, in
     if (s->region.red && which >= FDTD_FIELD_PML_PX)
         return (set_error(s, "this FP32 solve keeps the reduced PML state (no split pressures or face velocities "
                              "along axes without absorption); create it with pml_state = FDTD_PML_STATE_FULL to "
-                             "read them"),
+                             "access them"),
                 FDTD_ERR_UNSUPPORTED);
     // extent of the requested grid (cells, or faces of one orientation)
     int ext[3] = {s->N[0], s->N[1], s->N[2]};
@@ -507,7 +516,8 @@ fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, in
     std::vector<char> raw(np * w);
     std::vector<float> inc;
     CUDA_TRY(s, cudaMemcpyAsync(raw.data(), src, np * w, cudaMemcpyDeviceToHost, s->stream));
-    if (!f64 && which == FDTD_FIELD_PRESSURE_PREV) {
+    const bool fp32_prev = !f64 && which == FDTD_FIELD_PRESSURE_PREV;
+    if (fp32_prev) {
         inc.resize(np);
         CUDA_TRY(s, cudaMemcpyAsync(inc.data(), P.dinc, np * 4, cudaMemcpyDeviceToHost, s->stream));
     }
@@ -515,13 +525,15 @@ fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, in
     const ShellBoxes& B = s->shell;
     const bool zc = P.zcount > 0 && which >= FDTD_FIELD_PML_PX;
     std::vector<char> zraw;
+    void* zsrc = nullptr;
     if (zc) {
-        const void* zsrc = which <= FDTD_FIELD_PML_PZ ? P.zpd[which - FDTD_FIELD_PML_PX] : P.zv[vbuf][which - FDTD_FIELD_VX];
+        zsrc = which <= FDTD_FIELD_PML_PZ ? P.zpd[which - FDTD_FIELD_PML_PX] : P.zv[vbuf][which - FDTD_FIELD_VX];
         zraw.resize(P.zcount * w);
         CUDA_TRY(s, cudaMemcpyAsync(zraw.data(), zsrc, P.zcount * w, cudaMemcpyDeviceToHost, s->stream));
     }
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-    if (zc) {
+    // every (padded grid index, compact index) pair of the z-slab box
+    auto for_compact = [&](auto&& fn) {
         const int b = B.zbox, V = B.vz;
         const int X0 = B.x0[b], Y0 = B.y0[b], nxb = B.nx[b], nyb = B.ny[b];
         auto slot = [&](int z) -> long long {  // compact slot of the cell (or its low face) z in the row
@@ -541,23 +553,54 @@ fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, in
                         q = ((z - 1) % V != V - 1) ? qc + 1 : (long long)B.ng[b] * V;
                     }
                     if (q < 0 || (dface != 2 && z == s->N[2])) continue;
-                    const long long c = x * s->SX + y * s->SY + z;
-                    if (f64) std::memcpy(raw.data() + c * 8, zraw.data() + (row + q) * 8, 8);
-                    else std::memcpy(raw.data() + c * 4, zraw.data() + (row + q) * 4, 4);
+                    fn(x * s->SX + y * s->SY + z, row + q);
                 }
             }
+    };
+    double* r64 = (double*)raw.data();
+    float* r32 = (float*)raw.data();
+    if (!to_device) {
+        if (zc) for_compact([&](long long c, long long q) { std::memcpy(raw.data() + c * w, zraw.data() + q * w, w); });
+        long long o = 0;
+        for (int i = 0; i < ext[0]; ++i)
+            for (int j = 0; j < ext[1]; ++j)
+                for (int k = 0; k < ext[2]; ++k, ++o) {
+                    const long long c = i * s->SX + j * s->SY + k;
+                    if (f64) dense[o] = r64[c];
+                    else dense[o] = fp32_prev ? (double)r32[c] - (double)inc[c] : (double)r32[c];
+                }
+        return FDTD_OK;
     }
-    const double* r64 = (const double*)raw.data();
-    const float* r32 = (const float*)raw.data();
     long long o = 0;
     for (int i = 0; i < ext[0]; ++i)
         for (int j = 0; j < ext[1]; ++j)
             for (int k = 0; k < ext[2]; ++k, ++o) {
                 const long long c = i * s->SX + j * s->SY + k;
-                if (f64) out[o] = r64[c];
-                else out[o] = inc.empty() ? (double)r32[c] : (double)r32[c] - (double)inc[c];
+                if (f64) r64[c] = dense[o];
+                else if (fp32_prev) inc[c] = (float)((double)r32[c] - dense[o]);
+                else r32[c] = (float)dense[o];
             }
+    if (fp32_prev) {
+        CUDA_TRY(s, cudaMemcpyAsync(P.dinc, inc.data(), np * 4, cudaMemcpyHostToDevice, s->stream));
+    } else {
+        if (zc) for_compact([&](long long c, long long q) { std::memcpy(zraw.data() + q * w, raw.data() + c * w, w); });
+        CUDA_TRY(s, cudaMemcpyAsync(src, raw.data(), np * w, cudaMemcpyHostToDevice, s->stream));
+        if (zc) CUDA_TRY(s, cudaMemcpyAsync(zsrc, zraw.data(), P.zcount * w, cudaMemcpyHostToDevice, s->stream));
+    }
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     return FDTD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, int64_t count) {
+    return field_transfer(s, which, out, count, false);
+}
+
+fdtd_status fdtd_solver_set_field(fdtd_solver* s, int32_t which, const double* in, int64_t count) {
+    return field_transfer(s, which, const_cast<double*>(in), count, true);
 }
 
 // ---------------------------------------------------------------------------

@@ -145,6 +145,27 @@ class PML_WaveSolver:
         check(self._L.fdtd_solver_get_field(self._h, int(which), out.ctypes.data, count), self._h)
         return out
 
+    def set_field(self, which: int, values) -> None:
+        """The inverse of field(): a dense field (the reference's flat order) into the solve."""
+        a = np.ascontiguousarray(values, dtype=np.float64).ravel()
+        check(self._L.fdtd_solver_set_field(self._h, int(which), a.ctypes.data, a.size), self._h)
+
+    # ---- the reference's output files (FDTD_AcousticSimulator.cpp) ----
+    def save_snapshot(self, numbering: str, output_pattern: str = "%s") -> None:
+        """_SaveSimulationSnapshot(numbering): snapshot_<numbering>_*.dat files."""
+        check(self._L.fdtd_solver_save_snapshot(self._h, output_pattern.encode(), str(numbering).encode()), self._h)
+
+    def load_snapshot(self, numbering: str, output_pattern: str = "%s") -> None:
+        check(self._L.fdtd_solver_load_snapshot(self._h, output_pattern.encode(), str(numbering).encode()), self._h)
+
+    def save_config(self, output_pattern: str = "%s") -> None:
+        """SaveSolverConfig's position files."""
+        check(self._L.fdtd_solver_save_config(self._h, output_pattern.encode()), self._h)
+
+    def save_field_timestep(self, path: str, which: int = FIELD_PRESSURE) -> None:
+        """_SavePressureTimestep / _SaveVelocityTimestep: (n x 1) matrix, x fastest."""
+        check(self._L.fdtd_solver_save_field_timestep(self._h, int(which), path.encode()), self._h)
+
     def snapshot(self) -> bytes:
         n = C.c_int64(0)
         check(self._L.fdtd_solver_snapshot(self._h, None, C.byref(n)), self._h)
@@ -243,3 +264,19 @@ def device_count() -> int:
     n = C.c_int32(0)
     st = load().fdtd_device_count(C.byref(n))
     return int(n.value) if st == 0 else 0
+
+
+def write_matrix(path: str, a) -> None:
+    """IO::writeMatrixX<double>(a, path, IO::BINARY): int32 rows, int32 cols, row-major doubles."""
+    a = np.ascontiguousarray(np.atleast_2d(np.asarray(a, dtype=np.float64)))
+    check(load().fdtd_matrix_write(path.encode(), a.shape[0], a.shape[1], a.ctypes.data))
+
+
+def read_matrix(path: str) -> np.ndarray:
+    """MATRIX::read / the reader of write_matrix: a (rows, cols) array."""
+    L = load()
+    r, c = C.c_int32(0), C.c_int32(0)
+    check(L.fdtd_matrix_read(path.encode(), C.byref(r), C.byref(c), None, 0))
+    out = np.zeros((r.value, c.value), dtype=np.float64)
+    check(L.fdtd_matrix_read(path.encode(), C.byref(r), C.byref(c), out.ctypes.data, out.size))
+    return out

@@ -229,6 +229,12 @@ fdtd_status fdtd_solver_get_classification(fdtd_solver* s, uint8_t* flags_n, fdt
                                            int64_t* n_faces);
 /* Field read-back as doubles (FetchCell / GetGrid accessors). */
 fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, int64_t count);
+/* The inverse of fdtd_solver_get_field (no counterpart in the reference): a dense
+ * field into the solve (cells, or faces of one orientation, in the reference's flat
+ * order).  FP32 FDTD_FIELD_PRESSURE_PREV sets the compensated increment from the
+ * current pressure, so set FDTD_FIELD_PRESSURE first.  Split pressures and
+ * velocities need the full PML state (FDTD_ERR_UNSUPPORTED on the reduced one). */
+fdtd_status fdtd_solver_set_field(fdtd_solver* s, int32_t which, const double* in, int64_t count);
 /* Synchronise the solver's stream. */
 fdtd_status fdtd_solver_synchronize(fdtd_solver* s);
 /* The cudaStream_t every kernel of this solver is launched on (for event timing). */
@@ -240,6 +246,31 @@ const char* fdtd_solver_last_error(fdtd_solver* s);
  * capture cost.  A no-op without graph_steps, for moving scenes and before
  * the first (classifying) step. */
 fdtd_status fdtd_solver_prepare_graphs(fdtd_solver* s);
+/* ------------------------------------------------------------------------ */
+/* output files (fdtd_io.cpp)                                               */
+
+/* IO::writeMatrixX<double>(..., IO::BINARY) (src/utils/IO/IO.h:107-160) and
+ * MATRIX::write (src/linearalgebra/MATRIX_FAST.cpp:134-155): int32 rows, int32
+ * cols, rows*cols doubles, row-major. */
+fdtd_status fdtd_matrix_write(const char* path, int32_t rows, int32_t cols, const double* data);
+/* the reader (MATRIX::read, MATRIX_FAST.cpp:160-187); data may be NULL to query the size */
+fdtd_status fdtd_matrix_read(const char* path, int32_t* rows, int32_t* cols, double* data, int64_t capacity);
+/* FDTD_AcousticSimulator::_SaveSimulationSnapshot (FDTD_AcousticSimulator.cpp:381-415):
+ * snapshot_<numbering>_{p_pml_d, v_pml_d, p_collocated_d, p_pml_full, p_collocated_ind}
+ * composed with the output pattern's %s (CompositeFilename, :109-125; NULL: "%s").
+ * The collocated buffer the next step overwrites unread is written as zeros.
+ * Needs the full PML state. */
+fdtd_status fdtd_solver_save_snapshot(fdtd_solver* s, const char* output_pattern, const char* numbering);
+/* The inverse (no counterpart in the reference): pressures, split pressures and
+ * velocities of a snapshot of a grid of the same size into this solve. */
+fdtd_status fdtd_solver_load_snapshot(fdtd_solver* s, const char* output_pattern, const char* numbering);
+/* SaveSolverConfig's position files (FDTD_AcousticSimulator.cpp:146-230, :647-661):
+ * pressure_vertex_position.dat, velocity_<d>_vertex_position.dat, listening_position.dat */
+fdtd_status fdtd_solver_save_config(fdtd_solver* s, const char* output_pattern);
+/* _SavePressureTimestep / _SaveVelocityTimestep (FDTD_AcousticSimulator.cpp:253-307):
+ * which = FDTD_FIELD_PRESSURE or FDTD_FIELD_V{X,Y,Z}, x-fastest (n x 1) matrix */
+fdtd_status fdtd_solver_save_field_timestep(fdtd_solver* s, int32_t which, const char* path);
+
 /* PML state in effect: FDTD_PML_STATE_FULL, or FDTD_PML_STATE_AUTO when the
  * reduced state is used (no counterpart in the reference). */
 int32_t fdtd_solver_pml_state(fdtd_solver* s);

@@ -208,3 +208,19 @@ def test_scene_info_on_the_host(fdtd_lib):
     assert i32.n_interior_cells == 11239424 and i32.n_pml_cells == 5537792
     assert i32.algorithmic_bytes_per_step == 444989440.0
     assert i64.algorithmic_bytes_per_step == 2 * i32.algorithmic_bytes_per_step
+
+
+def test_matrix_file_layout(fdtd_lib, tmp_path):
+    """IO::writeMatrixX BINARY / MATRIX::write layout: int32 rows, int32 cols,
+    row-major doubles; the reader returns the same array."""
+    from acoustics_b200.solver import read_matrix, write_matrix
+    a = np.arange(12, dtype=np.float64).reshape(4, 3) * 0.5 - 1.0
+    p = str(tmp_path / "m.dat")
+    write_matrix(p, a)
+    raw = open(p, "rb").read()
+    assert np.frombuffer(raw[:8], dtype=np.int32).tolist() == [4, 3]
+    assert np.array_equal(np.frombuffer(raw[8:], dtype=np.float64), a.ravel())
+    assert len(raw) == 8 + 12 * 8
+    assert np.array_equal(read_matrix(p), a)
+    with pytest.raises(Exception):
+        read_matrix(str(tmp_path / "missing.dat"))
