@@ -24,7 +24,7 @@ EXPORTS = [
     "fdtd_solver_stream", "fdtd_solver_last_error", "fdtd_solver_last_launch_count", "fdtd_solver_pml_state",
     "fdtd_solver_prepare_graphs", "fdtd_solver_set_field", "fdtd_matrix_write", "fdtd_matrix_read",
     "fdtd_solver_save_snapshot", "fdtd_solver_load_snapshot", "fdtd_solver_save_config",
-    "fdtd_solver_save_field_timestep",
+    "fdtd_solver_save_field_timestep", "fdtd_solver_boundary_info",
     "fdtd_solver_snapshot", "fdtd_solver_restore", "fdtd_scene_from_xml", "fdtd_scene_desc_get",
     "fdtd_scene_number_of_steps", "fdtd_scene_output_pattern", "fdtd_scene_free", "fdtd_audio_append",
     "fdtd_solver_time_stencil", "fdtd_solver_time_kernel", "fdtd_interior_step_noalloc",
@@ -84,6 +84,7 @@ def load(build_if_missing: bool = False):
         "fdtd_solver_load_snapshot": ([vp, C.c_char_p, C.c_char_p], i32),
         "fdtd_solver_save_config": ([vp, C.c_char_p], i32),
         "fdtd_solver_save_field_timestep": ([vp, i32, C.c_char_p], i32),
+        "fdtd_solver_boundary_info": ([vp, C.POINTER(i64), C.POINTER(i64), C.POINTER(i64), C.POINTER(i32)], i32),
         "fdtd_solver_snapshot": ([vp, vp, C.POINTER(i64)], i32),
         "fdtd_solver_restore": ([vp, vp, i64], i32),
         "fdtd_scene_from_xml": ([C.c_char_p, C.POINTER(vp)], i32),

@@ -417,6 +417,16 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
     }
     for (int i = 0; i < sc->n_sources; ++i)
         if (!(sc->sources[i].width_time > 0)) return (set_error(nullptr, "source_width_time must be positive"), FDTD_ERR_INVALID_ARG);
+    if (sc->boundary_handling != FDTD_BOUNDARY_RASTERIZE && sc->boundary_handling != FDTD_BOUNDARY_FULLY_COUPLED)
+        return (set_error(nullptr, "unknown boundary_handling"), FDTD_ERR_INVALID_ARG);
+    if (sc->boundary_handling == FDTD_BOUNDARY_FULLY_COUPLED)
+        for (int i = 0; i < sc->n_objects; ++i) {
+            if (sc->objects[i].motion != FDTD_MOTION_STATIC)
+                return (set_error(nullptr, "FULLY_COUPLED boundaries are built for static scenes only"), FDTD_ERR_UNSUPPORTED);
+            if (sc->objects[i].shape == FDTD_SHAPE_ELLIPSOID)
+                return (set_error(nullptr, "FULLY_COUPLED boundaries need a closest-point query (spheres and boxes)"),
+                        FDTD_ERR_UNSUPPORTED);
+        }
     return FDTD_OK;
 }
 
@@ -577,9 +587,12 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         return (set_error(nullptr, "no CUDA device visible"), FDTD_ERR_CUDA);
     if (o.device < 0 || o.device >= ndev) return (set_error(nullptr, "device ordinal out of range"), FDTD_ERR_INVALID_ARG);
 
+    if (sc->boundary_handling == FDTD_BOUNDARY_FULLY_COUPLED && o.kernel != FDTD_KERNEL_FUSED)
+        return (set_error(nullptr, "FULLY_COUPLED boundaries run on the fused kernels"), FDTD_ERR_UNSUPPORTED);
     std::unique_ptr<fdtd_solver> s(new fdtd_solver());
     s->opt = o;
     s->precision = o.precision;
+    s->boundary_handling = sc->boundary_handling;
     CUDA_TRY(nullptr, cudaSetDevice(o.device));
     CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
@@ -751,6 +764,7 @@ fdtd_status fdtd_solver_destroy(fdtd_solver* s) {
     cudaStreamSynchronize(s->stream);
     for (int i = 0; i < 4; ++i)
         if (s->graph_exec[i]) cudaGraphExecDestroy(s->graph_exec[i]);
+    free_fully_coupled(s);
     if (s->arena) cudaFree(s->arena);
     if (s->h_lis_stage) cudaFreeHost(s->h_lis_stage);
     cudaStreamSynchronize(s->stream2);
@@ -839,6 +853,11 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
         s->n_solid_pml = P.n_solid_pml;
     }
     CUDA_TRY(s, cudaMemsetAsync(d_count, 0, sizeof(int), s->stream));
+    if (s->boundary_handling == FDTD_BOUNDARY_FULLY_COUPLED) {
+        st = build_fully_coupled(s);
+        if (st != FDTD_OK) return st;
+    }
+    s->region.fc = P.fc_n > 0 ? 1 : 0;
     s->region.red = use_reduced_pml(s, n_solid == 0) ? 1 : 0;
     // default x planes per shell thread of the state in effect (tile_y overrides)
     if (s->opt.kernel == FDTD_KERNEL_FUSED) {

@@ -112,6 +112,7 @@ struct ShellBoxes {
 };
 
 struct SolveParams;
+struct FcRow;
 
 // Precomputed order-1 MLS of one listener (static classification): the sample
 // value is sum_r w_r * value_r over its rows.  A row is the pressure of a cell
@@ -183,6 +184,7 @@ struct RegionLaunch {
     int xb;            // x planes per interior thread
     int skip;          // kernels left out (timing of single kernels): 1 interior, 2 shell, 4 ghost list
     int red;           // FP32: the shell keeps the reduced PML state (k_pml_shell_red)
+    int fc;            // FULLY_COUPLED ghost cells: solve their system before the ghost list
 };
 
 // Two copies indexed by the step parity: the kernels of a step read
@@ -251,6 +253,36 @@ struct SolveParams {
     int* ghost_count;
     int ghost_cap;
     int precision;                // 0 fp64, 1 fp32 compensated
+    // FULLY_COUPLED ghost cells (static scenes; null under RASTERIZE)
+    const FcRow* fc_rows;         // [fc_n] one row per ghost face, owners ascending, directions ascending
+    const int* fc_idx;            // [np] per ghost (solid) cell: (first row << 6) | bulk-direction mask; -1 elsewhere
+    double* fc_b;                 // [fc_n] right-hand side of the step
+    double* fc_x;                 // [2][fc_n] ghost pressures by step parity
+    double* fc_work;              // [6][fc_n] BiCGSTAB vectors
+    int fc_n;
+    int fc_maxit;
+    int* fc_status;               // iterations of the last solve (negative: not converged)
+};
+
+// Row of the FULLY_COUPLED ghost-cell system (MAC_Grid::PML_pressureUpdateGhostCells,
+// MAC_Grid.cpp:1131-1425) of one ghost face; everything but the pressures and the
+// boundary acceleration is fixed for a static scene.
+//   kind 0: x = pg (diagonal +1)        kind 1: constraint, x = p_neig (diagonal +1)
+//   kind 2: immersed, -x + sum_u w_u x_u = -(weighted + sum_k w_k p_k + w_s r_s)
+//   kind 3: immersed row whose stencil failed the condition test, -x = -pg
+// with pg = p_neig - 0.75 h (g . n_cell), g = -rho a(bp, t), weighted = (g . ne) fdw,
+// r_s = (g . ne) h on the boundary row of the owner.
+struct FcRow {
+    int owner, nbr;               // padded indices of the solid cell and its bulk neighbour
+    int kind, obj, dim, sign;     // direction owner -> nbr
+    int si;                       // stencil slot of the boundary (Neumann) row, -1: none
+    int pad_;
+    double bp[3];                 // boundary point (acceleration sample)
+    double ne[3];                 // erected normal
+    double fdw;                   // finite-difference weight
+    double w[8];                  // interpolation weights at the image point
+    int cell[8];                  // known cell of slot k (padded index), -1: none
+    int unk[8];                   // unknown ghost row of slot k, -1: none
 };
 
 template <typename T>

@@ -109,9 +109,12 @@ FDTD_HD int lowest_object(const SolveParams& P, const double p[3], double* dista
     return id;
 }
 
-// FDTD_RigidObject::ReflectAgainstBoundary for a point outside the body
-// (FDTD_RigidObject.cpp:429-536, outside branch): boundary point bp, erected
-// normal n = normalize(x - bp), image point x + (x - bp), travelled distance.
+// FDTD_RigidObject::ReflectAgainstBoundary (FDTD_RigidObject.cpp:429-536, closest
+// point branch): bp the closest boundary point, dist the signed distance.
+// Outside the body the erected normal is x - bp and the image x + (x - bp);
+// inside it is bp - x and the image bp + (bp - x), outside the body.  The
+// normal is normalised.  (A box's closest point of an inside point lies on
+// the face nearest to it.)
 FDTD_HD void reflect_against_boundary(const DevObject& o, const double x[3], double image[3], double bp[3],
                                       double nrm[3], double& dist) {
     const double r[3] = {x[0] - o.c[0], x[1] - o.c[1], x[2] - o.c[2]};
@@ -123,13 +126,24 @@ FDTD_HD void reflect_against_boundary(const DevObject& o, const double x[3], dou
         double q[3], qc[3];
         for (int j = 0; j < 3; ++j) q[j] = o.R[0 * 3 + j] * r[0] + o.R[1 * 3 + j] * r[1] + o.R[2 * 3 + j] * r[2];
         for (int j = 0; j < 3; ++j) qc[j] = dmax(-o.size[j], dmin(o.size[j], q[j]));
+        dist = sdf_local(o, x);
+        if (dist < 0.0) {  // inside: onto the nearest face
+            int jm = 0;
+            for (int j = 1; j < 3; ++j)
+                if (o.size[j] - fabs(q[j]) < o.size[jm] - fabs(q[jm])) jm = j;
+            qc[jm] = q[jm] < 0.0 ? -o.size[jm] : o.size[jm];
+        }
         for (int i = 0; i < 3; ++i)
             bp[i] = o.c[i] + (o.R[i * 3 + 0] * qc[0] + o.R[i * 3 + 1] * qc[1] + o.R[i * 3 + 2] * qc[2]);
-        dist = sdf_local(o, x);
     }
     double e[3];
-    for (int i = 0; i < 3; ++i) e[i] = -bp[i] + x[i];
-    for (int i = 0; i < 3; ++i) image[i] = x[i] + e[i];
+    if (dist < 0.0) {
+        for (int i = 0; i < 3; ++i) e[i] = bp[i] - x[i];
+        for (int i = 0; i < 3; ++i) image[i] = bp[i] + e[i];
+    } else {
+        for (int i = 0; i < 3; ++i) e[i] = -bp[i] + x[i];
+        for (int i = 0; i < 3; ++i) image[i] = x[i] + e[i];
+    }
     const double en = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
     for (int i = 0; i < 3; ++i) nrm[i] = en > 0.0 ? e[i] / en : 0.0;
 }

@@ -472,7 +472,7 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     const bool has_interior = nx > 0 && ny > 0 && nz > 0 && !(R.skip & 1);
     const bool has_ghost = R.ghost_cap > 0 && !(R.skip & 4);
     const bool split = has_interior && S.s2 != nullptr;
-    const bool gside = split && has_ghost && S.s3 != nullptr;
+    const bool gside = split && (has_ghost || R.fc) && S.s3 != nullptr;
     const cudaStream_t si = split ? S.s2 : S.s;
     cudaError_t e = cudaSuccess;
     if (split) {
@@ -481,13 +481,19 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
         if (e == cudaSuccess && gside) e = cudaStreamWaitEvent(S.s3, S.fork, 0);
         if (e != cudaSuccess) return e;
     }
+    if (R.fc) {
+        // FULLY_COUPLED: this step's ghost pressures, before the cells that read them
+        k_fc_rhs<T><<<64, 256, 0, gside ? S.s3 : si>>>(dP, cur);
+        k_fc_solve<<<1, 1024, 0, gside ? S.s3 : si>>>(dP, cur);
+        l += 2;
+    }
     if (has_ghost) {
         // cells next to a solid: disjoint from the interior and shell cells
         const int blocks = (R.ghost_cap + 127) / 128 < 1184 ? (R.ghost_cap + 127) / 128 : 1184;
         k_ghost_cells<T><<<blocks, 128, 0, gside ? S.s3 : si>>>(dP, cur);
         ++l;
-        if (gside && (e = cudaEventRecord(S.ghost, S.s3)) != cudaSuccess) return e;
     }
+    if (gside && (e = cudaEventRecord(S.ghost, S.s3)) != cudaSuccess) return e;
     if (has_interior) {
         dim3 block(32, 8);
         const int xb = (R.xb == 4 || R.xb == 8) ? R.xb : 2;

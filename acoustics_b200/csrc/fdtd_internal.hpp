@@ -55,6 +55,9 @@ struct fdtd_solver {
     std::vector<double> listeners;
     int L = 0;
     bool moving = false;
+    int boundary_handling = 0;              // FDTD_BOUNDARY_*
+    std::vector<void*> fc_alloc;            // device arrays of the FULLY_COUPLED rows
+    long long fc_immersed = 0, fc_fallback = 0;
     // device
     fdtd::SolveParams hP{};
     fdtd::SolveParams* dP = nullptr;
@@ -91,4 +94,6 @@ void set_error(fdtd_solver* s, const std::string& msg);
 fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc);
 void classification_boxes(const fdtd_solver* s, std::vector<std::array<int, 6>>& boxes);
 void to_dev_objects(fdtd_solver* s);
+fdtd_status build_fully_coupled(fdtd_solver* s);
+void free_fully_coupled(fdtd_solver* s);
 }  // namespace fdtd

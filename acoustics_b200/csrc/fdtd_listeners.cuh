@@ -10,6 +10,7 @@
 // minimiser for a full-rank stencil, as with the reference's JacobiSVD.
 #pragma once
 #include "fdtd_device.cuh"
+#include "fdtd_coupled.cuh"
 #include "fdtd_geometry.cuh"
 
 namespace fdtd {
@@ -37,8 +38,8 @@ __device__ __forceinline__ void kth_face(unsigned mask, int k, int& d, int& s) {
 }
 
 template <typename T>
-__device__ void build_row(const SolveParams& P, const T* __restrict__ pold, double t, const double pt[3], int cell,
-                          uint8_t code, double v, int k, double A[4], double& b) {
+__device__ void build_row(const SolveParams& P, const T* __restrict__ pold, double t, int par, const double pt[3],
+                          int cell, uint8_t code, double v, int k, double A[4], double& b) {
     int i, j, kk;
     cell_ijk(P, cell, i, j, kk);
     const double cp[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][kk]};
@@ -51,7 +52,8 @@ __device__ void build_row(const SolveParams& P, const T* __restrict__ pold, doub
     kth_face(mask, k, d, s);
     const long long strides[3] = {P.SX, P.SY, 1};
     const long long nbr = cell + s * strides[d];
-    const double pg = ghost_pressure(P, P.gobj[cell], cp, d, s, (double)pold[nbr], t);
+    const double pg = P.fc_rows ? fc_ghost(P, par, cell, 2 * d + (s > 0 ? 1 : 0), (double)pold[nbr])
+                                : ghost_pressure(P, P.gobj[cell], cp, d, s, (double)pold[nbr], t);
     double fp[3] = {cp[0], cp[1], cp[2]};
     fp[d] += (s > 0 ? 1.0 : -1.0) * 0.25 * P.h;
     mls_row(pt, fp, pg, A, b);
@@ -155,8 +157,8 @@ __device__ void listener_body(const SolveParams& P, int newp, int li, double* __
         const double vq = __shfl_sync(0xffffffffu, v, owner);
         const int codeq = __shfl_sync(0xffffffffu, (int)code, owner);
         const int cellqq = __shfl_sync(0xffffffffu, cellq, owner);
-        if (half == 0 && has0) build_row<T>(P, pold, t, pt, cellqq, (uint8_t)codeq, vq, r - first, A0, b0);
-        if (half == 1 && has1) build_row<T>(P, pold, t, pt, cellqq, (uint8_t)codeq, vq, r - first, A1, b1);
+        if (half == 0 && has0) build_row<T>(P, pold, t, newp ^ 1, pt, cellqq, (uint8_t)codeq, vq, r - first, A0, b0);
+        if (half == 1 && has1) build_row<T>(P, pold, t, newp ^ 1, pt, cellqq, (uint8_t)codeq, vq, r - first, A1, b1);
         if constexpr (PREP) {
             if ((half == 0 && has0) || (half == 1 && has1)) {
                 // row source: the cell value, or the ghost face it stands for
@@ -301,7 +303,9 @@ __device__ __forceinline__ void listener_plan(const SolveParams& P, int newp, in
             cell_ijk(P, row.cell, i, j, k);
             const double cp[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
             const long long strides[3] = {P.SX, P.SY, 1};
-            val = ghost_pressure(P, P.gobj[row.cell], cp, d, sgn, (double)pold[row.cell + sgn * strides[d]], t);
+            const double pn = (double)pold[row.cell + sgn * strides[d]];
+            val = P.fc_rows ? fc_ghost(P, newp ^ 1, row.cell, 2 * d + (sgn > 0 ? 1 : 0), pn)
+                            : ghost_pressure(P, P.gobj[row.cell], cp, d, sgn, pn, t);
         }
         acc += row.w * val;
     }

@@ -23,6 +23,7 @@
 // HBM requests in flight; z neighbours come from the warp with shuffles.
 #pragma once
 #include "fdtd_device.cuh"
+#include "fdtd_coupled.cuh"
 #include "fdtd_geometry.cuh"
 #include "fdtd_stencil.cuh"
 
@@ -33,7 +34,7 @@ namespace fdtd {
 // ghost cells on both sides.
 template <typename T>
 __device__ __noinline__ T ghost_laplacian(const SolveParams& P, long long c, const int idx[3], unsigned mask, T p0,
-                                          const T nbp[3], const T nbm[3], double t, int* surrounded) {
+                                          const T nbp[3], const T nbm[3], double t, int par, int* surrounded) {
     const long long strides[3] = {P.SX, P.SY, 1};
     T lap = 0.0;
     int s = 0;
@@ -43,13 +44,16 @@ __device__ __noinline__ T ghost_laplacian(const SolveParams& P, long long c, con
         T gpv = 0, gnv = 0;
         if (gp || gn) {
             double own[3] = {P.cpos[0][idx[0]], P.cpos[1][idx[1]], P.cpos[2][idx[2]]};
+            // FULLY_COUPLED: the solved ghost pressures of this step; RASTERIZE: pg
             if (gp) {
                 own[d] = P.cpos[d][idx[d] + 1];
-                gpv = (T)ghost_pressure(P, P.gobj[c + strides[d]], own, d, -1, (double)p0, t);
+                gpv = P.fc_rows ? (T)fc_ghost(P, par, c + strides[d], 2 * d, (double)p0)
+                                : (T)ghost_pressure(P, P.gobj[c + strides[d]], own, d, -1, (double)p0, t);
             }
             if (gn) {
                 own[d] = P.cpos[d][idx[d] - 1];
-                gnv = (T)ghost_pressure(P, P.gobj[c - strides[d]], own, d, +1, (double)p0, t);
+                gnv = P.fc_rows ? (T)fc_ghost(P, par, c - strides[d], 2 * d + 1, (double)p0)
+                                : (T)ghost_pressure(P, P.gobj[c - strides[d]], own, d, +1, (double)p0, t);
             }
         }
         if (gp && gn) {
@@ -88,7 +92,7 @@ __device__ __forceinline__ void ghost_cells_body(const SolveParams& P, int cur, 
         const T nbm[3] = {pc[c - sx], pc[c - sy], pc[c - 1]};
         const int idx[3] = {x, y, z};
         int surrounded = 0;
-        T lap = ghost_laplacian<T>(P, c, idx, code & CLS_MASK, p0, nbp, nbm, t, &surrounded);
+        T lap = ghost_laplacian<T>(P, c, idx, code & CLS_MASK, p0, nbp, nbm, t, cur, &surrounded);
         lap = lap * (T)P.lap_scale;
         const bool cavity = (surrounded > 1) && (code & CLS_VALID);
         if constexpr (sizeof(T) == 8) {

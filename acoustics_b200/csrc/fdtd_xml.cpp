@@ -196,9 +196,14 @@ fdtd_status fdtd_scene_from_xml(const char* path, fdtd_scene** out) {
     D.time_step = 1.0 / freq;
     if (!get_real(solver, "boundary_condition_preset", v, false, 0.0, err)) return (set_error(nullptr, err), FDTD_ERR_INVALID_ARG);
     D.boundary_condition_preset = (int32_t)v;
+    // ImpulseResponseParser.cpp:547-555
     auto bh = solver->attr.find("boundary_handling");
-    if (bh != solver->attr.end() && bh->second != "rasterize")
-        return (set_error(nullptr, "boundary_handling '" + bh->second + "' is not on this path (rasterize only)"), FDTD_ERR_UNSUPPORTED);
+    D.boundary_handling = FDTD_BOUNDARY_RASTERIZE;
+    if (bh != solver->attr.end()) {
+        if (bh->second == "fully_coupled") D.boundary_handling = FDTD_BOUNDARY_FULLY_COUPLED;
+        else if (bh->second != "rasterize")
+            return (set_error(nullptr, "boundary handling type not understood: " + bh->second), FDTD_ERR_INVALID_ARG);
+    }
     auto op = solver->attr.find("output_pattern");
     sc->output_pattern = op == solver->attr.end() ? std::string("%s") : op->second;
     // solver_control_policy, static (ImpulseResponseParser.cpp:615-627) + per-axis extension

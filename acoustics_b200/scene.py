@@ -24,6 +24,7 @@ MOTION_STATIC, MOTION_BALLISTIC = 0, 1
 PRECISION_FP64, PRECISION_FP32_COMPENSATED = 0, 1
 KERNEL_FUSED, KERNEL_PHASED = 0, 1
 PML_STATE_AUTO, PML_STATE_FULL = 0, 1
+BOUNDARY_RASTERIZE, BOUNDARY_FULLY_COUPLED = 0, 1
 
 CELL_BULK, CELL_GHOST, CELL_VALID_HISTORY, CELL_PML, CELL_CONSTRAINT = 1, 2, 4, 8, 16
 (FIELD_PRESSURE, FIELD_PRESSURE_PREV, FIELD_PML_PX, FIELD_PML_PY, FIELD_PML_PZ,
@@ -67,6 +68,7 @@ class SceneDesc(C.Structure):
         ("n_listeners", C.c_int32),
         ("objects", C.POINTER(ObjectDesc)), ("constraints", C.POINTER(PlaneDesc)),
         ("sources", C.POINTER(GaussianSourceDesc)), ("listeners", C.POINTER(C.c_double)),
+        ("boundary_handling", C.c_int32), ("_reserved_scene", C.c_int32),
     ]
 
 
@@ -163,6 +165,7 @@ class Scene:
     pml_strength: float = 1.0e6
     boundary_condition_preset: int = 0
     air_viscosity_alpha: float = 0.0
+    boundary_handling: int = 0  # BOUNDARY_RASTERIZE / BOUNDARY_FULLY_COUPLED
     start_time: float = 0.0
     end_time: float = 0.0
     objects: List[RigidObject] = field(default_factory=list)
@@ -210,6 +213,7 @@ class Scene:
         desc.cell_size = self.cell_size
         desc.divisions[:] = [int(x) for x in self.divisions]
         desc.boundary_condition_preset = self.boundary_condition_preset
+        desc.boundary_handling = int(self.boundary_handling)
         desc.domain_center[:] = [float(x) for x in self.domain_center]
         desc.sound_speed, desc.density, desc.time_step = self.sound_speed, self.density, self.time_step
         desc.pml_width, desc.pml_strength = self.pml_width, self.pml_strength

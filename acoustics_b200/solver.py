@@ -145,6 +145,12 @@ class PML_WaveSolver:
         check(self._L.fdtd_solver_get_field(self._h, int(which), out.ctypes.data, count), self._h)
         return out
 
+    def boundary_info(self) -> dict:
+        """FULLY_COUPLED rows (total, immersed, fallen back) and the last solve's iterations."""
+        a, b, c, d = C.c_int64(0), C.c_int64(0), C.c_int64(0), C.c_int32(0)
+        check(self._L.fdtd_solver_boundary_info(self._h, C.byref(a), C.byref(b), C.byref(c), C.byref(d)), self._h)
+        return {"rows": a.value, "immersed": b.value, "fallback": c.value, "iterations": d.value}
+
     def set_field(self, which: int, values) -> None:
         """The inverse of field(): a dense field (the reference's flat order) into the solve."""
         a = np.ascontiguousarray(values, dtype=np.float64).ravel()
@@ -190,7 +196,8 @@ def scene_from_xml(path: str) -> Scene:
                    domain_center=tuple(d.domain_center), sound_speed=d.sound_speed, density=d.density,
                    pml_width=d.pml_width, pml_strength=d.pml_strength,
                    boundary_condition_preset=d.boundary_condition_preset,
-                   air_viscosity_alpha=d.air_viscosity_alpha, start_time=d.start_time, end_time=d.end_time)
+                   air_viscosity_alpha=d.air_viscosity_alpha, start_time=d.start_time, end_time=d.end_time,
+                   boundary_handling=d.boundary_handling)
         for i in range(d.n_objects):
             o = d.objects[i]
             sc.objects.append(RigidObject(o.shape, tuple(o.center), tuple(o.size), tuple(o.rotation), o.accel_kind,

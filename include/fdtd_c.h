@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define FDTD_ABI_VERSION 1
+#define FDTD_ABI_VERSION 2
 
 typedef int32_t fdtd_status;
 enum {
@@ -111,7 +111,15 @@ typedef struct {
     const fdtd_plane_desc* constraints;
     const fdtd_gaussian_source_desc* sources;
     const double* listeners;       /* 3 * n_listeners, world coordinates                  */
+    int32_t boundary_handling;     /* FDTD_BOUNDARY_* (<solver boundary_handling=>)       */
+    int32_t _reserved_scene;       /* 0 */
 } fdtd_scene_desc;
+
+enum {
+    FDTD_BOUNDARY_RASTERIZE = 0,      /* ghost pressure from the neighbour and the wall acceleration */
+    FDTD_BOUNDARY_FULLY_COUPLED = 1   /* image-point interpolation, all ghost cells solved together
+                                         (static scenes, fused kernels, single solves) */
+};
 
 enum {
     FDTD_PRECISION_FP64 = 0,              /* bit-faithful FP64 path                       */
@@ -271,6 +279,12 @@ fdtd_status fdtd_solver_save_config(fdtd_solver* s, const char* output_pattern);
  * which = FDTD_FIELD_PRESSURE or FDTD_FIELD_V{X,Y,Z}, x-fastest (n x 1) matrix */
 fdtd_status fdtd_solver_save_field_timestep(fdtd_solver* s, int32_t which, const char* path);
 
+/* FULLY_COUPLED diagnostics (no counterpart in the reference; it prints the same
+ * figures every step, MAC_Grid.cpp:1413-1418): ghost-face rows, rows interpolated
+ * at the image point, rows that fell back to the rasterized value, and the
+ * BiCGSTAB iterations of the last step (negative: not converged). */
+fdtd_status fdtd_solver_boundary_info(fdtd_solver* s, int64_t* n_rows, int64_t* n_immersed, int64_t* n_fallback,
+                                      int32_t* last_iterations);
 /* PML state in effect: FDTD_PML_STATE_FULL, or FDTD_PML_STATE_AUTO when the
  * reduced state is used (no counterpart in the reference). */
 int32_t fdtd_solver_pml_state(fdtd_solver* s);

@@ -38,6 +38,7 @@ namespace {
 
 const double EPS = 1e-10;                       // src/config.h:45
 const double DISTANCE_TOLERANCE = 0.0;          // Wavesolver_ConstantsAndTypes.h:76
+const double CONDN_LIM = 25.0;                  // Wavesolver_ConstantsAndTypes.h:98
 const double GAUSSIAN_CHECK_BOUND = 2.0;        // Wavesolver_ConstantsAndTypes.h:77
 const double AABB_CHECK_TOLERANCE_SCALE = 1.1;  // Wavesolver_ConstantsAndTypes.h:78
 const double MLS_FLEISHMAN_RAD = 0.018;         // math/MLSConstantsAndTypes.h:9
@@ -170,8 +171,9 @@ struct Obj {
         }
         return a;
     }
-    // ReflectAgainstBoundary for a point outside the body (FDTD_RigidObject.cpp:429-536):
-    // boundary point bp, erected normal n = normalize(x - bp), image x + (x - bp).
+    // ReflectAgainstBoundary (FDTD_RigidObject.cpp:429-536), closest-point branch:
+    // outside, erected normal x - bp and image x + (x - bp); inside, normal bp - x
+    // and image bp + (bp - x) (the mirror point outside the body).
     void Reflect(const V3& x, V3& image, V3& bp, V3& nrm, double& dist) const {
         V3 r;
         for (int i = 0; i < 3; ++i) r[i] = x[i] - c[i];
@@ -179,18 +181,31 @@ struct Obj {
             const double n = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
             for (int i = 0; i < 3; ++i) bp[i] = c[i] + r[i] / n * d.size[0];
             dist = n - d.size[0];
-        } else {  // box (axis frame via rotation): clamp to the surface
+        } else {  // box (axis frame via rotation)
             V3 q, qc;
             for (int j = 0; j < 3; ++j)
                 q[j] = d.rotation[0 * 3 + j] * r[0] + d.rotation[1 * 3 + j] * r[1] + d.rotation[2 * 3 + j] * r[2];
-            for (int j = 0; j < 3; ++j) qc[j] = std::max(-d.size[j], std::min(d.size[j], q[j]));
+            dist = sdf_local(x);
+            if (dist >= 0.0) {  // outside: clamp onto the box
+                for (int j = 0; j < 3; ++j) qc[j] = std::max(-d.size[j], std::min(d.size[j], q[j]));
+            } else {  // inside: the nearest face
+                int best = 0;
+                double gap = d.size[0] - std::fabs(q[0]);
+                for (int j = 1; j < 3; ++j)
+                    if (d.size[j] - std::fabs(q[j]) < gap) {
+                        gap = d.size[j] - std::fabs(q[j]);
+                        best = j;
+                    }
+                qc = q;
+                qc[best] = q[best] < 0.0 ? -d.size[best] : d.size[best];
+            }
             for (int i = 0; i < 3; ++i)
                 bp[i] = c[i] + (d.rotation[i * 3 + 0] * qc[0] + d.rotation[i * 3 + 1] * qc[1] + d.rotation[i * 3 + 2] * qc[2]);
-            dist = sdf_local(x);
         }
         V3 e;
-        for (int i = 0; i < 3; ++i) e[i] = -bp[i] + x[i];
-        for (int i = 0; i < 3; ++i) image[i] = x[i] + e[i];
+        const bool inside = dist < 0.0;
+        for (int i = 0; i < 3; ++i) e[i] = inside ? bp[i] - x[i] : x[i] - bp[i];
+        for (int i = 0; i < 3; ++i) image[i] = inside ? bp[i] + e[i] : x[i] + e[i];
         const double en = std::sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
         for (int i = 0; i < 3; ++i) nrm[i] = en > 0.0 ? e[i] / en : 0.0;
     }
@@ -221,6 +236,8 @@ struct Oracle {
     double h, c, rho, k, alpha;
     double absorptionWidth, absorptionStrength;
     int preset;
+    bool fullyCoupled = false;  // boundaryHandlingType (ImpulseResponseParser.cpp:547-555)
+    int fcIterations = 0;       // BiCGSTAB iterations of the last FULLY_COUPLED solve
     double endTime;
     // pressure field (ScalarField, ScalarField.cpp:29-50)
     int N[3];
@@ -545,6 +562,270 @@ struct Oracle {
         }
     }
 
+    // ----- FULLY_COUPLED ghost cells (MAC_Grid.cpp:1131-1425, use_immerse_interface) -----
+    // Trilinear Vandermonde rows in the scaled coordinates of FillVandermonde*S
+    // (MAC_Grid.cpp:4444-4510).
+    static void vdmRegular(const V3& x, const V3& org, double h, double* row) {
+        double q[3];
+        for (int d = 0; d < 3; ++d) q[d] = (x[d] - org[d]) / h + 0.5;
+        row[0] = q[0] * q[1] * q[2];
+        row[1] = q[0] * q[1];
+        row[2] = q[0] * q[2];
+        row[3] = q[1] * q[2];
+        row[4] = q[0];
+        row[5] = q[1];
+        row[6] = q[2];
+        row[7] = 1.0;
+    }
+    static void vdmBoundary(const V3& x, const V3& n, const V3& org, double h, double* row) {
+        double q[3];
+        for (int d = 0; d < 3; ++d) q[d] = (x[d] - org[d]) / h + 0.5;
+        row[0] = n[0] * q[1] * q[2] + n[1] * q[0] * q[2] + n[2] * q[0] * q[1];
+        row[1] = n[0] * q[1] + n[1] * q[0];
+        row[2] = n[0] * q[2] + n[2] * q[0];
+        row[3] = n[1] * q[2] + n[2] * q[1];
+        row[4] = n[0];
+        row[5] = n[1];
+        row[6] = n[2];
+        row[7] = 0.0;
+    }
+    // Condition number of the 8 x 8 matrix M from the eigenvalues of M^T M (cyclic
+    // Jacobi), and the solution of M w = v (Gaussian elimination with partial
+    // pivoting; a singular M gets the minimum-norm least-squares solution from the
+    // same eigen-decomposition).
+    static double conditionAndSolve(const double M[8][8], const double v[8], double w[8]) {
+        double G[8][8], Q[8][8];
+        for (int i = 0; i < 8; ++i)
+            for (int j = 0; j < 8; ++j) {
+                double a = 0.0;
+                for (int k = 0; k < 8; ++k) a += M[k][i] * M[k][j];
+                G[i][j] = a;
+                Q[i][j] = (i == j) ? 1.0 : 0.0;
+            }
+        for (int sweep = 0; sweep < 100; ++sweep) {
+            double off = 0.0;
+            for (int i = 0; i < 8; ++i)
+                for (int j = i + 1; j < 8; ++j) off += G[i][j] * G[i][j];
+            if (off < 1e-300) break;
+            for (int p = 0; p < 8; ++p)
+                for (int q = p + 1; q < 8; ++q) {
+                    if (std::fabs(G[p][q]) < 1e-300) continue;
+                    const double th = (G[q][q] - G[p][p]) / (2.0 * G[p][q]);
+                    const double t = (th >= 0 ? 1.0 : -1.0) / (std::fabs(th) + std::sqrt(th * th + 1.0));
+                    const double c = 1.0 / std::sqrt(t * t + 1.0), sn = t * c;
+                    for (int k = 0; k < 8; ++k) {
+                        const double gp = G[k][p], gq = G[k][q];
+                        G[k][p] = c * gp - sn * gq;
+                        G[k][q] = sn * gp + c * gq;
+                    }
+                    for (int k = 0; k < 8; ++k) {
+                        const double gp = G[p][k], gq = G[q][k];
+                        G[p][k] = c * gp - sn * gq;
+                        G[q][k] = sn * gp + c * gq;
+                    }
+                    for (int k = 0; k < 8; ++k) {
+                        const double qp = Q[k][p], qq = Q[k][q];
+                        Q[k][p] = c * qp - sn * qq;
+                        Q[k][q] = sn * qp + c * qq;
+                    }
+                }
+        }
+        double lmax = 0.0, lmin = 1e300;
+        for (int i = 0; i < 8; ++i) {
+            lmax = std::max(lmax, G[i][i]);
+            lmin = std::min(lmin, G[i][i]);
+        }
+        const double smax = std::sqrt(std::max(lmax, 0.0)), smin = std::sqrt(std::max(lmin, 0.0));
+        const double thr = 8.0 * 2.220446049250313e-16 * smax;
+        if (smin > thr) {
+            double A[8][9];
+            for (int i = 0; i < 8; ++i) {
+                for (int j = 0; j < 8; ++j) A[i][j] = M[i][j];
+                A[i][8] = v[i];
+            }
+            for (int c = 0; c < 8; ++c) {
+                int piv = c;
+                for (int r = c + 1; r < 8; ++r)
+                    if (std::fabs(A[r][c]) > std::fabs(A[piv][c])) piv = r;
+                for (int j = 0; j < 9; ++j) std::swap(A[c][j], A[piv][j]);
+                for (int r = c + 1; r < 8; ++r) {
+                    const double f = A[r][c] / A[c][c];
+                    for (int j = c; j < 9; ++j) A[r][j] -= f * A[c][j];
+                }
+            }
+            for (int i = 7; i >= 0; --i) {
+                double a = A[i][8];
+                for (int j = i + 1; j < 8; ++j) a -= A[i][j] * w[j];
+                w[i] = a / A[i][i];
+            }
+        } else {
+            // w = Q diag(1/lambda) Q^T M^T v over the eigenvalues above the threshold
+            double mtv[8], y[8];
+            for (int i = 0; i < 8; ++i) {
+                double a = 0.0;
+                for (int k = 0; k < 8; ++k) a += M[k][i] * v[k];
+                mtv[i] = a;
+            }
+            for (int j = 0; j < 8; ++j) {
+                double a = 0.0;
+                for (int i = 0; i < 8; ++i) a += Q[i][j] * mtv[i];
+                y[j] = std::sqrt(std::max(G[j][j], 0.0)) > thr ? a / G[j][j] : 0.0;
+            }
+            for (int i = 0; i < 8; ++i) {
+                double a = 0.0;
+                for (int j = 0; j < 8; ++j) a += Q[i][j] * y[j];
+                w[i] = a;
+            }
+        }
+        return smin > 0.0 ? smax / smin : std::numeric_limits<double>::infinity();
+    }
+
+    void PML_pressureUpdateGhostCells_FullyCoupled(const std::vector<double>& p, double t) {
+        const int n = (int)ghosts.size();
+        if (n == 0) return;
+        std::vector<Key> keys;
+        keys.reserve(n);
+        for (auto& m : ghosts) keys.push_back(m.first);
+        std::map<Key, int> rowOf;
+        for (int i = 0; i < n; ++i) rowOf[keys[i]] = i;
+        std::vector<double> diag(n, 1.0), rhs(n, 0.0);
+        std::vector<std::vector<std::pair<int, double>>> off(n);
+        for (int r = 0; r < n; ++r) {
+            const GhostCell& gc = ghosts.at(keys[r]);
+            const double p_neig = p[gc.neighbour];
+            if (gc.type == 1) {  // plane constraint: perfectly reflecting
+                rhs[r] = p_neig;
+                continue;
+            }
+            const Obj& o = objs[gc.boundaryObject];
+            V3 image, bp, ne;
+            double dist = gc.distance;
+            o.Reflect(gc.position, image, bp, ne, dist);
+            const V3 a = o.accel(bp, t);
+            V3 g;
+            for (int d = 0; d < 3; ++d) g[d] = a[d] * (-rho);
+            V3 ncell;
+            ncell[std::abs(gc.topology) - 1] = gc.topology > 0 ? 1.0 : -1.0;
+            const double g_nr = g[0] * ncell[0] + g[1] * ncell[1] + g[2] * ncell[2];
+            const double g_ne = g[0] * ne[0] + g[1] * ne[1] + g[2] * ne[2];
+            const double pg = p_neig - 0.75 * h * g_nr;
+            const double fdw = o.DistanceToMesh(gc.position) < DISTANCE_TOLERANCE ? -2.0 * std::fabs(dist) : -std::fabs(dist);
+            double weighted = g_ne * fdw;
+            std::vector<int> nb;
+            enclosingNeighbours(image, nb);
+            if (nb.size() != 8) {
+                rhs[r] = pg;
+                continue;
+            }
+            V3 org;
+            for (int q = 0; q < 8; ++q) {
+                const V3 cp = cellPosition(nb[q]);
+                for (int d = 0; d < 3; ++d) org[d] += cp[d];
+            }
+            for (int d = 0; d < 3; ++d) org[d] /= 8.0;
+            double Vr[8][8], vrow[8], rv[8] = {0};
+            int si = -1;
+            std::set<int> known;
+            std::map<int, Key> unknown;
+            vdmRegular(image, org, h, vrow);
+            for (int q = 0; q < 8; ++q) {
+                const int ci = nb[q];
+                if (ci == gc.owner) {
+                    vdmBoundary(bp, ne, org, h, Vr[q]);
+                    rv[q] = g_ne * h;
+                    si = q;
+                } else if (!isGhost[ci]) {
+                    vdmRegular(cellPosition(ci), org, h, Vr[q]);
+                    rv[q] = p[ci];
+                    known.insert(q);
+                } else {
+                    double best = std::numeric_limits<double>::max();
+                    Key bestKey = 0;
+                    for (const Key kk : ghostTree.at(ci)) {
+                        const GhostCell& gn = ghosts.at(kk);
+                        double d2 = 0.0;
+                        for (int d = 0; d < 3; ++d) d2 += (gn.position[d] - image[d]) * (gn.position[d] - image[d]);
+                        if (d2 < best) {
+                            best = d2;
+                            bestKey = kk;
+                        }
+                    }
+                    vdmRegular(ghosts.at(bestKey).position, org, h, Vr[q]);
+                    unknown[q] = bestKey;
+                }
+            }
+            // V^T w = v^T
+            double M[8][8], w[8];
+            for (int i = 0; i < 8; ++i)
+                for (int j = 0; j < 8; ++j) M[i][j] = Vr[j][i];
+            const double cond = conditionAndSolve(M, vrow, w);
+            if (cond > CONDN_LIM && si != -1) {
+                for (int q = 0; q < 8; ++q) w[q] = rv[q] = 0.0;
+                known.clear();
+                unknown.clear();
+                weighted = pg;
+            }
+            diag[r] = -1.0;
+            double b = -weighted;
+            for (const int q : known) b -= w[q] * rv[q];
+            if (si != -1) b -= w[si] * rv[si];
+            for (const auto& m : unknown) off[r].push_back({rowOf.at(m.second), w[m.first]});
+            rhs[r] = b;
+        }
+        // BiCGSTAB with the diagonal preconditioner, tolerance eps relative to |b|
+        auto apply = [&](const std::vector<double>& x, std::vector<double>& y) {
+            for (int r = 0; r < n; ++r) {
+                double a = diag[r] * x[r];
+                for (const auto& e : off[r]) a += e.second * x[e.first];
+                y[r] = a;
+            }
+        };
+        auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) {
+            double s = 0.0;
+            for (int i = 0; i < n; ++i) s += a[i] * b[i];
+            return s;
+        };
+        std::vector<double> x(n, 0.0), rr = rhs, r0 = rhs, pv(n, 0.0), v(n, 0.0), y(n), sv(n), z(n), tv(n), ax(n);
+        const double eps = 2.220446049250313e-16;
+        const double rhs2 = dot(rhs, rhs);
+        int it = 0;
+        if (rhs2 > 0.0) {
+            const double tol2 = eps * eps * rhs2;
+            double r0sq = rhs2, rho = 1.0, alpha = 1.0, om = 1.0, res = rhs2;
+            int restarts = 0;
+            const int maxit = std::min(2 * n, 1000);
+            while (res > tol2 && it < maxit) {
+                const double rhoOld = rho;
+                rho = dot(r0, rr);
+                if (std::fabs(rho) < eps * eps * r0sq) {
+                    apply(x, ax);
+                    for (int i = 0; i < n; ++i) rr[i] = rhs[i] - ax[i];
+                    r0 = rr;
+                    rho = r0sq = dot(rr, rr);
+                    if (restarts++ == 0) it = 0;
+                }
+                const double beta = (rho / rhoOld) * (alpha / om);
+                for (int i = 0; i < n; ++i) pv[i] = rr[i] + beta * (pv[i] - om * v[i]);
+                for (int i = 0; i < n; ++i) y[i] = pv[i] / diag[i];
+                apply(y, v);
+                alpha = rho / dot(r0, v);
+                for (int i = 0; i < n; ++i) sv[i] = rr[i] - alpha * v[i];
+                for (int i = 0; i < n; ++i) z[i] = sv[i] / diag[i];
+                apply(z, tv);
+                const double tt = dot(tv, tv);
+                om = tt > 0.0 ? dot(tv, sv) / tt : 0.0;
+                for (int i = 0; i < n; ++i) {
+                    x[i] += alpha * y[i] + om * z[i];
+                    rr[i] = sv[i] - om * tv[i];
+                }
+                res = dot(rr, rr);
+                ++it;
+            }
+        }
+        fcIterations = it;
+        for (int r = 0; r < n; ++r) ghosts.at(keys[r]).pressure = x[r];
+    }
+
     // MAC_Grid::PML_velocityUpdateCollocated (MAC_Grid.cpp:461-479)
     void PML_velocityUpdateCollocated(const std::vector<double>& pFull) {
 #pragma omp parallel for schedule(static)
@@ -858,7 +1139,8 @@ struct Oracle {
         if (st != FDTD_OK) return st;
         st = InterpolateFreshPressureCell(pCurr, currentTime);
         if (st != FDTD_OK) return st;
-        PML_pressureUpdateGhostCells(pCurr, currentTime);
+        if (fullyCoupled) PML_pressureUpdateGhostCells_FullyCoupled(pCurr, currentTime);
+        else PML_pressureUpdateGhostCells(pCurr, currentTime);
         PML_velocityUpdateCollocated(pCurr);
         pressureFieldLaplacianGhostCell(pCurr, lapCurr);
         PML_pressureUpdateCollocated(currentTime, pLast, pCurr, pNext, lapCurr, lapLast);
@@ -886,6 +1168,7 @@ struct Oracle {
         k = s->time_step;
         alpha = s->air_viscosity_alpha;
         preset = s->boundary_condition_preset;
+        fullyCoupled = s->boundary_handling == FDTD_BOUNDARY_FULLY_COUPLED;
         endTime = s->end_time;
         if (preset != 0) { err = "boundary_condition_preset != 0 unsupported"; return FDTD_ERR_UNSUPPORTED; }
         if (s->pml_width < 1.5) { err = "PML width < 1.5 cells reaches the Engquist branch"; return FDTD_ERR_UNSUPPORTED; }

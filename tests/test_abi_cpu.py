@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol(fdtd_lib):
 
 
 def test_abi_version(fdtd_lib):
-    assert fdtd_lib.fdtd_abi_version() == 1
+    assert fdtd_lib.fdtd_abi_version() == 2
 
 
 def test_struct_layouts_match_header(tmp_path):
@@ -118,6 +118,10 @@ def test_xml_scene_reader(fdtd_lib, tmp_path):
     assert src.width_space == 343.0 * 2e-4                      # parser default c * sigma_t
     assert src.normalize_constant == -1.0 / (np.sqrt(2.0 * np.pi) * src.width_space) ** 3  # sign flip
     assert np.array_equal(sc.listeners, [[0.01, 0.02, 0.03], [-0.01, 0.0, 0.0]])
+    assert sc.boundary_handling == S.BOUNDARY_RASTERIZE
+    # ImpulseResponseParser.cpp:547-555
+    p.write_text(SCENE_XML.replace('<solver ', '<solver boundary_handling="fully_coupled" ', 1))
+    assert scene_from_xml(str(p)).boundary_handling == S.BOUNDARY_FULLY_COUPLED
 
 
 @pytest.mark.parametrize("bad,status", [
@@ -127,6 +131,7 @@ def test_xml_scene_reader(fdtd_lib, tmp_path):
     (SCENE_XML.replace("analytic_sphere", "rigid_sound_object", 1).replace(
         "radius=\"0.04\"", "", 1), -7),
     (SCENE_XML.replace('type="static"', 'type="dynamic"'), -7),
+    (SCENE_XML.replace('<solver ', '<solver boundary_handling="voxelized" ', 1), -1),
 ])
 def test_xml_errors(fdtd_lib, tmp_path, bad, status):
     p = tmp_path / "bad.xml"
