@@ -389,8 +389,8 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
         return (set_error(nullptr, "boundary_condition_preset other than 0 (Engquist walls) is not on this path"), FDTD_ERR_UNSUPPORTED);
     if (sc->pml_width < 1.5)
         return (set_error(nullptr, "PML width below 1.5 cells reaches the Engquist-Majda branch (MAC_Grid.cpp:533-920)"), FDTD_ERR_UNSUPPORTED);
-    if (sc->air_viscosity_alpha != 0.0)
-        return (set_error(nullptr, "air viscosity (alpha > 0) is not on this path"), FDTD_ERR_UNSUPPORTED);
+    if (!(sc->air_viscosity_alpha >= 0.0))
+        return (set_error(nullptr, "air_viscosity_alpha must be non-negative"), FDTD_ERR_INVALID_ARG);
     if (sc->n_objects < 0 || sc->n_objects > FDTD_MAX_OBJECTS)
         return (set_error(nullptr, "too many objects (max " + std::to_string(FDTD_MAX_OBJECTS) + ")"), FDTD_ERR_INVALID_ARG);
     if (sc->n_sources < 0 || sc->n_sources > FDTD_MAX_SOURCES)
@@ -472,6 +472,10 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
         if (o.kernel != FDTD_KERNEL_PHASED) cv.add(&P.v[1][d], n * w);  // double-buffered faces
     }
     if (o.kernel == FDTD_KERNEL_PHASED) cv.add((void**)&s->d_lap, n * 8);
+    if (sc->air_viscosity_alpha > 0.0) {  // Laplacians of this and the previous step
+        cv.add(&P.lapv[0], n * w);
+        cv.add(&P.lapv[1], n * w);
+    }
     // spatial factors of the sources over their region (one table per source)
     s->region.src_region = source_region(s);
     {
@@ -666,6 +670,8 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     P.c = s->c;
     P.k = s->k;
     P.c2k2 = (s->c * s->k) * (s->c * s->k);
+    P.kcalp = s->c * sc->air_viscosity_alpha * s->k;  // MAC_Grid.cpp:486
+    P.visc = sc->air_viscosity_alpha > 0.0 ? 1 : 0;
     P.lap_scale = 1.0 / (s->h * s->h);
     P.q = 0.75 * s->h;
     P.quarter_h = 0.25 * s->h;
@@ -794,6 +800,8 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     CUDA_TRY(s, cudaMemsetAsync(P.p[0], 0, np * w, s->stream));
     CUDA_TRY(s, cudaMemsetAsync(P.p[1], 0, np * w, s->stream));
     if (P.dinc) CUDA_TRY(s, cudaMemsetAsync(P.dinc, 0, np * 4, s->stream));
+    for (int b = 0; b < 2; ++b)
+        if (P.lapv[b]) CUDA_TRY(s, cudaMemsetAsync(P.lapv[b], 0, np * w, s->stream));
     for (int d = 0; d < 3; ++d) {
         CUDA_TRY(s, cudaMemsetAsync(P.pd[d], 0, np * w, s->stream));
         CUDA_TRY(s, cudaMemsetAsync(P.v[0][d], 0, np * w, s->stream));

@@ -327,6 +327,8 @@ fdtd_status fdtd_batch_add(fdtd_batch* b, const fdtd_scene_desc* scene, int32_t 
     if (!b || !scene || steps < 0) return batch_fail(b, FDTD_ERR_INVALID_ARG, "fdtd_batch_add: invalid arguments");
     if (scene && scene->boundary_handling != FDTD_BOUNDARY_RASTERIZE)
         return batch_fail(b, FDTD_ERR_UNSUPPORTED, "batched members use RASTERIZE boundaries");
+    if (scene && scene->air_viscosity_alpha != 0.0)
+        return batch_fail(b, FDTD_ERR_UNSUPPORTED, "batched members have no air viscosity");
     fdtd_options o = b->opt;
     o.graph_steps = 0;
     fdtd_solver* s = nullptr;

@@ -169,6 +169,9 @@ struct KArgs {
     const uint8_t* axflag[3];     // AXF_* per index, [N_d + 8] (zero past N_d)
     const AxisCoef<T>* coef[3];   // [N_d + 8]
     T inv_h, c2k2, lap_scale;
+    T kcalp;                      // air viscosity c alpha k
+    const T* lapl;                // Laplacian of the previous step (viscosity)
+    T* lapc;                      // Laplacian of this step (viscosity)
     SolveParams* P;               // device copy (for the step-constant advance)
     int cur;
     int advance;                  // the shell kernel advances consts[cur^1]
@@ -205,6 +208,9 @@ struct SolveParams {
     double h, inv_h, rho, c, k;
     double c2k2;          // (c k)^2
     double lap_scale;     // 1/(h*h)
+    double kcalp;         // c alpha k (air viscosity, MAC_Grid.cpp:926-930); 0 without
+    int visc;             // alpha > 0: lapv holds the Laplacians of two steps
+    void* lapv[2];        // T[np] each: the Laplacian of the step of that parity
     double q;             // 0.75*h  (ghost extrapolation distance, MAC_Grid.cpp:1281)
     double quarter_h;     // 0.25*h
     double bmin[3];
@@ -312,6 +318,9 @@ inline KArgs<double> make_kargs<double>(SolveParams* dP, const SolveParams& P, i
         A.coef[d] = P.coef_d[d];
     }
     A.inv_h = P.inv_h; A.c2k2 = P.c2k2; A.lap_scale = P.lap_scale;
+    A.kcalp = P.kcalp;
+    A.lapc = (double*)P.lapv[cur];
+    A.lapl = (const double*)P.lapv[cur ^ 1];
     return A;
 }
 
@@ -339,6 +348,9 @@ inline KArgs<float> make_kargs<float>(SolveParams* dP, const SolveParams& P, int
         A.coef[d] = P.coef_f[d];
     }
     A.inv_h = (float)P.inv_h; A.c2k2 = (float)P.c2k2; A.lap_scale = (float)P.lap_scale;
+    A.kcalp = (float)P.kcalp;
+    A.lapc = (float*)P.lapv[cur];
+    A.lapl = (const float*)P.lapv[cur ^ 1];
     return A;
 }
 

@@ -305,6 +305,8 @@ __global__ void k_phase_pressure(const SolveParams* __restrict__ Pp, int cur, co
             if (((mask >> (2 * dd)) & 3u) == 3u) ++surrounded;
         double pnext;
         if (surrounded > 1 && (code & CLS_VALID)) pnext = pc[c];
+        else if (P.visc && (code & CLS_VALID))  // air viscosity (MAC_Grid.cpp:926-930)
+            pnext = 2.0 * pc[c] - pn[c] - ((const double*)P.lapv[cur ^ 1])[c] * P.kcalp + lap[c] * (P.c2k2 + P.kcalp);
         else pnext = 2.0 * pc[c] - pn[c] + lap[c] * P.c2k2;
         if (P.n_src > 0) {
             double src = 0.0;

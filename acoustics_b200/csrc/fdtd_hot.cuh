@@ -74,7 +74,7 @@ __device__ __forceinline__ void stv(T* p, const Vec<T, V>& v) {
 // shuffle when that lane holds the neighbouring group of the same row, else
 // from memory.  Cells of a group outside the box or not plain bulk are masked
 // (scalar stores for partial groups).  Every thread of the CTA must call it.
-template <typename T, int XB>
+template <typename T, int XB, bool VISC = false>
 __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box, int tu, int tx) {
     constexpr bool COMP = sizeof(T) == 4;
     constexpr int V = 16 / (int)sizeof(T);
@@ -105,7 +105,7 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
     const bool zm_mem = (lane == 0) || (g == 0);
     const bool zp_mem = (lane == 31) || (g == ng - 1);
 
-    VT pcol[XB + 2], ym[XB], yp[XB], prev[XB];
+    VT pcol[XB + 2], ym[XB], yp[XB], prev[XB], lapl[XB];
     uint32_t code[XB];
     T zme[XB], zpe[XB];
     pcol[0] = ldv(pc - sx);
@@ -126,6 +126,7 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
             }
             if constexpr (V == 4) code[i] = *reinterpret_cast<const uint32_t*>(cls + i * sx);
             else code[i] = *reinterpret_cast<const uint16_t*>(cls + i * sx);
+            if constexpr (VISC) lapl[i] = ldv(A.lapl + off + i * sx);
             zme[i] = zm_mem ? pc[i * sx - 1] : (T)0;
             zpe[i] = zp_mem ? pc[i * sx + V] : (T)0;
         }
@@ -138,7 +139,7 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
         const T right = __shfl_down_sync(0xffffffffu, c0.e[0], 1);
         const T zm_edge = zm_mem ? zme[i] : left;
         const T zp_edge = zp_mem ? zpe[i] : right;
-        VT outp, outd;
+        VT outp, outd, outl;
         unsigned act = 0;
 #pragma unroll
         for (int e = 0; e < V; ++e) {
@@ -155,31 +156,38 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
             lap = lap + (yp[i].e[e] + ym[i].e[e] - (T)2.0 * p0);
             lap = lap + (zp + zm - (T)2.0 * p0);
             lap = lap * A.lap_scale;
+            // air viscosity on cells with a valid history (MAC_Grid.cpp:926-930)
+            const bool visc = VISC && (cb & CLS_VALID);
             if constexpr (!COMP) {
-                outp.e[e] = (T)2.0 * p0 - prev[i].e[e] + lap * A.c2k2;
+                if (visc) outp.e[e] = (T)2.0 * p0 - prev[i].e[e] - lapl[i].e[e] * A.kcalp + lap * (A.c2k2 + A.kcalp);
+                else outp.e[e] = (T)2.0 * p0 - prev[i].e[e] + lap * A.c2k2;
             } else {
-                const float d = fmaf(lap, A.c2k2, prev[i].e[e]);
+                float d = fmaf(lap, A.c2k2, prev[i].e[e]);
+                if (visc) d = fmaf(A.kcalp, lap - lapl[i].e[e], d);
                 outd.e[e] = d;
                 outp.e[e] = p0 + d;
             }
+            outl.e[e] = lap;
         }
         if (act == (1u << V) - 1u) {
             stv(pn + i * sx, outp);
             if constexpr (COMP) stv(dinc + i * sx, outd);
+            if constexpr (VISC) stv(A.lapc + off + i * sx, outl);
         } else if (act) {
 #pragma unroll
             for (int e = 0; e < V; ++e)
                 if ((act >> e) & 1u) {
                     pn[i * sx + e] = outp.e[e];
                     if constexpr (COMP) dinc[i * sx + e] = outd.e[e];
+                    if constexpr (VISC) A.lapc[off + i * sx + e] = outl.e[e];
                 }
         }
     }
 }
 
-template <typename T, int XB>
+template <typename T, int XB, bool VISC = false>
 __global__ void __launch_bounds__(256) k_interior(const KArgs<T> A, Box3 box) {
-    interior_tile<T, XB>(A, box, blockIdx.x, blockIdx.y);
+    interior_tile<T, XB, VISC>(A, box, blockIdx.x, blockIdx.y);
 }
 
 // Masked store of a z vector: one vector store when every cell is selected,
@@ -496,9 +504,10 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     if (gside && (e = cudaEventRecord(S.ghost, S.s3)) != cudaSuccess) return e;
     if (has_interior) {
         dim3 block(32, 8);
-        const int xb = (R.xb == 4 || R.xb == 8) ? R.xb : 2;
+        const int xb = (!hP.visc && (R.xb == 4 || R.xb == 8)) ? R.xb : 2;
         dim3 grid(interior_unit_tiles(b, 16 / (int)sizeof(T)), (nx + xb - 1) / xb);
-        if (xb == 2) k_interior<T, 2><<<grid, block, 0, si>>>(A, b);
+        if (hP.visc) k_interior<T, 2, true><<<grid, block, 0, si>>>(A, b);
+        else if (xb == 2) k_interior<T, 2><<<grid, block, 0, si>>>(A, b);
         else if (xb == 8) k_interior<T, 8><<<grid, block, 0, si>>>(A, b);
         else k_interior<T, 4><<<grid, block, 0, si>>>(A, b);
         ++l;

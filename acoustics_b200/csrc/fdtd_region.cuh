@@ -95,10 +95,20 @@ __device__ __forceinline__ void ghost_cells_body(const SolveParams& P, int cur, 
         T lap = ghost_laplacian<T>(P, c, idx, code & CLS_MASK, p0, nbp, nbm, t, cur, &surrounded);
         lap = lap * (T)P.lap_scale;
         const bool cavity = (surrounded > 1) && (code & CLS_VALID);
+        // air viscosity on cells with a valid history (MAC_Grid.cpp:926-930)
+        const bool visc = P.visc && (code & CLS_VALID);
+        T lapl = 0;
+        if (P.visc) {
+            lapl = ((const T*)P.lapv[cur ^ 1])[c];
+            ((T*)P.lapv[cur])[c] = lap;
+        }
         if constexpr (sizeof(T) == 8) {
-            pn[c] = cavity ? p0 : (T)2.0 * p0 - pn[c] + lap * (T)P.c2k2;
+            if (cavity) pn[c] = p0;
+            else if (visc) pn[c] = (T)2.0 * p0 - pn[c] - lapl * (T)P.kcalp + lap * (T)(P.c2k2 + P.kcalp);
+            else pn[c] = (T)2.0 * p0 - pn[c] + lap * (T)P.c2k2;
         } else {
-            const float d = cavity ? 0.0f : P.dinc[c] + (float)(lap * (T)P.c2k2);
+            float d = cavity ? 0.0f : P.dinc[c] + (float)(lap * (T)P.c2k2);
+            if (!cavity && visc) d = fmaf((float)P.kcalp, (float)(lap - lapl), d);
             P.dinc[c] = d;
             pn[c] = p0 + d;
         }

@@ -65,6 +65,12 @@ bool sources_active_window(const fdtd_solver* s, double t, int n) {
     return false;
 }
 
+// The Laplacian array of the phased path: with air viscosity the one of the
+// step's parity (the previous step's stays for the update), else the single one.
+double* phased_lap(const fdtd_solver* s, int cur) {
+    return s->hP.visc ? (double*)s->hP.lapv[cur] : s->d_lap;
+}
+
 StepStreams step_streams(const fdtd_solver* s) {
     return StepStreams{s->stream, s->stream2, s->stream3, s->ev_fork, s->ev_join, s->ev_ghost};
 }
@@ -116,7 +122,7 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         }
         int l = 0;
         if (s->opt.kernel == FDTD_KERNEL_PHASED) {
-            CUDA_TRY(s, launch_phased_fp64(s->dP, s->N, cur, s->d_lap, s->stream, &l));
+            CUDA_TRY(s, launch_phased_fp64(s->dP, s->N, cur, phased_lap(s, cur), s->stream, &l));
         } else {
             CUDA_TRY(s, launch_step_regions_fp64(s->dP, s->hP, s->region, cur, step_streams(s), &l));
         }
@@ -342,7 +348,7 @@ fdtd_status fdtd_solver_time_kernel(fdtd_solver* s, int32_t which, int32_t n_lau
         if (which == 4) {
             e = launch_listeners(s->dP, s->precision, c, s->L, s->d_lis, s->stream);
         } else if (s->precision == FDTD_PRECISION_FP64) {
-            if (s->opt.kernel == FDTD_KERNEL_PHASED) e = launch_phased_fp64(s->dP, s->N, c, s->d_lap, s->stream, nullptr);
+            if (s->opt.kernel == FDTD_KERNEL_PHASED) e = launch_phased_fp64(s->dP, s->N, c, phased_lap(s, c), s->stream, nullptr);
             else e = launch_step_regions_fp64(s->dP, s->hP, R, c, step_streams(s), nullptr);
         } else {
             e = launch_step_regions_fp32(s->dP, s->hP, R, c, step_streams(s), nullptr);
@@ -636,6 +642,8 @@ std::vector<std::pair<void*, size_t>> snap_regions(fdtd_solver* s) {
             r.push_back({P.zv[0][d], (size_t)P.zcount * w});
             r.push_back({P.zv[1][d], (size_t)P.zcount * w});
         }
+    for (int b = 0; b < 2; ++b)
+        if (P.lapv[b]) r.push_back({P.lapv[b], np * (s->precision == FDTD_PRECISION_FP64 ? 8 : 4)});
     r.push_back({P.consts, 2 * sizeof(StepConsts)});
     r.push_back({P.dev_error, sizeof(int)});
     return r;

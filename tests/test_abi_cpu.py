@@ -166,7 +166,10 @@ def test_invalid_scenes_are_rejected_before_device_use(fdtd_lib):
     bad = []
     sc = S.config1(); sc.pml_width = 1.0; bad.append((sc, -7))
     sc = S.config1(); sc.boundary_condition_preset = 1; bad.append((sc, -7))
-    sc = S.config1(); sc.air_viscosity_alpha = 0.1; bad.append((sc, -7))
+    sc = S.config1(); sc.air_viscosity_alpha = -0.1; bad.append((sc, -1))
+    sc = S.config1(); sc.boundary_handling = 7; bad.append((sc, -1))
+    sc = S.config1(); sc.boundary_handling = S.BOUNDARY_FULLY_COUPLED
+    sc.objects.append(S.RigidObject(S.SHAPE_ELLIPSOID, (0.05, 0, 0), (0.01, 0.01, 0.01))); bad.append((sc, -7))
     sc = S.config1(); sc.cell_size = -1.0; bad.append((sc, -1))
     sc = S.config1(); sc.objects = [S.RigidObject(S.SHAPE_SPHERE, (0, 0, 0), (0.01, 0, 0))] * 9; bad.append((sc, -1))
     for sc, status in bad:

@@ -163,3 +163,28 @@ def test_fp32_fractional_pml_width(oracle_lib, fdtd_lib, pml_width):
     yo = oracle_lib.OracleSolver(sc).step(150)
     yg = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED).step(150)
     assert rel_l2(yg, yo) <= TOL_FP32
+
+
+@pytest.mark.parametrize("kernel,precision,tol", [(S.KERNEL_FUSED, S.PRECISION_FP64, TOL_FP64),
+                                                  (S.KERNEL_PHASED, S.PRECISION_FP64, TOL_FP64),
+                                                  (S.KERNEL_FUSED, S.PRECISION_FP32_COMPENSATED, TOL_FP32)])
+def test_air_viscosity(oracle_lib, fdtd_lib, kernel, precision, tol):
+    """alpha > 0: the update of a cell with a valid history adds
+    c alpha k (lap^n - lap^{n-1}) (MAC_Grid.cpp:926-930)."""
+    sc = S.config1(divisions=(40, 36, 44), pml_width=6, radius=0.02)
+    sc.air_viscosity_alpha = 2e-5
+    yo = oracle_lib.OracleSolver(sc).step(200)
+    yg = PML_WaveSolver(sc, precision=precision, kernel=kernel).step(200)
+    assert rel_l2(yg, yo) <= tol
+    sc.air_viscosity_alpha = 0.0
+    y0 = oracle_lib.OracleSolver(sc).step(200)
+    assert rel_l2(yo, y0) > 1e-4  # the term is visible
+
+
+def test_air_viscosity_moving_bodies(oracle_lib, fdtd_lib):
+    sc = moving_scene(steps=80)
+    sc.air_viscosity_alpha = 2e-5
+    o = oracle_lib.OracleSolver(sc)
+    g = PML_WaveSolver(sc)
+    yo, yg = o.step(80), g.step(80)
+    assert rel_l2(yg, yo) <= TOL_FP64
