@@ -148,8 +148,35 @@ static void iteration_box(const fdtd_solver* s, double mn[3], double mx[3], int 
 }
 
 // The object and constraint boxes that classifyCells_FAST iterates (MAC_Grid.cpp:3510-3551)
-void classification_boxes(const fdtd_solver* s, std::vector<std::array<int, 6>>& boxes) {
-    boxes.clear();
+void classification_boxes(const fdtd_solver* s, ClsBoxes& B) {
+    B.n = 0;
+    B.first[0] = 0;
+    B.ufirst[0] = 0;
+    auto push = [&](const int st[3], const int rg[3]) {
+        for (int d = 0; d < 3; ++d) {
+            B.lo[B.n][d] = st[d];
+            B.rg[B.n][d] = rg[d];
+        }
+        const bool empty = rg[0] <= 0 || rg[1] <= 0 || rg[2] <= 0;
+        B.first[B.n + 1] = B.first[B.n] + (empty ? 0 : (long long)rg[0] * rg[1] * rg[2]);
+        // units reached: rows lo-1 .. lo+rg (clipped), chunks holding cells lo2-1 .. lo2+rg2
+        long long units = 0;
+        if (!empty) {
+            for (int d = 0; d < 2; ++d) {
+                const int a = std::max(0, st[d] - 1), b = std::min(s->N[d] - 1, st[d] + rg[d]);
+                B.u0[B.n][d] = a;
+                B.un[B.n][d] = std::max(0, b - a + 1);
+            }
+            const int ka = std::max(0, st[2] - 1), kb = std::min(s->N[2] - 1, st[2] + rg[2]);
+            B.u0[B.n][2] = ka / CLS_CHUNK;
+            B.un[B.n][2] = kb >= ka ? kb / CLS_CHUNK - ka / CLS_CHUNK + 1 : 0;
+            units = (long long)B.un[B.n][0] * B.un[B.n][1] * B.un[B.n][2];
+        } else {
+            for (int d = 0; d < 3; ++d) B.u0[B.n][d] = B.un[B.n][d] = 0;
+        }
+        B.ufirst[B.n + 1] = B.ufirst[B.n] + units;
+        ++B.n;
+    };
     for (const auto& o : s->objs) {
         double mn[3] = {o.umin[0], o.umin[1], o.umin[2]}, mx[3] = {o.umax[0], o.umax[1], o.umax[2]};
         for (const auto& pl : s->planes) {
@@ -158,7 +185,7 @@ void classification_boxes(const fdtd_solver* s, std::vector<std::array<int, 6>>&
         }
         int st[3], rg[3];
         iteration_box(s, mn, mx, st, rg);
-        boxes.push_back({st[0], st[1], st[2], rg[0], rg[1], rg[2]});
+        push(st, rg);
     }
     for (const auto& pl : s->planes) {
         const double NEG_INF = std::numeric_limits<double>::lowest(), POS_INF = std::numeric_limits<double>::max();
@@ -167,7 +194,7 @@ void classification_boxes(const fdtd_solver* s, std::vector<std::array<int, 6>>&
         else mn[pl.normal_dir] = pl.height;
         int st[3], rg[3];
         iteration_box(s, mn, mx, st, rg);
-        boxes.push_back({st[0], st[1], st[2], rg[0], rg[1], rg[2]});
+        push(st, rg);
     }
 }
 
@@ -195,17 +222,12 @@ fdtd_status upload_params(fdtd_solver* s) {
 }
 
 fdtd_status run_classification(fdtd_solver* s) {
-    std::vector<std::array<int, 6>> boxes;
-    classification_boxes(s, boxes);
-    CUDA_TRY(s, launch_cls_reset(s->dP, s->ncell, s->stream));
-    s->launches++;
-    for (const auto& b : boxes) {
-        const int st[3] = {b[0], b[1], b[2]}, rg[3] = {b[3], b[4], b[5]};
-        CUDA_TRY(s, launch_cls_solid(s->dP, st, rg, s->stream));
-        s->launches++;
-    }
-    CUDA_TRY(s, launch_cls_ghost(s->dP, s->ncell, s->stream));
-    s->launches++;
+    ClsBoxes& B = s->hP.boxes;
+    classification_boxes(s, B);
+    CUDA_TRY(s, cudaMemcpyAsync(&s->dP->boxes, &B, sizeof(ClsBoxes), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, launch_classify(s->dP, s->N, B, false, s->stream));
+    s->cls_boxes_current = true;
+    s->launches += B.ufirst[B.n] > 0 ? 3 : 2;
     return FDTD_OK;
 }
 
@@ -541,6 +563,9 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
         s->region.ghost_cap = (int)std::min<double>(cells, (double)n);
         cv.add((void**)&s->d_ghost_list, (size_t)s->region.ghost_cap * 4);
         cv.add((void**)&s->d_ghost_count, 16);
+        // fresh cells were solid the step before: fewer than the solid cells of the boxes
+        P.fresh_cap = s->moving ? s->region.ghost_cap : 0;
+        cv.add((void**)&P.fresh_list, (size_t)std::max(1, P.fresh_cap) * 4);
     }
 }
 
@@ -598,7 +623,17 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     s->precision = o.precision;
     s->boundary_handling = sc->boundary_handling;
     CUDA_TRY(nullptr, cudaSetDevice(o.device));
-    CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    bool any_moving = false;
+    for (int i = 0; i < sc->n_objects; ++i) any_moving = any_moving || sc->objects[i].motion != FDTD_MOTION_STATIC;
+    if (any_moving) {
+        // moving bodies: the classification on the solver stream goes before the
+        // blocks of the PML shell that runs beside it on stream5
+        int least = 0, greatest = 0;
+        CUDA_TRY(nullptr, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        CUDA_TRY(nullptr, cudaStreamCreateWithPriority(&s->stream, cudaStreamNonBlocking, greatest));
+    } else {
+        CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+    }
     CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
     CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream3, cudaStreamNonBlocking));
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_ghost, cudaEventDisableTiming));
@@ -607,6 +642,9 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_lis[0], cudaEventDisableTiming));
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_lis[1], cudaEventDisableTiming));
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_lis_join, cudaEventDisableTiming));
+    CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream5, cudaStreamNonBlocking));
+    CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_sfork, cudaEventDisableTiming));
+    CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_sdone, cudaEventDisableTiming));
     if (s->precision == FDTD_PRECISION_FP32_COMPENSATED) CUDA_TRY(nullptr, prepare_fp32_kernels());
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
@@ -617,6 +655,7 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         cudaStreamDestroy(s->stream2);
         cudaStreamDestroy(s->stream3);
         cudaStreamDestroy(s->stream4);
+        cudaStreamDestroy(s->stream5);
         return FDTD_ERR_UNSUPPORTED;
     }
     for (int i = 0; i < sc->n_objects; ++i) {
@@ -683,6 +722,7 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     P.ghost_list = s->d_ghost_list;
     P.ghost_count = s->d_ghost_count;
     P.ghost_cap = s->region.ghost_cap;
+    P.fresh_count = s->d_ghost_count + 1;
     s->region.interior = s->interior;
     s->region.shell = s->shell;
     s->region.sources = 0;
@@ -776,13 +816,15 @@ fdtd_status fdtd_solver_destroy(fdtd_solver* s) {
     cudaStreamSynchronize(s->stream2);
     if (s->stream3) cudaStreamSynchronize(s->stream3);
     if (s->stream4) cudaStreamSynchronize(s->stream4);
+    if (s->stream5) cudaStreamSynchronize(s->stream5);
     cudaEventDestroy(s->ev_fork);
     cudaEventDestroy(s->ev_join);
-    for (cudaEvent_t ev : {s->ev_ghost, s->ev_step, s->ev_lis[0], s->ev_lis[1], s->ev_lis_join})
+    for (cudaEvent_t ev : {s->ev_ghost, s->ev_step, s->ev_lis[0], s->ev_lis[1], s->ev_lis_join, s->ev_sfork, s->ev_sdone})
         if (ev) cudaEventDestroy(ev);
     cudaStreamDestroy(s->stream2);
     if (s->stream3) cudaStreamDestroy(s->stream3);
     if (s->stream4) cudaStreamDestroy(s->stream4);
+    if (s->stream5) cudaStreamDestroy(s->stream5);
     cudaStreamDestroy(s->stream);
     delete s;
     return FDTD_OK;

@@ -198,6 +198,26 @@ struct StepConsts {
     int64_t step;
 };
 
+// Iteration boxes of one classification (MAC_Grid::classifyCells_FAST,
+// MAC_Grid.cpp:3608-3653): one per object, clipped by the constraints, and
+// one per constraint; a cell outside all of them is bulk.  first[b] is the
+// number of cells of the boxes before b.  The classification sweep works on
+// units of 256 cells of a z row (row (i, j), chunk ch); the units a box
+// reaches (a cell of the unit or a neighbour of one in the box) are rows
+// u0[b][0] + [0, un[b][0]) x u0[b][1] + [0, un[b][1]), chunks u0[b][2] + [0,
+// un[b][2]), and ufirst[b] counts those of the boxes before b.
+constexpr int CLS_MAX_BOXES = FDTD_MAX_OBJECTS + 4;
+constexpr int CLS_CHUNK = 256;
+struct ClsBoxes {
+    int n;
+    int lo[CLS_MAX_BOXES][3];
+    int rg[CLS_MAX_BOXES][3];
+    long long first[CLS_MAX_BOXES + 1];
+    int u0[CLS_MAX_BOXES][3];
+    int un[CLS_MAX_BOXES][3];
+    long long ufirst[CLS_MAX_BOXES + 1];
+};
+
 struct SolveParams {
     int N[3];
     int vN[3][3];         // velocity grid divisions per face orientation
@@ -258,6 +278,10 @@ struct SolveParams {
     int* ghost_list;              // non-PML bulk cells with a solid neighbour
     int* ghost_count;
     int ghost_cap;
+    ClsBoxes boxes;               // iteration boxes of the latest classification
+    int* fresh_list;              // bulk cells without a valid history (found by the classification sweep)
+    int* fresh_count;             // may exceed fresh_cap: the fresh-cell kernel then sweeps every cell
+    int fresh_cap;
     int precision;                // 0 fp64, 1 fp32 compensated
     // FULLY_COUPLED ghost cells (static scenes; null under RASTERIZE)
     const FcRow* fc_rows;         // [fc_n] one row per ghost face, owners ascending, directions ascending

@@ -17,35 +17,82 @@ namespace fdtd {
 // Cell classification (MAC_Grid::classifyCells_FAST, MAC_Grid.cpp:3455-3891)
 // ---------------------------------------------------------------------------
 
-// validHistory <- isBulk; isBulk <- true (MAC_Grid.cpp:3464-3472)
-__global__ void k_cls_reset(const SolveParams* __restrict__ Pp, long long n) {
-    const SolveParams& P = *Pp;
-    uint8_t* cls = P.cls;
-    if (blockIdx.x == 0 && threadIdx.x == 0) *P.ghost_count = 0;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        dense_ijk(P, t, i, j, k);
-        const long long c = cidx(P, i, j, k);
-        const uint8_t code = cls[c];
-        cls[c] = CLS_BULK | ((code & CLS_BULK) ? CLS_VALID : 0);
-    }
+// A classification is two launches.  k_cls_boxes visits the cells of the
+// iteration boxes (each cell once) and makes their new bulk / valid bits, the
+// solid test of MAC_Grid.cpp:3608-3653 with the zeroing of solid pressures
+// (MAC_Grid.cpp:3796-3798).  k_cls_sweep then visits every cell as "quads":
+// four cells of one z row, read and written as one 32-bit word (rows start at
+// multiples of 8 bytes, and a quad never reaches past its row's padding), one
+// quad per thread.  A cell outside every box is bulk with
+// validHistory <- isBulk (MAC_Grid.cpp:3464-3472); only quads within one cell
+// of a box look further (neighbour masks, closest objects, lists).
+struct ClsQuad {
+    int i, j, k0, nk;
+    long long c0;
+};
+
+// bytes of a quad word that are cells (the rest is row padding, left as it was)
+__device__ __forceinline__ uint32_t quad_cells(int nk) { return nk >= 4 ? 0xFFFFFFFFu : (1u << (8 * nk)) - 1u; }
+
+constexpr uint32_t QUAD_BULK = 0x01010101u * CLS_BULK;
+constexpr uint32_t QUAD_VALID = 0x01010101u * CLS_VALID;
+
+__device__ __forceinline__ bool in_box(const ClsBoxes& B, int b, int i, int j, int k) {
+    return i >= B.lo[b][0] && i < B.lo[b][0] + B.rg[b][0] && j >= B.lo[b][1] && j < B.lo[b][1] + B.rg[b][1] &&
+           k >= B.lo[b][2] && k < B.lo[b][2] + B.rg[b][2];
 }
 
-// Solid test over one object / constraint iteration box (MAC_Grid.cpp:3608-3653)
-// and zeroing of the pressure buffers at solid cells (MAC_Grid.cpp:3796-3798).
-__global__ void k_cls_solid(const SolveParams* __restrict__ Pp, int s0, int s1, int s2, int r0, int r1, int r2) {
+// 0xFF at the bytes of cells k0 .. k0+3 of row (i, j) that lie in some box
+__device__ uint32_t box_bytes(const ClsBoxes& B, int i, int j, int k0) {
+    uint32_t m = 0;
+    for (int b = 0; b < B.n; ++b) {
+        if (i < B.lo[b][0] || i >= B.lo[b][0] + B.rg[b][0] || j < B.lo[b][1] || j >= B.lo[b][1] + B.rg[b][1]) continue;
+        const int lo = max(k0, B.lo[b][2]) - k0, hi = min(k0 + 4, B.lo[b][2] + B.rg[b][2]) - k0;
+        if (hi > lo) m |= (hi >= 4 ? 0xFFFFFFFFu : (1u << (8 * hi)) - 1u) & ~((1u << (8 * lo)) - 1u);
+    }
+    return m;
+}
+
+// some box reaches a cell of the quad or one of its six neighbours
+__device__ __forceinline__ bool quad_near(const ClsBoxes& B, const ClsQuad& q) {
+    for (int b = 0; b < B.n; ++b) {
+        if (B.rg[b][0] <= 0 || B.rg[b][1] <= 0 || B.rg[b][2] <= 0) continue;
+        if (q.i + 1 >= B.lo[b][0] && q.i - 1 < B.lo[b][0] + B.rg[b][0] && q.j + 1 >= B.lo[b][1] &&
+            q.j - 1 < B.lo[b][1] + B.rg[b][1] && q.k0 + q.nk >= B.lo[b][2] && q.k0 - 1 < B.lo[b][2] + B.rg[b][2])
+            return true;
+    }
+    return false;
+}
+
+// Solid test of the box cells, each cell once (in its first box).  Also
+// empties the ghost-neighbour and fresh-cell lists the sweep fills.
+__global__ void __launch_bounds__(128) k_cls_boxes(const SolveParams* __restrict__ Pp) {
     const SolveParams& P = *Pp;
-    const long long total = (long long)r0 * r1 * r2;
+    const ClsBoxes& B = P.boxes;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        *P.ghost_count = 0;
+        *P.fresh_count = 0;
+    }
+    const long long total = B.first[B.n];
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < total;
          t += (long long)gridDim.x * blockDim.x) {
-        const int i = s0 + (int)(t / ((long long)r1 * r2));
-        const int j = s1 + (int)((t / r2) % r1);
-        const int k = s2 + (int)(t % r2);
+        int b = 0;
+        while (t >= B.first[b + 1]) ++b;
+        const long long r = t - B.first[b];
+        const int r1 = B.rg[b][1], r2 = B.rg[b][2];
+        const int i = B.lo[b][0] + (int)(r / ((long long)r1 * r2));
+        const int j = B.lo[b][1] + (int)((r / r2) % r1);
+        const int k = B.lo[b][2] + (int)(r % r2);
+        bool dup = false;
+        for (int e = 0; e < b; ++e) dup = dup || in_box(B, e, i, j, k);
+        if (dup) continue;
         const long long c = cidx(P, i, j, k);
         const double pos[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
         int type = 0;
-        if (!is_fluid(P, pos, type)) {
-            P.cls[c] = P.cls[c] & (uint8_t)~CLS_BULK;
+        const bool fluid = is_fluid(P, pos, type);
+        const uint8_t old = P.cls[c];
+        P.cls[c] = (uint8_t)((fluid ? CLS_BULK : 0) | ((old & CLS_BULK) ? CLS_VALID : 0) | (old & CLS_MASK));
+        if (!fluid) {
             P.gobj[c] = type ? GOBJ_CONSTRAINT : 0;
             if (P.precision == 0) {
                 ((double*)P.p[0])[c] = 0.0;
@@ -59,41 +106,229 @@ __global__ void k_cls_solid(const SolveParams* __restrict__ Pp, int s0, int s1, 
     }
 }
 
-// Neighbour masks: for a solid cell the directions of its bulk neighbours (one
-// ghost face each, MakeGhostCell MAC_Grid.cpp:4310-4340) and its closest
-// object (LowestObjectDistance, MAC_Grid.cpp:3810-3814); for a bulk cell the
-// directions of its solid (ghost) neighbours, read by the Laplacian.
-__global__ void k_cls_ghost(const SolveParams* __restrict__ Pp, long long n) {
-    const SolveParams& P = *Pp;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        dense_ijk(P, t, i, j, k);
-        const long long c = cidx(P, i, j, k);
-        const int idx[3] = {i, j, k};
-        const long long strides[3] = {P.SX, P.SY, 1};
-        const uint8_t code = P.cls[c];
-        const bool bulk = code & CLS_BULK;
-        unsigned mask = 0;
-        for (int d = 0; d < 3; ++d) {
-            if (idx[d] > 0) {
-                const bool nb = P.cls[c - strides[d]] & CLS_BULK;
-                if (bulk != nb) mask |= 1u << (2 * d);
-            }
-            if (idx[d] + 1 < P.N[d]) {
-                const bool nb = P.cls[c + strides[d]] & CLS_BULK;
-                if (bulk != nb) mask |= 1u << (2 * d + 1);
-            }
-        }
-        if (!bulk) {
-            const double pos[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
+// The cells of a quad that need more than their mask: solid cells (closest
+// object), non-PML bulk cells with a solid neighbour (ghost-neighbour list) and
+// fresh cells (fresh-cell list); `sel` has the bulk bit set at those bytes,
+// `code` the quad's new bulk / valid bits.
+__device__ __noinline__ void cls_cells(const SolveParams& P, const ClsQuad q, uint32_t sel, uint32_t code,
+                                       uint32_t listed, uint32_t fresh) {
+    while (sel) {
+        const int m = (__ffs(sel) - 1) >> 3;
+        sel &= ~(0xFFu << (8 * m));
+        const int k = q.k0 + m;
+        const long long c = q.c0 + m;
+        if (!((code >> (8 * m)) & CLS_BULK)) {
+            const double pos[3] = {P.cpos[0][q.i], P.cpos[1][q.j], P.cpos[2][k]};
             const int o = lowest_object(P, pos);
             P.gobj[c] = (P.gobj[c] & GOBJ_CONSTRAINT) | (uint8_t)(o < 0 ? GOBJ_NONE : o);
-        } else if (mask && !(P.pml_cell[0][i] || P.pml_cell[1][j] || P.pml_cell[2][k])) {
+            continue;
+        }
+        if (((listed >> (8 * m)) & CLS_BULK) && !(P.pml_cell[0][q.i] || P.pml_cell[1][q.j] || P.pml_cell[2][k])) {
             // non-PML bulk cell next to a solid: updated by k_ghost_cells
             const int slot = atomicAdd(P.ghost_count, 1);
             if (slot < P.ghost_cap) P.ghost_list[slot] = (int)c;
         }
-        P.cls[c] = (uint8_t)((code & (CLS_BULK | CLS_VALID)) | mask);
+        if ((fresh >> (8 * m)) & CLS_BULK) {
+            const int slot = atomicAdd(P.fresh_count, 1);
+            if (slot < P.fresh_cap) P.fresh_list[slot] = (int)c;
+        }
+    }
+}
+
+// New bulk bits of the quad of row (i, j) at k0: from memory in the boxes
+// (written by k_cls_boxes and not changed by the sweep), bulk elsewhere.
+__device__ __forceinline__ uint32_t quad_bulk(const SolveParams& P, const ClsBoxes& B, int i, int j, int k0) {
+    const uint32_t m = box_bytes(B, i, j, k0);
+    const uint32_t w = m ? *(const uint32_t*)(P.cls + (long long)i * P.SX + (long long)j * P.SY + k0) : 0u;
+    return (w & m & QUAD_BULK) | (QUAD_BULK & ~m);
+}
+
+// Quads within one cell of a box.  Neighbour masks: for a solid cell the
+// directions of its bulk neighbours (one ghost face each, MakeGhostCell
+// MAC_Grid.cpp:4310-4340) and its closest object (LowestObjectDistance,
+// MAC_Grid.cpp:3810-3814); for a bulk cell the directions of its solid (ghost)
+// neighbours, read by the Laplacian.  Mask bit 2d + (s > 0) is set where the
+// neighbour in direction s along axis d exists and differs in bulk-ness; the
+// four cells are compared at once, byte by byte of the words.
+__device__ __noinline__ void cls_sweep_near(const SolveParams& P, const ClsQuad q, uint32_t own, int collect_fresh) {
+    const ClsBoxes& B = P.boxes;
+    const uint32_t cells = quad_cells(q.nk);
+    const uint32_t inb = box_bytes(B, q.i, q.j, q.k0);
+    const uint32_t reset = QUAD_BULK | ((own & QUAD_BULK) >> 1);  // CLS_VALID is CLS_BULK >> 1
+    const uint32_t base = (own & inb & (QUAD_BULK | QUAD_VALID)) | (reset & ~inb);
+    // a missing neighbour reads as the cell itself (no difference, no face)
+    const uint32_t xm = q.i > 0 ? quad_bulk(P, B, q.i - 1, q.j, q.k0) : base;
+    const uint32_t xp = q.i + 1 < P.N[0] ? quad_bulk(P, B, q.i + 1, q.j, q.k0) : base;
+    const uint32_t ym = q.j > 0 ? quad_bulk(P, B, q.i, q.j - 1, q.k0) : base;
+    const uint32_t yp = q.j + 1 < P.N[1] ? quad_bulk(P, B, q.i, q.j + 1, q.k0) : base;
+    uint32_t zlo = base & 0xFFu, zhi = base >> 24;
+    if (q.k0 > 0) {
+        bool in = false;
+        for (int b = 0; b < B.n; ++b) in = in || in_box(B, b, q.i, q.j, q.k0 - 1);
+        zlo = in ? (P.cls[q.c0 - 1] & CLS_BULK) : CLS_BULK;
+    }
+    if (q.k0 + 4 < P.N[2]) {
+        bool in = false;
+        for (int b = 0; b < B.n; ++b) in = in || in_box(B, b, q.i, q.j, q.k0 + 4);
+        zhi = in ? (P.cls[q.c0 + 4] & CLS_BULK) : CLS_BULK;
+    }
+    const uint32_t zm = (base << 8) | zlo;
+    const uint32_t zp = (base >> 8) | (zhi << 24);
+    uint32_t mask = (((base ^ xm) & QUAD_BULK) >> 7) | (((base ^ xp) & QUAD_BULK) >> 6) |
+                    (((base ^ ym) & QUAD_BULK) >> 5) | (((base ^ yp) & QUAD_BULK) >> 4) |
+                    (((base ^ zm) & QUAD_BULK) >> 3) | (((base ^ zp) & QUAD_BULK) >> 2);
+    // a quad that ends inside its word: the last cell's +z neighbour is padding
+    if (q.nk < 4) mask &= ~(0x20u << (8 * (q.nk - 1)));
+    const uint32_t bulk = base & QUAD_BULK & cells;
+    const uint32_t solid = ~base & QUAD_BULK & cells;
+    // bulk cells with a nonzero mask (a 6-bit byte plus 0x3F carries into bit 6)
+    const uint32_t listed = bulk & (((mask + 0x3F3F3F3Fu) & 0x40404040u) << 1);
+    const uint32_t fresh = collect_fresh ? bulk & ~((base & QUAD_VALID) << 1) : 0u;
+    const uint32_t sel = solid | listed | fresh;
+    if (sel) cls_cells(P, q, sel, base, listed, fresh);
+    const uint32_t out = ((base | mask) & cells) | (own & ~cells);
+    if (out != own) *(uint32_t*)(P.cls + q.c0) = out;
+}
+
+// One quad of the sweep with its word `own`.
+__device__ __forceinline__ void cls_sweep_quad(const SolveParams& P, const ClsQuad& q, uint32_t own, int collect_fresh) {
+    if (quad_near(P.boxes, q)) {
+        cls_sweep_near(P, q, own, collect_fresh);
+        return;
+    }
+    // no solid cell within one cell: bulk, history from the last step, no mask
+    const uint32_t cells = quad_cells(q.nk);
+    const uint32_t out = ((QUAD_BULK | ((own & QUAD_BULK) >> 1)) & cells) | (own & ~cells);
+    if (out != own) {
+        *(uint32_t*)(P.cls + q.c0) = out;
+        const uint32_t fresh = collect_fresh ? ~own & QUAD_BULK & cells : 0u;
+        if (fresh) cls_cells(P, q, fresh, out, 0u, fresh);
+    }
+}
+
+// The two quads of a lane in a unit that some box reaches.
+__device__ __noinline__ void cls_sweep_lane_near(const SolveParams& P, int i, int j, int k0, uint2 w, int collect_fresh) {
+    ClsQuad q;
+    q.i = i;
+    q.j = j;
+    q.k0 = k0;
+    q.nk = min(4, P.N[2] - k0);
+    q.c0 = (long long)i * P.SX + (long long)j * P.SY + k0;
+    cls_sweep_quad(P, q, w.x, collect_fresh);
+    if (k0 + 4 >= P.N[2]) return;
+    q.k0 = k0 + 4;
+    q.nk = min(4, P.N[2] - k0 - 4);
+    q.c0 += 4;
+    cls_sweep_quad(P, q, w.y, collect_fresh);
+}
+
+// Box b reaches unit (i, j, ch): a cell of it, or a neighbour of one, is in the box.
+__device__ __forceinline__ bool unit_in(const ClsBoxes& B, int b, int i, int j, int ch) {
+    return i >= B.u0[b][0] && i < B.u0[b][0] + B.un[b][0] && j >= B.u0[b][1] && j < B.u0[b][1] + B.un[b][1] &&
+           ch >= B.u0[b][2] && ch < B.u0[b][2] + B.un[b][2];
+}
+
+// Units no box reaches: bulk cells with the history of the last step and no
+// mask; the cells that were solid the step before are fresh.  A warp takes
+// CLS_UNITS consecutive units (256 cells of a z row each) and loads all of them
+// first, 8 bytes a lane (rows start at multiples of 8 bytes and a lane's 8 bytes
+// stay inside its row's padding).  Units some box reaches are left to k_cls_near.
+constexpr int CLS_UNITS = 8;
+
+__global__ void __launch_bounds__(256) k_cls_sweep(const SolveParams* __restrict__ Pp, int nunits, int chunks,
+                                                   int collect_fresh) {
+    const SolveParams& P = *Pp;
+    const ClsBoxes& B = P.boxes;
+    const int lane = threadIdx.x & 31;
+    const int first = ((blockIdx.x * blockDim.x + threadIdx.x) >> 5) * CLS_UNITS;
+    if (first >= nunits) return;  // whole warps
+    const int N1 = P.N[1], N2 = P.N[2];
+    const long long SX = P.SX, SY = P.SY;
+    // lane r < CLS_UNITS tests unit first + r against the boxes
+    bool lane_near = false;
+    if (lane < CLS_UNITS && first + lane < nunits) {
+        const int u = first + lane;
+        const int row = u / chunks;
+        const int i = row / N1, j = row - (row / N1) * N1;
+        for (int b = 0; b < B.n && !lane_near; ++b) lane_near = unit_in(B, b, i, j, u - row * chunks);
+    }
+    const unsigned near_units = __ballot_sync(0xffffffffu, lane_near);
+    // the warp's first unit; later ones step through chunks, then rows
+    const int row0 = first / chunks;
+    const int i0 = row0 / N1, j0 = row0 - i0 * N1, ch0 = first - row0 * chunks;
+    const int nu = min(CLS_UNITS, nunits - first);
+    uint2 d[CLS_UNITS];
+    {
+        int i = i0, j = j0, ch = ch0;
+#pragma unroll
+        for (int r = 0; r < CLS_UNITS; ++r) {
+            d[r] = make_uint2(0u, 0u);
+            const int k0 = ch * CLS_CHUNK + lane * 8;
+            if (r < nu && !((near_units >> r) & 1u) && k0 < N2)
+                d[r] = *(const uint2*)(P.cls + i * SX + j * SY + k0);
+            if (++ch == chunks) {
+                ch = 0;
+                if (++j == N1) {
+                    j = 0;
+                    ++i;
+                }
+            }
+        }
+    }
+    const unsigned long long bulk8 = 0x0101010101010101ull * CLS_BULK;
+    int i = i0, j = j0, ch = ch0;
+#pragma unroll
+    for (int r = 0; r < CLS_UNITS; ++r) {
+        const int k0 = ch * CLS_CHUNK + lane * 8;
+        const int ci = i, cj = j;
+        if (++ch == chunks) {
+            ch = 0;
+            if (++j == N1) {
+                j = 0;
+                ++i;
+            }
+        }
+        if (r >= nu || ((near_units >> r) & 1u) || k0 >= N2) continue;
+        const unsigned long long w = ((unsigned long long)d[r].y << 32) | d[r].x;
+        const int nk = min(8, N2 - k0);
+        const unsigned long long cells = nk >= 8 ? ~0ull : (1ull << (8 * nk)) - 1ull;
+        const unsigned long long out = ((bulk8 | ((w & bulk8) >> 1)) & cells) | (w & ~cells);
+        if (out == w) continue;
+        const long long c = ci * SX + cj * SY + k0;
+        *(uint2*)(P.cls + c) = make_uint2((uint32_t)out, (uint32_t)(out >> 32));
+        unsigned long long fresh = collect_fresh ? ~w & bulk8 & cells : 0ull;
+        while (fresh) {
+            const int m = (__ffsll((long long)fresh) - 1) >> 3;
+            fresh &= ~(0xFFull << (8 * m));
+            const int slot = atomicAdd(P.fresh_count, 1);
+            if (slot < P.fresh_cap) P.fresh_list[slot] = (int)(c + m);
+        }
+    }
+}
+
+// Units some box reaches, one warp each, every unit once (in the first box
+// that reaches it); a lane takes two quads.
+__global__ void __launch_bounds__(256) k_cls_near(const SolveParams* __restrict__ Pp, int collect_fresh) {
+    const SolveParams& P = *Pp;
+    const ClsBoxes& B = P.boxes;
+    const int lane = threadIdx.x & 31;
+    const long long total = B.ufirst[B.n];
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    for (long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; t < total; t += nwarps) {
+        int b = 0;
+        while (t >= B.ufirst[b + 1]) ++b;
+        const long long r = t - B.ufirst[b];
+        const int nj = B.un[b][1], nc = B.un[b][2];
+        const int i = B.u0[b][0] + (int)(r / ((long long)nj * nc));
+        const int j = B.u0[b][1] + (int)((r / nc) % nj);
+        const int ch = B.u0[b][2] + (int)(r % nc);
+        bool dup = false;
+        for (int e = 0; e < b && !dup; ++e) dup = unit_in(B, e, i, j, ch);
+        if (dup) continue;
+        const int k0 = ch * CLS_CHUNK + lane * 8;
+        if (k0 >= P.N[2]) continue;
+        const uint2 w = *(const uint2*)(P.cls + (long long)i * P.SX + (long long)j * P.SY + k0);
+        cls_sweep_lane_near(P, i, j, k0, w, collect_fresh);
     }
 }
 
@@ -104,9 +339,11 @@ __global__ void k_cls_ghost(const SolveParams* __restrict__ Pp, long long n) {
 // MAC_Grid.cpp:1993-2254): a cell that is bulk now but was solid before gets
 // p = p_MLS(image point) + rho (a . n) |s| in p^{n-1} and p^n.
 // ---------------------------------------------------------------------------
+// Out of line: the few fresh cells of a step run this once per launch, and one
+// copy of the code misses the instruction cache less than several inlined ones.
 template <typename T>
-__device__ double fresh_value(const SolveParams& P, const T* __restrict__ pa, const T* __restrict__ pb, bool diff,
-                              long long c, double t, int* status) {
+__device__ __noinline__ double fresh_value(const SolveParams& P, const T* __restrict__ pa, const T* __restrict__ pb,
+                                           bool diff, long long c, double t, int* status) {
     // value of buffer "a" (or a - b when diff) at cell n
     auto val = [&](long long n) -> double { return diff ? (double)pa[n] - (double)pb[n] : (double)pa[n]; };
     int i, j, k;
@@ -123,31 +360,41 @@ __device__ double fresh_value(const SolveParams& P, const T* __restrict__ pa, co
     reflect_against_boundary(o, cp, image, bp, nrm, travelled);
     int cells[8];
     const int nc = enclosing_neighbours(P, image, cells);
+    // the flags, values and positions of the stencil cells, loaded together
+    // (one round trip to memory instead of one per cell)
+    uint8_t code[8];
+    double vals[8], npos[8][3];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        if (q >= nc) break;
+        const int n = cells[q];
+        int ni, nj, nn;
+        cell_ijk(P, n, ni, nj, nn);
+        code[q] = P.cls[n];
+        vals[q] = val(n);
+        npos[q][0] = P.cpos[0][ni];
+        npos[q][1] = P.cpos[1][nj];
+        npos[q][2] = P.cpos[2][nn];
+    }
     double A[8 * 4], b[8];
     int kept[8];
     int nk = 0;
     for (int q = 0; q < nc; ++q) {
-        const int n = cells[q];
-        if (!(P.cls[n] & CLS_VALID)) continue;
-        int ni, nj, nn;
-        cell_ijk(P, n, ni, nj, nn);
-        const double np_[3] = {P.cpos[0][ni], P.cpos[1][nj], P.cpos[2][nn]};
-        mls_row(image, np_, val(n), &A[nk * 4], b[nk]);
-        kept[nk++] = n;
+        if (!(code[q] & CLS_VALID)) continue;
+        mls_row(image, npos[q], vals[q], &A[nk * 4], b[nk]);
+        kept[nk++] = q;
     }
     if (nk < 4) {
         if (nk != 0) {
             double md = DBL_MAX;
             int mid = -1;
-            for (int q = 0; q < nk; ++q) {
-                const int n = kept[q];
-                int ni, nj, nn;
-                cell_ijk(P, n, ni, nj, nn);
-                const double dx = image[0] - P.cpos[0][ni], dy = image[1] - P.cpos[1][nj], dz = image[2] - P.cpos[2][nn];
+            for (int e = 0; e < nk; ++e) {
+                const int q = kept[e];
+                const double dx = image[0] - npos[q][0], dy = image[1] - npos[q][1], dz = image[2] - npos[q][2];
                 const double d2 = dx * dx + dy * dy + dz * dz;
-                if (d2 < md) { md = d2; mid = n; }
+                if (d2 < md) { md = d2; mid = q; }
             }
-            return val(mid);
+            return vals[mid];
         }
         const int idx[3] = {i, j, k};
         const long long strides[3] = {P.SX, P.SY, 1};
@@ -168,33 +415,76 @@ __device__ double fresh_value(const SolveParams& P, const T* __restrict__ pa, co
 }
 
 template <typename T>
+__device__ __forceinline__ void fresh_cell(const SolveParams& P, int cur, long long c, double t, int* st) {
+    if (sizeof(T) == 8) {
+        double* pl = (double*)P.p[cur ^ 1];
+        double* pc = (double*)P.p[cur];
+        const double vl = fresh_value<double>(P, pl, pl, false, c, t, st);
+        const double vc = fresh_value<double>(P, pc, pc, false, c, t, st);
+        pl[c] = vl;
+        pc[c] = vc;
+    } else {
+        // FP32 keeps p^n and the increment; p^{n-1} = p^n - d
+        float* pc = (float*)P.p[cur];
+        const double vc = fresh_value<float>(P, pc, pc, false, c, t, st);
+        const double vl = fresh_value<float>(P, pc, P.dinc, true, c, t, st);
+        pc[c] = (float)vc;
+        P.dinc[c] = (float)(vc - vl);
+    }
+}
+
+// Fresh cells of the classification just made, from the list the ghost sweep
+// filled; a list that overflowed is replaced by a sweep over every cell.  Each
+// fresh value reads only cells with a valid history, never another fresh cell,
+// so the order does not matter.  On the list, the two values of a cell (p^n
+// and p^{n-1}) are made by a pair of lanes: unit 2 f + w, w = 0 for p^n.
+template <typename T>
 __global__ void k_fresh_cells(const SolveParams* __restrict__ Pp, int cur, long long n, int* status) {
     const SolveParams& P = *Pp;
     const double t = P.consts[cur].t;
-    for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
-        int i, j, k;
-        dense_ijk(P, q, i, j, k);
-        const long long c = cidx(P, i, j, k);
-        const uint8_t code = P.cls[c];
-        if (!(code & CLS_BULK) || (code & CLS_VALID)) continue;
-        int st = 0;
-        if (sizeof(T) == 8) {
-            double* pl = (double*)P.p[cur ^ 1];
-            double* pc = (double*)P.p[cur];
-            const double vl = fresh_value<double>(P, pl, pl, false, c, t, &st);
-            const double vc = fresh_value<double>(P, pc, pc, false, c, t, &st);
-            pl[c] = vl;
-            pc[c] = vc;
-        } else {
-            // FP32 keeps p^n and the increment; p^{n-1} = p^n - d
-            float* pc = (float*)P.p[cur];
-            const double vc = fresh_value<float>(P, pc, pc, false, c, t, &st);
-            const double vl = fresh_value<float>(P, pc, P.dinc, true, c, t, &st);
-            pc[c] = (float)vc;
-            P.dinc[c] = (float)(vc - vl);
+    const int count = *P.fresh_count;
+    int st = 0;
+    if (count <= P.fresh_cap) {
+        const int units = 2 * count;
+        const int lane = threadIdx.x & 31;
+        // whole warps step together, so the pair exchange below sees both lanes
+        for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < units; base += gridDim.x * blockDim.x) {
+            const int u = base + lane;
+            const bool act = u < units;
+            const int w = u & 1;
+            const long long c = act ? P.fresh_list[u >> 1] : 0;
+            double v = 0.0;
+            if (act) {
+                if (sizeof(T) == 8) {
+                    const double* buf = (const double*)P.p[cur ^ w];
+                    v = fresh_value<double>(P, buf, buf, false, c, t, &st);
+                } else {
+                    const float* pc = (const float*)P.p[cur];
+                    v = w ? fresh_value<float>(P, pc, P.dinc, true, c, t, &st)
+                          : fresh_value<float>(P, pc, pc, false, c, t, &st);
+                }
+            }
+            const double other = __shfl_xor_sync(0xffffffffu, v, 1);
+            if (!act) continue;
+            if (sizeof(T) == 8) {
+                ((double*)P.p[cur ^ w])[c] = v;
+            } else if (w == 0) {
+                // FP32 keeps p^n and the increment; p^{n-1} = p^n - d
+                ((float*)P.p[cur])[c] = (float)v;
+                P.dinc[c] = (float)(v - other);
+            }
         }
-        if (st) atomicMax(status, st);
+    } else {
+        for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+            int i, j, k;
+            dense_ijk(P, q, i, j, k);
+            const long long c = cidx(P, i, j, k);
+            const uint8_t code = P.cls[c];
+            if (!(code & CLS_BULK) || (code & CLS_VALID)) continue;
+            fresh_cell<T>(P, cur, c, t, &st);
+        }
     }
+    if (st) atomicMax(status, st);
 }
 
 // ---------------------------------------------------------------------------
@@ -393,15 +683,14 @@ cudaError_t launch_listener_prep(SolveParams* dP, int precision, int newp, int n
     return cudaGetLastError();
 }
 
-cudaError_t launch_cls_reset(const SolveParams* dP, long long ncell, cudaStream_t s) {
-    k_cls_reset<<<grid_for(ncell, 256), 256, 0, s>>>(dP, ncell);
-    return cudaGetLastError();
-}
-
-cudaError_t launch_cls_solid(const SolveParams* dP, const int start[3], const int range[3], cudaStream_t s) {
-    const long long total = (long long)range[0] * range[1] * range[2];
-    if (total <= 0) return cudaSuccess;
-    k_cls_solid<<<grid_for(total, 128), 128, 0, s>>>(dP, start[0], start[1], start[2], range[0], range[1], range[2]);
+cudaError_t launch_classify(const SolveParams* dP, const int N[3], const ClsBoxes& B, bool collect_fresh,
+                            cudaStream_t s) {
+    k_cls_boxes<<<grid_for(B.first[B.n], 128), 128, 0, s>>>(dP);
+    const int chunks = (N[2] + CLS_CHUNK - 1) / CLS_CHUNK;
+    const int nunits = N[0] * N[1] * chunks;
+    const int warps = (nunits + CLS_UNITS - 1) / CLS_UNITS;
+    k_cls_sweep<<<(warps + 7) / 8, 256, 0, s>>>(dP, nunits, chunks, collect_fresh ? 1 : 0);
+    if (B.ufirst[B.n] > 0) k_cls_near<<<grid_for((B.ufirst[B.n] + 7) / 8, 1), 256, 0, s>>>(dP, collect_fresh ? 1 : 0);
     return cudaGetLastError();
 }
 
@@ -429,15 +718,12 @@ cudaError_t launch_cls_history(const SolveParams* dP, long long ncell, int* coun
     return cudaGetLastError();
 }
 
-cudaError_t launch_cls_ghost(const SolveParams* dP, long long ncell, cudaStream_t s) {
-    k_cls_ghost<<<grid_for(ncell, 256), 256, 0, s>>>(dP, ncell);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_fresh_cells(const SolveParams* dP, int precision, int cur, long long ncell, int* d_status,
                                cudaStream_t s) {
-    if (precision == 0) k_fresh_cells<double><<<grid_for(ncell, 256), 256, 0, s>>>(dP, cur, ncell, d_status);
-    else k_fresh_cells<float><<<grid_for(ncell, 256), 256, 0, s>>>(dP, cur, ncell, d_status);
+    // sized for the list (a few thousand cells a step); the sweep fallback strides
+    const int grid = 2 * 148;
+    if (precision == 0) k_fresh_cells<double><<<grid, 128, 0, s>>>(dP, cur, ncell, d_status);
+    else k_fresh_cells<float><<<grid, 128, 0, s>>>(dP, cur, ncell, d_status);
     return cudaGetLastError();
 }
 

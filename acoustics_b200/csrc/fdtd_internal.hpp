@@ -41,6 +41,14 @@ struct fdtd_solver {
     cudaStream_t stream4 = nullptr;
     cudaEvent_t ev_step = nullptr, ev_lis[2] = {nullptr, nullptr}, ev_lis_join = nullptr;
     bool lis_pending[2] = {false, false};
+    // moving bodies clear of the PML: the shell kernel of a step runs on stream5
+    // beside that step's classification
+    cudaStream_t stream5 = nullptr;
+    cudaEvent_t ev_sfork = nullptr, ev_sdone = nullptr;
+    // hP.boxes are the boxes of the classification the cell flags hold (the
+    // solid cells lie in them); cleared when the flags are loaded from elsewhere
+    bool cls_boxes_current = false;
+    long long overlapped_steps = 0;
     // geometry
     double h = 0, c = 0, rho = 0, k = 0, end_time = 0, start_time = 0;
     int N[3] = {0, 0, 0};
@@ -92,7 +100,7 @@ struct fdtd_solver {
 namespace fdtd {
 void set_error(fdtd_solver* s, const std::string& msg);
 fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc);
-void classification_boxes(const fdtd_solver* s, std::vector<std::array<int, 6>>& boxes);
+void classification_boxes(const fdtd_solver* s, ClsBoxes& B);
 void to_dev_objects(fdtd_solver* s);
 fdtd_status build_fully_coupled(fdtd_solver* s);
 void free_fully_coupled(fdtd_solver* s);

@@ -34,9 +34,11 @@ cudaError_t launch_listener_prep(SolveParams* dP, int precision, int newp, int n
 cudaError_t launch_consts_init(const SolveParams* dP, double t0, cudaStream_t s);
 cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int n_lis, double* out_row,
                              cudaStream_t s);
-cudaError_t launch_cls_reset(const SolveParams* dP, long long ncell, cudaStream_t s);
-cudaError_t launch_cls_solid(const SolveParams* dP, const int start[3], const int range[3], cudaStream_t s);
-cudaError_t launch_cls_ghost(const SolveParams* dP, long long ncell, cudaStream_t s);
+// cell classification over the boxes B (a copy of dP->boxes): the box solid
+// test, the sweep over the units no box reaches and the one over those it does
+// (3 launches; the last only when some box has cells)
+cudaError_t launch_classify(const SolveParams* dP, const int N[3], const ClsBoxes& B, bool collect_fresh,
+                            cudaStream_t s);
 cudaError_t launch_cls_history(const SolveParams* dP, long long ncell, int* count, int* list, int cap, cudaStream_t s);
 cudaError_t launch_fresh_cells(const SolveParams* dP, int precision, int cur, long long ncell, int* d_status,
                                cudaStream_t s);

@@ -27,23 +27,30 @@ using namespace fdtd;
 
 namespace {
 
+// Classification over the boxes already in s->hP.boxes.
 void classification_launches(fdtd_solver* s, fdtd_status& st) {
-    std::vector<std::array<int, 6>> boxes;
-    classification_boxes(s, boxes);
-    cudaError_t e = launch_cls_reset(s->dP, s->ncell, s->stream);
-    s->launches++;
-    for (const auto& b : boxes) {
-        if (e != cudaSuccess) break;
-        const int a[3] = {b[0], b[1], b[2]}, r[3] = {b[3], b[4], b[5]};
-        e = launch_cls_solid(s->dP, a, r, s->stream);
-        s->launches++;
-    }
-    if (e == cudaSuccess) e = launch_cls_ghost(s->dP, s->ncell, s->stream);
-    s->launches++;
+    const ClsBoxes& B = s->hP.boxes;
+    // pageable source: the copy is staged before the call returns
+    cudaError_t e = cudaMemcpyAsync(&s->dP->boxes, &B, sizeof(ClsBoxes), cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess) e = launch_classify(s->dP, s->N, B, s->moving, s->stream);
+    s->launches += B.ufirst[B.n] > 0 ? 3 : 2;
     if (e != cudaSuccess) {
         set_error(s, std::string("classification launch: ") + cudaGetErrorString(e));
         st = FDTD_ERR_CUDA;
     }
+}
+
+// Every box with cells lies inside the non-PML box, two cells from its faces.
+// The classification writes pressures only at solid cells (in the boxes of
+// this step) and fresh cells (in those of the step before); the shell kernel
+// reads and writes the PML cells and reads one cell beyond them.
+bool boxes_clear_of_shell(const fdtd_solver* s, const ClsBoxes& B) {
+    for (int b = 0; b < B.n; ++b) {
+        if (B.first[b + 1] == B.first[b]) continue;
+        for (int d = 0; d < 3; ++d)
+            if (B.lo[b][d] < s->interior.lo[d] + 2 || B.lo[b][d] + B.rg[b][d] > s->interior.hi[d] - 2) return false;
+    }
+    return true;
 }
 
 // True when a Gaussian source may contribute at a step starting at time t:
@@ -98,9 +105,36 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_lis[cur], 0));
         s->lis_pending[cur] = false;
     }
+    const bool fused = s->opt.kernel == FDTD_KERNEL_FUSED;
+    bool shell_ahead = false;
     if (classify) {
         // MAC_Grid::classifyCells_FAST + InterpolateFreshPressureCell (PML_WaveSolver.cpp:807-812)
+        const ClsBoxes prev = s->hP.boxes;
+        classification_boxes(s, s->hP.boxes);
+        // Moving bodies clear of the PML: the shell kernel reads nothing the
+        // classification writes, so it starts first, on stream5, beside it.
+        shell_ahead = s->moving && fused && s->cls_boxes_current && s->n_solid_pml == 0 && !s->hP.visc &&
+                      s->stream5 && s->interior.hi[0] > s->interior.lo[0] && boxes_clear_of_shell(s, prev) &&
+                      boxes_clear_of_shell(s, s->hP.boxes);
+        if (shell_ahead) {
+            RegionLaunch R = s->region;
+            R.skip |= 1 | 4;  // the shell only
+            R.sources = 0;
+            R.fc = 0;
+            const StepStreams S5{s->stream5, nullptr, nullptr, s->ev_fork, s->ev_join, s->ev_ghost};
+            CUDA_TRY(s, cudaEventRecord(s->ev_sfork, s->stream));
+            CUDA_TRY(s, cudaStreamWaitEvent(s->stream5, s->ev_sfork, 0));
+            int l = 0;
+            if (s->precision == FDTD_PRECISION_FP64)
+                CUDA_TRY(s, launch_step_regions_fp64(s->dP, s->hP, R, cur, S5, &l));
+            else
+                CUDA_TRY(s, launch_step_regions_fp32(s->dP, s->hP, R, cur, S5, &l));
+            s->launches += l;
+            s->overlapped_steps++;
+            CUDA_TRY(s, cudaEventRecord(s->ev_sdone, s->stream5));
+        }
         classification_launches(s, st);
+        s->cls_boxes_current = true;
         if (st != FDTD_OK) return st;
         if (s->moving) {
             CUDA_TRY(s, launch_fresh_cells(s->dP, s->precision, cur, s->ncell, s->d_status, s->stream));
@@ -114,7 +148,8 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
     }
     // the region-split path advances the step constants inside its shell kernel;
     // the prologue then only runs to re-zero solid cells inside the PML
-    const bool fused = s->opt.kernel == FDTD_KERNEL_FUSED;
+    RegionLaunch R = s->region;
+    if (shell_ahead) R.skip |= 2;
     if (s->precision == FDTD_PRECISION_FP64) {
         if (!fused || s->n_solid_pml > 0) {
             CUDA_TRY(s, launch_prologue_fp64(s->dP, cur, fused ? 0 : 1, s->n_solid_pml, s->stream));
@@ -124,7 +159,7 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         if (s->opt.kernel == FDTD_KERNEL_PHASED) {
             CUDA_TRY(s, launch_phased_fp64(s->dP, s->N, cur, phased_lap(s, cur), s->stream, &l));
         } else {
-            CUDA_TRY(s, launch_step_regions_fp64(s->dP, s->hP, s->region, cur, step_streams(s), &l));
+            CUDA_TRY(s, launch_step_regions_fp64(s->dP, s->hP, R, cur, step_streams(s), &l));
         }
         s->launches += l;
     } else {
@@ -133,9 +168,10 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
             s->launches++;
         }
         int l = 0;
-        CUDA_TRY(s, launch_step_regions_fp32(s->dP, s->hP, s->region, cur, step_streams(s), &l));
+        CUDA_TRY(s, launch_step_regions_fp32(s->dP, s->hP, R, cur, step_streams(s), &l));
         s->launches += l;
     }
+    if (shell_ahead) CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_sdone, 0));
     if (s->L > 0 && dev_row) {
         // the phased path keeps p^{n+1} in the same slot as the fused one
         if (listeners_aside(s) && !classify) {
@@ -383,6 +419,8 @@ void* fdtd_solver_stream(fdtd_solver* s) { return s ? (void*)s->stream : nullptr
 const char* fdtd_solver_last_error(fdtd_solver* s) { return s ? s->err.c_str() : ""; }
 
 int64_t fdtd_solver_last_launch_count(fdtd_solver* s) { return s ? s->last_launches : 0; }
+
+int64_t fdtd_solver_overlapped_steps(fdtd_solver* s) { return s ? s->overlapped_steps : 0; }
 
 fdtd_status fdtd_solver_prepare_graphs(fdtd_solver* s) {
     if (!s) return FDTD_ERR_INVALID_ARG;
@@ -702,6 +740,7 @@ fdtd_status fdtd_solver_restore(fdtd_solver* s, const void* buffer, int64_t byte
     s->step_index = h.step_index;
     s->time = h.time;
     s->state_time = h.state_time;
+    s->cls_boxes_current = false;  // the flags came from the snapshot, not from hP.boxes
     to_dev_objects(s);
     CUDA_TRY(s, cudaMemcpy(s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice));
     return FDTD_OK;

@@ -98,6 +98,11 @@ class PML_WaveSolver:
     def last_launch_count(self) -> int:
         return int(self._L.fdtd_solver_last_launch_count(self._h))
 
+    def overlapped_steps(self) -> int:
+        """Steps whose PML-shell kernel ran beside the step's cell classification
+        (moving bodies clear of the PML); execution statistics only."""
+        return int(self._L.fdtd_solver_overlapped_steps(self._h))
+
     def prepare_graphs(self):
         """Capture the CUDA graph of the next graph_steps-long chunk now (nothing runs)."""
         check(self._L.fdtd_solver_prepare_graphs(self._h), self._h)

@@ -175,6 +175,15 @@ def profile_run(args):
         print(json.dumps({"profile_run": "config3_batch", "members": len(scenes), "steps": args.steps,
                           "launches": launches}))
         return 0
+    if args.profile_moving:
+        # configuration 5: every step reclassifies the two moving spheres
+        sc = S.config5()
+        g = PML_WaveSolver(sc, precision=prec)
+        y = g.step(3 + args.steps)
+        g.close()
+        print(json.dumps({"profile_run": sc.name, "cells": sc.n_cells, "steps": 3 + args.steps,
+                          "max_abs_listener": float(np.abs(y).max())}))
+        return 0
     sc = S.config2(n=args.profile_n)
     kern = S.KERNEL_PHASED if args.precision == "fp64-plain" else S.KERNEL_FUSED
     g = PML_WaveSolver(sc, precision=prec, kernel=kern, tile_y=args.tile_y, x_chunk=args.x_chunk)
@@ -235,6 +244,36 @@ def bench_batched(peak: float, fp64_check: bool = True):
         errs = [float(np.linalg.norm(a - c) / np.linalg.norm(c)) for a, c in zip(y32, y64)]
         out["listener_rel_l2_vs_fp64_max"] = max(errs)
         out["listener_rel_l2_vs_fp64_median"] = float(np.median(errs))
+    return out
+
+
+def bench_moving(peak: float, steps: int = 300):
+    """Configuration 5: 384x384x256, two ballistic spheres that meet mid-run, every
+    step reclassified (solid / ghost cells, fresh-cell MLS), FP32 compensated and
+    FP64, CUDA-event time of `steps` steps from the 50th (the spheres move through
+    the grid all along)."""
+    import torch
+
+    from acoustics_b200 import scene as S
+    from acoustics_b200.solver import PML_WaveSolver
+    sc = S.config5()
+    out = {"workload": "config5: 384x384x256 moving spheres, per-step reclassification", "cells": sc.n_cells,
+           "steps": steps}
+    for name, prec in (("fp32", S.PRECISION_FP32_COMPENSATED), ("fp64", S.PRECISION_FP64)):
+        g = PML_WaveSolver(sc, precision=prec)
+        g.step(50)
+        g.synchronize()
+        ext = torch.cuda.ExternalStream(g.stream)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(ext)
+        g.step(steps)
+        b.record(ext)
+        b.synchronize()
+        ms = a.elapsed_time(b) / steps
+        alg = float(g.info().algorithmic_bytes_per_step)
+        out[name] = {"ms_per_step": ms, "gcell_steps_s": sc.n_cells / (ms / 1e3) / 1e9,
+                     "hbm_frac": alg / (ms / 1e3) / 1e9 / peak}
+        g.close()
     return out
 
 
@@ -317,7 +356,10 @@ def main():
     ap.add_argument("--tile-y", type=int, default=0, help="PML-shell x planes per thread (1, 2, 4; 0 default)")
     ap.add_argument("--x-chunk", type=int, default=0, help="interior x planes per thread (2, 4, 8; 0 default)")
     ap.add_argument("--no-batched", action="store_true", help="skip the 64-scene batch (config 3)")
+    ap.add_argument("--profile-moving", action="store_true",
+                    help="with --profile: step the moving-body solve (config 5) instead of the 256^3 solve")
     ap.add_argument("--no-served", action="store_true", help="skip the serving stream (config 4)")
+    ap.add_argument("--no-moving", action="store_true", help="skip the moving-body solve (config 5)")
     ap.add_argument("--serve-rate", type=float, default=4.0)
     ap.add_argument("--serve-requests", type=int, default=16)
     args = ap.parse_args()
@@ -427,7 +469,9 @@ def main():
         if "fp64_plain" in variants and "fp32_compensated" in variants:
             variants["fp32_over_fp64_plain"] = variants["fp32_compensated"]["gcell_steps_s"] / variants["fp64_plain"]["gcell_steps_s"]
 
-    batched = served = None
+    batched = served = moving = None
+    if rank == 0 and world == 1 and not args.no_moving:
+        moving = bench_moving(peak)
     if rank == 0 and world == 1 and not args.no_batched:
         batched = bench_batched(peak)
     if rank == 0 and world == 1 and not args.no_served:
@@ -464,6 +508,8 @@ def main():
             line["batched"] = batched
         if served:
             line["served"] = served
+        if moving:
+            line["moving"] = moving
         if cpu:
             line["cpu_baseline"] = cpu
         print(json.dumps(line), flush=True)

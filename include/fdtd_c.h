@@ -290,6 +290,10 @@ fdtd_status fdtd_solver_boundary_info(fdtd_solver* s, int64_t* n_rows, int64_t* 
 int32_t fdtd_solver_pml_state(fdtd_solver* s);
 /* Kernel launches issued by the most recent fdtd_solver_step* call. */
 int64_t fdtd_solver_last_launch_count(fdtd_solver* s);
+/* Steps since creation whose PML-shell kernel ran beside the step's cell
+ * classification (moving bodies two cells clear of the PML); the others ran it
+ * after.  Execution statistics only: the results are the same either way. */
+int64_t fdtd_solver_overlapped_steps(fdtd_solver* s);
 
 /* Profiling hook (no counterpart in the reference): launch the dominant step kernel
  * n_launches times back to back on the solver's stream (alternating buffer parity,

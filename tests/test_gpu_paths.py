@@ -188,3 +188,21 @@ def test_air_viscosity_moving_bodies(oracle_lib, fdtd_lib):
     g = PML_WaveSolver(sc)
     yo, yg = o.step(80), g.step(80)
     assert rel_l2(yg, yo) <= TOL_FP64
+
+
+def test_config5_full_size_first_steps(oracle_lib, fdtd_lib):
+    """Configuration 5 at full size (384x384x256, two ballistic spheres, per-step
+    reclassification): the first steps against the FP64 oracle, classification
+    bit-exact after each chunk."""
+    sc = S.config5(steps=6)
+    o = oracle_lib.OracleSolver(sc)
+    g = PML_WaveSolver(sc)
+    for chunk in range(2):
+        yo, yg = o.step(3), g.step(3)
+        assert rel_l2(yg, yo) <= TOL_FP64, chunk
+        fo, go = o.classification()
+        fg, gg = g.GetGrid()
+        assert np.array_equal(fo, fg), chunk
+        assert np.array_equal(go, gg), chunk
+    # the spheres stay clear of the PML: every step ran its shell beside the classification
+    assert g.overlapped_steps() == 6
