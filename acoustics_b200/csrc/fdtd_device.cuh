@@ -11,7 +11,7 @@
 // reference's dense i*Ny*Nz + j*Nz + k.
 //   cls[N]      u8   bit7 bulk, bit6 valid history, bits0-5 solid-neighbour mask
 //                    (bit 2d: -d side, bit 2d+1: +d side)
-//   gobj[N]     u8   for solid cells: closest object (LowestObjectDistance) | 0x80 constraint
+//   gobj[N]     u8   for ghost cells: closest object (LowestObjectDistance) | 0x80 constraint (every solid cell)
 //   p[2][N]     T    pressure ping-pong (FP64: p^n and p^{n-1}, p^{n+1} overwrites p^{n-1};
 //                    FP32: p^n and p^{n+1})
 //   dinc[N]     f32  FP32 only: increment p^n - p^{n-1} (compensated accumulation)

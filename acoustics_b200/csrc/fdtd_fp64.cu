@@ -106,7 +106,7 @@ __global__ void __launch_bounds__(128) k_cls_boxes(const SolveParams* __restrict
     }
 }
 
-// The cells of a quad that need more than their mask: solid cells (closest
+// The cells of a quad that need more than their mask: ghost cells (closest
 // object), non-PML bulk cells with a solid neighbour (ghost-neighbour list) and
 // fresh cells (fresh-cell list); `sel` has the bulk bit set at those bytes,
 // `code` the quad's new bulk / valid bits.
@@ -145,9 +145,10 @@ __device__ __forceinline__ uint32_t quad_bulk(const SolveParams& P, const ClsBox
 
 // Quads within one cell of a box.  Neighbour masks: for a solid cell the
 // directions of its bulk neighbours (one ghost face each, MakeGhostCell
-// MAC_Grid.cpp:4310-4340) and its closest object (LowestObjectDistance,
-// MAC_Grid.cpp:3810-3814); for a bulk cell the directions of its solid (ghost)
-// neighbours, read by the Laplacian.  Mask bit 2d + (s > 0) is set where the
+// MAC_Grid.cpp:4310-4340) and, where it has one, its closest object
+// (LowestObjectDistance, MAC_Grid.cpp:3810-3814; only ghost faces read it);
+// for a bulk cell the directions of its solid (ghost) neighbours, read by the
+// Laplacian.  Mask bit 2d + (s > 0) is set where the
 // neighbour in direction s along axis d exists and differs in bulk-ness; the
 // four cells are compared at once, byte by byte of the words.
 __device__ __noinline__ void cls_sweep_near(const SolveParams& P, const ClsQuad q, uint32_t own, int collect_fresh) {
@@ -180,11 +181,14 @@ __device__ __noinline__ void cls_sweep_near(const SolveParams& P, const ClsQuad 
     // a quad that ends inside its word: the last cell's +z neighbour is padding
     if (q.nk < 4) mask &= ~(0x20u << (8 * (q.nk - 1)));
     const uint32_t bulk = base & QUAD_BULK & cells;
-    const uint32_t solid = ~base & QUAD_BULK & cells;
-    // bulk cells with a nonzero mask (a 6-bit byte plus 0x3F carries into bit 6)
-    const uint32_t listed = bulk & (((mask + 0x3F3F3F3Fu) & 0x40404040u) << 1);
+    // cells with a nonzero mask (a 6-bit byte plus 0x3F carries into bit 6)
+    const uint32_t masked = ((mask + 0x3F3F3F3Fu) & 0x40404040u) << 1;
+    // ghost cells: the solid cells whose closest object is read (ghost faces);
+    // k_cls_boxes has reset the object of every solid cell of this step
+    const uint32_t ghost = ~base & QUAD_BULK & cells & masked;
+    const uint32_t listed = bulk & masked;
     const uint32_t fresh = collect_fresh ? bulk & ~((base & QUAD_VALID) << 1) : 0u;
-    const uint32_t sel = solid | listed | fresh;
+    const uint32_t sel = ghost | listed | fresh;
     if (sel) cls_cells(P, q, sel, base, listed, fresh);
     const uint32_t out = ((base | mask) & cells) | (own & ~cells);
     if (out != own) *(uint32_t*)(P.cls + q.c0) = out;
