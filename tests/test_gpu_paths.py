@@ -190,19 +190,24 @@ def test_air_viscosity_moving_bodies(oracle_lib, fdtd_lib):
     assert rel_l2(yg, yo) <= TOL_FP64
 
 
-def test_config5_full_size_first_steps(oracle_lib, fdtd_lib):
+@pytest.mark.parametrize("precision,tol", [(S.PRECISION_FP64, TOL_FP64), (S.PRECISION_FP32_COMPENSATED, TOL_FP32)])
+def test_config5_full_size_first_steps(oracle_lib, fdtd_lib, precision, tol):
     """Configuration 5 at full size (384x384x256, two ballistic spheres, per-step
     reclassification): the first steps against the FP64 oracle, classification
-    bit-exact after each chunk."""
+    bit-exact after every step."""
     sc = S.config5(steps=6)
     o = oracle_lib.OracleSolver(sc)
-    g = PML_WaveSolver(sc)
-    for chunk in range(2):
-        yo, yg = o.step(3), g.step(3)
-        assert rel_l2(yg, yo) <= TOL_FP64, chunk
+    g = PML_WaveSolver(sc, precision=precision)
+    ys_o, ys_g = [], []
+    for step in range(6):
+        ys_o.append(o.step(1))
+        ys_g.append(g.step(1))
         fo, go = o.classification()
         fg, gg = g.GetGrid()
-        assert np.array_equal(fo, fg), chunk
-        assert np.array_equal(go, gg), chunk
+        assert np.array_equal(fo, fg), step
+        assert np.array_equal(go, gg), step
+    assert rel_l2(np.concatenate(ys_g), np.concatenate(ys_o)) <= tol
+    # the pulse has not reached the listeners yet: compare the whole pressure field
+    assert rel_l2(g.field(S.FIELD_PRESSURE), o.field(S.FIELD_PRESSURE)) <= tol
     # the spheres stay clear of the PML: every step ran its shell beside the classification
     assert g.overlapped_steps() == 6
