@@ -91,13 +91,27 @@ static void half_extent(const HostObject& o, double e[3]) {
 // BoundingBox::Update / Union arithmetic of FDTD_MovableObject.h:81-99
 void host_update_bbox(HostObject& o) {
     for (int d = 0; d < 3; ++d) { o.umin[d] = o.bmin[d]; o.umax[d] = o.bmax[d]; }
-    double e[3];
-    half_extent(o, e);
-    for (int d = 0; d < 3; ++d) { o.bmin[d] = o.c[d] - e[d]; o.bmax[d] = o.c[d] + e[d]; }
+    if (o.d.shape == FDTD_SHAPE_MESH) {
+        for (int d = 0; d < 3; ++d) { o.bmin[d] = o.c[d] + o.mlo[d]; o.bmax[d] = o.c[d] + o.mhi[d]; }
+    } else {
+        double e[3];
+        half_extent(o, e);
+        for (int d = 0; d < 3; ++d) { o.bmin[d] = o.c[d] - e[d]; o.bmax[d] = o.c[d] + e[d]; }
+    }
     for (int d = 0; d < 3; ++d) {
         o.umin[d] = std::min(o.bmin[d], o.umin[d]);
         o.umax[d] = std::max(o.bmax[d], o.umax[d]);
     }
+}
+
+HostObject make_host_object(const fdtd_scene_desc* sc, int i) {
+    HostObject h;
+    h.d = sc->objects[i];
+    if (h.d.shape == FDTD_SHAPE_MESH) {
+        const fdtd_mesh_desc& m = sc->meshes[h.d.mesh];
+        mesh_extent(m.vertices, (size_t)m.n_vertices, h.d.rotation, h.mlo, h.mhi);
+    }
+    return h;
 }
 
 void host_reset_union(HostObject& o) {
@@ -122,6 +136,7 @@ static void to_dev_object(const HostObject& o, DevObject& d) {
     d.amp = o.d.accel_amplitude;
     d.t0 = o.d.accel_t0;
     d.tau = o.d.accel_tau;
+    d.mesh = o.mview;
 }
 
 void to_dev_objects(fdtd_solver* s) {
@@ -424,9 +439,21 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
     if ((sc->n_objects > 0 && !sc->objects) || (sc->n_sources > 0 && !sc->sources) ||
         (sc->n_constraints > 0 && !sc->constraints))
         return (set_error(nullptr, "scene array missing"), FDTD_ERR_INVALID_ARG);
+    if (sc->n_meshes < 0 || (sc->n_meshes > 0 && !sc->meshes))
+        return (set_error(nullptr, "scene mesh array missing"), FDTD_ERR_INVALID_ARG);
     for (int i = 0; i < sc->n_objects; ++i) {
         const auto& o = sc->objects[i];
-        if (o.shape < 0 || o.shape > 2) return (set_error(nullptr, "unknown object shape"), FDTD_ERR_INVALID_ARG);
+        if (o.shape < 0 || o.shape > FDTD_SHAPE_MESH) return (set_error(nullptr, "unknown object shape"), FDTD_ERR_INVALID_ARG);
+        if (o.shape == FDTD_SHAPE_MESH) {
+            if (o.mesh < 0 || o.mesh >= sc->n_meshes)
+                return (set_error(nullptr, "object mesh index out of range"), FDTD_ERR_INVALID_ARG);
+            MeshHost m;
+            std::string err;
+            if (!build_mesh(sc->meshes[o.mesh], m, err)) return (set_error(nullptr, err), FDTD_ERR_GEOMETRY);
+            if (sc->boundary_handling == FDTD_BOUNDARY_FULLY_COUPLED)
+                return (set_error(nullptr, "FULLY_COUPLED boundaries are built for analytic spheres and boxes"),
+                        FDTD_ERR_UNSUPPORTED);
+        }
         if (o.accel_kind == FDTD_ACCEL_GAUSSIAN_PULSATION && o.shape != FDTD_SHAPE_SPHERE)
             return (set_error(nullptr, "pulsating acceleration is defined for spheres only"), FDTD_ERR_UNSUPPORTED);
         if (o.motion == FDTD_MOTION_BALLISTIC && o.shape == FDTD_SHAPE_ELLIPSOID)
@@ -434,7 +461,7 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
         if (o.accel_kind != FDTD_ACCEL_NONE && !(o.accel_tau > 0))
             return (set_error(nullptr, "accel_tau must be positive"), FDTD_ERR_INVALID_ARG);
         for (int d = 0; d < 3; ++d)
-            if ((o.shape != FDTD_SHAPE_SPHERE || d == 0) && !(o.size[d] > 0))
+            if (o.shape != FDTD_SHAPE_MESH && (o.shape != FDTD_SHAPE_SPHERE || d == 0) && !(o.size[d] > 0))
                 return (set_error(nullptr, "object size must be positive"), FDTD_ERR_INVALID_ARG);
     }
     for (int i = 0; i < sc->n_sources; ++i)
@@ -547,8 +574,7 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
     {
         double cells = 4096;
         for (int i = 0; i < sc->n_objects; ++i) {
-            HostObject tmp;
-            tmp.d = sc->objects[i];
+            HostObject tmp = make_host_object(sc, i);
             host_object_pose(tmp, sc->start_time);
             host_update_bbox(tmp);
             double vol = 1.0;
@@ -659,10 +685,20 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         return FDTD_ERR_UNSUPPORTED;
     }
     for (int i = 0; i < sc->n_objects; ++i) {
-        HostObject h;
-        h.d = sc->objects[i];
+        HostObject h = make_host_object(sc, i);
         s->objs.push_back(h);
         if (h.d.motion != FDTD_MOTION_STATIC) s->moving = true;
+    }
+    // meshes of the objects: hierarchy and pseudo-normals (validated above)
+    s->meshes.resize(sc->n_meshes);
+    for (int i = 0; i < sc->n_objects; ++i) {
+        const int m = sc->objects[i].shape == FDTD_SHAPE_MESH ? sc->objects[i].mesh : -1;
+        if (m < 0 || !s->meshes[m].tris.empty()) continue;
+        std::string err;
+        if (!build_mesh(sc->meshes[m], s->meshes[m], err)) {
+            set_error(nullptr, err);
+            return FDTD_ERR_GEOMETRY;
+        }
     }
     for (int i = 0; i < sc->n_constraints; ++i) s->planes.push_back(sc->constraints[i]);
     for (int i = 0; i < sc->n_sources; ++i) {
@@ -691,6 +727,21 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     s->arena_bytes = cv.off;
     for (auto& r : cv.req) *r.first = (char*)base + r.second;
     const long long ncell = s->ncell;
+    // meshes: hierarchy and triangles, one device allocation each
+    for (size_t m = 0; m < s->meshes.size(); ++m) {
+        const MeshHost& M = s->meshes[m];
+        if (M.tris.empty()) continue;
+        const size_t nb = M.nodes.size() * sizeof(MeshNode), tb = M.tris.size() * sizeof(MeshTri);
+        void* d = nullptr;
+        CUDA_TRY(nullptr, cudaMalloc(&d, nb + tb));
+        s->mesh_alloc.push_back(d);
+        s->arena_bytes += nb + tb;
+        CUDA_TRY(nullptr, cudaMemcpy(d, M.nodes.data(), nb, cudaMemcpyHostToDevice));
+        CUDA_TRY(nullptr, cudaMemcpy((char*)d + nb, M.tris.data(), tb, cudaMemcpyHostToDevice));
+        const MeshView v{(const MeshNode*)d, (const MeshTri*)((char*)d + nb), (int)M.nodes.size(), (int)M.tris.size()};
+        for (auto& o : s->objs)
+            if (o.d.shape == FDTD_SHAPE_MESH && o.d.mesh == (int)m) o.mview = v;
+    }
 
     // ---- constants ----
     for (int d = 0; d < 3; ++d) {
@@ -811,6 +862,7 @@ fdtd_status fdtd_solver_destroy(fdtd_solver* s) {
     for (int i = 0; i < 4; ++i)
         if (s->graph_exec[i]) cudaGraphExecDestroy(s->graph_exec[i]);
     free_fully_coupled(s);
+    for (void* p : s->mesh_alloc) cudaFree(p);
     if (s->arena) cudaFree(s->arena);
     if (s->h_lis_stage) cudaFreeHost(s->h_lis_stage);
     cudaStreamSynchronize(s->stream2);
@@ -951,6 +1003,14 @@ fdtd_status fdtd_scene_info(const fdtd_scene_desc* sc, const fdtd_options* opt, 
     info->n_pml_cells = s.n_pml;
     info->n_interior_cells = s.n_interior;
     info->device_bytes = (int64_t)cv.off;
+    // meshes: triangles plus a hierarchy of at most two nodes per triangle
+    std::vector<char> counted(std::max(0, sc->n_meshes), 0);
+    for (int i = 0; i < sc->n_objects; ++i) {
+        const int m = sc->objects[i].shape == FDTD_SHAPE_MESH ? sc->objects[i].mesh : -1;
+        if (m < 0 || counted[m]) continue;
+        counted[m] = 1;
+        info->device_bytes += (int64_t)sc->meshes[m].n_triangles * (int64_t)(sizeof(MeshTri) + 2 * sizeof(MeshNode));
+    }
     info->time = sc->start_time;
     info->time_step = s.k;
     const double w = s.precision == FDTD_PRECISION_FP64 ? 8.0 : 4.0;

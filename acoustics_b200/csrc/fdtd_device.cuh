@@ -21,6 +21,7 @@
 // (MAC_Grid.cpp:2495-2523, :2653-2677): every coefficient depends on one
 // coordinate only.
 #pragma once
+#include "fdtd_mesh.cuh"
 #include <cmath>
 #include <cstdint>
 
@@ -51,11 +52,12 @@ constexpr uint8_t GOBJ_NONE = 0x7F;
 
 struct DevObject {
     int shape, accel_kind, motion, _pad;
-    double c[3];        // current centre
+    double c[3];        // current centre (a mesh's object-frame origin)
     double R[9];        // object->world rotation, row-major
     double size[3];
     double bmin[3], bmax[3], bdim[3], bcen[3];  // _bboxWorld
     double amp, t0, tau, dir[3];
+    MeshView mesh;      // FDTD_SHAPE_MESH: device hierarchy and triangles
 };
 
 struct DevPlane {

@@ -33,6 +33,7 @@ FDTD_HD double sdf_local(const DevObject& o, const double p[3]) {
     if (o.shape == 0) return sqrt(r0 * r0 + r1 * r1 + r2 * r2) - o.size[0];
     double q[3];
     for (int j = 0; j < 3; ++j) q[j] = o.R[0 * 3 + j] * r0 + o.R[1 * 3 + j] * r1 + o.R[2 * 3 + j] * r2;
+    if (o.shape == 3) return mesh_sdf(o.mesh, q);
     if (o.shape == 1) {
         double out = 0.0, in = -DBL_MAX;
         for (int j = 0; j < 3; ++j) {
@@ -118,6 +119,34 @@ FDTD_HD int lowest_object(const SolveParams& P, const double p[3], double* dista
 FDTD_HD void reflect_against_boundary(const DevObject& o, const double x[3], double image[3], double bp[3],
                                       double nrm[3], double& dist) {
     const double r[3] = {x[0] - o.c[0], x[1] - o.c[1], x[2] - o.c[2]};
+    if (o.shape == 3) {
+        // mesh: closest point of the reference's search (FDTD_RigidObject.cpp:453-512;
+        // KD_NEAREST_TOLERANCE is 0, so its push-along-the-normal branch never runs)
+        double q[3], cpo[3];
+        for (int j = 0; j < 3; ++j) q[j] = o.R[0 * 3 + j] * r[0] + o.R[1 * 3 + j] * r[1] + o.R[2 * 3 + j] * r[2];
+        int tri = 0;
+        dist = mesh_closest_ref(o.mesh, q, cpo, tri);
+        for (int i = 0; i < 3; ++i)
+            bp[i] = o.c[i] + (o.R[i * 3 + 0] * cpo[0] + o.R[i * 3 + 1] * cpo[1] + o.R[i * 3 + 2] * cpo[2]);
+        const double g[3] = {bp[0] - x[0], bp[1] - x[1], bp[2] - x[2]};
+        double e[3];
+        if (sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) > 1e-10) {  // EPS, config.h:45
+            if (dist < 0.0) {
+                for (int i = 0; i < 3; ++i) e[i] = bp[i] - x[i];
+                for (int i = 0; i < 3; ++i) image[i] = bp[i] + e[i];
+            } else {
+                for (int i = 0; i < 3; ++i) e[i] = -bp[i] + x[i];
+                for (int i = 0; i < 3; ++i) image[i] = x[i] + e[i];
+            }
+        } else {  // on the triangle: its normal
+            const double* n = o.mesh.tris[tri].nf;
+            for (int i = 0; i < 3; ++i) e[i] = o.R[i * 3 + 0] * n[0] + o.R[i * 3 + 1] * n[1] + o.R[i * 3 + 2] * n[2];
+            for (int i = 0; i < 3; ++i) image[i] = x[i];
+        }
+        const double en = sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+        for (int i = 0; i < 3; ++i) nrm[i] = en > 0.0 ? e[i] / en : 0.0;
+        return;
+    }
     if (o.shape == 0) {
         const double n = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
         for (int i = 0; i < 3; ++i) bp[i] = o.c[i] + r[i] / n * o.size[0];

@@ -16,7 +16,21 @@ struct HostObject {
     double c[3] = {0, 0, 0};
     double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};  // _bboxWorld
     double umin[3] = {0, 0, 0}, umax[3] = {0, 0, 0};  // _bboxWorldUnion2Steps
+    double mlo[3] = {0, 0, 0}, mhi[3] = {0, 0, 0};    // mesh: extent of rotation * v about the centre
+    MeshView mview{};                                 // mesh: device hierarchy and triangles
 };
+
+// A validated mesh with its pseudo-normals and hierarchy (fdtd_mesh.cpp).
+struct MeshHost {
+    std::vector<MeshNode> nodes;
+    std::vector<MeshTri> tris;  // leaf order
+    std::vector<double> vertices;
+};
+bool build_mesh(const fdtd_mesh_desc& md, MeshHost& out, std::string& err);
+void mesh_extent(const double* verts, size_t nv, const double R[9], double lo[3], double hi[3]);
+// A host object of scene object i at rest (mesh extent set; pose and box not yet).
+HostObject make_host_object(const fdtd_scene_desc* sc, int i);
+bool read_obj(const char* path, double scale, std::vector<double>& verts, std::vector<int32_t>& tris, std::string& err);
 
 struct AxisTables {
     std::vector<uint8_t> pml_cell, pml_face;
@@ -58,6 +72,8 @@ struct fdtd_solver {
     double bmin[3] = {0, 0, 0}, bmax[3] = {0, 0, 0};
     fdtd::AxisTables tab[3];
     std::vector<fdtd::HostObject> objs;
+    std::vector<fdtd::MeshHost> meshes;     // the scene's meshes (those objects use)
+    std::vector<void*> mesh_alloc;          // their device copies
     std::vector<fdtd_plane_desc> planes;
     std::vector<fdtd_gaussian_source_desc> sources;
     std::vector<double> listeners;

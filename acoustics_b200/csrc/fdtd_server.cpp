@@ -38,16 +38,32 @@ struct SceneCopy {
     std::vector<fdtd_plane_desc> planes;
     std::vector<fdtd_gaussian_source_desc> srcs;
     std::vector<double> lis;
+    std::vector<fdtd_mesh_desc> meshes;
+    std::vector<std::vector<double>> mverts;
+    std::vector<std::vector<int32_t>> mtris;
     void take(const fdtd_scene_desc& s) {
         d = s;
         objs.assign(s.objects, s.objects + std::max(0, s.n_objects));
         planes.assign(s.constraints, s.constraints + std::max(0, s.n_constraints));
         srcs.assign(s.sources, s.sources + std::max(0, s.n_sources));
         lis.assign(s.listeners, s.listeners + 3 * (size_t)std::max(0, s.n_listeners));
+        const int nm = s.meshes ? std::max(0, s.n_meshes) : 0;
+        meshes.assign(s.meshes, s.meshes + nm);
+        mverts.resize(nm);
+        mtris.resize(nm);
+        for (int m = 0; m < nm; ++m) {
+            const fdtd_mesh_desc& M = s.meshes[m];
+            mverts[m].assign(M.vertices, M.vertices + 3 * (size_t)std::max(0, M.n_vertices));
+            mtris[m].assign(M.triangles, M.triangles + 3 * (size_t)std::max(0, M.n_triangles));
+            meshes[m].vertices = mverts[m].data();
+            meshes[m].triangles = mtris[m].data();
+        }
         d.objects = objs.empty() ? nullptr : objs.data();
         d.constraints = planes.empty() ? nullptr : planes.data();
         d.sources = srcs.empty() ? nullptr : srcs.data();
         d.listeners = lis.empty() ? nullptr : lis.data();
+        d.meshes = meshes.empty() ? nullptr : meshes.data();
+        d.n_meshes = nm;
     }
 };
 

@@ -157,6 +157,9 @@ struct fdtd_scene {
     std::vector<fdtd_plane_desc> planes;
     std::vector<fdtd_gaussian_source_desc> sources;
     std::vector<double> listeners;
+    std::vector<fdtd_mesh_desc> meshes;
+    std::vector<std::vector<double>> mverts;
+    std::vector<std::vector<int32_t>> mtris;
     int32_t steps = 0;
     std::string output_pattern;
 };
@@ -227,13 +230,41 @@ fdtd_status fdtd_scene_from_xml(const char* path, fdtd_scene** out) {
     if (const XNode* scene = root->child("scene")) {
         for (auto& kid : scene->kids) {
             const XNode* n = kid.get();
-            if (n->name == "analytic_sphere" || n->name == "analytic_box" || n->name == "analytic_ellipsoid") {
+            const bool mesh_obj = n->name == "rigid_object" || n->name == "rigid_sound_object";
+            if (mesh_obj || n->name == "analytic_sphere" || n->name == "analytic_box" || n->name == "analytic_ellipsoid") {
                 fdtd_object_desc o{};
-                o.shape = n->name == "analytic_sphere" ? FDTD_SHAPE_SPHERE : n->name == "analytic_box" ? FDTD_SHAPE_BOX : FDTD_SHAPE_ELLIPSOID;
+                o.shape = mesh_obj ? FDTD_SHAPE_MESH
+                                   : n->name == "analytic_sphere" ? FDTD_SHAPE_SPHERE
+                                   : n->name == "analytic_box"    ? FDTD_SHAPE_BOX
+                                                                  : FDTD_SHAPE_ELLIPSOID;
                 const char* c3[3] = {"center_x", "center_y", "center_z"};
+                const char* ip3[3] = {"initial_position_x", "initial_position_y", "initial_position_z"};
                 for (int d = 0; d < 3; ++d)
-                    if (!get_real(n, c3[d], o.center[d], false, 0.0, err)) return (set_error(nullptr, err), FDTD_ERR_INVALID_ARG);
-                if (o.shape == FDTD_SHAPE_SPHERE) {
+                    if (!get_real(n, mesh_obj ? ip3[d] : c3[d], o.center[d], false, 0.0, err))
+                        return (set_error(nullptr, err), FDTD_ERR_INVALID_ARG);
+                if (mesh_obj) {
+                    // ImpulseResponseParser.cpp:210-219: <working_directory>/<object_prefix>.obj,
+                    // scaled (the distance-field resolution has no counterpart: distances are exact)
+                    auto wd = n->attr.find("working_directory"), op = n->attr.find("object_prefix");
+                    if (wd == n->attr.end() || op == n->attr.end())
+                        return (set_error(nullptr, "<" + n->name + "> needs working_directory and object_prefix"),
+                                FDTD_ERR_INVALID_ARG);
+                    double scale = 1.0;
+                    if (!get_real(n, "scale", scale, false, 1.0, err)) return (set_error(nullptr, err), FDTD_ERR_INVALID_ARG);
+                    std::string file = wd->second + "/" + op->second + ".obj";
+                    if (!std::ifstream(file) && !file.empty() && file[0] != '/') {
+                        // relative to the XML file when not found from the working directory
+                        const std::string xp_dir = std::string(path).substr(0, std::string(path).find_last_of('/') + 1);
+                        if (std::ifstream(xp_dir + file)) file = xp_dir + file;
+                    }
+                    std::vector<double> v;
+                    std::vector<int32_t> t;
+                    if (!fdtd::read_obj(file.c_str(), scale, v, t, err)) return (set_error(nullptr, err), FDTD_ERR_IO);
+                    o.mesh = (int32_t)sc->meshes.size();
+                    sc->meshes.push_back(fdtd_mesh_desc{(int32_t)(v.size() / 3), (int32_t)(t.size() / 3), nullptr, nullptr});
+                    sc->mverts.push_back(std::move(v));
+                    sc->mtris.push_back(std::move(t));
+                } else if (o.shape == FDTD_SHAPE_SPHERE) {
                     if (!get_real(n, "radius", o.size[0], true, 0, err)) return (set_error(nullptr, err), FDTD_ERR_INVALID_ARG);
                 } else {
                     const char* pre = o.shape == FDTD_SHAPE_BOX ? "half_" : "semi_";
@@ -280,8 +311,8 @@ fdtd_status fdtd_scene_from_xml(const char* path, fdtd_scene** out) {
                 p.normal_dir = (int32_t)dir;
                 p.normal_sign = (int32_t)sign;
                 sc->planes.push_back(p);
-            } else if (n->name == "rigid_sound_object" || n->name == "rigid_object_sequence" || n->name == "shell_object") {
-                return (set_error(nullptr, "<" + n->name + "> (mesh-backed objects) is not on this path; use analytic_* primitives"),
+            } else if (n->name == "rigid_object_sequence" || n->name == "shell_object") {
+                return (set_error(nullptr, "<" + n->name + "> (keyframed object sequences, shell objects) is not on this path"),
                         FDTD_ERR_UNSUPPORTED);
             }
         }
@@ -329,6 +360,12 @@ fdtd_status fdtd_scene_from_xml(const char* path, fdtd_scene** out) {
     D.constraints = sc->planes.data();
     D.sources = sc->sources.data();
     D.listeners = sc->listeners.data();
+    for (size_t m = 0; m < sc->meshes.size(); ++m) {
+        sc->meshes[m].vertices = sc->mverts[m].data();
+        sc->meshes[m].triangles = sc->mtris[m].data();
+    }
+    D.n_meshes = (int32_t)sc->meshes.size();
+    D.meshes = sc->meshes.empty() ? nullptr : sc->meshes.data();
     *out = sc.release();
     return FDTD_OK;
 }

@@ -18,7 +18,7 @@ from typing import List, Optional, Sequence
 
 import numpy as np
 
-SHAPE_SPHERE, SHAPE_BOX, SHAPE_ELLIPSOID = 0, 1, 2
+SHAPE_SPHERE, SHAPE_BOX, SHAPE_ELLIPSOID, SHAPE_MESH = 0, 1, 2, 3
 ACCEL_NONE, ACCEL_GAUSSIAN_TRANSLATION, ACCEL_GAUSSIAN_PULSATION = 0, 1, 2
 MOTION_STATIC, MOTION_BALLISTIC = 0, 1
 PRECISION_FP64, PRECISION_FP32_COMPENSATED = 0, 1
@@ -35,11 +35,12 @@ STATUS = {
     -3: "FDTD_ERR_CUDA", -4: "FDTD_ERR_NUMERIC", -5: "FDTD_ERR_TIMEOUT",
     -6: "FDTD_ERR_GEOMETRY", -7: "FDTD_ERR_UNSUPPORTED", -8: "FDTD_ERR_IO", -9: "FDTD_ERR_BUSY",
 }
+STATUS_CODE = {name: code for code, name in STATUS.items()}
 
 
 class ObjectDesc(C.Structure):
     _fields_ = [
-        ("shape", C.c_int32), ("accel_kind", C.c_int32), ("motion", C.c_int32), ("_pad", C.c_int32),
+        ("shape", C.c_int32), ("accel_kind", C.c_int32), ("motion", C.c_int32), ("mesh", C.c_int32),
         ("center", C.c_double * 3), ("rotation", C.c_double * 9), ("size", C.c_double * 3),
         ("accel_amplitude", C.c_double), ("accel_t0", C.c_double), ("accel_tau", C.c_double),
         ("accel_dir", C.c_double * 3), ("velocity", C.c_double * 3), ("gravity", C.c_double * 3),
@@ -57,6 +58,11 @@ class GaussianSourceDesc(C.Structure):
     ]
 
 
+class MeshDesc(C.Structure):
+    _fields_ = [("n_vertices", C.c_int32), ("n_triangles", C.c_int32),
+                ("vertices", C.POINTER(C.c_double)), ("triangles", C.POINTER(C.c_int32))]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [
         ("cell_size", C.c_double), ("divisions", C.c_int32 * 3),
@@ -68,7 +74,7 @@ class SceneDesc(C.Structure):
         ("n_listeners", C.c_int32),
         ("objects", C.POINTER(ObjectDesc)), ("constraints", C.POINTER(PlaneDesc)),
         ("sources", C.POINTER(GaussianSourceDesc)), ("listeners", C.POINTER(C.c_double)),
-        ("boundary_handling", C.c_int32), ("_reserved_scene", C.c_int32),
+        ("boundary_handling", C.c_int32), ("n_meshes", C.c_int32), ("meshes", C.POINTER(MeshDesc)),
     ]
 
 
@@ -133,6 +139,15 @@ class RigidObject:
     motion: int = MOTION_STATIC
     velocity: Sequence[float] = (0.0, 0.0, 0.0)
     gravity: Sequence[float] = (0.0, 0.0, 0.0)
+    mesh: int = 0  # SHAPE_MESH: index into Scene.meshes
+
+
+@dataclass
+class TriangleMesh:
+    """Closed triangle mesh in its object frame (world = rotation @ v + center),
+    counter-clockwise from outside; see fdtd_mesh_desc."""
+    vertices: np.ndarray   # (n, 3) float64
+    triangles: np.ndarray  # (m, 3) int32
 
 
 @dataclass
@@ -172,6 +187,7 @@ class Scene:
     constraints: List[PlaneConstraint] = field(default_factory=list)
     sources: List[GaussianSource] = field(default_factory=list)
     listeners: Optional[np.ndarray] = None
+    meshes: List[TriangleMesh] = field(default_factory=list)
     steps: int = 0
     name: str = "scene"
 
@@ -189,6 +205,7 @@ class Scene:
         for i, o in enumerate(self.objects):
             d = objs[i]
             d.shape, d.accel_kind, d.motion = int(o.shape), int(o.accel_kind), int(o.motion)
+            d.mesh = int(o.mesh)
             d.center[:] = [float(x) for x in o.center]
             d.rotation[:] = [float(x) for x in o.rotation]
             sz = list(o.size) + [0.0] * (3 - len(o.size))
@@ -207,6 +224,15 @@ class Scene:
             srcs[i].width_space = s.width_space
             srcs[i].offset_time = s.offset_time
             srcs[i].normalize_constant = s.normalize_constant
+        mesh_arrays = []
+        meshes = (MeshDesc * max(1, len(self.meshes)))()
+        for i, m in enumerate(self.meshes):
+            v = np.ascontiguousarray(np.asarray(m.vertices, dtype=np.float64).reshape(-1, 3))
+            t = np.ascontiguousarray(np.asarray(m.triangles, dtype=np.int32).reshape(-1, 3))
+            mesh_arrays += [v, t]
+            meshes[i].n_vertices, meshes[i].n_triangles = v.shape[0], t.shape[0]
+            meshes[i].vertices = v.ctypes.data_as(C.POINTER(C.c_double))
+            meshes[i].triangles = t.ctypes.data_as(C.POINTER(C.c_int32))
         L = self.n_listeners
         lis = np.ascontiguousarray(np.asarray(self.listeners if L else np.zeros((1, 3)), dtype=np.float64).reshape(-1))
         desc = SceneDesc()
@@ -225,7 +251,9 @@ class Scene:
         desc.constraints = C.cast(planes, C.POINTER(PlaneDesc))
         desc.sources = C.cast(srcs, C.POINTER(GaussianSourceDesc))
         desc.listeners = lis.ctypes.data_as(C.POINTER(C.c_double))
-        return desc, (objs, planes, srcs, lis)
+        desc.n_meshes = len(self.meshes)
+        desc.meshes = C.cast(meshes, C.POINTER(MeshDesc))
+        return desc, (objs, planes, srcs, lis, meshes, mesh_arrays)
 
     # ---- geometry helpers (BoundingBox.h:89-99, ScalarField.cpp:29-50) ----
     def bbox(self):
@@ -248,6 +276,57 @@ class Scene:
             masks.append(((c - mn[d]) <= w) | ((mx[d] - c) <= w))
         inner = [int((~m).sum()) for m in masks]
         return self.n_cells - inner[0] * inner[1] * inner[2]
+
+
+def icosphere(radius: float, level: int = 2) -> TriangleMesh:
+    """Closed sphere mesh: an icosahedron with each triangle split into four
+    `level` times, vertices on the sphere; counter-clockwise from outside."""
+    g = (1.0 + 5.0 ** 0.5) / 2.0
+    v = [(-1, g, 0), (1, g, 0), (-1, -g, 0), (1, -g, 0), (0, -1, g), (0, 1, g), (0, -1, -g), (0, 1, -g),
+         (g, 0, -1), (g, 0, 1), (-g, 0, -1), (-g, 0, 1)]
+    v = [np.asarray(p, dtype=np.float64) / np.linalg.norm(p) for p in v]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    for _ in range(level):
+        mid = {}
+
+        def m(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in mid:
+                p = v[a] + v[b]
+                v.append(p / np.linalg.norm(p))
+                mid[key] = len(v) - 1
+            return mid[key]
+
+        nf = []
+        for a, b, c in f:
+            ab, bc, ca = m(a, b), m(b, c), m(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        f = nf
+    V = np.asarray(v) * radius
+    T = np.asarray(f, dtype=np.int32)
+    # outward orientation
+    n = np.cross(V[T[:, 1]] - V[T[:, 0]], V[T[:, 2]] - V[T[:, 0]])
+    flip = np.einsum("ij,ij->i", n, V[T].mean(axis=1)) < 0
+    T[flip] = T[flip][:, ::-1]
+    return TriangleMesh(V, T)
+
+
+def box_mesh(half) -> TriangleMesh:
+    """Closed box mesh with half extents `half`, two triangles per face,
+    counter-clockwise from outside."""
+    hx, hy, hz = [float(x) for x in half]
+    V = np.array([[sx * hx, sy * hy, sz * hz] for sx in (-1, 1) for sy in (-1, 1) for sz in (-1, 1)])
+    quads = [(0, 1, 3, 2), (4, 6, 7, 5), (0, 4, 5, 1), (2, 3, 7, 6), (0, 2, 6, 4), (1, 5, 7, 3)]
+    T = []
+    for a, b, c, d in quads:
+        T += [(a, b, c), (a, c, d)]
+    T = np.asarray(T, dtype=np.int32)
+    n = np.cross(V[T[:, 1]] - V[T[:, 0]], V[T[:, 2]] - V[T[:, 0]])
+    flip = np.einsum("ij,ij->i", n, V[T].mean(axis=1)) < 0
+    T[flip] = T[flip][:, ::-1]
+    return TriangleMesh(V, T)
 
 
 def reference_time_step(h: float, c: float = 343.0) -> float:

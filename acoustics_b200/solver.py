@@ -196,7 +196,7 @@ def scene_from_xml(path: str) -> Scene:
     check(L.fdtd_scene_from_xml(path.encode(), C.byref(h)))
     try:
         d = L.fdtd_scene_desc_get(h).contents
-        from .scene import GaussianSource, PlaneConstraint, RigidObject
+        from .scene import GaussianSource, PlaneConstraint, RigidObject, TriangleMesh
         sc = Scene(cell_size=d.cell_size, divisions=tuple(d.divisions), time_step=d.time_step,
                    domain_center=tuple(d.domain_center), sound_speed=d.sound_speed, density=d.density,
                    pml_width=d.pml_width, pml_strength=d.pml_strength,
@@ -207,7 +207,12 @@ def scene_from_xml(path: str) -> Scene:
             o = d.objects[i]
             sc.objects.append(RigidObject(o.shape, tuple(o.center), tuple(o.size), tuple(o.rotation), o.accel_kind,
                                           o.accel_amplitude, o.accel_t0, o.accel_tau, tuple(o.accel_dir), o.motion,
-                                          tuple(o.velocity), tuple(o.gravity)))
+                                          tuple(o.velocity), tuple(o.gravity), int(o.mesh)))
+        for i in range(d.n_meshes):
+            m = d.meshes[i]
+            v = np.ctypeslib.as_array(m.vertices, shape=(m.n_vertices * 3,)).reshape(-1, 3).copy()
+            t = np.ctypeslib.as_array(m.triangles, shape=(m.n_triangles * 3,)).reshape(-1, 3).copy()
+            sc.meshes.append(TriangleMesh(v, t))
         for i in range(d.n_constraints):
             p = d.constraints[i]
             sc.constraints.append(PlaneConstraint(p.normal_dir, p.normal_sign, p.height))
@@ -292,3 +297,16 @@ def read_matrix(path: str) -> np.ndarray:
     out = np.zeros((r.value, c.value), dtype=np.float64)
     check(L.fdtd_matrix_read(path.encode(), C.byref(r), C.byref(c), out.ctypes.data, out.size))
     return out
+
+
+def read_obj(path: str, scale: float = 1.0):
+    """Wavefront .obj surface mesh as a TriangleMesh (the library's reader:
+    "v" and "f" records, polygons fanned, coordinates times `scale`)."""
+    from .scene import TriangleMesh
+    L = load()
+    nv, nt = C.c_int32(0), C.c_int32(0)
+    check(L.fdtd_read_obj(str(path).encode(), float(scale), C.byref(nv), C.byref(nt), None, None))
+    v = np.zeros((nv.value, 3), dtype=np.float64)
+    t = np.zeros((nt.value, 3), dtype=np.int32)
+    check(L.fdtd_read_obj(str(path).encode(), float(scale), C.byref(nv), C.byref(nt), v.ctypes.data, t.ctypes.data))
+    return TriangleMesh(v, t)

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define FDTD_ABI_VERSION 2
+#define FDTD_ABI_VERSION 3
 
 typedef int32_t fdtd_status;
 enum {
@@ -43,7 +43,21 @@ enum {
 /* ---------------------------------------------------------------------------
  * Scene description (plain data, copied at create time)
  * ------------------------------------------------------------------------- */
-enum { FDTD_SHAPE_SPHERE = 0, FDTD_SHAPE_BOX = 1, FDTD_SHAPE_ELLIPSOID = 2 };
+enum { FDTD_SHAPE_SPHERE = 0, FDTD_SHAPE_BOX = 1, FDTD_SHAPE_ELLIPSOID = 2,
+       FDTD_SHAPE_MESH = 3 /* closed triangle mesh (FDTD_RigidObject over a surface .obj) */ };
+
+/* A closed, consistently oriented triangle mesh in its object frame (the
+ * reference's FDTD_RigidObject::_mesh after MeshObjReader's scaling,
+ * FDTD_RigidObject.cpp:84-93): world = rotation * v + center.  Triangles are
+ * counter-clockwise seen from outside; every edge must be shared by exactly two
+ * triangles (the signed distance field of FDTD_RigidObject.cpp:59-76 rejects
+ * meshes with a boundary). */
+typedef struct {
+    int32_t n_vertices;
+    int32_t n_triangles;
+    const double* vertices;    /* 3 * n_vertices                                        */
+    const int32_t* triangles;  /* 3 * n_triangles vertex indices                        */
+} fdtd_mesh_desc;
 
 /* Boundary normal-acceleration model of an object (replaces the vibrational
  * sources summed by FDTD_RigidObject::EvaluateBoundaryAcceleration,
@@ -60,8 +74,8 @@ typedef struct {
     int32_t shape;
     int32_t accel_kind;
     int32_t motion;
-    int32_t _pad;
-    double center[3];     /* body centre at t = 0 (world)                            */
+    int32_t mesh;         /* FDTD_SHAPE_MESH: index into fdtd_scene_desc.meshes; else 0 */
+    double center[3];     /* body centre at t = 0 (world); a mesh's object-frame origin */
     double rotation[9];   /* row-major object->world rotation (identity if unused)    */
     double size[3];       /* sphere: size[0]=radius; box: half extents; ellipsoid: semi-axes */
     double accel_amplitude;
@@ -112,7 +126,8 @@ typedef struct {
     const fdtd_gaussian_source_desc* sources;
     const double* listeners;       /* 3 * n_listeners, world coordinates                  */
     int32_t boundary_handling;     /* FDTD_BOUNDARY_* (<solver boundary_handling=>)       */
-    int32_t _reserved_scene;       /* 0 */
+    int32_t n_meshes;
+    const fdtd_mesh_desc* meshes;  /* meshes of the FDTD_SHAPE_MESH objects                */
 } fdtd_scene_desc;
 
 enum {
@@ -429,6 +444,13 @@ const fdtd_scene_desc* fdtd_scene_desc_get(const fdtd_scene* sc);
 int32_t fdtd_scene_number_of_steps(const fdtd_scene* sc);
 const char* fdtd_scene_output_pattern(const fdtd_scene* sc);
 void fdtd_scene_free(fdtd_scene* sc);
+
+/* Wavefront .obj surface mesh (MeshObjReader::read with a scale, as the
+ * <rigid_object scale=> attribute applies it): the "v" and "f" records, polygons
+ * fanned into triangles, indices made 0-based.  Call with NULL arrays for the
+ * counts, then with arrays of 3 * count entries. */
+fdtd_status fdtd_read_obj(const char* path, double scale, int32_t* n_vertices, int32_t* n_triangles,
+                          double* vertices, int32_t* triangles);
 
 /* all_audio.dat writer (AudioOutput, src/wavesolver/AudioOutput.cpp:27-64): appends
  * n_steps*n_listeners raw doubles. */

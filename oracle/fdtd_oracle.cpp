@@ -79,13 +79,194 @@ struct OBox {
     }
 };
 
-// Analytic rigid object standing in for FDTD_RigidObject's mesh + ADF
-// (FDTD_RigidObject.cpp:256-277): sign convention negative inside.
+// Closed triangle mesh in its object frame (FDTD_RigidObject::_mesh).  Two
+// queries over every triangle in index order (a strict < keeps the first of
+// equal squared distances):
+//  * Sdf: exact distance to the closest triangle point, signed by the
+//    pseudo-normal of the closest feature (face, edge or vertex) as the
+//    reference's adaptive distance field signs its samples
+//    (AdaptiveDistanceField.cpp:170-195, Baerentzen 2002; its tolerance of 1e-6 m,
+//    Wavesolver_ConstantsAndTypes.h:88-91, is what the exact distance stands for);
+//  * Closest: TriangleMesh::ComputeClosestPointOnMeshHelper
+//    (TriangleMesh.hpp:819-985) over all triangles (the reference's k-d tree
+//    hands it the 100 nearest), sign from the closest triangle's plane side.
+struct OMesh {
+    struct Tri {
+        V3 p[3];
+        V3 nf;     // unit face normal (p1 - p0) x (p2 - p0)
+        V3 ne[3];  // edges p0p1, p1p2, p2p0: sum of the two unit face normals
+        V3 nv[3];  // vertices: angle-weighted sum of the unit face normals
+    };
+    std::vector<Tri> t;
+    std::vector<double> verts;
+
+    static double dot(const V3& a, const V3& b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+    static V3 sub(const V3& a, const V3& b) { return V3(a[0] - b[0], a[1] - b[1], a[2] - b[2]); }
+
+    bool build(const fdtd_mesh_desc& m) {
+        const int nt = m.n_triangles;
+        t.assign(nt, Tri());
+        verts.assign(m.vertices, m.vertices + 3 * (size_t)m.n_vertices);
+        std::map<std::pair<int, int>, int> edge;  // directed edge -> triangle
+        for (int k = 0; k < nt; ++k) {
+            for (int j = 0; j < 3; ++j) {
+                const int v = m.triangles[3 * k + j];
+                t[k].p[j] = V3(m.vertices[3 * v], m.vertices[3 * v + 1], m.vertices[3 * v + 2]);
+            }
+            const V3 a = sub(t[k].p[1], t[k].p[0]), b = sub(t[k].p[2], t[k].p[0]);
+            const V3 n(a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0]);
+            const double ln = std::sqrt(dot(n, n));
+            if (!(ln > 0.0)) return false;
+            for (int d = 0; d < 3; ++d) t[k].nf[d] = n[d] / ln;
+            for (int j = 0; j < 3; ++j) edge[{m.triangles[3 * k + j], m.triangles[3 * k + (j + 1) % 3]}] = k;
+        }
+        for (int k = 0; k < nt; ++k)
+            for (int j = 0; j < 3; ++j) {
+                const auto r = edge.find({m.triangles[3 * k + (j + 1) % 3], m.triangles[3 * k + j]});
+                if (r == edge.end()) return false;  // open mesh
+                for (int d = 0; d < 3; ++d) t[k].ne[j][d] = t[k].nf[d] + t[r->second].nf[d];
+            }
+        std::vector<double> vn(verts.size(), 0.0);
+        for (int k = 0; k < nt; ++k)
+            for (int j = 0; j < 3; ++j) {
+                const V3 a = sub(t[k].p[(j + 1) % 3], t[k].p[j]), b = sub(t[k].p[(j + 2) % 3], t[k].p[j]);
+                double cs = dot(a, b) / (std::sqrt(dot(a, a)) * std::sqrt(dot(b, b)));
+                cs = std::max(-1.0, std::min(1.0, cs));
+                const double ang = std::acos(cs);
+                const int v = m.triangles[3 * k + j];
+                for (int d = 0; d < 3; ++d) vn[3 * v + d] += ang * t[k].nf[d];
+            }
+        for (int k = 0; k < nt; ++k)
+            for (int j = 0; j < 3; ++j) {
+                const int v = m.triangles[3 * k + j];
+                t[k].nv[j] = V3(vn[3 * v], vn[3 * v + 1], vn[3 * v + 2]);
+            }
+        return true;
+    }
+
+    // closest point of a triangle by its Voronoi regions (Ericson, Real-Time
+    // Collision Detection 5.1.5); region 0 face, 1-3 edges p0p1 / p1p2 / p2p0, 4-6 vertices
+    static V3 ClosestExact(const V3& q, const Tri& T, int& region) {
+        const V3& a = T.p[0];
+        const V3& b = T.p[1];
+        const V3& c = T.p[2];
+        const V3 ab = sub(b, a), ac = sub(c, a), aq = sub(q, a), bq = sub(q, b), cq = sub(q, c);
+        const double d1 = dot(ab, aq), d2 = dot(ac, aq);
+        if (d1 <= 0.0 && d2 <= 0.0) { region = 4; return a; }
+        const double d3 = dot(ab, bq), d4 = dot(ac, bq);
+        if (d3 >= 0.0 && d4 <= d3) { region = 5; return b; }
+        const double vc = d1 * d4 - d3 * d2;
+        if (vc <= 0.0 && d1 >= 0.0 && d3 <= 0.0) {
+            const double v = d1 / (d1 - d3);
+            region = 1;
+            return V3(a[0] + v * ab[0], a[1] + v * ab[1], a[2] + v * ab[2]);
+        }
+        const double d5 = dot(ab, cq), d6 = dot(ac, cq);
+        if (d6 >= 0.0 && d5 <= d6) { region = 6; return c; }
+        const double vb = d5 * d2 - d1 * d6;
+        if (vb <= 0.0 && d2 >= 0.0 && d6 <= 0.0) {
+            const double w = d2 / (d2 - d6);
+            region = 3;
+            return V3(a[0] + w * ac[0], a[1] + w * ac[1], a[2] + w * ac[2]);
+        }
+        const double va = d3 * d6 - d5 * d4;
+        if (va <= 0.0 && (d4 - d3) >= 0.0 && (d5 - d6) >= 0.0) {
+            const double w = (d4 - d3) / ((d4 - d3) + (d5 - d6));
+            region = 2;
+            return V3(b[0] + w * (c[0] - b[0]), b[1] + w * (c[1] - b[1]), b[2] + w * (c[2] - b[2]));
+        }
+        const double den = 1.0 / (va + vb + vc);
+        const double v = vb * den, w = vc * den;
+        region = 0;
+        return V3(a[0] + ab[0] * v + ac[0] * w, a[1] + ab[1] * v + ac[1] * w, a[2] + ab[2] * v + ac[2] * w);
+    }
+
+    double Sdf(const V3& q) const {
+        double best = DMAX, s = 0.0;
+        for (const Tri& T : t) {
+            int region;
+            const V3 cp = ClosestExact(q, T, region);
+            const V3 r = sub(q, cp);
+            const double d2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+            if (d2 < best) {
+                best = d2;
+                const V3& n = region == 0 ? T.nf : (region <= 3 ? T.ne[region - 1] : T.nv[region - 4]);
+                s = dot(r, n);
+            }
+        }
+        const double d = std::sqrt(best);
+        return s < 0.0 ? -d : d;
+    }
+
+    // one triangle of ComputeClosestPointOnMeshHelper (TriangleMesh.hpp:835-948)
+    static double ClosestRefTri(const V3& q, const Tri& T, V3& cp) {
+        const V3& p0 = T.p[0];
+        const V3& p1 = T.p[1];
+        const V3& p2 = T.p[2];
+        const V3 e0 = sub(p2, p0), e1 = sub(p1, p0);
+        const double dot00 = dot(e0, e0), dot01 = dot(e0, e1), dot11 = dot(e1, e1);
+        const V3 n(e1[1] * e0[2] - e1[2] * e0[1], e1[2] * e0[0] - e1[0] * e0[2], e1[0] * e0[1] - e1[1] * e0[0]);
+        const double dp = n[0] * p0[0] + n[1] * p0[1] + n[2] * p0[2];
+        const double tt = (dp - dot(n, q)) / dot(n, n);
+        const V3 pp(q[0] + n[0] * tt, q[1] + n[1] * tt, q[2] + n[2] * tt);
+        const double sgn = tt >= 0.0 ? -1.0 : 1.0;
+        const V3 e2 = sub(pp, p0);
+        const double dot02 = dot(e0, e2), dot12 = dot(e1, e2);
+        const double denom = dot00 * dot11 - dot01 * dot01;
+        const double inv = 1. / denom;
+        const double u = (dot11 * dot02 - dot01 * dot12) * inv;
+        const double v = (dot00 * dot12 - dot01 * dot02) * inv;
+        auto along = [&](const V3& e, const V3& o, double l, double sq) {
+            V3 r;
+            for (int i = 0; i < 3; ++i) r[i] = l > sq ? pp[i] + (e[i] - o[i]) : pp[i] + (e[i] * l / sq - o[i]);
+            return r;
+        };
+        if (u >= 0 && v >= 0 && (u + v) < 1) cp = pp;
+        else if (u < 0 && v >= 0 && (u + v) < 1) cp = along(e1, e2, std::max(dot12, 0.0), dot11);
+        else if (u >= 0 && v < 0 && (u + v) < 1) cp = along(e0, e2, std::max(dot02, 0.0), dot00);
+        else if (u >= 0 && v >= 0 && (u + v) >= 1) {
+            const V3 e12 = sub(p2, p1), o12 = sub(pp, p1);
+            cp = along(e12, o12, std::max(dot(o12, e12), 0.0), dot(e12, e12));
+        } else if (u < 0 && v < 0 && (u + v) < 1) cp = p0;
+        else if (u < 0 && v >= 0 && (u + v) >= 1) cp = p1;
+        else if (u >= 0 && v < 0 && (u + v) >= 1) cp = p2;
+        else {
+            double dd[3];
+            for (int k = 0; k < 3; ++k) {
+                const V3 r = sub(pp, T.p[k]);
+                dd[k] = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+            }
+            cp = dd[0] < dd[1] ? (dd[0] < dd[2] ? p0 : p2) : (dd[1] < dd[2] ? p1 : p2);
+        }
+        const V3 r = sub(q, cp);
+        return sgn * (r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    }
+
+    double Closest(const V3& q, V3& cp, int& tri) const {
+        double best = DMAX;
+        tri = -1;
+        for (int k = 0; k < (int)t.size(); ++k) {
+            V3 c;
+            const double ds = ClosestRefTri(q, t[k], c);
+            if (std::fabs(ds) < std::fabs(best)) {
+                best = ds;
+                tri = k;
+                cp = c;
+            }
+        }
+        return best >= 0.0 ? std::sqrt(best) : -std::sqrt(-best);
+    }
+};
+
+// Rigid object: an analytic body standing in for FDTD_RigidObject's mesh + ADF
+// (FDTD_RigidObject.cpp:256-277), or a triangle mesh; negative inside.
 struct Obj {
     fdtd_object_desc d;
     V3 c;        // current centre
     OBox box;    // _bboxWorld
     OBox ubox;   // _bboxWorldUnion2Steps
+    const OMesh* mesh = nullptr;
+    V3 mlo, mhi;  // mesh: extent of rotation * v
 
     void pose(double t) {  // ballistic kinematics x(t) = x0 + v t + g t^2/2
         for (int a = 0; a < 3; ++a) {
@@ -114,6 +295,8 @@ struct Obj {
         ubox = box;
         V3 e = half_extent(), a, b;
         for (int i = 0; i < 3; ++i) { a[i] = c[i] - e[i]; b[i] = c[i] + e[i]; }
+        if (mesh)
+            for (int i = 0; i < 3; ++i) { a[i] = c[i] + mlo[i]; b[i] = c[i] + mhi[i]; }
         box.Update(a, b);
         ubox.Union(box);
     }
@@ -127,6 +310,7 @@ struct Obj {
         V3 q;  // object frame: R^T r
         for (int j = 0; j < 3; ++j)
             q[j] = d.rotation[0 * 3 + j] * r[0] + d.rotation[1 * 3 + j] * r[1] + d.rotation[2 * 3 + j] * r[2];
+        if (mesh) return mesh->Sdf(q);
         if (d.shape == FDTD_SHAPE_BOX) {
             double out = 0.0, in = -DMAX;
             for (int j = 0; j < 3; ++j) {
@@ -177,6 +361,31 @@ struct Obj {
     void Reflect(const V3& x, V3& image, V3& bp, V3& nrm, double& dist) const {
         V3 r;
         for (int i = 0; i < 3; ++i) r[i] = x[i] - c[i];
+        if (mesh) {
+            // FDTD_RigidObject.cpp:453-512 (KD_NEAREST_TOLERANCE = 0: no push along the normal)
+            V3 q, cpo;
+            for (int j = 0; j < 3; ++j)
+                q[j] = d.rotation[0 * 3 + j] * r[0] + d.rotation[1 * 3 + j] * r[1] + d.rotation[2 * 3 + j] * r[2];
+            int tri = 0;
+            dist = mesh->Closest(q, cpo, tri);
+            for (int i = 0; i < 3; ++i)
+                bp[i] = c[i] + (d.rotation[i * 3 + 0] * cpo[0] + d.rotation[i * 3 + 1] * cpo[1] + d.rotation[i * 3 + 2] * cpo[2]);
+            const V3 g(bp[0] - x[0], bp[1] - x[1], bp[2] - x[2]);
+            V3 e;
+            if (std::sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]) > 1e-10) {  // EPS, config.h:45
+                const bool in = dist < 0.0;
+                for (int i = 0; i < 3; ++i) e[i] = in ? bp[i] - x[i] : -bp[i] + x[i];
+                for (int i = 0; i < 3; ++i) image[i] = in ? bp[i] + e[i] : x[i] + e[i];
+            } else {
+                const V3& n = mesh->t[tri].nf;
+                for (int i = 0; i < 3; ++i)
+                    e[i] = d.rotation[i * 3 + 0] * n[0] + d.rotation[i * 3 + 1] * n[1] + d.rotation[i * 3 + 2] * n[2];
+                image = x;
+            }
+            const double en = std::sqrt(e[0] * e[0] + e[1] * e[1] + e[2] * e[2]);
+            for (int i = 0; i < 3; ++i) nrm[i] = en > 0.0 ? e[i] / en : 0.0;
+            return;
+        }
         if (d.shape == FDTD_SHAPE_SPHERE) {
             const double n = std::sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
             for (int i = 0; i < 3; ++i) bp[i] = c[i] + r[i] / n * d.size[0];
@@ -246,6 +455,7 @@ struct Oracle {
     int vN[3][3];  // velocity grid divisions
     V3 vmin[3];
     // objects, constraints, sources, listeners
+    std::vector<OMesh> meshes;  // before objs: objects point into it
     std::vector<Obj> objs;
     std::vector<fdtd_plane_desc> planes;
     std::vector<fdtd_gaussian_source_desc> srcs;
@@ -1193,9 +1403,25 @@ struct Oracle {
         }
         absorptionWidth = s->pml_width * h;  // setPMLBoundaryWidth (MAC_Grid.cpp:146-150)
         absorptionStrength = s->pml_strength;
+        meshes.resize(std::max(0, s->n_meshes));
+        for (int m = 0; m < (int)meshes.size(); ++m)
+            if (!meshes[m].build(s->meshes[m])) { err = "mesh is open or degenerate"; return FDTD_ERR_GEOMETRY; }
         for (int i = 0; i < s->n_objects; ++i) {
             Obj o;
             o.d = s->objects[i];
+            if (o.d.shape == FDTD_SHAPE_MESH) {
+                if (o.d.mesh < 0 || o.d.mesh >= (int)meshes.size()) { err = "mesh index"; return FDTD_ERR_INVALID_ARG; }
+                o.mesh = &meshes[o.d.mesh];
+                const std::vector<double>& v = o.mesh->verts;
+                for (int d = 0; d < 3; ++d) { o.mlo[d] = DMAX; o.mhi[d] = -DMAX; }
+                for (size_t k = 0; k + 2 < v.size(); k += 3)
+                    for (int d = 0; d < 3; ++d) {
+                        const double w = o.d.rotation[d * 3 + 0] * v[k] + o.d.rotation[d * 3 + 1] * v[k + 1] +
+                                         o.d.rotation[d * 3 + 2] * v[k + 2];
+                        o.mlo[d] = std::min(o.mlo[d], w);
+                        o.mhi[d] = std::max(o.mhi[d], w);
+                    }
+            }
             objs.push_back(o);
         }
         for (int i = 0; i < s->n_constraints; ++i) planes.push_back(s->constraints[i]);

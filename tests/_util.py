@@ -25,3 +25,17 @@ def small_config2(n=80, steps=150):
     sc.listeners = np.asarray(sc.listeners) * 0.5
     sc.steps = steps
     return sc
+
+
+def small_scene_with(*objects, meshes=(), n=40, steps=20):
+    """A small static scene (n^3, h = 5 mm, PML 6) with the given objects and
+    meshes, one source and two listeners away from the domain centre."""
+    from acoustics_b200 import scene as S
+    h = 0.005
+    sc = S.Scene(cell_size=h, divisions=(n, n, n), time_step=S.reference_time_step(h), pml_width=6, steps=steps,
+                 name="small_with_objects")
+    sc.objects.extend(objects)
+    sc.meshes.extend(meshes)
+    sc.sources.append(S.GaussianSource((0.0, 0.06, 0.0), 1e-4))
+    sc.listeners = np.array([[0.0, -0.06, 0.01], [0.05, 0.0, -0.02]])
+    return sc

@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol(fdtd_lib):
 
 
 def test_abi_version(fdtd_lib):
-    assert fdtd_lib.fdtd_abi_version() == 2
+    assert fdtd_lib.fdtd_abi_version() == 3
 
 
 def test_struct_layouts_match_header(tmp_path):
@@ -128,7 +128,10 @@ def test_xml_scene_reader(fdtd_lib, tmp_path):
     ("<impulse_response><solver cellsize='0.005'/></impulse_response>", -1),
     ("<impulse_response>", -1),
     ("<other/>", -1),
+    # a mesh object without its working_directory / object_prefix
     (SCENE_XML.replace("analytic_sphere", "rigid_sound_object", 1).replace(
+        "radius=\"0.04\"", "", 1), -1),
+    (SCENE_XML.replace("analytic_sphere", "rigid_object_sequence", 1).replace(
         "radius=\"0.04\"", "", 1), -7),
     (SCENE_XML.replace('type="static"', 'type="dynamic"'), -7),
     (SCENE_XML.replace('<solver ', '<solver boundary_handling="voxelized" ', 1), -1),
