@@ -525,14 +525,10 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
         cv.add(&P.lapv[0], n * w);
         cv.add(&P.lapv[1], n * w);
     }
-    // spatial factors of the sources over their region (one table per source)
+    // per-axis spatial factors of the sources
     s->region.src_region = source_region(s);
-    {
-        const Box3& r = s->region.src_region;
-        P.src_cells = (long long)(r.hi[0] - r.lo[0]) * (r.hi[1] - r.lo[1]) * (r.hi[2] - r.lo[2]);
-        if (P.src_cells > 0 && !s->sources.empty())
-            cv.add((void**)&P.src_g, (size_t)P.src_cells * s->sources.size() * 8);
-    }
+    if (!s->sources.empty())
+        for (int d = 0; d < 3; ++d) cv.add((void**)&P.src_ax[d], s->sources.size() * (size_t)N[d] * 8);
     // compact storage of the z-slab box (region-split path)
     const ShellBoxes& SB = s->shell;
     if (o.kernel == FDTD_KERNEL_FUSED && SB.zbox >= 0) {
@@ -796,6 +792,24 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         D.wt = g.width_time;
         D.scale = 1. / 3.6836 * g.normalize_constant;
     }
+    // Gaussian sources (GaussianPressureSource.cpp:6-30): zero outside the box
+    // x_s +- 2 sigma_s (strict, per axis), exp(-|x - x_s|^2 / 2 sigma_s^2) * scale
+    // inside, the product of one factor per axis
+    if (!s->sources.empty())
+        for (int d = 0; d < 3; ++d) {
+            std::vector<double> g(s->sources.size() * (size_t)N[d], 0.0);
+            for (size_t i = 0; i < s->sources.size(); ++i) {
+                const DevSource& S = P.src[i];
+                for (int x = 0; x < N[d]; ++x) {
+                    const double px = s->tab[d].cpos[x];
+                    if (!(px < S.bmax[d] && px > S.bmin[d])) continue;
+                    double v = std::exp(-((px - S.cen[d]) * (px - S.cen[d])) / S.denom);
+                    if (d == 0) v *= S.scale;
+                    g[i * N[d] + x] = v;
+                }
+            }
+            CUDA_TRY(s.get(), cudaMemcpy((void*)P.src_ax[d], g.data(), g.size() * 8, cudaMemcpyHostToDevice));
+        }
     // tables
     for (int d = 0; d < 3; ++d) {
         auto& T = s->tab[d];
@@ -929,7 +943,6 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     fdtd_status st = upload_params(s);
     if (st != FDTD_OK) return st;
     CUDA_TRY(s, launch_consts_init(s->dP, t0, s->stream));
-    if (P.src_g) CUDA_TRY(s, launch_source_factors(s->dP, s->region.src_region, P.n_src, P.src_cells, s->stream));
     s->launches = 0;
     st = run_classification(s);
     if (st != FDTD_OK) return st;

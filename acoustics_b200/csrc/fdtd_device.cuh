@@ -274,9 +274,9 @@ struct SolveParams {
     int lis_ready;                // plans valid for the current classification
     int* solid_pml;               // solid cells inside the PML (re-zeroed every step)
     int n_solid_pml;
-    double* src_g;                // [n_src][src_cells] spatial factor exp(-r^2/2w^2)*scale of each
-                                  // source over the source region (zero outside its box)
-    long long src_cells;          // cells of the source region
+    double* src_ax[3];            // [n_src][N_d] per-axis spatial factors of each source:
+                                  // exp(-(x_d - c_d)^2 / 2w^2) inside the source box (the
+                                  // x factor times the source scale), 0 outside
     int* ghost_list;              // non-PML bulk cells with a solid neighbour
     int* ghost_count;
     int ghost_cap;
@@ -424,8 +424,8 @@ struct BatchLaunch {
     int n_members;
     int xb, xs;
     int ghost_blocks;            // per member
-    int src_blocks;              // per member (0: no member has a source)
     int solid_blocks;            // per member (0: no member has a solid cell inside its PML)
+    int src_blocks;              // per member (0: no member has a source)
 };
 
 // z-vector groups of the interior box: groups start at multiples of V = 16 /
@@ -457,6 +457,26 @@ __host__ __device__ __forceinline__ void dense_ijk(const SolveParams& P, long lo
     const long long r = t - i * yz;
     j = (int)(r / P.N[2]);
     k = (int)(r - (long long)j * P.N[2]);
+}
+
+// Some Gaussian source contributes at the step of parity `cur` (its time
+// factor has not underflowed to zero).
+__device__ __forceinline__ bool sources_on(const SolveParams& P, int cur) {
+    bool any = false;
+    for (int s = 0; s < P.n_src; ++s) any |= P.consts[cur].src_tf[s] != 0.0;
+    return any;
+}
+
+// sum_s G_s(x, t + k/2) at cell (x, y, z) (GaussianPressureSource.cpp:6-30): the
+// product of the per-axis spatial factors times the step's time factor.
+__device__ __forceinline__ double source_term(const SolveParams& P, int cur, int x, int y, int z) {
+    double src = 0.0;
+    for (int s = 0; s < P.n_src; ++s) {
+        const double tf = P.consts[cur].src_tf[s];
+        if (tf == 0.0) continue;
+        src += ((P.src_ax[0][s * P.N[0] + x] * P.src_ax[1][s * P.N[1] + y]) * P.src_ax[2][s * P.N[2] + z]) * tf;
+    }
+    return src;
 }
 
 // consts[cur^1] <- the next step's constants (PML_WaveSolver.cpp:825,

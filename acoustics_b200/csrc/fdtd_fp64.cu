@@ -627,38 +627,6 @@ cudaError_t launch_prologue_fp64(const SolveParams* dP, int cur, int advance, in
     return cudaGetLastError();
 }
 
-// Spatial factor of each Gaussian source over the source region
-// (GaussianPressureSource.cpp:6-30 without the time factor), once per reset:
-// the per-step source update is then one multiply-add per source and cell.
-__global__ void k_source_factors(const SolveParams* __restrict__ Pp, Box3 r) {
-    const SolveParams& P = *Pp;
-    const int nx = r.hi[0] - r.lo[0], ny = r.hi[1] - r.lo[1], nz = r.hi[2] - r.lo[2];
-    const long long R = (long long)nx * ny * nz;
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < R * P.n_src;
-         t += (long long)gridDim.x * blockDim.x) {
-        const int s = (int)(t / R);
-        const long long q = t - s * R;
-        const int z = r.lo[2] + (int)(q % nz);
-        const int y = r.lo[1] + (int)((q / nz) % ny);
-        const int x = r.lo[0] + (int)(q / ((long long)nz * ny));
-        const double px = P.cpos[0][x], py = P.cpos[1][y], pz = P.cpos[2][z];
-        const DevSource& S = P.src[s];
-        double v = 0.0;
-        if (px < S.bmax[0] && px > S.bmin[0] && py < S.bmax[1] && py > S.bmin[1] && pz < S.bmax[2] && pz > S.bmin[2]) {
-            v = (px - S.cen[0]) * (px - S.cen[0]) + (py - S.cen[1]) * (py - S.cen[1]) + (pz - S.cen[2]) * (pz - S.cen[2]);
-            v = -v / S.denom;
-            v = exp(v);
-            v *= S.scale;
-        }
-        P.src_g[t] = v;
-    }
-}
-
-cudaError_t launch_source_factors(const SolveParams* dP, Box3 region, int n_src, long long cells, cudaStream_t s) {
-    if (cells <= 0 || n_src <= 0) return cudaSuccess;
-    k_source_factors<<<grid_for(cells * n_src, 256), 256, 0, s>>>(dP, region);
-    return cudaGetLastError();
-}
 
 cudaError_t launch_consts_init(const SolveParams* dP, double t0, cudaStream_t s) {
     k_consts_init<<<1, 32, 0, s>>>(dP, t0);

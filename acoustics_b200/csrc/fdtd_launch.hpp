@@ -29,7 +29,6 @@ cudaError_t launch_batch_tail_any(int precision, const BatchLaunch& L, cudaStrea
 
 // fdtd_fp64.cu (compiled with -fmad=false)
 cudaError_t launch_prologue_fp64(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s);
-cudaError_t launch_source_factors(const SolveParams* dP, Box3 region, int n_src, long long cells, cudaStream_t s);
 cudaError_t launch_listener_prep(SolveParams* dP, int precision, int newp, int n_lis, cudaStream_t s);
 cudaError_t launch_consts_init(const SolveParams* dP, double t0, cudaStream_t s);
 cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int n_lis, double* out_row,

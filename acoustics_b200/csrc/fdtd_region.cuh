@@ -117,7 +117,7 @@ __device__ __forceinline__ void ghost_cells_body(const SolveParams& P, int cur, 
 
 // pNext += k * sum_s G_s(x, t + k/2) over the bounding box of the source
 // supports clipped to the non-PML box (GaussianPressureSource.cpp:6-30), with
-// G_s = (spatial factor, precomputed per reset) * (time factor of the step).
+// G_s = (product of the per-axis spatial factors) * (time factor of the step).
 template <typename T>
 __device__ __forceinline__ void sources_body(const SolveParams& P, int cur, const Box3& region, int bid, int nblocks) {
     const StepConsts& sc = P.consts[cur];
@@ -134,8 +134,7 @@ __device__ __forceinline__ void sources_body(const SolveParams& P, int cur, cons
         const int x = region.lo[0] + (int)(t / ((long long)nz * ny));
         const long long c = cidx(P, x, y, z);
         if (!(P.cls[c] & CLS_BULK)) continue;
-        double src = 0.0;
-        for (int s = 0; s < P.n_src; ++s) src += P.src_g[s * total + t] * sc.src_tf[s];
+        const double src = source_term(P, cur, x, y, z);
         if constexpr (sizeof(T) == 8) {
             pn[c] += src * P.k;
         } else {
