@@ -82,3 +82,31 @@ def test_box_mesh_classifies_like_the_analytic_box(fdtd_lib):
     assert np.array_equal(fa, fm)
     assert np.array_equal(ga, gm)
     assert rel_l2(ym, ya) <= TOL_FP64
+
+
+def test_mesh_members_in_batch_and_server(fdtd_lib):
+    """A static mesh scene batched with analytic ones, and served through the
+    solve server (which keeps its own copy of the mesh arrays): the series
+    equal a standalone solver's bit for bit."""
+    from acoustics_b200.batch import SolveBatch
+    from acoustics_b200.server import SolveServer
+    P32 = S.PRECISION_FP32_COMPENSATED
+    mesh = mesh_scene(False, steps=60)
+    rng = np.random.default_rng(11)
+    others = [S.random_scene(rng, 28, 48, 3, 4, 40, 80, f"a{i}", pml=6) for i in range(3)]
+
+    def alone(sc):
+        with PML_WaveSolver(sc, precision=P32) as g:
+            return g.step(sc.steps)
+
+    with SolveBatch([others[0], mesh, others[1]], precision=P32, graph_steps=8) as b:
+        b.run()
+        for m, sc in enumerate([others[0], mesh, others[1]]):
+            assert np.array_equal(b.output(m), alone(sc)), f"member {m}"
+    with SolveServer(precision=P32, graph_steps=8, chunk_steps=16) as srv:
+        ids = [srv.submit(others[2])]
+        im = srv.submit(mesh)
+        y, _ = srv.result(im)
+        for i in ids:
+            srv.result(i)
+    assert np.array_equal(y, alone(mesh))
