@@ -17,6 +17,9 @@
 // rotating pressure buffers, full-grid split pressures and face velocities,
 // the PML cell lists with cached coefficients, and the ghost-cell map keyed by
 // Szudzik's pairing.  Every function cites the reference file:line it follows.
+// Bodies are analytic primitives or closed triangle meshes; mesh queries scan
+// every triangle in index order (the library walks a hierarchy over the same
+// triangles and breaks ties the same way).
 // Compile with -ffp-contract=off so that no multiply-add is fused.
 
 #include "../include/fdtd_c.h"
