@@ -289,3 +289,17 @@ extern "C" fdtd_status fdtd_read_obj(const char* path, double scale, int32_t* n_
     if (triangles) std::memcpy(triangles, t.data(), t.size() * sizeof(int32_t));
     return FDTD_OK;
 }
+
+extern "C" fdtd_status fdtd_mesh_signed_distance(const fdtd_mesh_desc* mesh, int64_t n, const double* points,
+                                                 double* out) {
+    if (!mesh || n < 0 || (n > 0 && (!points || !out))) return FDTD_ERR_INVALID_ARG;
+    fdtd::MeshHost M;
+    std::string err;
+    if (!fdtd::build_mesh(*mesh, M, err)) {
+        fdtd::set_error(nullptr, err);
+        return FDTD_ERR_GEOMETRY;
+    }
+    const fdtd::MeshView v{M.nodes.data(), M.tris.data(), (int)M.nodes.size(), (int)M.tris.size()};
+    for (int64_t i = 0; i < n; ++i) out[i] = fdtd::mesh_sdf(v, points + 3 * i);
+    return FDTD_OK;
+}

@@ -452,6 +452,13 @@ void fdtd_scene_free(fdtd_scene* sc);
 fdtd_status fdtd_read_obj(const char* path, double scale, int32_t* n_vertices, int32_t* n_triangles,
                           double* vertices, int32_t* triangles);
 
+/* Signed distance (negative inside) of n points to a closed mesh, in the mesh's
+ * frame: the query the cell classification makes of mesh bodies (exact distance
+ * to the closest triangle point, sign of the closest feature's pseudo-normal),
+ * on the host.  FDTD_ERR_GEOMETRY for a mesh that is open or inconsistently
+ * oriented. */
+fdtd_status fdtd_mesh_signed_distance(const fdtd_mesh_desc* mesh, int64_t n, const double* points, double* out);
+
 /* all_audio.dat writer (AudioOutput, src/wavesolver/AudioOutput.cpp:27-64): appends
  * n_steps*n_listeners raw doubles. */
 fdtd_status fdtd_audio_append(const char* path, const double* data, int64_t count);

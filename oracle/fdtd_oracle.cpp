@@ -1479,6 +1479,14 @@ int oracle_set_threads(int n) {
 #endif
 }
 
+// Signed distance of n points to a mesh in its frame (OMesh::Sdf, every triangle).
+int oracle_mesh_sdf(const fdtd_mesh_desc* mesh, long long n, const double* points, double* out) {
+    OMesh m;
+    if (!mesh || !m.build(*mesh)) return FDTD_ERR_GEOMETRY;
+    for (long long i = 0; i < n; ++i) out[i] = m.Sdf(V3(points[3 * i], points[3 * i + 1], points[3 * i + 2]));
+    return 0;
+}
+
 int oracle_create(const fdtd_scene_desc* scene, void** out) {
     Oracle* o = new Oracle();
     const int st = o->init(scene);

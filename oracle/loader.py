@@ -52,6 +52,8 @@ def lib():
         L.oracle_set_threads.restype = C.c_int
         L.oracle_mls_c0.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_double)]
         L.oracle_mls_c0.restype = C.c_int
+        L.oracle_mesh_sdf.argtypes = [C.c_void_p, C.c_longlong, C.c_void_p, C.c_void_p]
+        L.oracle_mesh_sdf.restype = C.c_int
         _lib = L
     return _lib
 

@@ -150,3 +150,43 @@ def test_oracle_mesh_sphere_close_to_analytic(oracle_lib):
     # the icosphere lies inside the sphere: it is never solid where the sphere is not
     assert not np.any(solid_m & ~solid_a)
     assert (solid_a != solid_m).sum() < 0.02 * solid_a.sum()
+
+
+def _mesh_desc(m):
+    v = np.ascontiguousarray(np.asarray(m.vertices, dtype=np.float64).reshape(-1, 3))
+    t = np.ascontiguousarray(np.asarray(m.triangles, dtype=np.int32).reshape(-1, 3))
+    d = S.MeshDesc()
+    d.n_vertices, d.n_triangles = v.shape[0], t.shape[0]
+    d.vertices = v.ctypes.data_as(C.POINTER(C.c_double))
+    d.triangles = t.ctypes.data_as(C.POINTER(C.c_int32))
+    return d, (v, t)
+
+
+@pytest.mark.parametrize("shape", ["icosphere", "box"])
+def test_mesh_distance_hierarchy_equals_brute_force(fdtd_lib, oracle_lib, shape):
+    """The library's hierarchy walk (pruning, nearer child first, ties to the
+    lowest triangle index) returns the oracle's every-triangle scan bit for bit:
+    random points around the body, its vertices and its edge midpoints."""
+    from oracle.loader import lib as olib
+    m = S.icosphere(0.03, 3) if shape == "icosphere" else S.box_mesh((0.02, 0.011, 0.015))
+    rng = np.random.default_rng(3)
+    ext = np.abs(m.vertices).max(axis=0)
+    pts = [rng.uniform(-1.6 * ext, 1.6 * ext, size=(20000, 3)), m.vertices,
+           0.5 * (m.vertices[m.triangles[:, 0]] + m.vertices[m.triangles[:, 1]])]
+    pts = np.ascontiguousarray(np.concatenate(pts))
+    desc, keep = _mesh_desc(m)
+    a = np.zeros(len(pts))
+    b = np.zeros(len(pts))
+    assert fdtd_lib.fdtd_mesh_signed_distance(C.byref(desc), len(pts), pts.ctypes.data, a.ctypes.data) == 0
+    assert olib().oracle_mesh_sdf(C.byref(desc), len(pts), pts.ctypes.data, b.ctypes.data) == 0
+    assert np.array_equal(a, b)
+    if shape == "icosphere":  # inscribed polyhedron: within the facet depth of the sphere's distance
+        r = np.linalg.norm(pts[:20000], axis=1) - 0.03
+        assert np.all(np.abs(a[:20000] - r) < 0.03 * 0.01)
+        assert np.all(np.sign(a[:20000][np.abs(r) > 1e-3]) == np.sign(r[np.abs(r) > 1e-3]))
+    else:  # a box mesh is exact: the analytic box distance
+        half = np.array([0.02, 0.011, 0.015])
+        q = np.abs(pts[:20000]) - half
+        out = np.linalg.norm(np.maximum(q, 0.0), axis=1)
+        inn = np.minimum(q.max(axis=1), 0.0)
+        assert np.allclose(a[:20000], out + inn, rtol=0, atol=1e-15)
