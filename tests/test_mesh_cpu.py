@@ -190,3 +190,46 @@ def test_mesh_distance_hierarchy_equals_brute_force(fdtd_lib, oracle_lib, shape)
         out = np.linalg.norm(np.maximum(q, 0.0), axis=1)
         inn = np.minimum(q.max(axis=1), 0.0)
         assert np.allclose(a[:20000], out + inn, rtol=0, atol=1e-15)
+
+
+def l_prism(scale=0.01):
+    """Closed extruded L (the union of the boxes [0,2]x[0,1]x[0,1] and
+    [0,1]x[0,2]x[0,1], times `scale`): a body with concave edges and vertices."""
+    poly = [(0, 0), (2, 0), (2, 1), (1, 1), (1, 2), (0, 2)]  # counter-clockwise from +z
+    n = len(poly)
+    V = [(x, y, 0.0) for x, y in poly] + [(x, y, 1.0) for x, y in poly]
+    T = []
+    for a, b, c in [(0, 1, 2), (0, 2, 3), (0, 3, 4), (0, 4, 5)]:  # star-shaped from vertex 0
+        T.append((n + a, n + b, n + c))  # top, normal +z
+        T.append((a, c, b))              # bottom, normal -z
+    for i in range(n):
+        j = (i + 1) % n
+        T += [(i, j, n + j), (i, n + j, n + i)]
+    return S.TriangleMesh(np.asarray(V) * scale, np.asarray(T, dtype=np.int32))
+
+
+def test_concave_mesh_signs_and_distances(fdtd_lib, oracle_lib):
+    """Signs at concave edges and vertices (pseudo-normals), and exterior
+    distances, against the L's closed form; library and oracle equal."""
+    from oracle.loader import lib as olib
+    m = l_prism(0.01)
+    rng = np.random.default_rng(4)
+    p = np.ascontiguousarray(rng.uniform(-0.01, 0.03, size=(40000, 3)))
+    desc, keep = _mesh_desc(m)
+    a = np.zeros(len(p))
+    b = np.zeros(len(p))
+    assert fdtd_lib.fdtd_mesh_signed_distance(C.byref(desc), len(p), p.ctypes.data, a.ctypes.data) == 0
+    assert olib().oracle_mesh_sdf(C.byref(desc), len(p), p.ctypes.data, b.ctypes.data) == 0
+    assert np.array_equal(a, b)
+
+    def box_dist(q, lo, hi):
+        d = np.maximum(np.maximum(lo - q, q - hi), 0.0)
+        return np.linalg.norm(d, axis=1)
+    d1 = box_dist(p, np.array([0, 0, 0.0]), np.array([0.02, 0.01, 0.01]))
+    d2 = box_dist(p, np.array([0, 0, 0.0]), np.array([0.01, 0.02, 0.01]))
+    inside = (d1 == 0) | (d2 == 0)
+    outside = np.minimum(d1, d2)
+    clear = (outside > 1e-9) | inside
+    assert np.all(a[inside & (np.abs(a) > 1e-12)] < 0)
+    assert np.all(a[~inside] > 0)
+    assert np.allclose(a[~inside & clear], outside[~inside & clear], rtol=0, atol=1e-15)
