@@ -324,15 +324,32 @@ extern "C" {
 fdtd_status fdtd_solver_step(fdtd_solver* s, int32_t n_steps, double* listener_out) {
     if (!s || n_steps < 0) return (set_error(s, "invalid arguments"), FDTD_ERR_INVALID_ARG);
     const int L = s->L;
+    // rows of consecutive chunks gather in the pinned staging buffer (copies in
+    // stream order, before the next chunk rewrites the device ring); the host
+    // waits only when the buffer is full and at the end
+    int staged = 0, staged_first = 0;
+    auto flush = [&]() -> fdtd_status {
+        if (staged == 0) return FDTD_OK;
+        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+        std::memcpy(listener_out + (size_t)staged_first * L, s->h_lis_stage, (size_t)staged * L * 8);
+        staged = 0;
+        return FDTD_OK;
+    };
     fdtd_status st = run_steps(s, n_steps, [&](int first, int count) -> fdtd_status {
         if (listener_out && L > 0) {
-            CUDA_TRY(s, cudaMemcpyAsync(s->h_lis_stage, s->d_lis, (size_t)count * L * 8, cudaMemcpyDeviceToHost,
-                                        s->stream));
-            CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-            std::memcpy(listener_out + (size_t)first * L, s->h_lis_stage, (size_t)count * L * 8);
+            if (staged + count > s->lis_cap_steps) {
+                const fdtd_status f = flush();
+                if (f != FDTD_OK) return f;
+            }
+            if (staged == 0) staged_first = first;
+            CUDA_TRY(s, cudaMemcpyAsync(s->h_lis_stage + (size_t)staged * L, s->d_lis, (size_t)count * L * 8,
+                                        cudaMemcpyDeviceToHost, s->stream));
+            staged += count;
         }
         return FDTD_OK;
     });
+    if (st != FDTD_OK) return st;
+    st = flush();
     if (st != FDTD_OK) return st;
     st = check_device_errors(s);
     if (st != FDTD_OK) return st;

@@ -344,7 +344,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=20)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp64", "fp64-plain"])
-    ap.add_argument("--graph-steps", type=int, default=50)
+    ap.add_argument("--graph-steps", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
     ap.add_argument("--accuracy-steps", type=int, default=4000)
