@@ -232,14 +232,14 @@ struct Carver {
 };
 
 fdtd_status upload_params(fdtd_solver* s) {
-    CUDA_TRY(s, cudaMemcpyAsync(s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, fdtd::counted_copyAsync(s, s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice, s->stream));
     return FDTD_OK;
 }
 
 fdtd_status run_classification(fdtd_solver* s) {
     ClsBoxes& B = s->hP.boxes;
     classification_boxes(s, B);
-    CUDA_TRY(s, cudaMemcpyAsync(&s->dP->boxes, &B, sizeof(ClsBoxes), cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, fdtd::counted_copyAsync(s, &s->dP->boxes, &B, sizeof(ClsBoxes), cudaMemcpyHostToDevice, s->stream));
     CUDA_TRY(s, launch_classify(s->dP, s->N, B, false, s->stream));
     s->cls_boxes_current = true;
     s->launches += B.ufirst[B.n] > 0 ? 3 : 2;
@@ -732,8 +732,8 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         CUDA_TRY(nullptr, cudaMalloc(&d, nb + tb));
         s->mesh_alloc.push_back(d);
         s->arena_bytes += nb + tb;
-        CUDA_TRY(nullptr, cudaMemcpy(d, M.nodes.data(), nb, cudaMemcpyHostToDevice));
-        CUDA_TRY(nullptr, cudaMemcpy((char*)d + nb, M.tris.data(), tb, cudaMemcpyHostToDevice));
+        CUDA_TRY(nullptr, fdtd::counted_copy(s.get(), d, M.nodes.data(), nb, cudaMemcpyHostToDevice));
+        CUDA_TRY(nullptr, fdtd::counted_copy(s.get(), (char*)d + nb, M.tris.data(), tb, cudaMemcpyHostToDevice));
         const MeshView v{(const MeshNode*)d, (const MeshTri*)((char*)d + nb), (int)M.nodes.size(), (int)M.tris.size()};
         for (auto& o : s->objs)
             if (o.d.shape == FDTD_SHAPE_MESH && o.d.mesh == (int)m) o.mview = v;
@@ -808,25 +808,25 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
                     g[i * N[d] + x] = v;
                 }
             }
-            CUDA_TRY(s.get(), cudaMemcpy((void*)P.src_ax[d], g.data(), g.size() * 8, cudaMemcpyHostToDevice));
+            CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.src_ax[d], g.data(), g.size() * 8, cudaMemcpyHostToDevice));
         }
     // tables
     for (int d = 0; d < 3; ++d) {
         auto& T = s->tab[d];
         std::vector<float> f1(T.pupd.begin(), T.pupd.end()), f2(T.pdiv.begin(), T.pdiv.end());
         std::vector<float> f3(T.vupd.begin(), T.vupd.end()), f4(T.vgrad.begin(), T.vgrad.end());
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pml_cell[d], T.pml_cell.data(), N[d], cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pml_face[d], T.pml_face.data(), N[d] + 1, cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.cpos[d], T.cpos.data(), N[d] * 8, cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.fpos[d], T.fpos.data(), (N[d] + 1) * 8, cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pupd[d], T.pupd.data(), N[d] * 8, cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pdiv[d], T.pdiv.data(), N[d] * 8, cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.vupd[d], T.vupd.data(), (N[d] + 1) * 8, cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.vgrad[d], T.vgrad.data(), (N[d] + 1) * 8, cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pupd_f[d], f1.data(), N[d] * 4, cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.pdiv_f[d], f2.data(), N[d] * 4, cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.vupd_f[d], f3.data(), (N[d] + 1) * 4, cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.vgrad_f[d], f4.data(), (N[d] + 1) * 4, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.pml_cell[d], T.pml_cell.data(), N[d], cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.pml_face[d], T.pml_face.data(), N[d] + 1, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.cpos[d], T.cpos.data(), N[d] * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.fpos[d], T.fpos.data(), (N[d] + 1) * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.pupd[d], T.pupd.data(), N[d] * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.pdiv[d], T.pdiv.data(), N[d] * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.vupd[d], T.vupd.data(), (N[d] + 1) * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.vgrad[d], T.vgrad.data(), (N[d] + 1) * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.pupd_f[d], f1.data(), N[d] * 4, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.pdiv_f[d], f2.data(), N[d] * 4, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.vupd_f[d], f3.data(), (N[d] + 1) * 4, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.vgrad_f[d], f4.data(), (N[d] + 1) * 4, cudaMemcpyHostToDevice));
         // packed flags and coefficient quads of the shell kernel
         std::vector<uint8_t> fl(N[d] + 8, 0);
         std::vector<AxisCoef<double>> cd(N[d] + 8, AxisCoef<double>{0.0, 0.0, 0.0, 0.0});
@@ -851,12 +851,12 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
             cf[i].pupd = (float)cd[i].pupd;
             cf[i].pdiv = (float)cd[i].pdiv;
         }
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.axflag[d], fl.data(), fl.size(), cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.coef_d[d], cd.data(), cd.size() * sizeof(cd[0]), cudaMemcpyHostToDevice));
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.coef_f[d], cf.data(), cf.size() * sizeof(cf[0]), cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.axflag[d], fl.data(), fl.size(), cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.coef_d[d], cd.data(), cd.size() * sizeof(cd[0]), cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.coef_f[d], cf.data(), cf.size() * sizeof(cf[0]), cudaMemcpyHostToDevice));
     }
     if (s->L > 0)
-        CUDA_TRY(s.get(), cudaMemcpy((void*)P.listeners, s->listeners.data(), s->listeners.size() * 8, cudaMemcpyHostToDevice));
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.listeners, s->listeners.data(), s->listeners.size() * 8, cudaMemcpyHostToDevice));
     CUDA_TRY(s.get(), cudaMallocHost((void**)&s->h_lis_stage, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8));
     s->xb = (o.x_chunk == 2 || o.x_chunk == 4 || o.x_chunk == 8) ? o.x_chunk : 2;
     s->region.xb = s->xb;
@@ -953,7 +953,7 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     int n_solid = 0;
     CUDA_TRY(s, cudaMemsetAsync(d_count, 0, sizeof(int), s->stream));
     CUDA_TRY(s, launch_cls_history(s->dP, s->ncell, d_count, nullptr, 0, s->stream));
-    CUDA_TRY(s, cudaMemcpyAsync(&n_solid, d_count, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, fdtd::counted_copyAsync(s, &n_solid, d_count, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     if (s->d_solid_pml) {
         cudaFree(s->d_solid_pml);

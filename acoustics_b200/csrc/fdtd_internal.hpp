@@ -110,10 +110,28 @@ struct fdtd_solver {
     long long launches = 0;
     long long last_launches = 0;
     long long graph_launches_per_exec = 0;
+    // bytes this handle copied between host and device memory since creation
+    long long bytes_h2d = 0, bytes_d2h = 0;
     std::string err;
 };
 
 namespace fdtd {
+// Host<->device copies of a solver handle, added to its transfer totals
+// (fdtd_solver_transfer_bytes); s may be NULL.
+inline void count_transfer(fdtd_solver* s, size_t n, cudaMemcpyKind kind) {
+    if (!s) return;
+    if (kind == cudaMemcpyHostToDevice) s->bytes_h2d += (long long)n;
+    else if (kind == cudaMemcpyDeviceToHost) s->bytes_d2h += (long long)n;
+}
+inline cudaError_t counted_copy(fdtd_solver* s, void* dst, const void* src, size_t n, cudaMemcpyKind kind) {
+    count_transfer(s, n, kind);
+    return cudaMemcpy(dst, src, n, kind);
+}
+inline cudaError_t counted_copyAsync(fdtd_solver* s, void* dst, const void* src, size_t n, cudaMemcpyKind kind,
+                                     cudaStream_t stream) {
+    count_transfer(s, n, kind);
+    return cudaMemcpyAsync(dst, src, n, kind, stream);
+}
 void set_error(fdtd_solver* s, const std::string& msg);
 fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc);
 void classification_boxes(const fdtd_solver* s, ClsBoxes& B);

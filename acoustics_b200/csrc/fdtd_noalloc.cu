@@ -1,15 +1,13 @@
 // fdtd_noalloc.cu — an interior leapfrog step that allocates no memory.
 //
 // Some callers cannot call cudaMalloc at the point where they step the field:
-// code that is being captured into a CUDA graph (an allocation is not a
-// capturable operation and invalidates the capture), real-time audio callbacks
-// that must not block on the allocator or on the implicit device
-// synchronisation cudaMalloc may perform, and host applications whose memory
-// pool already owns the GPU's free memory so that an extra allocation fails.
-// This entry point serves them: the caller passes the pressure buffers, and the
-// Laplacian scratch of the plain (one kernel per phase) path lives in a
-// file-scope __device__ array of FDTD_NOALLOC_MAX_CELLS doubles that every GPU
-// loading the library keeps until the process exits.
+// real-time audio callbacks that must not block on the allocator or on the
+// device synchronisation an allocation may imply, and host applications whose
+// own memory pool already owns the GPU's free memory, so that one more
+// allocation fails.  This entry point serves them: the caller passes the
+// pressure buffers, and the Laplacian scratch of the plain (one kernel per
+// phase) path lives in a file-scope __device__ array of FDTD_NOALLOC_MAX_CELLS
+// doubles that every GPU loading the library keeps until the process exits.
 //
 // It is a variant of the plain FP64 path's Laplacian and pressure kernels
 // (MAC_Grid::pressureFieldLaplacianGhostCell, MAC_Grid.cpp:187-299, and the
@@ -34,7 +32,13 @@ __device__ __align__(256) double g_noalloc_lap[FDTD_NOALLOC_MAX_CELLS];
 
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
-double* g_scratch[kMaxDevices] = {nullptr};
+// The scratch address per device, with the context it was looked up in: a new
+// primary context (after cudaDeviceReset) may place the array elsewhere.
+struct ScratchEntry {
+    void* ctx = nullptr;
+    double* ptr = nullptr;
+};
+ScratchEntry g_scratch[kMaxDevices];
 fdtd_status fail(fdtd_status st, const std::string& msg) {
     fdtd::set_error(nullptr, msg);  // readable through fdtd_last_error()
     return st;
@@ -72,22 +76,46 @@ __global__ void k_noalloc_update(const double* __restrict__ pc, const double* pl
     }
 }
 
-// Set-up, once per device and with that device current: the device address of
-// the scratch array (its name in host code is only a host-side stand-in).
+// The current context (CUcontext) through the driver entry point that the
+// runtime exposes; NULL when the driver does not provide it.
+void* current_context() {
+    using GetCurrent = int (*)(void**);  // CUresult cuCtxGetCurrent(CUcontext*)
+    static GetCurrent fn = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &f, 12000, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            f = nullptr;
+        return reinterpret_cast<GetCurrent>(f);
+    }();
+    void* ctx = nullptr;
+    if (!fn || fn(&ctx) != 0) return nullptr;
+    return ctx;
+}
+
+// Set-up, once per device and context, with that device current: the device
+// address of the scratch array (its name in host code is only a host-side
+// stand-in).
 fdtd_status scratch_for_current_device(double** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
     if (dev < 0 || dev >= kMaxDevices) return fail(FDTD_ERR_INVALID_ARG, "device ordinal beyond 63");
+    // makes the device's primary context current (creating it if needed)
+    e = cudaSetDevice(dev);
+    if (e != cudaSuccess) return fail(FDTD_ERR_CUDA, std::string("cudaSetDevice: ") + cudaGetErrorString(e));
+    void* ctx = current_context();
     std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_scratch[dev]) {
+    ScratchEntry& ent = g_scratch[dev];
+    if (!ent.ptr || !ctx || ent.ctx != ctx) {
         void* ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_noalloc_lap);
         if (e != cudaSuccess || !ptr)
             return fail(FDTD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-        g_scratch[dev] = static_cast<double*>(ptr);
+        ent.ptr = static_cast<double*>(ptr);
+        ent.ctx = ctx;
     }
-    *out = g_scratch[dev];
+    *out = ent.ptr;
     return FDTD_OK;
 }
 

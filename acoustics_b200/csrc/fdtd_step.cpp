@@ -31,7 +31,7 @@ namespace {
 void classification_launches(fdtd_solver* s, fdtd_status& st) {
     const ClsBoxes& B = s->hP.boxes;
     // pageable source: the copy is staged before the call returns
-    cudaError_t e = cudaMemcpyAsync(&s->dP->boxes, &B, sizeof(ClsBoxes), cudaMemcpyHostToDevice, s->stream);
+    cudaError_t e = fdtd::counted_copyAsync(s, &s->dP->boxes, &B, sizeof(ClsBoxes), cudaMemcpyHostToDevice, s->stream);
     if (e == cudaSuccess) e = launch_classify(s->dP, s->N, B, s->moving, s->stream);
     s->launches += B.ufirst[B.n] > 0 ? 3 : 2;
     if (e != cudaSuccess) {
@@ -203,7 +203,7 @@ fdtd_status after_step(fdtd_solver* s) {
             host_update_bbox(o);
         }
         to_dev_objects(s);
-        CUDA_TRY(s, cudaMemcpyAsync(&s->dP->obj[0], &s->hP.obj[0], sizeof(DevObject) * s->objs.size(),
+        CUDA_TRY(s, fdtd::counted_copyAsync(s, &s->dP->obj[0], &s->hP.obj[0], sizeof(DevObject) * s->objs.size(),
                                     cudaMemcpyHostToDevice, s->stream));
     }
     return FDTD_OK;
@@ -212,11 +212,11 @@ fdtd_status after_step(fdtd_solver* s) {
 fdtd_status check_device_errors(fdtd_solver* s) {
     int dev_error = 0;
     int status[4] = {0, 0, 0, 0};
-    CUDA_TRY(s, cudaMemcpyAsync(&dev_error, s->hP.dev_error, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
-    CUDA_TRY(s, cudaMemcpyAsync(status, s->d_status, sizeof(status), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, fdtd::counted_copyAsync(s, &dev_error, s->hP.dev_error, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, fdtd::counted_copyAsync(s, status, s->d_status, sizeof(status), cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     int ghosts = 0;
-    CUDA_TRY(s, cudaMemcpy(&ghosts, s->d_ghost_count, sizeof(int), cudaMemcpyDeviceToHost));
+    CUDA_TRY(s, fdtd::counted_copy(s, &ghosts, s->d_ghost_count, sizeof(int), cudaMemcpyDeviceToHost));
     if (ghosts > s->region.ghost_cap) {
         set_error(s, "ghost-neighbour list overflow (" + std::to_string(ghosts) + " > " +
                          std::to_string(s->region.ghost_cap) + ")");
@@ -342,7 +342,7 @@ fdtd_status fdtd_solver_step(fdtd_solver* s, int32_t n_steps, double* listener_o
                 if (f != FDTD_OK) return f;
             }
             if (staged == 0) staged_first = first;
-            CUDA_TRY(s, cudaMemcpyAsync(s->h_lis_stage + (size_t)staged * L, s->d_lis, (size_t)count * L * 8,
+            CUDA_TRY(s, fdtd::counted_copyAsync(s, s->h_lis_stage + (size_t)staged * L, s->d_lis, (size_t)count * L * 8,
                                         cudaMemcpyDeviceToHost, s->stream));
             staged += count;
         }
@@ -363,7 +363,7 @@ fdtd_status fdtd_solver_step_device(fdtd_solver* s, int32_t n_steps, void* devic
     double* out = (double*)device_listener_out;
     fdtd_status st = run_steps(s, n_steps, [&](int first, int count) -> fdtd_status {
         if (out && L > 0)
-            CUDA_TRY(s, cudaMemcpyAsync(out + (size_t)first * L, s->d_lis, (size_t)count * L * 8,
+            CUDA_TRY(s, fdtd::counted_copyAsync(s, out + (size_t)first * L, s->d_lis, (size_t)count * L * 8,
                                         cudaMemcpyDeviceToDevice, s->stream));
         return FDTD_OK;
     });
@@ -375,7 +375,7 @@ fdtd_status fdtd_solver_fetch_listeners(fdtd_solver* s, double* out) {
     if (s->L == 0) return FDTD_OK;
     CUDA_TRY(s, cudaSetDevice(s->opt.device));
     CUDA_TRY(s, launch_listeners(s->dP, s->precision, s->cur, s->L, s->d_lis, s->stream));
-    CUDA_TRY(s, cudaMemcpyAsync(out, s->d_lis, (size_t)s->L * 8, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, fdtd::counted_copyAsync(s, out, s->d_lis, (size_t)s->L * 8, cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     return FDTD_OK;
 }
@@ -439,6 +439,13 @@ int64_t fdtd_solver_last_launch_count(fdtd_solver* s) { return s ? s->last_launc
 
 int64_t fdtd_solver_overlapped_steps(fdtd_solver* s) { return s ? s->overlapped_steps : 0; }
 
+fdtd_status fdtd_solver_transfer_bytes(fdtd_solver* s, int64_t* host_to_device, int64_t* device_to_host) {
+    if (!s || !host_to_device || !device_to_host) return (set_error(s, "invalid arguments"), FDTD_ERR_INVALID_ARG);
+    *host_to_device = s->bytes_h2d;
+    *device_to_host = s->bytes_d2h;
+    return FDTD_OK;
+}
+
 fdtd_status fdtd_solver_prepare_graphs(fdtd_solver* s) {
     if (!s) return FDTD_ERR_INVALID_ARG;
     const int G = s->opt.graph_steps;
@@ -480,8 +487,8 @@ fdtd_status fdtd_solver_get_classification(fdtd_solver* s, uint8_t* flags, fdtd_
     if (!s) return FDTD_ERR_INVALID_ARG;
     CUDA_TRY(s, cudaSetDevice(s->opt.device));
     std::vector<uint8_t> pcls(s->np), pgobj(s->np);
-    CUDA_TRY(s, cudaMemcpyAsync(pcls.data(), s->hP.cls, s->np, cudaMemcpyDeviceToHost, s->stream));
-    CUDA_TRY(s, cudaMemcpyAsync(pgobj.data(), s->hP.gobj, s->np, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, fdtd::counted_copyAsync(s, pcls.data(), s->hP.cls, s->np, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, fdtd::counted_copyAsync(s, pgobj.data(), s->hP.gobj, s->np, cudaMemcpyDeviceToHost, s->stream));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     // dense (reference) order and indices
     std::vector<uint8_t> cls(s->ncell), gobj(s->ncell);
@@ -576,11 +583,11 @@ fdtd_status field_transfer(fdtd_solver* s, int32_t which, double* dense, int64_t
     const long long np = s->np;
     std::vector<char> raw(np * w);
     std::vector<float> inc;
-    CUDA_TRY(s, cudaMemcpyAsync(raw.data(), src, np * w, cudaMemcpyDeviceToHost, s->stream));
+    CUDA_TRY(s, fdtd::counted_copyAsync(s, raw.data(), src, np * w, cudaMemcpyDeviceToHost, s->stream));
     const bool fp32_prev = !f64 && which == FDTD_FIELD_PRESSURE_PREV;
     if (fp32_prev) {
         inc.resize(np);
-        CUDA_TRY(s, cudaMemcpyAsync(inc.data(), P.dinc, np * 4, cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(s, fdtd::counted_copyAsync(s, inc.data(), P.dinc, np * 4, cudaMemcpyDeviceToHost, s->stream));
     }
     // the z-slab box keeps its PML state in compact arrays (ShellBoxes)
     const ShellBoxes& B = s->shell;
@@ -590,7 +597,7 @@ fdtd_status field_transfer(fdtd_solver* s, int32_t which, double* dense, int64_t
     if (zc) {
         zsrc = which <= FDTD_FIELD_PML_PZ ? P.zpd[which - FDTD_FIELD_PML_PX] : P.zv[vbuf][which - FDTD_FIELD_VX];
         zraw.resize(P.zcount * w);
-        CUDA_TRY(s, cudaMemcpyAsync(zraw.data(), zsrc, P.zcount * w, cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(s, fdtd::counted_copyAsync(s, zraw.data(), zsrc, P.zcount * w, cudaMemcpyDeviceToHost, s->stream));
     }
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     // every (padded grid index, compact index) pair of the z-slab box
@@ -642,11 +649,11 @@ fdtd_status field_transfer(fdtd_solver* s, int32_t which, double* dense, int64_t
                 else r32[c] = (float)dense[o];
             }
     if (fp32_prev) {
-        CUDA_TRY(s, cudaMemcpyAsync(P.dinc, inc.data(), np * 4, cudaMemcpyHostToDevice, s->stream));
+        CUDA_TRY(s, fdtd::counted_copyAsync(s, P.dinc, inc.data(), np * 4, cudaMemcpyHostToDevice, s->stream));
     } else {
         if (zc) for_compact([&](long long c, long long q) { std::memcpy(zraw.data() + q * w, raw.data() + c * w, w); });
-        CUDA_TRY(s, cudaMemcpyAsync(src, raw.data(), np * w, cudaMemcpyHostToDevice, s->stream));
-        if (zc) CUDA_TRY(s, cudaMemcpyAsync(zsrc, zraw.data(), P.zcount * w, cudaMemcpyHostToDevice, s->stream));
+        CUDA_TRY(s, fdtd::counted_copyAsync(s, src, raw.data(), np * w, cudaMemcpyHostToDevice, s->stream));
+        if (zc) CUDA_TRY(s, fdtd::counted_copyAsync(s, zsrc, zraw.data(), P.zcount * w, cudaMemcpyHostToDevice, s->stream));
     }
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     return FDTD_OK;
@@ -724,7 +731,7 @@ fdtd_status fdtd_solver_snapshot(fdtd_solver* s, void* buffer, int64_t* bytes) {
     std::memcpy(p, s->objs.data(), s->objs.size() * sizeof(HostObject));
     p += s->objs.size() * sizeof(HostObject);
     for (auto& r : regs) {
-        CUDA_TRY(s, cudaMemcpyAsync(p, r.first, r.second, cudaMemcpyDeviceToHost, s->stream));
+        CUDA_TRY(s, fdtd::counted_copyAsync(s, p, r.first, r.second, cudaMemcpyDeviceToHost, s->stream));
         p += r.second;
     }
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
@@ -750,7 +757,7 @@ fdtd_status fdtd_solver_restore(fdtd_solver* s, const void* buffer, int64_t byte
     std::memcpy(s->objs.data(), p, s->objs.size() * sizeof(HostObject));
     p += s->objs.size() * sizeof(HostObject);
     for (auto& r : regs) {
-        CUDA_TRY(s, cudaMemcpy(r.first, p, r.second, cudaMemcpyHostToDevice));
+        CUDA_TRY(s, fdtd::counted_copy(s, r.first, p, r.second, cudaMemcpyHostToDevice));
         p += r.second;
     }
     s->cur = h.cur;
@@ -759,7 +766,7 @@ fdtd_status fdtd_solver_restore(fdtd_solver* s, const void* buffer, int64_t byte
     s->state_time = h.state_time;
     s->cls_boxes_current = false;  // the flags came from the snapshot, not from hP.boxes
     to_dev_objects(s);
-    CUDA_TRY(s, cudaMemcpy(s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice));
+    CUDA_TRY(s, fdtd::counted_copy(s, s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice));
     return FDTD_OK;
 }
 

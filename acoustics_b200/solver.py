@@ -103,6 +103,12 @@ class PML_WaveSolver:
         (moving bodies clear of the PML); execution statistics only."""
         return int(self._L.fdtd_solver_overlapped_steps(self._h))
 
+    def transfer_bytes(self):
+        """(host-to-device, device-to-host) bytes this solve has copied since creation."""
+        a, b = C.c_int64(0), C.c_int64(0)
+        check(self._L.fdtd_solver_transfer_bytes(self._h, C.byref(a), C.byref(b)), self._h)
+        return int(a.value), int(b.value)
+
     def prepare_graphs(self):
         """Capture the CUDA graph of the next graph_steps-long chunk now (nothing runs)."""
         check(self._L.fdtd_solver_prepare_graphs(self._h), self._h)

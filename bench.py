@@ -247,40 +247,42 @@ def bench_batched(peak: float, fp64_check: bool = True):
     return out
 
 
-def bench_moving(peak: float, steps: int = 300):
-    """Configuration 5: 384x384x256, two ballistic spheres that meet mid-run, every
-    step reclassified (solid / ghost cells, fresh-cell MLS), FP32 compensated and
-    FP64, CUDA-event time of `steps` steps from the 50th (the spheres move through
-    the grid all along)."""
+def bench_moving(peak: float):
+    """Configuration 5: 384x384x256, two ballistic spheres that touch mid-run,
+    every step reclassified (solid / ghost cells, fresh-cell MLS); the whole
+    6000-step run from creation, FP32 compensated and FP64, CUDA-event time on
+    the solver stream.  The FP32 listener series is checked against FP64."""
     import torch
 
     from acoustics_b200 import scene as S
     from acoustics_b200.solver import PML_WaveSolver
     sc = S.config5()
     out = {"workload": "config5: 384x384x256 moving spheres, per-step reclassification", "cells": sc.n_cells,
-           "steps": steps}
+           "steps": sc.steps}
+    ys = {}
     for name, prec in (("fp32", S.PRECISION_FP32_COMPENSATED), ("fp64", S.PRECISION_FP64)):
         g = PML_WaveSolver(sc, precision=prec)
-        g.step(50)
         g.synchronize()
         ext = torch.cuda.ExternalStream(g.stream)
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         a.record(ext)
-        g.step(steps)
+        ys[name] = g.step(sc.steps)
         b.record(ext)
         b.synchronize()
-        ms = a.elapsed_time(b) / steps
+        ms = a.elapsed_time(b) / sc.steps
         alg = float(g.info().algorithmic_bytes_per_step)
         out[name] = {"ms_per_step": ms, "gcell_steps_s": sc.n_cells / (ms / 1e3) / 1e9,
-                     "hbm_frac": alg / (ms / 1e3) / 1e9 / peak}
+                     "hbm_frac": alg / (ms / 1e3) / 1e9 / peak, "overlapped_steps": g.overlapped_steps()}
         g.close()
+    out["fp32_listener_rel_l2_vs_fp64"] = float(np.linalg.norm(ys["fp32"] - ys["fp64"]) / np.linalg.norm(ys["fp64"]))
     return out
 
 
-def bench_served(peak: float, rate: float, n_requests: int, fifo_baseline: bool = True):
+def bench_served(peak: float, rate: float, n_requests: int, fifo_plain: bool = False):
     """Poisson request stream (config4) into the solve server (FP32, continuous
-    batching) and, as the baseline, served first-in first-out by the plain FP64
-    GPU path (one kernel per reference phase), one request at a time."""
+    batching) and, as the baseline, the same requests served first-in first-out
+    one at a time by the plain FP64 GPU single-solve path (fused kernels, graphs);
+    optionally also by the phased FP64 path (one kernel per reference phase)."""
     from acoustics_b200 import scene as S
     from acoustics_b200.batch import scene_info
     from acoustics_b200.server import SolveServer
@@ -312,28 +314,31 @@ def bench_served(peak: float, rate: float, n_requests: int, fifo_baseline: bool 
                 "span_s": st["span_s"], "peak_members": st["peak_members"],
                 "peak_device_gb": st["peak_device_bytes"] / 1e9}
 
-    base = serve(1.0)
-    base.pop("rate_per_s")
-    out.update(base)
-    # faster arrivals until the GPU, not the stream, sets the pace
-    out["rate_sweep"] = [serve(f) for f in (4.0, 16.0)]
-    if fifo_baseline:
+    def fifo(kernel, graph_steps):
         t0 = time.perf_counter()
         lat64 = []
         for t_arr, sc in reqs:
             d = t0 + t_arr - time.perf_counter()
             if d > 0:
                 time.sleep(d)
-            g = PML_WaveSolver(sc, precision=S.PRECISION_FP64, kernel=S.KERNEL_PHASED)
+            g = PML_WaveSolver(sc, precision=S.PRECISION_FP64, kernel=kernel, graph_steps=graph_steps)
             g.step(sc.steps)
             g.close()
             lat64.append(time.perf_counter() - (t0 + t_arr))
         span = time.perf_counter() - (t0 + reqs[0][0])
-        out["fifo_fp64_plain"] = {"p50_latency_s": float(np.percentile(lat64, 50)),
-                                  "p99_latency_s": float(np.percentile(lat64, 99)),
-                                  "solves_per_s": n_requests / span, "gcell_steps_s": cell_steps / span / 1e9}
-        out["solves_per_s_vs_fifo_fp64"] = out["solves_per_s"] / out["fifo_fp64_plain"]["solves_per_s"]
-        out["p99_vs_fifo_fp64"] = out["p99_latency_s"] / out["fifo_fp64_plain"]["p99_latency_s"]
+        return {"p50_latency_s": float(np.percentile(lat64, 50)), "p99_latency_s": float(np.percentile(lat64, 99)),
+                "solves_per_s": n_requests / span, "gcell_steps_s": cell_steps / span / 1e9}
+
+    base = serve(1.0)
+    base.pop("rate_per_s")
+    out.update(base)
+    # faster arrivals until the GPU, not the stream, sets the pace
+    out["rate_sweep"] = [serve(f) for f in (4.0, 16.0)]
+    out["fifo_fp64_fused"] = fifo(S.KERNEL_FUSED, 16)
+    out["solves_per_s_vs_fifo_fp64_fused"] = out["solves_per_s"] / out["fifo_fp64_fused"]["solves_per_s"]
+    out["p99_vs_fifo_fp64_fused"] = out["p99_latency_s"] / out["fifo_fp64_fused"]["p99_latency_s"]
+    if fifo_plain:
+        out["fifo_fp64_plain"] = fifo(S.KERNEL_PHASED, 0)
     return out
 
 
@@ -347,7 +352,8 @@ def main():
     ap.add_argument("--graph-steps", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-variants", action="store_true")
-    ap.add_argument("--accuracy-steps", type=int, default=4000)
+    ap.add_argument("--fifo-plain", action="store_true",
+                    help="also serve the request stream FIFO on the phased FP64 path (one kernel per phase)")
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--profile", action="store_true", help="only run --steps steps of the bench solve (for ncu)")
     ap.add_argument("--profile-n", type=int, default=256, help="grid edge of the --profile solve")
@@ -421,33 +427,56 @@ def main():
     y_ours = dev_out[W * L:(W + K) * L].cpu().numpy().reshape(K, L)
     solver.close()
 
-    # end to end through the public API: create (scene upload + classification),
-    # K steps with listener rows read back to host memory every chunk, destroy
-    torch.cuda.synchronize()
-    dist.barrier(ranks)
-    t0 = time.perf_counter()
-    s2 = PML_WaveSolver(sc, precision=prec, kernel=kern, graph_steps=G, device=local)
-    y_e2e = s2.step(K)
-    s2.close()
-    e2e_s = time.perf_counter() - t0
-    e2e_s = dist.max_over_ranks(e2e_s, ranks)
-    e2e_val = world * sc.n_cells * K / e2e_s / 1e9
-    scene_bytes = 4096 + 8 * 3 * L
+    # end to end through the public API, a whole solve of the configured length
+    # (independent of --steps): create (scene tables uploaded, first
+    # classification), sc.steps steps with the listener rows copied to host
+    # memory, destroy.  Both precisions; their series are the accuracy check.
+    def e2e_solve(p2):
+        torch.cuda.synchronize()
+        dist.barrier(ranks)
+        t0 = time.perf_counter()
+        s2 = PML_WaveSolver(sc, precision=p2, kernel=S.KERNEL_FUSED, graph_steps=G, device=local)
+        y = s2.step(sc.steps)
+        h2d, d2h = s2.transfer_bytes()
+        s2.close()
+        dt = dist.max_over_ranks(time.perf_counter() - t0, ranks)
+        return y, {"value": world * sc.n_cells * sc.steps / dt / 1e9, "unit": UNIT,
+                   "h2d_bytes_per_step": h2d / sc.steps, "d2h_bytes_per_step": d2h / sc.steps,
+                   "steps": sc.steps, "seconds": dt}
 
-    variants = {}
+    y_e2e32, e2e32 = e2e_solve(S.PRECISION_FP32_COMPENSATED)
+    y_e2e64, e2e64 = e2e_solve(S.PRECISION_FP64)
+    y_e2e = y_e2e64 if prec == S.PRECISION_FP64 else y_e2e32
+    e2e = dict(e2e64 if prec == S.PRECISION_FP64 else e2e32)
+    e2e["note"] = (f"whole {sc.steps}-step solve through PML_WaveSolver: create (scene upload, classification), "
+                   f"steps with listener rows to host, destroy; bytes counted by fdtd_solver_transfer_bytes")
+    # the timed rows must be the rows of the same solve stepped through the public API
+    n_cmp = max(0, min(K, sc.steps - W))
+    rows_equal = bool(np.array_equal(y_ours[:n_cmp], y_e2e[W:W + n_cmp]))
+    fp32_err = float(np.linalg.norm(y_e2e32 - y_e2e64) / np.linalg.norm(y_e2e64))
+    checked = {"timed_rows_equal_e2e_rows": rows_equal, "rows_compared": n_cmp,
+               "fp32_listener_rel_l2_vs_fp64": fp32_err, "steps": sc.steps,
+               "fp32_within_1e-4": fp32_err <= 1e-4,
+               "finite": bool(np.all(np.isfinite(y_e2e32)) and np.all(np.isfinite(y_e2e64)))}
+    if not (rows_equal and checked["fp32_within_1e-4"] and checked["finite"]):
+        print(json.dumps({"error": "bench output check failed", "checked": checked}), flush=True)
+        dist.shutdown(ranks)
+        return 3
+
+    variants = {"e2e_fp32_compensated": e2e32, "e2e_fp64_fused": e2e64}
     if not args.no_variants:
         for name, p2, k2 in (("fp64_fused", S.PRECISION_FP64, S.KERNEL_FUSED),
                              ("fp64_plain", S.PRECISION_FP64, S.KERNEL_PHASED),
                              ("fp32_compensated", S.PRECISION_FP32_COMPENSATED, S.KERNEL_FUSED)):
             sv = PML_WaveSolver(sc, precision=p2, kernel=k2, graph_steps=G if k2 == S.KERNEL_FUSED else 0, device=local)
-            n = min(K, 200)
-            sv.step_device(5, dev_out.data_ptr())
+            n = min(max(K, 50), 200)
+            sv.step_device(5, 0)
             sv.prepare_graphs()
             sv.synchronize()
             ext2 = torch.cuda.ExternalStream(sv.stream)
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(ext2)
-            sv.step_device(n, dev_out.data_ptr())
+            sv.step_device(n, 0)
             b.record(ext2)
             b.synchronize()
             t = a.elapsed_time(b) / n
@@ -455,19 +484,14 @@ def main():
             ab = float(sv.info().algorithmic_bytes_per_step)
             variants[name] = {"gcell_steps_s": sc.n_cells / (t / 1e3) / 1e9, "ms_per_step": t,
                               "kernel_ms": kms, "kernel_hbm_frac": ab / (kms / 1e3) / 1e9 / peak,
-                              "alg_bytes_per_step": ab}
+                              "alg_bytes_per_step": ab, "steps_timed": n}
             sv.close()
-        if args.accuracy_steps > 0:
-            ref = PML_WaveSolver(sc, precision=S.PRECISION_FP64, device=local)
-            y64 = ref.step(args.accuracy_steps)
-            ref.close()
-            f32 = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED, graph_steps=G, device=local)
-            y32 = f32.step(args.accuracy_steps)
-            f32.close()
-            variants["fp32_listener_rel_l2_vs_fp64"] = float(np.linalg.norm(y32 - y64) / np.linalg.norm(y64))
-            variants["accuracy_steps"] = args.accuracy_steps
-        if "fp64_plain" in variants and "fp32_compensated" in variants:
-            variants["fp32_over_fp64_plain"] = variants["fp32_compensated"]["gcell_steps_s"] / variants["fp64_plain"]["gcell_steps_s"]
+        f32, f64, f64p = (variants[k]["gcell_steps_s"] for k in ("fp32_compensated", "fp64_fused", "fp64_plain"))
+        variants["fp32_over_fp64_fused"] = f32 / f64
+        variants["fp32_over_fp64_plain"] = f32 / f64p
+        variants["note"] = ("fp64_fused is the plain FP64 single-solve path (region-split fused kernels, <=1e-12 "
+                            "vs the oracle) and the honest denominator; fp64_plain is one kernel per reference "
+                            "phase")
 
     batched = served = moving = None
     if rank == 0 and world == 1 and not args.no_moving:
@@ -475,7 +499,16 @@ def main():
     if rank == 0 and world == 1 and not args.no_batched:
         batched = bench_batched(peak)
     if rank == 0 and world == 1 and not args.no_served:
-        served = bench_served(peak, args.serve_rate, args.serve_requests)
+        served = bench_served(peak, args.serve_rate, args.serve_requests, fifo_plain=args.fifo_plain)
+    if "fp64_fused" in variants:
+        # the north-star ratios against the plain FP64 single-solve path
+        f64 = variants["fp64_fused"]["gcell_steps_s"]
+        if batched:
+            batched["over_fp64_fused"] = batched["gcell_steps_s"] / f64
+        if served:
+            served["over_fp64_fused"] = served["gcell_steps_s"] / f64
+            for r in served["rate_sweep"]:
+                r["over_fp64_fused"] = r["gcell_steps_s"] / f64
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -496,10 +529,12 @@ def main():
                        "parallelism": f"replicas x{world} (independent solves)"},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic, "peak_kind": peak_kind,
-                         "kernel": kname, "kernel_ms": kernel_ms, "alg_bytes_per_launch": alg_bytes},
-            "e2e": {"value": e2e_val, "unit": UNIT, "h2d_bytes_per_step": scene_bytes / K,
-                    "d2h_bytes_per_step": 8 * L,
-                    "note": "create (scene upload, classification) + K steps with listener rows to host + destroy"},
+                         "frac_dram": (traffic / (kernel_ms / 1e3) / 1e9 / peak) if traffic else None,
+                         "kernel": kname, "kernel_ms": kernel_ms, "alg_bytes_per_launch": alg_bytes,
+                         "note": "frac: algorithmic bytes / CUDA-event time of the step-kernel group; frac_dram: "
+                                 "the same with the ncu DRAM bytes of that group (traffic)"},
+            "e2e": e2e,
+            "checked": checked,
             "gpu_launches": int(launches),
             "clocks": clocks,
             "variants": variants,

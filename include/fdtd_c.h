@@ -309,6 +309,10 @@ int64_t fdtd_solver_last_launch_count(fdtd_solver* s);
  * classification (moving bodies two cells clear of the PML); the others ran it
  * after.  Execution statistics only: the results are the same either way. */
 int64_t fdtd_solver_overlapped_steps(fdtd_solver* s);
+/* Bytes this handle has copied from host to device memory and back since its
+ * creation (scene tables, meshes, per-step object poses, listener rows, status
+ * words); no counterpart in the reference, whose state lives in host memory. */
+fdtd_status fdtd_solver_transfer_bytes(fdtd_solver* s, int64_t* host_to_device, int64_t* device_to_host);
 
 /* Profiling hook (no counterpart in the reference): launch the dominant step kernel
  * n_launches times back to back on the solver's stream (alternating buffer parity,
@@ -325,9 +329,9 @@ fdtd_status fdtd_solver_time_kernel(fdtd_solver* s, int32_t which, int32_t n_lau
 
 /* Interior leapfrog step that allocates nothing.  No counterpart in the
  * reference: it exists for callers that cannot call cudaMalloc where they step
- * the field — code being captured into a CUDA graph (allocation is not
- * capturable), real-time callbacks that must not block on the allocator, hosts
- * whose own memory pool already holds the GPU's free memory.
+ * the field — real-time callbacks that must not block on the allocator or on
+ * the synchronisation an allocation may imply, and hosts whose own memory pool
+ * already holds the GPU's free memory.
  * One step of the plain path's Laplacian + leapfrog (MAC_Grid.cpp:187-299,
  * :921-935) on the box lo <= (i,j,k) < hi of a dims[0] x dims[1] x dims[2] FP64
  * grid (flat index i*dims[1]*dims[2] + j*dims[2] + k, device pointers), every box
@@ -337,9 +341,10 @@ fdtd_status fdtd_solver_time_kernel(fdtd_solver* s, int32_t which, int32_t n_lau
  * Requires 1 <= lo < hi <= dims-1 per axis and at most FDTD_NOALLOC_MAX_CELLS
  * box cells (FDTD_ERR_INVALID_ARG otherwise).  The Laplacian scratch is one
  * static device array of FDTD_NOALLOC_MAX_CELLS doubles (8 MiB) that every GPU
- * loading the library keeps until exit.  The first call on a device looks up
- * that array's device address (cudaGetSymbolAddress) with the device current:
- * make it before any stream capture.  Calls share the array, so calls that
+ * loading the library keeps until exit.  The first call on a device (and the
+ * first after a device reset gave it a new context) looks up that array's
+ * device address (cudaGetSymbolAddress) with the device current: make that
+ * call before any stream capture.  Calls share the array, so calls that
  * overlap on the GPU race; serialise them on one stream.  `stream` is a
  * cudaStream_t (NULL: the legacy default stream); the call only enqueues work. */
 #define FDTD_NOALLOC_MAX_CELLS (1 << 20)

@@ -1,6 +1,6 @@
 """The allocation-free interior step, for callers that cannot call cudaMalloc
-where they step the field (code under CUDA graph capture, real-time callbacks,
-hosts whose memory pool owns the free HBM).
+where they step the field (real-time callbacks that must not block on the
+allocator, hosts whose memory pool owns the free HBM).
 
 It is checked through the C-ABI against the library's own FP64 step on the
 non-PML cells of a source-free, body-free solve, on two calls in a row.  This
@@ -68,6 +68,41 @@ def test_noalloc_interior_step_matches_solver_on_two_calls():
         full[box] = p_next.reshape(dims)[box]
         p_prev, p_cur = p_cur, full.reshape(-1).contiguous()
     g.close()
+
+
+def test_noalloc_in_place_equals_separate_output():
+    """p_next may be p_prev: the step written over p^{n-1} equals the step written
+    into a separate buffer, on two calls in a row."""
+    import torch
+
+    lib = load()
+    dims = (36, 40, 44)
+    g = torch.Generator().manual_seed(3)
+    p_cur = torch.rand(dims, generator=g, dtype=torch.float64).reshape(-1).cuda()
+    p_prev = torch.rand(dims, generator=g, dtype=torch.float64).reshape(-1).cuda()
+    cdims = (C.c_int32 * 3)(*dims)
+    lo = (C.c_int32 * 3)(2, 3, 1)
+    hi = (C.c_int32 * 3)(30, 37, 41)
+    c2k2, lap_scale = 0.08, 1.0
+    for call in range(2):
+        sep = torch.zeros_like(p_cur)
+        st = lib.fdtd_interior_step_noalloc(C.c_void_p(p_cur.data_ptr()), C.c_void_p(p_prev.data_ptr()),
+                                            C.c_void_p(sep.data_ptr()), cdims, lo, hi, c2k2, lap_scale, None)
+        assert st == 0, lib.fdtd_last_error()
+        inplace = p_prev.clone()
+        st = lib.fdtd_interior_step_noalloc(C.c_void_p(p_cur.data_ptr()), C.c_void_p(inplace.data_ptr()),
+                                            C.c_void_p(inplace.data_ptr()), cdims, lo, hi, c2k2, lap_scale, None)
+        assert st == 0, lib.fdtd_last_error()
+        torch.cuda.synchronize()
+        box = tuple(slice(lo[d], hi[d]) for d in range(3))
+        a = sep.cpu().numpy().reshape(dims)[box]
+        b = inplace.cpu().numpy().reshape(dims)[box]
+        assert np.array_equal(a, b), call
+        # outside the box the in-place buffer keeps p^{n-1}
+        outside = np.ones(dims, dtype=bool)
+        outside[box] = False
+        assert np.array_equal(inplace.cpu().numpy().reshape(dims)[outside], p_prev.cpu().numpy().reshape(dims)[outside])
+        p_prev, p_cur = p_cur, inplace
 
 
 def test_noalloc_rejects_boxes_beyond_the_scratch_limit():
