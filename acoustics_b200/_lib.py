@@ -17,11 +17,11 @@ LIB_PATH = os.environ.get("FDTD_B200_LIB") or os.path.join(HERE, "_lib", "libfdt
 
 # every symbol include/fdtd_c.h declares
 EXPORTS = [
-    "fdtd_abi_version", "fdtd_last_error", "fdtd_device_count", "fdtd_gaussian_source_defaults",
+    "fdtd_abi_version", "fdtd_last_error", "fdtd_device_count", "fdtd_debug_inject_failure", "fdtd_gaussian_source_defaults",
     "fdtd_solver_create", "fdtd_solver_destroy", "fdtd_solver_reset", "fdtd_solver_step",
     "fdtd_solver_step_device", "fdtd_solver_fetch_listeners", "fdtd_solver_info_get",
     "fdtd_solver_get_classification", "fdtd_solver_get_field", "fdtd_solver_synchronize",
-    "fdtd_solver_stream", "fdtd_solver_last_error", "fdtd_solver_last_launch_count", "fdtd_solver_pml_state",
+    "fdtd_solver_stream", "fdtd_solver_last_error", "fdtd_solver_last_launch_count", "fdtd_solver_pml_state", "fdtd_solver_shell_staging",
     "fdtd_solver_overlapped_steps", "fdtd_solver_transfer_bytes", "fdtd_read_obj", "fdtd_mesh_signed_distance",
     "fdtd_solver_prepare_graphs", "fdtd_solver_set_field", "fdtd_matrix_write", "fdtd_matrix_read",
     "fdtd_solver_save_snapshot", "fdtd_solver_load_snapshot", "fdtd_solver_save_config",
@@ -34,6 +34,7 @@ EXPORTS = [
     "fdtd_batch_last_launch_count", "fdtd_batch_device_bytes", "fdtd_scene_device_bytes", "fdtd_scene_info",
     "fdtd_server_create", "fdtd_server_submit", "fdtd_server_poll", "fdtd_server_wait", "fdtd_server_result",
     "fdtd_server_drain", "fdtd_server_stats_get", "fdtd_server_request_error", "fdtd_server_destroy",
+    "fdtd_server_cancel", "fdtd_batch_member_snapshot", "fdtd_batch_add_snapshot",
 ]
 
 _lib = None
@@ -62,6 +63,7 @@ def load(build_if_missing: bool = False):
         "fdtd_abi_version": ([], i32),
         "fdtd_last_error": ([], C.c_char_p),
         "fdtd_device_count": ([C.POINTER(i32)], i32),
+        "fdtd_debug_inject_failure": ([i32, i32], i32),
         "fdtd_gaussian_source_defaults": ([C.POINTER(GaussianSourceDesc), dbl], i32),
         "fdtd_solver_create": ([C.POINTER(SceneDesc), C.POINTER(Options), C.POINTER(vp)], i32),
         "fdtd_solver_destroy": ([vp], i32),
@@ -81,6 +83,7 @@ def load(build_if_missing: bool = False):
         "fdtd_read_obj": ([C.c_char_p, dbl, C.POINTER(i32), C.POINTER(i32), vp, vp], i32),
         "fdtd_mesh_signed_distance": ([vp, i64, vp, vp], i32),
         "fdtd_solver_pml_state": ([vp], i32),
+        "fdtd_solver_shell_staging": ([vp], i32),
         "fdtd_solver_prepare_graphs": ([vp], i32),
         "fdtd_solver_set_field": ([vp, i32, vp, i64], i32),
         "fdtd_matrix_write": ([C.c_char_p, i32, i32, vp], i32),
@@ -124,6 +127,9 @@ def load(build_if_missing: bool = False):
         "fdtd_server_stats_get": ([vp, C.POINTER(ServerStats)], i32),
         "fdtd_server_request_error": ([vp, i64], C.c_char_p),
         "fdtd_server_destroy": ([vp], i32),
+        "fdtd_server_cancel": ([vp, i64], i32),
+        "fdtd_batch_member_snapshot": ([vp, i32, vp, C.POINTER(i64)], i32),
+        "fdtd_batch_add_snapshot": ([vp, C.POINTER(SceneDesc), i32, vp, i64, vp, i64, C.POINTER(i32)], i32),
     }
     for name, (args, res) in sig.items():
         fn = getattr(L, name)

@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -23,11 +24,21 @@ using namespace fdtd;
 
 namespace {
 thread_local std::string g_last_error;
+// fdtd_debug_inject_failure: which allocation fails next, and after how many more calls
+std::atomic<int> g_inject_what{FDTD_INJECT_NONE};
+std::atomic<int> g_inject_after{0};
 const double EPS = 1e-10;                  // src/config.h:45
 const double GAUSSIAN_CHECK_BOUND = 2.0;   // Wavesolver_ConstantsAndTypes.h:77
 }  // namespace
 
 namespace fdtd {
+bool inject_failure(int what) {
+    if (g_inject_what.load() != what) return false;
+    if (g_inject_after.fetch_sub(1) != 0) return false;
+    g_inject_what.store(FDTD_INJECT_NONE);
+    return true;
+}
+
 void set_error(fdtd_solver* s, const std::string& msg) {
     g_last_error = msg;
     if (s) s->err = msg;
@@ -609,6 +620,15 @@ fdtd_status fdtd_device_count(int32_t* count) {
     return FDTD_OK;
 }
 
+fdtd_status fdtd_debug_inject_failure(int32_t what, int32_t after) {
+    if (what < FDTD_INJECT_NONE || what > FDTD_INJECT_HOST_ALLOC || after < 0)
+        return (set_error(nullptr, "fdtd_debug_inject_failure: invalid arguments"), FDTD_ERR_INVALID_ARG);
+    g_inject_what.store(FDTD_INJECT_NONE);
+    g_inject_after.store(after);
+    g_inject_what.store(what);
+    return FDTD_OK;
+}
+
 fdtd_status fdtd_gaussian_source_defaults(fdtd_gaussian_source_desc* src, double sound_speed) {
     if (!src) return FDTD_ERR_INVALID_ARG;
     // ImpulseResponseParser.cpp:660-663
@@ -641,6 +661,13 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     if (sc->boundary_handling == FDTD_BOUNDARY_FULLY_COUPLED && o.kernel != FDTD_KERNEL_FUSED)
         return (set_error(nullptr, "FULLY_COUPLED boundaries run on the fused kernels"), FDTD_ERR_UNSUPPORTED);
     std::unique_ptr<fdtd_solver> s(new fdtd_solver());
+    // a failure below releases what was created so far (streams, events, memory)
+    struct Release {
+        std::unique_ptr<fdtd_solver>& s;
+        ~Release() {
+            if (s) fdtd_solver_destroy(s.release());
+        }
+    } release{s};
     s->opt = o;
     s->precision = o.precision;
     s->boundary_handling = sc->boundary_handling;
@@ -673,11 +700,6 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     solver_init_geometry(s.get(), sc);
     if (s->np >= (1LL << 31)) {
         set_error(nullptr, "grid too large: cell indices are 32-bit (padded cells >= 2^31)");
-        cudaStreamDestroy(s->stream);
-        cudaStreamDestroy(s->stream2);
-        cudaStreamDestroy(s->stream3);
-        cudaStreamDestroy(s->stream4);
-        cudaStreamDestroy(s->stream5);
         return FDTD_ERR_UNSUPPORTED;
     }
     for (int i = 0; i < sc->n_objects; ++i) {
@@ -713,10 +735,9 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     const int* N = s->N;
     SolveParams& P = s->hP;
     void* base = nullptr;
-    cudaError_t e = cudaMalloc(&base, cv.off);
+    cudaError_t e = inject_failure(FDTD_INJECT_DEVICE_ALLOC) ? cudaErrorMemoryAllocation : cudaMalloc(&base, cv.off);
     if (e != cudaSuccess) {
         set_error(nullptr, std::string("cudaMalloc of ") + std::to_string(cv.off) + " bytes failed: " + cudaGetErrorString(e));
-        cudaStreamDestroy(s->stream);
         return FDTD_ERR_OOM;
     }
     s->arena = base;
@@ -857,7 +878,9 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     }
     if (s->L > 0)
         CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.listeners, s->listeners.data(), s->listeners.size() * 8, cudaMemcpyHostToDevice));
-    CUDA_TRY(s.get(), cudaMallocHost((void**)&s->h_lis_stage, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8));
+    CUDA_TRY(s.get(), inject_failure(FDTD_INJECT_HOST_ALLOC)
+                          ? cudaErrorMemoryAllocation
+                          : cudaMallocHost((void**)&s->h_lis_stage, (size_t)s->lis_cap_steps * std::max(1, s->L) * 8));
     s->xb = (o.x_chunk == 2 || o.x_chunk == 4 || o.x_chunk == 8) ? o.x_chunk : 2;
     s->region.xb = s->xb;
     // tile_y: x planes each PML-shell thread marches over
@@ -872,26 +895,22 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
 fdtd_status fdtd_solver_destroy(fdtd_solver* s) {
     if (!s) return FDTD_OK;
     cudaSetDevice(s->opt.device);
-    cudaStreamSynchronize(s->stream);
+    // (also releases a solver whose creation failed part way: null handles are skipped)
+    for (cudaStream_t st : {s->stream, s->stream2, s->stream3, s->stream4, s->stream5})
+        if (st) cudaStreamSynchronize(st);
     for (int i = 0; i < 4; ++i)
         if (s->graph_exec[i]) cudaGraphExecDestroy(s->graph_exec[i]);
     free_fully_coupled(s);
+    free_shell_tma(s);
     for (void* p : s->mesh_alloc) cudaFree(p);
+    if (s->d_solid_pml) cudaFree(s->d_solid_pml);
     if (s->arena) cudaFree(s->arena);
     if (s->h_lis_stage) cudaFreeHost(s->h_lis_stage);
-    cudaStreamSynchronize(s->stream2);
-    if (s->stream3) cudaStreamSynchronize(s->stream3);
-    if (s->stream4) cudaStreamSynchronize(s->stream4);
-    if (s->stream5) cudaStreamSynchronize(s->stream5);
-    cudaEventDestroy(s->ev_fork);
-    cudaEventDestroy(s->ev_join);
-    for (cudaEvent_t ev : {s->ev_ghost, s->ev_step, s->ev_lis[0], s->ev_lis[1], s->ev_lis_join, s->ev_sfork, s->ev_sdone})
+    for (cudaEvent_t ev : {s->ev_fork, s->ev_join, s->ev_ghost, s->ev_step, s->ev_lis[0], s->ev_lis[1], s->ev_lis_join,
+                           s->ev_sfork, s->ev_sdone})
         if (ev) cudaEventDestroy(ev);
-    cudaStreamDestroy(s->stream2);
-    if (s->stream3) cudaStreamDestroy(s->stream3);
-    if (s->stream4) cudaStreamDestroy(s->stream4);
-    if (s->stream5) cudaStreamDestroy(s->stream5);
-    cudaStreamDestroy(s->stream);
+    for (cudaStream_t st : {s->stream2, s->stream3, s->stream4, s->stream5, s->stream})
+        if (st) cudaStreamDestroy(st);
     delete s;
     return FDTD_OK;
 }
@@ -974,6 +993,14 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     }
     s->region.fc = P.fc_n > 0 ? 1 : 0;
     s->region.red = use_reduced_pml(s, n_solid == 0) ? 1 : 0;
+    // reduced state: the TMA-staged shell kernel where it applies (tiles and
+    // tensor maps of this solve), else the per-thread cp.async kernel
+    free_shell_tma(s);
+    if (s->region.red && s->opt.shell_staging == FDTD_SHELL_STAGING_AUTO) {
+        st = build_shell_tma(s);
+        if (st != FDTD_OK && st != FDTD_ERR_UNSUPPORTED) return st;
+        if (st == FDTD_ERR_UNSUPPORTED) s->err.clear();
+    }
     // default x planes per shell thread of the state in effect (tile_y overrides)
     if (s->opt.kernel == FDTD_KERNEL_FUSED) {
         const int xs = shell_planes(s, s->opt.tile_y);

@@ -323,6 +323,75 @@ fdtd_status fdtd_batch_create(int32_t n, const fdtd_scene_desc* scenes, const in
     return FDTD_OK;
 }
 
+namespace {
+// the slot of a new member: the first released one, else a new one
+int32_t place_member(fdtd_batch* b, Member&& mb) {
+    size_t slot = b->members.size();
+    for (size_t i = 0; i < b->members.size(); ++i)
+        if (b->members[i].released) {
+            slot = i;
+            break;
+        }
+    if (slot == b->members.size()) b->members.push_back(std::move(mb));
+    else b->members[slot] = std::move(mb);
+    b->dirty = true;
+    return (int32_t)slot;
+}
+}  // namespace
+
+fdtd_status fdtd_batch_member_snapshot(fdtd_batch* b, int32_t member, void* buffer, int64_t* bytes) {
+    if (!b || !bytes || member < 0 || member >= (int32_t)b->members.size() || b->members[member].released ||
+        !b->members[member].s)
+        return batch_fail(b, FDTD_ERR_INVALID_ARG, "fdtd_batch_member_snapshot: no such member");
+    fdtd_solver* s = b->members[member].s;
+    if (buffer) {
+        BATCH_TRY(b, cudaSetDevice(b->opt.device));
+        BATCH_TRY(b, cudaStreamSynchronize(b->stream));  // the member's batched steps are done
+    }
+    const fdtd_status st = fdtd_solver_snapshot(s, buffer, bytes);
+    if (st != FDTD_OK) return batch_fail(b, st, fdtd_solver_last_error(s));
+    return FDTD_OK;
+}
+
+fdtd_status fdtd_batch_add_snapshot(fdtd_batch* b, const fdtd_scene_desc* scene, int32_t steps_total,
+                                    const void* snapshot, int64_t bytes, const double* rows, int64_t steps_done,
+                                    int32_t* member) {
+    if (!b || !scene || !snapshot || steps_total < 0 || steps_done < 0 || steps_done > steps_total)
+        return batch_fail(b, FDTD_ERR_INVALID_ARG, "fdtd_batch_add_snapshot: invalid arguments");
+    if (scene->boundary_handling != FDTD_BOUNDARY_RASTERIZE)
+        return batch_fail(b, FDTD_ERR_UNSUPPORTED, "batched members use RASTERIZE boundaries");
+    if (scene->air_viscosity_alpha != 0.0)
+        return batch_fail(b, FDTD_ERR_UNSUPPORTED, "batched members have no air viscosity");
+    if (scene->n_listeners > 0 && steps_done > 0 && !rows)
+        return batch_fail(b, FDTD_ERR_INVALID_ARG, "fdtd_batch_add_snapshot: rows missing");
+    fdtd_options o = b->opt;
+    o.graph_steps = 0;
+    o.shell_staging = FDTD_SHELL_STAGING_RING;
+    fdtd_solver* s = nullptr;
+    fdtd_status st = fdtd_solver_create(scene, &o, &s);
+    if (st != FDTD_OK) return batch_fail(b, st, fdtd_last_error());
+    auto fail = [&](fdtd_status code, const std::string& m) {
+        fdtd_solver_destroy(s);
+        return batch_fail(b, code, m);
+    };
+    if (s->moving) return fail(FDTD_ERR_UNSUPPORTED, "moving bodies are stepped by fdtd_solver, not in batches");
+    st = fdtd_solver_restore(s, snapshot, bytes);
+    if (st != FDTD_OK) return fail(st, fdtd_solver_last_error(s));
+    if (s->step_index != steps_done) return fail(FDTD_ERR_INVALID_ARG, "snapshot step differs from steps_done");
+    st = rebuild_listener_plans(s);
+    if (st != FDTD_OK) return fail(st, fdtd_solver_last_error(s));
+    Member mb;
+    mb.s = s;
+    mb.total = steps_total;
+    mb.done = steps_done;
+    mb.L = s->L;
+    if (mb.L > 0 && steps_done > 0) mb.rows.assign(rows, rows + (size_t)steps_done * mb.L);
+    mb.active = mb.done < mb.total;
+    const int32_t slot = place_member(b, std::move(mb));
+    if (member) *member = slot;
+    return FDTD_OK;
+}
+
 fdtd_status fdtd_batch_add(fdtd_batch* b, const fdtd_scene_desc* scene, int32_t steps, int32_t* member) {
     if (!b || !scene || steps < 0) return batch_fail(b, FDTD_ERR_INVALID_ARG, "fdtd_batch_add: invalid arguments");
     if (scene && scene->boundary_handling != FDTD_BOUNDARY_RASTERIZE)
@@ -331,6 +400,7 @@ fdtd_status fdtd_batch_add(fdtd_batch* b, const fdtd_scene_desc* scene, int32_t 
         return batch_fail(b, FDTD_ERR_UNSUPPORTED, "batched members have no air viscosity");
     fdtd_options o = b->opt;
     o.graph_steps = 0;
+    o.shell_staging = FDTD_SHELL_STAGING_RING;  // the batch kernels stage per thread
     fdtd_solver* s = nullptr;
     fdtd_status st = fdtd_solver_create(scene, &o, &s);
     if (st != FDTD_OK) return batch_fail(b, st, fdtd_last_error());
@@ -354,16 +424,8 @@ fdtd_status fdtd_batch_add(fdtd_batch* b, const fdtd_scene_desc* scene, int32_t 
         mb.done = 1;
     }
     mb.active = mb.done < mb.total;
-    size_t slot = b->members.size();
-    for (size_t i = 0; i < b->members.size(); ++i)
-        if (b->members[i].released) {
-            slot = i;
-            break;
-        }
-    if (slot == b->members.size()) b->members.push_back(std::move(mb));
-    else b->members[slot] = std::move(mb);
-    b->dirty = true;
-    if (member) *member = (int32_t)slot;
+    const int32_t slot = place_member(b, std::move(mb));
+    if (member) *member = slot;
     return FDTD_OK;
 }
 

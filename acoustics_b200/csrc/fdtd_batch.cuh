@@ -111,6 +111,7 @@ __global__ void __launch_bounds__(128) k_batch_listeners(const BatchDesc<T>* __r
     double* row = d.ring + (size_t)(step % d.ring_cap) * d.n_lis;
     if (d.P->lis_ready) listener_plan<T>(*d.P, d.cur ^ 1, r.li, row);
     else listener_body<T>(*d.P, d.cur ^ 1, r.li, row);
+    flag_nonfinite(*d.P, row, r.li);
 }
 
 template <typename T>

@@ -115,6 +115,7 @@ struct ShellBoxes {
 
 struct SolveParams;
 struct FcRow;
+struct TmaStep;
 
 // Precomputed order-1 MLS of one listener (static classification): the sample
 // value is sum_r w_r * value_r over its rows.  A row is the pressure of a cell
@@ -190,6 +191,7 @@ struct RegionLaunch {
     int skip;          // kernels left out (timing of single kernels): 1 interior, 2 shell, 4 ghost list
     int red;           // FP32: the shell keeps the reduced PML state (k_pml_shell_red)
     int fc;            // FULLY_COUPLED ghost cells: solve their system before the ghost list
+    const TmaStep* tma;  // reduced state: the TMA-staged shell (k_pml_shell_tma) when not null (host memory)
 };
 
 // Two copies indexed by the step parity: the kernels of a step read

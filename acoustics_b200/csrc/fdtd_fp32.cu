@@ -1,5 +1,7 @@
-// fdtd_fp32.cu — FP32 fused step kernel with compensated (increment-form)
-// pressure accumulation.  Multiply-add contraction is allowed here.
+// fdtd_fp32.cu — FP32 fused step kernels with compensated (increment-form)
+// pressure accumulation.  Built with -fmad=false like every device unit: the
+// FP32 kernels request their FMAs explicitly (fmaf), so no result depends on
+// how the compiler contracts one instantiation or another.
 #include <cuda_runtime.h>
 
 #include "fdtd_device.cuh"
@@ -30,7 +32,10 @@ namespace fdtd {
 // The reduced-state shell kernels stage their loads in more than the default
 // 48 KB of dynamic shared memory: raise their limit on the current device.
 cudaError_t prepare_fp32_kernels() {
-    cudaError_t e = cudaSuccess;
+    // the TMA-staged shell: a 4-stage ring of up to 24 KB stages
+    cudaError_t e = cudaFuncSetAttribute(k_pml_shell_tma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         TMA_STAGES * 24 * 1024 + 8 * TMA_STAGES);
+    if (e != cudaSuccess) return e;
     if (red_smem_bytes() > 0) {
         e = cudaFuncSetAttribute(k_pml_shell_red<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, red_smem_bytes());
         if (e == cudaSuccess)

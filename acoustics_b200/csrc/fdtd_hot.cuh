@@ -464,6 +464,7 @@ __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_pml_shell(
 }  // namespace fdtd
 
 #include "fdtd_shell_red.cuh"
+#include "fdtd_shell_tma.cuh"
 
 namespace fdtd {
 
@@ -515,7 +516,10 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     const int nblk = (R.skip & 2) ? 0 : R.shell.block_first[R.shell.n];
     if (nblk > 0) {
         if constexpr (sizeof(T) == 4) {
-            if (R.red) k_pml_shell_red<float><<<nblk, dim3(32, 8), red_smem_bytes(), S.s>>>(A, R.shell);
+            if (R.red && R.tma)
+                k_pml_shell_tma<float><<<R.tma->launch.ntiles, TMA_THREADS, tma_smem_bytes(R.tma->launch), S.s>>>(
+                    A, R.tma->maps[cur], R.tma->launch, R.tma->d_tiles, hP.dev_error);
+            else if (R.red) k_pml_shell_red<float><<<nblk, dim3(32, 8), red_smem_bytes(), S.s>>>(A, R.shell);
             else k_pml_shell<T><<<nblk, dim3(32, 8), 0, S.s>>>(A, R.shell);
         } else {
             k_pml_shell<T><<<nblk, dim3(32, 8), 0, S.s>>>(A, R.shell);

@@ -8,6 +8,7 @@
 
 #include "../../include/fdtd_c.h"
 #include "fdtd_device.cuh"
+#include "fdtd_tma.hpp"
 
 namespace fdtd {
 
@@ -110,6 +111,7 @@ struct fdtd_solver {
     long long launches = 0;
     long long last_launches = 0;
     long long graph_launches_per_exec = 0;
+    fdtd::TmaStep* tma = nullptr;     // tiles and tensor maps of the TMA-staged shell (reduced state)
     // bytes this handle copied between host and device memory since creation
     long long bytes_h2d = 0, bytes_d2h = 0;
     std::string err;
@@ -133,6 +135,14 @@ inline cudaError_t counted_copyAsync(fdtd_solver* s, void* dst, const void* src,
     return cudaMemcpyAsync(dst, src, n, kind, stream);
 }
 void set_error(fdtd_solver* s, const std::string& msg);
+// listener plans of a static solve from its current classification (after a restore)
+fdtd_status rebuild_listener_plans(fdtd_solver* s);
+// fdtd_debug_inject_failure: true when this allocation of kind `what` is to fail
+bool inject_failure(int what);
+// TMA-staged PML shell (fdtd_tma.cpp)
+bool tma_encoder_available();
+fdtd_status build_shell_tma(fdtd_solver* s);
+void free_shell_tma(fdtd_solver* s);
 fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc);
 void classification_boxes(const fdtd_solver* s, ClsBoxes& B);
 void to_dev_objects(fdtd_solver* s);

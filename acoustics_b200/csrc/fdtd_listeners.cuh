@@ -262,6 +262,11 @@ __device__ void listener_body(const SolveParams& P, int newp, int li, double* __
     if (!ok) atomicOr(P.dev_error, 1);
 }
 
+// FDTD_ERR_NUMERIC for a listener sample that is not finite (lane 0 wrote it).
+__device__ __forceinline__ void flag_nonfinite(const SolveParams& P, const double* out_row, int li) {
+    if ((threadIdx.x & 31) == 0 && !isfinite(out_row[li])) atomicOr(P.dev_error, 1);
+}
+
 // Listener li from its plan: sum_r w_r value_r as a warp reduction.  A NaN
 // among the enclosing cells (which the full fit drops) falls back to it.
 template <typename T>
@@ -328,6 +333,7 @@ __global__ void __launch_bounds__(128) k_listeners_warp(const SolveParams* __res
     if (li >= Pp->n_lis) return;  // the whole warp leaves together
     if (Pp->lis_ready) listener_plan<T>(*Pp, newp, li, out_row);
     else listener_body<T>(*Pp, newp, li, out_row);
+    flag_nonfinite(*Pp, out_row, li);
 }
 
 }  // namespace fdtd

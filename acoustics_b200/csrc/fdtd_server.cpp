@@ -8,7 +8,12 @@
 //   retire  finished members: copy their series out, release the slot and its
 //           device bytes, wake waiters.
 // Admission is in arrival order (no overtaking), so a large request at the
-// head waits for memory instead of being starved by smaller ones.  Latency is
+// head waits for memory instead of being starved by smaller ones.  With
+// preemption on, a head that does not fit may evict running members with much
+// more work left (their state and rows move to host memory, fdtd_batch_member_
+// snapshot) and they queue again right behind it; re-admitted, they continue
+// from the snapshot (fdtd_batch_add_snapshot).  A cancelled request leaves the
+// queue, or its member is released after the chunk in progress.  Latency is
 // measured on the host clock from submit to the retirement of the request.
 #include <cuda_runtime.h>
 
@@ -81,6 +86,10 @@ struct Request {
     std::vector<double> out;
     Clock::time_point t_submit, t_done;
     std::string err;
+    bool cancel = false;            // cancellation asked while running
+    std::vector<char> snap;         // evicted: the member's state ...
+    std::vector<double> rows;       // ... and its listener rows so far
+    int64_t evicted_steps = -1;     // steps done when evicted (-1: never)
 };
 
 }  // namespace
@@ -101,7 +110,7 @@ struct fdtd_server {
     std::string create_err;
     bool ready = false, failed_start = false;
     // statistics
-    int64_t submitted = 0, completed = 0, failed = 0, peak_members = 0, peak_bytes = 0;
+    int64_t submitted = 0, completed = 0, failed = 0, cancelled = 0, evictions = 0, peak_members = 0, peak_bytes = 0;
     std::vector<double> latencies;
     double cell_steps_done = 0;
     bool have_first = false;
@@ -120,9 +129,77 @@ void finish(fdtd_server* S, Request& r, int32_t state, int32_t status, const std
         S->latencies.push_back(std::chrono::duration<double>(r.t_done - r.t_submit).count());
         S->cell_steps_done += r.cells * r.steps;
         S->t_last = r.t_done;
+    } else if (state == FDTD_REQ_CANCELLED) {
+        S->cancelled++;
     } else {
         S->failed++;
     }
+    r.snap.clear();
+    r.snap.shrink_to_fit();
+    r.rows.clear();
+    r.rows.shrink_to_fit();
+}
+
+// Members to evict so that `need` more bytes fit: running members whose
+// remaining cell-steps exceed twice the head's, most remaining work first.
+// Returns an empty list when evicting them all would not make room.  (Lock held.)
+std::vector<int32_t> eviction_plan(fdtd_server* S, const Request& head) {
+    std::vector<std::pair<double, int32_t>> cand;
+    for (const auto& mr : S->running) {
+        const Request& r = *S->reqs[mr.second];
+        if (r.cancel) continue;
+        const double left = r.cells * (double)(r.steps - r.steps_done);
+        if (left > 2.0 * head.cells * head.steps) cand.push_back({left, mr.first});
+    }
+    std::sort(cand.begin(), cand.end(), [](const auto& a, const auto& b) { return a.first > b.first; });
+    std::vector<int32_t> out;
+    int64_t used = S->used_bytes;
+    for (const auto& c : cand) {
+        if (used + head.bytes <= S->cfg.hbm_budget_bytes) break;
+        out.push_back(c.second);
+        used -= S->reqs[S->running[c.second]]->bytes;
+    }
+    if (used + head.bytes > S->cfg.hbm_budget_bytes) out.clear();
+    return out;
+}
+
+// Move member m to host memory and queue its request again behind the head.
+void evict(fdtd_server* S, int32_t m) {
+    int64_t id;
+    {
+        std::lock_guard<std::mutex> g(S->mu);
+        id = S->running[m];
+    }
+    Request* r = S->reqs[id].get();  // the worker owns running requests' members
+    int64_t done = 0, total = 0, bytes = 0;
+    int32_t nl = 0, mst = 0;
+    fdtd_status st = fdtd_batch_member_info(S->batch, m, &done, &total, &nl, &mst);
+    std::vector<double> rows((size_t)done * nl);
+    std::vector<char> snap;
+    if (st == FDTD_OK && mst == FDTD_OK && !rows.empty()) st = fdtd_batch_output(S->batch, m, rows.data(), (int64_t)rows.size());
+    if (st == FDTD_OK && mst == FDTD_OK) st = fdtd_batch_member_snapshot(S->batch, m, nullptr, &bytes);
+    if (st == FDTD_OK && mst == FDTD_OK) {
+        snap.resize((size_t)bytes);
+        st = fdtd_batch_member_snapshot(S->batch, m, snap.data(), &bytes);
+    }
+    const std::string err = st != FDTD_OK ? fdtd_last_error() : "";
+    fdtd_batch_release(S->batch, m);
+    std::lock_guard<std::mutex> g(S->mu);
+    S->running.erase(m);
+    S->used_bytes -= r->bytes;
+    r->member = -1;
+    if (st != FDTD_OK || mst != FDTD_OK) {
+        finish(S, *r, FDTD_REQ_FAILED, st != FDTD_OK ? st : mst, err.empty() ? "device-side error flag set" : err);
+        S->cv_done.notify_all();
+        return;
+    }
+    r->snap.swap(snap);
+    r->rows.swap(rows);
+    r->steps_done = done;
+    r->evicted_steps = done;
+    r->state = FDTD_REQ_QUEUED;
+    S->queue.insert(S->queue.empty() ? S->queue.end() : S->queue.begin() + 1, id);
+    S->evictions++;
 }
 
 void worker_main(fdtd_server* S) {
@@ -145,6 +222,7 @@ void worker_main(fdtd_server* S) {
     for (;;) {
         // ---- admit ----
         std::vector<Request*> admit;
+        std::vector<int32_t> victims;
         {
             std::unique_lock<std::mutex> lk(S->mu);
             S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty() || !S->running.empty(); });
@@ -153,7 +231,10 @@ void worker_main(fdtd_server* S) {
             size_t slots = S->running.size();
             while (!S->queue.empty() && slots < (size_t)S->cfg.max_members) {
                 Request* r = S->reqs[S->queue.front()].get();
-                if (used + r->bytes > S->cfg.hbm_budget_bytes) break;  // head waits for memory
+                if (used + r->bytes > S->cfg.hbm_budget_bytes) {  // head waits for memory
+                    if (S->cfg.preempt && admit.empty()) victims = eviction_plan(S, *r);
+                    break;
+                }
                 S->queue.pop_front();
                 used += r->bytes;
                 slots++;
@@ -162,10 +243,31 @@ void worker_main(fdtd_server* S) {
             S->used_bytes = used;
             S->peak_bytes = std::max(S->peak_bytes, used);
         }
+        if (!victims.empty()) {
+            for (int32_t m : victims) evict(S, m);
+            continue;  // admit the head now
+        }
         for (Request* r : admit) {
             int32_t m = -1;
-            fdtd_status st = fdtd_batch_add(S->batch, &r->scene.d, r->steps, &m);
+            fdtd_status st;
+            if (r->evicted_steps >= 0) {
+                st = fdtd_batch_add_snapshot(S->batch, &r->scene.d, r->steps, r->snap.data(), (int64_t)r->snap.size(),
+                                             r->rows.empty() ? nullptr : r->rows.data(), r->evicted_steps, &m);
+                if (st == FDTD_OK) {
+                    r->snap.clear();
+                    r->snap.shrink_to_fit();
+                    r->rows.clear();
+                    r->rows.shrink_to_fit();
+                }
+            } else {
+                st = fdtd_batch_add(S->batch, &r->scene.d, r->steps, &m);
+            }
             std::lock_guard<std::mutex> g(S->mu);
+            if (r->state == FDTD_REQ_CANCELLED) {  // cancelled while it was being admitted
+                if (st == FDTD_OK) fdtd_batch_release(S->batch, m);
+                S->used_bytes -= r->bytes;
+                continue;
+            }
             if (st != FDTD_OK) {
                 S->used_bytes -= r->bytes;
                 finish(S, *r, FDTD_REQ_FAILED, st, fdtd_last_error());
@@ -197,6 +299,22 @@ void worker_main(fdtd_server* S) {
             int64_t done = 0, total = 0;
             int32_t nl = 0, mst = 0;
             fdtd_batch_member_info(S->batch, mr.first, &done, &total, &nl, &mst);
+            bool cancelled;
+            {
+                std::lock_guard<std::mutex> g(S->mu);
+                cancelled = S->reqs[mr.second]->cancel;
+            }
+            if (cancelled) {
+                fdtd_batch_release(S->batch, mr.first);
+                std::lock_guard<std::mutex> g(S->mu);
+                Request& r = *S->reqs[mr.second];
+                r.steps_done = done;
+                S->running.erase(mr.first);
+                S->used_bytes -= r.bytes;
+                finish(S, r, FDTD_REQ_CANCELLED, FDTD_ERR_CANCELLED, "request cancelled");
+                S->cv_done.notify_all();
+                continue;
+            }
             const bool ok = st == FDTD_OK && mst == FDTD_OK;
             const bool finished = !ok || done >= total;
             std::vector<double> out;
@@ -327,13 +445,13 @@ fdtd_status fdtd_server_wait(fdtd_server* S, int64_t id, double timeout_s) {
     if (!find(S, id)) return (fdtd::set_error(nullptr, "unknown request"), FDTD_ERR_INVALID_ARG);
     auto pred = [&] {
         Request* r = find(S, id);
-        return !r || r->state == FDTD_REQ_DONE || r->state == FDTD_REQ_FAILED;
+        return !r || r->state == FDTD_REQ_DONE || r->state == FDTD_REQ_FAILED || r->state == FDTD_REQ_CANCELLED;
     };
     if (timeout_s < 0) S->cv_done.wait(lk, pred);
     else if (!S->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s), pred))
         return (fdtd::set_error(nullptr, "wait timed out"), FDTD_ERR_TIMEOUT);
     Request* r = find(S, id);
-    return r && r->state == FDTD_REQ_FAILED ? r->status : FDTD_OK;
+    return r && (r->state == FDTD_REQ_FAILED || r->state == FDTD_REQ_CANCELLED) ? r->status : FDTD_OK;
 }
 
 fdtd_status fdtd_server_result(fdtd_server* S, int64_t id, double* out, int64_t count, int64_t* steps,
@@ -342,7 +460,7 @@ fdtd_status fdtd_server_result(fdtd_server* S, int64_t id, double* out, int64_t 
     std::lock_guard<std::mutex> g(S->mu);
     Request* r = find(S, id);
     if (!r) return (fdtd::set_error(nullptr, "unknown request"), FDTD_ERR_INVALID_ARG);
-    if (r->state == FDTD_REQ_FAILED) {
+    if (r->state == FDTD_REQ_FAILED || r->state == FDTD_REQ_CANCELLED) {
         fdtd::set_error(nullptr, r->err);
         return r->status;
     }
@@ -379,6 +497,9 @@ fdtd_status fdtd_server_stats_get(fdtd_server* S, fdtd_server_stats* st) {
     st->running = (int64_t)S->running.size();
     st->peak_members = S->peak_members;
     st->peak_device_bytes = S->peak_bytes;
+    st->device_bytes_in_use = S->used_bytes;
+    st->cancelled = S->cancelled;
+    st->evictions = S->evictions;
     st->p50_latency_s = pct(S->latencies, 0.50);
     st->p99_latency_s = pct(S->latencies, 0.99);
     double sum = 0;
@@ -392,6 +513,27 @@ fdtd_status fdtd_server_stats_get(fdtd_server* S, fdtd_server_stats* st) {
         }
     }
     return FDTD_OK;
+}
+
+fdtd_status fdtd_server_cancel(fdtd_server* S, int64_t id) {
+    if (!S) return FDTD_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> g(S->mu);
+    Request* r = find(S, id);
+    if (!r) return (fdtd::set_error(nullptr, "unknown request"), FDTD_ERR_INVALID_ARG);
+    if (r->state == FDTD_REQ_QUEUED) {
+        auto it = std::find(S->queue.begin(), S->queue.end(), id);
+        if (it != S->queue.end()) S->queue.erase(it);
+        finish(S, *r, FDTD_REQ_CANCELLED, FDTD_ERR_CANCELLED, "request cancelled");
+        S->cv_done.notify_all();
+        S->cv_work.notify_all();
+        return FDTD_OK;
+    }
+    if (r->state == FDTD_REQ_RUNNING) {
+        r->cancel = true;  // the worker releases the member after the chunk in progress
+        S->cv_work.notify_all();
+        return FDTD_OK;
+    }
+    return (fdtd::set_error(nullptr, "request already finished"), FDTD_ERR_INVALID_ARG);
 }
 
 const char* fdtd_server_request_error(fdtd_server* S, int64_t id) {

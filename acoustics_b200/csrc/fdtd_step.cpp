@@ -227,8 +227,12 @@ fdtd_status check_device_errors(fdtd_solver* s) {
         return FDTD_ERR_GEOMETRY;
     }
     if (dev_error & 1) {
-        set_error(s, "degenerate listener stencil (no cell or rank-deficient MLS)");
+        set_error(s, "listener sample not finite, or a degenerate listener stencil (no cell or rank-deficient MLS)");
         return FDTD_ERR_NUMERIC;
+    }
+    if (dev_error & fdtd::FDTD_DEV_ERR_TMA_TIMEOUT) {
+        set_error(s, "a tensor copy of the PML-shell kernel did not complete within its bounded wait");
+        return FDTD_ERR_TIMEOUT;
     }
     return FDTD_OK;
 }
@@ -438,6 +442,11 @@ const char* fdtd_solver_last_error(fdtd_solver* s) { return s ? s->err.c_str() :
 int64_t fdtd_solver_last_launch_count(fdtd_solver* s) { return s ? s->last_launches : 0; }
 
 int64_t fdtd_solver_overlapped_steps(fdtd_solver* s) { return s ? s->overlapped_steps : 0; }
+
+int32_t fdtd_solver_shell_staging(fdtd_solver* s) {
+    if (!s || !s->region.red) return -1;
+    return s->region.tma ? FDTD_SHELL_STAGING_TMA : FDTD_SHELL_STAGING_RING;
+}
 
 fdtd_status fdtd_solver_transfer_bytes(fdtd_solver* s, int64_t* host_to_device, int64_t* device_to_host) {
     if (!s || !host_to_device || !device_to_host) return (set_error(s, "invalid arguments"), FDTD_ERR_INVALID_ARG);
@@ -664,6 +673,9 @@ fdtd_status field_transfer(fdtd_solver* s, int32_t which, double* dense, int64_t
 extern "C" {
 
 fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, int64_t count) {
+    // the read-back stages the field in host memory
+    if (s && fdtd::inject_failure(FDTD_INJECT_HOST_ALLOC))
+        return (set_error(s, "host staging buffer of the field read-back: allocation failed"), FDTD_ERR_OOM);
     return field_transfer(s, which, out, count, false);
 }
 
@@ -711,6 +723,23 @@ std::vector<std::pair<void*, size_t>> snap_regions(fdtd_solver* s) {
     return r;
 }
 }  // namespace
+
+}  // extern "C"
+
+namespace fdtd {
+// Listener plans (fixed MLS weights) of a static solve from its current
+// classification, as its first step builds them; used after a restore.
+fdtd_status rebuild_listener_plans(fdtd_solver* s) {
+    if (s->moving || s->L <= 0) return FDTD_OK;
+    CUDA_TRY(s, cudaSetDevice(s->opt.device));
+    CUDA_TRY(s, launch_listener_prep(s->dP, s->precision, s->cur, s->L, s->stream));
+    s->hP.lis_ready = 1;
+    CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    return FDTD_OK;
+}
+}  // namespace fdtd
+
+extern "C" {
 
 fdtd_status fdtd_solver_snapshot(fdtd_solver* s, void* buffer, int64_t* bytes) {
     if (!s || !bytes) return FDTD_ERR_INVALID_ARG;

@@ -24,6 +24,7 @@ MOTION_STATIC, MOTION_BALLISTIC = 0, 1
 PRECISION_FP64, PRECISION_FP32_COMPENSATED = 0, 1
 KERNEL_FUSED, KERNEL_PHASED = 0, 1
 PML_STATE_AUTO, PML_STATE_FULL = 0, 1
+SHELL_STAGING_AUTO, SHELL_STAGING_RING, SHELL_STAGING_TMA = 0, 1, 2
 BOUNDARY_RASTERIZE, BOUNDARY_FULLY_COUPLED = 0, 1
 
 CELL_BULK, CELL_GHOST, CELL_VALID_HISTORY, CELL_PML, CELL_CONSTRAINT = 1, 2, 4, 8, 16
@@ -34,6 +35,7 @@ STATUS = {
     0: "FDTD_OK", 1: "FDTD_END_OF_TIME", -1: "FDTD_ERR_INVALID_ARG", -2: "FDTD_ERR_OOM",
     -3: "FDTD_ERR_CUDA", -4: "FDTD_ERR_NUMERIC", -5: "FDTD_ERR_TIMEOUT",
     -6: "FDTD_ERR_GEOMETRY", -7: "FDTD_ERR_UNSUPPORTED", -8: "FDTD_ERR_IO", -9: "FDTD_ERR_BUSY",
+    -10: "FDTD_ERR_CANCELLED",
 }
 STATUS_CODE = {name: code for code, name in STATUS.items()}
 
@@ -82,23 +84,24 @@ class Options(C.Structure):
     _fields_ = [
         ("precision", C.c_int32), ("device", C.c_int32), ("kernel", C.c_int32),
         ("graph_steps", C.c_int32), ("tile_y", C.c_int32), ("x_chunk", C.c_int32),
-        ("pml_state", C.c_int32), ("_reserved1", C.c_int32),
+        ("pml_state", C.c_int32), ("shell_staging", C.c_int32),
     ]
 
 
 class ServerConfig(C.Structure):
     _fields_ = [("hbm_budget_bytes", C.c_int64), ("max_members", C.c_int32), ("chunk_steps", C.c_int32),
-                ("_pad", C.c_int32)]
+                ("preempt", C.c_int32)]
 
 
 class ServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("submitted", "completed", "failed", "queued", "running", "peak_members",
                                          "peak_device_bytes")] + \
                [(n, C.c_double) for n in ("p50_latency_s", "p99_latency_s", "mean_latency_s", "span_s",
-                                          "solves_per_s", "cell_steps_per_s")]
+                                          "solves_per_s", "cell_steps_per_s")] + \
+               [(n, C.c_int64) for n in ("device_bytes_in_use", "cancelled", "evictions")]
 
 
-REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED = 0, 1, 2, 3
+REQ_QUEUED, REQ_RUNNING, REQ_DONE, REQ_FAILED, REQ_CANCELLED = 0, 1, 2, 3, 4
 
 
 class SolverInfo(C.Structure):

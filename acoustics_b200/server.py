@@ -5,6 +5,9 @@ The reference steps one scene per process (src/wavesolver/SimWorld.cpp:517-590);
 their device bytes fit the budget, keeps their grids resident and steps all
 admitted scenes together (fdtd_server_* in include/fdtd_c.h).  A request's
 listener series equals that of `PML_WaveSolver` on the same scene and options.
+Requests can be cancelled; with `preempt` a queue head that does not fit evicts
+members with much more work left to host memory (the reference's snapshot,
+FDTD_AcousticSimulator.cpp:381-415), which resume where they stopped.
 """
 from __future__ import annotations
 
@@ -14,19 +17,19 @@ from typing import Dict, Tuple
 import numpy as np
 
 from ._lib import FDTDError, check, load
-from .scene import (KERNEL_FUSED, PRECISION_FP32_COMPENSATED, REQ_DONE, REQ_FAILED, Options, Scene, ServerConfig,
-                    ServerStats)
+from .scene import (KERNEL_FUSED, PRECISION_FP32_COMPENSATED, REQ_CANCELLED, REQ_DONE, REQ_FAILED, Options, Scene,
+                    ServerConfig, ServerStats)
 
 
 class SolveServer:
     def __init__(self, precision: int = PRECISION_FP32_COMPENSATED, graph_steps: int = 16, device: int = 0,
                  hbm_budget_bytes: int = 0, max_members: int = 0, chunk_steps: int = 0, tile_y: int = 0,
-                 x_chunk: int = 0):
+                 x_chunk: int = 0, preempt: bool = False):
         self._L = load()
         opt = Options(precision=precision, device=device, kernel=KERNEL_FUSED, graph_steps=graph_steps,
                       tile_y=tile_y, x_chunk=x_chunk)
         cfg = ServerConfig(hbm_budget_bytes=int(hbm_budget_bytes), max_members=int(max_members),
-                           chunk_steps=int(chunk_steps))
+                           chunk_steps=int(chunk_steps), preempt=1 if preempt else 0)
         h = C.c_void_p()
         check(self._L.fdtd_server_create(C.byref(opt), C.byref(cfg), C.byref(h)))
         self._h = h
@@ -60,6 +63,10 @@ class SolveServer:
         check(self._L.fdtd_server_result(self._h, int(rid), buf.ctypes.data, buf.size, None, None, C.byref(lat)))
         return buf[: steps.value * nl.value].reshape(steps.value, nl.value), float(lat.value)
 
+    def cancel(self, rid: int):
+        """Cancel a queued or running request (its wait / result raise FDTD_ERR_CANCELLED)."""
+        check(self._L.fdtd_server_cancel(self._h, int(rid)))
+
     def drain(self, timeout_s: float = -1.0):
         check(self._L.fdtd_server_drain(self._h, float(timeout_s)))
 
@@ -86,4 +93,4 @@ class SolveServer:
         self.close()
 
 
-__all__ = ["SolveServer", "REQ_DONE", "REQ_FAILED"]
+__all__ = ["SolveServer", "REQ_DONE", "REQ_FAILED", "REQ_CANCELLED"]

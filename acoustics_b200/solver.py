@@ -24,12 +24,12 @@ class PML_WaveSolver:
 
     def __init__(self, scene: Scene, precision: int = PRECISION_FP64, kernel: int = KERNEL_FUSED,
                  graph_steps: int = 0, device: int = 0, tile_y: int = 0, x_chunk: int = 0,
-                 pml_state: int = PML_STATE_AUTO):
+                 pml_state: int = PML_STATE_AUTO, shell_staging: int = 0):
         self._L = load()
         self.scene = scene
         desc, self._keep = scene.to_c()
         opt = Options(precision=precision, device=device, kernel=kernel, graph_steps=graph_steps,
-                      tile_y=tile_y, x_chunk=x_chunk, pml_state=pml_state)
+                      tile_y=tile_y, x_chunk=x_chunk, pml_state=pml_state, shell_staging=shell_staging)
         h = C.c_void_p()
         check(self._L.fdtd_solver_create(C.byref(desc), C.byref(opt), C.byref(h)))
         self._h = h
@@ -60,6 +60,11 @@ class PML_WaveSolver:
     def pml_state(self) -> int:
         """PML_STATE_AUTO when this solve keeps the reduced PML state, else PML_STATE_FULL."""
         return int(self._L.fdtd_solver_pml_state(self._h))
+
+    def shell_staging(self) -> int:
+        """SHELL_STAGING_TMA or SHELL_STAGING_RING for the reduced-state PML shell in
+        effect, -1 when the solve keeps the full PML state."""
+        return int(self._L.fdtd_solver_shell_staging(self._h))
 
     def Reinitialize_PML_WaveSolver(self, start_time: float = 0.0):
         check(self._L.fdtd_solver_reset(self._h, float(start_time)), self._h)

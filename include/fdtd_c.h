@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define FDTD_ABI_VERSION 3
+#define FDTD_ABI_VERSION 4
 
 typedef int32_t fdtd_status;
 enum {
@@ -37,7 +37,8 @@ enum {
     FDTD_ERR_GEOMETRY = -6,        /* fresh cell inside an object (MAC_Grid.cpp:2050-2053) */
     FDTD_ERR_UNSUPPORTED = -7,     /* a reference feature outside this library's scope */
     FDTD_ERR_IO = -8,
-    FDTD_ERR_BUSY = -9             /* server queue full / slot table full */
+    FDTD_ERR_BUSY = -9,            /* server queue full / slot table full */
+    FDTD_ERR_CANCELLED = -10       /* the request was cancelled (fdtd_server_cancel) */
 };
 
 /* ---------------------------------------------------------------------------
@@ -154,8 +155,20 @@ typedef struct {
     int32_t tile_y;           /* fused path: x planes a PML-shell thread marches over; 0: 8   */
     int32_t x_chunk;          /* fused path: interior x planes per thread (2, 4, 8); 0: 2        */
     int32_t pml_state;        /* FDTD_PML_STATE_*                                        */
-    int32_t _reserved1;       /* 0 */
+    int32_t shell_staging;    /* FDTD_SHELL_STAGING_*                                    */
 } fdtd_options;
+
+enum {
+    /* How the PML-shell kernel of FP32 solves on the reduced PML state stages its
+     * loads (same results either way):
+     * AUTO: 3-D tensor copies (TMA) of every plane into a shared-memory ring,
+     * where the driver provides the tensor-map encoder and the shell fits its
+     * windows; else per-thread asynchronous copies (cp.async).  Batch members
+     * use the per-thread copies. */
+    FDTD_SHELL_STAGING_AUTO = 0,
+    FDTD_SHELL_STAGING_RING = 1,  /* per-thread cp.async ring always */
+    FDTD_SHELL_STAGING_TMA = 2    /* reported by fdtd_solver_shell_staging: tensor copies in effect */
+};
 
 enum {
     /* FP32 fused solves of static scenes with no solid cell inside the PML keep the
@@ -219,6 +232,16 @@ typedef struct fdtd_solver fdtd_solver;
 int32_t fdtd_abi_version(void);
 const char* fdtd_last_error(void);           /* thread-local message of the last failed call */
 fdtd_status fdtd_device_count(int32_t* count);
+
+/* Host-side failure injection for tests of the error paths (no counterpart in
+ * the reference; nothing is done to the GPU): the (after+1)-th allocation of the
+ * chosen kind from now on, counted over the process, fails as if memory were
+ * exhausted, and the call that made it returns FDTD_ERR_OOM.  Device: the arena
+ * of fdtd_solver_create (also reached by fdtd_batch_add and the solve server's
+ * admissions).  Host: the pinned listener staging buffer of fdtd_solver_create
+ * and the staging of fdtd_solver_get_field.  FDTD_INJECT_NONE disarms. */
+enum { FDTD_INJECT_NONE = 0, FDTD_INJECT_DEVICE_ALLOC = 1, FDTD_INJECT_HOST_ALLOC = 2 };
+fdtd_status fdtd_debug_inject_failure(int32_t what, int32_t after);
 
 /* Parser defaults of <gaussian_pressure_source> (ImpulseResponseParser.cpp:657-669):
  * width_space <= 0 -> sound_speed*width_time; normalize_constant == 0 ->
@@ -303,6 +326,10 @@ fdtd_status fdtd_solver_boundary_info(fdtd_solver* s, int64_t* n_rows, int64_t* 
 /* PML state in effect: FDTD_PML_STATE_FULL, or FDTD_PML_STATE_AUTO when the
  * reduced state is used (no counterpart in the reference). */
 int32_t fdtd_solver_pml_state(fdtd_solver* s);
+/* Staging of the reduced-state PML-shell kernel in effect: FDTD_SHELL_STAGING_TMA
+ * or FDTD_SHELL_STAGING_RING; -1 when the solve keeps the full PML state (no
+ * counterpart in the reference). */
+int32_t fdtd_solver_shell_staging(fdtd_solver* s);
 /* Kernel launches issued by the most recent fdtd_solver_step* call. */
 int64_t fdtd_solver_last_launch_count(fdtd_solver* s);
 /* Steps since creation whose PML-shell kernel ran beside the step's cell
@@ -378,6 +405,17 @@ fdtd_status fdtd_batch_member_info(fdtd_batch* b, int32_t member, int64_t* steps
                                    int32_t* n_listeners, int32_t* status);
 /* listener series of a member so far: steps_done x n_listeners doubles */
 fdtd_status fdtd_batch_output(fdtd_batch* b, int32_t member, double* out, int64_t count);
+/* The state of a member (fdtd_solver_snapshot of its solve; query the size with
+ * buffer NULL).  With fdtd_batch_add_snapshot it moves a member out of device
+ * memory and back, as the solve server's eviction does. */
+fdtd_status fdtd_batch_member_snapshot(fdtd_batch* b, int32_t member, void* buffer, int64_t* bytes);
+/* Add a member that continues from a snapshot of a member (or solver) of the
+ * same scene and options: steps_total counts from the solve's start, rows holds
+ * its listener series so far (steps_done x n_listeners doubles, steps_done = the
+ * snapshot's step; NULL when n_listeners is 0).  No step runs here. */
+fdtd_status fdtd_batch_add_snapshot(fdtd_batch* b, const fdtd_scene_desc* scene, int32_t steps_total,
+                                    const void* snapshot, int64_t bytes, const double* rows, int64_t steps_done,
+                                    int32_t* member);
 /* stop a member if it still runs, free its device memory and series; its index becomes free */
 fdtd_status fdtd_batch_release(fdtd_batch* b, int32_t member);
 fdtd_status fdtd_batch_destroy(fdtd_batch* b);
@@ -406,10 +444,19 @@ typedef struct {
     int64_t hbm_budget_bytes;  /* device bytes the members may hold; 0: 90% of free memory at create */
     int32_t max_members;       /* members stepped together; 0: 256; 1 gives FIFO service           */
     int32_t chunk_steps;       /* batched steps between admissions; 0: max(graph_steps, 32)       */
-    int32_t _pad;
+    int32_t preempt;           /* 1: evict running members to admit a shorter queue head (below)   */
 } fdtd_server_config;
+/* Eviction (preempt = 1; the reference's snapshot, FDTD_AcousticSimulator.cpp:381-415,
+ * used as the server's preemption): when the request at the head of the queue
+ * does not fit the free budget, running members with more than twice its
+ * cell-steps still to go are evicted, most remaining work first, until it fits.
+ * An evicted member's state (fdtd_batch_member_snapshot) and listener rows stay
+ * in host memory, its device memory is released, and it goes back into the
+ * queue right behind the head; re-admitted, it continues where it stopped and
+ * its series equals an uninterrupted solve's bit for bit. */
 
-enum { FDTD_REQ_QUEUED = 0, FDTD_REQ_RUNNING = 1, FDTD_REQ_DONE = 2, FDTD_REQ_FAILED = 3 };
+enum { FDTD_REQ_QUEUED = 0, FDTD_REQ_RUNNING = 1, FDTD_REQ_DONE = 2, FDTD_REQ_FAILED = 3,
+       FDTD_REQ_CANCELLED = 4 };
 
 typedef struct {
     int64_t submitted, completed, failed, queued, running;
@@ -419,6 +466,9 @@ typedef struct {
     double span_s;                  /* first submit -> last completion                         */
     double solves_per_s;            /* completed / span_s                                      */
     double cell_steps_per_s;        /* sum of cells x steps of completed requests / span_s     */
+    int64_t device_bytes_in_use;    /* footprints of the members now admitted                  */
+    int64_t cancelled;              /* requests cancelled                                      */
+    int64_t evictions;              /* members evicted to host memory (preempt)                */
 } fdtd_server_stats;
 
 fdtd_status fdtd_server_create(const fdtd_options* options, const fdtd_server_config* config, fdtd_server** out);
@@ -433,8 +483,14 @@ fdtd_status fdtd_server_wait(fdtd_server* srv, int64_t request, double timeout_s
 /* steps x n_listeners doubles and the latency; the request is forgotten afterwards */
 fdtd_status fdtd_server_result(fdtd_server* srv, int64_t request, double* out, int64_t count, int64_t* steps,
                                int32_t* n_listeners, double* latency_s);
-/* block until every submitted request is done or failed */
+/* block until every submitted request is done, failed or cancelled */
 fdtd_status fdtd_server_drain(fdtd_server* srv, double timeout_s);
+/* Cancel a queued or running request: a queued one leaves the queue, a running
+ * one is stopped at the end of the batched chunk in progress and its device
+ * memory released; its state becomes FDTD_REQ_CANCELLED and fdtd_server_wait /
+ * fdtd_server_result return FDTD_ERR_CANCELLED.  FDTD_ERR_INVALID_ARG for an
+ * unknown or already finished request.  (No counterpart in the reference.) */
+fdtd_status fdtd_server_cancel(fdtd_server* srv, int64_t request);
 fdtd_status fdtd_server_stats_get(fdtd_server* srv, fdtd_server_stats* stats);
 /* the error text of a failed request */
 const char* fdtd_server_request_error(fdtd_server* srv, int64_t request);

@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol(fdtd_lib):
 
 
 def test_abi_version(fdtd_lib):
-    assert fdtd_lib.fdtd_abi_version() == 3
+    assert fdtd_lib.fdtd_abi_version() == 4
 
 
 def test_struct_layouts_match_header(tmp_path):
