@@ -45,8 +45,14 @@ def scene_info(scene: Scene, precision: int = PRECISION_FP32_COMPENSATED, kernel
 class SolveBatch:
     def __init__(self, scenes: Sequence[Scene] = (), steps: Optional[Sequence[int]] = None,
                  precision: int = PRECISION_FP32_COMPENSATED, graph_steps: int = 16, device: int = 0,
-                 tile_y: int = 0, x_chunk: int = 0):
+                 tile_y: int = 0, x_chunk: int = 0, tune: bool = True):
+        """`tile_y` / `x_chunk` 0 with `tune`: the autotuned shapes of the grid
+        class of `scenes` (acoustics_b200.autotune; tuned now on a cache miss)."""
         self._L = load()
+        if tune and scenes and tile_y == 0 and x_chunk == 0:
+            from .autotune import shapes_for
+            x_chunk, tile_y = shapes_for(list(scenes), precision, device=device)
+        self.shape = (x_chunk, tile_y)
         opt = Options(precision=precision, device=device, kernel=KERNEL_FUSED, graph_steps=graph_steps,
                       tile_y=tile_y, x_chunk=x_chunk)
         h = C.c_void_p()

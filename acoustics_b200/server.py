@@ -24,8 +24,14 @@ from .scene import (KERNEL_FUSED, PRECISION_FP32_COMPENSATED, REQ_CANCELLED, REQ
 class SolveServer:
     def __init__(self, precision: int = PRECISION_FP32_COMPENSATED, graph_steps: int = 16, device: int = 0,
                  hbm_budget_bytes: int = 0, max_members: int = 0, chunk_steps: int = 0, tile_y: int = 0,
-                 x_chunk: int = 0, preempt: bool = False):
+                 x_chunk: int = 0, preempt: bool = False, tune_for=None):
+        """`tune_for`: scenes typical of the requests; with `tile_y` / `x_chunk` 0 the
+        batched step uses the autotuned shapes of their grid class."""
         self._L = load()
+        if tune_for and tile_y == 0 and x_chunk == 0:
+            from .autotune import shapes_for
+            x_chunk, tile_y = shapes_for(list(tune_for), precision, device=device)
+        self.shape = (x_chunk, tile_y)
         opt = Options(precision=precision, device=device, kernel=KERNEL_FUSED, graph_steps=graph_steps,
                       tile_y=tile_y, x_chunk=x_chunk)
         cfg = ServerConfig(hbm_budget_bytes=int(hbm_budget_bytes), max_members=int(max_members),

@@ -168,7 +168,7 @@ def profile_run(args):
         # the 64 uneven scenes stepped eagerly (no graphs), so every kernel is listed
         from acoustics_b200.batch import SolveBatch
         scenes = S.config3()
-        b = SolveBatch(scenes, precision=prec, graph_steps=0, tile_y=args.tile_y, x_chunk=args.x_chunk)
+        b = SolveBatch(scenes, precision=prec, graph_steps=0, tile_y=args.tile_y, x_chunk=args.x_chunk, tune=False)
         b.step(args.steps)
         launches = b.last_launch_count()
         b.close()
@@ -212,7 +212,15 @@ def bench_batched(peak: float, fp64_check: bool = True):
     out = {"workload": "config3: 64 uneven scenes, edges log-uniform [48,160], 1000-3000 steps",
            "scenes": len(scenes), "cells": int(sum(i.n_cells for i in infos)),
            "cell_steps": int(cell_steps), "graph_steps": 16}
-    b = SolveBatch(scenes, precision=P32, graph_steps=16)
+    # tile shapes from the autotuner (every candidate timed on a sample of the
+    # scenes, outside the timed region; cached per grid class)
+    from acoustics_b200 import autotune
+    t0 = time.perf_counter()
+    tuned = autotune.tune(scenes, P32)
+    out["autotune"] = {"x_chunk": tuned["x_chunk"], "tile_y": tuned["tile_y"], "key": tuned["key"],
+                       "timings_ms_per_step": tuned["timings_ms"], "sample_scenes": tuned["sample_scenes"],
+                       "seconds": time.perf_counter() - t0}
+    b = SolveBatch(scenes, precision=P32, graph_steps=16, x_chunk=tuned["x_chunk"], tile_y=tuned["tile_y"])
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     b.run()
@@ -237,7 +245,7 @@ def bench_batched(peak: float, fp64_check: bool = True):
     out.update({"one_by_one_seconds": dt1, "one_by_one_gcell_steps_s": cell_steps / dt1 / 1e9,
                 "speedup_vs_one_by_one": dt1 / dt})
     if fp64_check:
-        b64 = SolveBatch(scenes, precision=S.PRECISION_FP64, graph_steps=16)
+        b64 = SolveBatch(scenes, precision=S.PRECISION_FP64, graph_steps=16, tune=False)
         b64.run()
         y64 = [b64.output(m) for m in range(len(scenes))]
         b64.close()
@@ -297,7 +305,7 @@ def bench_served(peak: float, rate: float, n_requests: int, fifo_plain: bool = F
 
     def serve(scale):
         # the same requests arriving `scale` times faster (seeded gaps / scale)
-        with SolveServer(precision=P32, graph_steps=16, chunk_steps=32) as srv:
+        with SolveServer(precision=P32, graph_steps=16, chunk_steps=32, tune_for=[sc for _, sc in reqs]) as srv:
             t0 = time.perf_counter()
             ids = []
             for t_arr, sc in reqs:

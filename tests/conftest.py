@@ -9,6 +9,10 @@ if ROOT not in sys.path:
 
 
 def pytest_configure(config):
+    # tuned tile shapes of this session only (the autotuner runs on a cache miss)
+    if "FDTD_TUNE_CACHE" not in os.environ:
+        import tempfile
+        os.environ["FDTD_TUNE_CACHE"] = os.path.join(tempfile.mkdtemp(prefix="fdtd_tune_"), "tuned.json")
     config.addinivalue_line("markers", "gpu: needs a CUDA device (B200, sm_100a)")
     config.addinivalue_line("markers", "slow: long-running")
 
