@@ -265,13 +265,16 @@ fdtd_status run_classification(fdtd_solver* s) {
 namespace fdtd {
 
 // Whether a solve keeps the reduced PML state (k_pml_shell_red): FP32 fused
-// solves of static scenes with no solid PML cell, the five-box shell, and, along
+// solves of static scenes with no solid PML cell, or of moving bodies that stay
+// two cells clear of the PML at every step until end_time, the five-box shell, and, along
 // every axis, unit decay factors on both faces of every cell outside that axis'
 // PML (the condition under which the plain axes of a PML cell telescope into one
 // leapfrog increment exactly).
 bool use_reduced_pml(const fdtd_solver* s, bool no_solid_pml) {
     if (s->precision != FDTD_PRECISION_FP32_COMPENSATED || s->opt.kernel != FDTD_KERNEL_FUSED) return false;
-    if (s->opt.pml_state != FDTD_PML_STATE_AUTO || s->moving || !no_solid_pml) return false;
+    if (s->opt.pml_state != FDTD_PML_STATE_AUTO || !no_solid_pml) return false;
+    // moving bodies only when they stay clear of the PML until end_time
+    if (s->moving && !moving_clear_of_pml(const_cast<fdtd_solver*>(s))) return false;
     if (s->shell.n != 5 || s->shell.zbox != 4) return false;
     for (int d = 0; d < 3; ++d) {
         const auto& T = s->tab[d];

@@ -135,6 +135,8 @@ inline cudaError_t counted_copyAsync(fdtd_solver* s, void* dst, const void* src,
     return cudaMemcpyAsync(dst, src, n, kind, stream);
 }
 void set_error(fdtd_solver* s, const std::string& msg);
+// moving bodies two cells clear of the PML through [start_time, end_time]
+bool moving_clear_of_pml(fdtd_solver* s);
 // listener plans of a static solve from its current classification (after a restore)
 fdtd_status rebuild_listener_plans(fdtd_solver* s);
 // fdtd_debug_inject_failure: true when this allocation of kind `what` is to fail

@@ -111,6 +111,11 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         // MAC_Grid::classifyCells_FAST + InterpolateFreshPressureCell (PML_WaveSolver.cpp:807-812)
         const ClsBoxes prev = s->hP.boxes;
         classification_boxes(s, s->hP.boxes);
+        if (s->moving && s->region.red && !boxes_clear_of_shell(s, s->hP.boxes)) {
+            // past the end time the bodies were checked for: the reduced PML state no longer holds
+            set_error(s, "a moving body came within two cells of the PML of a reduced-state solve (past its end_time)");
+            return FDTD_ERR_UNSUPPORTED;
+        }
         // Moving bodies clear of the PML: the shell kernel reads nothing the
         // classification writes, so it starts first, on stream5, beside it.
         shell_ahead = s->moving && fused && s->cls_boxes_current && s->n_solid_pml == 0 && !s->hP.visc &&
@@ -727,6 +732,40 @@ std::vector<std::pair<void*, size_t>> snap_regions(fdtd_solver* s) {
 }  // extern "C"
 
 namespace fdtd {
+// Moving bodies that stay two cells clear of the PML at every step of
+// [start_time, end_time]: the per-step classification boxes of the whole run,
+// posed and unioned as the step driver does, are checked on the host.  Then no
+// PML cell is ever solid or next to a solid, and the reduced PML state is exact.
+bool moving_clear_of_pml(fdtd_solver* s) {
+    if (!s->moving || !(s->end_time > s->start_time) || !(s->k > 0)) return false;
+    const double nsteps = std::ceil((s->end_time - s->start_time) / s->k) + 2.0;
+    if (nsteps > 2.0e7) return false;
+    std::vector<HostObject> objs = s->objs;
+    double t = s->start_time;
+    for (auto& o : objs) {
+        host_object_pose(o, t);
+        host_update_bbox(o);
+        host_reset_union(o);
+    }
+    bool clear = true;
+    std::swap(s->objs, objs);  // classification_boxes reads s->objs
+    ClsBoxes B;
+    for (long long i = 0; i <= (long long)nsteps && clear; ++i) {
+        if (i > 0) {
+            t += s->k;
+            for (auto& o : s->objs) {
+                if (o.d.motion == FDTD_MOTION_STATIC) continue;
+                host_object_pose(o, t);
+                host_update_bbox(o);
+            }
+        }
+        classification_boxes(s, B);
+        clear = boxes_clear_of_shell(s, B);
+    }
+    std::swap(s->objs, objs);
+    return clear;
+}
+
 // Listener plans (fixed MLS weights) of a static solve from its current
 // classification, as its first step builds them; used after a restore.
 fdtd_status rebuild_listener_plans(fdtd_solver* s) {

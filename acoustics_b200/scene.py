@@ -491,6 +491,9 @@ def config5(seed: int = 7, steps: int = 6000) -> Scene:
         sc.objects.append(RigidObject(SHAPE_SPHERE, tuple(x0), (r, 0, 0), motion=MOTION_BALLISTIC,
                                       velocity=tuple(v0), gravity=tuple(g)))
     sc.sources.append(GaussianSource((0.0, 0.12, 0.0), 1e-4))
+    # the run ends after `steps` steps (<time_end>): the library can then check
+    # that the spheres stay clear of the PML throughout
+    sc.end_time = steps * k
     lis = []
     rng2 = np.random.default_rng(seed + 100)
     lo, hi = _non_pml_box(sc, 2.0)

@@ -120,6 +120,32 @@ def test_moving_bodies(oracle_lib, fdtd_lib, precision, tol):
         assert np.array_equal(go, gg), chunk
 
 
+def test_moving_bodies_reduced_pml_state(oracle_lib, fdtd_lib):
+    """Moving bodies that stay clear of the PML until end_time keep the reduced
+    PML state (TMA-staged shell): classification bit-exact after every chunk,
+    listener series within 1e-4 of the FP64 oracle and 1e-5 of the full state."""
+    sc = moving_scene()
+    sc.end_time = sc.steps * sc.time_step
+    o = oracle_lib.OracleSolver(sc)
+    g = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED)
+    f = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED, pml_state=S.PML_STATE_FULL)
+    assert g.pml_state() == S.PML_STATE_AUTO and f.pml_state() == S.PML_STATE_FULL
+    assert g.shell_staging() == S.SHELL_STAGING_TMA
+    yo, yg, yf = [], [], []
+    for chunk in range(4):
+        yo.append(o.step(40))
+        yg.append(g.step(40))
+        yf.append(f.step(40))
+        fo, go = o.classification()
+        fg, gg = g.GetGrid()
+        assert np.array_equal(fo, fg), chunk
+        assert np.array_equal(go, gg), chunk
+    yo, yg, yf = np.concatenate(yo), np.concatenate(yg), np.concatenate(yf)
+    assert rel_l2(yg, yo) <= TOL_FP32
+    assert rel_l2(yg, yf) <= 1e-5
+    assert g.overlapped_steps() > 0
+
+
 def test_reduced_pml_state_fp32(oracle_lib, fdtd_lib):
     """FP32 static solves keep the reduced PML state (one leapfrog increment for
     the axes without absorption of a PML cell): listener series and pressure
