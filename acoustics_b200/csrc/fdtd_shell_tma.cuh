@@ -3,31 +3,33 @@
 //
 // The arithmetic per cell is that of shell_tile_red_impl (fdtd_shell_red.cuh),
 // in the same order, so the two kernels give the same bits; what changes is how
-// the operands reach the threads.  A CTA of 128 threads owns one tile of the
-// shell: TY rows x TZ cells of a (y, z) window, four consecutive z cells per
-// thread, and marches along x over the tile's planes.  Per x plane one thread
-// issues 3-D bulk tensor copies (cp.async.bulk.tensor, this GPU's memory only,
-// no multicast) of every array the tile reads into one stage of a 4-stage
-// shared-memory ring, completed on that stage's mbarrier:
+// the work is cut and how the operands reach the threads.
+//
+// Tiles.  The shell is cut by absorbing axes: every tile holds cells that
+// absorb along the same axes (x only, y only, z only, the three edges' pairs,
+// the corners), so the update of a tile is one of seven specialised bodies
+// with no per-cell axis tests, and a tile stages only the arrays its axes use.
+// A CTA of 128 threads owns one tile: ty rows x tz cells of a (y, z) window
+// (four consecutive z cells per thread), marching along x over at most 16
+// planes.  Window shapes follow the extents of the tile class (a z-PML window
+// is as wide as the z slab, y-slab tiles as high as the y slab), so the copies
+// carry few cells outside the shell.
+//
+// Staging.  Per x plane one thread issues 3-D bulk tensor copies
+// (cp.async.bulk.tensor, tensor maps in device memory describing this GPU's
+// arrays, no multicast) of every array the tile reads into one stage of a
+// 4-stage shared-memory ring, completed on that stage's mbarrier:
 //   P   p^n with a one-cell halo in y and a four-cell halo in z (z stays a
 //       multiple of 4: the copy's innermost coordinate is 16-byte aligned;
 //       halo cells outside the grid read as zeros and are never used)
-//   VX  x faces of the plane (x slabs), VY the TY+1 y faces of its rows,
-//   VZ  the TZ+4 z faces of its rows, A0..A2 the reduced split state.
+//   VX  x faces of the plane, VY the ty+1 y faces of its rows, VZ the tz+4 z
+//       faces of its rows, A0..A2 the reduced split state.
 // At plane x the threads read P of x-1, x, x+1 and the faces of x and x+1 from
-// the ring: no per-thread address, clamp or predicate work for loads, each p
-// value crosses L2 -> SM about 1.4 times instead of 5.  Results are stored
-// from registers with 16-byte vector stores.  All storage is the grid's
-// (the z slabs too: a tile window reads their 16-cell rows as 3-D boxes).
-//
-// Tiles (host side, build_tma_tiles): x slabs and y slabs in TZ0 x TY0 = 64 x 8
-// windows, z slabs in TZ1 x TY1 windows (TZ1 = the slab width rounded up to a
-// power of two, TY1 = 512 / TZ1); each tile covers at most 16 x planes.
+// the ring and store their results from registers with 16-byte vector stores.
 // Every wait on an mbarrier is bounded: after about a second without
 // completion the kernel records FDTD_DEV_ERR_TMA_TIMEOUT, waits (bounded) for
 // its copies still in flight and returns.
 #pragma once
-
 #include "fdtd_tma.hpp"
 
 namespace fdtd {
@@ -53,7 +55,7 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
         : "memory");
     return ok != 0;
 }
-// bounded wait: false after ~2^22 polls (each poll may suspend the thread for a
+// bounded wait: false after 2^22 polls (each poll may suspend the thread for a
 // while inside try_wait), about a second
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     for (int it = 0; it < (1 << 22); ++it)
@@ -70,16 +72,17 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
 }
 
 // Copies of ring stage j (plane x0 - 1 + j): P always; the x faces of planes
-// x0..x0+nx (x slabs); the other arrays of planes x0..x0+nx-1.
-__device__ __forceinline__ void tma_issue_stage(const TmaMaps& M, const TmaShape& S, int sh, const TmaTile& T,
+// x0..x0+nx (tiles absorbing along x); the other arrays of planes x0..x0+nx-1.
+__device__ __forceinline__ void tma_issue_stage(const CUtensorMap* m, const TmaShape& S, const TmaTile& T,
                                                 uint32_t stage, uint32_t bar, int j) {
     const int xs = T.x0 - 1 + j;
+    const bool ex = T.cls & TC_X, ey = T.cls & TC_Y, ez = T.cls & TC_Z;
     const bool state = j >= 1 && j <= T.nx;
-    const bool vx = T.kind == 0 && j >= 1 && j <= T.nx + 1;
-    const bool vy = state && (T.flags & TT_VY);
-    const bool vz = state && (T.flags & TT_VZ);
-    const bool a1 = state && T.kind != 2;
-    const bool a2 = state && (T.flags & TT_A2);
+    const bool vx = ex && j >= 1 && j <= T.nx + 1;
+    const bool vy = state && ey;
+    const bool vz = state && ez;
+    const bool a1 = state && (ex || ey);
+    const bool a2 = state && (ez || (ex && ey));
     uint32_t bytes = S.bytes[TB_P];
     if (vx) bytes += S.bytes[TB_VX];
     if (vy) bytes += S.bytes[TB_VY];
@@ -88,7 +91,6 @@ __device__ __forceinline__ void tma_issue_stage(const TmaMaps& M, const TmaShape
     if (a1) bytes += S.bytes[TB_A1];
     if (a2) bytes += S.bytes[TB_A2];
     mbar_expect_tx(bar, bytes);
-    const CUtensorMap* m = M.m[sh];
     tma_load_3d(stage + S.off[TB_P], &m[TB_P], T.z0 - 4, T.y0 - 1, xs, bar);
     if (vx) tma_load_3d(stage + S.off[TB_VX], &m[TB_VX], T.z0, T.y0, xs, bar);
     if (vy) tma_load_3d(stage + S.off[TB_VY], &m[TB_VY], T.z0, T.y0, xs, bar);
@@ -98,83 +100,91 @@ __device__ __forceinline__ void tma_issue_stage(const TmaMaps& M, const TmaShape
     if (a2) tma_load_3d(stage + S.off[TB_A2], &m[TB_A2], T.z0, T.y0, xs, bar);
 }
 
-template <int V>
-__device__ __forceinline__ Vec<float, V> lds(const unsigned char* base, int elem) {
-    return *reinterpret_cast<const Vec<float, V>*>(base + 4 * elem);
+__device__ __forceinline__ Vec<float, 4> lds4(const unsigned char* base, int elem) {
+    return *reinterpret_cast<const Vec<float, 4>*>(base + 4 * elem);
+}
+__device__ __forceinline__ float lds1(const unsigned char* base, int elem) {
+    return *reinterpret_cast<const float*>(base + 4 * elem);
 }
 
-// One plane of one thread's four cells.  KIND / EY as in shell_tile_red_impl;
+// Per-thread constants of a tile: its cells and their flags and coefficients.
+struct TmaThread {
+    int r, lz, zc, y;
+    unsigned inbox;              // cells of the box among the four
+    uint8_t gy;                  // y flags of the row
+    unsigned zm[6];              // z flag bits of the four cells (flag_mask)
+    AxisCoef<float> cz[5];       // z coefficients of the cells and the next face (EZ)
+    AxisCoef<float> cyl, cyr;    // y coefficients of the row (EY)
+};
+
+// One plane of one thread's four cells, for a tile absorbing along EX / EY / EZ.
 // sM, s0, sP: the ring stages of planes x-1, x, x+1.
-template <int KIND, bool EY>
+template <bool EX, bool EY, bool EZ>
 __device__ __forceinline__ void tma_plane(const KArgs<float>& A, const TmaShape& S, const unsigned char* sM,
-                                          const unsigned char* s0, const unsigned char* sP, int x, int y, int r,
-                                          int zc, int lz, unsigned inbox, uint8_t gy, const unsigned (&zm)[6],
-                                          const AxisCoef<float> (&cz)[5], const AxisCoef<float>& cyl,
-                                          const AxisCoef<float>& cyr) {
+                                          const unsigned char* s0, const unsigned char* sP, int x,
+                                          const TmaThread& H) {
     using T = float;
     constexpr int V = 4;
     constexpr unsigned ALL = 0xFu;
-    constexpr bool EX = KIND == 0;
     using VT = Vec<T, V>;
     const int tz = S.tz;
-    const int pw = tz + 8;                       // P row width
-    const int pc = (r + 1) * pw + lz + 4;        // this thread's cells in P
-    const unsigned zpml = zm[0], zflo = zm[1], zfhi = zm[2], znext = zm[3], zhlo = zm[4], zhhi = zm[5];
-    const unsigned ezm = zpml & inbox;
-    const unsigned mpy = (gy & AXF_PML) ? ALL : 0u;
-    const unsigned mpx = EX ? ALL : 0u;
-    const unsigned fyl = ((gy & AXF_FACE_LO) ? ALL : 0u) | ((gy & AXF_HAS_LO) ? (mpx | zpml) : 0u);
-    const unsigned fyr = ((gy & AXF_FACE_HI) ? ALL : 0u) | ((gy & AXF_HAS_HI) ? (mpx | zpml) : 0u);
-    const unsigned fzl = zflo | (zhlo & (mpx | mpy));
-    const unsigned fzr = zfhi | (zhhi & (mpx | mpy));
-    const unsigned m_yl = EY ? inbox & fyl : 0u;
-    const unsigned m_yr = EY ? inbox & fyr & ((gy & AXF_NEXT_PML) ? 0u : ALL) : 0u;
-    const unsigned m_zl = ezm & fzl;
-    const unsigned m_zr = ezm & fzr & ~znext;
-    const unsigned m_a1 = KIND == 2 ? 0u : inbox;
-    const unsigned m_a2 = (KIND == 0 && EY) ? inbox : ezm;
+    const int pw = tz + 8;                      // P row width
+    const int pc = (H.r + 1) * pw + H.lz + 4;   // this thread's cells in P
+    const unsigned inbox = H.inbox;
+    // masks of the face rules (as in shell_tile_red_impl; the axis sets are the tile's)
+    const unsigned zpml = EZ ? ALL : 0u;
+    const unsigned mpx = EX ? ALL : 0u, mpy = EY ? ALL : 0u;
+    const unsigned ezm = EZ ? inbox : 0u;
 
     const unsigned char* P0 = s0 + S.off[TB_P];
-    const VT p0 = lds<V>(P0, pc);
-    const VT pm = lds<V>(sM + S.off[TB_P], pc);
-    const VT pp = lds<V>(sP + S.off[TB_P], pc);
-    const VT ym = lds<V>(P0, pc - pw);
-    const VT yp = lds<V>(P0, pc + pw);
-    const T zme = *reinterpret_cast<const T*>(P0 + 4 * (pc - 1));
-    const T zpe = *reinterpret_cast<const T*>(P0 + 4 * (pc + V));
-    const int ai = r * tz + lz;                 // this thread's cells in the TZ-wide buffers
+    const VT p0 = lds4(P0, pc);
+    const VT pm = lds4(sM + S.off[TB_P], pc);
+    const VT pp = lds4(sP + S.off[TB_P], pc);
+    const VT ym = lds4(P0, pc - pw);
+    const VT yp = lds4(P0, pc + pw);
+    const T zme = lds1(P0, pc - 1);
+    const T zpe = lds1(P0, pc + V);
+    const int ai = H.r * tz + H.lz;             // this thread's cells in the tz-wide buffers
     VT vxl, vxr, vyl, vyr, vzl, a0, a1, a2;
     T vze = 0.0f;
     AxisCoef<T> cxl, cxr;
-    uint8_t g = 0;
-    if constexpr (EX) {
-        vxl = lds<V>(s0 + S.off[TB_VX], ai);
-        vxr = lds<V>(sP + S.off[TB_VX], ai);
-        g = __ldg(A.axflag[0] + x);
-        cxl = A.coef[0][x];
-        cxr = A.coef[0][x + 1];
-    }
-    if constexpr (EY) {
-        vyl = lds<V>(s0 + S.off[TB_VY], ai);
-        vyr = lds<V>(s0 + S.off[TB_VY], ai + tz);
-    }
-    if (ezm) {
-        const int zi = r * (tz + 4) + lz;
-        vzl = lds<V>(s0 + S.off[TB_VZ], zi);
-        vze = *reinterpret_cast<const T*>(s0 + S.off[TB_VZ] + 4 * (zi + V));
-    }
-    a0 = lds<V>(s0 + S.off[TB_A0], ai);
-    if constexpr (KIND != 2) a1 = lds<V>(s0 + S.off[TB_A1], ai);
-    if ((KIND == 0 && EY) || ezm) a2 = lds<V>(s0 + S.off[TB_A2], ai);
-
     unsigned fxl = 0, fxr = 0, m_xl = 0, m_xr = 0;
     if constexpr (EX) {
+        vxl = lds4(s0 + S.off[TB_VX], ai);
+        vxr = lds4(sP + S.off[TB_VX], ai);
+        const uint8_t g = __ldg(A.axflag[0] + x);
+        cxl = A.coef[0][x];
+        cxr = A.coef[0][x + 1];
         const unsigned oyz = mpy | zpml;
         fxl = ((g & AXF_FACE_LO) ? ALL : 0u) | ((g & AXF_HAS_LO) ? oyz : 0u);
         fxr = ((g & AXF_FACE_HI) ? ALL : 0u) | ((g & AXF_HAS_HI) ? oyz : 0u);
         m_xl = inbox & fxl;
         m_xr = inbox & fxr & ((g & AXF_NEXT_PML) ? 0u : ALL);
     }
+    unsigned fyl = 0, fyr = 0, m_yl = 0, m_yr = 0;
+    if constexpr (EY) {
+        vyl = lds4(s0 + S.off[TB_VY], ai);
+        vyr = lds4(s0 + S.off[TB_VY], ai + tz);
+        const uint8_t gy = H.gy;
+        fyl = ((gy & AXF_FACE_LO) ? ALL : 0u) | ((gy & AXF_HAS_LO) ? (mpx | zpml) : 0u);
+        fyr = ((gy & AXF_FACE_HI) ? ALL : 0u) | ((gy & AXF_HAS_HI) ? (mpx | zpml) : 0u);
+        m_yl = inbox & fyl;
+        m_yr = inbox & fyr & ((gy & AXF_NEXT_PML) ? 0u : ALL);
+    }
+    unsigned fzl = 0, fzr = 0, m_zl = 0, m_zr = 0;
+    if constexpr (EZ) {
+        const int zi = H.r * (tz + 4) + H.lz;
+        vzl = lds4(s0 + S.off[TB_VZ], zi);
+        vze = lds1(s0 + S.off[TB_VZ], zi + V);
+        fzl = H.zm[1] | (H.zm[4] & (mpx | mpy));
+        fzr = H.zm[2] | (H.zm[5] & (mpx | mpy));
+        m_zl = ezm & fzl;
+        m_zr = ezm & fzr & ~H.zm[3];
+    }
+    a0 = lds4(s0 + S.off[TB_A0], ai);
+    if constexpr (EX || EY) a1 = lds4(s0 + S.off[TB_A1], ai);
+    if constexpr (EZ || (EX && EY)) a2 = lds4(s0 + S.off[TB_A2], ai);
+
     const float ls = A.lap_scale, c2k2 = A.c2k2, inv_h = A.inv_h;
     VT nxl, nxr, nyl, nyr, nzl, o0, o1, o2, pn;
     T nzr[V];
@@ -183,7 +193,6 @@ __device__ __forceinline__ void tma_plane(const KArgs<float>& A, const TmaShape&
         const T pz = p0.e[e];
         const T pzm = e > 0 ? p0.e[e - 1] : zme;
         const T pzp = e < V - 1 ? p0.e[e + 1] : zpe;
-        const bool ez = (ezm >> e) & 1u;
         T lap = 0.0f, sn = 0.0f, so = 0.0f;
         if constexpr (EX) {
             const T l0 = vxl.e[e], r0 = vxr.e[e];
@@ -200,11 +209,11 @@ __device__ __forceinline__ void tma_plane(const KArgs<float>& A, const TmaShape&
         }
         if constexpr (EY) {
             const T l0 = vyl.e[e], r0 = vyr.e[e];
-            const T vl = ((fyl >> e) & 1u) ? vel_update<T>(l0, cyl.vupd, cyl.vgrad, pz, ym.e[e]) : l0;
-            const T vr = ((fyr >> e) & 1u) ? vel_update<T>(r0, cyr.vupd, cyr.vgrad, yp.e[e], pz) : r0;
+            const T vl = ((fyl >> e) & 1u) ? vel_update<T>(l0, H.cyl.vupd, H.cyl.vgrad, pz, ym.e[e]) : l0;
+            const T vr = ((fyr >> e) & 1u) ? vel_update<T>(r0, H.cyr.vupd, H.cyr.vgrad, yp.e[e], pz) : r0;
             nyl.e[e] = vl;
             nyr.e[e] = vr;
-            const T a = pd_update<T>(a1.e[e], cyl.pupd, cyl.pdiv, vr, vl, inv_h);
+            const T a = pd_update<T>(a1.e[e], H.cyl.pupd, H.cyl.pdiv, vr, vl, inv_h);
             o1.e[e] = a;
             sn = sn + a;
             so = so + a1.e[e];
@@ -212,30 +221,34 @@ __device__ __forceinline__ void tma_plane(const KArgs<float>& A, const TmaShape&
             lap = lap + (yp.e[e] + ym.e[e] - 2.0f * pz);
         }
         T az = 0.0f;
-        if (ez) {
+        if constexpr (EZ) {
             const T l0 = vzl.e[e], r0 = e < V - 1 ? vzl.e[e + 1] : vze;
-            const T vl = ((fzl >> e) & 1u) ? vel_update<T>(l0, cz[e].vupd, cz[e].vgrad, pz, pzm) : l0;
-            const T vr = ((fzr >> e) & 1u) ? vel_update<T>(r0, cz[e + 1].vupd, cz[e + 1].vgrad, pzp, pz) : r0;
+            const T vl = ((fzl >> e) & 1u) ? vel_update<T>(l0, H.cz[e].vupd, H.cz[e].vgrad, pz, pzm) : l0;
+            const T vr = ((fzr >> e) & 1u) ? vel_update<T>(r0, H.cz[e + 1].vupd, H.cz[e + 1].vgrad, pzp, pz) : r0;
             nzl.e[e] = vl;
             nzr[e] = vr;
-            az = pd_update<T>(a2.e[e], cz[e].pupd, cz[e].pdiv, vr, vl, inv_h);
+            az = pd_update<T>(a2.e[e], H.cz[e].pupd, H.cz[e].pdiv, vr, vl, inv_h);
             sn = sn + az;
             so = so + a2.e[e];
         } else {
-            nzl.e[e] = 0.0f;
-            nzr[e] = 0.0f;
             lap = lap + (pzp + pzm - 2.0f * pz);
         }
-        const T qold = EX ? (EY ? a2.e[e] : a1.e[e]) : a0.e[e];
-        const T qn = fmaf(lap * ls, c2k2, qold);
-        const bool plain = !(EX && EY && ez);
-        pn.e[e] = (sn + (pz - so)) + (plain ? qn : 0.0f);
-        if constexpr (!EX) o0.e[e] = qn;
-        if constexpr (EX && !EY) o1.e[e] = qn;
-        o2.e[e] = ez ? az : qn;
+        if constexpr (EX && EY && EZ) {
+            // a corner cell has no plain axis
+            pn.e[e] = (sn + (pz - so)) + 0.0f;
+            o2.e[e] = az;
+        } else {
+            // the increment of the plain axes
+            const T qold = EX ? (EY ? a2.e[e] : a1.e[e]) : a0.e[e];
+            const T qn = fmaf(lap * ls, c2k2, qold);
+            pn.e[e] = (sn + (pz - so)) + qn;
+            if constexpr (!EX) o0.e[e] = qn;
+            if constexpr (EX && !EY) o1.e[e] = qn;
+            o2.e[e] = EZ ? az : qn;
+        }
     }
     const int sx = (int)A.sx, sy = (int)A.sy;
-    const unsigned c = (unsigned)x * A.sx + (unsigned)y * A.sy + zc;
+    const unsigned c = (unsigned)x * A.sx + (unsigned)H.y * A.sy + H.zc;
     if constexpr (EX) {
         st_masked<T, V>(A.vn[0] + c, nxl, m_xl);
         st_masked<T, V>(A.vn[0] + c + sx, nxr, m_xr);
@@ -244,31 +257,71 @@ __device__ __forceinline__ void tma_plane(const KArgs<float>& A, const TmaShape&
         st_masked<T, V>(A.vn[1] + c, nyl, m_yl);
         st_masked<T, V>(A.vn[1] + c + sy, nyr, m_yr);
     }
-    st_masked<T, V>(A.vn[2] + c, nzl, m_zl);
-    if (m_zr) {
+    if constexpr (EZ) {
+        st_masked<T, V>(A.vn[2] + c, nzl, m_zl);
+        if (m_zr) {
 #pragma unroll
-        for (int e = 0; e < V; ++e)
-            if ((m_zr >> e) & 1u) A.vn[2][c + e + 1] = nzr[e];
+            for (int e = 0; e < V; ++e)
+                if ((m_zr >> e) & 1u) A.vn[2][c + e + 1] = nzr[e];
+        }
     }
     st_masked<T, V>(A.pd[0] + c, o0, inbox);
-    if constexpr (KIND != 2) st_masked<T, V>(A.pd[1] + c, o1, m_a1);
-    st_masked<T, V>(A.pd[2] + c, o2, m_a2);
+    if constexpr (EX || EY) st_masked<T, V>(A.pd[1] + c, o1, inbox);
+    if constexpr (EZ || (EX && EY)) st_masked<T, V>(A.pd[2] + c, o2, inbox);
     st_masked<T, V>(A.pn + c, pn, inbox);
+}
+
+// The planes of one tile; false when a stage did not arrive within its bounded wait.
+template <bool EX, bool EY, bool EZ>
+__device__ __forceinline__ bool tma_tile(const KArgs<float>& A, const TmaShape& S, const TmaTile& T,
+                                         const CUtensorMap* maps, unsigned char* ring, int stage_bytes,
+                                         uint64_t* full, const TmaThread& H, int& waited, int& issued) {
+    const int tid = threadIdx.x;
+    const int nst = T.nx + 2;  // stages of the tile (planes x0-1 .. x0+nx)
+    const uint32_t rs = smem_u32(ring);
+    bool ok = true;
+    for (int j = 0; j < 2 && j < nst; ++j) {
+        if (ok) ok = mbar_wait(smem_u32(&full[j]), 0);
+        if (ok) waited = j + 1;
+    }
+    for (int i = 0; i < T.nx; ++i) {
+        const int jn = i + 2;  // stage of plane x+1
+        if (ok && jn < nst) {
+            ok = mbar_wait(smem_u32(&full[jn % TMA_STAGES]), (jn / TMA_STAGES) & 1);
+            if (ok) waited = jn + 1;
+        }
+        // (after a failed wait the plane is computed from whatever the stage
+        // holds, in bounds, and the solve reports the error)
+        if (H.inbox)
+            tma_plane<EX, EY, EZ>(A, S, ring + (i % TMA_STAGES) * stage_bytes,
+                                  ring + ((i + 1) % TMA_STAGES) * stage_bytes, ring + (jn % TMA_STAGES) * stage_bytes,
+                                  T.x0 + i, H);
+        // every thread is done with the stage of plane x-1 (and all waits held)
+        if (__syncthreads_or(!ok)) return false;
+        const int jf = i + TMA_STAGES;
+        if (jf < nst) {
+            if (tid == 0)
+                tma_issue_stage(maps, S, T, rs + (jf % TMA_STAGES) * stage_bytes, smem_u32(&full[jf % TMA_STAGES]),
+                                jf);
+            issued = jf + 1;
+        }
+    }
+    return true;
 }
 
 // (a template so that every translation unit may include it; instantiated for float only)
 template <typename TT>
-__global__ void __launch_bounds__(TMA_THREADS, 3)
-    k_pml_shell_tma(const KArgs<TT> A, const __grid_constant__ TmaMaps M, const TmaLaunch Lc,
-                    const TmaTile* __restrict__ tiles, int* __restrict__ dev_error) {
+__global__ void __launch_bounds__(TMA_THREADS, 4)
+    k_pml_shell_tma(const KArgs<TT> A, const TmaLaunch Lc, const TmaTile* __restrict__ tiles,
+                    const CUtensorMap* __restrict__ maps, int* __restrict__ dev_error) {
     static_assert(sizeof(TT) == 4, "the reduced PML state is an FP32 path");
     // the ring: TMA_STAGES stages of Lc.stage_bytes, then one mbarrier per stage
     extern __shared__ __align__(128) unsigned char tma_ring[];
     uint64_t* full = reinterpret_cast<uint64_t*>(tma_ring + TMA_STAGES * Lc.stage_bytes);
     if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) advance_consts(*A.P, A.cur);
     const TmaTile T = tiles[blockIdx.x];
-    const int sh = T.kind == 2 ? 1 : 0;
-    const TmaShape& S = Lc.shape[sh];
+    const TmaShape& S = Lc.shape[T.shape];
+    const CUtensorMap* m = maps + ((size_t)A.cur * Lc.nshape + T.shape) * TB_N;
     const int tid = threadIdx.x;
     const uint32_t ring = smem_u32(tma_ring);
     // tensor copies land on 128-byte boundaries (every buffer size is a multiple of 128)
@@ -276,7 +329,7 @@ __global__ void __launch_bounds__(TMA_THREADS, 3)
         if (tid == 0) atomicOr(dev_error, FDTD_DEV_ERR_TMA_TIMEOUT);
         return;
     }
-    const int nst = T.nx + 2;  // stages of the tile (planes x0-1 .. x0+nx)
+    const int nst = T.nx + 2;
     if (tid == 0) {
 #pragma unroll
         for (int s = 0; s < TMA_STAGES; ++s) mbar_init(smem_u32(&full[s]), 1);
@@ -286,80 +339,50 @@ __global__ void __launch_bounds__(TMA_THREADS, 3)
     __syncthreads();
     if (tid == 0)
         for (int j = 0; j < TMA_STAGES && j < nst; ++j)
-            tma_issue_stage(M, S, sh, T, ring + j * Lc.stage_bytes, smem_u32(&full[j]), j);
+            tma_issue_stage(m, S, T, ring + j * Lc.stage_bytes, smem_u32(&full[j]), j);
 
     // this thread's cells: row r of the window, z group lz .. lz+3
+    TmaThread H;
     const int gpr = S.tz / 4;
-    const int r = tid / gpr;
-    const int lz = (tid - r * gpr) * 4;
-    const int zc = T.z0 + lz;
-    const int y = T.y0 + (r < T.ny ? r : T.ny - 1);
-    const bool row_on = r < T.ny && r < S.ty;
-    unsigned inbox = 0;
+    H.r = tid / gpr;
+    H.lz = (tid - H.r * gpr) * 4;
+    H.zc = T.z0 + H.lz;
+    const bool row_on = H.r < T.ny;
+    H.y = T.y0 + (row_on ? H.r : T.ny - 1);
+    H.inbox = 0;
 #pragma unroll
-    for (int e = 0; e < 4; ++e) inbox |= (row_on && zc + e >= T.zlo && zc + e < T.zhi ? 1u : 0u) << e;
-    const uint8_t gy = __ldg(A.axflag[1] + y);
-    unsigned zm[6];
+    for (int e = 0; e < 4; ++e) H.inbox |= (row_on && H.zc + e >= T.zlo && H.zc + e < T.zhi ? 1u : 0u) << e;
+    H.gy = __ldg(A.axflag[1] + H.y);
     {
         uint8_t gz[4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) gz[e] = zc + e < A.N2 ? __ldg(A.axflag[2] + zc + e) : (uint8_t)0;
+        for (int e = 0; e < 4; ++e) gz[e] = H.zc + e < A.N2 ? __ldg(A.axflag[2] + H.zc + e) : (uint8_t)0;
 #pragma unroll
-        for (int k = 0; k < 6; ++k) zm[k] = flag_mask<4>(gz, k);
+        for (int k = 0; k < 6; ++k) H.zm[k] = flag_mask<4>(gz, k);
     }
-    AxisCoef<float> cz[5];
-    if (zm[0] & inbox) {
+    if ((T.cls & TC_Z) && H.inbox) {
 #pragma unroll
-        for (int e = 0; e <= 4; ++e) cz[e] = A.coef[2][zc + e];
+        for (int e = 0; e <= 4; ++e) H.cz[e] = A.coef[2][H.zc + e];
     }
-    AxisCoef<float> cyl{}, cyr{};
-    const bool ey = T.kind == 1 || (T.kind == 0 && (gy & AXF_PML));
-    if (ey) {
-        cyl = A.coef[1][y];
-        cyr = A.coef[1][y + 1];
+    if (T.cls & TC_Y) {
+        H.cyl = A.coef[1][H.y];
+        H.cyr = A.coef[1][H.y + 1];
     }
 
-    // stages 0..waited-1 have arrived; 0..issued-1 were issued
-    bool ok = true;
-    int waited = 0;
-    for (int j = 0; j < 2 && j < nst; ++j) {
-        if (ok) ok = mbar_wait(smem_u32(&full[j]), 0);
-        if (ok) waited = j + 1;
+    int waited = 0, issued = nst < TMA_STAGES ? nst : TMA_STAGES;
+    bool done;
+    unsigned char* R = tma_ring;
+    const int sb = Lc.stage_bytes;
+    switch (T.cls) {
+        case TC_X: done = tma_tile<true, false, false>(A, S, T, m, R, sb, full, H, waited, issued); break;
+        case TC_Y: done = tma_tile<false, true, false>(A, S, T, m, R, sb, full, H, waited, issued); break;
+        case TC_Z: done = tma_tile<false, false, true>(A, S, T, m, R, sb, full, H, waited, issued); break;
+        case TC_X | TC_Y: done = tma_tile<true, true, false>(A, S, T, m, R, sb, full, H, waited, issued); break;
+        case TC_X | TC_Z: done = tma_tile<true, false, true>(A, S, T, m, R, sb, full, H, waited, issued); break;
+        case TC_Y | TC_Z: done = tma_tile<false, true, true>(A, S, T, m, R, sb, full, H, waited, issued); break;
+        default: done = tma_tile<true, true, true>(A, S, T, m, R, sb, full, H, waited, issued); break;
     }
-    int issued = nst < TMA_STAGES ? nst : TMA_STAGES;
-    bool fail = false;
-    for (int i = 0; i < T.nx; ++i) {
-        const int jn = i + 2;  // stage of plane x+1
-        if (ok && jn < nst) {
-            ok = mbar_wait(smem_u32(&full[jn % TMA_STAGES]), (jn / TMA_STAGES) & 1);
-            if (ok) waited = jn + 1;
-        }
-        const int x = T.x0 + i;
-        const unsigned char* sM = tma_ring + (i % TMA_STAGES) * Lc.stage_bytes;
-        const unsigned char* s0 = tma_ring + ((i + 1) % TMA_STAGES) * Lc.stage_bytes;
-        const unsigned char* sP = tma_ring + (jn % TMA_STAGES) * Lc.stage_bytes;
-        // (after a failed wait the plane is computed from whatever the stage
-        // holds, in bounds, and the solve reports the error)
-        if (inbox) {
-            if (T.kind == 2) tma_plane<2, false>(A, S, sM, s0, sP, x, y, r, zc, lz, inbox, gy, zm, cz, cyl, cyr);
-            else if (T.kind == 1) tma_plane<1, true>(A, S, sM, s0, sP, x, y, r, zc, lz, inbox, gy, zm, cz, cyl, cyr);
-            else if (ey) tma_plane<0, true>(A, S, sM, s0, sP, x, y, r, zc, lz, inbox, gy, zm, cz, cyl, cyr);
-            else tma_plane<0, false>(A, S, sM, s0, sP, x, y, r, zc, lz, inbox, gy, zm, cz, cyl, cyr);
-        }
-        // every thread is done with the stage of plane x-1 (and all waits held)
-        if (__syncthreads_or(!ok)) {
-            fail = true;
-            break;
-        }
-        const int jf = i + TMA_STAGES;
-        if (jf < nst) {
-            if (tid == 0)
-                tma_issue_stage(M, S, sh, T, ring + (jf % TMA_STAGES) * Lc.stage_bytes,
-                                smem_u32(&full[jf % TMA_STAGES]), jf);
-            issued = jf + 1;
-        }
-    }
-    if (fail && tid == 0) {
+    if (!done && tid == 0) {
         atomicOr(dev_error, FDTD_DEV_ERR_TMA_TIMEOUT);
         // wait (bounded) for the copies this CTA still has in flight
         for (int j = waited; j < issued; ++j) (void)mbar_wait(smem_u32(&full[j % TMA_STAGES]), (j / TMA_STAGES) & 1);

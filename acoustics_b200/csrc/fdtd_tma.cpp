@@ -79,12 +79,6 @@ int shape_bytes(const TmaShape& S) {
     return end;
 }
 
-bool any_pml(const std::vector<uint8_t>& cell, int a, int b) {
-    for (int i = std::max(a, 0); i < std::min(b, (int)cell.size()); ++i)
-        if (cell[i]) return true;
-    return false;
-}
-
 }  // namespace
 
 bool tma_encoder_available() { return encode_tiled() != nullptr; }
@@ -92,15 +86,16 @@ bool tma_encoder_available() { return encode_tiled() != nullptr; }
 void free_shell_tma(fdtd_solver* s) {
     if (!s->tma) return;
     if (s->tma->d_tiles) cudaFree(s->tma->d_tiles);
+    if (s->tma->d_maps) cudaFree(s->tma->d_maps);
     delete s->tma;
     s->tma = nullptr;
     s->region.tma = nullptr;
 }
 
-// Tiles and maps of this solve's shell (the five-box shell of the reduced
-// state: x slabs over the whole (y, z) face, y slabs over the inner x range,
-// z slabs over the inner x and y ranges).  FDTD_ERR_UNSUPPORTED when the
-// layout does not fit the kernel (the caller then keeps the cp.async kernel).
+// Tiles and maps of this solve's shell, cut by absorbing axes: for every
+// non-empty set of axes, the cells whose x, y and z each lie in that axis' PML
+// ranges exactly for the axes of the set.  FDTD_ERR_UNSUPPORTED when the layout
+// does not fit the kernel (the caller then keeps the cp.async kernel).
 fdtd_status build_shell_tma(fdtd_solver* s) {
     free_shell_tma(s);
     if (!tma_encoder_available()) return (set_error(s, "cuTensorMapEncodeTiled unavailable"), FDTD_ERR_UNSUPPORTED);
@@ -110,96 +105,134 @@ fdtd_status build_shell_tma(fdtd_solver* s) {
     for (int d = 0; d < 3; ++d)
         if (!(lo[d] > 0 && hi[d] < N[d] && lo[d] < hi[d]))
             return (set_error(s, "shell layout outside the TMA kernel's"), FDTD_ERR_UNSUPPORTED);
-    constexpr int TZ0 = 64, TY0 = 8;
-    // z-slab windows: [0, lo2) and [hi2 rounded down to 4, N2)
-    const int zh0 = hi[2] / 4 * 4;
-    const int zw = std::max((lo[2] + 3) / 4 * 4, (N[2] - zh0 + 3) / 4 * 4);
-    int TZ1 = 4;
-    while (TZ1 < zw) TZ1 *= 2;
-    if (TZ1 > 64) return (set_error(s, "z slabs wider than the TMA kernel's windows"), FDTD_ERR_UNSUPPORTED);
-    const int TY1 = 512 / TZ1;
+    struct Range {
+        int a, b;
+    };
+    // the ranges of one axis inside / outside its PML
+    auto ranges = [&](int d, bool pml) {
+        std::vector<Range> r;
+        if (pml) {
+            r.push_back({0, lo[d]});
+            r.push_back({hi[d], N[d]});
+        } else {
+            r.push_back({lo[d], hi[d]});
+        }
+        return r;
+    };
+    // window shape of a class: z windows start on multiples of 4
+    auto shape_of = [&](bool ey, bool ez, int& tz, int& ty) -> bool {
+        if (ez) {
+            const int need = std::max((lo[2] + 3) / 4 * 4, (N[2] - hi[2] / 4 * 4 + 3) / 4 * 4);
+            tz = 4;
+            while (tz < need) tz *= 2;
+            if (tz > 64) return false;
+        } else {
+            const int z0 = lo[2] / 4 * 4, span = hi[2] - z0;
+            tz = 64;
+            int waste = (span + 63) / 64 * 64 - span;
+            for (int c : {32, 16}) {
+                const int w = (span + c - 1) / c * c - span;
+                if (w < waste) {
+                    waste = w;
+                    tz = c;
+                }
+            }
+        }
+        const int ty_max = 512 / tz;
+        const int ey_ext = ey ? std::max(lo[1], N[1] - hi[1]) : hi[1] - lo[1];
+        ty = std::min(ty_max, ey_ext);
+        return ty > 0;
+    };
+    std::unique_ptr<TmaStep> T(new TmaStep());
+    std::memset(T.get(), 0, sizeof(TmaStep));
+    TmaLaunch& L = T->launch;
+    int cls_shape[8];
+    unsigned used[TMA_MAX_SHAPES] = {0};
+    for (int cls = 1; cls < 8; ++cls) {
+        const bool ex = cls & TC_X, ey = cls & TC_Y, ez = cls & TC_Z;
+        int tz = 0, ty = 0;
+        if (!shape_of(ey, ez, tz, ty))
+            return (set_error(s, "PML slabs wider than the TMA kernel's windows"), FDTD_ERR_UNSUPPORTED);
+        int sh = -1;
+        for (int k = 0; k < L.nshape; ++k)
+            if (L.shape[k].tz == tz && L.shape[k].ty == ty) sh = k;
+        if (sh < 0) {
+            sh = L.nshape++;
+            L.shape[sh].tz = tz;
+            L.shape[sh].ty = ty;
+        }
+        cls_shape[cls] = sh;
+        used[sh] |= (1u << TB_P) | (1u << TB_A0);
+        if (ex) used[sh] |= 1u << TB_VX;
+        if (ey) used[sh] |= 1u << TB_VY;
+        if (ez) used[sh] |= 1u << TB_VZ;
+        if (ex || ey) used[sh] |= 1u << TB_A1;
+        if (ez || (ex && ey)) used[sh] |= 1u << TB_A2;
+    }
+    L.stage_bytes = 0;
+    for (int k = 0; k < L.nshape; ++k) {
+        L.shape[k] = make_shape(L.shape[k].tz, L.shape[k].ty, used[k]);
+        L.stage_bytes = std::max(L.stage_bytes, shape_bytes(L.shape[k]));
+    }
 
-    // x planes per tile: 16, or fewer until the tiles fill three CTAs per SM
+    // x planes per tile: 16, or fewer until the tiles fill four CTAs per SM
     std::vector<TmaTile> tiles;
     for (int XS = 16; XS >= 4; XS /= 2) {
         tiles.clear();
-        auto add = [&](int kind, int x0, int x1, int y0, int ny, int z0, int zlo, int zhi, int flags) {
-            for (int xa = x0; xa < x1; xa += XS) {
-                TmaTile t{};
-                t.kind = kind;
-                t.x0 = xa;
-                t.nx = std::min(XS, x1 - xa);
-                t.y0 = y0;
-                t.ny = ny;
-                t.z0 = z0;
-                t.zlo = zlo;
-                t.zhi = zhi;
-                t.flags = flags;
-                tiles.push_back(t);
-            }
-        };
-        const auto& py = s->tab[1].pml_cell;
-        const auto& pz = s->tab[2].pml_cell;
-        // x slabs: every row absorbs along x; rows of the y PML also along y, z-PML cells along z
-        for (int side = 0; side < 2; ++side) {
-            const int xa = side ? hi[0] : 0, xb = side ? N[0] : lo[0];
-            for (int y0 = 0; y0 < N[1]; y0 += TY0)
-                for (int z0 = 0; z0 < N[2]; z0 += TZ0) {
-                    const int ny = std::min(TY0, N[1] - y0);
-                    const bool vy = any_pml(py, y0, y0 + ny), vz = any_pml(pz, z0, z0 + TZ0);
-                    add(0, xa, xb, y0, ny, z0, 0, N[2], (vy ? TT_VY : 0) | (vz ? TT_VZ : 0) | (vy || vz ? TT_A2 : 0));
-                }
+        for (int cls = 1; cls < 8; ++cls) {
+            const bool ex = cls & TC_X, ey = cls & TC_Y, ez = cls & TC_Z;
+            const TmaShape& S = L.shape[cls_shape[cls]];
+            for (const Range& rx : ranges(0, ex))
+                for (const Range& ry : ranges(1, ey))
+                    for (const Range& rz : ranges(2, ez)) {
+                        if (rx.b <= rx.a || ry.b <= ry.a || rz.b <= rz.a) continue;
+                        for (int z0 = rz.a / 4 * 4; z0 < rz.b; z0 += S.tz)
+                            for (int y0 = ry.a; y0 < ry.b; y0 += S.ty)
+                                for (int x0 = rx.a; x0 < rx.b; x0 += XS) {
+                                    TmaTile t{};
+                                    t.cls = cls;
+                                    t.shape = cls_shape[cls];
+                                    t.x0 = x0;
+                                    t.nx = std::min(XS, rx.b - x0);
+                                    t.y0 = y0;
+                                    t.ny = std::min(S.ty, ry.b - y0);
+                                    t.z0 = z0;
+                                    t.zlo = rz.a;
+                                    t.zhi = rz.b;
+                                    tiles.push_back(t);
+                                }
+                    }
         }
-        // y slabs
-        for (int side = 0; side < 2; ++side) {
-            const int ya = side ? hi[1] : 0, yb = side ? N[1] : lo[1];
-            for (int y0 = ya; y0 < yb; y0 += TY0)
-                for (int z0 = 0; z0 < N[2]; z0 += TZ0) {
-                    const bool vz = any_pml(pz, z0, z0 + TZ0);
-                    add(1, lo[0], hi[0], y0, std::min(TY0, yb - y0), z0, 0, N[2], TT_VY | (vz ? TT_VZ | TT_A2 : 0));
-                }
-        }
-        // z slabs
-        for (int side = 0; side < 2; ++side) {
-            const int z0 = side ? zh0 : 0, zlo = side ? hi[2] : 0, zhi = side ? N[2] : lo[2];
-            for (int y0 = lo[1]; y0 < hi[1]; y0 += TY1)
-                add(2, lo[0], hi[0], y0, std::min(TY1, hi[1] - y0), z0, zlo, zhi, TT_VZ | TT_A2);
-        }
-        if ((int)tiles.size() >= 3 * 148) break;
+        if ((int)tiles.size() >= 4 * 148) break;
     }
-    std::unique_ptr<TmaStep> T(new TmaStep());
-    std::memset(T.get(), 0, sizeof(TmaStep));
-    const unsigned all = (1u << TB_N) - 1u;
-    const unsigned zs = (1u << TB_P) | (1u << TB_VZ) | (1u << TB_A0) | (1u << TB_A2);
-    T->launch.shape[0] = make_shape(TZ0, TY0, all);
-    T->launch.shape[1] = make_shape(TZ1, TY1, zs);
-    T->launch.stage_bytes = std::max(shape_bytes(T->launch.shape[0]), shape_bytes(T->launch.shape[1]));
-    T->launch.ntiles = (int)tiles.size();
+    L.ntiles = (int)tiles.size();
+
+    // maps [parity][shape][buffer], in device memory
+    std::vector<CUtensorMap> maps((size_t)2 * L.nshape * TB_N);
+    std::memset(maps.data(), 0, maps.size() * sizeof(CUtensorMap));
     const SolveParams& P = s->hP;
     for (int c = 0; c < 2; ++c)
-        for (int sh = 0; sh < 2; ++sh) {
-            const TmaShape& S = T->launch.shape[sh];
-            CUtensorMap* m = T->maps[c].m[sh];
-            bool ok = encode(&m[TB_P], P.p[c], s, S.tz + 8, S.ty + 2) &&
-                      encode(&m[TB_VZ], P.v[c][2], s, S.tz + 4, S.ty) && encode(&m[TB_A0], P.pd[0], s, S.tz, S.ty) &&
-                      encode(&m[TB_A2], P.pd[2], s, S.tz, S.ty);
-            if (ok && sh == 0)
-                ok = encode(&m[TB_VX], P.v[c][0], s, S.tz, S.ty) && encode(&m[TB_VY], P.v[c][1], s, S.tz, S.ty + 1) &&
-                     encode(&m[TB_A1], P.pd[1], s, S.tz, S.ty);
+        for (int sh = 0; sh < L.nshape; ++sh) {
+            const TmaShape& S = L.shape[sh];
+            CUtensorMap* m = &maps[((size_t)c * L.nshape + sh) * TB_N];
+            bool ok = encode(&m[TB_P], P.p[c], s, S.tz + 8, S.ty + 2) && encode(&m[TB_A0], P.pd[0], s, S.tz, S.ty);
+            if (ok && S.bytes[TB_VX]) ok = encode(&m[TB_VX], P.v[c][0], s, S.tz, S.ty);
+            if (ok && S.bytes[TB_VY]) ok = encode(&m[TB_VY], P.v[c][1], s, S.tz, S.ty + 1);
+            if (ok && S.bytes[TB_VZ]) ok = encode(&m[TB_VZ], P.v[c][2], s, S.tz + 4, S.ty);
+            if (ok && S.bytes[TB_A1]) ok = encode(&m[TB_A1], P.pd[1], s, S.tz, S.ty);
+            if (ok && S.bytes[TB_A2]) ok = encode(&m[TB_A2], P.pd[2], s, S.tz, S.ty);
             if (!ok) return (set_error(s, "cuTensorMapEncodeTiled rejected a shell map"), FDTD_ERR_UNSUPPORTED);
         }
-    const size_t tb = tiles.size() * sizeof(TmaTile);
+    const size_t tb = tiles.size() * sizeof(TmaTile), mb = maps.size() * sizeof(CUtensorMap);
     cudaError_t e = cudaMalloc((void**)&T->d_tiles, tb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&T->d_maps, mb);
+    if (e == cudaSuccess) e = counted_copy(s, T->d_tiles, tiles.data(), tb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = counted_copy(s, T->d_maps, maps.data(), mb, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
-        T->d_tiles = nullptr;
-        cuda_fail(s, e, "cudaMalloc (shell tiles)");
+        if (T->d_tiles) cudaFree(T->d_tiles);
+        if (T->d_maps) cudaFree(T->d_maps);
+        cuda_fail(s, e, "shell tiles and tensor maps");
         return e == cudaErrorMemoryAllocation ? FDTD_ERR_OOM : FDTD_ERR_CUDA;
-    }
-    e = counted_copy(s, T->d_tiles, tiles.data(), tb, cudaMemcpyHostToDevice);
-    if (e != cudaSuccess) {
-        cudaFree(T->d_tiles);
-        cuda_fail(s, e, "copy of the shell tiles");
-        return FDTD_ERR_CUDA;
     }
     s->tma = T.release();
     s->region.tma = s->tma;

@@ -10,48 +10,51 @@ namespace fdtd {
 
 constexpr int TMA_THREADS = 128;
 constexpr int TMA_STAGES = 4;
+constexpr int TMA_MAX_SHAPES = 8;
 // bit the shell kernel sets in the solve's dev_error flags when a stage never arrives
 constexpr int FDTD_DEV_ERR_TMA_TIMEOUT = 2;
 
-enum : int { TT_VY = 1, TT_VZ = 2, TT_A2 = 4 };
+// Axis set of a tile: the axes along which every cell of the tile absorbs.
+enum : int { TC_X = 1, TC_Y = 2, TC_Z = 4 };
+// Buffers of a ring stage.
 enum : int { TB_P = 0, TB_VX = 1, TB_VY = 2, TB_VZ = 3, TB_A0 = 4, TB_A1 = 5, TB_A2 = 6, TB_N = 7 };
 
-// One tile of the shell.
+// One tile of the shell: cells x in [x0, x0+nx), y in [y0, y0+ny),
+// z in [zlo, zhi) of the window [z0, z0 + tz) of its shape, all with the same
+// absorbing axes.
 struct alignas(16) TmaTile {
-    int kind;       // 0 x slab, 1 y slab, 2 z slab
-    int x0, nx;     // planes [x0, x0 + nx)
-    int y0, ny;     // rows [y0, y0 + ny), ny <= TY of the shape
-    int z0;         // first z of the window (multiple of 4)
-    int zlo, zhi;   // cells of the box in the window: z in [zlo, zhi)
-    int flags;      // TT_*: y faces / z faces / third split array are read
+    int cls;        // TC_* bits (never 0)
+    int shape;      // index into TmaLaunch::shape
+    int x0, nx;
+    int y0, ny;
+    int z0;         // multiple of 4
+    int zlo, zhi;
     int pad[3];
 };
 
-// Window shape and stage layout (byte offsets of the buffers in a stage).
+// Window shape (tz x ty cells; tz / 4 * ty <= TMA_THREADS) and the byte
+// offsets / sizes of the buffers of a stage (size 0: not used by the shape's tiles).
 struct TmaShape {
     int tz, ty;
     int off[TB_N];
     int bytes[TB_N];
 };
 
-// Tensor maps of the arrays, per window shape; P and the faces depend on the
-// buffer parity of the step, so the host passes the maps of this step.
-struct TmaMaps {
-    CUtensorMap m[2][TB_N];  // [shape][TB_*]; A0..A2 are the three split arrays
-};
-
 struct TmaLaunch {
-    TmaShape shape[2];
+    TmaShape shape[TMA_MAX_SHAPES];
+    int nshape;
     int stage_bytes;  // bytes of one ring stage (multiple of 128)
     int ntiles;
+    int pad;
 };
 
-// Everything a step needs to launch the kernel (host memory of the solver):
-// the maps of both buffer parities and the device tile table.
+// Everything a step needs to launch the kernel: the launch description (host
+// memory), the device tile table and the device tensor maps
+// [parity of p^n][shape][TB_*] (64-byte aligned, written before any launch).
 struct TmaStep {
-    TmaMaps maps[2];  // [parity of p^n]
     TmaLaunch launch;
     TmaTile* d_tiles;
+    CUtensorMap* d_maps;
 };
 
 // dynamic shared memory of the kernel: the ring and one mbarrier per stage
