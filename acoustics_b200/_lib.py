@@ -22,7 +22,8 @@ EXPORTS = [
     "fdtd_solver_step_device", "fdtd_solver_fetch_listeners", "fdtd_solver_info_get",
     "fdtd_solver_get_classification", "fdtd_solver_get_field", "fdtd_solver_synchronize",
     "fdtd_solver_stream", "fdtd_solver_last_error", "fdtd_solver_last_launch_count", "fdtd_solver_pml_state", "fdtd_solver_shell_staging",
-    "fdtd_solver_overlapped_steps", "fdtd_solver_transfer_bytes", "fdtd_read_obj", "fdtd_mesh_signed_distance",
+    "fdtd_solver_overlapped_steps", "fdtd_solver_transfer_bytes", "fdtd_read_obj",
+    "fdtd_read_kinematics", "fdtd_keyframe_pose", "fdtd_mesh_signed_distance",
     "fdtd_solver_prepare_graphs", "fdtd_solver_set_field", "fdtd_matrix_write", "fdtd_matrix_read",
     "fdtd_solver_save_snapshot", "fdtd_solver_load_snapshot", "fdtd_solver_save_config",
     "fdtd_solver_save_field_timestep", "fdtd_solver_boundary_info",
@@ -81,6 +82,8 @@ def load(build_if_missing: bool = False):
         "fdtd_solver_overlapped_steps": ([vp], i64),
         "fdtd_solver_transfer_bytes": ([vp, C.POINTER(i64), C.POINTER(i64)], i32),
         "fdtd_read_obj": ([C.c_char_p, dbl, C.POINTER(i32), C.POINTER(i32), vp, vp], i32),
+        "fdtd_read_kinematics": ([C.c_char_p, C.POINTER(i32), vp, i64], i32),
+        "fdtd_keyframe_pose": ([vp, dbl, vp, vp], i32),
         "fdtd_mesh_signed_distance": ([vp, i64, vp, vp], i32),
         "fdtd_solver_pml_state": ([vp], i32),
         "fdtd_solver_shell_staging": ([vp], i32),

@@ -77,6 +77,17 @@ static bool inside_pml_1d(double x, double mn, double mx, double w) {
 }
 
 void host_object_pose(HostObject& o, double t) {
+    if (o.d.motion == FDTD_MOTION_KEYFRAMED && o.kf) {
+        // FDTD_Objects::AnimateObjects -> SetRigidBodyTransform: rotation R * R0, centre to the frame's
+        double R[9];
+        keyframe_pose(o.kf, o.kf_n, o.kf_step, t, o.c, R);
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                o.d.rotation[i * 3 + j] =
+                    R[i * 3 + 0] * o.R0[0 * 3 + j] + R[i * 3 + 1] * o.R0[1 * 3 + j] + R[i * 3 + 2] * o.R0[2 * 3 + j];
+        if (o.d.shape == FDTD_SHAPE_MESH && o.mv) mesh_extent(o.mv, (size_t)o.mv_n, o.d.rotation, o.mlo, o.mhi);
+        return;
+    }
     for (int a = 0; a < 3; ++a) {
         if (o.d.motion == FDTD_MOTION_BALLISTIC)
             o.c[a] = o.d.center[a] + o.d.velocity[a] * t + 0.5 * o.d.gravity[a] * t * t;
@@ -118,10 +129,20 @@ void host_update_bbox(HostObject& o) {
 HostObject make_host_object(const fdtd_scene_desc* sc, int i) {
     HostObject h;
     h.d = sc->objects[i];
+    for (int k = 0; k < 9; ++k) h.R0[k] = h.d.rotation[k];
     if (h.d.shape == FDTD_SHAPE_MESH) {
         const fdtd_mesh_desc& m = sc->meshes[h.d.mesh];
         mesh_extent(m.vertices, (size_t)m.n_vertices, h.d.rotation, h.mlo, h.mhi);
+        h.mv = m.vertices;
+        h.mv_n = m.n_vertices;
     }
+    if (h.d.motion == FDTD_MOTION_KEYFRAMED)
+        for (int k = 0; k < sc->n_tracks; ++k)
+            if (sc->tracks[k].object == i) {
+                h.kf = sc->tracks[k].frames;
+                h.kf_n = sc->tracks[k].n_frames;
+                h.kf_step = sc->tracks[k].step;
+            }
     return h;
 }
 
@@ -455,6 +476,12 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
         return (set_error(nullptr, "scene array missing"), FDTD_ERR_INVALID_ARG);
     if (sc->n_meshes < 0 || (sc->n_meshes > 0 && !sc->meshes))
         return (set_error(nullptr, "scene mesh array missing"), FDTD_ERR_INVALID_ARG);
+    if (sc->n_tracks < 0 || (sc->n_tracks > 0 && !sc->tracks))
+        return (set_error(nullptr, "scene keyframe-track array missing"), FDTD_ERR_INVALID_ARG);
+    for (int k = 0; k < sc->n_tracks; ++k)
+        if (sc->tracks[k].object < 0 || sc->tracks[k].object >= sc->n_objects ||
+            sc->objects[sc->tracks[k].object].motion != FDTD_MOTION_KEYFRAMED)
+            return (set_error(nullptr, "keyframe track of an object that is not keyframed"), FDTD_ERR_INVALID_ARG);
     for (int i = 0; i < sc->n_objects; ++i) {
         const auto& o = sc->objects[i];
         if (o.shape < 0 || o.shape > FDTD_SHAPE_MESH) return (set_error(nullptr, "unknown object shape"), FDTD_ERR_INVALID_ARG);
@@ -470,8 +497,25 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
         }
         if (o.accel_kind == FDTD_ACCEL_GAUSSIAN_PULSATION && o.shape != FDTD_SHAPE_SPHERE)
             return (set_error(nullptr, "pulsating acceleration is defined for spheres only"), FDTD_ERR_UNSUPPORTED);
-        if (o.motion == FDTD_MOTION_BALLISTIC && o.shape == FDTD_SHAPE_ELLIPSOID)
+        if (o.motion != FDTD_MOTION_STATIC && o.shape == FDTD_SHAPE_ELLIPSOID)
             return (set_error(nullptr, "moving ellipsoids are not supported (no closest-point query)"), FDTD_ERR_UNSUPPORTED);
+        if (o.motion < FDTD_MOTION_STATIC || o.motion > FDTD_MOTION_KEYFRAMED)
+            return (set_error(nullptr, "unknown object motion"), FDTD_ERR_INVALID_ARG);
+        if (o.motion == FDTD_MOTION_KEYFRAMED) {
+            int found = 0;
+            for (int k = 0; k < sc->n_tracks; ++k)
+                if (sc->tracks && sc->tracks[k].object == i) {
+                    const fdtd_keyframe_track& t = sc->tracks[k];
+                    if (t.n_frames < 1 || !t.frames || !(t.step > 0))
+                        return (set_error(nullptr, "keyframe track needs frames and a positive step"), FDTD_ERR_INVALID_ARG);
+                    for (long long q = 0; q < 7LL * t.n_frames; ++q)
+                        if (!std::isfinite(t.frames[q]))
+                            return (set_error(nullptr, "keyframe track has a non-finite value"), FDTD_ERR_INVALID_ARG);
+                    ++found;
+                }
+            if (found != 1)
+                return (set_error(nullptr, "a keyframed object needs exactly one keyframe track"), FDTD_ERR_INVALID_ARG);
+        }
         if (o.accel_kind != FDTD_ACCEL_NONE && !(o.accel_tau > 0))
             return (set_error(nullptr, "accel_tau must be positive"), FDTD_ERR_INVALID_ARG);
         for (int d = 0; d < 3; ++d)
@@ -719,6 +763,19 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
         if (!build_mesh(sc->meshes[m], s->meshes[m], err)) {
             set_error(nullptr, err);
             return FDTD_ERR_GEOMETRY;
+        }
+    }
+    // keyframe tracks and mesh vertices the objects read after creation: solver-owned copies
+    s->kf_store.resize(s->objs.size());
+    for (size_t i = 0; i < s->objs.size(); ++i) {
+        HostObject& o = s->objs[i];
+        if (o.kf) {
+            s->kf_store[i].assign(o.kf, o.kf + 7 * (size_t)o.kf_n);
+            o.kf = s->kf_store[i].data();
+        }
+        if (o.d.shape == FDTD_SHAPE_MESH) {
+            o.mv = s->meshes[o.d.mesh].vertices.data();
+            o.mv_n = (int)(s->meshes[o.d.mesh].vertices.size() / 3);
         }
     }
     for (int i = 0; i < sc->n_constraints; ++i) s->planes.push_back(sc->constraints[i]);

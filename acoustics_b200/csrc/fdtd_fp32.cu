@@ -32,9 +32,9 @@ namespace fdtd {
 // The reduced-state shell kernels stage their loads in more than the default
 // 48 KB of dynamic shared memory: raise their limit on the current device.
 cudaError_t prepare_fp32_kernels() {
-    // the TMA-staged shell: a 4-stage ring of up to 24 KB stages
+    // the TMA-staged shell: a ring of up to 24 KB stages
     cudaError_t e = cudaFuncSetAttribute(k_pml_shell_tma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         TMA_STAGES * 24 * 1024 + 8 * TMA_STAGES);
+                                         TMA_STAGES * 24 * 1024 + 16 * TMA_STAGES);
     if (e != cudaSuccess) return e;
     if (red_smem_bytes() > 0) {
         e = cudaFuncSetAttribute(k_pml_shell_red<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, red_smem_bytes());
@@ -43,6 +43,13 @@ cudaError_t prepare_fp32_kernels() {
                                      red_smem_bytes());
     }
     return e;
+}
+
+int tma_blocks_per_sm(int smem_bytes) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_pml_shell_tma<float>, TMA_BLOCK, smem_bytes) != cudaSuccess)
+        return 1;
+    return n;
 }
 
 cudaError_t launch_batch_fp32(const BatchLaunch& L, const StepStreams& S, int* launches) {

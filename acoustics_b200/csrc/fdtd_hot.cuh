@@ -517,8 +517,8 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     if (nblk > 0) {
         if constexpr (sizeof(T) == 4) {
             if (R.red && R.tma)
-                k_pml_shell_tma<float><<<R.tma->launch.ntiles, TMA_THREADS, tma_smem_bytes(R.tma->launch), S.s>>>(
-                    A, R.tma->launch, R.tma->d_tiles, R.tma->d_maps, hP.dev_error);
+                k_pml_shell_tma<float><<<R.tma->grid, TMA_BLOCK, tma_smem_bytes(R.tma->launch), S.s>>>(
+                    A, R.tma->launch, R.tma->d_tiles, R.tma->d_cta_first, R.tma->d_maps, hP.dev_error);
             else if (R.red) k_pml_shell_red<float><<<nblk, dim3(32, 8), red_smem_bytes(), S.s>>>(A, R.shell);
             else k_pml_shell<T><<<nblk, dim3(32, 8), 0, S.s>>>(A, R.shell);
         } else {

@@ -19,6 +19,14 @@ struct HostObject {
     double umin[3] = {0, 0, 0}, umax[3] = {0, 0, 0};  // _bboxWorldUnion2Steps
     double mlo[3] = {0, 0, 0}, mhi[3] = {0, 0, 0};    // mesh: extent of rotation * v about the centre
     MeshView mview{};                                 // mesh: device hierarchy and triangles
+    // FDTD_MOTION_KEYFRAMED: the track (solver-owned frames) and the rest rotation it turns
+    const double* kf = nullptr;
+    int kf_n = 0;
+    double kf_step = 0;
+    double R0[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    // meshes: object-frame vertices (solver-owned) for the extent of a turned mesh
+    const double* mv = nullptr;
+    int mv_n = 0;
 };
 
 // A validated mesh with its pseudo-normals and hierarchy (fdtd_mesh.cpp).
@@ -39,6 +47,9 @@ struct AxisTables {
 };
 
 void host_object_pose(HostObject& o, double t);
+// keyframed pose at time t: centre and the rotation that turns the rest pose (fdtd_kinematics.cpp)
+void keyframe_pose(const double* frames, int n, double step, double t, double com[3], double R[9]);
+bool read_kinematics(const char* path, std::vector<double>& frames, std::string& err);
 void host_update_bbox(HostObject& o);
 void host_reset_union(HostObject& o);
 
@@ -74,6 +85,7 @@ struct fdtd_solver {
     fdtd::AxisTables tab[3];
     std::vector<fdtd::HostObject> objs;
     std::vector<fdtd::MeshHost> meshes;     // the scene's meshes (those objects use)
+    std::vector<std::vector<double>> kf_store;  // keyframe tracks of the objects (empty: none)
     std::vector<void*> mesh_alloc;          // their device copies
     std::vector<fdtd_plane_desc> planes;
     std::vector<fdtd_gaussian_source_desc> sources;

@@ -46,6 +46,8 @@ struct SceneCopy {
     std::vector<fdtd_mesh_desc> meshes;
     std::vector<std::vector<double>> mverts;
     std::vector<std::vector<int32_t>> mtris;
+    std::vector<fdtd_keyframe_track> tracks;
+    std::vector<std::vector<double>> tframes;
     void take(const fdtd_scene_desc& s) {
         d = s;
         objs.assign(s.objects, s.objects + std::max(0, s.n_objects));
@@ -69,6 +71,16 @@ struct SceneCopy {
         d.listeners = lis.empty() ? nullptr : lis.data();
         d.meshes = meshes.empty() ? nullptr : meshes.data();
         d.n_meshes = nm;
+        const int nt = s.tracks ? std::max(0, s.n_tracks) : 0;
+        tracks.assign(s.tracks, s.tracks + nt);
+        tframes.resize(nt);
+        for (int k = 0; k < nt; ++k) {
+            const fdtd_keyframe_track& T = s.tracks[k];
+            if (T.frames && T.n_frames > 0) tframes[k].assign(T.frames, T.frames + 7 * (size_t)T.n_frames);
+            tracks[k].frames = tframes[k].empty() ? nullptr : tframes[k].data();
+        }
+        d.tracks = tracks.empty() ? nullptr : tracks.data();
+        d.n_tracks = nt;
     }
 };
 

@@ -15,10 +15,14 @@
 // is as wide as the z slab, y-slab tiles as high as the y slab), so the copies
 // carry few cells outside the shell.
 //
-// Staging.  Per x plane one thread issues 3-D bulk tensor copies
-// (cp.async.bulk.tensor, tensor maps in device memory describing this GPU's
-// arrays, no multicast) of every array the tile reads into one stage of a
-// 4-stage shared-memory ring, completed on that stage's mbarrier:
+// Staging.  The kernel is persistent: a CTA walks a list of tiles (balanced on
+// the host by their bytes).  A producer warp issues, per x plane, 3-D bulk
+// tensor copies (cp.async.bulk.tensor, tensor maps in device memory describing
+// this GPU's arrays, no multicast) of every array the tile reads into one stage
+// of a TMA_STAGES-deep shared-memory ring, completed on the stage's "full"
+// mbarrier; the stage sequence runs on across tiles, so the ring never drains
+// between them.  Four consumer warps compute; each releases a stage on its
+// "empty" mbarrier when done with it, and the producer refills it then.
 //   P   p^n with a one-cell halo in y and a four-cell halo in z (z stays a
 //       multiple of 4: the copy's innermost coordinate is 16-byte aligned;
 //       halo cells outside the grid read as zeros and are never used)
@@ -271,57 +275,55 @@ __device__ __forceinline__ void tma_plane(const KArgs<float>& A, const TmaShape&
     st_masked<T, V>(A.pn + c, pn, inbox);
 }
 
-// The planes of one tile; false when a stage did not arrive within its bounded wait.
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
+}
+
+// Consumer side of one tile: its planes, reading the stages g0 .. g0+nx+1 of
+// the CTA's global stage sequence; every consumer warp releases each stage once
+// it no longer needs it.  False when a stage did not arrive within its bounded wait.
 template <bool EX, bool EY, bool EZ>
 __device__ __forceinline__ bool tma_tile(const KArgs<float>& A, const TmaShape& S, const TmaTile& T,
-                                         const CUtensorMap* maps, unsigned char* ring, int stage_bytes,
-                                         uint64_t* full, const TmaThread& H, int& waited, int& issued) {
-    const int tid = threadIdx.x;
-    const int nst = T.nx + 2;  // stages of the tile (planes x0-1 .. x0+nx)
-    const uint32_t rs = smem_u32(ring);
-    bool ok = true;
-    for (int j = 0; j < 2 && j < nst; ++j) {
-        if (ok) ok = mbar_wait(smem_u32(&full[j]), 0);
-        if (ok) waited = j + 1;
-    }
+                                         unsigned char* ring, int stage_bytes, uint64_t* full, uint64_t* empty,
+                                         const TmaThread& H, int g0) {
+    const bool lead = (threadIdx.x & 31) == 0;
+    auto slot = [&](int g) { return g % TMA_STAGES; };
+    auto wait_full = [&](int g) { return mbar_wait(smem_u32(&full[slot(g)]), (g / TMA_STAGES) & 1); };
+    auto release = [&](int g) {
+        __syncwarp();
+        if (lead) mbar_arrive(smem_u32(&empty[slot(g)]));
+    };
+    if (!wait_full(g0) || !wait_full(g0 + 1)) return false;
     for (int i = 0; i < T.nx; ++i) {
-        const int jn = i + 2;  // stage of plane x+1
-        if (ok && jn < nst) {
-            ok = mbar_wait(smem_u32(&full[jn % TMA_STAGES]), (jn / TMA_STAGES) & 1);
-            if (ok) waited = jn + 1;
-        }
-        // (after a failed wait the plane is computed from whatever the stage
-        // holds, in bounds, and the solve reports the error)
+        const int g = g0 + i;  // stage of plane x-1
+        if (!wait_full(g + 2)) return false;
         if (H.inbox)
-            tma_plane<EX, EY, EZ>(A, S, ring + (i % TMA_STAGES) * stage_bytes,
-                                  ring + ((i + 1) % TMA_STAGES) * stage_bytes, ring + (jn % TMA_STAGES) * stage_bytes,
-                                  T.x0 + i, H);
-        // every thread is done with the stage of plane x-1 (and all waits held)
-        if (__syncthreads_or(!ok)) return false;
-        const int jf = i + TMA_STAGES;
-        if (jf < nst) {
-            if (tid == 0)
-                tma_issue_stage(maps, S, T, rs + (jf % TMA_STAGES) * stage_bytes, smem_u32(&full[jf % TMA_STAGES]),
-                                jf);
-            issued = jf + 1;
-        }
+            tma_plane<EX, EY, EZ>(A, S, ring + slot(g) * stage_bytes, ring + slot(g + 1) * stage_bytes,
+                                  ring + slot(g + 2) * stage_bytes, T.x0 + i, H);
+        release(g);  // plane x-1 is no longer read
     }
+    release(g0 + T.nx);
+    release(g0 + T.nx + 1);
     return true;
 }
 
+// Persistent kernel: CTA b processes tiles cta_first[b] .. cta_first[b+1]-1 (a
+// balanced assignment made on the host).  Warps 0-3 compute; warp 4 (one
+// lane) issues the stages of the CTA's tiles in sequence, running ahead of the
+// computation by up to TMA_STAGES stages (a stage is refilled once every
+// consumer warp has released it).
 // (a template so that every translation unit may include it; instantiated for float only)
 template <typename TT>
-__global__ void __launch_bounds__(TMA_THREADS, 4)
+__global__ void __launch_bounds__(TMA_BLOCK, 3)
     k_pml_shell_tma(const KArgs<TT> A, const TmaLaunch Lc, const TmaTile* __restrict__ tiles,
-                    const CUtensorMap* __restrict__ maps, int* __restrict__ dev_error) {
+                    const int* __restrict__ cta_first, const CUtensorMap* __restrict__ maps,
+                    int* __restrict__ dev_error) {
     static_assert(sizeof(TT) == 4, "the reduced PML state is an FP32 path");
-    // the ring: TMA_STAGES stages of Lc.stage_bytes, then one mbarrier per stage
+    // the ring: TMA_STAGES stages of Lc.stage_bytes, then the full and the empty mbarriers
     extern __shared__ __align__(128) unsigned char tma_ring[];
     uint64_t* full = reinterpret_cast<uint64_t*>(tma_ring + TMA_STAGES * Lc.stage_bytes);
+    uint64_t* empty = full + TMA_STAGES;
     if (A.advance && blockIdx.x == 0 && threadIdx.x == 0) advance_consts(*A.P, A.cur);
-    const TmaTile T = tiles[blockIdx.x];
-    const TmaShape& S = Lc.shape[T.shape];
-    const CUtensorMap* m = maps + ((size_t)A.cur * Lc.nshape + T.shape) * TB_N;
     const int tid = threadIdx.x;
     const uint32_t ring = smem_u32(tma_ring);
     // tensor copies land on 128-byte boundaries (every buffer size is a multiple of 128)
@@ -329,63 +331,92 @@ __global__ void __launch_bounds__(TMA_THREADS, 4)
         if (tid == 0) atomicOr(dev_error, FDTD_DEV_ERR_TMA_TIMEOUT);
         return;
     }
-    const int nst = T.nx + 2;
     if (tid == 0) {
 #pragma unroll
-        for (int s = 0; s < TMA_STAGES; ++s) mbar_init(smem_u32(&full[s]), 1);
+        for (int s = 0; s < TMA_STAGES; ++s) {
+            mbar_init(smem_u32(&full[s]), 1);
+            mbar_init(smem_u32(&empty[s]), TMA_THREADS / 32);
+        }
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
         asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
     }
     __syncthreads();
-    if (tid == 0)
-        for (int j = 0; j < TMA_STAGES && j < nst; ++j)
-            tma_issue_stage(m, S, T, ring + j * Lc.stage_bytes, smem_u32(&full[j]), j);
+    const int t_begin = cta_first[blockIdx.x], t_end = cta_first[blockIdx.x + 1];
 
-    // this thread's cells: row r of the window, z group lz .. lz+3
-    TmaThread H;
-    const int gpr = S.tz / 4;
-    H.r = tid / gpr;
-    H.lz = (tid - H.r * gpr) * 4;
-    H.zc = T.z0 + H.lz;
-    const bool row_on = H.r < T.ny;
-    H.y = T.y0 + (row_on ? H.r : T.ny - 1);
-    H.inbox = 0;
-#pragma unroll
-    for (int e = 0; e < 4; ++e) H.inbox |= (row_on && H.zc + e >= T.zlo && H.zc + e < T.zhi ? 1u : 0u) << e;
-    H.gy = __ldg(A.axflag[1] + H.y);
-    {
-        uint8_t gz[4];
-#pragma unroll
-        for (int e = 0; e < 4; ++e) gz[e] = H.zc + e < A.N2 ? __ldg(A.axflag[2] + H.zc + e) : (uint8_t)0;
-#pragma unroll
-        for (int k = 0; k < 6; ++k) H.zm[k] = flag_mask<4>(gz, k);
-    }
-    if ((T.cls & TC_Z) && H.inbox) {
-#pragma unroll
-        for (int e = 0; e <= 4; ++e) H.cz[e] = A.coef[2][H.zc + e];
-    }
-    if (T.cls & TC_Y) {
-        H.cyl = A.coef[1][H.y];
-        H.cyr = A.coef[1][H.y + 1];
+    if (tid >= TMA_THREADS) {
+        // ---- producer: one lane issues every stage of the CTA's tiles ----
+        if (tid != TMA_THREADS) return;
+        int g = 0;
+        bool ok = true;
+        for (int t = t_begin; t < t_end && ok; ++t) {
+            const TmaTile T = tiles[t];
+            const TmaShape& S = Lc.shape[T.shape];
+            const CUtensorMap* m = maps + ((size_t)A.cur * Lc.nshape + T.shape) * TB_N;
+            for (int j = 0; j < T.nx + 2 && ok; ++j, ++g) {
+                const int sl = g % TMA_STAGES;
+                // the slot's previous stage (g - TMA_STAGES) has been released by every consumer warp
+                if (g >= TMA_STAGES) ok = mbar_wait(smem_u32(&empty[sl]), (g / TMA_STAGES - 1) & 1);
+                if (ok) tma_issue_stage(m, S, T, ring + sl * Lc.stage_bytes, smem_u32(&full[sl]), j);
+            }
+        }
+        if (!ok) atomicOr(dev_error, FDTD_DEV_ERR_TMA_TIMEOUT);
+        // no copy outlives the CTA: wait (bounded) for the last stages issued
+        for (int k = g - 1; k >= 0 && k >= g - TMA_STAGES; --k)
+            (void)mbar_wait(smem_u32(&full[k % TMA_STAGES]), (k / TMA_STAGES) & 1);
+        return;
     }
 
-    int waited = 0, issued = nst < TMA_STAGES ? nst : TMA_STAGES;
-    bool done;
-    unsigned char* R = tma_ring;
-    const int sb = Lc.stage_bytes;
-    switch (T.cls) {
-        case TC_X: done = tma_tile<true, false, false>(A, S, T, m, R, sb, full, H, waited, issued); break;
-        case TC_Y: done = tma_tile<false, true, false>(A, S, T, m, R, sb, full, H, waited, issued); break;
-        case TC_Z: done = tma_tile<false, false, true>(A, S, T, m, R, sb, full, H, waited, issued); break;
-        case TC_X | TC_Y: done = tma_tile<true, true, false>(A, S, T, m, R, sb, full, H, waited, issued); break;
-        case TC_X | TC_Z: done = tma_tile<true, false, true>(A, S, T, m, R, sb, full, H, waited, issued); break;
-        case TC_Y | TC_Z: done = tma_tile<false, true, true>(A, S, T, m, R, sb, full, H, waited, issued); break;
-        default: done = tma_tile<true, true, true>(A, S, T, m, R, sb, full, H, waited, issued); break;
-    }
-    if (!done && tid == 0) {
-        atomicOr(dev_error, FDTD_DEV_ERR_TMA_TIMEOUT);
-        // wait (bounded) for the copies this CTA still has in flight
-        for (int j = waited; j < issued; ++j) (void)mbar_wait(smem_u32(&full[j % TMA_STAGES]), (j / TMA_STAGES) & 1);
+    // ---- consumers ----
+    int g0 = 0;
+    for (int t = t_begin; t < t_end; ++t) {
+        const TmaTile T = tiles[t];
+        const TmaShape& S = Lc.shape[T.shape];
+        // this thread's cells: row r of the window, z group lz .. lz+3
+        TmaThread H;
+        const int gpr = S.tz / 4;
+        H.r = tid / gpr;
+        H.lz = (tid - H.r * gpr) * 4;
+        H.zc = T.z0 + H.lz;
+        const bool row_on = H.r < T.ny;
+        H.y = T.y0 + (row_on ? H.r : T.ny - 1);
+        H.inbox = 0;
+#pragma unroll
+        for (int e = 0; e < 4; ++e) H.inbox |= (row_on && H.zc + e >= T.zlo && H.zc + e < T.zhi ? 1u : 0u) << e;
+        H.gy = __ldg(A.axflag[1] + H.y);
+        {
+            uint8_t gz[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) gz[e] = H.zc + e < A.N2 ? __ldg(A.axflag[2] + H.zc + e) : (uint8_t)0;
+#pragma unroll
+            for (int k = 0; k < 6; ++k) H.zm[k] = flag_mask<4>(gz, k);
+        }
+        if ((T.cls & TC_Z) && H.inbox) {
+#pragma unroll
+            for (int e = 0; e <= 4; ++e) H.cz[e] = A.coef[2][H.zc + e];
+        }
+        if (T.cls & TC_Y) {
+            H.cyl = A.coef[1][H.y];
+            H.cyr = A.coef[1][H.y + 1];
+        }
+        unsigned char* R = tma_ring;
+        const int sb = Lc.stage_bytes;
+        bool done;
+        switch (T.cls) {
+            case TC_X: done = tma_tile<true, false, false>(A, S, T, R, sb, full, empty, H, g0); break;
+            case TC_Y: done = tma_tile<false, true, false>(A, S, T, R, sb, full, empty, H, g0); break;
+            case TC_Z: done = tma_tile<false, false, true>(A, S, T, R, sb, full, empty, H, g0); break;
+            case TC_X | TC_Y: done = tma_tile<true, true, false>(A, S, T, R, sb, full, empty, H, g0); break;
+            case TC_X | TC_Z: done = tma_tile<true, false, true>(A, S, T, R, sb, full, empty, H, g0); break;
+            case TC_Y | TC_Z: done = tma_tile<false, true, true>(A, S, T, R, sb, full, empty, H, g0); break;
+            default: done = tma_tile<true, true, true>(A, S, T, R, sb, full, empty, H, g0); break;
+        }
+        if (!done) {
+            // a stage never arrived: record it and leave (the producer's own
+            // bounded waits end, and it waits for its copies in flight)
+            if ((tid & 31) == 0) atomicOr(dev_error, FDTD_DEV_ERR_TMA_TIMEOUT);
+            return;
+        }
+        g0 += T.nx + 2;
     }
 }
 

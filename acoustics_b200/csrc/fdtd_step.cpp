@@ -822,7 +822,15 @@ fdtd_status fdtd_solver_restore(fdtd_solver* s, const void* buffer, int64_t byte
     CUDA_TRY(s, cudaSetDevice(s->opt.device));
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     const char* p = (const char*)buffer + sizeof(h);
+    // the pose state comes from the snapshot; what points into this solver's own
+    // storage (device meshes, keyframe tracks, mesh vertices) stays this solver's
+    const std::vector<HostObject> own = s->objs;
     std::memcpy(s->objs.data(), p, s->objs.size() * sizeof(HostObject));
+    for (size_t i = 0; i < s->objs.size(); ++i) {
+        s->objs[i].mview = own[i].mview;
+        s->objs[i].kf = own[i].kf;
+        s->objs[i].mv = own[i].mv;
+    }
     p += s->objs.size() * sizeof(HostObject);
     for (auto& r : regs) {
         CUDA_TRY(s, fdtd::counted_copy(s, r.first, p, r.second, cudaMemcpyHostToDevice));

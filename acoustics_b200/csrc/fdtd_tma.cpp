@@ -87,6 +87,7 @@ void free_shell_tma(fdtd_solver* s) {
     if (!s->tma) return;
     if (s->tma->d_tiles) cudaFree(s->tma->d_tiles);
     if (s->tma->d_maps) cudaFree(s->tma->d_maps);
+    if (s->tma->d_cta_first) cudaFree(s->tma->d_cta_first);
     delete s->tma;
     s->tma = nullptr;
     s->region.tma = nullptr;
@@ -175,7 +176,12 @@ fdtd_status build_shell_tma(fdtd_solver* s) {
         L.stage_bytes = std::max(L.stage_bytes, shape_bytes(L.shape[k]));
     }
 
-    // x planes per tile: 16, or fewer until the tiles fill four CTAs per SM
+    // persistent CTAs: as many as fit at once
+    int dev = 0, sms = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int per_sm = std::max(1, tma_blocks_per_sm(tma_smem_bytes(L)));
+    const int max_grid = sms * per_sm;
+    // x planes per tile: 16, or fewer until there are three tiles per CTA to balance
     std::vector<TmaTile> tiles;
     for (int XS = 16; XS >= 4; XS /= 2) {
         tiles.clear();
@@ -203,9 +209,47 @@ fdtd_status build_shell_tma(fdtd_solver* s) {
                                 }
                     }
         }
-        if ((int)tiles.size() >= 4 * 148) break;
+        if ((int)tiles.size() >= 3 * max_grid) break;
     }
     L.ntiles = (int)tiles.size();
+
+    // each CTA gets a list of tiles of about equal bytes (largest first, each to
+    // the least loaded CTA)
+    const int grid = std::max(1, std::min((int)tiles.size(), max_grid));
+    std::vector<double> cost(tiles.size());
+    for (size_t k = 0; k < tiles.size(); ++k) {
+        const TmaShape& S = L.shape[tiles[k].shape];
+        double b = 0;
+        for (int q = 0; q < TB_N; ++q) b += S.bytes[q];
+        cost[k] = b * (tiles[k].nx + 2);
+    }
+    std::vector<size_t> order(tiles.size());
+    for (size_t k = 0; k < order.size(); ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t b) { return cost[a] > cost[b]; });
+    std::vector<std::vector<size_t>> per_cta(grid);
+    std::vector<std::pair<double, int>> heap;  // (load, cta), min-heap
+    for (int b = 0; b < grid; ++b) heap.push_back({0.0, b});
+    auto cmp = [](const std::pair<double, int>& a, const std::pair<double, int>& b) {
+        return a.first > b.first || (a.first == b.first && a.second > b.second);
+    };
+    std::make_heap(heap.begin(), heap.end(), cmp);
+    for (size_t k : order) {
+        std::pop_heap(heap.begin(), heap.end(), cmp);
+        heap.back().first += cost[k];
+        per_cta[heap.back().second].push_back(k);
+        std::push_heap(heap.begin(), heap.end(), cmp);
+    }
+    std::vector<TmaTile> ordered;
+    std::vector<int> first(grid + 1, 0);
+    for (int b = 0; b < grid; ++b) {
+        first[b] = (int)ordered.size();
+        // a CTA's tiles in x order of their class: the ring runs on from one to the next
+        std::sort(per_cta[b].begin(), per_cta[b].end());
+        for (size_t k : per_cta[b]) ordered.push_back(tiles[k]);
+    }
+    first[grid] = (int)ordered.size();
+    tiles.swap(ordered);
+    T->grid = grid;
 
     // maps [parity][shape][buffer], in device memory
     std::vector<CUtensorMap> maps((size_t)2 * L.nshape * TB_N);
@@ -224,13 +268,17 @@ fdtd_status build_shell_tma(fdtd_solver* s) {
             if (!ok) return (set_error(s, "cuTensorMapEncodeTiled rejected a shell map"), FDTD_ERR_UNSUPPORTED);
         }
     const size_t tb = tiles.size() * sizeof(TmaTile), mb = maps.size() * sizeof(CUtensorMap);
+    const size_t fb = first.size() * sizeof(int);
     cudaError_t e = cudaMalloc((void**)&T->d_tiles, tb);
     if (e == cudaSuccess) e = cudaMalloc((void**)&T->d_maps, mb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&T->d_cta_first, fb);
     if (e == cudaSuccess) e = counted_copy(s, T->d_tiles, tiles.data(), tb, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = counted_copy(s, T->d_maps, maps.data(), mb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = counted_copy(s, T->d_cta_first, first.data(), fb, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) {
         if (T->d_tiles) cudaFree(T->d_tiles);
         if (T->d_maps) cudaFree(T->d_maps);
+        if (T->d_cta_first) cudaFree(T->d_cta_first);
         cuda_fail(s, e, "shell tiles and tensor maps");
         return e == cudaErrorMemoryAllocation ? FDTD_ERR_OOM : FDTD_ERR_CUDA;
     }

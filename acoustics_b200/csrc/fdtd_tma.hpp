@@ -8,8 +8,9 @@
 
 namespace fdtd {
 
-constexpr int TMA_THREADS = 128;
-constexpr int TMA_STAGES = 4;
+constexpr int TMA_THREADS = 128;                    // consumer threads (4 warps) of a CTA
+constexpr int TMA_BLOCK = TMA_THREADS + 32;         // + one producer warp
+constexpr int TMA_STAGES = 5;
 constexpr int TMA_MAX_SHAPES = 8;
 // bit the shell kernel sets in the solve's dev_error flags when a stage never arrives
 constexpr int FDTD_DEV_ERR_TMA_TIMEOUT = 2;
@@ -49,15 +50,20 @@ struct TmaLaunch {
 };
 
 // Everything a step needs to launch the kernel: the launch description (host
-// memory), the device tile table and the device tensor maps
+// memory), the device tile table (ordered by CTA: CTA b takes tiles
+// cta_first[b] .. cta_first[b+1]-1), and the device tensor maps
 // [parity of p^n][shape][TB_*] (64-byte aligned, written before any launch).
 struct TmaStep {
     TmaLaunch launch;
+    int grid;          // persistent CTAs
     TmaTile* d_tiles;
+    int* d_cta_first;  // grid + 1 offsets
     CUtensorMap* d_maps;
 };
 
-// dynamic shared memory of the kernel: the ring and one mbarrier per stage
-inline int tma_smem_bytes(const TmaLaunch& L) { return TMA_STAGES * L.stage_bytes + 8 * TMA_STAGES; }
+// dynamic shared memory of the kernel: the ring, then a full and an empty mbarrier per stage
+inline int tma_smem_bytes(const TmaLaunch& L) { return TMA_STAGES * L.stage_bytes + 16 * TMA_STAGES; }
+// CTAs of the kernel that fit on one SM with this dynamic shared memory (fdtd_fp32.cu)
+int tma_blocks_per_sm(int smem_bytes);
 
 }  // namespace fdtd

@@ -160,6 +160,8 @@ struct fdtd_scene {
     std::vector<fdtd_mesh_desc> meshes;
     std::vector<std::vector<double>> mverts;
     std::vector<std::vector<int32_t>> mtris;
+    std::vector<fdtd_keyframe_track> tracks;
+    std::vector<std::vector<double>> tframes;
     int32_t steps = 0;
     std::string output_pattern;
 };
@@ -180,8 +182,39 @@ fdtd_status fdtd_scene_from_xml(const char* path, fdtd_scene** out) {
     if (root->name != "impulse_response") return (set_error(nullptr, "root element must be <impulse_response>"), FDTD_ERR_INVALID_ARG);
     std::unique_ptr<fdtd_scene> sc(new fdtd_scene());
     std::string err;
+    // features outside this path are named before any file they refer to is read
+    if (const XNode* scene = root->child("scene"))
+        for (auto& kid : scene->kids) {
+            const XNode* n = kid.get();
+            if (n->name == "acoustic_shaders")
+                return (set_error(nullptr, "<acoustic_shaders> (modal transfer shaders) is not on this path"),
+                        FDTD_ERR_UNSUPPORTED);
+            if (n->name == "rigid_object_sequence" || n->name == "shell_object")
+                return (set_error(nullptr, "<" + n->name + "> (object-file sequences, shell objects) is not on this path"),
+                        FDTD_ERR_UNSUPPORTED);
+            if (n->name == "rigid_sound_object") {
+                auto on = [&](const char* a) {
+                    auto it = n->attr.find(a);
+                    return it != n->attr.end() && std::atof(it->second.c_str()) != 0.0;
+                };
+                if (on("has_modal_source") || n->attr.count("add_shader_by_id") || n->attr.count("mode_file") ||
+                    on("has_acc_noise_source"))
+                    return (set_error(nullptr, "<rigid_sound_object> with modal vibration sources or shaders is not on "
+                                               "this path (a <rigid_object> mesh is)"),
+                            FDTD_ERR_UNSUPPORTED);
+            }
+            if (n->name == "rigid_object" &&
+                (n->attr.count("has_harmonic_source") || n->attr.count("speaker_file") || n->attr.count("has_speaker_shader")))
+                return (set_error(nullptr, "<rigid_object> speaker / harmonic vibration sources are not on this path"),
+                        FDTD_ERR_UNSUPPORTED);
+        }
     const XNode* solver = root->child("solver");
     if (!solver) return (set_error(nullptr, "missing <solver>"), FDTD_ERR_INVALID_ARG);
+    {
+        auto tp = solver->attr.find("time_parallel");
+        if (tp != solver->attr.end() && std::atof(tp->second.c_str()) != 0.0)
+            return (set_error(nullptr, "time-parallel chunking (time_parallel) is not on this path"), FDTD_ERR_UNSUPPORTED);
+    }
     fdtd_scene_desc& D = sc->desc;
     double freq = 0, v = 0;
     // GetSolverSettings (ImpulseResponseParser.cpp:493-575)
@@ -300,6 +333,25 @@ fdtd_status fdtd_scene_from_xml(const char* path, fdtd_scene** out) {
                     if (!get_real(n, vk[d], o.velocity[d], false, 0.0, err) || !get_real(n, gk[d], o.gravity[d], false, 0.0, err))
                         return (set_error(nullptr, err), FDTD_ERR_INVALID_ARG);
                 }
+                // keyframes (ImpulseResponseParser.cpp:250-264): file_kinematics= kinematics_frame_rate=
+                auto kin = n->attr.find("file_kinematics");
+                if (kin != n->attr.end() && kin->second != "N/A") {
+                    double rate = 0;
+                    if (!get_real(n, "kinematics_frame_rate", rate, true, 0, err) || !(rate > 0))
+                        return (set_error(nullptr, err.empty() ? "kinematics_frame_rate must be positive" : err),
+                                FDTD_ERR_INVALID_ARG);
+                    std::string kf = kin->second;
+                    if (!std::ifstream(kf) && !kf.empty() && kf[0] != '/') {
+                        const std::string xp_dir = std::string(path).substr(0, std::string(path).find_last_of('/') + 1);
+                        if (std::ifstream(xp_dir + kf)) kf = xp_dir + kf;
+                    }
+                    std::vector<double> frames;
+                    if (!fdtd::read_kinematics(kf.c_str(), frames, err)) return (set_error(nullptr, err), FDTD_ERR_IO);
+                    o.motion = FDTD_MOTION_KEYFRAMED;
+                    sc->tracks.push_back(fdtd_keyframe_track{(int32_t)sc->objects.size(), (int32_t)(frames.size() / 7),
+                                                             1.0 / rate, nullptr});
+                    sc->tframes.push_back(std::move(frames));
+                }
                 sc->objects.push_back(o);
             } else if (n->name == "constraint") {
                 // ImpulseResponseParser.cpp:433-449
@@ -366,6 +418,9 @@ fdtd_status fdtd_scene_from_xml(const char* path, fdtd_scene** out) {
     }
     D.n_meshes = (int32_t)sc->meshes.size();
     D.meshes = sc->meshes.empty() ? nullptr : sc->meshes.data();
+    for (size_t k = 0; k < sc->tracks.size(); ++k) sc->tracks[k].frames = sc->tframes[k].data();
+    D.n_tracks = (int32_t)sc->tracks.size();
+    D.tracks = sc->tracks.empty() ? nullptr : sc->tracks.data();
     *out = sc.release();
     return FDTD_OK;
 }

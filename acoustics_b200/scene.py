@@ -20,7 +20,7 @@ import numpy as np
 
 SHAPE_SPHERE, SHAPE_BOX, SHAPE_ELLIPSOID, SHAPE_MESH = 0, 1, 2, 3
 ACCEL_NONE, ACCEL_GAUSSIAN_TRANSLATION, ACCEL_GAUSSIAN_PULSATION = 0, 1, 2
-MOTION_STATIC, MOTION_BALLISTIC = 0, 1
+MOTION_STATIC, MOTION_BALLISTIC, MOTION_KEYFRAMED = 0, 1, 2
 PRECISION_FP64, PRECISION_FP32_COMPENSATED = 0, 1
 KERNEL_FUSED, KERNEL_PHASED = 0, 1
 PML_STATE_AUTO, PML_STATE_FULL = 0, 1
@@ -65,6 +65,11 @@ class MeshDesc(C.Structure):
                 ("vertices", C.POINTER(C.c_double)), ("triangles", C.POINTER(C.c_int32))]
 
 
+class KeyframeTrackDesc(C.Structure):
+    _fields_ = [("object", C.c_int32), ("n_frames", C.c_int32), ("step", C.c_double),
+                ("frames", C.POINTER(C.c_double))]
+
+
 class SceneDesc(C.Structure):
     _fields_ = [
         ("cell_size", C.c_double), ("divisions", C.c_int32 * 3),
@@ -77,6 +82,7 @@ class SceneDesc(C.Structure):
         ("objects", C.POINTER(ObjectDesc)), ("constraints", C.POINTER(PlaneDesc)),
         ("sources", C.POINTER(GaussianSourceDesc)), ("listeners", C.POINTER(C.c_double)),
         ("boundary_handling", C.c_int32), ("n_meshes", C.c_int32), ("meshes", C.POINTER(MeshDesc)),
+        ("n_tracks", C.c_int32), ("tracks", C.POINTER(KeyframeTrackDesc)),
     ]
 
 
@@ -154,6 +160,15 @@ class TriangleMesh:
 
 
 @dataclass
+class KeyframeTrack:
+    """Keyframes of a MOTION_KEYFRAMED object (see fdtd_keyframe_track): frame i at
+    time i * step, frames[i] = (cx, cy, cz, qw, qx, qy, qz)."""
+    object: int
+    step: float
+    frames: np.ndarray  # (n, 7) float64
+
+
+@dataclass
 class PlaneConstraint:
     normal_dir: int
     normal_sign: int
@@ -191,6 +206,7 @@ class Scene:
     sources: List[GaussianSource] = field(default_factory=list)
     listeners: Optional[np.ndarray] = None
     meshes: List[TriangleMesh] = field(default_factory=list)
+    tracks: List[KeyframeTrack] = field(default_factory=list)
     steps: int = 0
     name: str = "scene"
 
@@ -236,6 +252,13 @@ class Scene:
             meshes[i].n_vertices, meshes[i].n_triangles = v.shape[0], t.shape[0]
             meshes[i].vertices = v.ctypes.data_as(C.POINTER(C.c_double))
             meshes[i].triangles = t.ctypes.data_as(C.POINTER(C.c_int32))
+        track_arrays = []
+        tracks = (KeyframeTrackDesc * max(1, len(self.tracks)))()
+        for i, t in enumerate(self.tracks):
+            f = np.ascontiguousarray(np.asarray(t.frames, dtype=np.float64).reshape(-1, 7))
+            track_arrays.append(f)
+            tracks[i].object, tracks[i].n_frames, tracks[i].step = int(t.object), f.shape[0], float(t.step)
+            tracks[i].frames = f.ctypes.data_as(C.POINTER(C.c_double))
         L = self.n_listeners
         lis = np.ascontiguousarray(np.asarray(self.listeners if L else np.zeros((1, 3)), dtype=np.float64).reshape(-1))
         desc = SceneDesc()
@@ -256,7 +279,9 @@ class Scene:
         desc.listeners = lis.ctypes.data_as(C.POINTER(C.c_double))
         desc.n_meshes = len(self.meshes)
         desc.meshes = C.cast(meshes, C.POINTER(MeshDesc))
-        return desc, (objs, planes, srcs, lis, meshes, mesh_arrays)
+        desc.n_tracks = len(self.tracks)
+        desc.tracks = C.cast(tracks, C.POINTER(KeyframeTrackDesc))
+        return desc, (objs, planes, srcs, lis, meshes, mesh_arrays, tracks, track_arrays)
 
     # ---- geometry helpers (BoundingBox.h:89-99, ScalarField.cpp:29-50) ----
     def bbox(self):

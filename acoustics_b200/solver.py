@@ -224,6 +224,11 @@ def scene_from_xml(path: str) -> Scene:
             v = np.ctypeslib.as_array(m.vertices, shape=(m.n_vertices * 3,)).reshape(-1, 3).copy()
             t = np.ctypeslib.as_array(m.triangles, shape=(m.n_triangles * 3,)).reshape(-1, 3).copy()
             sc.meshes.append(TriangleMesh(v, t))
+        from .scene import KeyframeTrack
+        for i in range(d.n_tracks):
+            t = d.tracks[i]
+            fr = np.ctypeslib.as_array(t.frames, shape=(t.n_frames * 7,)).reshape(-1, 7).copy()
+            sc.tracks.append(KeyframeTrack(int(t.object), float(t.step), fr))
         for i in range(d.n_constraints):
             p = d.constraints[i]
             sc.constraints.append(PlaneConstraint(p.normal_dir, p.normal_sign, p.height))

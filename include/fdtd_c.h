@@ -69,7 +69,28 @@ enum {
     FDTD_ACCEL_GAUSSIAN_PULSATION = 2    /* a(x,t) = g(t) * n(x) (sphere only, monopole) */
 };
 
-enum { FDTD_MOTION_STATIC = 0, FDTD_MOTION_BALLISTIC = 1 };
+enum {
+    FDTD_MOTION_STATIC = 0,
+    FDTD_MOTION_BALLISTIC = 1,
+    /* keyframes (fdtd_keyframe_track): centre of mass lerped and rotation slerped
+     * between frames, FDTD_RigidObject_Blender_Animator::GetRigidObjectTransform
+     * (FDTD_RigidObject_Animator.cpp:128-155) and FDTD_RigidObject::
+     * SetRigidBodyTransform (FDTD_RigidObject.cpp:549-566): the body's local origin
+     * goes to the frame's centre and its rest rotation is turned by the frame's */
+    FDTD_MOTION_KEYFRAMED = 2
+};
+
+/* Keyframes of one FDTD_MOTION_KEYFRAMED object: frame i at time i * step, with
+ * frames[7 i .. 7 i + 6] = centre x, y, z and rotation quaternion w, x, y, z
+ * (a kinematics file of FDTD_RigidObject_Animator.cpp:79-122 after its y-up
+ * correction; fdtd_read_kinematics reads one).  Before the first frame the first
+ * holds, after the last the last. */
+typedef struct {
+    int32_t object;          /* index into fdtd_scene_desc.objects */
+    int32_t n_frames;
+    double step;             /* seconds between frames (1 / kinematics_frame_rate) */
+    const double* frames;    /* 7 * n_frames */
+} fdtd_keyframe_track;
 
 typedef struct {
     int32_t shape;
@@ -129,6 +150,8 @@ typedef struct {
     int32_t boundary_handling;     /* FDTD_BOUNDARY_* (<solver boundary_handling=>)       */
     int32_t n_meshes;
     const fdtd_mesh_desc* meshes;  /* meshes of the FDTD_SHAPE_MESH objects                */
+    int32_t n_tracks;
+    const fdtd_keyframe_track* tracks;  /* one per FDTD_MOTION_KEYFRAMED object          */
 } fdtd_scene_desc;
 
 enum {
@@ -505,6 +528,16 @@ const fdtd_scene_desc* fdtd_scene_desc_get(const fdtd_scene* sc);
 int32_t fdtd_scene_number_of_steps(const fdtd_scene* sc);
 const char* fdtd_scene_output_pattern(const fdtd_scene* sc);
 void fdtd_scene_free(fdtd_scene* sc);
+
+/* A kinematics file of FDTD_RigidObject_Blender_Animator::ReadObjectKinData
+ * (FDTD_RigidObject_Animator.cpp:79-122): one line per frame, "frame tx ty tz qw
+ * qx qy qz"; w is clamped to [-1, 1] and every rotation is turned by -90 degrees
+ * about x (Blender's z-up to y-up, as the reference's animator does).  frames:
+ * 7 * n_frames doubles as in fdtd_keyframe_track (NULL to query n_frames). */
+fdtd_status fdtd_read_kinematics(const char* path, int32_t* n_frames, double* frames, int64_t capacity);
+/* Pose of a keyframed object at time t (host query, no GPU): centre com[3] and
+ * the rotation R[9] (row-major) that turns the rest pose. */
+fdtd_status fdtd_keyframe_pose(const fdtd_keyframe_track* track, double t, double* com, double* rotation);
 
 /* Wavefront .obj surface mesh (MeshObjReader::read with a scale, as the
  * <rigid_object scale=> attribute applies it): the "v" and "f" records, polygons

@@ -261,6 +261,43 @@ struct OMesh {
     }
 };
 
+// Quaternion arithmetic of the reference's Quaternion<double> (Quaternion.hpp):
+// q = (w, x, y, z); normalize only when |len^2 - 1| > EPS = 1e-12 (:186-195).
+struct OQuat {
+    double w, x, y, z;
+    double LengthSqr() const { return w * w + (x * x + y * y + z * z); }
+    void Normalize() {
+        double len = LengthSqr();
+        if (std::fabs(len - 1.0) > 1e-12) {
+            len = 1. / std::sqrt(len);
+            w *= len; x *= len; y *= len; z *= len;
+        }
+    }
+    double Dot(const OQuat& b) const { return w * b.w + x * b.x + y * b.y + z * b.z; }
+    OQuat Scaled(double s) const { return {w * s, x * s, y * s, z * s}; }
+    OQuat Plus(const OQuat& b) const { return {w + b.w, x + b.x, y + b.y, z + b.z}; }
+    OQuat Minus(const OQuat& b) const { return {w - b.w, x - b.x, y - b.y, z - b.z}; }
+    // Quaternion::slerp, live branch (Quaternion.hpp:392-420)
+    OQuat Slerp(double r, const OQuat& q2) const {
+        OQuat v0 = *this, v1 = q2;
+        v0.Normalize();
+        v1.Normalize();
+        double dot = v0.Dot(v1);
+        if (std::fabs(dot) > 0.9995) {
+            OQuat ret = v0.Plus(v1.Minus(v0).Scaled(r));
+            ret.Normalize();
+            return ret;
+        }
+        if (dot < 0.0) { v1 = v1.Scaled(-1.0); dot = -dot; }
+        dot = std::min(std::max(dot, -1.0), 1.0);
+        const double theta_0 = std::acos(dot);
+        const double theta = theta_0 * r;
+        OQuat v2 = v1.Minus(v0.Scaled(dot));
+        v2.Normalize();
+        return v0.Scaled(std::cos(theta)).Plus(v2.Scaled(std::sin(theta)));
+    }
+};
+
 // Rigid object: an analytic body standing in for FDTD_RigidObject's mesh + ADF
 // (FDTD_RigidObject.cpp:256-277), or a triangle mesh; negative inside.
 struct Obj {
@@ -270,8 +307,66 @@ struct Obj {
     OBox ubox;   // _bboxWorldUnion2Steps
     const OMesh* mesh = nullptr;
     V3 mlo, mhi;  // mesh: extent of rotation * v
+    // keyframed motion: frames (centre, quaternion) every kf_step seconds, rest rotation R0
+    std::vector<double> kf;
+    double kf_step = 0;
+    double R0[9];
+
+    void MeshExtent() {
+        if (!mesh) return;
+        const std::vector<double>& v = mesh->verts;
+        for (int d = 0; d < 3; ++d) { mlo[d] = DMAX; mhi[d] = -DMAX; }
+        for (size_t k = 0; k + 2 < v.size(); k += 3)
+            for (int d = 0; d < 3; ++d) {
+                const double w = d_rot(d, 0) * v[k] + d_rot(d, 1) * v[k + 1] + d_rot(d, 2) * v[k + 2];
+                mlo[d] = std::min(mlo[d], w);
+                mhi[d] = std::max(mhi[d], w);
+            }
+    }
+    double d_rot(int i, int j) const { return d.rotation[i * 3 + j]; }
+
+    // FDTD_RigidObject_Blender_Animator::GetRigidObjectTransform (FDTD_RigidObject_Animator.cpp:128-155),
+    // start time 0; then AnimateObjects' normalize (FDTD_Objects.cpp:577) and
+    // SetRigidBodyTransform's axis-angle rotation (FDTD_RigidObject.cpp:549-566)
+    void KeyframePose(double time) {
+        const int n = (int)(kf.size() / 7);
+        const double u = time / kf_step;
+        int idx_0 = 0;
+        if (u > 0) idx_0 = u >= (double)n ? n - 1 : (int)u;
+        idx_0 = std::min(std::max(0, idx_0), n - 1);
+        const int idx_1 = std::min(idx_0 + 1, n - 1);
+        const double t_0 = idx_0 * kf_step, t_1 = idx_1 * kf_step;
+        const double alpha = (idx_0 == idx_1 ? 1.0 : (time - t_0) / (t_1 - t_0));
+        const double* a = &kf[7 * (size_t)idx_0];
+        const double* b = &kf[7 * (size_t)idx_1];
+        for (int k = 0; k < 3; ++k) c[k] = a[k] * (1.0 - alpha) + b[k] * alpha;
+        OQuat q = OQuat{a[3], a[4], a[5], a[6]}.Slerp(alpha, OQuat{b[3], b[4], b[5], b[6]});
+        q.Normalize();
+        // Quaternion::toAxisRotR (Quaternion.hpp:298-313)
+        const double rad = 2.0 * std::acos(q.w);
+        double ax = 0.0, ay = 1.0, az = 0.0;
+        if (!(rad < 1e-12)) {
+            ax = q.x; ay = q.y; az = q.z;
+            const double l = std::sqrt(ax * ax + ay * ay + az * az);
+            if (l > 0) { ax /= l; ay /= l; az /= l; }
+        }
+        // the axis-angle matrix (Rodrigues), grouped as AngleAxis::toRotationMatrix
+        const double sn = std::sin(rad), cs = std::cos(rad);
+        const double sx = sn * ax, sy = sn * ay, sz = sn * az;
+        const double cx = (1.0 - cs) * ax, cy = (1.0 - cs) * ay, cz = (1.0 - cs) * az;
+        double R[9];
+        R[1] = cx * ay - sz; R[3] = cx * ay + sz;
+        R[2] = cx * az + sy; R[6] = cx * az - sy;
+        R[5] = cy * az - sx; R[7] = cy * az + sx;
+        R[0] = cx * ax + cs; R[4] = cy * ay + cs; R[8] = cz * az + cs;
+        for (int i = 0; i < 3; ++i)
+            for (int j = 0; j < 3; ++j)
+                d.rotation[i * 3 + j] = R[i * 3 + 0] * R0[0 * 3 + j] + R[i * 3 + 1] * R0[1 * 3 + j] + R[i * 3 + 2] * R0[2 * 3 + j];
+        MeshExtent();
+    }
 
     void pose(double t) {  // ballistic kinematics x(t) = x0 + v t + g t^2/2
+        if (d.motion == FDTD_MOTION_KEYFRAMED) { KeyframePose(t); return; }
         for (int a = 0; a < 3; ++a) {
             if (d.motion == FDTD_MOTION_BALLISTIC)
                 c[a] = d.center[a] + d.velocity[a] * t + 0.5 * d.gravity[a] * t * t;
@@ -1412,18 +1507,19 @@ struct Oracle {
         for (int i = 0; i < s->n_objects; ++i) {
             Obj o;
             o.d = s->objects[i];
+            for (int k = 0; k < 9; ++k) o.R0[k] = o.d.rotation[k];
             if (o.d.shape == FDTD_SHAPE_MESH) {
                 if (o.d.mesh < 0 || o.d.mesh >= (int)meshes.size()) { err = "mesh index"; return FDTD_ERR_INVALID_ARG; }
                 o.mesh = &meshes[o.d.mesh];
-                const std::vector<double>& v = o.mesh->verts;
-                for (int d = 0; d < 3; ++d) { o.mlo[d] = DMAX; o.mhi[d] = -DMAX; }
-                for (size_t k = 0; k + 2 < v.size(); k += 3)
-                    for (int d = 0; d < 3; ++d) {
-                        const double w = o.d.rotation[d * 3 + 0] * v[k] + o.d.rotation[d * 3 + 1] * v[k + 1] +
-                                         o.d.rotation[d * 3 + 2] * v[k + 2];
-                        o.mlo[d] = std::min(o.mlo[d], w);
-                        o.mhi[d] = std::max(o.mhi[d], w);
+                o.MeshExtent();
+            }
+            if (o.d.motion == FDTD_MOTION_KEYFRAMED) {
+                for (int k = 0; k < s->n_tracks; ++k)
+                    if (s->tracks[k].object == i) {
+                        o.kf.assign(s->tracks[k].frames, s->tracks[k].frames + 7 * (size_t)s->tracks[k].n_frames);
+                        o.kf_step = s->tracks[k].step;
                     }
+                if (o.kf.empty() || !(o.kf_step > 0)) { err = "keyframed object without a track"; return FDTD_ERR_INVALID_ARG; }
             }
             objs.push_back(o);
         }
