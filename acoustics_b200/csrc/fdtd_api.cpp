@@ -1056,7 +1056,10 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     // reduced state: the TMA-staged shell kernel where it applies (tiles and
     // tensor maps of this solve), else the per-thread cp.async kernel
     free_shell_tma(s);
-    if (s->region.red && s->opt.shell_staging == FDTD_SHELL_STAGING_AUTO) {
+    // (moving scenes run the shell beside the per-step classification on a
+    // low-priority stream: a persistent kernel would hold every SM the
+    // classification chain needs, so they keep the per-thread kernel)
+    if (s->region.red && s->opt.shell_staging == FDTD_SHELL_STAGING_AUTO && !s->moving) {
         st = build_shell_tma(s);
         if (st != FDTD_OK && st != FDTD_ERR_UNSUPPORTED) return st;
         if (st == FDTD_ERR_UNSUPPORTED) s->err.clear();

@@ -380,20 +380,29 @@ __device__ __noinline__ double fresh_value(const SolveParams& P, const T* __rest
         npos[q][1] = P.cpos[1][nj];
         npos[q][2] = P.cpos[2][nn];
     }
-    double A[8 * 4], b[8];
-    int kept[8];
+    // the MLS rows of the stencil cells with a valid history, in a fixed block of
+    // 8 (rows of the other cells zero), kept in registers
+    double A[8][4], b[8];
+    unsigned keptm = 0;
     int nk = 0;
-    for (int q = 0; q < nc; ++q) {
-        if (!(code[q] & CLS_VALID)) continue;
-        mls_row(image, npos[q], vals[q], &A[nk * 4], b[nk]);
-        kept[nk++] = q;
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+        const bool kq = q < nc && (code[q] & CLS_VALID);
+        if (kq) {
+            mls_row(image, npos[q], vals[q], A[q], b[q]);
+            keptm |= 1u << q;
+            ++nk;
+        } else {
+            A[q][0] = A[q][1] = A[q][2] = A[q][3] = 0.0;
+            b[q] = 0.0;
+        }
     }
     if (nk < 4) {
         if (nk != 0) {
             double md = DBL_MAX;
             int mid = -1;
-            for (int e = 0; e < nk; ++e) {
-                const int q = kept[e];
+            for (int q = 0; q < 8; ++q) {
+                if (!((keptm >> q) & 1u)) continue;
                 const double dx = image[0] - npos[q][0], dy = image[1] - npos[q][1], dz = image[2] - npos[q][2];
                 const double d2 = dx * dx + dy * dy + dz * dz;
                 if (d2 < md) { md = d2; mid = q; }
@@ -411,7 +420,7 @@ __device__ __noinline__ double fresh_value(const SolveParams& P, const T* __rest
         return 0.0;
     }
     double c0 = 0.0;
-    if (!householder_ls4(A, b, nk, c0)) c0 = 0.0;
+    if (!householder_ls4_rows8(A, b, nk, c0)) c0 = 0.0;
     double acc[3];
     boundary_accel(o, bp, t, acc);
     const double an = acc[0] * nrm[0] + acc[1] * nrm[1] + acc[2] * nrm[2];

@@ -287,6 +287,62 @@ FDTD_HD bool householder_ls4(double* A, double* b, int n, double& c0) {
     return true;
 }
 
+// The least-squares solve of householder_ls4 on a fixed block of 8 rows whose
+// unused rows are zero (the same minimiser: zero rows change no norm or dot
+// product), with every loop unrolled so the block stays in registers.  nk: the
+// rows in use, for the rank test.
+FDTD_HD bool householder_ls4_rows8(double (&A)[8][4], double (&b)[8], int nk, double& c0) {
+    double R[4][4];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        double s = 0.0;
+#pragma unroll
+        for (int i = j; i < 8; ++i) s += A[i][j] * A[i][j];
+        const double norm = sqrt(s);
+        if (!(norm > 0.0)) return false;
+        const double x0 = A[j][j];
+        const double alpha = x0 > 0.0 ? -norm : norm;
+        A[j][j] = x0 - alpha;
+        double vnorm2 = 0.0;
+#pragma unroll
+        for (int i = j; i < 8; ++i) vnorm2 += A[i][j] * A[i][j];
+#pragma unroll
+        for (int cc = j + 1; cc < 4; ++cc) {
+            double dot = 0.0;
+#pragma unroll
+            for (int i = j; i < 8; ++i) dot += A[i][j] * A[i][cc];
+            const double f = 2.0 * dot / vnorm2;
+#pragma unroll
+            for (int i = j; i < 8; ++i) A[i][cc] -= f * A[i][j];
+        }
+        {
+            double dot = 0.0;
+#pragma unroll
+            for (int i = j; i < 8; ++i) dot += A[i][j] * b[i];
+            const double f = 2.0 * dot / vnorm2;
+#pragma unroll
+            for (int i = j; i < 8; ++i) b[i] -= f * A[i][j];
+        }
+        R[j][j] = alpha;
+#pragma unroll
+        for (int cc = j + 1; cc < 4; ++cc) R[j][cc] = A[j][cc];
+    }
+    const double rmax = dmax(dmax(fabs(R[0][0]), fabs(R[1][1])), dmax(fabs(R[2][2]), fabs(R[3][3])));
+#pragma unroll
+    for (int j = 0; j < 4; ++j)
+        if (fabs(R[j][j]) <= (double)(nk > 4 ? nk : 4) * 2.220446049250313e-16 * rmax) return false;
+    double x[4];
+#pragma unroll
+    for (int j = 3; j >= 0; --j) {
+        double s2 = b[j];
+#pragma unroll
+        for (int cc = j + 1; cc < 4; ++cc) s2 -= R[j][cc] * x[cc];
+        x[j] = s2 / R[j][j];
+    }
+    c0 = x[0];
+    return true;
+}
+
 // Fill one weighted MLS row for sample point pt with value val, relative to p.
 FDTD_HD void mls_row(const double p[3], const double pt[3], double val, double* Arow, double& b) {
     const double dx = pt[0] - p[0], dy = pt[1] - p[1], dz = pt[2] - p[2];

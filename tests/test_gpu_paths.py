@@ -122,7 +122,7 @@ def test_moving_bodies(oracle_lib, fdtd_lib, precision, tol):
 
 def test_moving_bodies_reduced_pml_state(oracle_lib, fdtd_lib):
     """Moving bodies that stay clear of the PML until end_time keep the reduced
-    PML state (TMA-staged shell): classification bit-exact after every chunk,
+    PML state: classification bit-exact after every chunk,
     listener series within 1e-4 of the FP64 oracle and 1e-5 of the full state."""
     sc = moving_scene()
     sc.end_time = sc.steps * sc.time_step
@@ -130,7 +130,7 @@ def test_moving_bodies_reduced_pml_state(oracle_lib, fdtd_lib):
     g = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED)
     f = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED, pml_state=S.PML_STATE_FULL)
     assert g.pml_state() == S.PML_STATE_AUTO and f.pml_state() == S.PML_STATE_FULL
-    assert g.shell_staging() == S.SHELL_STAGING_TMA
+    assert g.shell_staging() == S.SHELL_STAGING_RING  # beside the classification: the per-thread kernel
     yo, yg, yf = [], [], []
     for chunk in range(4):
         yo.append(o.step(40))
