@@ -1059,7 +1059,7 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     // (moving scenes run the shell beside the per-step classification on a
     // low-priority stream: a persistent kernel would hold every SM the
     // classification chain needs, so they keep the per-thread kernel)
-    if (s->region.red && s->opt.shell_staging == FDTD_SHELL_STAGING_AUTO && !s->moving) {
+    if (s->region.red && s->opt.shell_staging == FDTD_SHELL_STAGING_TMA && !s->moving) {
         st = build_shell_tma(s);
         if (st != FDTD_OK && st != FDTD_ERR_UNSUPPORTED) return st;
         if (st == FDTD_ERR_UNSUPPORTED) s->err.clear();

@@ -183,15 +183,17 @@ typedef struct {
 
 enum {
     /* How the PML-shell kernel of FP32 solves on the reduced PML state stages its
-     * loads (same results either way):
-     * AUTO: 3-D tensor copies (TMA) of every plane into a shared-memory ring
-     * (a persistent kernel), for static scenes where the driver provides the
-     * tensor-map encoder and the shell fits its windows; else per-thread
-     * asynchronous copies (cp.async).  Batch members and moving scenes use the
-     * per-thread copies. */
+     * loads (same results, bit for bit, either way):
+     * RING: per-thread asynchronous copies (cp.async) into a shared-memory ring;
+     * TMA: 3-D tensor copies (TMA) of every plane into a shared-memory ring, a
+     * persistent producer / consumer kernel over tiles cut by absorbing axes,
+     * for static single solves where the driver provides the tensor-map encoder
+     * and the shell fits its windows (else RING);
+     * AUTO: the faster of the two on B200 as measured, RING.
+     * Batch members and moving scenes use RING. */
     FDTD_SHELL_STAGING_AUTO = 0,
-    FDTD_SHELL_STAGING_RING = 1,  /* per-thread cp.async ring always */
-    FDTD_SHELL_STAGING_TMA = 2    /* reported by fdtd_solver_shell_staging: tensor copies in effect */
+    FDTD_SHELL_STAGING_RING = 1,
+    FDTD_SHELL_STAGING_TMA = 2
 };
 
 enum {

@@ -1,10 +1,9 @@
 """The TMA-staged PML shell (3-D tensor copies of every plane into a
-shared-memory ring) against the per-thread cp.async shell on the reduced PML
-state: the arithmetic per cell is the same, so listener series and pressure
-fields must be equal bit for bit, on grids whose edges and PML widths are not
-multiples of the kernel's windows.  The FP32 results of both stay within 1e-4
-of the FP64 oracle (tests/test_gpu_paths.py, tests/test_fullsize_gpu.py run
-the default, TMA, path)."""
+shared-memory ring, FDTD_SHELL_STAGING_TMA) against the per-thread cp.async
+shell (the default) on the reduced PML state: the arithmetic per cell is the
+same, so listener series and pressure fields must be equal bit for bit, on
+grids whose edges and PML widths are not multiples of the kernel's windows;
+with graphs it stays within 1e-4 of the FP64 oracle."""
 import numpy as np
 import pytest
 
@@ -37,8 +36,8 @@ SCENES = {
 def test_tma_shell_equals_ring_shell(fdtd_lib, name):
     sc = SCENES[name]()
     steps = 120
-    ring = PML_WaveSolver(sc, precision=F32, shell_staging=S.SHELL_STAGING_RING)
-    tma = PML_WaveSolver(sc, precision=F32)
+    ring = PML_WaveSolver(sc, precision=F32)
+    tma = PML_WaveSolver(sc, precision=F32, shell_staging=S.SHELL_STAGING_TMA)
     assert ring.pml_state() == S.PML_STATE_AUTO
     assert ring.shell_staging() == S.SHELL_STAGING_RING
     assert tma.shell_staging() == S.SHELL_STAGING_TMA
@@ -54,7 +53,7 @@ def test_tma_shell_equals_ring_shell(fdtd_lib, name):
 def test_tma_shell_with_graphs_against_oracle(oracle_lib, fdtd_lib):
     sc = small_config2()
     yo = oracle_lib.OracleSolver(sc).step(sc.steps)
-    g = PML_WaveSolver(sc, precision=F32, graph_steps=16)
+    g = PML_WaveSolver(sc, precision=F32, graph_steps=16, shell_staging=S.SHELL_STAGING_TMA)
     assert g.shell_staging() == S.SHELL_STAGING_TMA
     yg = g.step(sc.steps)
     assert rel_l2(yg, yo) <= 1e-4
