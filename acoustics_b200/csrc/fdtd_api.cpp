@@ -491,9 +491,7 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
             MeshHost m;
             std::string err;
             if (!build_mesh(sc->meshes[o.mesh], m, err)) return (set_error(nullptr, err), FDTD_ERR_GEOMETRY);
-            if (sc->boundary_handling == FDTD_BOUNDARY_FULLY_COUPLED)
-                return (set_error(nullptr, "FULLY_COUPLED boundaries are built for analytic spheres and boxes"),
-                        FDTD_ERR_UNSUPPORTED);
+
         }
         if (o.accel_kind == FDTD_ACCEL_GAUSSIAN_PULSATION && o.shape != FDTD_SHAPE_SPHERE)
             return (set_error(nullptr, "pulsating acceleration is defined for spheres only"), FDTD_ERR_UNSUPPORTED);
@@ -527,13 +525,10 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
     if (sc->boundary_handling != FDTD_BOUNDARY_RASTERIZE && sc->boundary_handling != FDTD_BOUNDARY_FULLY_COUPLED)
         return (set_error(nullptr, "unknown boundary_handling"), FDTD_ERR_INVALID_ARG);
     if (sc->boundary_handling == FDTD_BOUNDARY_FULLY_COUPLED)
-        for (int i = 0; i < sc->n_objects; ++i) {
-            if (sc->objects[i].motion != FDTD_MOTION_STATIC)
-                return (set_error(nullptr, "FULLY_COUPLED boundaries are built for static scenes only"), FDTD_ERR_UNSUPPORTED);
+        for (int i = 0; i < sc->n_objects; ++i)
             if (sc->objects[i].shape == FDTD_SHAPE_ELLIPSOID)
-                return (set_error(nullptr, "FULLY_COUPLED boundaries need a closest-point query (spheres and boxes)"),
+                return (set_error(nullptr, "FULLY_COUPLED boundaries need a closest-point query (spheres, boxes, meshes)"),
                         FDTD_ERR_UNSUPPORTED);
-        }
     return FDTD_OK;
 }
 

@@ -1,4 +1,4 @@
-// fdtd_coupled.cpp — FULLY_COUPLED ghost-cell rows of a static scene
+// fdtd_coupled.cpp — FULLY_COUPLED ghost-cell rows
 // (MAC_Grid::PML_pressureUpdateGhostCells, MAC_Grid.cpp:1131-1425, the branch
 // `use_immerse_interface`).
 //
@@ -12,10 +12,11 @@
 // sparse system.  The interpolation weights solve V^T w = v^T, V the 8 x 8
 // Vandermonde matrix of the stencil and v the row of the image point; a
 // stencil whose condition number exceeds CONDN_LIM = 25 and that contains the
-// Neumann row falls back to the rasterized value.  For a static scene all of
-// this depends on the geometry only, so it is computed here once per
-// classification; each step builds the right-hand side and solves the system
-// on the device (fdtd_coupled.cuh).
+// Neumann row falls back to the rasterized value.  All of this depends on the
+// geometry only, so it is computed here once per classification (once for a
+// static scene, every step for moving bodies); each step builds the right-hand
+// side and solves the system on the device (fdtd_coupled.cuh).  Mesh bodies are
+// reflected with their hierarchy in host memory.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
@@ -172,7 +173,7 @@ void free_fully_coupled(fdtd_solver* s) {
     P.fc_n = 0;
 }
 
-// Rows of the FULLY_COUPLED system after a classification (static scenes).
+// Rows of the FULLY_COUPLED system after a classification.
 fdtd_status build_fully_coupled(fdtd_solver* s) {
     free_fully_coupled(s);
     SolveParams& P = s->hP;
@@ -261,10 +262,17 @@ fdtd_status build_fully_coupled(fdtd_solver* s) {
         }
         return best;
     };
+    // the bodies as the host queries them: mesh hierarchies in host memory
+    std::vector<DevObject> hobj(P.obj, P.obj + std::max(0, P.n_obj));
+    for (size_t i = 0; i < hobj.size() && i < s->objs.size(); ++i)
+        if (hobj[i].shape == FDTD_SHAPE_MESH) {
+            const MeshHost& M = s->meshes[s->objs[i].d.mesh];
+            hobj[i].mesh = MeshView{M.nodes.data(), M.tris.data(), (int)M.nodes.size(), (int)M.tris.size()};
+        }
     for (long long ri = 0; ri < nrow; ++ri) {
         FcRow& r = rows[ri];
         if (r.kind == 1) continue;
-        const DevObject& o = P.obj[r.obj];
+        const DevObject& o = hobj[r.obj];
         double pos[3];
         centre(r.owner, pos);
         pos[r.dim] += (r.sign > 0 ? 1.0 : -1.0) * 0.25 * h;

@@ -144,6 +144,14 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         if (s->moving) {
             CUDA_TRY(s, launch_fresh_cells(s->dP, s->precision, cur, s->ncell, s->d_status, s->stream));
             s->launches++;
+            if (s->boundary_handling == FDTD_BOUNDARY_FULLY_COUPLED) {
+                // the coupled rows of this step's ghost faces (host build from the new flags)
+                st = build_fully_coupled(s);
+                if (st != FDTD_OK) return st;
+                s->region.fc = s->hP.fc_n > 0 ? 1 : 0;
+                CUDA_TRY(s, fdtd::counted_copyAsync(s, s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice,
+                                                    s->stream));
+            }
         } else if (s->L > 0) {
             // static classification: the listener fits become fixed weights
             CUDA_TRY(s, launch_listener_prep(s->dP, s->precision, cur ^ 1, s->L, s->stream));

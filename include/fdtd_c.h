@@ -157,7 +157,8 @@ typedef struct {
 enum {
     FDTD_BOUNDARY_RASTERIZE = 0,      /* ghost pressure from the neighbour and the wall acceleration */
     FDTD_BOUNDARY_FULLY_COUPLED = 1   /* image-point interpolation, all ghost cells solved together
-                                         (static scenes, fused kernels, single solves) */
+                                         (spheres, boxes and meshes; fused kernels, single solves;
+                                         moving bodies rebuild the rows on the host every step) */
 };
 
 enum {

@@ -50,7 +50,40 @@ def test_fully_coupled_only_where_built(fdtd_lib):
     sc = fc_scene()
     with pytest.raises(FDTDError):
         PML_WaveSolver(sc, kernel=S.KERNEL_PHASED)
-    sc.objects.append(S.RigidObject(S.SHAPE_SPHERE, (0.0, 0.05, 0.0), (0.01, 0, 0), motion=S.MOTION_BALLISTIC,
-                                    velocity=(1.0, 0, 0)))
-    with pytest.raises(FDTDError):
+    sc.objects.append(S.RigidObject(S.SHAPE_ELLIPSOID, (0.0, 0.05, 0.0), (0.01, 0.008, 0.006)))
+    with pytest.raises(FDTDError):  # no closest-point query for ellipsoids
         PML_WaveSolver(sc)
+
+
+@pytest.mark.parametrize("precision,tol", [(S.PRECISION_FP64, TOL_FC64), (S.PRECISION_FP32_COMPENSATED, TOL_FP32)])
+def test_fully_coupled_mesh_bodies(oracle_lib, fdtd_lib, precision, tol):
+    """Mesh bodies: an icosphere and a box mesh, reflected through their hierarchies."""
+    sc = fc_scene()
+    sc.objects = []
+    sc.meshes = [S.icosphere(0.025, level=2), S.box_mesh((0.02, 0.015, 0.01))]
+    sc.objects.append(S.RigidObject(S.SHAPE_MESH, (0.0, 0.0, 0.0), (0, 0, 0), mesh=0))
+    sc.objects.append(S.RigidObject(S.SHAPE_MESH, (0.05, -0.04, 0.02), (0, 0, 0), mesh=1,
+                                    accel_kind=S.ACCEL_GAUSSIAN_TRANSLATION, accel_amplitude=1e3,
+                                    accel_t0=3e-4, accel_tau=8e-5, accel_dir=(0.6, 0.8, 0.0)))
+    yo = oracle_lib.OracleSolver(sc).step(150)
+    g = PML_WaveSolver(sc, precision=precision)
+    yg = g.step(150)
+    assert g.boundary_info()["immersed"] > 0
+    assert rel_l2(yg, yo) <= tol
+
+
+@pytest.mark.parametrize("precision,tol", [(S.PRECISION_FP64, TOL_FC64), (S.PRECISION_FP32_COMPENSATED, TOL_FP32)])
+def test_fully_coupled_moving_bodies(oracle_lib, fdtd_lib, precision, tol):
+    """A moving sphere beside the static box: the coupled rows are rebuilt every step."""
+    sc = fc_scene()
+    sc.objects[0] = S.RigidObject(S.SHAPE_SPHERE, (-0.02, 0.0, 0.0), (0.025, 0, 0), motion=S.MOTION_BALLISTIC,
+                                  velocity=(40.0, 0, 0))
+    o = oracle_lib.OracleSolver(sc)
+    g = PML_WaveSolver(sc, precision=precision)
+    for chunk in range(3):
+        yo, yg = o.step(30), g.step(30)
+        fo, go = o.classification()
+        fg, gg = g.GetGrid()
+        assert np.array_equal(fo, fg) and np.array_equal(go, gg), chunk
+        assert rel_l2(yg, yo) <= tol, chunk
+    assert g.boundary_info()["immersed"] > 0

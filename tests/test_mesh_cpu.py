@@ -74,13 +74,13 @@ def test_invalid_meshes_are_rejected(fdtd_lib, defect):
     assert fdtd_lib.fdtd_last_error()
 
 
-def test_mesh_index_and_boundary_handling_checked(fdtd_lib):
+def test_mesh_index_checked(fdtd_lib):
     m = S.icosphere(0.02, 1)
     sc = small_scene_with(S.RigidObject(S.SHAPE_MESH, (0.0, 0.0, 0.0), (0, 0, 0), mesh=1), meshes=[m])
     assert _status_of(fdtd_lib, sc) == S.STATUS_CODE["FDTD_ERR_INVALID_ARG"]
     sc = small_scene_with(S.RigidObject(S.SHAPE_MESH, (0.0, 0.0, 0.0), (0, 0, 0), mesh=0), meshes=[m])
-    sc.boundary_handling = S.BOUNDARY_FULLY_COUPLED
-    assert _status_of(fdtd_lib, sc) == S.STATUS_CODE["FDTD_ERR_UNSUPPORTED"]
+    sc.boundary_handling = S.BOUNDARY_FULLY_COUPLED  # mesh bodies take the coupled rows too
+    assert _status_of(fdtd_lib, sc) == S.STATUS_CODE["FDTD_OK"]
     sc = small_scene_with(S.RigidObject(S.SHAPE_MESH, (0.0, 0.0, 0.0), (0, 0, 0), mesh=0,
                                         accel_kind=S.ACCEL_GAUSSIAN_PULSATION, accel_amplitude=1.0,
                                         accel_tau=1e-4), meshes=[m])
