@@ -59,21 +59,35 @@ void set_error(fdtd_solver* s, const std::string& msg) {
 // ---------------------------------------------------------------------------
 namespace fdtd {
 
-// MAC_Grid::PML_absorptionCoefficient, quadratic profile, preset 0 (MAC_Grid.cpp:4064-4090);
-// pow(x,2) written as x*x (the compiler folds it identically without fast-math).
-static double absorption(double x, double mn, double mx, double w, double S) {
+// MAC_Grid::PML_absorptionCoefficient, quadratic profile (MAC_Grid.cpp:4064-4101),
+// along axis d for boundary preset `preset` (0: PML on every side; 1: on the
+// low sides and +y; 2: on +z only); pow(x,2) written as x*x (the compiler
+// folds it identically without fast-math).
+static double absorption(double x, double mn, double mx, double w, double S, int preset, int d) {
     const double hMin = x - mn, hMax = mx - x;
     const double a2 = w * w;
     const double distMin = w - hMin, distMax = w - hMax;
-    if (hMin <= w) return S * (distMin * distMin) / a2;
-    if (hMax <= w) return S * (distMax * distMax) / a2;
+    if (preset == 0) {
+        if (hMin <= w) return S * (distMin * distMin) / a2;
+        if (hMax <= w) return S * (distMax * distMax) / a2;
+    } else if (preset == 1) {
+        if (hMin <= w) return S * (distMin * distMin) / a2;
+        if (d == 1 && hMax <= w) return S * (distMax * distMax) / a2;
+    } else if (preset == 2) {
+        if (d != 2 || hMin <= w) return 0.0;
+        if (hMax <= w) return S * (distMax * distMax) / a2;
+    }
     return 0.0;
 }
 
 // one dimension of MAC_Grid::InsidePML (MAC_Grid.cpp:4027-4062)
-static bool inside_pml_1d(double x, double mn, double mx, double w) {
+static bool inside_pml_1d(double x, double mn, double mx, double w, int preset, int d) {
     const double pmlWidth = w + 1E-12;
-    return (x - mn) <= pmlWidth || (mx - x) <= pmlWidth;
+    const double hMin = x - mn, hMax = mx - x;
+    if (preset == 0) return hMin <= pmlWidth || hMax <= pmlWidth;
+    if (preset == 1) return hMin <= pmlWidth || (d == 1 && hMax <= pmlWidth);
+    if (preset == 2) return d == 2 && hMax <= pmlWidth;
+    return false;
 }
 
 void host_object_pose(HostObject& o, double t) {
@@ -296,7 +310,7 @@ bool use_reduced_pml(const fdtd_solver* s, bool no_solid_pml) {
     if (s->opt.pml_state != FDTD_PML_STATE_AUTO || !no_solid_pml) return false;
     // moving bodies only when they stay clear of the PML until end_time
     if (s->moving && !moving_clear_of_pml(const_cast<fdtd_solver*>(s))) return false;
-    if (s->shell.n != 5 || s->shell.zbox != 4) return false;
+    if (s->shell.n != 5 || s->shell.zbox != 4 || !s->eng.empty()) return false;
     for (int d = 0; d < 3; ++d) {
         const auto& T = s->tab[d];
         for (int i = 0; i < s->N[d]; ++i) {
@@ -358,12 +372,122 @@ void build_shell_boxes(fdtd_solver* s, int xs) {
     }
 }
 
+// The cells of the Engquist-Majda branch of MAC_Grid::PML_pressureUpdateCollocated
+// (MAC_Grid.cpp:515-533): non-PML cells with a boundary normal at offset 1 and
+// none at offset 0 (ScalarField::boundaryCellNormal, ScalarField.h:202-213).
+// They exist where a side has no PML (presets 1 and 2) or the PML is under
+// 1.5 cells; non-PML cells on the domain edge itself are never updated.
+static void build_engquist(fdtd_solver* s) {
+    s->eng.clear();
+    const int* N = s->N;
+    const long long stride[3] = {s->SX, s->SY, 1};
+    auto normal = [&](const int* ijk, int off, int* n) {
+        for (int d = 0; d < 3; ++d) n[d] = ijk[d] == off ? -1 : (ijk[d] == N[d] - 1 - off ? 1 : 0);
+    };
+    auto is_pml = [&](const int* a) {
+        return s->tab[0].pml_cell[a[0]] || s->tab[1].pml_cell[a[1]] || s->tab[2].pml_cell[a[2]];
+    };
+    auto edge1 = [&](int d, int i) { return i == 1 || i == N[d] - 2; };
+    for (int i = 0; i < N[0]; ++i)
+        for (int j = 0; j < N[1]; ++j) {
+            const bool all_z = edge1(0, i) || edge1(1, j);
+            for (int l = 0; l < N[2]; ++l) {
+                if (!all_z && l != 1 && l != N[2] - 2) continue;
+                const int ijk[3] = {i, j, l};
+                if (is_pml(ijk)) continue;
+                int n0[3], n1[3];
+                normal(ijk, 0, n0);
+                if (n0[0] || n0[1] || n0[2]) continue;
+                normal(ijk, 1, n1);
+                const int btype = std::abs(n1[0]) + std::abs(n1[1]) + std::abs(n1[2]);
+                if (btype == 0) continue;
+                EngCell e{};
+                e.c = (unsigned)(i * s->SX + j * s->SY + l);
+                e.flags = btype;
+                // axis order: the reference's di, dj, dk of each type
+                int di = 0, dj = 1, dk = 2;
+                if (btype == 1) {
+                    while (n1[di] == 0) ++di;
+                    dj = (di + 1) % 3;
+                    dk = (di + 2) % 3;
+                } else if (btype == 2) {
+                    while (n1[di] == 0) ++di;
+                    dj = di + 1;
+                    while (n1[dj] == 0) ++dj;
+                    dk = dj != di + 1 ? (di + 1) % 3 : (di + 2) % 3;
+                }
+                const int ax[3] = {di, dj, dk};
+                // offset of the cell displaced by (u, v, w) along (di, dj, dk)
+                auto off = [&](int u, int v, int w, bool* pml) {
+                    int a[3] = {i, j, l};
+                    const int du[3] = {u, v, w};
+                    long long o = 0;
+                    for (int q = 0; q < 3; ++q) {
+                        const int d = ax[q];
+                        a[d] += du[q];
+                        o += (long long)du[q] * stride[d];
+                    }
+                    if (pml) *pml = is_pml(a);
+                    return (int)o;
+                };
+                const int ni = n1[di], nj = n1[dj], nk = n1[dk];
+                // tangential neighbours clamped to the grid as the reference clamps them
+                auto clampd = [&](int q, int sgn) {
+                    const int d = ax[q], v = ijk[d] + sgn;
+                    return std::min(std::max(v, 0), N[d] - 1) - ijk[d];
+                };
+                bool px[4] = {false, false, false, false};
+                if (btype == 1) {
+                    e.o[0] = off(ni, 0, 0, &px[0]);
+                    e.o[1] = off(-ni, 0, 0, nullptr);
+                    e.o[2] = off(0, clampd(1, 1), 0, nullptr);
+                    e.o[3] = off(0, clampd(1, -1), 0, nullptr);
+                    e.o[4] = off(0, 0, clampd(2, 1), nullptr);
+                    e.o[5] = off(0, 0, clampd(2, -1), nullptr);
+                } else if (btype == 2) {
+                    e.o[0] = off(ni, 0, 0, &px[0]);
+                    e.o[1] = off(0, nj, 0, &px[1]);
+                    e.o[2] = off(ni, nj, 0, &px[3]);
+                    e.o[3] = off(-ni, 0, 0, nullptr);
+                    e.o[4] = off(0, -nj, 0, nullptr);
+                    e.o[5] = off(0, 0, clampd(2, 1), nullptr);
+                    e.o[6] = off(0, 0, clampd(2, -1), nullptr);
+                } else {
+                    e.o[0] = off(ni, 0, 0, &px[0]);
+                    e.o[1] = off(0, nj, 0, &px[1]);
+                    e.o[2] = off(0, 0, nk, &px[2]);
+                    e.o[3] = off(-ni, 0, 0, nullptr);
+                    e.o[4] = off(0, -nj, 0, nullptr);
+                    e.o[5] = off(0, 0, -nk, nullptr);
+                    e.o[6] = off(ni, nj, nk, &px[3]);
+                }
+                for (int q = 0; q < 4; ++q)
+                    if (px[q]) e.flags |= 16 << q;
+                s->eng.push_back(e);
+            }
+        }
+}
+
+// Cells the interior kernel updates: the non-PML box less the cells on the
+// domain edge (never updated) and one cell inside it (the Engquist cells).
+static Box3 update_box(const fdtd_solver* s) {
+    Box3 b = s->interior;
+    for (int d = 0; d < 3; ++d) {
+        b.lo[d] = std::max(b.lo[d], 2);
+        b.hi[d] = std::min(b.hi[d], s->N[d] - 2);
+    }
+    if (b.lo[0] >= b.hi[0] || b.lo[1] >= b.hi[1] || b.lo[2] >= b.hi[2])
+        for (int d = 0; d < 3; ++d) b.lo[d] = b.hi[d] = 0;
+    return b;
+}
+
 fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
     s->h = sc->cell_size;
     s->c = sc->sound_speed;
     s->rho = sc->density;
     s->k = sc->time_step;
     s->end_time = sc->end_time;
+    s->preset = sc->boundary_condition_preset;
     // BoundingBox(cellSize, divisions, center) (BoundingBox.h:89-99) -> ScalarField (ScalarField.cpp:29-50)
     for (int d = 0; d < 3; ++d) {
         const double mn = sc->domain_center[d] - s->h * (double)sc->divisions[d] / 2.0;
@@ -397,8 +521,8 @@ fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
             double p = s->bmin[d];
             p += (0.5 + (double)i) * s->h;  // ScalarField::cellPosition (ScalarField.cpp:131-140)
             T.cpos[i] = p;
-            T.pml_cell[i] = inside_pml_1d(p, s->bmin[d], s->bmax[d], w);
-            const double sigma = absorption(p, s->bmin[d], s->bmax[d], w, S);
+            T.pml_cell[i] = inside_pml_1d(p, s->bmin[d], s->bmax[d], w, s->preset, d);
+            const double sigma = absorption(p, s->bmin[d], s->bmax[d], w, S, s->preset, d);
             const double directional = one_over_k + sigma / 2.0;           // MAC_Grid.h:550-553
             T.pupd[i] = (1.0 / s->k - sigma / 2.0) / directional;          // MAC_Grid.h:558-561
             T.pdiv[i] = (-1.0 * s->rho * s->c * s->c / directional);       // MAC_Grid.h:566-569
@@ -408,8 +532,8 @@ fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
             double p = vmin;
             p += (0.5 + (double)i) * s->h;
             T.fpos[i] = p;
-            T.pml_face[i] = inside_pml_1d(p, s->bmin[d], s->bmax[d], w);
-            const double sigma = absorption(p, s->bmin[d], s->bmax[d], w, S);
+            T.pml_face[i] = inside_pml_1d(p, s->bmin[d], s->bmax[d], w, s->preset, d);
+            const double sigma = absorption(p, s->bmin[d], s->bmax[d], w, S, s->preset, d);
             double u = 1.0 / s->k - sigma / 2.0;  // MAC_Grid.h:530-536
             u /= 1.0 / s->k + sigma / 2.0;
             T.vupd[i] = u;
@@ -442,6 +566,7 @@ fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
     if (lo[0] >= hi[0] || lo[1] >= hi[1] || lo[2] >= hi[2])
         for (int d = 0; d < 3; ++d) s->interior.lo[d] = s->interior.hi[d] = 0;
     build_shell_boxes(s, FDTD_SHELL_PLANES);
+    build_engquist(s);
     (void)N;
     return FDTD_OK;
 }
@@ -457,10 +582,9 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
             return (set_error(nullptr, "divisions must lie in [4, 4096]"), FDTD_ERR_INVALID_ARG);
     if ((long long)sc->divisions[0] * sc->divisions[1] * sc->divisions[2] >= (1LL << 31))
         return (set_error(nullptr, "grid has 2^31 cells or more (flat index is int32, as ScalarField)"), FDTD_ERR_INVALID_ARG);
-    if (sc->boundary_condition_preset != 0)
-        return (set_error(nullptr, "boundary_condition_preset other than 0 (Engquist walls) is not on this path"), FDTD_ERR_UNSUPPORTED);
-    if (sc->pml_width < 1.5)
-        return (set_error(nullptr, "PML width below 1.5 cells reaches the Engquist-Majda branch (MAC_Grid.cpp:533-920)"), FDTD_ERR_UNSUPPORTED);
+    if (sc->boundary_condition_preset < 0 || sc->boundary_condition_preset > 2)
+        return (set_error(nullptr, "boundary_condition_preset must be 0, 1 or 2"), FDTD_ERR_INVALID_ARG);
+    if (!(sc->pml_width >= 0.0)) return (set_error(nullptr, "PML_width must be non-negative"), FDTD_ERR_INVALID_ARG);
     if (!(sc->air_viscosity_alpha >= 0.0))
         return (set_error(nullptr, "air_viscosity_alpha must be non-negative"), FDTD_ERR_INVALID_ARG);
     if (sc->n_objects < 0 || sc->n_objects > FDTD_MAX_OBJECTS)
@@ -533,16 +657,17 @@ static fdtd_status validate_scene(const fdtd_scene_desc* sc) {
 }
 
 // Bounding box of the Gaussian source supports (cells whose centre may lie
-// strictly inside a source's box) clipped to the non-PML box.
+// strictly inside a source's box) clipped to the interior kernel's box.
 static Box3 source_region(const fdtd_solver* s) {
     Box3 r{};
+    const Box3 U = update_box(s);  // the Engquist cells add their sources themselves
     bool any = false;
     for (const auto& g : s->sources) {
         for (int d = 0; d < 3; ++d) {
             const double a = (g.position[d] - 2.0 * g.width_space - s->bmin[d]) / s->h - 0.5;
             const double b = (g.position[d] + 2.0 * g.width_space - s->bmin[d]) / s->h - 0.5;
-            const int lo = std::max(s->interior.lo[d], (int)std::floor(a));
-            const int hi = std::min(s->interior.hi[d], (int)std::ceil(b) + 1);
+            const int lo = std::max(U.lo[d], (int)std::floor(a));
+            const int hi = std::min(U.hi[d], (int)std::ceil(b) + 1);
             if (!any) { r.lo[d] = lo; r.hi[d] = hi; }
             else { r.lo[d] = std::min(r.lo[d], lo); r.hi[d] = std::max(r.hi[d], hi); }
         }
@@ -564,6 +689,12 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
     cv.add((void**)&s->dP, sizeof(SolveParams));
     cv.add((void**)&P.cls, n);
     cv.add((void**)&P.gobj, n);
+    // static scenes: rows of the non-PML box with plain cells only (the interior skips their flags)
+    if (!s->moving) cv.add((void**)&P.plain_rows, ((size_t)N[0] * N[1] + 31) / 32 * 4);
+    if (!s->eng.empty()) {
+        cv.add((void**)&P.eng, s->eng.size() * sizeof(EngCell));
+        cv.add((void**)&P.eng_buf, s->eng.size() * ENG_BUF * 8);
+    }
     cv.add(&P.p[0], n * w);
     cv.add(&P.p[1], n * w);
     if (s->precision != FDTD_PRECISION_FP64) cv.add((void**)&P.dinc, n * 4);
@@ -740,6 +871,10 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
     solver_init_geometry(s.get(), sc);
+    if (!s->eng.empty() && o.kernel == FDTD_KERNEL_PHASED) {
+        set_error(nullptr, "the phased kernel path needs a PML of 1.5 cells or more on every side");
+        return FDTD_ERR_UNSUPPORTED;
+    }
     if (s->np >= (1LL << 31)) {
         set_error(nullptr, "grid too large: cell indices are 32-bit (padded cells >= 2^31)");
         return FDTD_ERR_UNSUPPORTED;
@@ -846,7 +981,12 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     P.ghost_count = s->d_ghost_count;
     P.ghost_cap = s->region.ghost_cap;
     P.fresh_count = s->d_ghost_count + 1;
-    s->region.interior = s->interior;
+    s->region.interior = update_box(s.get());
+    P.eng_n = (int)s->eng.size();
+    P.eng_lambda = s->c * s->k / s->h;  // MAC_Grid.cpp:488
+    if (P.eng_n > 0)
+        CUDA_TRY(s.get(), fdtd::counted_copy(s.get(), (void*)P.eng, s->eng.data(), s->eng.size() * sizeof(EngCell),
+                                             cudaMemcpyHostToDevice));
     s->region.shell = s->shell;
     s->region.sources = 0;
     for (int i = 0; i < P.n_plane; ++i) {
@@ -996,6 +1136,9 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     }
     // initFieldRasterized: every cell bulk with valid history (MAC_Grid.cpp:2459-2470, :4170-4180)
     CUDA_TRY(s, cudaMemsetAsync(P.cls, CLS_BULK | CLS_VALID, np, s->stream));
+    if (P.eng_buf) CUDA_TRY(s, cudaMemsetAsync(P.eng_buf, 0, s->eng.size() * ENG_BUF * 8, s->stream));
+    if (P.plain_rows)  // no row is known plain until the first step's classification
+        CUDA_TRY(s, cudaMemsetAsync(P.plain_rows, 0, ((size_t)s->N[0] * s->N[1] + 31) / 32 * 4, s->stream));
     CUDA_TRY(s, cudaMemsetAsync(P.gobj, GOBJ_NONE, np, s->stream));
     CUDA_TRY(s, cudaMemsetAsync(P.consts, 0, 2 * sizeof(StepConsts), s->stream));
     CUDA_TRY(s, cudaMemsetAsync(P.dev_error, 0, sizeof(int), s->stream));

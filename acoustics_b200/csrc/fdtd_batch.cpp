@@ -375,6 +375,7 @@ fdtd_status fdtd_batch_add_snapshot(fdtd_batch* b, const fdtd_scene_desc* scene,
         return batch_fail(b, code, m);
     };
     if (s->moving) return fail(FDTD_ERR_UNSUPPORTED, "moving bodies are stepped by fdtd_solver, not in batches");
+    if (!s->eng.empty()) return fail(FDTD_ERR_UNSUPPORTED, "batched members have a PML on every side");
     st = fdtd_solver_restore(s, snapshot, bytes);
     if (st != FDTD_OK) return fail(st, fdtd_solver_last_error(s));
     if (s->step_index != steps_done) return fail(FDTD_ERR_INVALID_ARG, "snapshot step differs from steps_done");
@@ -407,6 +408,10 @@ fdtd_status fdtd_batch_add(fdtd_batch* b, const fdtd_scene_desc* scene, int32_t 
     if (s->moving) {
         fdtd_solver_destroy(s);
         return batch_fail(b, FDTD_ERR_UNSUPPORTED, "moving bodies are stepped by fdtd_solver, not in batches");
+    }
+    if (!s->eng.empty()) {
+        fdtd_solver_destroy(s);
+        return batch_fail(b, FDTD_ERR_UNSUPPORTED, "batched members have a PML on every side");
     }
     Member mb;
     mb.s = s;

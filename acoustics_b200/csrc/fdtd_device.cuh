@@ -163,6 +163,7 @@ struct KArgs {
     T* pn;                        // p^{n+1} (FP64: also p^{n-1} in place)
     float* dinc;                  // FP32 increment
     const uint8_t* cls;
+    const uint32_t* plain_rows;   // see SolveParams::plain_rows (null: read every classification byte)
     T* pd[3];
     const T* vo[3];
     T* vn[3];
@@ -222,6 +223,25 @@ struct ClsBoxes {
     long long ufirst[CLS_MAX_BOXES + 1];
 };
 
+// One non-PML bulk cell one cell inside the domain edge (the Engquist-Majda
+// cells, live where a side has no PML).  o[]: signed offsets of its stencil
+// cells in the padded layout, by type:
+//   face   (1): ii_p, ii_n, jj_p, jj_n, kk_p, kk_n, -
+//   edge   (2): ii_p, jj_p, (ii_p, jj_p), ii_n, jj_n, kk_p, kk_n
+//   corner (3): ii_p, jj_p, kk_p, ii_n, jj_n, kk_n, (ii_p, jj_p, kk_p)
+// (ii along the first axis with a boundary normal; jj_n / jj_p and kk_n / kk_p
+// clamped to the grid as the reference clamps them).  flags: bits 0-1 the
+// type, bit 4+e when exterior cell e (or, e = 3, the diagonal cell) is a PML
+// cell, whose next pressure comes from the PML update.
+struct alignas(16) EngCell {
+    unsigned c;
+    int flags;
+    int o[7];
+    int pad;
+};
+constexpr int ENG_BUF = 10;   // doubles per cell: p^{n+1}, exterior values of steps n, n-1, n-2
+constexpr int DEV_ERR_ENGQUIST = 4;  // an Engquist stencil met a solid cell
+
 struct SolveParams {
     int N[3];
     int vN[3][3];         // velocity grid divisions per face orientation
@@ -261,6 +281,12 @@ struct SolveParams {
     // state
     uint8_t* cls;
     uint8_t* gobj;
+    const EngCell* eng;           // [eng_n] Engquist-Majda cells (sides without PML); null when none
+    double* eng_buf;              // [eng_n][ENG_BUF]
+    int eng_n;
+    double eng_lambda;            // c k / h
+    uint32_t* plain_rows;         // static scenes: bit x*N1+y set when every cell of row (x, y) in the
+                                  // non-PML z range is plain bulk (no solid, no solid neighbour); null otherwise
     void* p[2];
     float* dinc;
     void* pd[3];
@@ -335,6 +361,7 @@ inline KArgs<double> make_kargs<double>(SolveParams* dP, const SolveParams& P, i
     A.pn = (double*)P.p[cur ^ 1];
     A.dinc = P.dinc;
     A.cls = P.cls;
+    A.plain_rows = P.plain_rows;
     for (int d = 0; d < 3; ++d) {
         A.pd[d] = (double*)P.pd[d];
         A.vo[d] = (const double*)P.v[cur][d];
@@ -365,6 +392,7 @@ inline KArgs<float> make_kargs<float>(SolveParams* dP, const SolveParams& P, int
     A.pn = (float*)P.p[cur ^ 1];
     A.dinc = P.dinc;
     A.cls = P.cls;
+    A.plain_rows = P.plain_rows;
     for (int d = 0; d < 3; ++d) {
         A.pd[d] = (float*)P.pd[d];
         A.vo[d] = (const float*)P.v[cur][d];

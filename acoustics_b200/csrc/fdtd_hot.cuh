@@ -25,6 +25,8 @@
 // cell when the right one is not a PML cell (the x = W h layer on the low side),
 // so the interior kernel never touches velocities.
 #pragma once
+#include <algorithm>
+
 #include "fdtd_device.cuh"
 #include "fdtd_region.cuh"
 #include "fdtd_stencil.cuh"
@@ -124,7 +126,11 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
             } else {
                 prev[i] = ldv(pn + i * sx);
             }
-            if constexpr (V == 4) code[i] = *reinterpret_cast<const uint32_t*>(cls + i * sx);
+            // a row known plain reads no flag byte (the viscous form needs the valid bit)
+            const long long rb = (long long)(x0 + i) * A.N1 + yc;
+            const bool plain = !VISC && A.plain_rows && ((A.plain_rows[rb >> 5] >> (rb & 31)) & 1u);
+            if (plain) code[i] = V == 4 ? 0x80808080u : 0x8080u;
+            else if constexpr (V == 4) code[i] = *reinterpret_cast<const uint32_t*>(cls + i * sx);
             else code[i] = *reinterpret_cast<const uint16_t*>(cls + i * sx);
             if constexpr (VISC) lapl[i] = ldv(A.lapl + off + i * sx);
             zme[i] = zm_mem ? pc[i * sx - 1] : (T)0;
@@ -463,6 +469,7 @@ __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_pml_shell(
 
 }  // namespace fdtd
 
+#include "fdtd_engquist.cuh"
 #include "fdtd_shell_red.cuh"
 #include "fdtd_shell_tma.cuh"
 
@@ -484,6 +491,12 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     const bool gside = split && (has_ghost || R.fc) && S.s3 != nullptr;
     const cudaStream_t si = split ? S.s2 : S.s;
     cudaError_t e = cudaSuccess;
+    const unsigned eng_blocks = hP.eng_n > 0 ? (unsigned)std::min((hP.eng_n + 127) / 128, 148 * 8) : 0u;
+    if (eng_blocks) {
+        // Engquist cells read p^{n-1} of their stencils: before any kernel writes p^{n+1}
+        k_engquist_predict<T><<<eng_blocks, 128, 0, S.s>>>(dP, cur);
+        ++l;
+    }
     if (split) {
         e = cudaEventRecord(S.fork, S.s);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(S.s2, S.fork, 0);
@@ -542,6 +555,11 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
         e = cudaEventRecord(S.join, S.s2);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(S.s, S.join, 0);
         if (e != cudaSuccess) return e;
+    }
+    if (eng_blocks) {
+        // after every kernel that reads p^n: the exterior values go into both buffers
+        k_engquist_commit<T><<<eng_blocks, 128, 0, S.s>>>(dP, cur);
+        ++l;
     }
     if (launches) *launches += l;
     return cudaGetLastError();

@@ -92,6 +92,8 @@ struct fdtd_solver {
     std::vector<double> listeners;
     int L = 0;
     bool moving = false;
+    int preset = 0;                 // boundary_condition_preset
+    std::vector<fdtd::EngCell> eng;  // Engquist-Majda cells (sides without PML)
     int boundary_handling = 0;              // FDTD_BOUNDARY_*
     std::vector<void*> fc_alloc;            // device arrays of the FULLY_COUPLED rows
     long long fc_immersed = 0, fc_fallback = 0;

@@ -85,7 +85,10 @@ StepStreams step_streams(const fdtd_solver* s) {
 // Listener rows of static scenes run on stream4 beside the next step.  Not for
 // moving bodies or solid cells inside the PML: the next step's classification /
 // prologue rewrites cells of the pressure they read.
-bool listeners_aside(const fdtd_solver* s) { return s->stream4 && !s->moving && s->n_solid_pml == 0; }
+// (not with Engquist cells: the step after writes the exterior cells of the pressure they read)
+bool listeners_aside(const fdtd_solver* s) {
+    return s->stream4 && !s->moving && s->n_solid_pml == 0 && s->eng.empty();
+}
 
 // Make the solver stream wait for every listener launch on stream4.
 fdtd_status join_listeners(fdtd_solver* s) {
@@ -119,6 +122,7 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         // Moving bodies clear of the PML: the shell kernel reads nothing the
         // classification writes, so it starts first, on stream5, beside it.
         shell_ahead = s->moving && fused && s->cls_boxes_current && s->n_solid_pml == 0 && !s->hP.visc &&
+                      s->eng.empty() &&
                       s->stream5 && s->interior.hi[0] > s->interior.lo[0] && boxes_clear_of_shell(s, prev) &&
                       boxes_clear_of_shell(s, s->hP.boxes);
         if (shell_ahead) {
@@ -152,7 +156,12 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
                 CUDA_TRY(s, fdtd::counted_copyAsync(s, s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice,
                                                     s->stream));
             }
-        } else if (s->L > 0) {
+        } else if (s->hP.plain_rows) {
+            CUDA_TRY(s, launch_plain_rows(s->dP, s->hP.plain_rows, ((long long)s->N[0] * s->N[1] + 31) / 32,
+                                          s->interior, s->stream));
+            s->launches++;
+        }
+        if (!s->moving && s->L > 0) {
             // static classification: the listener fits become fixed weights
             CUDA_TRY(s, launch_listener_prep(s->dP, s->precision, cur ^ 1, s->L, s->stream));
             s->launches += 2;
@@ -242,6 +251,11 @@ fdtd_status check_device_errors(fdtd_solver* s) {
     if (dev_error & 1) {
         set_error(s, "listener sample not finite, or a degenerate listener stencil (no cell or rank-deficient MLS)");
         return FDTD_ERR_NUMERIC;
+    }
+    if (dev_error & fdtd::DEV_ERR_ENGQUIST) {
+        set_error(s, "a solid cell reaches the stencil of an Engquist-Majda boundary cell (the ghost-pressure forms of "
+                     "MAC_Grid.cpp:533-920 are not built): keep bodies and constraints three cells from sides without PML");
+        return FDTD_ERR_UNSUPPORTED;
     }
     if (dev_error & fdtd::FDTD_DEV_ERR_TMA_TIMEOUT) {
         set_error(s, "a tensor copy of the PML-shell kernel did not complete within its bounded wait");
@@ -731,6 +745,7 @@ std::vector<std::pair<void*, size_t>> snap_regions(fdtd_solver* s) {
         }
     for (int b = 0; b < 2; ++b)
         if (P.lapv[b]) r.push_back({P.lapv[b], np * (s->precision == FDTD_PRECISION_FP64 ? 8 : 4)});
+    if (P.eng_buf) r.push_back({P.eng_buf, s->eng.size() * ENG_BUF * 8});
     r.push_back({P.consts, 2 * sizeof(StepConsts)});
     r.push_back({P.dev_error, sizeof(int)});
     return r;
@@ -851,6 +866,15 @@ fdtd_status fdtd_solver_restore(fdtd_solver* s, const void* buffer, int64_t byte
     s->cls_boxes_current = false;  // the flags came from the snapshot, not from hP.boxes
     to_dev_objects(s);
     CUDA_TRY(s, fdtd::counted_copy(s, s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice));
+    if (s->hP.plain_rows) {  // plain rows of the restored flags (none before the first step)
+        const long long words = ((long long)s->N[0] * s->N[1] + 31) / 32;
+        if (s->step_index > 0) {
+            CUDA_TRY(s, launch_plain_rows(s->dP, s->hP.plain_rows, words, s->interior, s->stream));
+        } else {
+            CUDA_TRY(s, cudaMemsetAsync(s->hP.plain_rows, 0, words * 4, s->stream));
+        }
+        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+    }
     return FDTD_OK;
 }
 

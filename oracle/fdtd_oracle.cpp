@@ -545,6 +545,7 @@ struct Oracle {
     int preset;
     bool fullyCoupled = false;  // boundaryHandlingType (ImpulseResponseParser.cpp:547-555)
     int fcIterations = 0;       // BiCGSTAB iterations of the last FULLY_COUPLED solve
+    bool engquistMissingGhost = false;  // an Engquist stencil met a ghost cell without a face record
     double endTime;
     // pressure field (ScalarField, ScalarField.cpp:29-50)
     int N[3];
@@ -601,18 +602,25 @@ struct Oracle {
         return p;
     }
 
-    // MAC_Grid::InsidePML (MAC_Grid.cpp:4027-4062), preset 0
+    // MAC_Grid::InsidePML (MAC_Grid.cpp:4027-4062).  Preset 0: PML on every
+    // side; 1: on the low sides and +y (walls +x, +z); 2: on +z only.
     bool InsidePML(const V3& x) const {
         const double pmlWidth = absorptionWidth + 1E-12;
         for (int d = 0; d < 3; ++d) {
             const double hMin = x[d] - bmin[d];
             const double hMax = bmax[d] - x[d];
-            if (hMin <= pmlWidth) return true;
-            if (hMax <= pmlWidth) return true;
+            if (preset == 0) {
+                if (hMin <= pmlWidth) return true;
+                if (hMax <= pmlWidth) return true;
+            } else if (preset == 1) {
+                if (hMin <= pmlWidth || (d == 1 && hMax <= pmlWidth)) return true;
+            } else if (preset == 2) {
+                if (d == 2 && hMax <= pmlWidth) return true;
+            }
         }
         return false;
     }
-    // MAC_Grid::PML_absorptionCoefficient, quadratic profile (MAC_Grid.cpp:4064-4090).
+    // MAC_Grid::PML_absorptionCoefficient, quadratic profile (MAC_Grid.cpp:4064-4101).
     // pow(x,2) is folded to x*x by the compiler without fast-math; written out here.
     double PML_absorptionCoefficient(const V3& x, int d) const {
         const double w = absorptionWidth;
@@ -621,9 +629,30 @@ struct Oracle {
         const double a2 = w * w;
         const double distMin = w - hMin;
         const double distMax = w - hMax;
-        if (hMin <= w) return absorptionStrength * (distMin * distMin) / a2;
-        if (hMax <= w) return absorptionStrength * (distMax * distMax) / a2;
+        if (preset == 0) {
+            if (hMin <= w) return absorptionStrength * (distMin * distMin) / a2;
+            if (hMax <= w) return absorptionStrength * (distMax * distMax) / a2;
+        } else if (preset == 1) {
+            if (hMin <= w) return absorptionStrength * (distMin * distMin) / a2;
+            if (d == 1 && hMax <= w) return absorptionStrength * (distMax * distMax) / a2;
+        } else if (preset == 2) {
+            if (d != 2 || hMin <= w) return 0.0;
+            if (hMax <= w) return absorptionStrength * (distMax * distMax) / a2;
+        }
         return 0.0;
+    }
+    // ScalarField::boundaryCellNormal (ScalarField.h:202-213): -1 / +1 where the
+    // cell sits `off` cells from the low / high side of an axis
+    void boundaryCellNormal(const int ijk[3], int off, int n[3]) const {
+        for (int d = 0; d < 3; ++d) n[d] = ijk[d] == off ? -1 : (ijk[d] == N[d] - 1 - off ? 1 : 0);
+    }
+    // ScalarField::cellIndex(d0, d1, d2, i0, i1, i2): indices given per permuted axis
+    int cellIndexP(int d0, int d1, int d2, int i0, int i1, int i2) const {
+        int a[3];
+        a[d0] = i0;
+        a[d1] = i1;
+        a[d2] = i2;
+        return cellIndex(a[0], a[1], a[2]);
     }
 
     // ----- objects (FDTD_Objects.cpp) -----
@@ -1181,8 +1210,111 @@ struct Oracle {
         }
     }
 
-    // MAC_Grid::PML_pressureUpdateCollocated (MAC_Grid.cpp:481-946); the
-    // Engquist-Majda branch (:533-920) is unreachable for PML width >= 2.
+    // A neighbour's pressure as the Engquist branch reads it: the ghost
+    // pressure of the face (ci, nb) when nb is a ghost cell, else buf[nb].
+    double engquistValue(int ci, int nb, const std::vector<double>& buf) {
+        if (!isGhost[nb]) return buf[nb];
+        const auto it = ghosts.find(MakeKey(nb, ci));
+        if (it == ghosts.end()) {
+            engquistMissingGhost = true;  // the reference's map lookup throws here
+            return 0.0;
+        }
+        return it->second.pressure;
+    }
+
+    // The Engquist-Majda absorbing update of a non-PML bulk cell one cell from
+    // the domain edge (MAC_Grid.cpp:533-920, ENGQUIST_ORDER 2 for faces; the
+    // edge and corner forms the reference keeps are first order).  nml: the
+    // cell's boundary normal at offset 1.  Writes the extrapolated exterior
+    // pressures into pCurr (zero at the diagonal exterior cell), as the
+    // reference does, and returns pNext before the source term.  No boundary
+    // interface exists in a single solve, so every blend is the ABC value.
+    double engquistUpdate(int ci, const int ijk[3], const int nml[3], const std::vector<double>& pLast,
+                          std::vector<double>& pCurr) {
+        const double lambda = c * k / h;
+        const double lambda2 = lambda * lambda;
+        const int btype = std::abs(nml[0]) + std::abs(nml[1]) + std::abs(nml[2]);
+        const double pC = pCurr[ci], pL = pLast[ci];
+        if (btype == 1) {
+            int di = 0;
+            while (nml[di] == 0) ++di;
+            const int dj = (di + 1) % 3, dk = (di + 2) % 3;
+            const int ii = ijk[di], jj = ijk[dj], kk = ijk[dk];
+            const int ii_n = ii - nml[di], ii_p = ii + nml[di];
+            const int jj_n = std::max(jj - 1, 0), jj_p = std::min(jj + 1, N[dj] - 1);
+            const int kk_n = std::max(kk - 1, 0), kk_p = std::min(kk + 1, N[dk] - 1);
+            const int nIp = cellIndexP(di, dj, dk, ii_p, jj, kk), nIn = cellIndexP(di, dj, dk, ii_n, jj, kk);
+            const int nJp = cellIndexP(di, dj, dk, ii, jj_p, kk), nJn = cellIndexP(di, dj, dk, ii, jj_n, kk);
+            const int nKp = cellIndexP(di, dj, dk, ii, jj, kk_p), nKn = cellIndexP(di, dj, dk, ii, jj, kk_n);
+            const double pl_ii_p = engquistValue(ci, nIp, pLast);
+            const double p_ii_n = engquistValue(ci, nIn, pCurr), pl_ii_n = engquistValue(ci, nIn, pLast);
+            const double p_jj_p = engquistValue(ci, nJp, pCurr);
+            const double p_jj_n = engquistValue(ci, nJn, pCurr);
+            const double p_kk_p = engquistValue(ci, nKp, pCurr);
+            const double p_kk_n = engquistValue(ci, nKn, pCurr);
+            double p1 = (2. / lambda2 + 4. / lambda - 6. - 4. * lambda) * pC - (1. / lambda2 + 2. / lambda) * pL +
+                        pl_ii_p - pl_ii_n + 2. * p_ii_n + (lambda + 1.) * (p_jj_p + p_jj_n + p_kk_p + p_kk_n);
+            p1 *= (lambda2 / (1. + 2. * lambda));
+            double p_ii_p;
+            if (isGhost[nIp]) {
+                p_ii_p = engquistValue(ci, nIp, pCurr);
+            } else {
+                p_ii_p = pl_ii_p + p_ii_n - pl_ii_n - 2. / lambda * (p1 + pL - 2. * pC) +
+                         lambda * (p_jj_p + p_jj_n + p_kk_p + p_kk_n - 4. * pC);
+            }
+            pCurr[nIp] = p_ii_p;
+            return 2.0 * pC - pL + lambda2 * (p_ii_n + p_jj_p + p_jj_n + p_kk_p + p_kk_n + p_ii_p - 6. * pC);
+        }
+        if (btype == 2) {
+            int di = 0;
+            while (nml[di] == 0) ++di;
+            int dj = di + 1;
+            while (nml[dj] == 0) ++dj;
+            const int dk = dj != di + 1 ? (di + 1) % 3 : (di + 2) % 3;
+            const int ii = ijk[di], jj = ijk[dj], kk = ijk[dk];
+            const int ii_n = ii - nml[di], jj_n = jj - nml[dj];
+            const int ii_p = ii + nml[di], jj_p = jj + nml[dj];
+            const int kk_n = std::max(kk - 1, 0), kk_p = std::min(kk + 1, N[dk] - 1);
+            const double p_ii_n = engquistValue(ci, cellIndexP(di, dj, dk, ii_n, jj, kk), pCurr);
+            const double p_jj_n = engquistValue(ci, cellIndexP(di, dj, dk, ii, jj_n, kk), pCurr);
+            const double p_kk_p = engquistValue(ci, cellIndexP(di, dj, dk, ii, jj, kk_p), pCurr);
+            const double p_kk_n = engquistValue(ci, cellIndexP(di, dj, dk, ii, jj, kk_n), pCurr);
+            double p1 = (2. / lambda2 - 6.) * pC + (2.0 * lambda - 1.0) / lambda2 * pL + 2. * p_ii_n + 2. * p_jj_n +
+                        p_kk_p + p_kk_n;
+            p1 *= (lambda2 / (1. + 2. * lambda));
+            const int nIp = cellIndexP(di, dj, dk, ii_p, jj, kk), nJp = cellIndexP(di, dj, dk, ii, jj_p, kk);
+            const double p_ii_p = isGhost[nIp] ? engquistValue(ci, nIp, pCurr) : (pL - p1) / lambda + p_ii_n;
+            const double p_jj_p = isGhost[nJp] ? engquistValue(ci, nJp, pCurr) : (pL - p1) / lambda + p_jj_n;
+            pCurr[nIp] = p_ii_p;
+            pCurr[nJp] = p_jj_p;
+            pCurr[cellIndexP(di, dj, dk, ii_p, jj_p, kk)] = 0.0;
+            return 2.0 * pC - pL + lambda2 * (p_ii_n + p_jj_n + p_kk_p + p_kk_n + p_ii_p + p_jj_p - 6. * pC);
+        }
+        // corner
+        const int ii = ijk[0], jj = ijk[1], kk = ijk[2];
+        const int ii_n = ii - nml[0], jj_n = jj - nml[1], kk_n = kk - nml[2];
+        const int ii_p = ii + nml[0], jj_p = jj + nml[1], kk_p = kk + nml[2];
+        const double p_ii_n = engquistValue(ci, cellIndex(ii_n, jj, kk), pCurr);
+        const double p_jj_n = engquistValue(ci, cellIndex(ii, jj_n, kk), pCurr);
+        const double p_kk_n = engquistValue(ci, cellIndex(ii, jj, kk_n), pCurr);
+        double p1 = (2. / lambda2 - 6.) * pC + (3.0 * lambda - 1.0) / lambda2 * pL + 2. * p_ii_n + 2. * p_jj_n +
+                    2. * p_kk_n;
+        p1 *= (lambda2 / (1. + 3. * lambda));
+        const int nIp = cellIndex(ii_p, jj, kk), nJp = cellIndex(ii, jj_p, kk), nKp = cellIndex(ii, jj, kk_p);
+        const double p_ii_p = isGhost[nIp] ? engquistValue(ci, nIp, pCurr) : (pL - p1) / lambda + p_ii_n;
+        const double p_jj_p = isGhost[nJp] ? engquistValue(ci, nJp, pCurr) : (pL - p1) / lambda + p_jj_n;
+        const double p_kk_p = isGhost[nKp] ? engquistValue(ci, nKp, pCurr) : (pL - p1) / lambda + p_kk_n;
+        pCurr[nIp] = p_ii_p;
+        pCurr[nJp] = p_jj_p;
+        pCurr[nKp] = p_kk_p;
+        pCurr[cellIndex(ii_p, jj_p, kk_p)] = 0.0;
+        return 2.0 * pC - pL + lambda2 * (p_ii_n + p_jj_n + p_kk_n + p_ii_p + p_jj_p + p_kk_p - 6. * pC);
+    }
+
+    // MAC_Grid::PML_pressureUpdateCollocated (MAC_Grid.cpp:481-946).  Non-PML
+    // bulk cells on the domain edge are left as they are; those one cell inside
+    // it take the Engquist-Majda update (live only where a side has no PML:
+    // presets 1 / 2, or a PML under 1.5 cells).
     void PML_pressureUpdateCollocated(double t, std::vector<double>& pLast, std::vector<double>& pCurr,
                                       std::vector<double>& pNext, const std::vector<double>& lapC,
                                       const std::vector<double>& lapL) {
@@ -1207,7 +1339,14 @@ struct Oracle {
         for (int ci = 0; ci < ncell; ++ci) {
             if (!isBulk[ci] || isPML[ci]) continue;
             const V3 pos = cellPosition(ci);
-            if (isCavity[ci] && validHistory[ci]) {
+            int ijk[3], nml[3], nml0[3];
+            cellIJK(ci, ijk);
+            boundaryCellNormal(ijk, 1, nml);
+            boundaryCellNormal(ijk, 0, nml0);
+            if (nml0[0] != 0 || nml0[1] != 0 || nml0[2] != 0) continue;
+            if (nml[0] != 0 || nml[1] != 0 || nml[2] != 0) {
+                pNext[ci] = engquistUpdate(ci, ijk, nml, pLast, pCurr);
+            } else if (isCavity[ci] && validHistory[ci]) {
                 pNext[ci] = pLast[ci] = pCurr[ci];
             } else if (alpha > 0.0 && validHistory[ci]) {
                 pNext[ci] = 2.0 * pCurr[ci] - pLast[ci] - lapL[ci] * kcalp + lapC[ci] * (c2_k2 + kcalp);
@@ -1452,6 +1591,10 @@ struct Oracle {
         PML_velocityUpdateCollocated(pCurr);
         pressureFieldLaplacianGhostCell(pCurr, lapCurr);
         PML_pressureUpdateCollocated(currentTime, pLast, pCurr, pNext, lapCurr, lapLast);
+        if (engquistMissingGhost) {
+            err = "an Engquist cell has a ghost neighbour without a face record";
+            return FDTD_ERR_UNSUPPORTED;
+        }
         pColInd = (pColInd + 1) % 3;
         lapInd = (lapInd + 1) % 2;
         currentTime += k;
@@ -1478,8 +1621,7 @@ struct Oracle {
         preset = s->boundary_condition_preset;
         fullyCoupled = s->boundary_handling == FDTD_BOUNDARY_FULLY_COUPLED;
         endTime = s->end_time;
-        if (preset != 0) { err = "boundary_condition_preset != 0 unsupported"; return FDTD_ERR_UNSUPPORTED; }
-        if (s->pml_width < 1.5) { err = "PML width < 1.5 cells reaches the Engquist branch"; return FDTD_ERR_UNSUPPORTED; }
+        if (preset < 0 || preset > 2) { err = "boundary_condition_preset must be 0, 1 or 2"; return FDTD_ERR_INVALID_ARG; }
         // BoundingBox(cellSize, divisions, center) (BoundingBox.h:89-99), per-axis divisions
         V3 mn, mx;
         for (int d = 0; d < 3; ++d) {

@@ -167,8 +167,8 @@ def test_create_without_device_fails_cleanly(fdtd_lib):
 
 def test_invalid_scenes_are_rejected_before_device_use(fdtd_lib):
     bad = []
-    sc = S.config1(); sc.pml_width = 1.0; bad.append((sc, -7))
-    sc = S.config1(); sc.boundary_condition_preset = 1; bad.append((sc, -7))
+    sc = S.config1(); sc.pml_width = -1.0; bad.append((sc, -1))
+    sc = S.config1(); sc.boundary_condition_preset = 3; bad.append((sc, -1))
     sc = S.config1(); sc.air_viscosity_alpha = -0.1; bad.append((sc, -1))
     sc = S.config1(); sc.boundary_handling = 7; bad.append((sc, -1))
     sc = S.config1(); sc.boundary_handling = S.BOUNDARY_FULLY_COUPLED

@@ -237,3 +237,23 @@ def test_config5_full_size_first_steps(oracle_lib, fdtd_lib, precision, tol):
     assert rel_l2(g.field(S.FIELD_PRESSURE), o.field(S.FIELD_PRESSURE)) <= tol
     # the spheres stay clear of the PML: every step ran its shell beside the classification
     assert g.overlapped_steps() == 6
+
+
+@pytest.mark.parametrize("precision", [S.PRECISION_FP64, S.PRECISION_FP32_COMPENSATED])
+def test_long_host_call_staging(fdtd_lib, precision):
+    """One host call of 700 steps with 16-step graphs (more rows than the pinned
+    staging buffer holds, the classifying step first) gives the rows that the
+    device-output call writes, bit for bit."""
+    import torch
+    sc = S.config1()
+    n = 700
+    a = PML_WaveSolver(sc, precision=precision, graph_steps=16)
+    ya = a.step(n)
+    b = PML_WaveSolver(sc, precision=precision, graph_steps=16)
+    buf = torch.zeros((n, sc.listeners.shape[0]), dtype=torch.float64, device="cuda")
+    b.step_device(n, buf.data_ptr())
+    b.synchronize()
+    assert np.abs(ya).max() > 0
+    assert np.array_equal(ya, buf.cpu().numpy())
+    a.close()
+    b.close()
