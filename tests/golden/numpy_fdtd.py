@@ -7,8 +7,10 @@ MAC_Grid::classifyCells_FAST (MAC_Grid.cpp:3455-3891, spheres only, no
 constraints), PML_pressureUpdateGhostCells in RASTERIZE mode with no boundary
 acceleration (ghost pressure = neighbour pressure, MAC_Grid.cpp:1254-1281),
 PML_velocityUpdateCollocated (:461-479), pressureFieldLaplacianGhostCell
-(:187-299), PML_pressureUpdateCollocated (:481-946) and the Gaussian pressure
-source (GaussianPressureSource.cpp:6-30).  Listeners are sampled with the
+(:187-299), PML_pressureUpdateCollocated (:481-946) with its Engquist-Majda
+branch for sides without PML (:533-920; boundary presets of :4027-4101) over
+three rotating pressure buffers, and the Gaussian pressure source
+(GaussianPressureSource.cpp:6-30).  Listeners are sampled with the
 order-1 weighted least squares of MLSModeInterpolator::lookup through
 numpy.linalg.lstsq.
 """
@@ -37,17 +39,28 @@ class NumpyFDTD:
         W = sc.pml_width * h
         S = sc.pml_strength
 
+        preset = int(getattr(sc, "boundary_condition_preset", 0))
+        self.preset = preset
+        # sides that absorb, per axis (low, high): preset 0 all; 1 the low sides
+        # and +y; 2 +z only (MAC_Grid.cpp:4027-4101)
+        sides = {0: [(True, True)] * 3, 1: [(True, False), (True, True), (True, False)],
+                 2: [(False, False), (False, False), (False, True)]}[preset]
+
         def sigma(x, d):
             hmin, hmax = x - mn[d], mx[d] - x
             out = np.zeros_like(x)
-            lo = hmin <= W
-            hi = (~lo) & (hmax <= W)
-            out[lo] = S * ((W - hmin[lo]) ** 2) / (W * W)
-            out[hi] = S * ((W - hmax[hi]) ** 2) / (W * W)
+            lo = (hmin <= W) & sides[d][0]
+            if preset == 2:  # the reference tests the low side first and returns 0 there
+                hi = (hmin > W) & (hmax <= W) & sides[d][1]
+            else:
+                hi = (~(hmin <= W) if preset == 0 else ~lo) & (hmax <= W) & sides[d][1]
+            with np.errstate(invalid="ignore", divide="ignore"):  # W = 0: 0/0 on the outer faces, as the reference
+                out[lo] = S * ((W - hmin[lo]) ** 2) / (W * W)
+                out[hi] = S * ((W - hmax[hi]) ** 2) / (W * W)
             return out
 
         def inside(x, d):
-            return ((x - mn[d]) <= W + 1e-12) | ((mx[d] - x) <= W + 1e-12)
+            return (((x - mn[d]) <= W + 1e-12) & sides[d][0]) | (((mx[d] - x) <= W + 1e-12) & sides[d][1])
 
         k = self.k
         self.pml_c = [inside(self.cpos[d], d) for d in range(3)]
@@ -107,6 +120,18 @@ class NumpyFDTD:
             self.srcs.append((lo, hi, (hi + lo) / 2.0, ws, g.width_time, g.offset_time, C))
         self.p_prev = np.zeros(N)
         self.p_cur = np.zeros(N)
+        self.p_spare = np.zeros(N)  # the third rotating buffer: the next pressure is written into it
+        # boundary normals at offset 0 and 1 (ScalarField::boundaryCellNormal)
+        idx = np.meshgrid(*[np.arange(n) for n in N], indexing="ij")
+
+        def normal(off):
+            return np.stack([np.where(idx[d] == off, -1, np.where(idx[d] == N[d] - 1 - off, 1, 0)) for d in range(3)])
+
+        self.idx = idx
+        self.nml0, self.nml1 = normal(0), normal(1)
+        edge0 = (self.nml0 != 0).any(axis=0)
+        self.eng = self.bulk & ~self.is_pml & ~edge0 & (self.nml1 != 0).any(axis=0)
+        self.edge0 = edge0
         self.pd = [np.zeros(N) for _ in range(3)]
         self.v = [np.zeros([N[e] + (1 if e == d else 0) for e in range(3)]) for d in range(3)]
         self.t = 0.0
@@ -170,8 +195,8 @@ class NumpyFDTD:
         lap = lap * (1.0 / (h * h))
         lap[~self.bulk] = 0.0
         c2k2 = (self.c * k) * (self.c * k)
-        new = self.p_prev.copy()
-        interior = self.bulk & ~self.is_pml
+        new = self.p_spare  # keeps its values where nothing writes (non-PML cells on the edge)
+        interior = self.bulk & ~self.is_pml & ~self.edge0 & ~self.eng
         upd = 2.0 * p - self.p_prev + lap * c2k2
         cav = interior & (surrounded > 1)
         upd = np.where(cav, p, upd)
@@ -189,6 +214,11 @@ class NumpyFDTD:
                 src = src + np.where(inb, val, 0.0)
             upd = upd + src * k
         new[interior] = upd[interior]
+        if self.eng.any():
+            e_new = self._engquist(p, self.p_prev)
+            if self.srcs:
+                e_new = e_new + (src * k)[self.eng]
+            new[self.eng] = e_new
         # PML split pressures
         for d in range(3):
             shp = [1, 1, 1]
@@ -206,9 +236,92 @@ class NumpyFDTD:
         pml_sum = self.pd[0] + self.pd[1] + self.pd[2]
         new[self.is_pml] = pml_sum[self.is_pml]
         new[~self.bulk & ~self.is_pml] = 0.0
-        self.p_prev, self.p_cur = p, new
+        self.p_spare, self.p_prev, self.p_cur = self.p_prev, p, new
         self.t += k
         return self.sample()
+
+    def _engquist(self, pc, pl):
+        """MAC_Grid.cpp:533-920 over every Engquist cell at once: p^{n+1} of the
+        cells; the exterior values (zero on the diagonal) go into pc in place."""
+        N = self.N
+        lam = self.c * self.k / self.h
+        lam2 = lam * lam
+        cells = np.nonzero(self.eng)
+        m = len(cells[0])
+        X = np.stack(cells)                       # (3, m) coordinates
+        nml = self.nml1[:, cells[0], cells[1], cells[2]]
+        btype = np.abs(nml).sum(axis=0)
+        out = np.zeros(m)
+        writes = []
+
+        def at(a, C):
+            return a[C[0], C[1], C[2]]
+
+        for t in (1, 2, 3):
+            sel = np.nonzero(btype == t)[0]
+            if len(sel) == 0:
+                continue
+            n = nml[:, sel]
+            r = np.arange(len(sel))
+            nz = np.abs(n) > 0
+            if t == 1:
+                di = np.argmax(nz, axis=0)
+                dj, dk = (di + 1) % 3, (di + 2) % 3
+            elif t == 2:
+                di = np.argmax(nz, axis=0)
+                dk = np.argmin(nz, axis=0)
+                dj = 3 - di - dk
+            else:
+                di, dj, dk = np.zeros(len(sel), int), np.ones(len(sel), int), np.full(len(sel), 2)
+
+            def shift(axis, amount, clamp=False):
+                C = X[:, sel].copy()
+                C[axis, r] = C[axis, r] + amount
+                if clamp:
+                    C[axis, r] = np.clip(C[axis, r], 0, np.asarray(N)[axis] - 1)
+                return C
+
+            ni, nj, nk = n[di, r], n[dj, r], n[dk, r]
+            C0 = X[:, sel]
+            pC, pL = at(pc, C0), at(pl, C0)
+            if t == 1:
+                Cip = shift(di, ni)
+                pl_ii_p = at(pl, Cip)
+                Cin = shift(di, -ni)
+                p_ii_n, pl_ii_n = at(pc, Cin), at(pl, Cin)
+                p_jj_p, p_jj_n = at(pc, shift(dj, 1, True)), at(pc, shift(dj, -1, True))
+                p_kk_p, p_kk_n = at(pc, shift(dk, 1, True)), at(pc, shift(dk, -1, True))
+                p1 = ((2. / lam2 + 4. / lam - 6. - 4. * lam) * pC - (1. / lam2 + 2. / lam) * pL + pl_ii_p - pl_ii_n
+                      + 2. * p_ii_n + (lam + 1.) * (p_jj_p + p_jj_n + p_kk_p + p_kk_n))
+                p1 = p1 * (lam2 / (1. + 2. * lam))
+                x0 = (pl_ii_p + p_ii_n - pl_ii_n - 2. / lam * (p1 + pL - 2. * pC)
+                      + lam * (p_jj_p + p_jj_n + p_kk_p + p_kk_n - 4. * pC))
+                out[sel] = 2.0 * pC - pL + lam2 * (p_ii_n + p_jj_p + p_jj_n + p_kk_p + p_kk_n + x0 - 6. * pC)
+                writes.append((Cip, x0))
+            elif t == 2:
+                p_ii_n, p_jj_n = at(pc, shift(di, -ni)), at(pc, shift(dj, -nj))
+                p_kk_p, p_kk_n = at(pc, shift(dk, 1, True)), at(pc, shift(dk, -1, True))
+                p1 = (2. / lam2 - 6.) * pC + (2.0 * lam - 1.0) / lam2 * pL + 2. * p_ii_n + 2. * p_jj_n + p_kk_p + p_kk_n
+                p1 = p1 * (lam2 / (1. + 2. * lam))
+                x0 = (pL - p1) / lam + p_ii_n
+                x1 = (pL - p1) / lam + p_jj_n
+                out[sel] = 2.0 * pC - pL + lam2 * (p_ii_n + p_jj_n + p_kk_p + p_kk_n + x0 + x1 - 6. * pC)
+                Cd = shift(di, ni)
+                Cd[dj, r] = Cd[dj, r] + nj
+                writes += [(shift(di, ni), x0), (shift(dj, nj), x1), (Cd, np.zeros(len(sel)))]
+            else:
+                p_ii_n, p_jj_n, p_kk_n = at(pc, shift(0, -ni)), at(pc, shift(1, -nj)), at(pc, shift(2, -nk))
+                p1 = (2. / lam2 - 6.) * pC + (3.0 * lam - 1.0) / lam2 * pL + 2. * p_ii_n + 2. * p_jj_n + 2. * p_kk_n
+                p1 = p1 * (lam2 / (1. + 3. * lam))
+                x0 = (pL - p1) / lam + p_ii_n
+                x1 = (pL - p1) / lam + p_jj_n
+                x2 = (pL - p1) / lam + p_kk_n
+                out[sel] = 2.0 * pC - pL + lam2 * (p_ii_n + p_jj_n + p_kk_n + x0 + x1 + x2 - 6. * pC)
+                Cd = X[:, sel] + n
+                writes += [(shift(0, ni), x0), (shift(1, nj), x1), (shift(2, nk), x2), (Cd, np.zeros(len(sel)))]
+        for C, v in writes:
+            pc[C[0], C[1], C[2]] = v
+        return out
 
     def sample(self):
         if self.listeners is None:

@@ -153,3 +153,26 @@ def test_translating_sphere_dipole_known_answer(oracle_lib):
     # antisymmetric along the acceleration axis, ~zero broadside
     assert np.allclose(y[:, 0], -y[:, 1], atol=0.05 * np.abs(on).max())
     assert np.abs(y[:, 2]).max() < 0.05 * np.abs(on).max()
+
+
+@pytest.mark.parametrize("preset,pml", [(1, 4.0), (2, 4.0), (0, 1.0), (0, 0.0)])
+def test_oracle_engquist_matches_numpy_restatement(oracle_lib, preset, pml):
+    """Sides without PML (wall presets, thin PML): the Engquist-Majda cells, the
+    exterior values written into the current buffer and the untouched edge
+    cells of three rotating buffers, against the numpy restatement."""
+    from tests.golden.numpy_fdtd import NumpyFDTD
+    h = 0.005
+    sc = S.Scene(cell_size=h, divisions=(22, 20, 24), time_step=S.reference_time_step(h), pml_width=pml, steps=90)
+    sc.boundary_condition_preset = preset
+    sc.objects.append(S.RigidObject(S.SHAPE_SPHERE, (0.004, -0.003, 0.0), (0.012, 0, 0)))
+    sc.sources.append(S.GaussianSource((0.02, 0.015, 0.025), 5e-5))
+    sc.listeners = np.array([[-0.02, 0.02, -0.02], [0.0475, 0.01, 0.0], [0.01, -0.01, 0.0525]])
+    o = oracle_lib.OracleSolver(sc)
+    npf = NumpyFDTD(sc)
+    assert npf.eng.any()
+    yo = o.step(sc.steps)
+    yn = np.array([npf.step() for _ in range(sc.steps)])
+    assert np.abs(yo).max() > 0
+    assert rel_l2(yo, yn) < 1e-11, rel_l2(yo, yn)
+    assert rel_l2(o.field(S.FIELD_PRESSURE), npf.p_cur.reshape(-1)) < 1e-11
+    assert rel_l2(o.field(S.FIELD_PRESSURE_PREV), npf.p_prev.reshape(-1)) < 1e-11
