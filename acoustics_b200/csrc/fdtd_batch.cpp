@@ -379,8 +379,6 @@ fdtd_status fdtd_batch_add_snapshot(fdtd_batch* b, const fdtd_scene_desc* scene,
     st = fdtd_solver_restore(s, snapshot, bytes);
     if (st != FDTD_OK) return fail(st, fdtd_solver_last_error(s));
     if (s->step_index != steps_done) return fail(FDTD_ERR_INVALID_ARG, "snapshot step differs from steps_done");
-    st = rebuild_listener_plans(s);
-    if (st != FDTD_OK) return fail(st, fdtd_solver_last_error(s));
     Member mb;
     mb.s = s;
     mb.total = steps_total;

@@ -191,8 +191,11 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
     }
 }
 
+#ifndef FDTD_INTERIOR_MINB
+#define FDTD_INTERIOR_MINB 1
+#endif
 template <typename T, int XB, bool VISC = false>
-__global__ void __launch_bounds__(256) k_interior(const KArgs<T> A, Box3 box) {
+__global__ void __launch_bounds__(256, FDTD_INTERIOR_MINB) k_interior(const KArgs<T> A, Box3 box) {
     interior_tile<T, XB, VISC>(A, box, blockIdx.x, blockIdx.y);
 }
 

@@ -169,12 +169,15 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         }
     }
     // the region-split path advances the step constants inside its shell kernel;
-    // the prologue then only runs to re-zero solid cells inside the PML
+    // the prologue then only runs to re-zero solid cells inside the PML, or to
+    // advance the constants of a grid without PML cells
     RegionLaunch R = s->region;
     if (shell_ahead) R.skip |= 2;
+    const bool no_shell = R.shell.block_first[R.shell.n] == 0;
+    const int advance = (!fused || no_shell) ? 1 : 0;
     if (s->precision == FDTD_PRECISION_FP64) {
-        if (!fused || s->n_solid_pml > 0) {
-            CUDA_TRY(s, launch_prologue_fp64(s->dP, cur, fused ? 0 : 1, s->n_solid_pml, s->stream));
+        if (advance || s->n_solid_pml > 0) {
+            CUDA_TRY(s, launch_prologue_fp64(s->dP, cur, advance, s->n_solid_pml, s->stream));
             s->launches++;
         }
         int l = 0;
@@ -185,8 +188,8 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         }
         s->launches += l;
     } else {
-        if (!fused || s->n_solid_pml > 0) {
-            CUDA_TRY(s, launch_prologue_fp32(s->dP, cur, fused ? 0 : 1, s->n_solid_pml, s->stream));
+        if (advance || s->n_solid_pml > 0) {
+            CUDA_TRY(s, launch_prologue_fp32(s->dP, cur, advance, s->n_solid_pml, s->stream));
             s->launches++;
         }
         int l = 0;
@@ -875,6 +878,9 @@ fdtd_status fdtd_solver_restore(fdtd_solver* s, const void* buffer, int64_t byte
         }
         CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     }
+    // the fixed listener weights of the restored classification (a first step
+    // classifies and derives them itself)
+    if (s->step_index > 0) return rebuild_listener_plans(s);
     return FDTD_OK;
 }
 
