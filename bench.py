@@ -186,7 +186,8 @@ def profile_run(args):
         return 0
     sc = S.config2(n=args.profile_n)
     kern = S.KERNEL_PHASED if args.precision == "fp64-plain" else S.KERNEL_FUSED
-    g = PML_WaveSolver(sc, precision=prec, kernel=kern, tile_y=args.tile_y, x_chunk=args.x_chunk)
+    g = PML_WaveSolver(sc, precision=prec, kernel=kern, tile_y=args.tile_y, x_chunk=args.x_chunk,
+                       shell_staging=args.profile_staging)
     y = g.step(3 + args.steps)
     g.close()
     print(json.dumps({"profile_run": sc.name, "cells": sc.n_cells, "steps": 3 + args.steps,
@@ -365,6 +366,8 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=15.0)
     ap.add_argument("--profile", action="store_true", help="only run --steps steps of the bench solve (for ncu)")
     ap.add_argument("--profile-n", type=int, default=256, help="grid edge of the --profile solve")
+    ap.add_argument("--profile-staging", type=int, default=0,
+                    help="PML-shell staging of the --profile solve (0 default ring, 2 TMA tensor copies)")
     ap.add_argument("--profile-batch", action="store_true",
                     help="with --profile: step the 64-scene batch (config 3) instead of the 256^3 solve")
     ap.add_argument("--tile-y", type=int, default=0, help="PML-shell x planes per thread (1, 2, 4; 0 default)")

@@ -129,14 +129,14 @@ typedef struct {
 typedef struct {
     double cell_size;              /* <solver cellsize>                                   */
     int32_t divisions[3];          /* <solver_control_policy gridresolution> (per axis)   */
-    int32_t boundary_condition_preset; /* only 0 ("no wall") is on this path            */
+    int32_t boundary_condition_preset; /* 0 PML on every side; 1 walls +x, +z; 2 PML on +z only (MAC_Grid.cpp:4027-4101) */
     double domain_center[3];
     double sound_speed;
     double density;
     double time_step;              /* 1 / timestepfrequency                               */
     double pml_width;              /* cells                                               */
     double pml_strength;
-    double air_viscosity_alpha;    /* 0 on this path                                      */
+    double air_viscosity_alpha;    /* MAC_Grid.cpp:926-930; 0: no viscosity              */
     double start_time;
     double end_time;               /* <= 0: no end                                         */
     int32_t n_objects;
