@@ -689,8 +689,6 @@ static void carve_arena(fdtd_solver* s, const fdtd_scene_desc* sc, const fdtd_op
     cv.add((void**)&s->dP, sizeof(SolveParams));
     cv.add((void**)&P.cls, n);
     cv.add((void**)&P.gobj, n);
-    // static scenes: rows of the non-PML box with plain cells only (the interior skips their flags)
-    if (!s->moving) cv.add((void**)&P.plain_rows, ((size_t)N[0] * N[1] + 31) / 32 * 4);
     if (!s->eng.empty()) {
         cv.add((void**)&P.eng, s->eng.size() * sizeof(EngCell));
         cv.add((void**)&P.eng_buf, s->eng.size() * ENG_BUF * 8);
@@ -1137,8 +1135,6 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     // initFieldRasterized: every cell bulk with valid history (MAC_Grid.cpp:2459-2470, :4170-4180)
     CUDA_TRY(s, cudaMemsetAsync(P.cls, CLS_BULK | CLS_VALID, np, s->stream));
     if (P.eng_buf) CUDA_TRY(s, cudaMemsetAsync(P.eng_buf, 0, s->eng.size() * ENG_BUF * 8, s->stream));
-    if (P.plain_rows)  // no row is known plain until the first step's classification
-        CUDA_TRY(s, cudaMemsetAsync(P.plain_rows, 0, ((size_t)s->N[0] * s->N[1] + 31) / 32 * 4, s->stream));
     CUDA_TRY(s, cudaMemsetAsync(P.gobj, GOBJ_NONE, np, s->stream));
     CUDA_TRY(s, cudaMemsetAsync(P.consts, 0, 2 * sizeof(StepConsts), s->stream));
     CUDA_TRY(s, cudaMemsetAsync(P.dev_error, 0, sizeof(int), s->stream));

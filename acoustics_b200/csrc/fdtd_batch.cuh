@@ -30,7 +30,7 @@ namespace fdtd {
 // arguments are read through references into its descriptor in global memory
 // (L1-resident after the first warp), so a CTA starts without a barrier.
 template <typename T, int XB>
-__global__ void __launch_bounds__(256, FDTD_INTERIOR_MINB) k_batch_interior(const BatchDesc<T>* __restrict__ D,
+__global__ void __launch_bounds__(256) k_batch_interior(const BatchDesc<T>* __restrict__ D,
                                                         const BatchTile* __restrict__ tiles) {
     const BatchTile tile = tiles[blockIdx.x];
     const BatchDesc<T>& d = D[tile.m];
@@ -49,7 +49,7 @@ __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_batch_shel
 
 // Shell tiles of members that keep the reduced PML state (FP32 only).
 template <typename T>
-__global__ void FDTD_SHELL_RED_BOUNDS k_batch_shell_red(const BatchDesc<T>* __restrict__ D,
+__global__ void __launch_bounds__(256, FDTD_SHELL_RED_MINB) k_batch_shell_red(const BatchDesc<T>* __restrict__ D,
                                                                       const BatchTile* __restrict__ tiles) {
     static_assert(sizeof(T) == 4, "the reduced PML state is an FP32 path");
     const BatchTile tile = tiles[blockIdx.x];

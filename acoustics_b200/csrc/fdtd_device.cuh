@@ -163,7 +163,6 @@ struct KArgs {
     T* pn;                        // p^{n+1} (FP64: also p^{n-1} in place)
     float* dinc;                  // FP32 increment
     const uint8_t* cls;
-    const uint32_t* plain_rows;   // see SolveParams::plain_rows (null: read every classification byte)
     T* pd[3];
     const T* vo[3];
     T* vn[3];
@@ -285,8 +284,6 @@ struct SolveParams {
     double* eng_buf;              // [eng_n][ENG_BUF]
     int eng_n;
     double eng_lambda;            // c k / h
-    uint32_t* plain_rows;         // static scenes: bit x*N1+y set when every cell of row (x, y) in the
-                                  // non-PML z range is plain bulk (no solid, no solid neighbour); null otherwise
     void* p[2];
     float* dinc;
     void* pd[3];
@@ -361,7 +358,6 @@ inline KArgs<double> make_kargs<double>(SolveParams* dP, const SolveParams& P, i
     A.pn = (double*)P.p[cur ^ 1];
     A.dinc = P.dinc;
     A.cls = P.cls;
-    A.plain_rows = P.plain_rows;
     for (int d = 0; d < 3; ++d) {
         A.pd[d] = (double*)P.pd[d];
         A.vo[d] = (const double*)P.v[cur][d];
@@ -392,7 +388,6 @@ inline KArgs<float> make_kargs<float>(SolveParams* dP, const SolveParams& P, int
     A.pn = (float*)P.p[cur ^ 1];
     A.dinc = P.dinc;
     A.cls = P.cls;
-    A.plain_rows = P.plain_rows;
     for (int d = 0; d < 3; ++d) {
         A.pd[d] = (float*)P.pd[d];
         A.vo[d] = (const float*)P.v[cur][d];

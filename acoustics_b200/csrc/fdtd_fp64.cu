@@ -696,37 +696,6 @@ __global__ void k_cls_history(const SolveParams* __restrict__ Pp, long long n, i
     }
 }
 
-// Plain rows of a static classification: one warp per row (x, y) of the non-PML
-// box, eight flag bytes a lane over its z range; the bit is set when every cell
-// is bulk without a solid neighbour (the interior kernel then reads no flag
-// byte of the row).  The bitmap was cleared before.
-__global__ void k_plain_rows(const SolveParams* __restrict__ Pp, Box3 b) {
-    const SolveParams& P = *Pp;
-    const int lane = threadIdx.x & 31;
-    const int ny = b.hi[1] - b.lo[1];
-    const long long rows = (long long)(b.hi[0] - b.lo[0]) * ny;
-    for (long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; w < rows;
-         w += ((long long)gridDim.x * blockDim.x) >> 5) {
-        const int x = b.lo[0] + (int)(w / ny), y = b.lo[1] + (int)(w % ny);
-        const uint8_t* row = P.cls + (long long)x * P.SX + (long long)y * P.SY;
-        bool plain = true;
-        for (int z = b.lo[2] + lane; z < b.hi[2]; z += 32) plain = plain && (row[z] & (CLS_BULK | CLS_MASK)) == CLS_BULK;
-        if (__all_sync(0xffffffffu, plain) && lane == 0) {
-            const long long bit = (long long)x * P.N[1] + y;
-            atomicOr(&P.plain_rows[bit >> 5], 1u << (bit & 31));
-        }
-    }
-}
-
-cudaError_t launch_plain_rows(const SolveParams* dP, uint32_t* bitmap, long long words, const Box3& b,
-                              cudaStream_t s) {
-    cudaError_t e = cudaMemsetAsync(bitmap, 0, words * 4, s);
-    const long long rows = (long long)(b.hi[0] - b.lo[0]) * (b.hi[1] - b.lo[1]);
-    if (e != cudaSuccess || rows <= 0 || b.hi[2] <= b.lo[2]) return e;
-    k_plain_rows<<<(unsigned)std::min<long long>((rows + 7) / 8, 148 * 32), 256, 0, s>>>(dP, b);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_cls_history(const SolveParams* dP, long long ncell, int* count, int* list, int cap, cudaStream_t s) {
     k_cls_history<<<grid_for(ncell, 256), 256, 0, s>>>(dP, ncell, count, list, cap);
     return cudaGetLastError();

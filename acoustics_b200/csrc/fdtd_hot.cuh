@@ -126,11 +126,7 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
             } else {
                 prev[i] = ldv(pn + i * sx);
             }
-            // a row known plain reads no flag byte (the viscous form needs the valid bit)
-            const long long rb = (long long)(x0 + i) * A.N1 + yc;
-            const bool plain = !VISC && A.plain_rows && ((A.plain_rows[rb >> 5] >> (rb & 31)) & 1u);
-            if (plain) code[i] = V == 4 ? 0x80808080u : 0x8080u;
-            else if constexpr (V == 4) code[i] = *reinterpret_cast<const uint32_t*>(cls + i * sx);
+            if constexpr (V == 4) code[i] = *reinterpret_cast<const uint32_t*>(cls + i * sx);
             else code[i] = *reinterpret_cast<const uint16_t*>(cls + i * sx);
             if constexpr (VISC) lapl[i] = ldv(A.lapl + off + i * sx);
             zme[i] = zm_mem ? pc[i * sx - 1] : (T)0;
@@ -191,11 +187,8 @@ __device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box
     }
 }
 
-#ifndef FDTD_INTERIOR_MINB
-#define FDTD_INTERIOR_MINB 1
-#endif
 template <typename T, int XB, bool VISC = false>
-__global__ void __launch_bounds__(256, FDTD_INTERIOR_MINB) k_interior(const KArgs<T> A, Box3 box) {
+__global__ void __launch_bounds__(256) k_interior(const KArgs<T> A, Box3 box) {
     interior_tile<T, XB, VISC>(A, box, blockIdx.x, blockIdx.y);
 }
 

@@ -38,9 +38,6 @@ cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int
 // (3 launches; the last only when some box has cells)
 cudaError_t launch_classify(const SolveParams* dP, const int N[3], const ClsBoxes& B, bool collect_fresh,
                             cudaStream_t s);
-// plain-row bitmap of a static classification over the non-PML box b (cleared first)
-cudaError_t launch_plain_rows(const SolveParams* dP, uint32_t* bitmap, long long words, const Box3& b,
-                              cudaStream_t s);
 cudaError_t launch_cls_history(const SolveParams* dP, long long ncell, int* count, int* list, int cap, cudaStream_t s);
 cudaError_t launch_fresh_cells(const SolveParams* dP, int precision, int cur, long long ncell, int* d_status,
                                cudaStream_t s);

@@ -410,13 +410,8 @@ __device__ __forceinline__ void shell_tile_red(const KArgs<float>& A, const Shel
 }
 
 // (a template so that every translation unit may include it; instantiated for float only)
-#ifdef FDTD_SHELL_RED_MAXREG
-#define FDTD_SHELL_RED_BOUNDS __maxnreg__(FDTD_SHELL_RED_MAXREG)
-#else
-#define FDTD_SHELL_RED_BOUNDS __launch_bounds__(256, FDTD_SHELL_RED_MINB)
-#endif
 template <typename T>
-__global__ void FDTD_SHELL_RED_BOUNDS k_pml_shell_red(const KArgs<T> A, const ShellBoxes B) {
+__global__ void __launch_bounds__(256, FDTD_SHELL_RED_MINB) k_pml_shell_red(const KArgs<T> A, const ShellBoxes B) {
     static_assert(sizeof(T) == 4, "the reduced PML state is an FP32 path");
     if (A.advance && blockIdx.x == 0 && threadIdx.x == 0 && threadIdx.y == 0) advance_consts(*A.P, A.cur);
     int b, tu, tx;

@@ -156,10 +156,6 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
                 CUDA_TRY(s, fdtd::counted_copyAsync(s, s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice,
                                                     s->stream));
             }
-        } else if (s->hP.plain_rows) {
-            CUDA_TRY(s, launch_plain_rows(s->dP, s->hP.plain_rows, ((long long)s->N[0] * s->N[1] + 31) / 32,
-                                          s->interior, s->stream));
-            s->launches++;
         }
         if (!s->moving && s->L > 0) {
             // static classification: the listener fits become fixed weights
@@ -869,15 +865,6 @@ fdtd_status fdtd_solver_restore(fdtd_solver* s, const void* buffer, int64_t byte
     s->cls_boxes_current = false;  // the flags came from the snapshot, not from hP.boxes
     to_dev_objects(s);
     CUDA_TRY(s, fdtd::counted_copy(s, s->dP, &s->hP, sizeof(SolveParams), cudaMemcpyHostToDevice));
-    if (s->hP.plain_rows) {  // plain rows of the restored flags (none before the first step)
-        const long long words = ((long long)s->N[0] * s->N[1] + 31) / 32;
-        if (s->step_index > 0) {
-            CUDA_TRY(s, launch_plain_rows(s->dP, s->hP.plain_rows, words, s->interior, s->stream));
-        } else {
-            CUDA_TRY(s, cudaMemsetAsync(s->hP.plain_rows, 0, words * 4, s->stream));
-        }
-        CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-    }
     // the fixed listener weights of the restored classification (a first step
     // classifies and derives them itself)
     if (s->step_index > 0) return rebuild_listener_plans(s);
