@@ -448,55 +448,199 @@ __device__ __forceinline__ void fresh_cell(const SolveParams& P, int cur, long l
     }
 }
 
-// Fresh cells of the classification just made, from the list the ghost sweep
-// filled; a list that overflowed is replaced by a sweep over every cell.  Each
-// fresh value reads only cells with a valid history, never another fresh cell,
-// so the order does not matter.  On the list, the two values of a cell (p^n
-// and p^{n-1}) are made by a pair of lanes: unit 2 f + w, w = 0 for p^n.
+// The fresh value of one cell computed by a half-warp: lane q < 8 of the half
+// holds the MLS row of stencil cell q (bits of q = x, y, z of the 2x2x2
+// enclosing cells; a cell repeated at the domain edge keeps its first lane), so
+// the eight rows, their weights and the Householder updates run in parallel.
+// Every reduction adds the lanes' terms in row order from zero, and zero rows
+// add nothing, so the result is bit-equal to householder_ls4_rows8 over the
+// same rows.  All 32 lanes must call it with the same cell (both halves take
+// the same branches: they share the image point and the stencil flags).
 template <typename T>
-__global__ void k_fresh_cells(const SolveParams* __restrict__ Pp, int cur, long long n, int* status) {
+__device__ __noinline__ double fresh_value_half(const SolveParams& P, const T* __restrict__ pa,
+                                                const T* __restrict__ pb, bool diff, long long c, double t,
+                                                int* status) {
+    const int q = threadIdx.x & 15;
+    const int base = threadIdx.x & 16;  // first lane of this half
+    auto sum_rows = [&](double x, int from) {
+        double acc = 0.0;
+        for (int i = from; i < 8; ++i) acc += __shfl_sync(0xffffffffu, x, base + i);
+        return acc;
+    };
+    auto from_row = [&](double x, int i) { return __shfl_sync(0xffffffffu, x, base + i); };
+    int i, j, k;
+    cell_ijk(P, c, i, j, k);
+    const double cp[3] = {P.cpos[0][i], P.cpos[1][j], P.cpos[2][k]};
+    double distance = DBL_MAX;
+    const int oid = lowest_object(P, cp, &distance);
+    if (oid < 0 || distance < DISTANCE_TOLERANCE) {
+        *status = 2;
+        return 0.0;
+    }
+    const DevObject& o = P.obj[oid];
+    double image[3], bp[3], nrm[3], travelled;
+    reflect_against_boundary(o, cp, image, bp, nrm, travelled);
+    // enclosing cells of the image point (enclosing_neighbours)
+    int a0[3], a1[3];
+    for (int d = 0; d < 3; ++d) {
+        double df = image[d] - P.bmin[d];
+        df -= P.h / 2.0;
+        int i0 = (int)(df / P.h);
+        i0 = i0 < 0 ? 0 : i0;
+        i0 = i0 > P.N[d] - 1 ? P.N[d] - 1 : i0;
+        a0[d] = i0;
+        a1[d] = (df < 0.0 ? 0 : (i0 + 1 < P.N[d] - 1 ? i0 + 1 : P.N[d] - 1));
+    }
+    const int bx = (q >> 2) & 1, by = (q >> 1) & 1, bz = q & 1;
+    const bool in_stencil = q < 8 && !(bx && a1[0] == a0[0]) && !(by && a1[1] == a0[1]) && !(bz && a1[2] == a0[2]);
+    const int ni = bx ? a1[0] : a0[0], nj = by ? a1[1] : a0[1], nn = bz ? a1[2] : a0[2];
+    double Ar[4] = {0.0, 0.0, 0.0, 0.0}, br = 0.0, vq = 0.0, pq[3] = {0.0, 0.0, 0.0};
+    bool valid = false;
+    if (in_stencil) {
+        const long long n = cidx(P, ni, nj, nn);
+        valid = (P.cls[n] & CLS_VALID) != 0;
+        vq = diff ? (double)pa[n] - (double)pb[n] : (double)pa[n];
+        pq[0] = P.cpos[0][ni];
+        pq[1] = P.cpos[1][nj];
+        pq[2] = P.cpos[2][nn];
+        if (valid) mls_row(image, pq, vq, Ar, br);
+    }
+    const unsigned kept = (__ballot_sync(0xffffffffu, valid) >> base) & 0xffu;
+    const int nk = __popc(kept);
+    if (nk < 4) {
+        if (nk != 0) {
+            // the valid stencil cell nearest the image point (first in row order on ties)
+            double md = DBL_MAX;
+            int mid = -1;
+            for (int r = 0; r < 8; ++r) {
+                const double dx = image[0] - from_row(pq[0], r), dy = image[1] - from_row(pq[1], r),
+                             dz = image[2] - from_row(pq[2], r);
+                const double d2 = dx * dx + dy * dy + dz * dz;
+                if (((kept >> r) & 1u) && d2 < md) {
+                    md = d2;
+                    mid = r;
+                }
+            }
+            double vm = 0.0;
+            for (int r = 0; r < 8; ++r) {
+                const double v = from_row(vq, r);
+                if (r == mid) vm = v;
+            }
+            return vm;
+        }
+        const int idx[3] = {i, j, k};
+        const long long strides[3] = {P.SX, P.SY, 1};
+        for (int d = 0; d < 3; ++d)
+            for (int s = 1; s >= -1; s -= 2) {
+                if (idx[d] + s < 0 || idx[d] + s >= P.N[d]) continue;
+                const long long n = c + s * strides[d];
+                if (P.cls[n] & CLS_BULK) return diff ? (double)pa[n] - (double)pb[n] : (double)pa[n];
+            }
+        return 0.0;
+    }
+    // Householder QR of the 8 x 4 block, one row per lane (householder_ls4_rows8)
+    double R[4][4];
+    bool ok = true;
+#pragma unroll
+    for (int jc = 0; jc < 4; ++jc) {
+        const double s = sum_rows(q >= jc && q < 8 ? Ar[jc] * Ar[jc] : 0.0, jc);
+        const double norm = sqrt(s);
+        if (!(norm > 0.0)) {
+            ok = false;
+            break;
+        }
+        const double x0 = from_row(Ar[jc], jc);
+        const double alpha = x0 > 0.0 ? -norm : norm;
+        if (q == jc) Ar[jc] = x0 - alpha;
+        const double vnorm2 = sum_rows(q >= jc && q < 8 ? Ar[jc] * Ar[jc] : 0.0, jc);
+#pragma unroll
+        for (int cc = jc + 1; cc < 4; ++cc) {
+            const double dot = sum_rows(q >= jc && q < 8 ? Ar[jc] * Ar[cc] : 0.0, jc);
+            const double f = 2.0 * dot / vnorm2;
+            if (q >= jc && q < 8) Ar[cc] -= f * Ar[jc];
+        }
+        {
+            const double dot = sum_rows(q >= jc && q < 8 ? Ar[jc] * br : 0.0, jc);
+            const double f = 2.0 * dot / vnorm2;
+            if (q >= jc && q < 8) br -= f * Ar[jc];
+        }
+        R[jc][jc] = alpha;
+#pragma unroll
+        for (int cc = jc + 1; cc < 4; ++cc) R[jc][cc] = from_row(Ar[cc], jc);
+    }
+    double c0 = 0.0;
+    if (ok) {
+        const double rmax = dmax(dmax(fabs(R[0][0]), fabs(R[1][1])), dmax(fabs(R[2][2]), fabs(R[3][3])));
+#pragma unroll
+        for (int jc = 0; jc < 4; ++jc)
+            if (fabs(R[jc][jc]) <= (double)(nk > 4 ? nk : 4) * 2.220446049250313e-16 * rmax) ok = false;
+    }
+    if (ok) {
+        double bq[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) bq[r] = from_row(br, r);
+        double x[4];
+#pragma unroll
+        for (int jc = 3; jc >= 0; --jc) {
+            double s2 = bq[jc];
+#pragma unroll
+            for (int cc = jc + 1; cc < 4; ++cc) s2 -= R[jc][cc] * x[cc];
+            x[jc] = s2 / R[jc][jc];
+        }
+        c0 = x[0];
+    }
+    double acc[3];
+    boundary_accel(o, bp, t, acc);
+    const double an = acc[0] * nrm[0] + acc[1] * nrm[1] + acc[2] * nrm[2];
+    return c0 + P.rho * an * fabs(travelled);
+}
+
+// Fresh cells of the classification just made, from the list the ghost sweep
+// filled, one warp per cell: the half-warp 16 w + q makes the value of buffer w
+// (p^n for w = 0, p^{n-1} for w = 1).  A list that overflowed is replaced by a
+// sweep over every cell, a thread per cell.  Each fresh value reads only cells
+// with a valid history, never another fresh cell, so the order does not matter.
+template <typename T>
+__global__ void __launch_bounds__(128) k_fresh_cells(const SolveParams* __restrict__ Pp, int cur, long long n,
+                                                     int* status) {
     const SolveParams& P = *Pp;
     const double t = P.consts[cur].t;
     const int count = *P.fresh_count;
     int st = 0;
-    if (count <= P.fresh_cap) {
-        const int units = 2 * count;
-        const int lane = threadIdx.x & 31;
-        // whole warps step together, so the pair exchange below sees both lanes
-        for (int base = blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < units; base += gridDim.x * blockDim.x) {
-            const int u = base + lane;
-            const bool act = u < units;
-            const int w = u & 1;
-            const long long c = act ? P.fresh_list[u >> 1] : 0;
-            double v = 0.0;
-            if (act) {
-                if (sizeof(T) == 8) {
-                    const double* buf = (const double*)P.p[cur ^ w];
-                    v = fresh_value<double>(P, buf, buf, false, c, t, &st);
-                } else {
-                    const float* pc = (const float*)P.p[cur];
-                    v = w ? fresh_value<float>(P, pc, P.dinc, true, c, t, &st)
-                          : fresh_value<float>(P, pc, pc, false, c, t, &st);
-                }
-            }
-            const double other = __shfl_xor_sync(0xffffffffu, v, 1);
-            if (!act) continue;
-            if (sizeof(T) == 8) {
-                ((double*)P.p[cur ^ w])[c] = v;
-            } else if (w == 0) {
-                // FP32 keeps p^n and the increment; p^{n-1} = p^n - d
-                ((float*)P.p[cur])[c] = (float)v;
-                P.dinc[c] = (float)(v - other);
-            }
-        }
-    } else {
-        for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+    if (count > P.fresh_cap) {
+        for (long long q = blockIdx.x * (long long)blockDim.x + threadIdx.x; q < n;
+             q += (long long)gridDim.x * blockDim.x) {
             int i, j, k;
             dense_ijk(P, q, i, j, k);
             const long long c = cidx(P, i, j, k);
             const uint8_t code = P.cls[c];
             if (!(code & CLS_BULK) || (code & CLS_VALID)) continue;
             fresh_cell<T>(P, cur, c, t, &st);
+        }
+        if (st) atomicMax(status, st);
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const int w = lane >> 4;
+    for (int f = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; f < count; f += (gridDim.x * blockDim.x) >> 5) {
+        const long long c = P.fresh_list[f];
+        double v;
+        if (sizeof(T) == 8) {
+            const double* buf = (const double*)P.p[cur ^ w];
+            v = fresh_value_half<double>(P, buf, buf, false, c, t, &st);
+        } else {
+            const float* pc = (const float*)P.p[cur];
+            v = w ? fresh_value_half<float>(P, pc, P.dinc, true, c, t, &st)
+                  : fresh_value_half<float>(P, pc, pc, false, c, t, &st);
+        }
+        const double other = __shfl_xor_sync(0xffffffffu, v, 16);
+        if ((lane & 15) != 0) continue;
+        if (sizeof(T) == 8) {
+            ((double*)P.p[cur ^ w])[c] = v;
+        } else if (w == 0) {
+            // FP32 keeps p^n and the increment; p^{n-1} = p^n - d
+            ((float*)P.p[cur])[c] = (float)v;
+            P.dinc[c] = (float)(v - other);
         }
     }
     if (st) atomicMax(status, st);
@@ -703,8 +847,8 @@ cudaError_t launch_cls_history(const SolveParams* dP, long long ncell, int* coun
 
 cudaError_t launch_fresh_cells(const SolveParams* dP, int precision, int cur, long long ncell, int* d_status,
                                cudaStream_t s) {
-    // sized for the list (a few thousand cells a step); the sweep fallback strides
-    const int grid = 2 * 148;
+    // the list, a warp per cell (a few thousand cells a step at most)
+    const int grid = 4 * 148;
     if (precision == 0) k_fresh_cells<double><<<grid, 128, 0, s>>>(dP, cur, ncell, d_status);
     else k_fresh_cells<float><<<grid, 128, 0, s>>>(dP, cur, ncell, d_status);
     return cudaGetLastError();

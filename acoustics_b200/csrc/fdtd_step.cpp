@@ -85,9 +85,38 @@ StepStreams step_streams(const fdtd_solver* s) {
 // Listener rows of static scenes run on stream4 beside the next step.  Not for
 // moving bodies or solid cells inside the PML: the next step's classification /
 // prologue rewrites cells of the pressure they read.
-// (not with Engquist cells: the step after writes the exterior cells of the pressure they read)
-bool listeners_aside(const fdtd_solver* s) {
-    return s->stream4 && !s->moving && s->n_solid_pml == 0 && s->eng.empty();
+// True when no listener stencil (the cells its MLS may read, two cells around
+// them) meets a classification box: the classification of the next step writes
+// flags and pressures only inside its boxes, its fresh cells lie in the boxes of
+// this step.
+bool listeners_clear_of(const fdtd_solver* s, const ClsBoxes& B) {
+    for (int l = 0; l < s->L; ++l) {
+        int lo[3], hi[3];
+        for (int d = 0; d < 3; ++d) {
+            const double diff = (s->listeners[3 * (size_t)l + d] - s->bmin[d]) - s->h / 2.0;
+            const int a0 = std::min(std::max((int)(diff / s->h), 0), s->N[d] - 1);
+            lo[d] = a0 - 2;
+            hi[d] = a0 + 4;
+        }
+        for (int b = 0; b < B.n; ++b) {
+            if (B.first[b + 1] == B.first[b]) continue;
+            bool meet = true;
+            for (int d = 0; d < 3; ++d) meet = meet && lo[d] < B.lo[b][d] + B.rg[b][d] && B.lo[b][d] < hi[d];
+            if (meet) return false;
+        }
+    }
+    return true;
+}
+
+// The listener rows of a step run on stream4 beside the next step: static
+// scenes after their first step, moving scenes while every listener stencil is
+// clear of this step's classification boxes (the next step waits for them if
+// its own boxes reach a stencil).  Not with Engquist cells (the step after
+// writes the exterior cells of the pressure they read) or solids in the PML
+// (re-zeroed at the start of every step).
+bool listeners_aside(const fdtd_solver* s, bool classify) {
+    if (!s->stream4 || s->n_solid_pml != 0 || !s->eng.empty()) return false;
+    return s->moving ? listeners_clear_of(s, s->hP.boxes) : !classify;
 }
 
 // Make the solver stream wait for every listener launch on stream4.
@@ -114,6 +143,12 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
         // MAC_Grid::classifyCells_FAST + InterpolateFreshPressureCell (PML_WaveSolver.cpp:807-812)
         const ClsBoxes prev = s->hP.boxes;
         classification_boxes(s, s->hP.boxes);
+        // the rows of the step before still being read beside this step: this
+        // step's classification must not write under a listener stencil first
+        if (s->lis_pending[cur ^ 1] && !listeners_clear_of(s, s->hP.boxes)) {
+            CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_lis[cur ^ 1], 0));
+            s->lis_pending[cur ^ 1] = false;
+        }
         if (s->moving && s->region.red && !boxes_clear_of_shell(s, s->hP.boxes)) {
             // past the end time the bodies were checked for: the reduced PML state no longer holds
             set_error(s, "a moving body came within two cells of the PML of a reduced-state solve (past its end_time)");
@@ -195,7 +230,7 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
     if (shell_ahead) CUDA_TRY(s, cudaStreamWaitEvent(s->stream, s->ev_sdone, 0));
     if (s->L > 0 && dev_row) {
         // the phased path keeps p^{n+1} in the same slot as the fused one
-        if (listeners_aside(s) && !classify) {
+        if (listeners_aside(s, classify)) {
             CUDA_TRY(s, cudaEventRecord(s->ev_step, s->stream));
             CUDA_TRY(s, cudaStreamWaitEvent(s->stream4, s->ev_step, 0));
             CUDA_TRY(s, launch_listeners(s->dP, s->precision, cur ^ 1, s->L, dev_row, s->stream4));
@@ -424,7 +459,11 @@ fdtd_status fdtd_solver_time_kernel(fdtd_solver* s, int32_t which, int32_t n_lau
     if (which == 1) R.skip = 2 | 4;
     if (which == 2) R.skip = 1 | 4;
     if (which == 3) R.skip = 1 | 2;
-    CUDA_TRY(s, cudaEventRecord(e0, s->stream));
+    // the launches are captured into a graph and the graph is timed: device time
+    // only, whatever the host's launch rate (a step forks to three streams)
+    fdtd_status jst = join_listeners(s);
+    if (jst != FDTD_OK) return jst;
+    CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
     int c = s->cur;
     for (int i = 0; i < n_launches; ++i) {
         cudaError_t e;
@@ -437,17 +476,37 @@ fdtd_status fdtd_solver_time_kernel(fdtd_solver* s, int32_t which, int32_t n_lau
             e = launch_step_regions_fp32(s->dP, s->hP, R, c, step_streams(s), nullptr);
         }
         if (e != cudaSuccess) {
+            cudaGraph_t g = nullptr;
+            cudaStreamEndCapture(s->stream, &g);
+            if (g) cudaGraphDestroy(g);
             set_error(s, std::string("stencil launch: ") + cudaGetErrorString(e));
             return FDTD_ERR_CUDA;
         }
         if (which != 4) c ^= 1;
     }
-    CUDA_TRY(s, cudaEventRecord(e1, s->stream));
-    CUDA_TRY(s, cudaEventSynchronize(e1));
-    CUDA_TRY(s, cudaEventElapsedTime(elapsed_ms, e0, e1));
+    cudaGraph_t g = nullptr;
+    CUDA_TRY(s, cudaStreamEndCapture(s->stream, &g));
+    cudaGraphExec_t x = nullptr;
+    cudaError_t ge = cudaGraphInstantiate(&x, g, 0);
+    cudaGraphDestroy(g);
+    if (ge != cudaSuccess) {
+        set_error(s, std::string("stencil graph: ") + cudaGetErrorString(ge));
+        return FDTD_ERR_CUDA;
+    }
+    // one untimed replay, one timed: 2 n launches, so the parity comes back
+    ge = cudaGraphLaunch(x, s->stream);
+    if (ge == cudaSuccess) ge = cudaEventRecord(e0, s->stream);
+    if (ge == cudaSuccess) ge = cudaGraphLaunch(x, s->stream);
+    if (ge == cudaSuccess) ge = cudaEventRecord(e1, s->stream);
+    if (ge == cudaSuccess) ge = cudaEventSynchronize(e1);
+    if (ge == cudaSuccess) ge = cudaEventElapsedTime(elapsed_ms, e0, e1);
+    cudaGraphExecDestroy(x);
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
-    s->cur = c;
+    if (ge != cudaSuccess) {
+        set_error(s, std::string("stencil timing: ") + cudaGetErrorString(ge));
+        return FDTD_ERR_CUDA;
+    }
     return FDTD_OK;
 }
 

@@ -368,14 +368,15 @@ int64_t fdtd_solver_overlapped_steps(fdtd_solver* s);
  * words); no counterpart in the reference, whose state lives in host memory. */
 fdtd_status fdtd_solver_transfer_bytes(fdtd_solver* s, int64_t* host_to_device, int64_t* device_to_host);
 
-/* Profiling hook (no counterpart in the reference): launch the dominant step kernel
- * n_launches times back to back on the solver's stream (alternating buffer parity,
- * no prologue or listener work) between two CUDA events and return the elapsed
- * milliseconds.  The solver state is left advanced by those launches; use a solver
- * created for measurement. */
+/* Profiling hook (no counterpart in the reference): the step kernels n_launches
+ * times back to back (alternating buffer parity, no prologue, source or listener
+ * work), captured into a CUDA graph that is replayed once untimed and once
+ * between two CUDA events on the solver stream: device time only, whatever the
+ * host's launch rate.  Returns the elapsed milliseconds of the timed replay.  The
+ * fields are left in an unspecified state; use a solver created for measurement. */
 fdtd_status fdtd_solver_time_stencil(fdtd_solver* s, int32_t n_launches, float* elapsed_ms);
-/* CUDA-event time of n back-to-back launches of one part of the step on the
- * solver stream: which = 0 the step kernels (as fdtd_solver_time_stencil),
+/* The same for one part of the step: which = 0 the step kernels (as
+ * fdtd_solver_time_stencil),
  * 1 the interior kernel, 2 the PML-shell kernel, 3 the ghost-cell list kernel,
  * 4 the listener kernel.  Parts 1-4 need FDTD_KERNEL_FUSED.  The fields are
  * left in an unspecified state (timing only). */
