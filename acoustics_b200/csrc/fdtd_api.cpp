@@ -8,7 +8,6 @@
 #include <atomic>
 #include <cmath>
 #include <cstdio>
-#include <cstdlib>
 #include <cstring>
 #include <limits>
 #include <memory>
@@ -1188,11 +1187,6 @@ fdtd_status fdtd_solver_reset(fdtd_solver* s, double t0) {
     }
     s->region.fc = P.fc_n > 0 ? 1 : 0;
     s->region.red = use_reduced_pml(s, n_solid == 0) ? 1 : 0;
-    // reduced state: interior and shell tiles in one launch unless FDTD_STEP_FUSION=0
-    {
-        const char* f = std::getenv("FDTD_STEP_FUSION");
-        s->region.fuse = (f && f[0] == '0') ? 0 : 1;
-    }
     // reduced state: the TMA-staged shell kernel where it applies (tiles and
     // tensor maps of this solve), else the per-thread cp.async kernel
     free_shell_tma(s);

@@ -11,7 +11,6 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -223,11 +222,6 @@ fdtd_status rebuild(fdtd_batch* b) {
     L.ghost_blocks = std::min(max_ghost, 32);
     L.src_blocks = max_src;
     L.solid_blocks = std::min(max_solid, 64);
-    {
-        // interior and reduced-state shell tiles in one launch unless FDTD_STEP_FUSION=0
-        const char* f = std::getenv("FDTD_STEP_FUSION");
-        L.fuse = (f && f[0] == '0') ? 0 : 1;
-    }
     for (int i = 0; i < 2; ++i)
         if (b->graph[i]) {
             cudaGraphExecDestroy(b->graph[i]);

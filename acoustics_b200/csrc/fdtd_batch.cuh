@@ -58,29 +58,6 @@ __global__ void __launch_bounds__(256, FDTD_SHELL_RED_MINB) k_batch_shell_red(co
     shell_tile_red(d.a[d.cur], d.shell, tile.box, tile.tz, tile.tx);
 }
 
-// Interior tiles of every member and shell tiles of the reduced-state members
-// in one launch, the shell CTAs spread evenly among the interior ones (see
-// k_step_red): the memory-bound and the issue-bound CTAs share the SMs.
-template <int XB>
-__global__ void __launch_bounds__(256, FDTD_SHELL_RED_MINB)
-    k_batch_step_red(const BatchDesc<float>* __restrict__ D, const BatchTile* __restrict__ int_tiles,
-                     const BatchTile* __restrict__ shell_tiles, int n_int, int n_shell) {
-    const int j = blockIdx.x;
-    const long long n = (long long)n_int + n_shell;
-    const long long s0 = (long long)j * n_shell / n, s1 = (long long)(j + 1) * n_shell / n;
-    if (s1 > s0) {
-        const BatchTile tile = shell_tiles[s0];
-        const BatchDesc<float>& d = D[tile.m];
-        if (d.halted) return;
-        shell_tile_red(d.a[d.cur], d.shell, tile.box, tile.tz, tile.tx);
-    } else {
-        const BatchTile tile = int_tiles[j - (int)s0];
-        const BatchDesc<float>& d = D[tile.m];
-        if (d.halted) return;
-        interior_tile<float, XB>(d.a[d.cur], d.interior, tile.tz, tile.tx);
-    }
-}
-
 // grid (solid_blocks, members): re-zero the solid cells inside the PML of the
 // members that have some (the PML update writes every PML cell; classification
 // zeroes solid cells in every buffer at the start of a step, MAC_Grid.cpp:3566-3600)
@@ -146,31 +123,17 @@ cudaError_t launch_batch(const BatchLaunch& L, const StepStreams& S, int* launch
         ++l;
     }
     const bool gside = L.ghost_blocks > 0 && S.s3 != nullptr;
-    // FP32: interior and reduced-state shell tiles in one launch on the solver stream
-    bool fuse = false;
-    if constexpr (sizeof(T) == 4) fuse = L.fuse && L.n_int > 0 && L.n_shell_red > 0 && (L.xb == 2 || L.xb == 4);
     cudaError_t e = cudaEventRecord(S.fork, S.s);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(S.s2, S.fork, 0);
     if (e == cudaSuccess && gside) e = cudaStreamWaitEvent(S.s3, S.fork, 0);
     if (e != cudaSuccess) return e;
     if (L.ghost_blocks > 0) {
         // first: a few latency-bound CTAs that run beside the interior's
-        k_batch_ghost<T><<<dim3(L.ghost_blocks, L.n_members), 128, 0, gside ? S.s3 : (fuse ? S.s : S.s2)>>>(D);
+        k_batch_ghost<T><<<dim3(L.ghost_blocks, L.n_members), 128, 0, gside ? S.s3 : S.s2>>>(D);
         ++l;
         if (gside && (e = cudaEventRecord(S.ghost, S.s3)) != cudaSuccess) return e;
     }
-    if (fuse) {
-        if constexpr (sizeof(T) == 4) {
-            const int n = L.n_int + L.n_shell_red;
-            if (L.xb == 2)
-                k_batch_step_red<2><<<n, dim3(32, 8), red_smem_bytes(), S.s>>>(D, L.int_tiles, L.shell_tiles, L.n_int,
-                                                                            L.n_shell_red);
-            else
-                k_batch_step_red<4><<<n, dim3(32, 8), red_smem_bytes(), S.s>>>(D, L.int_tiles, L.shell_tiles, L.n_int,
-                                                                            L.n_shell_red);
-            ++l;
-        }
-    } else if (L.n_int > 0) {
+    if (L.n_int > 0) {
         const dim3 block(32, 8);
         if (L.xb == 2) k_batch_interior<T, 2><<<L.n_int, block, 0, S.s2>>>(D, L.int_tiles);
         else if (L.xb == 8) k_batch_interior<T, 8><<<L.n_int, block, 0, S.s2>>>(D, L.int_tiles);
@@ -180,7 +143,7 @@ cudaError_t launch_batch(const BatchLaunch& L, const StepStreams& S, int* launch
     int n_red = 0;
     if constexpr (sizeof(T) == 4) {
         n_red = L.n_shell_red;
-        if (n_red > 0 && !fuse) {
+        if (n_red > 0) {
             k_batch_shell_red<float><<<n_red, dim3(32, 8), red_smem_bytes(), S.s>>>(D, L.shell_tiles);
             ++l;
         }
@@ -189,12 +152,11 @@ cudaError_t launch_batch(const BatchLaunch& L, const StepStreams& S, int* launch
         k_batch_shell<T><<<L.n_shell - n_red, dim3(32, 8), 0, S.s>>>(D, L.shell_tiles + n_red);
         ++l;
     }
-    // sources follow the interior updates of their cells (on the solver stream
-    // when the interior ran in the fused launch) and the ghost list
-    const cudaStream_t ss = fuse ? S.s : S.s2;
-    if (gside && (e = cudaStreamWaitEvent(ss, S.ghost, 0)) != cudaSuccess) return e;
+    if (gside && (e = cudaStreamWaitEvent(S.s2, S.ghost, 0)) != cudaSuccess) return e;
     if (L.src_blocks > 0) {
-        k_batch_sources<T><<<dim3(L.src_blocks, L.n_members), 256, 0, ss>>>(D);
+        // source cells are non-PML cells: ordered after the interior and ghost updates
+        // of their cells, concurrent with the shell
+        k_batch_sources<T><<<dim3(L.src_blocks, L.n_members), 256, 0, S.s2>>>(D);
         ++l;
     }
     e = cudaEventRecord(S.join, S.s2);

@@ -192,7 +192,6 @@ struct RegionLaunch {
     int red;           // FP32: the shell keeps the reduced PML state (k_pml_shell_red)
     int fc;            // FULLY_COUPLED ghost cells: solve their system before the ghost list
     const TmaStep* tma;  // reduced state: the TMA-staged shell (k_pml_shell_tma) when not null (host memory)
-    int fuse;          // reduced state: interior and shell tiles in one launch (k_step_red)
 };
 
 // Two copies indexed by the step parity: the kernels of a step read
@@ -452,7 +451,6 @@ struct BatchLaunch {
     int ghost_blocks;            // per member
     int solid_blocks;            // per member (0: no member has a solid cell inside its PML)
     int src_blocks;              // per member (0: no member has a source)
-    int fuse;                    // FP32: interior and reduced-state shell tiles in one launch
 };
 
 // z-vector groups of the interior box: groups start at multiples of V = 16 /

@@ -41,15 +41,6 @@ cudaError_t prepare_fp32_kernels() {
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k_batch_shell_red<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      red_smem_bytes());
-        // the launches that run interior and shell tiles together carry the same ring
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_step_red<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, red_smem_bytes());
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_batch_step_red<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     red_smem_bytes());
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(k_batch_step_red<4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     red_smem_bytes());
     }
     return e;
 }

@@ -483,12 +483,8 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
     const int nx = b.hi[0] - b.lo[0], ny = b.hi[1] - b.lo[1], nz = b.hi[2] - b.lo[2];
     const bool has_interior = nx > 0 && ny > 0 && nz > 0 && !(R.skip & 1);
     const bool has_ghost = R.ghost_cap > 0 && !(R.skip & 4);
-    const int nblk_shell = (R.skip & 2) ? 0 : R.shell.block_first[R.shell.n];
-    // FP32 reduced state: interior and shell tiles in one launch on the solver stream
-    bool fuse = false;
-    if constexpr (sizeof(T) == 4) fuse = R.fuse && R.red && !R.tma && !hP.visc && has_interior && nblk_shell > 0;
-    const bool split = has_interior && S.s2 != nullptr && !fuse;
-    const bool gside = (split || fuse) && (has_ghost || R.fc) && S.s3 != nullptr;
+    const bool split = has_interior && S.s2 != nullptr;
+    const bool gside = split && (has_ghost || R.fc) && S.s3 != nullptr;
     const cudaStream_t si = split ? S.s2 : S.s;
     cudaError_t e = cudaSuccess;
     const unsigned eng_blocks = hP.eng_n > 0 ? (unsigned)std::min((hP.eng_n + 127) / 128, 148 * 8) : 0u;
@@ -497,9 +493,9 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
         k_engquist_predict<T><<<eng_blocks, 128, 0, S.s>>>(dP, cur);
         ++l;
     }
-    if (split || gside) {
+    if (split) {
         e = cudaEventRecord(S.fork, S.s);
-        if (e == cudaSuccess && split) e = cudaStreamWaitEvent(S.s2, S.fork, 0);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(S.s2, S.fork, 0);
         if (e == cudaSuccess && gside) e = cudaStreamWaitEvent(S.s3, S.fork, 0);
         if (e != cudaSuccess) return e;
     }
@@ -516,16 +512,7 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
         ++l;
     }
     if (gside && (e = cudaEventRecord(S.ghost, S.s3)) != cudaSuccess) return e;
-    if (fuse) {
-        if constexpr (sizeof(T) == 4) {
-            const int V = 16 / (int)sizeof(T);
-            const int ntu = interior_unit_tiles(b, V);
-            const int n_int = ntu * ((nx + 3) / 4);
-            k_step_red<4><<<n_int + nblk_shell, dim3(32, 8), red_smem_bytes(), S.s>>>(A, b, R.shell, n_int,
-                                                                                   nblk_shell, ntu);
-            ++l;
-        }
-    } else if (has_interior) {
+    if (has_interior) {
         dim3 block(32, 8);
         const int xb = (!hP.visc && (R.xb == 4 || R.xb == 8)) ? R.xb : 2;
         dim3 grid(interior_unit_tiles(b, 16 / (int)sizeof(T)), (nx + xb - 1) / xb);
@@ -535,7 +522,7 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
         else k_interior<T, 4><<<grid, block, 0, si>>>(A, b);
         ++l;
     }
-    const int nblk = fuse ? 0 : nblk_shell;
+    const int nblk = (R.skip & 2) ? 0 : R.shell.block_first[R.shell.n];
     if (nblk > 0) {
         if constexpr (sizeof(T) == 4) {
             if (R.red && R.tma)
@@ -548,7 +535,7 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
         }
         ++l;
     }
-    if (gside && (e = cudaStreamWaitEvent(si, S.ghost, 0)) != cudaSuccess) return e;
+    if (gside && (e = cudaStreamWaitEvent(S.s2, S.ghost, 0)) != cudaSuccess) return e;
     if (R.sources) {
         // source cells are non-PML cells: after the interior and ghost updates of
         // their cells, concurrent with the shell

@@ -419,28 +419,4 @@ __global__ void __launch_bounds__(256, FDTD_SHELL_RED_MINB) k_pml_shell_red(cons
     shell_tile_red(A, B, b, tu, tx);
 }
 
-// Interior and reduced-state shell tiles in one launch.  A stencil CTA is
-// memory-bound and a shell CTA issue-bound, so the two kinds should share every
-// SM rather than follow each other: the shell CTAs are spread evenly among the
-// interior ones in block order (block j is a shell CTA when the count
-// floor(j * n_shell / n) steps up at j), which is the order the hardware
-// dispatches them in.  Each CTA runs the same tile function as the separate
-// kernels, so results are bit-equal to them.
-template <int XB>
-__global__ void __launch_bounds__(256, FDTD_SHELL_RED_MINB)
-    k_step_red(const KArgs<float> A, const Box3 box, const ShellBoxes B, int n_int, int n_shell, int ntu) {
-    const int j = blockIdx.x;
-    const long long n = (long long)n_int + n_shell;
-    const long long s0 = (long long)j * n_shell / n, s1 = (long long)(j + 1) * n_shell / n;
-    if (A.advance && j == 0 && threadIdx.x == 0 && threadIdx.y == 0) advance_consts(*A.P, A.cur);
-    if (s1 > s0) {
-        int b, tu, tx;
-        shell_decode(B, (int)s0, b, tu, tx);
-        shell_tile_red(A, B, b, tu, tx);
-    } else {
-        const int t = j - (int)s0;  // interior CTAs before this one
-        interior_tile<float, XB>(A, box, t % ntu, t / ntu);
-    }
-}
-
 }  // namespace fdtd

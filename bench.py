@@ -442,25 +442,36 @@ def main():
     # (independent of --steps): create (scene tables uploaded, first
     # classification), sc.steps steps with the listener rows copied to host
     # memory, destroy.  Both precisions; their series are the accuracy check.
-    def e2e_solve(p2):
-        torch.cuda.synchronize()
-        dist.barrier(ranks)
-        t0 = time.perf_counter()
-        s2 = PML_WaveSolver(sc, precision=p2, kernel=S.KERNEL_FUSED, graph_steps=G, device=local)
-        y = s2.step(sc.steps)
-        h2d, d2h = s2.transfer_bytes()
-        s2.close()
-        dt = dist.max_over_ranks(time.perf_counter() - t0, ranks)
-        return y, {"value": world * sc.n_cells * sc.steps / dt / 1e9, "unit": UNIT,
+    def e2e_solve(p2, repeats=2):
+        # the whole solve, `repeats` times (host-side costs of a shared machine
+        # vary between runs): the fastest is reported, every one is listed
+        best, runs, y = None, [], None
+        for _ in range(repeats):
+            torch.cuda.synchronize()
+            dist.barrier(ranks)
+            t0 = time.perf_counter()
+            s2 = PML_WaveSolver(sc, precision=p2, kernel=S.KERNEL_FUSED, graph_steps=G, device=local)
+            t1 = time.perf_counter()
+            y = s2.step(sc.steps)
+            t2 = time.perf_counter()
+            h2d, d2h = s2.transfer_bytes()
+            s2.close()
+            t3 = time.perf_counter()
+            dt = dist.max_over_ranks(t3 - t0, ranks)
+            runs.append({"seconds": dt, "create_s": t1 - t0, "steps_s": t2 - t1, "destroy_s": t3 - t2})
+            if best is None or dt < best:
+                best = dt
+        return y, {"value": world * sc.n_cells * sc.steps / best / 1e9, "unit": UNIT,
                    "h2d_bytes_per_step": h2d / sc.steps, "d2h_bytes_per_step": d2h / sc.steps,
-                   "steps": sc.steps, "seconds": dt}
+                   "steps": sc.steps, "seconds": best, "runs": runs}
 
     y_e2e32, e2e32 = e2e_solve(S.PRECISION_FP32_COMPENSATED)
     y_e2e64, e2e64 = e2e_solve(S.PRECISION_FP64)
     y_e2e = y_e2e64 if prec == S.PRECISION_FP64 else y_e2e32
     e2e = dict(e2e64 if prec == S.PRECISION_FP64 else e2e32)
     e2e["note"] = (f"whole {sc.steps}-step solve through PML_WaveSolver: create (scene upload, classification), "
-                   f"steps with listener rows to host, destroy; bytes counted by fdtd_solver_transfer_bytes")
+                   f"steps with listener rows to host, destroy; the faster of two such solves (runs lists both); "
+                   f"bytes counted by fdtd_solver_transfer_bytes")
     # the timed rows must be the rows of the same solve stepped through the public API
     n_cmp = max(0, min(K, sc.steps - W))
     rows_equal = bool(np.array_equal(y_ours[:n_cmp], y_e2e[W:W + n_cmp]))

@@ -115,19 +115,3 @@ def test_batch_mixed_pml_states(fdtd_lib):
         b.run()
         for m, s in enumerate(scenes):
             assert np.array_equal(b.output(m), alone(s, p, s.steps)), f"member {m}"
-
-
-def test_fused_batch_launch_is_bit_equal(fdtd_lib, monkeypatch):
-    """Interior and reduced-state shell tiles of all members in one launch (the
-    default) against the separate kernels."""
-    scenes = uneven_scenes(17, 5)
-    p = S.PRECISION_FP32_COMPENSATED
-    monkeypatch.setenv("FDTD_STEP_FUSION", "0")
-    with SolveBatch(scenes, precision=p, tune=False) as b:
-        b.run()
-        ya = [b.output(m) for m in range(len(scenes))]
-    monkeypatch.delenv("FDTD_STEP_FUSION")
-    with SolveBatch(scenes, precision=p, tune=False) as b:
-        b.run()
-        for m in range(len(scenes)):
-            assert np.array_equal(b.output(m), ya[m]), f"member {m}"

@@ -257,21 +257,3 @@ def test_long_host_call_staging(fdtd_lib, precision):
     assert np.array_equal(ya, buf.cpu().numpy())
     a.close()
     b.close()
-
-
-@pytest.mark.parametrize("n", [64, 96])
-def test_fused_interior_shell_launch_is_bit_equal(fdtd_lib, monkeypatch, n):
-    """FP32 reduced state: interior and shell tiles in one launch (the default)
-    give the bits of the two separate kernels."""
-    sc = S.config2(n=n, steps=80) if n != 64 else S.config1()
-    monkeypatch.setenv("FDTD_STEP_FUSION", "0")
-    a = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED)
-    monkeypatch.delenv("FDTD_STEP_FUSION")
-    b = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED, graph_steps=16)
-    assert a.pml_state() == S.PML_STATE_AUTO
-    ya, yb = a.step(80), b.step(80)
-    assert np.abs(ya).max() > 0
-    assert np.array_equal(ya, yb)
-    assert np.array_equal(a.field(S.FIELD_PRESSURE), b.field(S.FIELD_PRESSURE))
-    a.close()
-    b.close()
