@@ -312,6 +312,52 @@ __global__ void __launch_bounds__(256) k_cls_sweep(const SolveParams* __restrict
     }
 }
 
+// The sweep of a moving-body step restricted to the units the boxes of the
+// step before reached: every cell outside them already holds bulk, a valid
+// history and no mask (the boxes are unions of a body's bounds over two steps,
+// so the solid, masked and fresh cells of the step before all lie in units they
+// reach), so the full sweep would write nothing there.  One warp per unit,
+// every unit once; units a box of this step reaches are left to k_cls_near.
+__global__ void __launch_bounds__(256) k_cls_sweep_prev(const SolveParams* __restrict__ Pp, const ClsBoxes prev,
+                                                        int collect_fresh) {
+    const SolveParams& P = *Pp;
+    const ClsBoxes& B = P.boxes;
+    const int lane = threadIdx.x & 31;
+    const long long total = prev.ufirst[prev.n];
+    const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
+    const unsigned long long bulk8 = 0x0101010101010101ull * CLS_BULK;
+    for (long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; t < total; t += nwarps) {
+        int b = 0;
+        while (t >= prev.ufirst[b + 1]) ++b;
+        const long long r = t - prev.ufirst[b];
+        const int nj = prev.un[b][1], nc = prev.un[b][2];
+        const int i = prev.u0[b][0] + (int)(r / ((long long)nj * nc));
+        const int j = prev.u0[b][1] + (int)((r / nc) % nj);
+        const int ch = prev.u0[b][2] + (int)(r % nc);
+        bool skip = false;
+        for (int e = 0; e < b && !skip; ++e) skip = unit_in(prev, e, i, j, ch);
+        for (int e = 0; e < B.n && !skip; ++e) skip = unit_in(B, e, i, j, ch);
+        if (skip) continue;
+        const int k0 = ch * CLS_CHUNK + lane * 8;
+        if (k0 >= P.N[2]) continue;
+        const long long c = (long long)i * P.SX + (long long)j * P.SY + k0;
+        const uint2 d = *(const uint2*)(P.cls + c);
+        const unsigned long long w = ((unsigned long long)d.y << 32) | d.x;
+        const int nk = min(8, P.N[2] - k0);
+        const unsigned long long cells = nk >= 8 ? ~0ull : (1ull << (8 * nk)) - 1ull;
+        const unsigned long long out = ((bulk8 | ((w & bulk8) >> 1)) & cells) | (w & ~cells);
+        if (out == w) continue;
+        *(uint2*)(P.cls + c) = make_uint2((uint32_t)out, (uint32_t)(out >> 32));
+        unsigned long long fresh = collect_fresh ? ~w & bulk8 & cells : 0ull;
+        while (fresh) {
+            const int m = (__ffsll((long long)fresh) - 1) >> 3;
+            fresh &= ~(0xFFull << (8 * m));
+            const int slot = atomicAdd(P.fresh_count, 1);
+            if (slot < P.fresh_cap) P.fresh_list[slot] = (int)(c + m);
+        }
+    }
+}
+
 // Units some box reaches, one warp each, every unit once (in the first box
 // that reaches it); a lane takes two quads.
 __global__ void __launch_bounds__(256) k_cls_near(const SolveParams* __restrict__ Pp, int collect_fresh) {
@@ -811,12 +857,19 @@ cudaError_t launch_listener_prep(SolveParams* dP, int precision, int newp, int n
 }
 
 cudaError_t launch_classify(const SolveParams* dP, const int N[3], const ClsBoxes& B, bool collect_fresh,
-                            cudaStream_t s) {
+                            cudaStream_t s, const ClsBoxes* prev) {
     k_cls_boxes<<<grid_for(B.first[B.n], 128), 128, 0, s>>>(dP);
-    const int chunks = (N[2] + CLS_CHUNK - 1) / CLS_CHUNK;
-    const int nunits = N[0] * N[1] * chunks;
-    const int warps = (nunits + CLS_UNITS - 1) / CLS_UNITS;
-    k_cls_sweep<<<(warps + 7) / 8, 256, 0, s>>>(dP, nunits, chunks, collect_fresh ? 1 : 0);
+    if (prev) {
+        const long long units = prev->ufirst[prev->n];
+        if (units > 0)
+            k_cls_sweep_prev<<<(unsigned)std::min<long long>((units + 7) / 8, 148 * 16), 256, 0, s>>>(
+                dP, *prev, collect_fresh ? 1 : 0);
+    } else {
+        const int chunks = (N[2] + CLS_CHUNK - 1) / CLS_CHUNK;
+        const int nunits = N[0] * N[1] * chunks;
+        const int warps = (nunits + CLS_UNITS - 1) / CLS_UNITS;
+        k_cls_sweep<<<(warps + 7) / 8, 256, 0, s>>>(dP, nunits, chunks, collect_fresh ? 1 : 0);
+    }
     if (B.ufirst[B.n] > 0) k_cls_near<<<grid_for((B.ufirst[B.n] + 7) / 8, 1), 256, 0, s>>>(dP, collect_fresh ? 1 : 0);
     return cudaGetLastError();
 }

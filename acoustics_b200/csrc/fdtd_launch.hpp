@@ -35,9 +35,11 @@ cudaError_t launch_listeners(const SolveParams* dP, int precision, int newp, int
                              cudaStream_t s);
 // cell classification over the boxes B (a copy of dP->boxes): the box solid
 // test, the sweep over the units no box reaches and the one over those it does
-// (3 launches; the last only when some box has cells)
+// (3 launches; the last only when some box has cells).  With `prev` (the boxes
+// of the classification before, when every cell outside them is known to hold
+// the default flags) the first sweep visits only the units those reached.
 cudaError_t launch_classify(const SolveParams* dP, const int N[3], const ClsBoxes& B, bool collect_fresh,
-                            cudaStream_t s);
+                            cudaStream_t s, const ClsBoxes* prev = nullptr);
 cudaError_t launch_cls_history(const SolveParams* dP, long long ncell, int* count, int* list, int cap, cudaStream_t s);
 cudaError_t launch_fresh_cells(const SolveParams* dP, int precision, int cur, long long ncell, int* d_status,
                                cudaStream_t s);

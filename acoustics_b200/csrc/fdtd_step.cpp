@@ -28,11 +28,11 @@ using namespace fdtd;
 namespace {
 
 // Classification over the boxes already in s->hP.boxes.
-void classification_launches(fdtd_solver* s, fdtd_status& st) {
+void classification_launches(fdtd_solver* s, fdtd_status& st, const ClsBoxes* prev) {
     const ClsBoxes& B = s->hP.boxes;
     // pageable source: the copy is staged before the call returns
     cudaError_t e = fdtd::counted_copyAsync(s, &s->dP->boxes, &B, sizeof(ClsBoxes), cudaMemcpyHostToDevice, s->stream);
-    if (e == cudaSuccess) e = launch_classify(s->dP, s->N, B, s->moving, s->stream);
+    if (e == cudaSuccess) e = launch_classify(s->dP, s->N, B, s->moving, s->stream, prev);
     s->launches += B.ufirst[B.n] > 0 ? 3 : 2;
     if (e != cudaSuccess) {
         set_error(s, std::string("classification launch: ") + cudaGetErrorString(e));
@@ -177,7 +177,9 @@ fdtd_status enqueue_step(fdtd_solver* s, int cur, double* dev_row, bool classify
             s->overlapped_steps++;
             CUDA_TRY(s, cudaEventRecord(s->ev_sdone, s->stream5));
         }
-        classification_launches(s, st);
+        // moving bodies after a classification of the step before: only the units
+        // its boxes reached can hold flags other than the defaults
+        classification_launches(s, st, (s->moving && s->cls_boxes_current) ? &prev : nullptr);
         s->cls_boxes_current = true;
         if (st != FDTD_OK) return st;
         if (s->moving) {
