@@ -18,7 +18,7 @@ LIB_PATH = os.environ.get("FDTD_B200_LIB") or os.path.join(HERE, "_lib", "libfdt
 # every symbol include/fdtd_c.h declares
 EXPORTS = [
     "fdtd_abi_version", "fdtd_last_error", "fdtd_device_count", "fdtd_debug_inject_failure", "fdtd_gaussian_source_defaults",
-    "fdtd_solver_create", "fdtd_solver_destroy", "fdtd_solver_reset", "fdtd_solver_step",
+    "fdtd_solver_create", "fdtd_solver_destroy", "fdtd_release_cached_memory", "fdtd_solver_reset", "fdtd_solver_step",
     "fdtd_solver_step_device", "fdtd_solver_fetch_listeners", "fdtd_solver_info_get",
     "fdtd_solver_get_classification", "fdtd_solver_get_field", "fdtd_solver_synchronize",
     "fdtd_solver_stream", "fdtd_solver_last_error", "fdtd_solver_last_launch_count", "fdtd_solver_pml_state", "fdtd_solver_shell_staging",
@@ -68,6 +68,7 @@ def load(build_if_missing: bool = False):
         "fdtd_gaussian_source_defaults": ([C.POINTER(GaussianSourceDesc), dbl], i32),
         "fdtd_solver_create": ([C.POINTER(SceneDesc), C.POINTER(Options), C.POINTER(vp)], i32),
         "fdtd_solver_destroy": ([vp], i32),
+        "fdtd_release_cached_memory": ([i32], None),
         "fdtd_solver_reset": ([vp, dbl], i32),
         "fdtd_solver_step": ([vp, i32, vp], i32),
         "fdtd_solver_step_device": ([vp, i32, vp], i32),

@@ -11,6 +11,7 @@
 #include <cstring>
 #include <limits>
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -78,6 +79,86 @@ static double absorption(double x, double mn, double mx, double w, double S, int
         if (hMax <= w) return S * (distMax * distMax) / a2;
     }
     return 0.0;
+}
+
+// Arena blocks of destroyed solvers, kept per device for the next solver:
+// cudaFree of a block of a few hundred MB synchronises the device and was
+// measured to take from a few ms to half a second, which a server creating and
+// destroying solves, or a caller timing whole solves, would pay every time.  A
+// block serves a request of at least half its size; when cudaMalloc fails, the
+// blocks kept for that device are freed and the allocation is tried again.
+namespace {
+struct KeptArena {
+    int device;
+    void* ptr;
+    size_t bytes;
+};
+std::mutex g_arena_mu;
+std::vector<KeptArena> g_arenas;  // oldest first
+constexpr size_t ARENAS_KEPT = 8;
+
+void free_kept(int device) {
+    std::vector<KeptArena> drop;
+    {
+        std::lock_guard<std::mutex> lk(g_arena_mu);
+        std::vector<KeptArena> keep;
+        for (const auto& a : g_arenas) (device < 0 || a.device == device ? drop : keep).push_back(a);
+        g_arenas.swap(keep);
+    }
+    int cur = -1;
+    cudaGetDevice(&cur);
+    for (const auto& a : drop) {
+        cudaSetDevice(a.device);
+        cudaFree(a.ptr);
+    }
+    if (cur >= 0) cudaSetDevice(cur);
+}
+}  // namespace
+
+cudaError_t arena_acquire(int device, size_t bytes, void** ptr, size_t* block_bytes) {
+    {
+        std::lock_guard<std::mutex> lk(g_arena_mu);
+        int best = -1;
+        for (int i = 0; i < (int)g_arenas.size(); ++i) {
+            const KeptArena& a = g_arenas[i];
+            if (a.device != device || a.bytes < bytes || a.bytes / 2 > bytes) continue;
+            if (best < 0 || a.bytes < g_arenas[best].bytes) best = i;
+        }
+        if (best >= 0) {
+            *ptr = g_arenas[best].ptr;
+            *block_bytes = g_arenas[best].bytes;
+            g_arenas.erase(g_arenas.begin() + best);
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e == cudaErrorMemoryAllocation) {
+        cudaGetLastError();
+        free_kept(device);
+        e = cudaMalloc(ptr, bytes);
+    }
+    if (e == cudaSuccess) *block_bytes = bytes;
+    return e;
+}
+
+void arena_release(int device, void* ptr, size_t block_bytes) {
+    if (!ptr) return;
+    KeptArena drop{-1, nullptr, 0};
+    {
+        std::lock_guard<std::mutex> lk(g_arena_mu);
+        g_arenas.push_back({device, ptr, block_bytes});
+        if (g_arenas.size() > ARENAS_KEPT) {
+            drop = g_arenas.front();
+            g_arenas.erase(g_arenas.begin());
+        }
+    }
+    if (drop.ptr) {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        cudaSetDevice(drop.device);
+        cudaFree(drop.ptr);
+        if (cur >= 0) cudaSetDevice(cur);
+    }
 }
 
 // one dimension of MAC_Grid::InsidePML (MAC_Grid.cpp:4027-4062)
@@ -923,12 +1004,15 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     const int* N = s->N;
     SolveParams& P = s->hP;
     void* base = nullptr;
-    cudaError_t e = inject_failure(FDTD_INJECT_DEVICE_ALLOC) ? cudaErrorMemoryAllocation : cudaMalloc(&base, cv.off);
+    size_t block = 0;
+    cudaError_t e = inject_failure(FDTD_INJECT_DEVICE_ALLOC) ? cudaErrorMemoryAllocation
+                                                             : arena_acquire(o.device, cv.off, &base, &block);
     if (e != cudaSuccess) {
         set_error(nullptr, std::string("cudaMalloc of ") + std::to_string(cv.off) + " bytes failed: " + cudaGetErrorString(e));
         return FDTD_ERR_OOM;
     }
     s->arena = base;
+    s->arena_block = block;
     s->arena_bytes = cv.off;
     for (auto& r : cv.req) *r.first = (char*)base + r.second;
     const long long ncell = s->ncell;
@@ -1085,6 +1169,8 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     return FDTD_OK;
 }
 
+void fdtd_release_cached_memory(int32_t device) { fdtd::free_kept(device); }
+
 fdtd_status fdtd_solver_destroy(fdtd_solver* s) {
     if (!s) return FDTD_OK;
     cudaSetDevice(s->opt.device);
@@ -1097,7 +1183,7 @@ fdtd_status fdtd_solver_destroy(fdtd_solver* s) {
     free_shell_tma(s);
     for (void* p : s->mesh_alloc) cudaFree(p);
     if (s->d_solid_pml) cudaFree(s->d_solid_pml);
-    if (s->arena) cudaFree(s->arena);
+    if (s->arena) arena_release(s->opt.device, s->arena, s->arena_block);
     if (s->h_lis_stage) cudaFreeHost(s->h_lis_stage);
     for (cudaEvent_t ev : {s->ev_fork, s->ev_join, s->ev_ghost, s->ev_step, s->ev_lis[0], s->ev_lis[1], s->ev_lis_join,
                            s->ev_sfork, s->ev_sdone})

@@ -102,6 +102,7 @@ struct fdtd_solver {
     fdtd::SolveParams* dP = nullptr;
     void* arena = nullptr;
     size_t arena_bytes = 0;
+    size_t arena_block = 0;         // bytes of the device block holding the arena (>= its carve)
     int* d_solid_pml = nullptr;
     int n_solid_pml = 0;
     double* d_lap = nullptr;
@@ -151,6 +152,10 @@ inline cudaError_t counted_copyAsync(fdtd_solver* s, void* dst, const void* src,
 void set_error(fdtd_solver* s, const std::string& msg);
 // moving bodies two cells clear of the PML through [start_time, end_time]
 bool moving_clear_of_pml(fdtd_solver* s);
+// Device blocks for solver arenas, kept after a solver is destroyed for the next
+// one on the same device (fdtd_api.cpp)
+cudaError_t arena_acquire(int device, size_t bytes, void** ptr, size_t* block_bytes);
+void arena_release(int device, void* ptr, size_t block_bytes);
 // listener plans of a static solve from its current classification (after a restore)
 fdtd_status rebuild_listener_plans(fdtd_solver* s);
 // fdtd_debug_inject_failure: true when this allocation of kind `what` is to fail

@@ -282,7 +282,12 @@ fdtd_status fdtd_gaussian_source_defaults(fdtd_gaussian_source_desc* src, double
  * (PML_WaveSolver.cpp:78-146) + FDTD_AcousticSimulator::ResetStartTime (:458-523). */
 fdtd_status fdtd_solver_create(const fdtd_scene_desc* scene, const fdtd_options* options,
                                fdtd_solver** out);
+/* Releases the solver's streams and events; its device block is kept for the next
+ * solver created on the same device (freed when an allocation would fail, or by
+ * fdtd_release_cached_memory). */
 fdtd_status fdtd_solver_destroy(fdtd_solver* s);
+/* Free the device blocks kept from destroyed solvers: of one device, or of all (device < 0). */
+void fdtd_release_cached_memory(int32_t device);
 /* Reinitialize_PML_WaveSolver(true, t0) + ResetCellHistory(true) (PML_WaveSolver.cpp:102-146) */
 fdtd_status fdtd_solver_reset(fdtd_solver* s, double start_time);
 /* n x (stepSystem() + FetchPressureData(listeners)) : SimWorld::StepWorld (SimWorld.cpp:507-592).

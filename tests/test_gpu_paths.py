@@ -257,3 +257,21 @@ def test_long_host_call_staging(fdtd_lib, precision):
     assert np.array_equal(ya, buf.cpu().numpy())
     a.close()
     b.close()
+
+
+def test_kept_device_blocks_start_clean(fdtd_lib):
+    """A destroyed solver's device block serves the next solver, which starts
+    from the same zero state: rows equal those of the first run; the kept
+    blocks can be released."""
+    sc = S.config1()
+    a = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED)
+    ya = a.step(120)
+    a.close()
+    b = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED)
+    yb = b.step(120)
+    b.close()
+    assert np.abs(ya).max() > 0 and np.array_equal(ya, yb)
+    fdtd_lib.fdtd_release_cached_memory(-1)
+    c = PML_WaveSolver(sc, precision=S.PRECISION_FP32_COMPENSATED)
+    assert np.array_equal(c.step(120), ya)
+    c.close()
