@@ -101,15 +101,18 @@ __host__ __device__ constexpr int shell_vz(int word) { return word == 4 ? FDTD_S
 // shares with other boxes stay in the grid arrays: it reads its high x / y
 // faces at the far box ends from there, and writes its low x / y faces at
 // x = x0 / y = y0 to both (the x / y slabs read them as their high faces).
+constexpr int SHELL_MAX_BOXES = 9;
 struct ShellBoxes {
     int n, xs, vz;
-    int x0[5], nx[5], y0[5], ny[5];
-    int za[5], zae[5], zb[5], zbe[5];
-    int gl[5], ng[5];
-    int tu[5], tx[5];
-    int block_first[6];
+    int x0[SHELL_MAX_BOXES], nx[SHELL_MAX_BOXES], y0[SHELL_MAX_BOXES], ny[SHELL_MAX_BOXES];
+    int za[SHELL_MAX_BOXES], zae[SHELL_MAX_BOXES], zb[SHELL_MAX_BOXES], zbe[SHELL_MAX_BOXES];
+    int gl[SHELL_MAX_BOXES], ng[SHELL_MAX_BOXES];
+    int tu[SHELL_MAX_BOXES], tx[SHELL_MAX_BOXES];
+    int zp[SHELL_MAX_BOXES];  // every group whole, in the box and outside the z PML
+    int block_first[SHELL_MAX_BOXES + 1];
     int zbox;     // box with compact storage (-1: none)
     int zrw;      // compact row width (elements): (ng + 1) * vz
+    int xy_slabs; // PML on both sides along x and y, and along z on one side at least
     long long cells;
 };
 

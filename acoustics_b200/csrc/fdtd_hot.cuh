@@ -448,7 +448,7 @@ __device__ __forceinline__ void shell_tile(const KArgs<T>& A, const ShellBoxes& 
 __device__ __forceinline__ void shell_decode(const ShellBoxes& B, int blk, int& b, int& tu, int& tx) {
     b = 0;
 #pragma unroll
-    for (int q = 1; q < 5; ++q)
+    for (int q = 1; q < SHELL_MAX_BOXES; ++q)
         if (q < B.n && blk >= B.block_first[q]) b = q;
     const int local = blk - B.block_first[b];
     tu = local % B.tu[b];

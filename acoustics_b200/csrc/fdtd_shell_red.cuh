@@ -175,7 +175,9 @@ __device__ __forceinline__ void red_unstage(const KArgs<float>& A, RedPlane<shel
     if ((KIND == 0 && EY) || ezm) L.a2 = *reinterpret_cast<const VT*>(sp + 9 * FV);
 }
 
-template <int KIND, bool EY, bool PF>
+// ZP: every group of box b is whole, in the box and outside the z PML (every
+// per-cell z mask is then known: all cells in, none absorbing along z).
+template <int KIND, bool EY, bool PF, bool ZP = false>
 __device__ __forceinline__ void shell_tile_red_impl(const KArgs<float>& A, const ShellBoxes& B, int b, int u, int tx) {
     using T = float;
     constexpr bool CMP = KIND == 2;
@@ -193,6 +195,7 @@ __device__ __forceinline__ void shell_tile_red_impl(const KArgs<float>& A, const
     unsigned inbox = 0;
 #pragma unroll
     for (int e = 0; e < V; ++e) inbox |= (zg + e >= zr0 && zg + e < zr1 ? 1u : 0u) << e;
+    if constexpr (ZP) inbox = ALL;
     const int x0 = B.x0[b] + tx * B.xs;
     const int x1 = min(x0 + B.xs, B.x0[b] + B.nx[b]);
     const int sx = (int)A.sx, sy = (int)A.sy;
@@ -209,7 +212,7 @@ __device__ __forceinline__ void shell_tile_red_impl(const KArgs<float>& A, const
     const uint8_t gy = __ldg(A.axflag[1] + y);
     uint8_t gz[V];
 #pragma unroll
-    for (int e = 0; e < V; ++e) gz[e] = __ldg(A.axflag[2] + zg + e);
+    for (int e = 0; e < V; ++e) gz[e] = ZP ? (uint8_t)0 : __ldg(A.axflag[2] + zg + e);
     const unsigned zpml = flag_mask<V>(gz, 0), zflo = flag_mask<V>(gz, 1), zfhi = flag_mask<V>(gz, 2);
     const unsigned znext = flag_mask<V>(gz, 3), zhlo = flag_mask<V>(gz, 4), zhhi = flag_mask<V>(gz, 5);
     const unsigned ezm = zpml & inbox;  // cells absorbing along z
@@ -398,12 +401,20 @@ __device__ __forceinline__ void shell_tile_red(const KArgs<float>& A, const Shel
     // columns with two absorbing axes hold more state per plane: they load one
     // plane at a time (PF_EY), the others issue the next plane's loads first
     constexpr bool PF = FDTD_SHELL_RED_PREFETCH != 0, PF_EY = FDTD_SHELL_RED_PREFETCH == 2;
+    // (B.zp is uniform per CTA: the plain-z boxes take their own path without divergence)
     if (b == B.zbox) {
         shell_tile_red_impl<2, false, PF>(A, B, b, u, tx);
     } else if (__ldg(A.axflag[0] + B.x0[b]) & AXF_PML) {
         const int y = B.y0[b] + u / B.ng[b];
-        if (__ldg(A.axflag[1] + y) & AXF_PML) shell_tile_red_impl<0, true, PF_EY>(A, B, b, u, tx);
-        else shell_tile_red_impl<0, false, PF>(A, B, b, u, tx);
+        if (__ldg(A.axflag[1] + y) & AXF_PML) {
+            if (B.zp[b]) shell_tile_red_impl<0, true, PF_EY, true>(A, B, b, u, tx);
+            else shell_tile_red_impl<0, true, PF_EY>(A, B, b, u, tx);
+        } else {
+            if (B.zp[b]) shell_tile_red_impl<0, false, PF, true>(A, B, b, u, tx);
+            else shell_tile_red_impl<0, false, PF>(A, B, b, u, tx);
+        }
+    } else if (B.zp[b]) {
+        shell_tile_red_impl<1, true, PF_EY, true>(A, B, b, u, tx);
     } else {
         shell_tile_red_impl<1, true, PF_EY>(A, B, b, u, tx);
     }
