@@ -29,6 +29,8 @@ SCENES = {
     "uneven_pml8": lambda: _uneven(22, 8),
     "uneven_pml5": lambda: _uneven(23, 5),
     "config2_128cube_pml8": lambda: S.config2(n=128),
+    # long rows: the default kernel runs the plain-z columns on their own boxes
+    "config2_192cube_pml12": lambda: S.config2(n=192),
 }
 
 
