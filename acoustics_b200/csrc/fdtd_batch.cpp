@@ -353,81 +353,90 @@ fdtd_status fdtd_batch_member_snapshot(fdtd_batch* b, int32_t member, void* buff
     return FDTD_OK;
 }
 
+}  // extern "C"
+
+namespace fdtd {
+
+fdtd_status batch_prepare(const fdtd_options& batch_opt, const fdtd_scene_desc* scene, int32_t steps_total,
+                          const void* snapshot, int64_t snapshot_bytes, const double* rows, int64_t steps_done,
+                          PreparedMember* out, std::string* err) {
+    auto fail = [&](fdtd_status code, const std::string& m, fdtd_solver* s) {
+        if (s) fdtd_solver_destroy(s);
+        *err = m;
+        return code;
+    };
+    if (!scene || !out || steps_total < 0 || steps_done < 0 || steps_done > steps_total)
+        return fail(FDTD_ERR_INVALID_ARG, "batch member: invalid arguments", nullptr);
+    if (scene->boundary_handling != FDTD_BOUNDARY_RASTERIZE)
+        return fail(FDTD_ERR_UNSUPPORTED, "batched members use RASTERIZE boundaries", nullptr);
+    if (scene->air_viscosity_alpha != 0.0)
+        return fail(FDTD_ERR_UNSUPPORTED, "batched members have no air viscosity", nullptr);
+    if (snapshot && scene->n_listeners > 0 && steps_done > 0 && !rows)
+        return fail(FDTD_ERR_INVALID_ARG, "batch member: rows missing", nullptr);
+    fdtd_options o = batch_opt;
+    o.graph_steps = 0;
+    o.shell_staging = FDTD_SHELL_STAGING_RING;  // the batch kernels stage per thread
+    fdtd_solver* s = nullptr;
+    fdtd_status st = fdtd_solver_create(scene, &o, &s);
+    if (st != FDTD_OK) return fail(st, fdtd_last_error(), nullptr);
+    if (s->moving) return fail(FDTD_ERR_UNSUPPORTED, "moving bodies are stepped by fdtd_solver, not in batches", s);
+    if (!s->eng.empty()) return fail(FDTD_ERR_UNSUPPORTED, "batched members have a PML on every side", s);
+    PreparedMember pm;
+    pm.s = s;
+    pm.total = steps_total;
+    if (snapshot) {
+        st = fdtd_solver_restore(s, snapshot, snapshot_bytes);
+        if (st != FDTD_OK) return fail(st, fdtd_solver_last_error(s), s);
+        if (s->step_index != steps_done) return fail(FDTD_ERR_INVALID_ARG, "snapshot step differs from steps_done", s);
+        pm.done = steps_done;
+        if (s->L > 0 && steps_done > 0) pm.rows.assign(rows, rows + (size_t)steps_done * s->L);
+    } else if (steps_total > 0) {
+        // the first step classifies the cells (MAC_Grid::classifyCells_FAST)
+        pm.rows.resize(s->L);
+        st = fdtd_solver_step(s, 1, s->L ? pm.rows.data() : nullptr);
+        if (st < 0) return fail(st, fdtd_solver_last_error(s), s);
+        pm.done = 1;
+    }
+    *out = std::move(pm);
+    return FDTD_OK;
+}
+
+int32_t batch_place(fdtd_batch* b, PreparedMember&& pm) {
+    Member mb;
+    mb.s = pm.s;
+    mb.total = pm.total;
+    mb.done = pm.done;
+    mb.L = pm.s->L;
+    mb.rows = std::move(pm.rows);
+    mb.active = mb.done < mb.total;
+    pm.s = nullptr;
+    return place_member(b, std::move(mb));
+}
+
+}  // namespace fdtd
+
+extern "C" {
+
 fdtd_status fdtd_batch_add_snapshot(fdtd_batch* b, const fdtd_scene_desc* scene, int32_t steps_total,
                                     const void* snapshot, int64_t bytes, const double* rows, int64_t steps_done,
                                     int32_t* member) {
-    if (!b || !scene || !snapshot || steps_total < 0 || steps_done < 0 || steps_done > steps_total)
-        return batch_fail(b, FDTD_ERR_INVALID_ARG, "fdtd_batch_add_snapshot: invalid arguments");
-    if (scene->boundary_handling != FDTD_BOUNDARY_RASTERIZE)
-        return batch_fail(b, FDTD_ERR_UNSUPPORTED, "batched members use RASTERIZE boundaries");
-    if (scene->air_viscosity_alpha != 0.0)
-        return batch_fail(b, FDTD_ERR_UNSUPPORTED, "batched members have no air viscosity");
-    if (scene->n_listeners > 0 && steps_done > 0 && !rows)
-        return batch_fail(b, FDTD_ERR_INVALID_ARG, "fdtd_batch_add_snapshot: rows missing");
-    fdtd_options o = b->opt;
-    o.graph_steps = 0;
-    o.shell_staging = FDTD_SHELL_STAGING_RING;
-    fdtd_solver* s = nullptr;
-    fdtd_status st = fdtd_solver_create(scene, &o, &s);
-    if (st != FDTD_OK) return batch_fail(b, st, fdtd_last_error());
-    auto fail = [&](fdtd_status code, const std::string& m) {
-        fdtd_solver_destroy(s);
-        return batch_fail(b, code, m);
-    };
-    if (s->moving) return fail(FDTD_ERR_UNSUPPORTED, "moving bodies are stepped by fdtd_solver, not in batches");
-    if (!s->eng.empty()) return fail(FDTD_ERR_UNSUPPORTED, "batched members have a PML on every side");
-    st = fdtd_solver_restore(s, snapshot, bytes);
-    if (st != FDTD_OK) return fail(st, fdtd_solver_last_error(s));
-    if (s->step_index != steps_done) return fail(FDTD_ERR_INVALID_ARG, "snapshot step differs from steps_done");
-    Member mb;
-    mb.s = s;
-    mb.total = steps_total;
-    mb.done = steps_done;
-    mb.L = s->L;
-    if (mb.L > 0 && steps_done > 0) mb.rows.assign(rows, rows + (size_t)steps_done * mb.L);
-    mb.active = mb.done < mb.total;
-    const int32_t slot = place_member(b, std::move(mb));
+    if (!b || !scene || !snapshot) return batch_fail(b, FDTD_ERR_INVALID_ARG, "fdtd_batch_add_snapshot: invalid arguments");
+    fdtd::PreparedMember pm;
+    std::string err;
+    const fdtd_status st = fdtd::batch_prepare(b->opt, scene, steps_total, snapshot, bytes, rows, steps_done, &pm, &err);
+    if (st != FDTD_OK) return batch_fail(b, st, err);
+    const int32_t slot = fdtd::batch_place(b, std::move(pm));
     if (member) *member = slot;
     return FDTD_OK;
 }
 
 fdtd_status fdtd_batch_add(fdtd_batch* b, const fdtd_scene_desc* scene, int32_t steps, int32_t* member) {
     if (!b || !scene || steps < 0) return batch_fail(b, FDTD_ERR_INVALID_ARG, "fdtd_batch_add: invalid arguments");
-    if (scene && scene->boundary_handling != FDTD_BOUNDARY_RASTERIZE)
-        return batch_fail(b, FDTD_ERR_UNSUPPORTED, "batched members use RASTERIZE boundaries");
-    if (scene && scene->air_viscosity_alpha != 0.0)
-        return batch_fail(b, FDTD_ERR_UNSUPPORTED, "batched members have no air viscosity");
-    fdtd_options o = b->opt;
-    o.graph_steps = 0;
-    o.shell_staging = FDTD_SHELL_STAGING_RING;  // the batch kernels stage per thread
-    fdtd_solver* s = nullptr;
-    fdtd_status st = fdtd_solver_create(scene, &o, &s);
-    if (st != FDTD_OK) return batch_fail(b, st, fdtd_last_error());
-    if (s->moving) {
-        fdtd_solver_destroy(s);
-        return batch_fail(b, FDTD_ERR_UNSUPPORTED, "moving bodies are stepped by fdtd_solver, not in batches");
-    }
-    if (!s->eng.empty()) {
-        fdtd_solver_destroy(s);
-        return batch_fail(b, FDTD_ERR_UNSUPPORTED, "batched members have a PML on every side");
-    }
-    Member mb;
-    mb.s = s;
-    mb.total = steps;
-    mb.L = s->L;
-    if (steps > 0) {
-        // the first step classifies the cells (MAC_Grid::classifyCells_FAST)
-        mb.rows.resize(mb.L);
-        st = fdtd_solver_step(s, 1, mb.L ? mb.rows.data() : nullptr);
-        if (st < 0) {
-            std::string m = fdtd_solver_last_error(s);
-            fdtd_solver_destroy(s);
-            return batch_fail(b, st, m);
-        }
-        mb.done = 1;
-    }
-    mb.active = mb.done < mb.total;
-    const int32_t slot = place_member(b, std::move(mb));
+    fdtd::PreparedMember pm;
+    std::string err;
+    const fdtd_status st = fdtd::batch_prepare(b->opt, scene, steps, nullptr, 0, nullptr, 0, &pm, &err);
+    if (st != FDTD_OK) return batch_fail(b, st, err);
+    const int32_t slot = fdtd::batch_place(b, std::move(pm));
     if (member) *member = slot;
     return FDTD_OK;
 }

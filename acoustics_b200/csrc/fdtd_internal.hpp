@@ -152,6 +152,19 @@ inline cudaError_t counted_copyAsync(fdtd_solver* s, void* dst, const void* src,
 void set_error(fdtd_solver* s, const std::string& msg);
 // moving bodies two cells clear of the PML through [start_time, end_time]
 bool moving_clear_of_pml(fdtd_solver* s);
+// A batch member made outside the batch: its solver created and its first step
+// run (or its snapshot restored), ready to be placed between two batched steps
+// (fdtd_batch.cpp).  batch_prepare touches no batch state, so a server prepares
+// members on another host thread while its batch steps.
+struct PreparedMember {
+    fdtd_solver* s = nullptr;
+    int64_t total = 0, done = 0;
+    std::vector<double> rows;
+};
+fdtd_status batch_prepare(const fdtd_options& batch_opt, const fdtd_scene_desc* scene, int32_t steps_total,
+                          const void* snapshot, int64_t snapshot_bytes, const double* rows, int64_t steps_done,
+                          PreparedMember* out, std::string* err);
+int32_t batch_place(fdtd_batch* b, PreparedMember&& pm);
 // Device blocks for solver arenas, kept after a solver is destroyed for the next
 // one on the same device (fdtd_api.cpp)
 cudaError_t arena_acquire(int device, size_t bytes, void** ptr, size_t* block_bytes);

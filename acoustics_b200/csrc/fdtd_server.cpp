@@ -3,7 +3,9 @@
 // Submitters (any host thread) append deep copies of their scenes to a queue.
 // One worker thread owns an fdtd_batch and loops:
 //   admit   while the queue head's device bytes fit the budget and a member
-//           slot is free: fdtd_batch_add (allocates, classifies, first step);
+//           slot is free: hand it to the preparer thread, which creates its
+//           solver (allocates, classifies, first step) beside the batched steps;
+//   place   members the preparer has finished join the batch;
 //   step    fdtd_batch_step(chunk) over all running members;
 //   retire  finished members: copy their series out, release the slot and its
 //           device bytes, wake waiters.
@@ -102,6 +104,10 @@ struct Request {
     std::vector<char> snap;         // evicted: the member's state ...
     std::vector<double> rows;       // ... and its listener rows so far
     int64_t evicted_steps = -1;     // steps done when evicted (-1: never)
+    fdtd::PreparedMember prep;      // made by the preparer thread
+    fdtd_status prep_status = FDTD_OK;
+    std::string prep_err;
+    bool in_prep = false;           // handed to the preparer, not yet placed (it reads snap and rows)
 };
 
 }  // namespace
@@ -118,6 +124,11 @@ struct fdtd_server {
     int64_t used_bytes = 0;
     bool stop = false;
     std::thread worker;
+    std::thread preparer;
+    std::condition_variable cv_prep;
+    std::deque<int64_t> to_prepare;      // admitted, waiting for the preparer
+    std::vector<int64_t> prepared;       // made, waiting to join the batch
+    int64_t preparing = 0;               // admitted and not yet placed
     fdtd_batch* batch = nullptr;
     std::string create_err;
     bool ready = false, failed_start = false;
@@ -146,10 +157,12 @@ void finish(fdtd_server* S, Request& r, int32_t state, int32_t status, const std
     } else {
         S->failed++;
     }
-    r.snap.clear();
-    r.snap.shrink_to_fit();
-    r.rows.clear();
-    r.rows.shrink_to_fit();
+    if (!r.in_prep) {  // (the worker drops them when the preparer is done with them)
+        r.snap.clear();
+        r.snap.shrink_to_fit();
+        r.rows.clear();
+        r.rows.shrink_to_fit();
+    }
 }
 
 // Members to evict so that `need` more bytes fit: running members whose
@@ -214,6 +227,43 @@ void evict(fdtd_server* S, int32_t m) {
     S->evictions++;
 }
 
+// Members are made on this thread while the worker steps the batch: a
+// request's solver creation and first step no longer stall every running solve.
+void preparer_main(fdtd_server* S) {
+    cudaSetDevice(S->opt.device);
+    for (;;) {
+        Request* r = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(S->mu);
+            S->cv_prep.wait(lk, [&] { return S->stop || !S->to_prepare.empty(); });
+            if (S->stop) return;
+            r = S->reqs[S->to_prepare.front()].get();
+            S->to_prepare.pop_front();
+        }
+        // the request's scene and snapshot are not touched by other threads meanwhile
+        fdtd::PreparedMember pm;
+        std::string err;
+        const bool resumed = r->evicted_steps >= 0;
+        const fdtd_status st =
+            fdtd::batch_prepare(S->opt, &r->scene.d, r->steps, resumed ? r->snap.data() : nullptr,
+                                resumed ? (int64_t)r->snap.size() : 0, resumed && !r->rows.empty() ? r->rows.data() : nullptr,
+                                resumed ? r->evicted_steps : 0, &pm, &err);
+        std::lock_guard<std::mutex> g(S->mu);
+        r->prep = std::move(pm);
+        r->prep_status = st;
+        r->prep_err = err;
+        S->prepared.push_back(r->id);
+        S->cv_work.notify_all();
+    }
+}
+
+// The queue head can be handed to the preparer now.  (Lock held.)
+bool admissible(const fdtd_server* S) {
+    if (S->queue.empty() || (int64_t)S->running.size() + S->preparing >= S->cfg.max_members) return false;
+    const Request& r = *S->reqs.at(S->queue.front());
+    return S->used_bytes + r.bytes <= S->cfg.hbm_budget_bytes;
+}
+
 void worker_main(fdtd_server* S) {
     cudaSetDevice(S->opt.device);
     {
@@ -232,60 +282,62 @@ void worker_main(fdtd_server* S) {
     }
     const int chunk = S->cfg.chunk_steps > 0 ? S->cfg.chunk_steps : std::max(S->opt.graph_steps, 32);
     for (;;) {
-        // ---- admit ----
-        std::vector<Request*> admit;
+        // ---- admit: queue heads go to the preparer ----
+        std::vector<int64_t> place;
         std::vector<int32_t> victims;
         {
             std::unique_lock<std::mutex> lk(S->mu);
-            S->cv_work.wait(lk, [&] { return S->stop || !S->queue.empty() || !S->running.empty(); });
+            S->cv_work.wait(lk, [&] { return S->stop || !S->prepared.empty() || !S->running.empty() || admissible(S); });
             if (S->stop) break;
-            int64_t used = S->used_bytes;
-            size_t slots = S->running.size();
-            while (!S->queue.empty() && slots < (size_t)S->cfg.max_members) {
-                Request* r = S->reqs[S->queue.front()].get();
-                if (used + r->bytes > S->cfg.hbm_budget_bytes) {  // head waits for memory
-                    if (S->cfg.preempt && admit.empty()) victims = eviction_plan(S, *r);
-                    break;
-                }
+            bool handed = false;
+            while (admissible(S)) {
+                const int64_t id = S->queue.front();
                 S->queue.pop_front();
-                used += r->bytes;
-                slots++;
-                admit.push_back(r);
+                S->used_bytes += S->reqs[id]->bytes;
+                S->reqs[id]->in_prep = true;
+                S->preparing++;
+                S->to_prepare.push_back(id);
+                handed = true;
             }
-            S->used_bytes = used;
-            S->peak_bytes = std::max(S->peak_bytes, used);
+            if (handed) S->cv_prep.notify_one();
+            S->peak_bytes = std::max(S->peak_bytes, S->used_bytes);
+            // a head that does not fit: evict only when nothing is on its way in
+            if (S->cfg.preempt && !S->queue.empty() && S->preparing == 0 && S->prepared.empty() &&
+                S->used_bytes + S->reqs[S->queue.front()]->bytes > S->cfg.hbm_budget_bytes)
+                victims = eviction_plan(S, *S->reqs[S->queue.front()]);
+            place.swap(S->prepared);
         }
         if (!victims.empty()) {
             for (int32_t m : victims) evict(S, m);
             continue;  // admit the head now
         }
-        for (Request* r : admit) {
-            int32_t m = -1;
-            fdtd_status st;
-            if (r->evicted_steps >= 0) {
-                st = fdtd_batch_add_snapshot(S->batch, &r->scene.d, r->steps, r->snap.data(), (int64_t)r->snap.size(),
-                                             r->rows.empty() ? nullptr : r->rows.data(), r->evicted_steps, &m);
-                if (st == FDTD_OK) {
-                    r->snap.clear();
-                    r->snap.shrink_to_fit();
-                    r->rows.clear();
-                    r->rows.shrink_to_fit();
-                }
-            } else {
-                st = fdtd_batch_add(S->batch, &r->scene.d, r->steps, &m);
-            }
+        // ---- place the members the preparer made ----
+        for (int64_t id : place) {
             std::lock_guard<std::mutex> g(S->mu);
-            if (r->state == FDTD_REQ_CANCELLED) {  // cancelled while it was being admitted
-                if (st == FDTD_OK) fdtd_batch_release(S->batch, m);
+            Request* r = S->reqs[id].get();
+            S->preparing--;
+            r->in_prep = false;
+            if (r->state == FDTD_REQ_CANCELLED) {  // cancelled while it was being prepared
+                if (r->prep.s) fdtd_solver_destroy(r->prep.s);
+                r->prep.s = nullptr;
                 S->used_bytes -= r->bytes;
+                r->snap.clear();
+                r->snap.shrink_to_fit();
+                r->rows.clear();
+                r->rows.shrink_to_fit();
                 continue;
             }
-            if (st != FDTD_OK) {
+            if (r->prep_status != FDTD_OK) {
                 S->used_bytes -= r->bytes;
-                finish(S, *r, FDTD_REQ_FAILED, st, fdtd_last_error());
+                finish(S, *r, FDTD_REQ_FAILED, r->prep_status, r->prep_err);
                 S->cv_done.notify_all();
                 continue;
             }
+            const int32_t m = fdtd::batch_place(S->batch, std::move(r->prep));
+            r->snap.clear();
+            r->snap.shrink_to_fit();
+            r->rows.clear();
+            r->rows.shrink_to_fit();
             r->member = m;
             r->state = FDTD_REQ_RUNNING;
             r->n_listeners = r->scene.d.n_listeners;
@@ -357,6 +409,7 @@ void worker_main(fdtd_server* S) {
             for (int64_t id : S->queue) finish(S, *S->reqs[id], FDTD_REQ_FAILED, st, "server stopped after a failed step");
             S->queue.clear();
             S->stop = true;
+            S->cv_prep.notify_all();
             S->cv_done.notify_all();
             break;
         }
@@ -398,12 +451,19 @@ fdtd_status fdtd_server_create(const fdtd_options* options, const fdtd_server_co
     }
     fdtd_server* raw = S.get();
     S->worker = std::thread(worker_main, raw);
+    S->preparer = std::thread(preparer_main, raw);
     {
         std::unique_lock<std::mutex> lk(S->mu);
         S->cv_done.wait(lk, [&] { return S->ready; });
     }
     if (S->failed_start) {
         S->worker.join();
+        {
+            std::lock_guard<std::mutex> g(S->mu);
+            S->stop = true;
+            S->cv_prep.notify_all();
+        }
+        S->preparer.join();
         fdtd::set_error(nullptr, S->create_err);
         return FDTD_ERR_CUDA;
     }
@@ -561,8 +621,16 @@ fdtd_status fdtd_server_destroy(fdtd_server* S) {
         std::lock_guard<std::mutex> g(S->mu);
         S->stop = true;
         S->cv_work.notify_all();
+        S->cv_prep.notify_all();
     }
     if (S->worker.joinable()) S->worker.join();
+    if (S->preparer.joinable()) S->preparer.join();
+    // members made but never placed
+    for (auto& kv : S->reqs)
+        if (kv.second->prep.s) {
+            fdtd_solver_destroy(kv.second->prep.s);
+            kv.second->prep.s = nullptr;
+        }
     if (S->batch) {
         cudaSetDevice(S->opt.device);
         fdtd_batch_destroy(S->batch);
