@@ -953,8 +953,16 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     } else {
         CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
     }
-    CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream2, cudaStreamNonBlocking));
-    CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream3, cudaStreamNonBlocking));
+    {
+        // moving bodies: the interior and ghost-list CTAs go before the remaining
+        // CTAs of the shell that started beside the classification (FP64 moving
+        // step 0.356 -> 0.344 ms; FP32 unchanged)
+        int least = 0, greatest = 0;
+        CUDA_TRY(nullptr, cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        const int pr = any_moving ? greatest : least;
+        CUDA_TRY(nullptr, cudaStreamCreateWithPriority(&s->stream2, cudaStreamNonBlocking, pr));
+        CUDA_TRY(nullptr, cudaStreamCreateWithPriority(&s->stream3, cudaStreamNonBlocking, pr));
+    }
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_ghost, cudaEventDisableTiming));
     CUDA_TRY(nullptr, cudaStreamCreateWithFlags(&s->stream4, cudaStreamNonBlocking));
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_step, cudaEventDisableTiming));
