@@ -3,6 +3,8 @@
 // is rounded on its own, in the order the reference writes it, which keeps the
 // FP64 path and the classification bit-reproducible against a CPU build of the
 // same expressions.
+#include <cooperative_groups.h>
+#include <cooperative_groups/scan.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -111,9 +113,13 @@ __global__ void __launch_bounds__(128) k_cls_boxes(const SolveParams* __restrict
 // The cells of a quad that need more than their mask: ghost cells (closest
 // object), non-PML bulk cells with a solid neighbour (ghost-neighbour list) and
 // fresh cells (fresh-cell list); `sel` has the bulk bit set at those bytes,
-// `code` the quad's new bulk / valid bits.
+// `code` the quad's new bulk / valid bits.  The list slots of the lanes that
+// call it together are taken with one atomic per list (an atomic per cell on
+// one counter serialises thousands of cells a step); the lists are unordered.
 __device__ __noinline__ void cls_cells(const SolveParams& P, const ClsQuad q, uint32_t sel, uint32_t code,
                                        uint32_t listed, uint32_t fresh) {
+    namespace cg = cooperative_groups;
+    uint32_t to_list = 0, to_fresh = 0;  // bytes (bulk bit) of this quad's cells for each list
     while (sel) {
         const int m = (__ffs(sel) - 1) >> 3;
         sel &= ~(0xFFu << (8 * m));
@@ -125,15 +131,32 @@ __device__ __noinline__ void cls_cells(const SolveParams& P, const ClsQuad q, ui
             P.gobj[c] = (P.gobj[c] & GOBJ_CONSTRAINT) | (uint8_t)(o < 0 ? GOBJ_NONE : o);
             continue;
         }
-        if (((listed >> (8 * m)) & CLS_BULK) && !(P.pml_cell[0][q.i] || P.pml_cell[1][q.j] || P.pml_cell[2][k])) {
-            // non-PML bulk cell next to a solid: updated by k_ghost_cells
-            const int slot = atomicAdd(P.ghost_count, 1);
-            if (slot < P.ghost_cap) P.ghost_list[slot] = (int)c;
-        }
-        if ((fresh >> (8 * m)) & CLS_BULK) {
-            const int slot = atomicAdd(P.fresh_count, 1);
-            if (slot < P.fresh_cap) P.fresh_list[slot] = (int)c;
-        }
+        // non-PML bulk cells next to a solid: updated by k_ghost_cells
+        if (((listed >> (8 * m)) & CLS_BULK) && !(P.pml_cell[0][q.i] || P.pml_cell[1][q.j] || P.pml_cell[2][k]))
+            to_list |= (uint32_t)CLS_BULK << (8 * m);
+        if ((fresh >> (8 * m)) & CLS_BULK) to_fresh |= (uint32_t)CLS_BULK << (8 * m);
+    }
+    const cg::coalesced_group g = cg::coalesced_threads();
+    const int nl = __popc(to_list), nf = __popc(to_fresh);
+    const int pl = cg::exclusive_scan(g, nl), pf = cg::exclusive_scan(g, nf);
+    const int tl = g.shfl(pl + nl, g.size() - 1), tf = g.shfl(pf + nf, g.size() - 1);
+    int bl = 0, bf = 0;
+    if (g.thread_rank() == 0) {
+        if (tl) bl = atomicAdd(P.ghost_count, tl);
+        if (tf) bf = atomicAdd(P.fresh_count, tf);
+    }
+    int sl = g.shfl(bl, 0) + pl, sf = g.shfl(bf, 0) + pf;
+    while (to_list) {
+        const int m = (__ffs(to_list) - 1) >> 3;
+        to_list &= ~(0xFFu << (8 * m));
+        if (sl < P.ghost_cap) P.ghost_list[sl] = (int)(q.c0 + m);
+        ++sl;
+    }
+    while (to_fresh) {
+        const int m = (__ffs(to_fresh) - 1) >> 3;
+        to_fresh &= ~(0xFFu << (8 * m));
+        if (sf < P.fresh_cap) P.fresh_list[sf] = (int)(q.c0 + m);
+        ++sf;
     }
 }
 
