@@ -266,6 +266,7 @@ fdtd_status capture(fdtd_batch* b, int n) {
     if (e != cudaSuccess) return batch_fail(b, FDTD_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
     e = cudaGraphInstantiate(&b->graph[f0], g, 0);
     cudaGraphDestroy(g);
+    if (e == cudaSuccess) e = cudaGraphUpload(b->graph[f0], b->stream);  // device-side setup now
     if (e != cudaSuccess) return batch_fail(b, FDTD_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
     return FDTD_OK;
 }

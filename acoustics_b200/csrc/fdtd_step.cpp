@@ -324,6 +324,8 @@ fdtd_status capture_graph(fdtd_solver* s, int cur, int n, bool src, cudaGraphExe
     }
     e = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
+    // the graph's device-side setup now, not at its first launch
+    if (e == cudaSuccess) e = cudaGraphUpload(*out, s->stream);
     if (e != cudaSuccess) {
         set_error(s, std::string("graph instantiate: ") + cudaGetErrorString(e));
         return FDTD_ERR_CUDA;
