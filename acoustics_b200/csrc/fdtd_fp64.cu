@@ -235,22 +235,6 @@ __device__ __forceinline__ void cls_sweep_quad(const SolveParams& P, const ClsQu
     }
 }
 
-// The two quads of a lane in a unit that some box reaches.
-__device__ __noinline__ void cls_sweep_lane_near(const SolveParams& P, int i, int j, int k0, uint2 w, int collect_fresh) {
-    ClsQuad q;
-    q.i = i;
-    q.j = j;
-    q.k0 = k0;
-    q.nk = min(4, P.N[2] - k0);
-    q.c0 = (long long)i * P.SX + (long long)j * P.SY + k0;
-    cls_sweep_quad(P, q, w.x, collect_fresh);
-    if (k0 + 4 >= P.N[2]) return;
-    q.k0 = k0 + 4;
-    q.nk = min(4, P.N[2] - k0 - 4);
-    q.c0 += 4;
-    cls_sweep_quad(P, q, w.y, collect_fresh);
-}
-
 // Box b reaches unit (i, j, ch): a cell of it, or a neighbour of one, is in the box.
 __device__ __forceinline__ bool unit_in(const ClsBoxes& B, int b, int i, int j, int ch) {
     return i >= B.u0[b][0] && i < B.u0[b][0] + B.un[b][0] && j >= B.u0[b][1] && j < B.u0[b][1] + B.un[b][1] &&
@@ -387,9 +371,13 @@ __global__ void __launch_bounds__(256) k_cls_near(const SolveParams* __restrict_
     const SolveParams& P = *Pp;
     const ClsBoxes& B = P.boxes;
     const int lane = threadIdx.x & 31;
-    const long long total = B.ufirst[B.n];
+    // two warps per unit, a quad per lane: the few units of a step spread over
+    // twice the warps, each walking half the chain
+    const long long total = 2 * B.ufirst[B.n];
     const long long nwarps = (long long)gridDim.x * (blockDim.x >> 5);
-    for (long long t = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; t < total; t += nwarps) {
+    for (long long th = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5; th < total; th += nwarps) {
+        const long long t = th >> 1;
+        const int half = (int)(th & 1);
         int b = 0;
         while (t >= B.ufirst[b + 1]) ++b;
         const long long r = t - B.ufirst[b];
@@ -400,10 +388,15 @@ __global__ void __launch_bounds__(256) k_cls_near(const SolveParams* __restrict_
         bool dup = false;
         for (int e = 0; e < b && !dup; ++e) dup = unit_in(B, e, i, j, ch);
         if (dup) continue;
-        const int k0 = ch * CLS_CHUNK + lane * 8;
+        const int k0 = ch * CLS_CHUNK + lane * 8 + 4 * half;
         if (k0 >= P.N[2]) continue;
-        const uint2 w = *(const uint2*)(P.cls + (long long)i * P.SX + (long long)j * P.SY + k0);
-        cls_sweep_lane_near(P, i, j, k0, w, collect_fresh);
+        ClsQuad q;
+        q.i = i;
+        q.j = j;
+        q.k0 = k0;
+        q.nk = min(4, P.N[2] - k0);
+        q.c0 = (long long)i * P.SX + (long long)j * P.SY + k0;
+        cls_sweep_quad(P, q, *(const uint32_t*)(P.cls + q.c0), collect_fresh);
     }
 }
 
@@ -893,7 +886,7 @@ cudaError_t launch_classify(const SolveParams* dP, const int N[3], const ClsBoxe
         const int warps = (nunits + CLS_UNITS - 1) / CLS_UNITS;
         k_cls_sweep<<<(warps + 7) / 8, 256, 0, s>>>(dP, nunits, chunks, collect_fresh ? 1 : 0);
     }
-    if (B.ufirst[B.n] > 0) k_cls_near<<<grid_for((B.ufirst[B.n] + 7) / 8, 1), 256, 0, s>>>(dP, collect_fresh ? 1 : 0);
+    if (B.ufirst[B.n] > 0) k_cls_near<<<grid_for((2 * B.ufirst[B.n] + 7) / 8, 1), 256, 0, s>>>(dP, collect_fresh ? 1 : 0);
     return cudaGetLastError();
 }
 
