@@ -20,7 +20,7 @@ OUT_DIR = os.path.join(HERE, "_lib")
 LIB = os.path.join(OUT_DIR, "libfdtd_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
-CU_FP64 = ["fdtd_fp64.cu", "fdtd_noalloc.cu", "fdtd_fp32.cu"]  # all compiled with -fmad=false
+CU_FP64 = ["fdtd_fp64.cu", "fdtd_noalloc.cu", "fdtd_fp32.cu", "fdtd_fetch.cu"]  # all compiled with -fmad=false
 CU_FAST = []
 CPP = ["fdtd_api.cpp", "fdtd_step.cpp", "fdtd_xml.cpp", "fdtd_batch.cpp", "fdtd_server.cpp", "fdtd_io.cpp", "fdtd_coupled.cpp",
        "fdtd_mesh.cpp", "fdtd_tma.cpp", "fdtd_kinematics.cpp"]

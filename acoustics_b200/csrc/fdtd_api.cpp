@@ -604,6 +604,7 @@ fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
     s->np = ((long long)s->N[0] + 1) * s->SX;
     const double w = sc->pml_width * s->h;  // setPMLBoundaryWidth (MAC_Grid.cpp:146-150)
     const double S = sc->pml_strength;
+    s->pml_strength = S;
     const double one_over_k = 1.0 / s->k;
     for (int d = 0; d < 3; ++d) {
         const int n = s->N[d];
@@ -611,6 +612,7 @@ fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
         T.pml_cell.assign(n, 0);
         T.pml_face.assign(n + 1, 0);
         T.cpos.assign(n, 0.0);
+        T.csig.assign(n, 0.0);
         T.fpos.assign(n + 1, 0.0);
         T.pupd.assign(n, 0.0);
         T.pdiv.assign(n, 0.0);
@@ -622,6 +624,7 @@ fdtd_status solver_init_geometry(fdtd_solver* s, const fdtd_scene_desc* sc) {
             T.cpos[i] = p;
             T.pml_cell[i] = inside_pml_1d(p, s->bmin[d], s->bmax[d], w, s->preset, d);
             const double sigma = absorption(p, s->bmin[d], s->bmax[d], w, S, s->preset, d);
+            T.csig[i] = sigma;
             const double directional = one_over_k + sigma / 2.0;           // MAC_Grid.h:550-553
             T.pupd[i] = (1.0 / s->k - sigma / 2.0) / directional;          // MAC_Grid.h:558-561
             T.pdiv[i] = (-1.0 * s->rho * s->c * s->c / directional);       // MAC_Grid.h:566-569

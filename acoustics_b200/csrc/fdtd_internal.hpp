@@ -44,6 +44,7 @@ bool read_obj(const char* path, double scale, std::vector<double>& verts, std::v
 struct AxisTables {
     std::vector<uint8_t> pml_cell, pml_face;
     std::vector<double> cpos, fpos, pupd, pdiv, vupd, vgrad;
+    std::vector<double> csig;  // absorption coefficient at the cell centres
 };
 
 void host_object_pose(HostObject& o, double t);
@@ -77,6 +78,7 @@ struct fdtd_solver {
     long long overlapped_steps = 0;
     // geometry
     double h = 0, c = 0, rho = 0, k = 0, end_time = 0, start_time = 0;
+    double pml_strength = 0;
     int N[3] = {0, 0, 0};
     long long ncell = 0, n_pml = 0, n_interior = 0;
     long long SX = 0, SY = 0, np = 0;  // padded strides and elements per device array

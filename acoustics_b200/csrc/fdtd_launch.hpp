@@ -48,6 +48,25 @@ cudaError_t launch_fresh_cells(const SolveParams* dP, int precision, int cur, lo
 cudaError_t launch_phased_fp64(const SolveParams* dP, const int N[3], int cur, double* lap, cudaStream_t s,
                                int* launches);
 
+// fdtd_fetch.cu: cell read-back (FetchCell / SampleAxisAlignedSlice).  A request
+// is a padded cell index and the element addresses of its split pressures
+// (a[0..2]) and of its lower (a[3+2d]) and upper (a[4+2d]) face velocities,
+// null where the solve does not hold them.
+struct FetchReq {
+    long long c;
+    const void* a[9];
+};
+struct FetchVal {
+    double p, p_prev;   // p^{n+1} (current) and p^n
+    double pdir[3];
+    double v[6];        // lower / upper face along x, y, z
+    double gc[6];       // ghost-face pressures of the last step toward -x,+x,-y,+y,-z,+z; -1: none
+    double lap;         // the Laplacian kept for the next step (air viscosity), else NaN
+    int cls, gobj;      // classification byte and ghost-object byte
+};
+cudaError_t launch_fetch_cells(const SolveParams* dP, bool fp64, int cur, const FetchReq* req, FetchVal* out, int n,
+                               cudaStream_t s);
+
 // fdtd_fp32.cu
 cudaError_t prepare_fp32_kernels();
 cudaError_t launch_prologue_fp32(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s);

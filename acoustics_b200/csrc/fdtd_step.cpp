@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <limits>
 #include <string>
 #include <vector>
 
@@ -386,6 +387,18 @@ fdtd_status run_steps(fdtd_solver* s, int n, Sink sink) {
     return FDTD_OK;
 }
 
+// FDTD_CELL_* bits of cell (i, j, k) from its classification and ghost-object bytes.
+uint8_t cell_flags(const fdtd_solver* s, uint8_t code, uint8_t gobj, int i, int j, int k) {
+    const bool bulk = code & CLS_BULK;
+    uint8_t f = 0;
+    if (bulk) f |= FDTD_CELL_BULK;
+    if (!bulk && (code & CLS_MASK)) f |= FDTD_CELL_GHOST;
+    if (code & CLS_VALID) f |= FDTD_CELL_VALID_HISTORY;
+    if (s->tab[0].pml_cell[i] || s->tab[1].pml_cell[j] || s->tab[2].pml_cell[k]) f |= FDTD_CELL_PML;
+    if (!bulk && (gobj & GOBJ_CONSTRAINT)) f |= FDTD_CELL_CONSTRAINT;
+    return f;
+}
+
 }  // namespace
 
 extern "C" {
@@ -607,15 +620,7 @@ fdtd_status fdtd_solver_get_classification(fdtd_solver* s, uint8_t* flags, fdtd_
         const bool bulk = code & CLS_BULK;
         const unsigned mask = code & CLS_MASK;
         const int i = (int)(c / sx), j = (int)((c / s->N[2]) % s->N[1]), k = (int)(c % s->N[2]);
-        if (flags) {
-            uint8_t f = 0;
-            if (bulk) f |= FDTD_CELL_BULK;
-            if (!bulk && mask) f |= FDTD_CELL_GHOST;
-            if (code & CLS_VALID) f |= FDTD_CELL_VALID_HISTORY;
-            if (s->tab[0].pml_cell[i] || s->tab[1].pml_cell[j] || s->tab[2].pml_cell[k]) f |= FDTD_CELL_PML;
-            if (!bulk && (gobj[c] & GOBJ_CONSTRAINT)) f |= FDTD_CELL_CONSTRAINT;
-            flags[c] = f;
-        }
+        if (flags) flags[c] = cell_flags(s, code, gobj[c], i, j, k);
         if (bulk || !mask) continue;
         // faces in key order: neighbour flat index ascending (-x, -y, -z, +z, +y, +x)
         static const int od[6] = {0, 1, 2, 2, 1, 0};
@@ -644,6 +649,30 @@ fdtd_status fdtd_solver_get_classification(fdtd_solver* s, uint8_t* flags, fdtd_
 }  // extern "C"
 
 namespace {
+
+// Index into the compact z-slab arrays of the PML state (ShellBoxes::zbox) of
+// the split pressure of cell (x, y, z) (dface < 0) or of its low face along
+// dface; -1 when that element lives in the padded arrays.
+long long zslab_index(const fdtd_solver* s, int dface, int x, int y, int z) {
+    const ShellBoxes& B = s->shell;
+    const int b = B.zbox, V = B.vz;
+    if (s->hP.zcount <= 0 || b < 0) return -1;
+    if (x < B.x0[b] || x >= B.x0[b] + B.nx[b] || y < B.y0[b] || y >= B.y0[b] + B.ny[b]) return -1;
+    if (dface != 2 && z >= s->N[2]) return -1;
+    auto slot = [&](int zz) -> long long {  // compact slot of the cell (or its low face) zz in the row
+        if (zz >= B.za[b] && zz < B.zae[b]) return (long long)(zz / V - B.za[b] / V) * V + zz % V;
+        if (zz >= B.zb[b] && zz < B.zbe[b]) return (long long)(B.gl[b] + zz / V - B.zb[b] / V) * V + zz % V;
+        return -1;
+    };
+    long long q = slot(z);
+    if (dface == 2 && q < 0 && z == B.zae[b] && z > 0) {
+        // boundary face after the first range: high face of its last cell
+        const long long qc = slot(z - 1);
+        q = ((z - 1) % V != V - 1) ? qc + 1 : (long long)B.ng[b] * V;
+    }
+    if (q < 0) return -1;
+    return ((long long)(x - B.x0[b]) * B.ny[b] + (y - B.y0[b])) * B.zrw + q;
+}
 
 // Field `which` between the device layout (padded arrays, the compact z-slab
 // arrays of the PML state) and a dense host array in the reference's flat order
@@ -700,28 +729,14 @@ fdtd_status field_transfer(fdtd_solver* s, int32_t which, double* dense, int64_t
     CUDA_TRY(s, cudaStreamSynchronize(s->stream));
     // every (padded grid index, compact index) pair of the z-slab box
     auto for_compact = [&](auto&& fn) {
-        const int b = B.zbox, V = B.vz;
-        const int X0 = B.x0[b], Y0 = B.y0[b], nxb = B.nx[b], nyb = B.ny[b];
-        auto slot = [&](int z) -> long long {  // compact slot of the cell (or its low face) z in the row
-            if (z >= B.za[b] && z < B.zae[b]) return (long long)(z / V - B.za[b] / V) * V + z % V;
-            if (z >= B.zb[b] && z < B.zbe[b]) return (long long)(B.gl[b] + z / V - B.zb[b] / V) * V + z % V;
-            return -1;
-        };
+        const int b = B.zbox;
         const int dface = which >= FDTD_FIELD_VX ? which - FDTD_FIELD_VX : -1;
-        for (int x = X0; x < X0 + nxb; ++x)
-            for (int y = Y0; y < Y0 + nyb; ++y) {
-                const long long row = ((long long)(x - X0) * nyb + (y - Y0)) * B.zrw;
+        for (int x = B.x0[b]; x < B.x0[b] + B.nx[b]; ++x)
+            for (int y = B.y0[b]; y < B.y0[b] + B.ny[b]; ++y)
                 for (int z = 0; z <= s->N[2]; ++z) {
-                    long long q = slot(z);
-                    if (dface == 2 && q < 0 && z == B.zae[b] && z > 0) {
-                        // boundary face after the first range: high face of its last cell
-                        const long long qc = slot(z - 1);
-                        q = ((z - 1) % V != V - 1) ? qc + 1 : (long long)B.ng[b] * V;
-                    }
-                    if (q < 0 || (dface != 2 && z == s->N[2])) continue;
-                    fn(x * s->SX + y * s->SY + z, row + q);
+                    const long long q = zslab_index(s, dface, x, y, z);
+                    if (q >= 0) fn(x * s->SX + y * s->SY + z, q);
                 }
-            }
     };
     double* r64 = (double*)raw.data();
     float* r32 = (float*)raw.data();
@@ -757,6 +772,131 @@ fdtd_status field_transfer(fdtd_solver* s, int32_t which, double* dense, int64_t
     return FDTD_OK;
 }
 
+// Device address of element (x, y, z) of a split pressure or face-velocity
+// field, where field_transfer finds it; null when the solve does not hold it
+// (the reduced PML state).
+const void* field_element(const fdtd_solver* s, int which, int x, int y, int z) {
+    const SolveParams& P = s->hP;
+    if (s->region.red) return nullptr;
+    const size_t w = s->precision == FDTD_PRECISION_FP64 ? 8 : 4;
+    const int vbuf = s->opt.kernel == FDTD_KERNEL_PHASED ? 0 : s->cur;
+    const int dface = which >= FDTD_FIELD_VX ? which - FDTD_FIELD_VX : -1;
+    const void* base = dface < 0 ? P.pd[which - FDTD_FIELD_PML_PX] : P.v[vbuf][dface];
+    if (!base) return nullptr;
+    const long long q = zslab_index(s, dface, x, y, z);
+    if (q >= 0) {
+        const void* zb = dface < 0 ? P.zpd[which - FDTD_FIELD_PML_PX] : P.zv[vbuf][dface];
+        return (const char*)zb + q * (long long)w;
+    }
+    return (const char*)base + (x * s->SX + y * s->SY + z) * (long long)w;
+}
+
+// MAC_Grid::GetCell (MAC_Grid.cpp:4182-4258) + the stored Laplacian of
+// PML_WaveSolver::FetchCell (PML_WaveSolver.cpp:439-447) for the cells of
+// dense indices `cells`: the device gathers (k_fetch_cells), the host fills
+// the geometry and PressureCellType (MAC_Grid.cpp:3977-3997).
+fdtd_status fetch_cells(fdtd_solver* s, const std::vector<long long>& cells, fdtd_cell* out) {
+    CUDA_TRY(s, cudaSetDevice(s->opt.device));
+    const int n = (int)cells.size();
+    if (n == 0) return FDTD_OK;
+    std::vector<FetchReq> req(n);
+    for (int q = 0; q < n; ++q) {
+        int ijk[3];
+        const long long t = cells[q];
+        ijk[0] = (int)(t / ((long long)s->N[1] * s->N[2]));
+        ijk[1] = (int)((t / s->N[2]) % s->N[1]);
+        ijk[2] = (int)(t % s->N[2]);
+        FetchReq& R = req[q];
+        R.c = ijk[0] * s->SX + ijk[1] * s->SY + ijk[2];
+        for (int d = 0; d < 3; ++d) {
+            int up[3] = {ijk[0], ijk[1], ijk[2]};
+            up[d] += 1;  // the upper face index never exceeds N[d] (MAC_Grid.cpp:4247-4249)
+            R.a[d] = field_element(s, FDTD_FIELD_PML_PX + d, ijk[0], ijk[1], ijk[2]);
+            R.a[3 + 2 * d] = field_element(s, FDTD_FIELD_VX + d, ijk[0], ijk[1], ijk[2]);
+            R.a[4 + 2 * d] = field_element(s, FDTD_FIELD_VX + d, up[0], up[1], up[2]);
+        }
+    }
+    const size_t req_bytes = (size_t)n * sizeof(FetchReq), val_bytes = (size_t)n * sizeof(FetchVal);
+    std::vector<FetchVal> vals(n);
+    void* dbuf = nullptr;
+    CUDA_TRY(s, cudaMallocAsync(&dbuf, req_bytes + val_bytes, s->stream));
+    FetchReq* dreq = (FetchReq*)dbuf;
+    FetchVal* dval = (FetchVal*)((char*)dbuf + req_bytes);
+    cudaError_t e = fdtd::counted_copyAsync(s, dreq, req.data(), req_bytes, cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess)
+        e = launch_fetch_cells(s->dP, s->precision == FDTD_PRECISION_FP64, s->cur, dreq, dval, n, s->stream);
+    if (e == cudaSuccess) {
+        ++s->launches;
+        e = fdtd::counted_copyAsync(s, vals.data(), dval, val_bytes, cudaMemcpyDeviceToHost, s->stream);
+    }
+    const cudaError_t ef = cudaFreeAsync(dbuf, s->stream);
+    if (e == cudaSuccess) e = ef;
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+    CUDA_TRY(s, e);
+    // the Laplacian kept for the next step: the phased path keeps the reference's
+    // (every cell, every step); the fused kernels keep it on the non-PML cells of
+    // a static scene (its other cells stay zero)
+    const bool visc = s->hP.visc != 0;
+    const bool phased = s->opt.kernel == FDTD_KERNEL_PHASED;
+    const double nan = std::numeric_limits<double>::quiet_NaN();
+    for (int q = 0; q < n; ++q) {
+        const long long t = cells[q];
+        const FetchVal& v = vals[q];
+        fdtd_cell& C = out[q];
+        std::memset(&C, 0, sizeof(C));
+        C.index = (int32_t)t;
+        C.indices[0] = (int32_t)(t / ((long long)s->N[1] * s->N[2]));
+        C.indices[1] = (int32_t)((t / s->N[2]) % s->N[1]);
+        C.indices[2] = (int32_t)(t % s->N[2]);
+        const int i = C.indices[0], j = C.indices[1], k = C.indices[2];
+        const uint8_t f = cell_flags(s, (uint8_t)v.cls, (uint8_t)v.gobj, i, j, k);
+        int32_t flags = f;
+        const bool pml = f & FDTD_CELL_PML;
+        if (pml) {
+            double m = std::numeric_limits<double>::min();
+            m = std::max(m, s->tab[0].csig[i]);
+            m = std::max(m, s->tab[1].csig[j]);
+            m = std::max(m, s->tab[2].csig[k]);
+            C.r_identity = -0.5 * m / s->pml_strength;
+        } else if (f & FDTD_CELL_BULK) {
+            C.r_identity = 0.5;
+        } else if (!(f & FDTD_CELL_GHOST)) {
+            C.r_identity = 1.0;
+        } else {
+            C.r_identity = -1.0;
+            C.n_gc_value = 6;
+        }
+        const double cp[3] = {s->tab[0].cpos[i], s->tab[1].cpos[j], s->tab[2].cpos[k]};
+        for (int d = 0; d < 3; ++d) {
+            C.centroid[d] = cp[d];
+            C.lower_corner[d] = cp[d] - s->h / 2.0;
+            C.upper_corner[d] = cp[d] + s->h / 2.0;
+        }
+        // ghost faces toward bulk neighbours; they hold zero until the first step computes them
+        const unsigned faces = C.n_gc_value ? (unsigned)(v.cls & CLS_MASK) : 0u;
+        for (int g = 0; g < 6; ++g)
+            C.gc_value[g] = ((faces >> g) & 1u) ? (s->step_index == 0 ? 0.0 : v.gc[g]) : -1.0;
+        for (int d = 0; d < 3; ++d) C.p_directional[d] = v.pdir[d];
+        C.p_full = v.p;
+        C.vx[0] = v.v[0], C.vx[1] = v.v[1];
+        C.vy[0] = v.v[2], C.vy[1] = v.v[3];
+        C.vz[0] = v.v[4], C.vz[1] = v.v[5];
+        if (!s->region.red) flags |= FDTD_CELLINFO_PML_STATE;
+        C.h = s->h;
+        if (s->step_index == 0) {
+            C.laplacian = 0.0;
+            flags |= FDTD_CELLINFO_LAPLACIAN;
+        } else if (visc && (phased || (!s->moving && !pml))) {
+            C.laplacian = v.lap;
+            flags |= FDTD_CELLINFO_LAPLACIAN;
+        } else {
+            C.laplacian = nan;
+        }
+        C.flags = flags;
+    }
+    return FDTD_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -770,6 +910,41 @@ fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, in
 
 fdtd_status fdtd_solver_set_field(fdtd_solver* s, int32_t which, const double* in, int64_t count) {
     return field_transfer(s, which, const_cast<double*>(in), count, true);
+}
+
+fdtd_status fdtd_solver_fetch_cell(fdtd_solver* s, int64_t cell_index, fdtd_cell* out) {
+    if (!s || !out) return FDTD_ERR_INVALID_ARG;
+    if (cell_index < 0 || cell_index >= s->ncell)
+        return (set_error(s, "cell_index out of range"), FDTD_ERR_INVALID_ARG);
+    return fetch_cells(s, std::vector<long long>{cell_index}, out);
+}
+
+fdtd_status fdtd_solver_sample_slice(fdtd_solver* s, int32_t dim, double offset, fdtd_cell* out, int64_t capacity,
+                                     int64_t* count) {
+    if (!s || !count) return FDTD_ERR_INVALID_ARG;
+    if (dim < 0 || dim > 2) return (set_error(s, "dim must be 0, 1 or 2"), FDTD_ERR_INVALID_ARG);
+    const int d1 = (dim + 1) % 3, d2 = (dim + 2) % 3;
+    const int64_t n = (int64_t)s->N[d1] * s->N[d2];
+    *count = n;
+    if (!out) return FDTD_OK;
+    if (capacity < n) return (set_error(s, "capacity below the slice's cell count"), FDTD_ERR_INVALID_ARG);
+    // the face grid along dim starts half a cell below the cells (MAC_Grid.cpp:103-113)
+    const double lower = s->bmin[dim] - s->h / 2.0;
+    const double r = (offset - lower) / s->h;
+    if (!(r > -1.0) || !(r < 2147483647.0))
+        return (set_error(s, "offset outside the grid along dim"), FDTD_ERR_INVALID_ARG);
+    const int k = std::min((int)r, s->N[dim] - 1);
+    std::vector<long long> cells((size_t)n);
+    size_t c = 0;
+    for (int a = 0; a < s->N[d1]; ++a)
+        for (int b = 0; b < s->N[d2]; ++b) {
+            int idx[3];
+            idx[dim] = k;
+            idx[d1] = a;
+            idx[d2] = b;
+            cells[c++] = ((long long)idx[0] * s->N[1] + idx[1]) * s->N[2] + idx[2];
+        }
+    return fetch_cells(s, cells, out);
 }
 
 // ---------------------------------------------------------------------------

@@ -127,6 +127,16 @@ class GhostFace(C.Structure):
     ]
 
 
+# fdtd_cell: MAC_Grid::Cell as GetCell fills it (MAC_Grid.h:187-215)
+CELL_DTYPE = np.dtype([
+    ("index", "<i4"), ("indices", "<i4", (3,)), ("flags", "<i4"), ("n_gc_value", "<i4"),
+    ("r_identity", "<f8"), ("centroid", "<f8", (3,)), ("lower_corner", "<f8", (3,)),
+    ("upper_corner", "<f8", (3,)), ("gc_value", "<f8", (6,)), ("p_directional", "<f8", (3,)),
+    ("p_full", "<f8"), ("vx", "<f8", (2,)), ("vy", "<f8", (2,)), ("vz", "<f8", (2,)), ("h", "<f8"),
+    ("laplacian", "<f8"),
+])
+CELLINFO_LAPLACIAN, CELLINFO_PML_STATE = 1 << 8, 1 << 9
+
 GHOST_FACE_DTYPE = np.dtype([
     ("owner_cell", "<i4"), ("neighbour_cell", "<i4"), ("topology", "<i4"), ("type", "<i4"),
     ("boundary_object", "<i4"), ("_pad", "<i4"), ("key", "<u8"),

@@ -15,7 +15,7 @@ from typing import Optional
 import numpy as np
 
 from ._lib import FDTDError, check, load
-from .scene import (FIELD_PRESSURE, GHOST_FACE_DTYPE, KERNEL_FUSED, PML_STATE_AUTO, PRECISION_FP64, Options,
+from .scene import (CELL_DTYPE, FIELD_PRESSURE, GHOST_FACE_DTYPE, KERNEL_FUSED, PML_STATE_AUTO, PRECISION_FP64, Options,
                     Scene, SceneDesc, SolverInfo)
 
 
@@ -151,6 +151,23 @@ class PML_WaveSolver:
         cap = C.c_int64(n.value)
         check(self._L.fdtd_solver_get_classification(self._h, None, faces.ctypes.data, C.byref(cap)), self._h)
         return flags, faces
+
+    def FetchCell(self, cell_index: int) -> np.void:
+        """One cell as MAC_Grid::GetCell fills it, plus the stored Laplacian
+        (PML_WaveSolver.cpp:439-447); a record of CELL_DTYPE."""
+        out = np.zeros(1, dtype=CELL_DTYPE)
+        check(self._L.fdtd_solver_fetch_cell(self._h, int(cell_index), out.ctypes.data), self._h)
+        return out[0]
+
+    def SampleAxisAlignedSlice(self, dim: int, offset: float) -> np.ndarray:
+        """The cells of the plane across axis `dim` at `offset` (MAC_Grid.cpp:1941-1963),
+        an array of CELL_DTYPE in the reference's order."""
+        n = C.c_int64(0)
+        check(self._L.fdtd_solver_sample_slice(self._h, int(dim), float(offset), None, 0, C.byref(n)), self._h)
+        out = np.zeros(n.value, dtype=CELL_DTYPE)
+        check(self._L.fdtd_solver_sample_slice(self._h, int(dim), float(offset), out.ctypes.data, out.size,
+                                               C.byref(n)), self._h)
+        return out
 
     def field(self, which: int = FIELD_PRESSURE) -> np.ndarray:
         N = list(self.divisions)

@@ -23,7 +23,7 @@
 extern "C" {
 #endif
 
-#define FDTD_ABI_VERSION 4
+#define FDTD_ABI_VERSION 5
 
 typedef int32_t fdtd_status;
 enum {
@@ -252,6 +252,43 @@ enum {
     FDTD_FIELD_VZ = 7
 };
 
+/* One cell as MAC_Grid::GetCell fills a MAC_Grid::Cell (src/wavesolver/MAC_Grid.h:187-215,
+ * MAC_Grid.cpp:4182-4258) for PML_WaveSolver::FetchCell (PML_WaveSolver.cpp:439-447).
+ * The Cell's s_identity is r_identity spelt out ("Pressure Bulk / Solid / Ghost / PML
+ * Cell") and its ghostCell pointer belongs to the finite-volume build; neither is here. */
+typedef struct {
+    int32_t index;            /* flat cell index (i*N1 + j)*N2 + k                            */
+    int32_t indices[3];
+    int32_t flags;            /* FDTD_CELL_* of the cell | FDTD_CELLINFO_*                   */
+    int32_t n_gc_value;       /* gcValue.size(): 6 for a ghost cell outside the PML, else 0   */
+    double r_identity;        /* PressureCellType (MAC_Grid.cpp:3977-3997): 0.5 bulk, 1 solid,
+                                 -1 ghost, PML: -0.5 * max_d sigma_d(centre) / pml_strength */
+    double centroid[3];
+    double lower_corner[3];   /* centroid -/+ h/2                                             */
+    double upper_corner[3];
+    double gc_value[6];       /* ghost faces toward -x,+x,-y,+y,-z,+z: the face pressure the
+                                 last step used (0 before the first step), -1 where that
+                                 neighbour is not bulk; all -1 when n_gc_value is 0         */
+    double p_directional[3];  /* split pressures _p[0..2]                                     */
+    double p_full;            /* current pressure _pCollocated[_pCollocatedInd]                */
+    double vx[2], vy[2], vz[2]; /* face velocities at the lower [0] and upper [1] face        */
+    double h;
+    double laplacian;         /* _pLaplacian[_pLaplacianInd], the Laplacian the last step kept
+                                 (of the pressure two steps before p_full); see
+                                 FDTD_CELLINFO_LAPLACIAN                                      */
+} fdtd_cell;
+
+enum {
+    /* laplacian holds the reference's value: 0 before the first step; after it, solves
+     * with air viscosity on the phased kernel (every cell) or on the fused kernels for
+     * the non-PML cells of a static scene.  Otherwise it is NaN (the fused kernels keep
+     * no Laplacian without air viscosity). */
+    FDTD_CELLINFO_LAPLACIAN = 1 << 8,
+    /* p_directional and the face velocities are held (NaN otherwise: the reduced PML
+     * state, FDTD_PML_STATE_AUTO) */
+    FDTD_CELLINFO_PML_STATE = 1 << 9
+};
+
 typedef struct fdtd_solver fdtd_solver;
 
 /* ------------------------------------------------------------------------ */
@@ -313,6 +350,17 @@ fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, in
  * current pressure, so set FDTD_FIELD_PRESSURE first.  Split pressures and
  * velocities need the full PML state (FDTD_ERR_UNSUPPORTED on the reduced one). */
 fdtd_status fdtd_solver_set_field(fdtd_solver* s, int32_t which, const double* in, int64_t count);
+/* PML_WaveSolver::FetchCell (PML_WaveSolver.cpp:439-447): cell cell_index (flat, in
+ * [0, n_cells)) at the current state. */
+fdtd_status fdtd_solver_fetch_cell(fdtd_solver* s, int64_t cell_index, fdtd_cell* out);
+/* PML_WaveSolver::SampleAxisAlignedSlice -> MAC_Grid::SampleAxisAlignedSlice
+ * (PML_WaveSolver.cpp:449-458, MAC_Grid.cpp:1941-1963): the cells of plane
+ * k = min((int)((offset - (bmin[dim] - h/2)) / h), N[dim] - 1) across axis dim, i over
+ * N[(dim+1)%3] outer, j over N[(dim+2)%3] inner.  *count <- N[(dim+1)%3]*N[(dim+2)%3];
+ * out may be NULL to query it, else capacity must reach it.  An offset a cell or more
+ * below the grid (k < 0) is FDTD_ERR_INVALID_ARG. */
+fdtd_status fdtd_solver_sample_slice(fdtd_solver* s, int32_t dim, double offset, fdtd_cell* out,
+                                     int64_t capacity, int64_t* count);
 /* Synchronise the solver's stream. */
 fdtd_status fdtd_solver_synchronize(fdtd_solver* s);
 /* The cudaStream_t every kernel of this solver is launched on (for event timing). */

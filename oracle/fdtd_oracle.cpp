@@ -1817,6 +1817,68 @@ int oracle_get_field(void* h, int which, double* out, int64_t count) {
     return FDTD_OK;
 }
 
+// MAC_Grid::GetCell (MAC_Grid.cpp:4182-4258, non-FV branch) and the stored
+// Laplacian of PML_WaveSolver::FetchCell (PML_WaveSolver.cpp:439-447).
+int oracle_fetch_cell(void* h, int64_t cell, fdtd_cell* out) {
+    Oracle* o = static_cast<Oracle*>(h);
+    if (cell < 0 || cell >= o->ncell) return FDTD_ERR_INVALID_ARG;
+    const int idx = (int)cell;
+    fdtd_cell& c = *out;
+    std::memset(&c, 0, sizeof(c));
+    c.index = idx;
+    int ijk[3];
+    o->cellIJK(idx, ijk);
+    for (int d = 0; d < 3; ++d) c.indices[d] = ijk[d];
+    const V3 pos = o->cellPosition(idx);
+    // PressureCellType (MAC_Grid.cpp:3977-3997)
+    for (int g = 0; g < 6; ++g) c.gc_value[g] = -1.0;
+    if (o->isPML[idx]) {
+        double m = std::numeric_limits<double>::min();
+        for (int d = 0; d < 3; ++d) m = std::max(m, o->PML_absorptionCoefficient(pos, d));
+        c.r_identity = -0.5 * m / o->absorptionStrength;
+    } else if (o->isBulk[idx]) {
+        c.r_identity = 0.5;
+    } else if (!o->isGhost[idx]) {
+        c.r_identity = 1.0;
+    } else {
+        c.r_identity = -1.0;
+        c.n_gc_value = 6;
+        int count = 0;
+        for (int dim = 0; dim < 3; ++dim)
+            for (int dir = -1; dir <= 1; dir += 2, ++count) {
+                int nb[3] = {ijk[0], ijk[1], ijk[2]};
+                nb[dim] += dir;
+                if (nb[dim] < 0 || nb[dim] >= o->N[dim]) continue;
+                const auto it = o->ghosts.find(MakeKey(idx, o->cellIndex(nb[0], nb[1], nb[2])));
+                if (it != o->ghosts.end()) c.gc_value[count] = it->second.pressure;
+            }
+    }
+    uint8_t f = 0;
+    if (o->isBulk[idx]) f |= FDTD_CELL_BULK;
+    if (o->isGhost[idx]) f |= FDTD_CELL_GHOST;
+    if (o->validHistory[idx]) f |= FDTD_CELL_VALID_HISTORY;
+    if (o->isPML[idx]) f |= FDTD_CELL_PML;
+    if (!o->isBulk[idx] && o->gcTypeOf[idx] == 1) f |= FDTD_CELL_CONSTRAINT;
+    c.flags = f | FDTD_CELLINFO_LAPLACIAN | FDTD_CELLINFO_PML_STATE;
+    for (int d = 0; d < 3; ++d) {
+        c.centroid[d] = pos[d];
+        c.lower_corner[d] = pos[d] - o->h / 2.0;
+        c.upper_corner[d] = pos[d] + o->h / 2.0;
+    }
+    for (int d = 0; d < 3; ++d) c.p_directional[d] = o->pDir[d][idx];
+    c.p_full = o->pCol[o->pColInd][idx];
+    double* vv[3] = {c.vx, c.vy, c.vz};
+    for (int d = 0; d < 3; ++d) {
+        int up[3] = {ijk[0], ijk[1], ijk[2]};
+        up[d] = std::min(up[d] + 1, o->N[d]);
+        vv[d][0] = o->vel[d][o->vIndex(d, ijk[0], ijk[1], ijk[2])];
+        vv[d][1] = o->vel[d][o->vIndex(d, up[0], up[1], up[2])];
+    }
+    c.h = o->h;
+    c.laplacian = o->lap[o->lapInd][idx];
+    return FDTD_OK;
+}
+
 // listener values at the current state (FetchPressureData)
 int oracle_fetch_listeners(void* h, double* out) {
     Oracle* o = static_cast<Oracle*>(h);

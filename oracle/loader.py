@@ -11,7 +11,7 @@ import subprocess
 
 import numpy as np
 
-from acoustics_b200.scene import GHOST_FACE_DTYPE, GhostFace, Scene
+from acoustics_b200.scene import CELL_DTYPE, GHOST_FACE_DTYPE, GhostFace, Scene
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
@@ -48,6 +48,8 @@ def lib():
         L.oracle_get_field.restype = C.c_int
         L.oracle_fetch_listeners.argtypes = [C.c_void_p, C.c_void_p]
         L.oracle_fetch_listeners.restype = C.c_int
+        L.oracle_fetch_cell.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        L.oracle_fetch_cell.restype = C.c_int
         L.oracle_set_threads.argtypes = [C.c_int]
         L.oracle_set_threads.restype = C.c_int
         L.oracle_mls_c0.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.POINTER(C.c_double)]
@@ -125,6 +127,14 @@ class OracleSolver:
         if st != 0:
             raise RuntimeError(f"oracle_get_field failed {st}")
         return out
+
+    def fetch_cell(self, cell_index: int) -> np.void:
+        """MAC_Grid::GetCell + the stored Laplacian, a record of CELL_DTYPE."""
+        out = np.zeros(1, dtype=CELL_DTYPE)
+        st = lib().oracle_fetch_cell(self._h, int(cell_index), out.ctypes.data)
+        if st != 0:
+            raise RuntimeError(f"oracle_fetch_cell failed {st}")
+        return out[0]
 
     def fetch_listeners(self) -> np.ndarray:
         out = np.zeros(max(self.L, 1))

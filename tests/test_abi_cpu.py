@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol(fdtd_lib):
 
 
 def test_abi_version(fdtd_lib):
-    assert fdtd_lib.fdtd_abi_version() == 4
+    assert fdtd_lib.fdtd_abi_version() == 5
 
 
 def test_struct_layouts_match_header(tmp_path):
@@ -63,6 +63,21 @@ int main(void) {
     assert offs == [S.SceneDesc.objects.offset, S.SceneDesc.listeners.offset, S.ObjectDesc.gravity.offset,
                     S.SolverInfo.algorithmic_bytes_per_step.offset]
     assert S.GHOST_FACE_DTYPE.itemsize == C.sizeof(S.GhostFace)
+
+
+def test_cell_dtype_matches_header(tmp_path):
+    """fdtd_cell (FetchCell / SampleAxisAlignedSlice) against CELL_DTYPE, field by field."""
+    fields = list(S.CELL_DTYPE.names)
+    prog = tmp_path / "cell.c"
+    prog.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"fdtd_c.h\"\nint main(void) {\n"
+                    + '  printf("%zu\\n", sizeof(fdtd_cell));\n'
+                    + "".join(f'  printf("%zu\\n", offsetof(fdtd_cell, {f}));\n' for f in fields)
+                    + "  return 0;\n}\n")
+    exe = tmp_path / "cell"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(prog), "-o", str(exe)], check=True)
+    out = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()]
+    assert out[0] == S.CELL_DTYPE.itemsize
+    assert out[1:] == [S.CELL_DTYPE.fields[f][1] for f in fields]
 
 
 def test_gaussian_source_defaults(fdtd_lib):
