@@ -451,10 +451,10 @@ fdtd_status fdtd_solver_time_kernel(fdtd_solver* s, int32_t which, int32_t n_lau
  * static device array of FDTD_NOALLOC_MAX_CELLS doubles (8 MiB) that every GPU
  * loading the library keeps until exit.  The first call on a device (and the
  * first after a device reset gave it a new context) looks up that array's
- * device address (cudaGetSymbolAddress) with the device current.  Calls share
- * the array, so calls that overlap on the GPU race; serialise them on one
- * stream.  `stream` is a cudaStream_t (NULL: the legacy default stream); the
- * call only enqueues work. */
+ * device address (cudaGetSymbolAddress) with the device current; make that
+ * first call before any stream capture.  Calls share the array, so calls that
+ * overlap on the GPU race; serialise them on one stream.  `stream` is a
+ * cudaStream_t (NULL: the legacy default stream); the call only enqueues work. */
 #define FDTD_NOALLOC_MAX_CELLS (1 << 20)
 fdtd_status fdtd_interior_step_noalloc(const double* p_curr, const double* p_prev, double* p_next,
                                        const int32_t dims[3], const int32_t lo[3], const int32_t hi[3],
