@@ -36,7 +36,7 @@ EXPORTS = [
     "fdtd_server_create", "fdtd_server_submit", "fdtd_server_poll", "fdtd_server_wait", "fdtd_server_result",
     "fdtd_server_drain", "fdtd_server_stats_get", "fdtd_server_request_error", "fdtd_server_destroy",
     "fdtd_server_cancel", "fdtd_batch_member_snapshot", "fdtd_batch_add_snapshot",
-    "fdtd_solver_fetch_cell", "fdtd_solver_sample_slice",
+    "fdtd_solver_fetch_cell", "fdtd_solver_sample_slice", "fdtd_solver_domain",
 ]
 
 _lib = None
@@ -92,6 +92,7 @@ def load(build_if_missing: bool = False):
         "fdtd_solver_prepare_graphs": ([vp], i32),
         "fdtd_solver_set_field": ([vp, i32, vp, i64], i32),
         "fdtd_solver_fetch_cell": ([vp, i64, vp], i32),
+        "fdtd_solver_domain": ([vp, vp, vp], i32),
         "fdtd_solver_sample_slice": ([vp, i32, dbl, vp, i64, C.POINTER(i64)], i32),
         "fdtd_matrix_write": ([C.c_char_p, i32, i32, vp], i32),
         "fdtd_matrix_read": ([C.c_char_p, C.POINTER(i32), C.POINTER(i32), vp, i64], i32),

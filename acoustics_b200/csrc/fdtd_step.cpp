@@ -912,6 +912,15 @@ fdtd_status fdtd_solver_set_field(fdtd_solver* s, int32_t which, const double* i
     return field_transfer(s, which, const_cast<double*>(in), count, true);
 }
 
+fdtd_status fdtd_solver_domain(fdtd_solver* s, double min_bound[3], double max_bound[3]) {
+    if (!s || !min_bound || !max_bound) return FDTD_ERR_INVALID_ARG;
+    for (int d = 0; d < 3; ++d) {
+        min_bound[d] = s->bmin[d];
+        max_bound[d] = s->bmax[d];
+    }
+    return FDTD_OK;
+}
+
 fdtd_status fdtd_solver_fetch_cell(fdtd_solver* s, int64_t cell_index, fdtd_cell* out) {
     if (!s || !out) return FDTD_ERR_INVALID_ARG;
     if (cell_index < 0 || cell_index >= s->ncell)

@@ -152,6 +152,12 @@ class PML_WaveSolver:
         check(self._L.fdtd_solver_get_classification(self._h, None, faces.ctypes.data, C.byref(cap)), self._h)
         return flags, faces
 
+    def GetSolverDomain(self):
+        """(min_bound, max_bound) of the pressure grid (PML_WaveSolver.cpp:458-471)."""
+        lo, hi = np.zeros(3), np.zeros(3)
+        check(self._L.fdtd_solver_domain(self._h, lo.ctypes.data, hi.ctypes.data), self._h)
+        return lo, hi
+
     def FetchCell(self, cell_index: int) -> np.void:
         """One cell as MAC_Grid::GetCell fills it, plus the stored Laplacian
         (PML_WaveSolver.cpp:439-447); a record of CELL_DTYPE."""

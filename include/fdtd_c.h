@@ -350,6 +350,9 @@ fdtd_status fdtd_solver_get_field(fdtd_solver* s, int32_t which, double* out, in
  * current pressure, so set FDTD_FIELD_PRESSURE first.  Split pressures and
  * velocities need the full PML state (FDTD_ERR_UNSUPPORTED on the reduced one). */
 fdtd_status fdtd_solver_set_field(fdtd_solver* s, int32_t which, const double* in, int64_t count);
+/* PML_WaveSolver::GetSolverDomain / GetSolverBBox (PML_WaveSolver.cpp:458-471): the
+ * pressure grid's bounding box, min_bound + h * divisions = max_bound. */
+fdtd_status fdtd_solver_domain(fdtd_solver* s, double min_bound[3], double max_bound[3]);
 /* PML_WaveSolver::FetchCell (PML_WaveSolver.cpp:439-447): cell cell_index (flat, in
  * [0, n_cells)) at the current state. */
 fdtd_status fdtd_solver_fetch_cell(fdtd_solver* s, int64_t cell_index, fdtd_cell* out);

@@ -208,3 +208,17 @@ def test_fetch_arguments(fdtd_lib):
     buf = np.zeros(n.value, dtype=S.CELL_DTYPE)
     assert fdtd_lib.fdtd_solver_sample_slice(g._h, 1, C.c_double(0.0), buf.ctypes.data, n.value - 1,
                                              C.byref(n)) == -1
+
+
+def test_solver_domain(fdtd_lib):
+    """GetSolverDomain: the grid's box, consistent with the cells' corners."""
+    sc = scene()
+    g = PML_WaveSolver(sc)
+    lo, hi = g.GetSolverDomain()
+    N, h = np.asarray(sc.divisions), sc.cell_size
+    assert np.array_equal(lo, -(h * N) / 2.0)
+    assert np.allclose(hi, lo + h * N, rtol=0, atol=1e-15)
+    first = g.FetchCell(0)
+    last = g.FetchCell(g.n_cells - 1)
+    assert np.allclose(first["lower_corner"], lo, rtol=0, atol=1e-15)
+    assert np.allclose(last["upper_corner"], hi, rtol=0, atol=1e-15)
