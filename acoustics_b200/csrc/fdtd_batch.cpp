@@ -49,6 +49,11 @@ struct fdtd_batch {
     int precision = 0;
     cudaStream_t stream = nullptr, stream2 = nullptr, stream3 = nullptr;
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_ghost = nullptr;
+    // listener rows of a step run on stream4 beside the next step; the advance of
+    // the next step (and with it every later kernel) waits on ev_lis[table of the step]
+    cudaStream_t stream4 = nullptr;
+    cudaEvent_t ev_step = nullptr, ev_lis[2] = {nullptr, nullptr}, ev_lis_join = nullptr;
+    bool lis_pending[2] = {false, false};
     std::vector<Member> members;
     // device tables
     void* d_descs = nullptr;
@@ -234,16 +239,39 @@ fdtd_status rebuild(fdtd_batch* b) {
 fdtd_status enqueue(fdtd_batch* b) {
     int l = 0;
     BatchLaunch L = b->L;
-    L.descs = static_cast<char*>(b->d_descs) + b->flip * b->table_bytes;
-    L.descs_other = static_cast<char*>(b->d_descs) + (b->flip ^ 1) * b->table_bytes;
+    const int p = b->flip;  // table of this step
+    L.descs = static_cast<char*>(b->d_descs) + p * b->table_bytes;
+    L.descs_other = static_cast<char*>(b->d_descs) + (p ^ 1) * b->table_bytes;
     b->flip ^= 1;
     const StepStreams SS{b->stream, b->stream2, b->stream3, b->ev_fork, b->ev_join, b->ev_ghost};
     cudaError_t e = b->precision == FDTD_PRECISION_FP64
                         ? launch_batch_fp64(L, SS, &l)
                         : launch_batch_fp32(L, SS, &l);
-    if (e == cudaSuccess) e = launch_batch_tail_any(b->precision, L, b->stream, &l);
+    // listener rows of this step beside the next step
+    const bool rows = L.n_refs > 0;
+    if (e == cudaSuccess && rows) e = cudaEventRecord(b->ev_step, b->stream);
+    if (e == cudaSuccess && rows) e = cudaStreamWaitEvent(b->stream4, b->ev_step, 0);
+    if (e == cudaSuccess && rows) e = launch_batch_listeners_any(b->precision, L, b->stream4, &l);
+    if (e == cudaSuccess && rows) e = cudaEventRecord(b->ev_lis[p], b->stream4);
+    // the rows of the step before read the pressure the next step overwrites and
+    // the table this step's advance marks halted members in
+    if (e == cudaSuccess && b->lis_pending[p ^ 1]) {
+        e = cudaStreamWaitEvent(b->stream, b->ev_lis[p ^ 1], 0);
+        b->lis_pending[p ^ 1] = false;
+    }
+    if (rows) b->lis_pending[p] = true;
+    if (e == cudaSuccess) e = launch_batch_advance_any(b->precision, L, b->stream, &l);
     b->launches += l;
     if (e != cudaSuccess) return batch_fail(b, FDTD_ERR_CUDA, std::string("batch launch: ") + cudaGetErrorString(e));
+    return FDTD_OK;
+}
+
+// Make the batch stream wait for every listener launch on stream4.
+fdtd_status join_listeners(fdtd_batch* b) {
+    if (!b->lis_pending[0] && !b->lis_pending[1]) return FDTD_OK;
+    BATCH_TRY(b, cudaEventRecord(b->ev_lis_join, b->stream4));
+    BATCH_TRY(b, cudaStreamWaitEvent(b->stream, b->ev_lis_join, 0));
+    b->lis_pending[0] = b->lis_pending[1] = false;
     return FDTD_OK;
 }
 
@@ -251,10 +279,13 @@ fdtd_status enqueue(fdtd_batch* b) {
 fdtd_status capture(fdtd_batch* b, int n) {
     cudaGraph_t g = nullptr;
     const int f0 = b->flip;
+    fdtd_status st = join_listeners(b);  // no dependency on work outside the capture
+    if (st != FDTD_OK) return st;
     BATCH_TRY(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     const long long l0 = b->launches;
-    fdtd_status st = FDTD_OK;
     for (int i = 0; i < n && st == FDTD_OK; ++i) st = enqueue(b);
+    if (st == FDTD_OK) st = join_listeners(b);  // the graph ends with every row written
+    b->lis_pending[0] = b->lis_pending[1] = false;
     cudaError_t e = cudaStreamEndCapture(b->stream, &g);
     b->graph_launches = b->launches - l0;
     b->launches = l0;
@@ -312,6 +343,11 @@ fdtd_status fdtd_batch_create(int32_t n, const fdtd_scene_desc* scenes, const in
     if (b->precision == FDTD_PRECISION_FP32_COMPENSATED) BATCH_TRY(nullptr, prepare_fp32_kernels());
     BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
     BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
+    BATCH_TRY(nullptr, cudaStreamCreateWithFlags(&b->stream4, cudaStreamNonBlocking));
+    BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_step, cudaEventDisableTiming));
+    BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_lis[0], cudaEventDisableTiming));
+    BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_lis[1], cudaEventDisableTiming));
+    BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_lis_join, cudaEventDisableTiming));
     for (int i = 0; i < n; ++i) {
         int32_t id;
         fdtd_status st = fdtd_batch_add(b.get(), &scenes[i], steps[i], &id);
@@ -483,6 +519,8 @@ fdtd_status fdtd_batch_step(fdtd_batch* b, int32_t n_steps, int32_t* n_active) {
             }
         }
         // rows, host mirrors, retirement
+        fdtd_status jst = join_listeners(b);
+        if (jst != FDTD_OK) return jst;
         std::vector<int> errs(b->members.size(), 0);
         for (size_t m = 0; m < b->members.size(); ++m) {
             Member& mb = b->members[m];
@@ -576,6 +614,7 @@ fdtd_status fdtd_batch_destroy(fdtd_batch* b) {
     if (!b) return FDTD_OK;
     cudaSetDevice(b->opt.device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->stream4) cudaStreamSynchronize(b->stream4);
     for (int i = 0; i < 2; ++i)
         if (b->graph[i]) cudaGraphExecDestroy(b->graph[i]);
     for (auto& mb : b->members)
@@ -587,6 +626,9 @@ fdtd_status fdtd_batch_destroy(fdtd_batch* b) {
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
     if (b->ev_ghost) cudaEventDestroy(b->ev_ghost);
+    for (cudaEvent_t ev : {b->ev_step, b->ev_lis[0], b->ev_lis[1], b->ev_lis_join})
+        if (ev) cudaEventDestroy(ev);
+    if (b->stream4) cudaStreamDestroy(b->stream4);
     if (b->stream2) cudaStreamDestroy(b->stream2);
     if (b->stream3) cudaStreamDestroy(b->stream3);
     if (b->stream) cudaStreamDestroy(b->stream);

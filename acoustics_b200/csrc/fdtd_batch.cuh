@@ -10,8 +10,8 @@
 // Per step:  k_batch_ghost (third stream)  ||  k_batch_interior (second stream)
 //            ||  k_batch_shell_red / k_batch_shell (PML tiles of the members with
 //            the reduced / full PML state), then k_batch_sources (second
-//            stream, after the ghost list), then k_batch_listeners and
-//            k_batch_advance (launch_batch_tail).
+//            stream, after the ghost list), then k_batch_advance; the listener
+//            rows (k_batch_listeners) on a fourth stream beside the next step.
 // The descriptors come in two tables, one per step parity (every member's
 // parity flips each step), so consecutive steps alternate tables and no kernel
 // flips parities on the device.
@@ -26,17 +26,42 @@
 
 namespace fdtd {
 
-// One CTA per tile of the tables (all members in one launch).  The member's
-// arguments are read through references into its descriptor in global memory
-// (L1-resident after the first warp), so a CTA starts without a barrier.
+#ifndef FDTD_BATCH_INT_TILES
+#define FDTD_BATCH_INT_TILES 4
+#endif
+
+// FDTD_BATCH_INT_TILES consecutive interior tiles per CTA.  The tiles are sorted
+// by member, so a CTA copies its member's arguments into registers once for the
+// tiles that share it: only the first waits on the chain tile -> descriptor ->
+// arguments before its data loads can issue.
 template <typename T, int XB>
-__global__ void __launch_bounds__(256) k_batch_interior(const BatchDesc<T>* __restrict__ D,
-                                                        const BatchTile* __restrict__ tiles) {
-    const BatchTile tile = tiles[blockIdx.x];
-    const BatchDesc<T>& d = D[tile.m];
-    if (d.halted) return;
-    interior_tile<T, XB>(d.a[d.cur], d.interior, tile.tz, tile.tx);
+__global__ void __launch_bounds__(256, XB == 2 ? 4 : 1) k_batch_interior(const BatchDesc<T>* __restrict__ D,
+                                                                         const BatchTile* __restrict__ tiles,
+                                                                         int n_tiles) {
+    constexpr int K = FDTD_BATCH_INT_TILES;
+    int m = -1;
+    bool halted = true;
+    KArgs<T> A;
+    Box3 box;
+#pragma unroll 1
+    for (int k = 0; k < K; ++k) {
+        const int t = blockIdx.x * K + k;
+        if (t >= n_tiles) break;  // uniform per CTA
+        const BatchTile tile = tiles[t];
+        if (tile.m != m) {
+            m = tile.m;
+            const BatchDesc<T>& d = D[m];
+            halted = d.halted != 0;
+            A = d.a[d.cur];
+            box = d.interior;
+        }
+        if (!halted) interior_tile<T, XB>(A, box, tile.tz, tile.tx);
+    }
 }
+
+// One CTA per shell tile of the tables (all members in one launch).  The
+// member's arguments are read through references into its descriptor in global
+// memory (L1-resident after the first warp), so a CTA starts without a barrier.
 
 template <typename T>
 __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_batch_shell(const BatchDesc<T>* __restrict__ D,
@@ -55,7 +80,8 @@ __global__ void __launch_bounds__(256, FDTD_SHELL_RED_MINB) k_batch_shell_red(co
     const BatchTile tile = tiles[blockIdx.x];
     const BatchDesc<T>& d = D[tile.m];
     if (d.halted) return;
-    shell_tile_red(d.a[d.cur], d.shell, tile.box, tile.tz, tile.tx);
+    const KArgs<float> A = d.a[d.cur];  // in registers: the plane loop reads them every plane
+    shell_tile_red(A, d.shell, tile.box, tile.tz, tile.tx);
 }
 
 // grid (solid_blocks, members): re-zero the solid cells inside the PML of the
@@ -135,9 +161,10 @@ cudaError_t launch_batch(const BatchLaunch& L, const StepStreams& S, int* launch
     }
     if (L.n_int > 0) {
         const dim3 block(32, 8);
-        if (L.xb == 2) k_batch_interior<T, 2><<<L.n_int, block, 0, S.s2>>>(D, L.int_tiles);
-        else if (L.xb == 8) k_batch_interior<T, 8><<<L.n_int, block, 0, S.s2>>>(D, L.int_tiles);
-        else k_batch_interior<T, 4><<<L.n_int, block, 0, S.s2>>>(D, L.int_tiles);
+        const unsigned grid = (unsigned)((L.n_int + FDTD_BATCH_INT_TILES - 1) / FDTD_BATCH_INT_TILES);
+        if (L.xb == 2) k_batch_interior<T, 2><<<grid, block, 0, S.s2>>>(D, L.int_tiles, L.n_int);
+        else if (L.xb == 8) k_batch_interior<T, 8><<<grid, block, 0, S.s2>>>(D, L.int_tiles, L.n_int);
+        else k_batch_interior<T, 4><<<grid, block, 0, S.s2>>>(D, L.int_tiles, L.n_int);
         ++l;
     }
     int n_red = 0;
@@ -168,23 +195,27 @@ cudaError_t launch_batch(const BatchLaunch& L, const StepStreams& S, int* launch
 
 // Last kernel of a batched step, one thread per member: write the member's
 // constants of the next step (consts[cur ^ 1]) and, after its last step, mark
-// it halted in both descriptor tables, so its kernels leave at once from the
-// next step on whatever the parity of the table (the tables alternate every
-// step, a halted member's state no longer does).  Members retire without a new
-// tile table or graph.
+// it halted, so its kernels leave at once from the next step on (the tables
+// alternate every step, a halted member's state no longer does).  The flag goes
+// into the next step's table D2 first and into this step's table D one step
+// later, by this kernel of the next step: the listener rows of this step, which
+// run beside the next step and read D, still see the member running.  (That
+// kernel of the next step waits for them.)  Members retire without a new tile
+// table or graph.
 template <typename T>
 __global__ void __launch_bounds__(128) k_batch_advance(BatchDesc<T>* __restrict__ D, BatchDesc<T>* __restrict__ D2,
                                                        int n) {
     const int m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= n) return;
     const BatchDesc<T>& d = D[m];
-    if (!d.active || d.halted) return;
+    if (!d.active) return;
+    if (d.halted) {
+        D2[m].halted = 1;
+        return;
+    }
     const long long step = d.P->consts[d.cur].step;
     advance_consts(*d.P, d.cur);
-    if (step + 1 >= d.total) {
-        D[m].halted = 1;
-        D2[m].halted = 1;
-    }
+    if (step + 1 >= d.total) D2[m].halted = 1;
 }
 
 // Listener rows of a batched step.  Instantiated in the FP64 translation unit
@@ -192,12 +223,18 @@ __global__ void __launch_bounds__(128) k_batch_advance(BatchDesc<T>* __restrict_
 // double-precision MLS arithmetic is compiled the same way (no FMA
 // contraction) and batch rows equal single-solve rows bit for bit.
 template <typename T>
-cudaError_t launch_batch_tail(const BatchLaunch& L, cudaStream_t s, int* launches) {
+cudaError_t launch_batch_listeners(const BatchLaunch& L, cudaStream_t s, int* launches) {
     BatchDesc<T>* D = static_cast<BatchDesc<T>*>(L.descs);
     if (L.n_refs > 0) {
         k_batch_listeners<T><<<(L.n_refs * 32 + 127) / 128, 128, 0, s>>>(D, L.refs, L.n_refs);
         if (launches) *launches += 1;
     }
+    return cudaGetLastError();
+}
+
+template <typename T>
+cudaError_t launch_batch_advance(const BatchLaunch& L, cudaStream_t s, int* launches) {
+    BatchDesc<T>* D = static_cast<BatchDesc<T>*>(L.descs);
     if (L.n_members > 0) {
         k_batch_advance<T><<<(L.n_members + 127) / 128, 128, 0, s>>>(D, static_cast<BatchDesc<T>*>(L.descs_other),
                                                                       L.n_members);

@@ -957,7 +957,10 @@ namespace fdtd {
 cudaError_t launch_batch_fp64(const BatchLaunch& L, const StepStreams& S, int* launches) {
     return launch_batch<double>(L, S, launches);
 }
-cudaError_t launch_batch_tail_any(int precision, const BatchLaunch& L, cudaStream_t s, int* launches) {
-    return precision == 0 ? launch_batch_tail<double>(L, s, launches) : launch_batch_tail<float>(L, s, launches);
+cudaError_t launch_batch_listeners_any(int precision, const BatchLaunch& L, cudaStream_t s, int* launches) {
+    return precision == 0 ? launch_batch_listeners<double>(L, s, launches) : launch_batch_listeners<float>(L, s, launches);
+}
+cudaError_t launch_batch_advance_any(int precision, const BatchLaunch& L, cudaStream_t s, int* launches) {
+    return precision == 0 ? launch_batch_advance<double>(L, s, launches) : launch_batch_advance<float>(L, s, launches);
 }
 }  // namespace fdtd

@@ -24,8 +24,9 @@ cudaError_t launch_step_regions_fp32(const SolveParams* dP, const SolveParams& h
 // batched step of many members (fdtd_batch.cuh)
 cudaError_t launch_batch_fp64(const BatchLaunch& L, const StepStreams& S, int* launches);
 cudaError_t launch_batch_fp32(const BatchLaunch& L, const StepStreams& S, int* launches);
-// listener rows + advance of a batched step, for either field type (FP64 unit)
-cudaError_t launch_batch_tail_any(int precision, const BatchLaunch& L, cudaStream_t s, int* launches);
+// listener rows / advance of a batched step, for either field type (FP64 unit)
+cudaError_t launch_batch_listeners_any(int precision, const BatchLaunch& L, cudaStream_t s, int* launches);
+cudaError_t launch_batch_advance_any(int precision, const BatchLaunch& L, cudaStream_t s, int* launches);
 
 // fdtd_fp64.cu (compiled with -fmad=false)
 cudaError_t launch_prologue_fp64(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s);
