@@ -34,8 +34,11 @@ namespace fdtd {
 // by member, so a CTA copies its member's arguments into registers once for the
 // tiles that share it: only the first waits on the chain tile -> descriptor ->
 // arguments before its data loads can issue.
+#ifndef FDTD_BATCH_INT_MINB
+#define FDTD_BATCH_INT_MINB 3
+#endif
 template <typename T, int XB>
-__global__ void __launch_bounds__(256, XB == 2 ? 4 : 1) k_batch_interior(const BatchDesc<T>* __restrict__ D,
+__global__ void __launch_bounds__(256, XB == 2 ? FDTD_BATCH_INT_MINB : 1) k_batch_interior(const BatchDesc<T>* __restrict__ D,
                                                                          const BatchTile* __restrict__ tiles,
                                                                          int n_tiles) {
     constexpr int K = FDTD_BATCH_INT_TILES;
