@@ -95,7 +95,11 @@ struct KeptArena {
 };
 std::mutex g_arena_mu;
 std::vector<KeptArena> g_arenas;  // oldest first
-constexpr size_t ARENAS_KEPT = 8;
+// kept blocks per process: at most this many and this many bytes (a destroy that
+// pushes past a limit frees the oldest blocks, which is where cudaFree's cost
+// returns, so the limits sit above what a server's or a benchmark's churn keeps)
+constexpr size_t ARENAS_KEPT = 256;
+constexpr size_t ARENAS_KEPT_BYTES = (size_t)16 << 30;
 
 void free_kept(int device) {
     std::vector<KeptArena> drop;
@@ -143,20 +147,25 @@ cudaError_t arena_acquire(int device, size_t bytes, void** ptr, size_t* block_by
 
 void arena_release(int device, void* ptr, size_t block_bytes) {
     if (!ptr) return;
-    KeptArena drop{-1, nullptr, 0};
+    std::vector<KeptArena> drop;
     {
         std::lock_guard<std::mutex> lk(g_arena_mu);
         g_arenas.push_back({device, ptr, block_bytes});
-        if (g_arenas.size() > ARENAS_KEPT) {
-            drop = g_arenas.front();
+        size_t total = 0;
+        for (const auto& a : g_arenas) total += a.bytes;
+        while (g_arenas.size() > 1 && (g_arenas.size() > ARENAS_KEPT || total > ARENAS_KEPT_BYTES)) {
+            total -= g_arenas.front().bytes;
+            drop.push_back(g_arenas.front());
             g_arenas.erase(g_arenas.begin());
         }
     }
-    if (drop.ptr) {
+    if (!drop.empty()) {
         int cur = -1;
         cudaGetDevice(&cur);
-        cudaSetDevice(drop.device);
-        cudaFree(drop.ptr);
+        for (const auto& a : drop) {
+            cudaSetDevice(a.device);
+            cudaFree(a.ptr);
+        }
         if (cur >= 0) cudaSetDevice(cur);
     }
 }

@@ -320,7 +320,8 @@ fdtd_status fdtd_gaussian_source_defaults(fdtd_gaussian_source_desc* src, double
 fdtd_status fdtd_solver_create(const fdtd_scene_desc* scene, const fdtd_options* options,
                                fdtd_solver** out);
 /* Releases the solver's streams and events; its device block is kept for the next
- * solver created on the same device (freed when an allocation would fail, or by
+ * solver created on the same device (freed when an allocation would fail, when the
+ * kept blocks pass 16 GiB or 256 blocks, oldest first, or by
  * fdtd_release_cached_memory). */
 fdtd_status fdtd_solver_destroy(fdtd_solver* s);
 /* Free the device blocks kept from destroyed solvers: of one device, or of all (device < 0). */
