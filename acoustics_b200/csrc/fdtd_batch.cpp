@@ -54,6 +54,11 @@ struct fdtd_batch {
     cudaStream_t stream4 = nullptr;
     cudaEvent_t ev_step = nullptr, ev_lis[2] = {nullptr, nullptr}, ev_lis_join = nullptr;
     bool lis_pending[2] = {false, false};
+    // the interior arguments in the kernel's parameter bank, one table per step
+    // parity (BatchIntParams<T>); empty when more members have interior tiles
+    // than the table holds (the tile table path then)
+    std::vector<char> int_params[2];
+    int int_ctas = 0;
     std::vector<Member> members;
     // device tables
     void* d_descs = nullptr;
@@ -134,6 +139,40 @@ fdtd_status grow(fdtd_batch* b, T** ptr, size_t* cap, size_t need) {
     return FDTD_OK;
 }
 
+// Interior entries of the parameter-bank table: (descriptor index, unit tiles, x tiles).
+struct IntEntry {
+    int m, tu, tx;
+};
+
+template <typename T>
+int fill_int_params(std::vector<char>& buf, const char* table, size_t dsz, const std::vector<IntEntry>& list) {
+    buf.assign(sizeof(BatchIntParams<T>), 0);
+    BatchIntParams<T>& P = *reinterpret_cast<BatchIntParams<T>*>(buf.data());
+    P.n = (int)list.size();
+    int ctas = 0;
+    for (size_t i = 0; i < list.size(); ++i) {
+        const BatchDesc<T>& d = *reinterpret_cast<const BatchDesc<T>*>(table + (size_t)list[i].m * dsz);
+        const KArgs<T>& A = d.a[d.cur];
+        BatchIntMember<T>& M = P.m[i];
+        M.pc = A.pc;
+        M.pn = A.pn;
+        M.dinc = A.dinc;
+        M.cls = A.cls;
+        M.sx = A.sx;
+        M.sy = A.sy;
+        M.c2k2 = A.c2k2;
+        M.lap_scale = A.lap_scale;
+        M.kcalp = A.kcalp;
+        M.box = d.interior;
+        M.tu = list[i].tu;
+        M.member = list[i].m;
+        P.first[i] = ctas;
+        ctas += list[i].tu * list[i].tx;
+    }
+    P.first[list.size()] = ctas;
+    return ctas;
+}
+
 // Rebuild descriptors and tile tables after a membership change.
 fdtd_status rebuild(fdtd_batch* b) {
     const bool f64 = b->precision == FDTD_PRECISION_FP64;
@@ -144,6 +183,7 @@ fdtd_status rebuild(fdtd_batch* b) {
     const size_t tbytes = std::max<size_t>(nm, 1) * dsz;
     std::vector<char> descs(2 * tbytes, 0);
     std::vector<BatchTile> it, st, st_full;
+    std::vector<IntEntry> int_list;
     std::vector<ListenerRef> refs;
     int max_ghost = 0, max_src = 0, max_solid = 0;
     for (size_t m = 0; m < nm; ++m) {
@@ -171,6 +211,7 @@ fdtd_status rebuild(fdtd_batch* b) {
             const int tu = interior_unit_tiles(I, f64 ? 2 : 4), tx = (nx + xb - 1) / xb;
             for (int x = 0; x < tx; ++x)
                 for (int u = 0; u < tu; ++u) it.push_back({(int)m, 0, u, 0, x});
+            if (tu > 0 && tx > 0) int_list.push_back({(int)m, tu, tx});
         }
         const ShellBoxes& B = mb.s->shell;
         // members with the reduced PML state come first in the shell table
@@ -215,6 +256,12 @@ fdtd_status rebuild(fdtd_batch* b) {
     b->flip = 0;
     L.int_tiles = b->d_int;
     L.n_int = (int)it.size();
+    b->int_ctas = 0;
+    for (int par = 0; par < 2; ++par) b->int_params[par].clear();
+    if (!int_list.empty() && int_list.size() <= (size_t)BATCH_PARAM_MEMBERS)
+        for (int par = 0; par < 2; ++par)
+            b->int_ctas = f64 ? fill_int_params<double>(b->int_params[par], &descs[par * tbytes], dsz, int_list)
+                              : fill_int_params<float>(b->int_params[par], &descs[par * tbytes], dsz, int_list);
     b->table_tiles = (int64_t)(it.size() + st.size());
     L.shell_tiles = b->d_shell;
     L.n_shell = (int)st.size();
@@ -241,6 +288,8 @@ fdtd_status enqueue(fdtd_batch* b) {
     BatchLaunch L = b->L;
     const int p = b->flip;  // table of this step
     L.descs = static_cast<char*>(b->d_descs) + p * b->table_bytes;
+    L.int_params = b->int_params[p].empty() ? nullptr : b->int_params[p].data();
+    L.int_ctas = b->int_ctas;
     L.descs_other = static_cast<char*>(b->d_descs) + (p ^ 1) * b->table_bytes;
     b->flip ^= 1;
     const StepStreams SS{b->stream, b->stream2, b->stream3, b->ev_fork, b->ev_join, b->ev_ghost};

@@ -62,6 +62,25 @@ __global__ void __launch_bounds__(256, XB == 2 ? FDTD_BATCH_INT_MINB : 1) k_batc
     }
 }
 
+// One CTA per interior tile, its member found by a binary search of the
+// parameter-bank table from blockIdx alone (warp-uniform, like its arguments);
+// a member's CTAs enumerate its tiles as the tile table does (x tile outer).
+template <typename T, int XB>
+__global__ void __launch_bounds__(256, XB == 2 ? 4 : 1)
+    k_batch_interior_p(const __grid_constant__ BatchIntParams<T> P, const BatchDesc<T>* __restrict__ D) {
+    const int blk = (int)blockIdx.x;
+    int lo = 0, hi = P.n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (P.first[mid] <= blk) lo = mid;
+        else hi = mid - 1;
+    }
+    const BatchIntMember<T>& M = P.m[lo];
+    if (D[M.member].halted) return;
+    const int local = blk - P.first[lo];
+    interior_tile<T, XB>(M, M.box, local % M.tu, local / M.tu);
+}
+
 // One CTA per shell tile of the tables (all members in one launch).  The
 // member's arguments are read through references into its descriptor in global
 // memory (L1-resident after the first warp), so a CTA starts without a barrier.
@@ -162,7 +181,14 @@ cudaError_t launch_batch(const BatchLaunch& L, const StepStreams& S, int* launch
         ++l;
         if (gside && (e = cudaEventRecord(S.ghost, S.s3)) != cudaSuccess) return e;
     }
-    if (L.n_int > 0) {
+    if (L.int_params && L.int_ctas > 0) {
+        const dim3 block(32, 8);
+        const BatchIntParams<T>& P = *static_cast<const BatchIntParams<T>*>(L.int_params);
+        if (L.xb == 2) k_batch_interior_p<T, 2><<<L.int_ctas, block, 0, S.s2>>>(P, D);
+        else if (L.xb == 8) k_batch_interior_p<T, 8><<<L.int_ctas, block, 0, S.s2>>>(P, D);
+        else k_batch_interior_p<T, 4><<<L.int_ctas, block, 0, S.s2>>>(P, D);
+        ++l;
+    } else if (L.n_int > 0) {
         const dim3 block(32, 8);
         const unsigned grid = (unsigned)((L.n_int + FDTD_BATCH_INT_TILES - 1) / FDTD_BATCH_INT_TILES);
         if (L.xb == 2) k_batch_interior<T, 2><<<grid, block, 0, S.s2>>>(D, L.int_tiles, L.n_int);

@@ -439,7 +439,33 @@ struct ListenerRef {
     int m, li;
 };
 
+// The interior arguments of one batch member for one step parity: the fields
+// interior_tile reads, passed in the kernel's parameter bank
+// (k_batch_interior_p) so that, like the single-solve kernel's, they take no
+// per-thread registers.
+template <typename T>
+struct BatchIntMember {
+    const T* pc;
+    T* pn;
+    float* dinc;
+    const uint8_t* cls;
+    unsigned sx, sy;
+    T c2k2, lap_scale, kcalp;
+    Box3 box;
+    int tu;      // unit tiles per x-plane tile
+    int member;  // descriptor index
+};
+constexpr int BATCH_PARAM_MEMBERS = 160;
+template <typename T>
+struct BatchIntParams {
+    int n;                                // members listed
+    int first[BATCH_PARAM_MEMBERS + 1];   // first CTA of each listed member; first[n]: all CTAs
+    BatchIntMember<T> m[BATCH_PARAM_MEMBERS];
+};
+
 struct BatchLaunch {
+    const void* int_params;      // host BatchIntParams<T> of this step's parity, or null (tile table)
+    int int_ctas;
     void* descs;                 // BatchDesc<T>[n_members] on the device (table of this step's parity)
     void* descs_other;           // the other parity's table (k_batch_advance marks halted members in both)
     const BatchTile* int_tiles;

@@ -76,8 +76,8 @@ __device__ __forceinline__ void stv(T* p, const Vec<T, V>& v) {
 // shuffle when that lane holds the neighbouring group of the same row, else
 // from memory.  Cells of a group outside the box or not plain bulk are masked
 // (scalar stores for partial groups).  Every thread of the CTA must call it.
-template <typename T, int XB, bool VISC = false>
-__device__ __forceinline__ void interior_tile(const KArgs<T>& A, const Box3& box, int tu, int tx) {
+template <typename T, int XB, bool VISC = false, typename AT = KArgs<T>>
+__device__ __forceinline__ void interior_tile(const AT& A, const Box3& box, int tu, int tx) {
     constexpr bool COMP = sizeof(T) == 4;
     constexpr int V = 16 / (int)sizeof(T);
     using VT = Vec16<T>;
