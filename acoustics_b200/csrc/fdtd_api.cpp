@@ -985,6 +985,7 @@ fdtd_status fdtd_solver_create(const fdtd_scene_desc* sc, const fdtd_options* op
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_sfork, cudaEventDisableTiming));
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_sdone, cudaEventDisableTiming));
     if (s->precision == FDTD_PRECISION_FP32_COMPENSATED) CUDA_TRY(nullptr, prepare_fp32_kernels());
+    else CUDA_TRY(nullptr, prepare_fp64_kernels());
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_fork, cudaEventDisableTiming));
     CUDA_TRY(nullptr, cudaEventCreateWithFlags(&s->ev_join, cudaEventDisableTiming));
     solver_init_geometry(s.get(), sc);

@@ -390,6 +390,7 @@ fdtd_status fdtd_batch_create(int32_t n, const fdtd_scene_desc* scenes, const in
     BATCH_TRY(nullptr, cudaStreamCreateWithFlags(&b->stream3, cudaStreamNonBlocking));
     BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_ghost, cudaEventDisableTiming));
     if (b->precision == FDTD_PRECISION_FP32_COMPENSATED) BATCH_TRY(nullptr, prepare_fp32_kernels());
+    else BATCH_TRY(nullptr, prepare_fp64_kernels());
     BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming));
     BATCH_TRY(nullptr, cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming));
     BATCH_TRY(nullptr, cudaStreamCreateWithFlags(&b->stream4, cudaStreamNonBlocking));

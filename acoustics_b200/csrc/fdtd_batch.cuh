@@ -205,7 +205,7 @@ cudaError_t launch_batch(const BatchLaunch& L, const StepStreams& S, int* launch
         }
     }
     if (L.n_shell > n_red) {
-        k_batch_shell<T><<<L.n_shell - n_red, dim3(32, 8), 0, S.s>>>(D, L.shell_tiles + n_red);
+        k_batch_shell<T><<<L.n_shell - n_red, dim3(32, 8), shell_smem_bytes<T>(), S.s>>>(D, L.shell_tiles + n_red);
         ++l;
     }
     if (gside && (e = cudaStreamWaitEvent(S.s2, S.ghost, 0)) != cudaSuccess) return e;

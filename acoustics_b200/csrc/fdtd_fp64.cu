@@ -957,6 +957,18 @@ namespace fdtd {
 cudaError_t launch_batch_fp64(const BatchLaunch& L, const StepStreams& S, int* launches) {
     return launch_batch<double>(L, S, launches);
 }
+cudaError_t prepare_fp64_kernels() {
+    // the full-state shell's ring of staged loads
+    cudaError_t e = cudaSuccess;
+    if (shell_smem_bytes<double>() > 0) {
+        e = cudaFuncSetAttribute(k_pml_shell<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 shell_smem_bytes<double>());
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_batch_shell<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     shell_smem_bytes<double>());
+    }
+    return e;
+}
 cudaError_t launch_batch_listeners_any(int precision, const BatchLaunch& L, cudaStream_t s, int* launches) {
     return precision == 0 ? launch_batch_listeners<double>(L, s, launches) : launch_batch_listeners<float>(L, s, launches);
 }

@@ -232,6 +232,39 @@ __device__ __forceinline__ T* sh_vn(const KArgs<T>& A, int d) {
     return CMP ? A.zvn[d] : A.vn[d];
 }
 
+// Per-thread asynchronous copies (cp.async) into shared memory, for the rings
+// of staged shell loads: a thread reads back only what it copied, so no barrier.
+__device__ __forceinline__ int threadIdx_lin() { return threadIdx.x + 32 * threadIdx.y; }
+template <int BYTES>
+__device__ __forceinline__ void cpa(unsigned saddr, const void* g) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(saddr), "l"(g), "n"(BYTES) : "memory");
+}
+__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cpa_wait() {
+    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+// x planes of the full-state shell (FP64) whose loads a thread keeps in flight
+// through a shared-memory ring; 0: the register prefetch of FDTD_SHELL_PREFETCH.
+// FP32 full-state tiles keep the register prefetch.
+#ifndef FDTD_SHELL_F64_STAGES
+#define FDTD_SHELL_F64_STAGES 3
+#endif
+template <typename T>
+__host__ __device__ constexpr int shell_full_stages() {
+    return sizeof(T) == 8 ? FDTD_SHELL_F64_STAGES : 0;
+}
+// one stage: ten vector fields and three scalar fields, each over the CTA's 256 threads
+template <typename T>
+__host__ __device__ constexpr int shell_stage_bytes() {
+    return 256 * (10 * (int)sizeof(T) * shell_vz(sizeof(T)) + 3 * (int)sizeof(T));
+}
+template <typename T>
+__host__ __device__ constexpr int shell_smem_bytes() {
+    return shell_full_stages<T>() * shell_stage_bytes<T>();
+}
+
 // Strides and edge flags of the compact storage (CMP only).
 struct ShellStore {
     int sx, sy;         // plane and row strides of that storage
@@ -249,6 +282,64 @@ struct ShellPlane {
     AxisCoef<T> cxr;
     uint8_t g;
 };
+
+// The loads of shell_load as asynchronous copies into ring stage `st` (the
+// shared address of this thread's vector slot 0 of the stage): vector field f at
+// st + f * 256 * VB, scalar field k at this thread's word of the scalar arrays.
+template <typename T, int V, bool CMP>
+__device__ __forceinline__ void shell_stage(const KArgs<T>& A, const ShellStore& S, unsigned st, int x,
+                                            bool last_plane, unsigned c, unsigned q, int oym, int oyp, int ozm) {
+    constexpr int W = (int)sizeof(T), VB = W * V;
+    constexpr unsigned FV = 256 * VB, FS = 256 * W, S0 = 10 * FV;
+    const unsigned sc = st + S0 - (unsigned)((VB - W) * threadIdx_lin());  // scalar field 0 of this thread
+    const int sx = (int)A.sx, sy = (int)A.sy;
+    const T* pc = A.pc + c;
+    cpa<VB>(st + 0 * FV, pc + (x + 1 < A.N0 ? sx : 0));
+    cpa<VB>(st + 1 * FV, pc - oym);
+    cpa<VB>(st + 2 * FV, pc + oyp);
+    cpa<W>(sc + 0 * FS, pc - ozm);
+    cpa<W>(sc + 1 * FS, pc + V);
+    if constexpr (CMP) {
+        cpa<VB>(st + 3 * FV, last_plane ? A.vo[0] + c + sx : A.zvo[0] + q + S.sx);
+        cpa<VB>(st + 4 * FV, A.zvo[1] + q);
+        cpa<VB>(st + 5 * FV, S.y_hi_grid ? A.vo[1] + c + sy : A.zvo[1] + q + S.sy);
+        cpa<VB>(st + 6 * FV, A.zvo[2] + q);
+        cpa<W>(sc + 2 * FS, A.zvo[2] + q + (S.spare ? S.spare : V));
+    } else {
+        cpa<VB>(st + 3 * FV, A.vo[0] + c + sx);
+        cpa<VB>(st + 4 * FV, A.vo[1] + c);
+        cpa<VB>(st + 5 * FV, A.vo[1] + c + sy);
+        cpa<VB>(st + 6 * FV, A.vo[2] + c);
+        cpa<W>(sc + 2 * FS, A.vo[2] + c + V);
+    }
+    cpa<VB>(st + 7 * FV, sh_pd<T, CMP>(A, 0) + q);
+    cpa<VB>(st + 8 * FV, sh_pd<T, CMP>(A, 1) + q);
+    cpa<VB>(st + 9 * FV, sh_pd<T, CMP>(A, 2) + q);
+}
+
+// Read back a completed stage (`sp`: generic pointer to this thread's vector slot 0).
+template <typename T, int V>
+__device__ __forceinline__ void shell_unstage(const KArgs<T>& A, ShellPlane<T, V>& L, const char* sp, int x) {
+    constexpr int W = (int)sizeof(T), VB = W * V;
+    constexpr int FV = 256 * VB, FS = 256 * W, S0 = 10 * FV;
+    using VT = Vec<T, V>;
+    const char* sc = sp + S0 - (VB - W) * threadIdx_lin();
+    L.g = __ldg(A.axflag[0] + x);
+    L.cxr = A.coef[0][x + 1];
+    L.pp = *reinterpret_cast<const VT*>(sp + 0 * FV);
+    L.ym = *reinterpret_cast<const VT*>(sp + 1 * FV);
+    L.yp = *reinterpret_cast<const VT*>(sp + 2 * FV);
+    L.zme = *reinterpret_cast<const T*>(sc + 0 * FS);
+    L.zpe = *reinterpret_cast<const T*>(sc + 1 * FS);
+    L.vxr = *reinterpret_cast<const VT*>(sp + 3 * FV);
+    L.vyl = *reinterpret_cast<const VT*>(sp + 4 * FV);
+    L.vyr = *reinterpret_cast<const VT*>(sp + 5 * FV);
+    L.vzl = *reinterpret_cast<const VT*>(sp + 6 * FV);
+    L.vze = *reinterpret_cast<const T*>(sc + 2 * FS);
+    L.a0 = *reinterpret_cast<const VT*>(sp + 7 * FV);
+    L.a1 = *reinterpret_cast<const VT*>(sp + 8 * FV);
+    L.a2 = *reinterpret_cast<const VT*>(sp + 9 * FV);
+}
 
 template <typename T, int V, bool CMP>
 __device__ __forceinline__ void shell_load(const KArgs<T>& A, const ShellStore& S, ShellPlane<T, V>& L, int x,
@@ -352,12 +443,39 @@ __device__ __forceinline__ void shell_tile_impl(const KArgs<T>& A, const ShellBo
     VT vxl = ldv<T, V>(sh_vo<T, CMP>(A, 0) + q0);
     AxisCoef<T> cxl = A.coef[0][x0];
     ShellPlane<T, V> cur, nxt;
-    if constexpr (FDTD_SHELL_PREFETCH) shell_load<T, V, CMP>(A, S, cur, x0, x0 + 1 == xend, c0, q0, oym, oyp, ozm);
+    constexpr int NS = shell_full_stages<T>();
+    constexpr bool PF = NS == 0 && FDTD_SHELL_PREFETCH;
+    extern __shared__ __align__(16) char full_ring[];
+    char* const sp0 = full_ring + threadIdx_lin() * (int)sizeof(T) * V;
+    const unsigned ss0 = (unsigned)__cvta_generic_to_shared(sp0);
+    if constexpr (NS > 0) {
+#pragma unroll
+        for (int k = 0; k < NS - 1; ++k) {
+            if (x0 + k < x1)
+                shell_stage<T, V, CMP>(A, S, ss0 + k * shell_stage_bytes<T>(), x0 + k, x0 + k + 1 == xend,
+                                       c0 + (unsigned)k * A.sx, q0 + (unsigned)(k * S.sx), oym, oyp, ozm);
+            cpa_commit();
+        }
+    } else if constexpr (PF) {
+        shell_load<T, V, CMP>(A, S, cur, x0, x0 + 1 == xend, c0, q0, oym, oyp, ozm);
+    }
+    int ring = 0;  // stage of plane x
 #pragma unroll 1
     for (int x = x0; x < x1; ++x) {
         const unsigned c = c0 + (unsigned)(x - x0) * A.sx;
         const unsigned q = CMP ? q0 + (unsigned)(x - x0) * S.sx : c;
-        if constexpr (FDTD_SHELL_PREFETCH) {
+        if constexpr (NS > 0) {
+            // the stage of plane x + NS - 1 is the one plane x - 1 was read from
+            const int st = ring == 0 ? NS - 1 : ring - 1;
+            if (x + NS - 1 < x1)
+                shell_stage<T, V, CMP>(A, S, ss0 + st * shell_stage_bytes<T>(), x + NS - 1, x + NS == xend,
+                                       c + (unsigned)(NS - 1) * A.sx, q + (unsigned)((NS - 1) * S.sx), oym, oyp,
+                                       ozm);
+            cpa_commit();
+            cpa_wait<NS - 1>();
+            shell_unstage<T, V>(A, cur, sp0 + ring * shell_stage_bytes<T>(), x);
+            ring = ring == NS - 1 ? 0 : ring + 1;
+        } else if constexpr (PF) {
             if (x + 1 < x1) shell_load<T, V, CMP>(A, S, nxt, x + 1, x + 2 == xend, c + sx, q + S.sx, oym, oyp, ozm);
         } else {
             shell_load<T, V, CMP>(A, S, cur, x, x + 1 == xend, c, q, oym, oyp, ozm);
@@ -434,8 +552,9 @@ __device__ __forceinline__ void shell_tile_impl(const KArgs<T>& A, const ShellBo
         p0 = cur.pp;
         vxl = cur.vxr;
         cxl = cxr;
-        if constexpr (FDTD_SHELL_PREFETCH) cur = nxt;
+        if constexpr (PF) cur = nxt;
     }
+    if constexpr (NS > 0) cpa_wait<0>();  // no copy outlives the thread
 }
 
 template <typename T>
@@ -529,9 +648,9 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
                 k_pml_shell_tma<float><<<R.tma->grid, TMA_BLOCK, tma_smem_bytes(R.tma->launch), S.s>>>(
                     A, R.tma->launch, R.tma->d_tiles, R.tma->d_cta_first, R.tma->d_maps, hP.dev_error);
             else if (R.red) k_pml_shell_red<float><<<nblk, dim3(32, 8), red_smem_bytes(), S.s>>>(A, R.shell);
-            else k_pml_shell<T><<<nblk, dim3(32, 8), 0, S.s>>>(A, R.shell);
+            else k_pml_shell<T><<<nblk, dim3(32, 8), shell_smem_bytes<T>(), S.s>>>(A, R.shell);
         } else {
-            k_pml_shell<T><<<nblk, dim3(32, 8), 0, S.s>>>(A, R.shell);
+            k_pml_shell<T><<<nblk, dim3(32, 8), shell_smem_bytes<T>(), S.s>>>(A, R.shell);
         }
         ++l;
     }

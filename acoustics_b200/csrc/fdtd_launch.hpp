@@ -70,6 +70,8 @@ cudaError_t launch_fetch_cells(const SolveParams* dP, bool fp64, int cur, const 
 
 // fdtd_fp32.cu
 cudaError_t prepare_fp32_kernels();
+// fdtd_fp64.cu: shared-memory limits of the FP64 kernels that stage loads
+cudaError_t prepare_fp64_kernels();
 cudaError_t launch_prologue_fp32(const SolveParams* dP, int cur, int advance, int n_solid_pml, cudaStream_t s);
 
 }  // namespace fdtd

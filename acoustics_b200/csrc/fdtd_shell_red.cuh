@@ -53,20 +53,9 @@ namespace fdtd {
 // consecutive words of its own (no bank conflict, no barrier: every thread
 // reads back only what it copied).
 constexpr int RED_NVEC = 10, RED_NSCA = 3;
-__device__ __forceinline__ int threadIdx_lin() { return threadIdx.x + 32 * threadIdx.y; }
 __host__ __device__ constexpr int red_stage_bytes() { return 256 * (RED_NVEC * 4 * shell_vz(4) + RED_NSCA * 4); }
 __host__ __device__ constexpr int red_smem_bytes() {
     return FDTD_SHELL_RED_STAGES > 0 ? FDTD_SHELL_RED_STAGES * red_stage_bytes() : 0;
-}
-
-template <int BYTES>
-__device__ __forceinline__ void cpa(unsigned saddr, const void* g) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(saddr), "l"(g), "n"(BYTES) : "memory");
-}
-__device__ __forceinline__ void cpa_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cpa_wait() {
-    asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 // Loads of one x plane of a reduced-state shell column.
