@@ -36,6 +36,14 @@ cudaError_t prepare_fp32_kernels() {
     cudaError_t e = cudaFuncSetAttribute(k_pml_shell_tma<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                          TMA_STAGES * 24 * 1024 + 16 * TMA_STAGES);
     if (e != cudaSuccess) return e;
+    if (shell_smem_bytes<float>() > 0) {
+        e = cudaFuncSetAttribute(k_pml_shell<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 shell_smem_bytes<float>());
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k_batch_shell<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     shell_smem_bytes<float>());
+        if (e != cudaSuccess) return e;
+    }
     if (red_smem_bytes() > 0) {
         e = cudaFuncSetAttribute(k_pml_shell_red<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, red_smem_bytes());
         if (e == cudaSuccess)

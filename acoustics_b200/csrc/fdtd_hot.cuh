@@ -245,15 +245,17 @@ __device__ __forceinline__ void cpa_wait() {
     asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
-// x planes of the full-state shell (FP64) whose loads a thread keeps in flight
-// through a shared-memory ring; 0: the register prefetch of FDTD_SHELL_PREFETCH.
-// FP32 full-state tiles keep the register prefetch.
+// x planes of the full-state shell whose loads a thread keeps in flight through
+// a shared-memory ring; 0: the register prefetch of FDTD_SHELL_PREFETCH.
 #ifndef FDTD_SHELL_F64_STAGES
 #define FDTD_SHELL_F64_STAGES 3
 #endif
+#ifndef FDTD_SHELL_F32_STAGES
+#define FDTD_SHELL_F32_STAGES 0
+#endif
 template <typename T>
 __host__ __device__ constexpr int shell_full_stages() {
-    return sizeof(T) == 8 ? FDTD_SHELL_F64_STAGES : 0;
+    return sizeof(T) == 8 ? FDTD_SHELL_F64_STAGES : FDTD_SHELL_F32_STAGES;
 }
 // one stage: ten vector fields and three scalar fields, each over the CTA's 256 threads
 template <typename T>
