@@ -3,9 +3,9 @@
 //
 // Every member keeps its own device state (the arrays of its fdtd_solver); a
 // descriptor per member holds its kernel arguments for both buffer parities,
-// its boxes, its listener ring and its current parity, which the last kernel
-// of a step flips.  Because the step constants live on the device, a captured
-// graph of an even number of batched steps replays for any step index.
+// its boxes, its listener ring and its parity in that table.  Because the step
+// constants live on the device, a captured graph of an even number of batched
+// steps replays for any step index.
 //
 // Per step:  k_batch_ghost (third stream)  ||  k_batch_interior (second stream)
 //            ||  k_batch_shell_red / k_batch_shell (PML tiles of the members with
@@ -15,9 +15,10 @@
 // The descriptors come in two tables, one per step parity (every member's
 // parity flips each step), so consecutive steps alternate tables and no kernel
 // flips parities on the device.
-// The shell and interior kernels run one CTA per entry of a tile table that
-// lists the tiles of every member (sorted by member), and call the same tile
-// functions as the single-solve kernels.
+// The shell kernels run one CTA per entry of a tile table that lists the tiles
+// of every member (sorted by member); the interior kernel finds its members'
+// arguments in its parameter bank (up to BATCH_PARAM_MEMBERS members, else a
+// tile table too).  Both call the same tile functions as the single-solve kernels.
 #pragma once
 #include "fdtd_device.cuh"
 #include "fdtd_hot.cuh"
@@ -30,8 +31,9 @@ namespace fdtd {
 #define FDTD_BATCH_INT_TILES 4
 #endif
 
-// FDTD_BATCH_INT_TILES consecutive interior tiles per CTA.  The tiles are sorted
-// by member, so a CTA copies its member's arguments into registers once for the
+// The tile-table interior (more members than the parameter-bank table holds):
+// FDTD_BATCH_INT_TILES consecutive tiles per CTA.  The tiles are sorted by
+// member, so a CTA copies its member's arguments into registers once for the
 // tiles that share it: only the first waits on the chain tile -> descriptor ->
 // arguments before its data loads can issue.
 #ifndef FDTD_BATCH_INT_MINB
