@@ -593,8 +593,12 @@ __global__ void __launch_bounds__(256, shell_min_blocks(sizeof(T))) k_pml_shell(
 namespace fdtd {
 
 // Host side: one region-split step (streams: StepStreams).  Launch order: the
-// ghost-cell list (s3), the interior (s2), the shell (s), then the sources (s2,
-// after the interior and the ghost list, whose cells they add to).
+// ghost-cell list (s3), the interior (s2), the shell (s) (FP64: the shell before
+// the interior), then the sources (s2, after the interior and the ghost list,
+// whose cells they add to).
+#ifndef FDTD_SHELL_FIRST_F64
+#define FDTD_SHELL_FIRST_F64 1
+#endif
 template <typename T>
 cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const RegionLaunch& R, int cur,
                            const StepStreams& S, int* launches) {
@@ -633,16 +637,24 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
         ++l;
     }
     if (gside && (e = cudaEventRecord(S.ghost, S.s3)) != cudaSuccess) return e;
-    if (has_interior) {
-        dim3 block(32, 8);
-        const int xb = (!hP.visc && (R.xb == 4 || R.xb == 8)) ? R.xb : 2;
-        dim3 grid(interior_unit_tiles(b, 16 / (int)sizeof(T)), (nx + xb - 1) / xb);
-        if (hP.visc) k_interior<T, 2, true><<<grid, block, 0, si>>>(A, b);
-        else if (xb == 2) k_interior<T, 2><<<grid, block, 0, si>>>(A, b);
-        else if (xb == 8) k_interior<T, 8><<<grid, block, 0, si>>>(A, b);
-        else k_interior<T, 4><<<grid, block, 0, si>>>(A, b);
-        ++l;
-    }
+    // FP64: the shell first.  A shell CTA (188 registers, the 141 KB ring) takes
+    // one per SM and leaves the registers of one interior CTA beside it, which
+    // the interior's CTAs, dispatched after, fill; FP32 CTAs of the two kernels
+    // do not fit one SM together, and the interior goes first.
+    constexpr bool shell_first = sizeof(T) == 8 && FDTD_SHELL_FIRST_F64;
+    auto launch_interior = [&]() {
+        if (has_interior) {
+            dim3 block(32, 8);
+            const int xb = (!hP.visc && (R.xb == 4 || R.xb == 8)) ? R.xb : 2;
+            dim3 grid(interior_unit_tiles(b, 16 / (int)sizeof(T)), (nx + xb - 1) / xb);
+            if (hP.visc) k_interior<T, 2, true><<<grid, block, 0, si>>>(A, b);
+            else if (xb == 2) k_interior<T, 2><<<grid, block, 0, si>>>(A, b);
+            else if (xb == 8) k_interior<T, 8><<<grid, block, 0, si>>>(A, b);
+            else k_interior<T, 4><<<grid, block, 0, si>>>(A, b);
+            ++l;
+        }
+    };
+    if (!shell_first) launch_interior();
     const int nblk = (R.skip & 2) ? 0 : R.shell.block_first[R.shell.n];
     if (nblk > 0) {
         if constexpr (sizeof(T) == 4) {
@@ -656,6 +668,7 @@ cudaError_t launch_regions(const SolveParams* dP, const SolveParams& hP, const R
         }
         ++l;
     }
+    if (shell_first) launch_interior();
     if (gside && (e = cudaStreamWaitEvent(S.s2, S.ghost, 0)) != cudaSuccess) return e;
     if (R.sources) {
         // source cells are non-PML cells: after the interior and ghost updates of
